@@ -1,0 +1,713 @@
+/*
+ * ozoracle.c — CPU restatement of the OzBLAS Ozaki-scheme path (FP64 in/out,
+ * FP64 slices, reproMode=1, no batched GEMM), an exact dot-product
+ * accumulator, and the seeded input generators.
+ *
+ * TEST INFRASTRUCTURE ONLY: the checker for the parity tests, never the
+ * thing measured or shipped.  Parity of this restatement with the reference
+ * library itself is pinned by tests/test_oracle.py (live, against oracle/_ref)
+ * and by the golden fixtures in tests/golden (generated from oracle/_ref).
+ *
+ * Citations are to mukunoki/ozblas, paths relative to the project root.
+ * Compile with -ffp-contract=off: every a*b+c below is meant to round twice
+ * unless it is written as fma().
+ */
+#define _GNU_SOURCE
+#include "ozoracle.h"
+
+#include <math.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+
+#define OZ_DEFAULT_MAXSPLIT 30 /* NumSplitDefaultMax, src/cpu/ozblas_common.h:5 */
+#define OZ_SPLIT_CONST 0.75    /* CONST, src/cpu/ozblas_split.cpp:9 */
+
+static int oz_max_split(const oz_flags *f) { return f->nSplitMax > 0 ? f->nSplitMax : OZ_DEFAULT_MAXSPLIT; }
+
+/* std::max(a, b) as the reference uses it: returns a unless a < b. */
+static inline double ref_max(double a, double b) { return (a < b) ? b : a; }
+
+/* getRho<double,double>, src/cpu/ozblas_split.cpp:19-34 */
+int oz_rho(int dim, int splitEpsMode) {
+    switch (splitEpsMode) {
+    case 2: return (int)ceil((53 - (106 - log2(1. * dim)) / 2));
+    case 9: return (int)ceil((53 - (53 - log2(2. * sqrt(dim))) / 2));
+    default: return (int)ceil((53 - (53 - log2(1. * dim)) / 2));
+    }
+}
+
+/* tau = (short)ceil(log2(|max|)), src/cpu/ozblas_split.cpp:145,801 */
+int oz_tau_libm(double v) {
+    const short tau = (short)ceil(log2(fabs(v)));
+    return tau;
+}
+
+/*
+ * One split level over ncol columns of length k (mono precision):
+ * src/cpu/ozblas_split.cpp:126-178 (column panel) and :62-103 (vector, same
+ * arithmetic with one column).  R holds the running remainders; S receives
+ * the slice; mx holds the per-column max of R on entry and of the new
+ * remainder on exit.  Returns the sum of the new maxima (the termination test).
+ */
+static double split_level_cols(int k, int ncol, int rho, double *R, int ldr, double *S, int lds, double *mx,
+                               int shift) {
+    double check = 0.;
+    for (int j = 0; j < ncol; j++) {
+        const short tau = (short)ceil(log2(fabs(mx[j])));
+        const double sigma = OZ_SPLIT_CONST * scalbn(1., rho + tau) * shift;
+        double m = 0.;
+        for (int i = 0; i < k; i++) {
+            double x = R[(size_t)j * ldr + i];
+            const double s = (x + sigma) - sigma;
+            x = x - s;
+            S[(size_t)j * lds + i] = s;
+            R[(size_t)j * ldr + i] = x;
+            m = ref_max(m, fabs(x));
+        }
+        mx[j] = m;
+        check += m;
+    }
+    return check;
+}
+
+/*
+ * Column-panel split driver, src/cpu/ozblas_split.cpp:254-289 (reproMode=1):
+ * level 0 always runs, then levels 1.. until one leaves an all-zero
+ * remainder (that level is counted) or maxS levels exist.  slices holds
+ * maxS panels of lds x ncol.  Returns the split count.
+ */
+int oz_split_cols(const oz_flags *f, int k, int ncol, const double *X, int ldx, int shift, double *slices,
+                  int lds) {
+    const int rho = oz_rho(k, f->splitEpsMode);
+    const int maxS = oz_max_split(f);
+    double *R = (double *)malloc(sizeof(double) * (size_t)(k > 0 ? k : 1) * (ncol > 0 ? ncol : 1));
+    double *mx = (double *)malloc(sizeof(double) * (ncol > 0 ? ncol : 1));
+    for (int j = 0; j < ncol; j++) {
+        double m = 0.;
+        for (int i = 0; i < k; i++) {
+            R[(size_t)j * k + i] = X[(size_t)j * ldx + i];
+            m = ref_max(m, fabs(X[(size_t)j * ldx + i]));
+        }
+        mx[j] = m;
+    }
+    split_level_cols(k, ncol, rho, R, k, slices, lds, mx, shift);
+    int s = 1;
+    while (s < maxS) {
+        const double c = split_level_cols(k, ncol, rho, R, k, slices + (size_t)s * lds * ncol, lds, mx, shift);
+        s++;
+        if (c == 0.) break;
+    }
+    free(R);
+    free(mx);
+    return s;
+}
+
+/*
+ * One split level over CSR rows: src/cpu/ozblas_split.cpp:779-815.
+ * rho comes from the row's nnz; sigma is divided (not multiplied) by shift.
+ */
+static double split_level_csr(int m, const int *rowptr, int epsmode, double *R, double *S, double *mx, int shift) {
+    double check = 0.;
+    for (int r = 0; r < m; r++) {
+        const int lo = rowptr[r], hi = rowptr[r + 1];
+        if (hi <= lo) { /* an empty row keeps max 0 and writes nothing */
+            mx[r] = 0.;
+            continue;
+        }
+        const int rho = oz_rho(hi - lo, epsmode);
+        const short tau = (short)ceil(log2(mx[r]));
+        const double sigma = OZ_SPLIT_CONST * scalbn(1., rho + tau) / shift;
+        double mm = 0.;
+        for (int i = lo; i < hi; i++) {
+            double x = R[i];
+            const double s = (x + sigma) - sigma;
+            x = x - s;
+            S[i] = s;
+            R[i] = x;
+            mm = ref_max(mm, fabs(x));
+        }
+        mx[r] = mm;
+        check += mm;
+    }
+    return check;
+}
+
+/* CSR row split driver, src/cpu/ozblas_split.cpp:875-928.  slices: maxS x lds. */
+int oz_split_rows_csr(const oz_flags *f, int m, const double *val, const int *rowptr, int shift, double *slices,
+                      int lds) {
+    const int maxS = oz_max_split(f);
+    const int nnz = rowptr[m] - rowptr[0];
+    double *R = (double *)malloc(sizeof(double) * (size_t)(rowptr[m] > 0 ? rowptr[m] : 1));
+    double *mx = (double *)malloc(sizeof(double) * (m > 0 ? m : 1));
+    (void)nnz;
+    for (int r = 0; r < m; r++) {
+        double mm = 0.;
+        for (int i = rowptr[r]; i < rowptr[r + 1]; i++) {
+            R[i] = val[i];
+            mm = ref_max(mm, fabs(val[i]));
+        }
+        mx[r] = mm;
+    }
+    for (int i = 0; i < rowptr[m]; i++) slices[i] = 0.;
+    split_level_csr(m, rowptr, f->splitEpsMode, R, slices, mx, shift);
+    int s = 1;
+    while (s < maxS) {
+        const double c = split_level_csr(m, rowptr, f->splitEpsMode, R, slices + (size_t)s * lds, mx, shift);
+        s++;
+        if (c == 0.) break;
+    }
+    free(R);
+    free(mx);
+    return s;
+}
+
+/* ------------------------------------------------------------------------ */
+/* NearSum (Rump, Ogita, Oishi), src/cpu/ozblas_sum.cpp:10-112               */
+/* ------------------------------------------------------------------------ */
+
+static void nearsum_transform(int n, double *v, double rho, double *tau1, double *tau2) {
+    const int emin = -1022, epse = 53; /* getEmin/getEpse<double>, src/cpu/ozblas_common.h */
+    if (n == 0) {
+        *tau1 = rho;
+        *tau2 = 0.;
+        return;
+    }
+    double mu = fabs(v[0]);
+    for (int i = 1; i < n; i++) mu = (mu > fabs(v[i])) ? mu : fabs(v[i]); /* MAX macro */
+    if (mu == 0.) {
+        *tau1 = rho;
+        *tau2 = 0.;
+        return;
+    }
+    const int M = (int)ceil(log2((double)(n + 2)));
+    double sigma = scalbn(1., (int)(M + ceil(log2(mu))));
+    double t = rho;
+    for (;;) {
+        double tau = 0.;
+        for (int i = 0; i < n; i++) {
+            const double tmp = (sigma + v[i]) - sigma;
+            v[i] -= tmp;
+            tau += tmp;
+        }
+        *tau1 = t + tau;
+        if ((sigma <= scalbn(1., emin)) || (fabs(*tau1) >= scalbn(1., 2 * M + 1 - epse) * sigma)) {
+            *tau2 = tau - (*tau1 - t);
+            return;
+        }
+        sigma = scalbn(1., M - epse) * sigma;
+        t = *tau1;
+    }
+}
+
+static void nearsum_transformk(int n, double *v, double rho, double *res, double *r) {
+    double tmp = 0., tau1, tau2;
+    nearsum_transform(n, v, rho, &tau1, &tau2);
+    for (int i = 0; i < n; i++) tmp += v[i];
+    *res = tau1 + (tau2 + tmp);
+    *r = tau2 - (*res - tau1);
+}
+
+static inline double ref_sign(double v) { return (v < 0) ? -1. : 1.; }
+
+double oz_nearsum(int n, double *vec) {
+    const double eps = scalbn(1., -53);
+    double res, r, delta, r2, res2, mu, delta2, tmp;
+    nearsum_transformk(n, vec, 0., &res, &r);
+    nearsum_transformk(n, vec, r, &delta, &r2);
+    if (delta == 0) return res;
+    res2 = res + ref_sign(delta) * eps * fabs(res);
+    if (res2 == res) {
+        mu = ref_sign(delta) * eps * fabs(res);
+        res2 = res + 2. * ref_sign(delta) * eps * fabs(res);
+    } else {
+        mu = (res2 - res) / 2.;
+    }
+    if (fabs(delta) < fabs(mu)) return res;
+    if (fabs(delta) > fabs(mu)) return res2;
+    nearsum_transformk(n, vec, r2, &delta2, &tmp);
+    if (delta2 == 0) return res + mu;
+    if (ref_sign(delta2) == ref_sign(mu)) return res2;
+    return res;
+}
+
+/* ------------------------------------------------------------------------ */
+/* GEMM driver, src/cpu/ozblas_gemm.cpp:3-315 (no m/n blocking)              */
+/* ------------------------------------------------------------------------ */
+
+static int imax(int a, int b) { return a > b ? a : b; }
+static int imin(int a, int b) { return a < b ? a : b; }
+
+/* Pair schedule: ik ascending, ia ascending, ib = ik - ia
+ * (src/cpu/ozblas_gemm.cpp:237-243 and the sum loops of ozblas_sum.cpp:340-360). */
+static int make_pairs(int nA, int nB, int maxlevel, int *pa, int *pb) {
+    int np = 0;
+    for (int ik = 0; ik <= maxlevel; ik++)
+        for (int ia = 0; ia < nA; ia++)
+            for (int ib = 0; ib < nB; ib++)
+                if (ia + ib == ik) {
+                    pa[np] = ia;
+                    pb[np] = ib;
+                    np++;
+                }
+    return np;
+}
+
+int oz_dgemm(const oz_flags *f, char ta, char tb, int m, int n, int k, double alpha, const double *A, int lda,
+             const double *B, int ldb, double beta, double *C, int ldc, oz_info *info) {
+    if (f->reproMode != 1) return -1;
+    const int is_dot = (m == 1 && n == 1);
+    const int fast = is_dot ? 0 : f->fastMode; /* src/cpu/ozblas_gemm.cpp:26-29 */
+    const int maxS = oz_max_split(f);
+    const int kk = k > 0 ? k : 1;
+    /* column panels: column i of Ap is row i of op(A); column j of Bp is column j of op(B) */
+    double *Ap = (double *)malloc(sizeof(double) * (size_t)kk * imax(m, 1));
+    double *Bp = (double *)malloc(sizeof(double) * (size_t)kk * imax(n, 1));
+    const int tA = !(ta == 'n' || ta == 'N'), tB = !(tb == 'n' || tb == 'N');
+    for (int i = 0; i < m; i++)
+        for (int l = 0; l < k; l++) Ap[(size_t)i * k + l] = tA ? A[(size_t)i * lda + l] : A[(size_t)l * lda + i];
+    for (int j = 0; j < n; j++)
+        for (int l = 0; l < k; l++) Bp[(size_t)j * k + l] = tB ? B[(size_t)l * ldb + j] : B[(size_t)j * ldb + l];
+    double *Sa = (double *)calloc((size_t)(maxS + 1) * kk * imax(m, 1), sizeof(double));
+    double *Sb = (double *)calloc((size_t)(maxS + 1) * kk * imax(n, 1), sizeof(double));
+    const int nA = oz_split_cols(f, k, m, Ap, k, 1, Sa, k);
+    const int nB = oz_split_cols(f, k, n, Bp, k, 1, Sb, k);
+    int maxlevel = (nA - 1) + (nB - 1);
+    maxlevel = imax(maxlevel - fast, imin(nA - 1, nB - 1)); /* src/cpu/ozblas_gemm.cpp:163-164 */
+    int *pa = (int *)malloc(sizeof(int) * nA * nB), *pb = (int *)malloc(sizeof(int) * nA * nB);
+    const int np = make_pairs(nA, nB, maxlevel, pa, pb);
+    double *terms = (double *)malloc(sizeof(double) * (np > 0 ? np : 1));
+    for (int j = 0; j < n; j++) {
+        for (int i = 0; i < m; i++) {
+            for (int p = 0; p < np; p++) {
+                const double *a = Sa + (size_t)pa[p] * k * m + (size_t)i * k;
+                const double *b = Sb + (size_t)pb[p] * k * n + (size_t)j * k;
+                double s = 0.;
+                for (int l = 0; l < k; l++) s += a[l] * b[l]; /* exact: any order gives these bits */
+                terms[p] = s;
+            }
+            double t = 0.;
+            if (f->sumMode == 1) {
+                t = oz_nearsum(np, terms);
+            } else {
+                for (int p = 0; p < np; p++) t += terms[p];
+            }
+            double *c = &C[(size_t)j * ldc + i];
+            *c = fma(alpha, t, (beta * *c)); /* src/cpu/ozblas_sum.cpp:366 */
+        }
+    }
+    if (info) {
+        info->nSplitA = (float)nA;
+        info->nSplitB = (float)nB;
+        if (is_dot)
+            info->nSplitC = 1.f;
+        else if (n == 1 && fast == 0)
+            info->nSplitC = (float)imin(maxlevel + 1, nA);
+        else
+            info->nSplitC = (float)np;
+    }
+    free(Ap);
+    free(Bp);
+    free(Sa);
+    free(Sb);
+    free(pa);
+    free(pb);
+    free(terms);
+    return 0;
+}
+
+/* DOT = GEMM('t','n',1,1,n) into a zero-initialised result, src/cpu/ozblas_dot.cpp:4-39 */
+double oz_ddot(const oz_flags *f, int n, const double *x, const double *y, oz_info *info) {
+    double ret = 0.;
+    oz_dgemm(f, 't', 'n', 1, 1, n, 1., x, n, y, n, 0., &ret, 1, info);
+    return ret;
+}
+
+/* NRM2 = sqrt(DOT(x,x)) on the host, src/cpu/ozblas_nrm2.cpp:3-31 */
+double oz_dnrm2(const oz_flags *f, int n, const double *x, oz_info *info) { return sqrt(oz_ddot(f, n, x, x, info)); }
+
+/* GEMV through GEMM with n=1, src/cpu/ozblas_gemv.cpp:4-30 */
+int oz_dgemv(const oz_flags *f, char ta, int m, int n, double alpha, const double *A, int lda, const double *x,
+             double beta, double *y, oz_info *info) {
+    if (ta == 'n' || ta == 'N') return oz_dgemm(f, 'n', 'n', m, 1, n, alpha, A, lda, x, n, beta, y, m, info);
+    return oz_dgemm(f, 't', 'n', n, 1, m, alpha, A, lda, x, m, beta, y, n, info);
+}
+
+/* ------------------------------------------------------------------------ */
+/* CSRMV, src/cpu/ozblas_csrmv.cpp:3-181, CSRMM src/cpu/ozblas_blas_wrapper.cpp:231-255 */
+/* ------------------------------------------------------------------------ */
+
+int oz_dcsrmv_presplit(const oz_flags *f, int m, int n, int nnz, double alpha, const double *aslices, int nA,
+                       int lds, const int *colind, const int *rowptr, const double *x, double beta, double *y,
+                       oz_info *info) {
+    const int maxS = oz_max_split(f);
+    const int nn = n > 0 ? n : 1;
+    double *Sx = (double *)calloc((size_t)(maxS + 1) * nn, sizeof(double));
+    const int nB = oz_split_cols(f, n, 1, x, n, 1, Sx, n); /* x: vector split, rho from n */
+    int maxlevel = (nA - 1) + (nB - 1);
+    maxlevel = imax(maxlevel - f->fastMode, imin(nA - 1, nB - 1));
+    int *pa = (int *)malloc(sizeof(int) * nA * nB), *pb = (int *)malloc(sizeof(int) * nA * nB);
+    const int np = make_pairs(nA, nB, maxlevel, pa, pb);
+    double *terms = (double *)malloc(sizeof(double) * (np > 0 ? np : 1));
+    for (int r = 0; r < m; r++) {
+        for (int p = 0; p < np; p++) {
+            const double *a = aslices + (size_t)pa[p] * lds;
+            const double *xs = Sx + (size_t)pb[p] * n;
+            double tr = 0.;
+            for (int i = rowptr[r]; i < rowptr[r + 1]; i++) tr = fma(a[i], xs[colind[i]], tr);
+            terms[p] = tr; /* alpha = 1, beta = 0 inside the slice CSRMM: C = 1 * tr */
+        }
+        double t = 0.;
+        if (f->sumMode == 1)
+            t = oz_nearsum(np, terms);
+        else
+            for (int p = 0; p < np; p++) t += terms[p];
+        y[r] = fma(alpha, t, (beta * y[r]));
+    }
+    if (info) {
+        int ic = 0;
+        for (int ia = 0; ia < imin(maxlevel + 1, nA); ia++) ic += imin(nB, maxlevel + 1 - ia);
+        info->nSplitA = (float)nA;
+        info->nSplitB = (float)nB;
+        info->nSplitC = (float)ic;
+    }
+    free(Sx);
+    free(pa);
+    free(pb);
+    free(terms);
+    (void)nnz;
+    return 0;
+}
+
+int oz_dcsrmv(const oz_flags *f, int m, int n, int nnz, double alpha, const double *val, const int *colind,
+              const int *rowptr, const double *x, double beta, double *y, oz_info *info) {
+    const int maxS = oz_max_split(f);
+    const int lds = nnz > 0 ? nnz : 1;
+    double *Sa = (double *)calloc((size_t)(maxS + 1) * lds, sizeof(double));
+    const int nA = oz_split_rows_csr(f, m, val, rowptr, 1, Sa, lds);
+    const int rc = oz_dcsrmv_presplit(f, m, n, nnz, alpha, Sa, nA, lds, colind, rowptr, x, beta, y, info);
+    free(Sa);
+    return rc;
+}
+
+/* SplitA with splitShift tuning, src/cpu/ozblas_csrmv.cpp:185-271 */
+int oz_dcsrmv_split_a(const oz_flags *f, int m, int nnz, const double *val, const int *rowptr, double *aslices,
+                      int lds, int *nsplit_out, int *shift_out) {
+    int s = oz_split_rows_csr(f, m, val, rowptr, 1, aslices, lds);
+    int shift = 1;
+    if (f->nSplitMax == 0) {
+        int sold;
+        shift = 1;
+        do {
+            sold = s;
+            shift *= 2;
+            s = oz_split_rows_csr(f, m, val, rowptr, shift, aslices, lds);
+        } while (sold == s && shift < 512);
+        if (sold == s) shift = 1;
+        s = oz_split_rows_csr(f, m, val, rowptr, shift, aslices, lds);
+    }
+    (void)nnz;
+    *nsplit_out = s;
+    *shift_out = shift;
+    return 0;
+}
+
+/* Unpreconditioned CG, src/cpu/ozblas_cg.cpp:23-128 (verbose=1: history every iteration) */
+int oz_dcg(const oz_flags *f, int n, int nnz, const double *val, const int *colind, const int *rowptr,
+           const double *b, double *x, int maxiter, double tol, double *hist, oz_info *info) {
+    const int maxS = oz_max_split(f);
+    const int lds = nnz > 0 ? nnz : 1;
+    double *Sa = (double *)calloc((size_t)(maxS + 1) * lds, sizeof(double));
+    int nA, shift;
+    oz_dcsrmv_split_a(f, n, nnz, val, rowptr, Sa, lds, &nA, &shift);
+    double *r = (double *)malloc(sizeof(double) * n), *p = (double *)malloc(sizeof(double) * n);
+    double *q = (double *)calloc(n, sizeof(double));
+    const double nrmb = oz_dnrm2(f, n, b, NULL);
+    memcpy(r, b, sizeof(double) * n);
+    oz_dcsrmv_presplit(f, n, n, nnz, -1., Sa, nA, lds, colind, rowptr, x, 1., r, NULL);
+    double dold = oz_ddot(f, n, r, r, NULL);
+    double resi = sqrt(dold);
+    int cnt = 0;
+    if (hist) hist[cnt] = resi / nrmb;
+    cnt++;
+    memcpy(p, r, sizeof(double) * n);
+    int it = 0;
+    while (it < maxiter) {
+        it++;
+        oz_dcsrmv_presplit(f, n, n, nnz, 1., Sa, nA, lds, colind, rowptr, p, 0., q, NULL);
+        const double tmp = oz_ddot(f, n, p, q, NULL);
+        const double alpha = dold / tmp;
+        for (int i = 0; i < n; i++) x[i] = fma(alpha, p[i], x[i]);
+        for (int i = 0; i < n; i++) r[i] = fma(-alpha, q[i], r[i]);
+        const double dnew = oz_ddot(f, n, r, r, NULL);
+        resi = sqrt(dnew);
+        const double beta = dnew / dold;
+        dold = dnew;
+        for (int i = 0; i < n; i++) p[i] = beta * p[i];
+        for (int i = 0; i < n; i++) p[i] = fma(1., r[i], p[i]);
+        if (hist) hist[cnt] = resi / nrmb;
+        cnt++;
+        if (resi / nrmb < tol) break;
+    }
+    if (info) {
+        info->cg_numiter = it;
+        info->splitShift = shift;
+        info->nSplitA_ = nA;
+    }
+    free(Sa);
+    free(r);
+    free(p);
+    free(q);
+    return 0;
+}
+
+/* ------------------------------------------------------------------------ */
+/* Exact accumulation (own code; the error oracle)                          */
+/* ------------------------------------------------------------------------ */
+
+/* value = sum_i limb[i] * 2^(32 i - ACC_OFF); products of doubles reach 2^-2148 */
+#define ACC_OFF 2208
+#define ACC_LIMBS 140
+
+typedef struct {
+    int64_t d[ACC_LIMBS];
+    long adds;
+    int special; /* nonzero if an inf/nan term was seen */
+} acc_t;
+
+static void acc_init(acc_t *a) {
+    memset(a->d, 0, sizeof(a->d));
+    a->adds = 0;
+    a->special = 0;
+}
+
+static void acc_norm(acc_t *a) {
+    for (int i = 0; i < ACC_LIMBS - 1; i++) {
+        const int64_t c = a->d[i] >> 32; /* arithmetic shift: floor division */
+        a->d[i] -= c * ((int64_t)1 << 32);
+        a->d[i + 1] += c;
+    }
+    a->adds = 0;
+}
+
+/* add sign * mag * 2^e (mag < 2^112) */
+static void acc_add_mag(acc_t *a, int sign, unsigned __int128 mag, int e) {
+    if (mag == 0) return;
+    int pos = e + ACC_OFF;
+    int li = pos >> 5, sh = pos & 31;
+    /* spread over up to 5 limbs */
+    unsigned __int128 lo = mag << sh; /* mag < 2^112, sh < 32 -> fits 144 bits? keep two parts */
+    unsigned __int128 hi = (sh == 0) ? 0 : (mag >> (128 - sh));
+    uint32_t parts[8];
+    for (int t = 0; t < 4; t++) parts[t] = (uint32_t)(lo >> (32 * t));
+    parts[4] = (uint32_t)hi;
+    for (int t = 0; t < 5; t++) {
+        if (li + t >= ACC_LIMBS) break;
+        a->d[li + t] += sign > 0 ? (int64_t)parts[t] : -(int64_t)parts[t];
+    }
+    if (++a->adds >= (1L << 29)) acc_norm(a);
+}
+
+/* split a finite double into sign, 53-bit integer mantissa and exponent of its lsb */
+static int dbl_parts(double v, int *sign, uint64_t *mant, int *e) {
+    uint64_t b;
+    memcpy(&b, &v, 8);
+    *sign = (b >> 63) ? -1 : 1;
+    const int be = (int)((b >> 52) & 0x7ff);
+    const uint64_t fr = b & ((1ULL << 52) - 1);
+    if (be == 0x7ff) return -1;
+    if (be == 0) {
+        *mant = fr;
+        *e = -1074;
+    } else {
+        *mant = fr | (1ULL << 52);
+        *e = be - 1075;
+    }
+    return 0;
+}
+
+static void acc_add_prod(acc_t *a, double x, double y) {
+    int sx, sy, ex, ey;
+    uint64_t mx, my;
+    if (dbl_parts(x, &sx, &mx, &ex) || dbl_parts(y, &sy, &my, &ey)) {
+        a->special = 1;
+        return;
+    }
+    acc_add_mag(a, sx * sy, (unsigned __int128)mx * my, ex + ey);
+}
+
+static void acc_add_dbl(acc_t *a, double x) {
+    int s, e;
+    uint64_t mt;
+    if (dbl_parts(x, &s, &mt, &e)) {
+        a->special = 1;
+        return;
+    }
+    acc_add_mag(a, s, (unsigned __int128)mt, e);
+}
+
+/* round the exact value to the nearest double, ties to even */
+static double acc_round(acc_t *a0) {
+    acc_t a = *a0;
+    if (a.special) return NAN;
+    acc_norm(&a);
+    int neg = a.d[ACC_LIMBS - 1] < 0;
+    if (neg) { /* two's complement negate of the multi-limb number (limbs are 32-bit digits after norm) */
+        int64_t carry = 1;
+        for (int i = 0; i < ACC_LIMBS; i++) {
+            int64_t v = (~a.d[i] & 0xffffffffLL) + carry;
+            carry = v >> 32;
+            a.d[i] = v & 0xffffffffLL;
+        }
+    }
+    int h = ACC_LIMBS - 1;
+    while (h >= 0 && a.d[h] == 0) h--;
+    if (h < 0) return 0.;
+    /* 96-bit window from limbs h, h-1, h-2 */
+    unsigned __int128 w = 0;
+    for (int t = 0; t < 3; t++) {
+        w <<= 32;
+        if (h - t >= 0) w |= (uint64_t)a.d[h - t];
+    }
+    int sticky = 0;
+    for (int i = h - 3; i >= 0; i--)
+        if (a.d[i]) {
+            sticky = 1;
+            break;
+        }
+    const int wlsb = 32 * (h - 2) - ACC_OFF; /* exponent of the window's lsb */
+    int msb = 127;
+    while (!((w >> msb) & 1)) msb--;
+    int drop = msb - 52; /* bits below the 53-bit mantissa */
+    int elsb = wlsb + drop;
+    if (elsb < -1074) { /* subnormal result */
+        drop += (-1074 - elsb);
+        elsb = -1074;
+    }
+    unsigned __int128 mant;
+    int round = 0, stk = sticky;
+    if (drop > 0) {
+        if (drop > 127) {
+            mant = 0;
+            round = 0;
+            stk = 1;
+        } else {
+            mant = w >> drop;
+            round = (int)((w >> (drop - 1)) & 1);
+            unsigned __int128 below = (drop >= 2) ? (w & (((unsigned __int128)1 << (drop - 1)) - 1)) : 0;
+            if (below) stk = 1;
+        }
+    } else {
+        mant = w << (-drop);
+    }
+    if (round && (stk || (mant & 1))) mant += 1;
+    double r = ldexp((double)(uint64_t)mant, elsb);
+    return neg ? -r : r;
+}
+
+double oz_exact_dot_rn(int n, const double *x, int incx, const double *y, int incy) {
+    acc_t *a = (acc_t *)malloc(sizeof(acc_t));
+    acc_init(a);
+    for (int i = 0; i < n; i++) acc_add_prod(a, x[(size_t)i * incx], y[(size_t)i * incy]);
+    const double r = acc_round(a);
+    free(a);
+    return r;
+}
+
+/* rn = RN(exact dot); relerr = |c - exact| / |exact| (0 when both are 0, inf when only exact is 0) */
+void oz_exact_dot_err(int n, const double *x, int incx, const double *y, int incy, double c, double *rn,
+                      double *relerr_exact) {
+    acc_t *a = (acc_t *)malloc(sizeof(acc_t));
+    acc_init(a);
+    for (int i = 0; i < n; i++) acc_add_prod(a, x[(size_t)i * incx], y[(size_t)i * incy]);
+    const double ex = acc_round(a);
+    acc_add_dbl(a, -c);
+    const double diff = acc_round(a);
+    *rn = ex;
+    if (ex == 0.)
+        *relerr_exact = (diff == 0.) ? 0. : INFINITY;
+    else
+        *relerr_exact = fabs(diff) / fabs(ex);
+    free(a);
+}
+
+double oz_exact_sum_rn(int n, const double *v) {
+    acc_t *a = (acc_t *)malloc(sizeof(acc_t));
+    acc_init(a);
+    for (int i = 0; i < n; i++) acc_add_dbl(a, v[i]);
+    const double r = acc_round(a);
+    free(a);
+    return r;
+}
+
+/* ------------------------------------------------------------------------ */
+/* Seeded inputs                                                            */
+/* ------------------------------------------------------------------------ */
+
+/* phi mode of mublasInitMat, testing/testing_common.cpp:703-717 (sequential drand48) */
+void oz_gen_phi(int m, int n, int ld, double *mat, double phi, int seed) {
+    if (ld < m) ld = m;
+    srand48(seed);
+    for (int j = 0; j < n; j++) {
+        for (int i = 0; i < m; i++) {
+            const double mu = 0.0, sigma = 1.0;
+            const double r1 = drand48();
+            const double r2 = drand48();
+            const double x1 = mu + (sqrt(-2. * log(r1)) * sin(2. * M_PI * r2)) * sigma;
+            const double val = (r1 - 0.5) * exp(phi * x1);
+            mat[(size_t)j * ld + i] = val;
+        }
+    }
+}
+
+/* N(0,1) by Box-Muller on drand48, one value per pair of draws */
+void oz_gen_normal(int n, double *x, int seed) {
+    srand48(seed);
+    for (int i = 0; i < n; i++) {
+        const double r1 = drand48();
+        const double r2 = drand48();
+        x[i] = sqrt(-2. * log(r1)) * sin(2. * M_PI * r2);
+    }
+}
+
+int64_t oz_stencil7_nnz(int nx, int ny, int nz) {
+    return 7LL * nx * ny * nz - 2LL * (ny * nz + nx * nz + nx * ny);
+}
+
+/* 7-point stencil on an nx*ny*nz grid, natural order (x fastest), ascending columns */
+void oz_gen_stencil7(int nx, int ny, int nz, int *rowptr, int *colind) {
+    int64_t p = 0;
+    int r = 0;
+    rowptr[0] = 0;
+    for (int z = 0; z < nz; z++)
+        for (int y = 0; y < ny; y++)
+            for (int x = 0; x < nx; x++, r++) {
+                if (z > 0) colind[p++] = r - nx * ny;
+                if (y > 0) colind[p++] = r - nx;
+                if (x > 0) colind[p++] = r - 1;
+                colind[p++] = r;
+                if (x < nx - 1) colind[p++] = r + 1;
+                if (y < ny - 1) colind[p++] = r + nx;
+                if (z < nz - 1) colind[p++] = r + nx * ny;
+                rowptr[r + 1] = (int)p;
+            }
+}
+
+/* Poisson values (6 on the diagonal, -1 off it) plus a 0.01*U(0,1) diagonal shift per row */
+void oz_gen_poisson_shift(int nx, int ny, int nz, int seed, const int *rowptr, const int *colind, double *val) {
+    const int n = nx * ny * nz;
+    srand48(seed);
+    for (int r = 0; r < n; r++) {
+        const double shift = 0.01 * drand48();
+        for (int i = rowptr[r]; i < rowptr[r + 1]; i++) val[i] = (colind[i] == r) ? 6.0 + shift : -1.0;
+    }
+}
+
+/* y = A x with a row-sequential fma chain (used to build b = A x_true) */
+void oz_csrmv_fma(int m, const double *val, const int *colind, const int *rowptr, const double *x, double *y) {
+    for (int r = 0; r < m; r++) {
+        double t = 0.;
+        for (int i = rowptr[r]; i < rowptr[r + 1]; i++) t = fma(val[i], x[colind[i]], t);
+        y[r] = t;
+    }
+}

@@ -1,0 +1,208 @@
+"""ozblas_b200 — B200 (sm_100a) Ozaki-scheme BLAS behind the cuozblas.h interface.
+
+Python view of the C ABI declared in ``include/cuozblas.h`` (ctypes over the
+in-tree ``libcuozblas_b200.so``).  Names and argument meanings follow the
+reference C++ API of mukunoki/ozblas (include/cuozblas.h:66-80):
+
+    h = Handle(work_bytes)                # cuozblasCreate
+    h.nSplitMax, h.sumMode, h.fastMode    # handle flags, same fields
+    dgemm(h, 'n', 'n', m, n, k, alpha, A, lda, B, ldb, beta, C, ldc)
+    ddot(h, n, x, y) -> float             # result on the host, like the reference
+    dnrm2, dgemv, daxpy, dcsrmv, dcsrmv_split_a, dcg, dgemm_i8
+
+Device arguments are CUDA tensors (torch) or raw device addresses (int).
+There is no CPU fallback: importing fails loudly when the library is missing.
+Errors are raised as ``OzblasError`` carrying the cuozblasStatus_t code
+(where the reference would have called exit(1)).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libcuozblas_b200.so")
+
+if not os.path.exists(LIB_PATH):
+    raise ImportError(
+        f"{LIB_PATH} is missing: build it with `python -m ozblas_b200.build` (nvcc, sm_100a). "
+        "ozblas_b200 has no CPU fallback.")
+
+_lib = C.CDLL(LIB_PATH)
+
+STATUS = {
+    0: "SUCCESS", 1: "NOT_INITIALIZED", 2: "INVALID_VALUE", 3: "WORKSPACE", 4: "NOT_SUPPORTED",
+    5: "INT32_BOUND", 6: "DEVICE_TIMEOUT", 7: "CUDA_ERROR",
+}
+
+
+class OzblasError(RuntimeError):
+    def __init__(self, fn, code):
+        super().__init__(f"{fn} failed: CUOZBLAS_STATUS_{STATUS.get(code, code)} ({code})")
+        self.code = code
+
+
+class HandleStruct(C.Structure):
+    """cuozblasHandle_t, field for field (mukunoki/ozblas include/cuozblas.h:7-63)."""
+    _fields_ = [
+        ("ch", C.c_void_p), ("csh", C.c_void_p),
+        ("devWork", C.c_void_p), ("devWorkCommon", C.c_void_p),
+        ("workSizeBytes", C.c_uint64), ("memAddr", C.c_uint64), ("nSplitMax", C.c_int32),
+        ("hstBatchAddr", C.c_void_p), ("devBatchAddr", C.c_void_p),
+        ("initialized", C.c_int32),
+        ("splitMode", C.c_int32), ("fastMode", C.c_int32), ("reproMode", C.c_int32), ("sumMode", C.c_int32),
+        ("useBatchedGemmFlag", C.c_int32), ("splitEpsMode", C.c_int32), ("precxFlag", C.c_int32),
+        ("nSplitA", C.c_float), ("nSplitB", C.c_float), ("nSplitC", C.c_float),
+        ("t_SplitA", C.c_float), ("t_SplitB", C.c_float), ("t_comp", C.c_float), ("t_sum", C.c_float),
+        ("t_total", C.c_float), ("n_comp", C.c_float), ("mbk", C.c_int32), ("nbk", C.c_int32),
+        ("nSplitA_", C.c_int32), ("splitShift", C.c_int32), ("memMaskSplitA", C.c_uint64),
+        ("trueresFlag", C.c_int32), ("verbose", C.c_int32), ("cg_numiter", C.c_int32),
+        ("cg_verbose1", C.c_void_p), ("cg_verbose2", C.c_void_p),
+        ("t_SplitMat_total", C.c_double), ("t_SplitVec_total", C.c_double), ("t_Sum_total", C.c_double),
+        ("t_AXPY_SCAL_total", C.c_double), ("t_DOT_NRM2_total", C.c_double), ("t_SpMV_SpMM_total", C.c_double),
+    ]
+
+
+_HP = C.POINTER(HandleStruct)
+_vp = C.c_void_p
+_i32 = C.c_int32
+_d = C.c_double
+_ch = C.c_char
+
+
+def _sig(name, args, res=C.c_int):
+    f = getattr(_lib, name)
+    f.argtypes = args
+    f.restype = res
+    return f
+
+
+_create = _sig("cuozblasHandleCreate", [_HP, C.c_uint64])
+_destroy = _sig("cuozblasHandleDestroy", [_HP])
+_setstream = _sig("cuozblasSetStream", [_HP, _vp])
+_ddot = _sig("cuozblasDdot", [_HP, _i32, _vp, _i32, _vp, _i32, C.POINTER(_d)])
+_dnrm2 = _sig("cuozblasDnrm2", [_HP, _i32, _vp, _i32, C.POINTER(_d)])
+_daxpy = _sig("cuozblasDaxpy", [_HP, _i32, _d, _vp, _i32, _vp, _i32])
+_dgemv = _sig("cuozblasDgemv", [_HP, _ch, _i32, _i32, _d, _vp, _i32, _vp, _i32, _d, _vp, _i32])
+_dgemm = _sig("cuozblasDgemm", [_HP, _ch, _ch, _i32, _i32, _i32, _d, _vp, _i32, _vp, _i32, _d, _vp, _i32])
+_dgemm_i8 = _sig("cuozblasDgemmI8", [_HP, _ch, _ch, _i32, _i32, _i32, _d, _vp, _i32, _vp, _i32, _d, _vp, _i32])
+_dcsrmv = _sig("cuozblasDcsrmv", [_HP, _ch, _i32, _i32, _i32, _d, _vp, _vp, _vp, _vp, _vp, _d, _vp])
+_dsplita = _sig("cuozblasDcsrmvSplitA", [_HP, _ch, _i32, _i32, _i32, _vp, _vp, _vp, C.POINTER(_vp)])
+_dcg = _sig("cuozblasDcg", [_HP, _ch, _i32, _i32, _vp, _vp, _vp, _vp, _vp, _vp, _i32, _d])
+rule_tau = _sig("cuozblasRuleTau", [_d])
+rule_rho = _sig("cuozblasRuleRho", [_i32, _i32])
+_version = _sig("cuozblasVersion", [], C.c_char_p)
+
+#: every C-ABI symbol include/cuozblas.h declares (checked by the CPU tests)
+C_ABI_SYMBOLS = [
+    "cuozblasHandleCreate", "cuozblasHandleDestroy", "cuozblasSetStream", "cuozblasDdot", "cuozblasDnrm2",
+    "cuozblasDaxpy", "cuozblasDgemv", "cuozblasDgemm", "cuozblasDcsrmv", "cuozblasDcsrmvSplitA", "cuozblasDcg",
+    "cuozblasDgemmI8", "cuozblasRuleTau", "cuozblasRuleRho", "cuozblasVersion",
+]
+
+
+def version() -> str:
+    return _version().decode()
+
+
+def _ptr(x):
+    if x is None:
+        return None
+    if isinstance(x, int):
+        return x
+    if hasattr(x, "data_ptr"):
+        if hasattr(x, "is_cuda") and not x.is_cuda:
+            raise ValueError("device tensor expected (x.is_cuda is False)")
+        return x.data_ptr()
+    raise TypeError(f"cannot take a device pointer of {type(x)}")
+
+
+def _chk(fn, code):
+    if code != 0:
+        raise OzblasError(fn, code)
+
+
+class Handle:
+    """cuozblasHandle_t owned from Python; attribute access reaches the C struct."""
+
+    def __init__(self, work_bytes: int = 4 << 30, stream=None):
+        object.__setattr__(self, "_h", HandleStruct())
+        _chk("cuozblasHandleCreate", _create(C.byref(self._h), int(work_bytes)))
+        if stream is not None:
+            self.set_stream(stream)
+
+    def set_stream(self, stream):
+        s = stream if isinstance(stream, int) else getattr(stream, "cuda_stream", stream)
+        _chk("cuozblasSetStream", _setstream(C.byref(self._h), s))
+
+    @property
+    def ref(self):
+        return C.byref(self._h)
+
+    def close(self):
+        if self._h.initialized:
+            _chk("cuozblasHandleDestroy", _destroy(C.byref(self._h)))
+
+    def __getattr__(self, name):
+        return getattr(object.__getattribute__(self, "_h"), name)
+
+    def __setattr__(self, name, value):
+        setattr(self._h, name, value)
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def dgemm(h, ta, tb, m, n, k, alpha, A, lda, B, ldb, beta, Cm, ldc):
+    _chk("cuozblasDgemm", _dgemm(h.ref, ta.encode(), tb.encode(), m, n, k, alpha, _ptr(A), lda, _ptr(B), ldb,
+                                 beta, _ptr(Cm), ldc))
+
+
+def dgemm_i8(h, ta, tb, m, n, k, alpha, A, lda, B, ldb, beta, Cm, ldc):
+    _chk("cuozblasDgemmI8", _dgemm_i8(h.ref, ta.encode(), tb.encode(), m, n, k, alpha, _ptr(A), lda, _ptr(B),
+                                      ldb, beta, _ptr(Cm), ldc))
+
+
+def ddot(h, n, x, y, incx=1, incy=1) -> float:
+    r = _d()
+    _chk("cuozblasDdot", _ddot(h.ref, n, _ptr(x), incx, _ptr(y), incy, C.byref(r)))
+    return r.value
+
+
+def dnrm2(h, n, x, incx=1) -> float:
+    r = _d()
+    _chk("cuozblasDnrm2", _dnrm2(h.ref, n, _ptr(x), incx, C.byref(r)))
+    return r.value
+
+
+def daxpy(h, n, alpha, x, y, incx=1, incy=1):
+    _chk("cuozblasDaxpy", _daxpy(h.ref, n, alpha, _ptr(x), incx, _ptr(y), incy))
+
+
+def dgemv(h, trans, m, n, alpha, A, lda, x, beta, y, incx=1, incy=1):
+    _chk("cuozblasDgemv", _dgemv(h.ref, trans.encode(), m, n, alpha, _ptr(A), lda, _ptr(x), incx, beta, _ptr(y),
+                                 incy))
+
+
+def dcsrmv(h, trans, m, n, nnz, alpha, val, colind, rowptr, x, beta, y, descr=None):
+    _chk("cuozblasDcsrmv", _dcsrmv(h.ref, trans.encode(), m, n, nnz, alpha, descr, _ptr(val), _ptr(colind),
+                                   _ptr(rowptr), _ptr(x), beta, _ptr(y)))
+
+
+def dcsrmv_split_a(h, trans, m, n, nnz, val, rowptr, descr=None) -> int:
+    out = _vp()
+    _chk("cuozblasDcsrmvSplitA", _dsplita(h.ref, trans.encode(), m, n, nnz, descr, _ptr(val), _ptr(rowptr),
+                                          C.byref(out)))
+    return out.value
+
+
+def dcg(h, trans, n, nnz, val, colind, rowptr, b, x, maxiter, tol, hist1=None, hist2=None, descr=None):
+    """CG; hist1/hist2 are host numpy float64 arrays of maxiter+1 entries (history per `h.verbose`)."""
+    h.cg_verbose1 = hist1.ctypes.data if hist1 is not None else None
+    h.cg_verbose2 = hist2.ctypes.data if hist2 is not None else None
+    _chk("cuozblasDcg", _dcg(h.ref, trans.encode(), n, nnz, descr, _ptr(val), _ptr(colind), _ptr(rowptr), _ptr(b),
+                             _ptr(x), maxiter, tol))
+    return h.cg_numiter

@@ -1,0 +1,353 @@
+// api.cu — the C ABI of include/cuozblas.h: handle lifecycle and the
+// BLAS-level entry points of the plain (FP64-slice) form.
+#include <math.h>
+#include <string.h>
+#include <sys/time.h>
+
+#include <new>
+
+#include "ozb_internal.h"
+
+namespace ozb {
+int launch_axpy(cuozblasHandle_t *h, int n, double alpha, const double *x, double *y);
+int launch_scal(cuozblasHandle_t *h, int n, double alpha, double *x);
+int launch_csrmv_plain(cuozblasHandle_t *h, int m, const double *val, const int *colind, const int *rowptr,
+                       const double *x, double alpha, double beta, double *y);
+int csrmv_presplit(cuozblasHandle_t *h, int m, int n, double alpha, const double *As, int nA, int64_t ld_s,
+                   const int *colind, const int *rowptr, const double *x, double beta, double *y);
+
+static double wall() {
+    struct timeval tv;
+    gettimeofday(&tv, nullptr);
+    return tv.tv_sec + tv.tv_usec * 1e-6;
+}
+
+int counter_init(cuozblasHandle_t *h) {
+    if (h == nullptr || h->initialized == 0 || state(h) == nullptr) return CUOZBLAS_STATUS_NOT_INITIALIZED;
+    h->splitShift = 1;
+    h->t_SplitA = h->t_SplitB = h->t_comp = h->t_sum = h->t_total = 0.f;
+    h->nSplitA = h->nSplitB = h->nSplitC = 0.f;
+    h->mbk = h->nbk = 0;
+    h->n_comp = 0.f;
+    state(h)->off = h->memMaskSplitA;
+    h->memAddr = h->memMaskSplitA;
+    return CUOZBLAS_STATUS_SUCCESS;
+}
+
+static int check_flags(cuozblasHandle_t *h) {
+    if (h->splitEpsMode != 0 && h->splitEpsMode != 9) return CUOZBLAS_STATUS_NOT_SUPPORTED;
+    if (h->sumMode != 0 && h->sumMode != 1) return CUOZBLAS_STATUS_NOT_SUPPORTED;
+    if (h->nSplitMax < 0 || h->nSplitMax > kMaxSplitDefault) return CUOZBLAS_STATUS_INVALID_VALUE;
+    return CUOZBLAS_STATUS_SUCCESS;
+}
+
+static int finish(cuozblasHandle_t *h, double t0) {
+    cudaError_t e = cudaStreamSynchronize(state(h)->stream);
+    h->t_total = (float)(wall() - t0);
+    if (e != cudaSuccess) {
+        fprintf(stderr, "cuozblas: CUDA error %s\n", cudaGetErrorString(e));
+        return CUOZBLAS_STATUS_CUDA_ERROR;
+    }
+    return CUOZBLAS_STATUS_SUCCESS;
+}
+
+// DOT into devWorkCommon[0], result to host.
+static int dot_impl(cuozblasHandle_t *h, int n, const double *x, const double *y, double *ret) {
+    State *st = state(h);
+    double *d = reinterpret_cast<double *>(h->devWorkCommon);
+    OZB_CHECK(cudaMemsetAsync(d, 0, sizeof(double), st->stream));
+    OZB_TRY(gemm_plain_core(h, 't', 'n', 1, 1, n, 1.0, x, n, y, n, 0.0, d, 1, 0));
+    OZB_CHECK(cudaMemcpyAsync(st->h_dbl, d, sizeof(double), cudaMemcpyDeviceToHost, st->stream));
+    OZB_CHECK(cudaStreamSynchronize(st->stream));
+    *ret = st->h_dbl[0];
+    return CUOZBLAS_STATUS_SUCCESS;
+}
+
+}  // namespace ozb
+
+using namespace ozb;
+
+extern "C" {
+
+const char *cuozblasVersion(void) { return "cuozblas-b200 0.1 (sm_100a; plain FP64-slice + INT8 tcgen05 forms)"; }
+
+int cuozblasRuleTau(double v) { return tau_rule(v); }
+int cuozblasRuleRho(int32_t dim, int32_t mode) { return rho_rule(dim, mode); }
+
+int cuozblasHandleCreate(cuozblasHandle_t *h, uint64_t workSizeBytes) {
+    if (!h) return CUOZBLAS_STATUS_INVALID_VALUE;
+    memset(h, 0, sizeof(*h));
+    State *st = new (std::nothrow) State();
+    if (!st) return CUOZBLAS_STATUS_CUDA_ERROR;
+    h->workSizeBytes = workSizeBytes;
+    // defaults of src/cuda/cuozblas.cpp:35-43
+    h->nSplitMax = 0;
+    h->memMaskSplitA = 0;
+    h->splitShift = 1;
+    h->splitMode = 0;
+    h->fastMode = 0;
+    h->reproMode = 1;
+    h->sumMode = 0;
+    h->useBatchedGemmFlag = 1;
+    h->splitEpsMode = 0;
+    h->precxFlag = 0;
+    cudaError_t e = cudaMalloc((void **)&h->devWorkCommon, sizeof(double) * 512);
+    if (e == cudaSuccess) e = cudaMalloc((void **)&h->devWork, workSizeBytes > 0 ? workSizeBytes : 256);
+    if (e == cudaSuccess) e = cudaMalloc((void **)&st->d_ints, sizeof(int) * 64);
+    if (e == cudaSuccess) e = cudaMallocHost((void **)&st->h_ints, sizeof(int) * 64);
+    if (e == cudaSuccess) e = cudaMallocHost((void **)&st->h_dbl, sizeof(double) * 64);
+    for (int i = 0; i < 4 && e == cudaSuccess; i++) e = cudaEventCreate(&st->ev[i]);
+    if (e != cudaSuccess) {
+        fprintf(stderr, "cuozblas: work memory allocation error (%1.3e bytes requested): %s\n",
+                (double)workSizeBytes, cudaGetErrorString(e));
+        if (h->devWork) cudaFree(h->devWork);
+        if (h->devWorkCommon) cudaFree(h->devWorkCommon);
+        if (st->d_ints) cudaFree(st->d_ints);
+        if (st->h_ints) cudaFreeHost(st->h_ints);
+        if (st->h_dbl) cudaFreeHost(st->h_dbl);
+        delete st;
+        memset(h, 0, sizeof(*h));
+        return CUOZBLAS_STATUS_CUDA_ERROR;
+    }
+    h->hstBatchAddr = reinterpret_cast<char *>(st);
+    h->devBatchAddr = nullptr;
+    h->initialized = 1;
+    return CUOZBLAS_STATUS_SUCCESS;
+}
+
+int cuozblasHandleDestroy(cuozblasHandle_t *h) {
+    if (!h || !h->initialized) return CUOZBLAS_STATUS_NOT_INITIALIZED;
+    State *st = state(h);
+    cudaStreamSynchronize(st->stream);
+    cudaFree(h->devWork);
+    cudaFree(h->devWorkCommon);
+    cudaFree(st->d_ints);
+    cudaFreeHost(st->h_ints);
+    cudaFreeHost(st->h_dbl);
+    for (int i = 0; i < 4; i++)
+        if (st->ev[i]) cudaEventDestroy(st->ev[i]);
+    delete st;
+    h->devWork = h->devWorkCommon = nullptr;
+    h->hstBatchAddr = nullptr;
+    h->initialized = 0;
+    return CUOZBLAS_STATUS_SUCCESS;
+}
+
+int cuozblasSetStream(cuozblasHandle_t *h, void *stream) {
+    if (!h || !h->initialized) return CUOZBLAS_STATUS_NOT_INITIALIZED;
+    state(h)->stream = reinterpret_cast<cudaStream_t>(stream);
+    return CUOZBLAS_STATUS_SUCCESS;
+}
+
+int cuozblasDgemm(cuozblasHandle_t *h, char transa, char transb, int32_t m, int32_t n, int32_t k, double alpha,
+                  const double *A, int32_t lda, const double *B, int32_t ldb, double beta, double *C, int32_t ldc) {
+    OZB_TRY(counter_init(h));
+    OZB_TRY(check_flags(h));
+    if (m < 0 || n < 0 || k < 0 || ldc < (m > 1 ? m : 1)) return CUOZBLAS_STATUS_INVALID_VALUE;
+    if (h->reproMode == 0 && h->nSplitMax == 1) return CUOZBLAS_STATUS_NOT_SUPPORTED;
+    if (m == 0 || n == 0) return CUOZBLAS_STATUS_SUCCESS;
+    const double t0 = wall();
+    OZB_TRY(gemm_plain_core(h, transa, transb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, h->fastMode));
+    return finish(h, t0);
+}
+
+int cuozblasDdot(cuozblasHandle_t *h, int32_t n, const double *x, int32_t incx, const double *y, int32_t incy,
+                 double *ret) {
+    OZB_TRY(counter_init(h));
+    OZB_TRY(check_flags(h));
+    if (incx != 1 || incy != 1 || n < 0 || ret == nullptr) return CUOZBLAS_STATUS_INVALID_VALUE;
+    const double t0 = wall();
+    OZB_TRY(dot_impl(h, n, x, y, ret));
+    h->t_SplitVec_total += h->t_SplitA + h->t_SplitB;
+    return finish(h, t0);
+}
+
+int cuozblasDnrm2(cuozblasHandle_t *h, int32_t n, const double *x, int32_t incx, double *ret) {
+    OZB_TRY(counter_init(h));
+    OZB_TRY(check_flags(h));
+    if (incx != 1 || n < 0 || ret == nullptr) return CUOZBLAS_STATUS_INVALID_VALUE;
+    const double t0 = wall();
+    double d = 0.0;
+    OZB_TRY(dot_impl(h, n, x, x, &d));
+    *ret = sqrt(d);  // host sqrt, src/cuda/cuozblas_nrm2.cu:24-29
+    return finish(h, t0);
+}
+
+int cuozblasDaxpy(cuozblasHandle_t *h, int32_t n, double alpha, const double *x, int32_t incx, double *y,
+                  int32_t incy) {
+    if (!h || !h->initialized) return CUOZBLAS_STATUS_NOT_INITIALIZED;
+    if (incx != 1 || incy != 1 || n < 0) return CUOZBLAS_STATUS_INVALID_VALUE;
+    OZB_TRY(launch_axpy(h, n, alpha, x, y));
+    return finish(h, wall());
+}
+
+int cuozblasDgemv(cuozblasHandle_t *h, char trans, int32_t m, int32_t n, double alpha, const double *A,
+                  int32_t lda, const double *x, int32_t incx, double beta, double *y, int32_t incy) {
+    OZB_TRY(counter_init(h));
+    OZB_TRY(check_flags(h));
+    if (incx != 1 || incy != 1 || m < 0 || n < 0) return CUOZBLAS_STATUS_INVALID_VALUE;
+    const double t0 = wall();
+    if (!is_trans(trans)) {
+        if (m == 0) return CUOZBLAS_STATUS_SUCCESS;
+        OZB_TRY(gemm_plain_core(h, 'n', 'n', m, 1, n, alpha, A, lda, x, n, beta, y, m, h->fastMode));
+    } else {
+        if (n == 0) return CUOZBLAS_STATUS_SUCCESS;
+        OZB_TRY(gemm_plain_core(h, 't', 'n', n, 1, m, alpha, A, lda, x, m, beta, y, n, h->fastMode));
+    }
+    return finish(h, t0);
+}
+
+static int64_t splitA_ld(int nnz) { return ((int64_t)(nnz > 0 ? nnz : 1) + 31) / 32 * 32; }
+
+int cuozblasDcsrmv(cuozblasHandle_t *h, char trans, int32_t m, int32_t n, int32_t nnz, double alpha,
+                   const void *descrA, const double *val, const int32_t *colind, const int32_t *rowptr,
+                   const double *x, double beta, double *y) {
+    (void)descrA;
+    OZB_TRY(counter_init(h));
+    OZB_TRY(check_flags(h));
+    if (is_trans(trans) || m < 0 || n < 0 || nnz < 0) return CUOZBLAS_STATUS_INVALID_VALUE;
+    const double t0 = wall();
+    const int maxS = h->nSplitMax > 0 ? h->nSplitMax : kMaxSplitDefault;
+    if (h->memMaskSplitA != 0) {  // `val` is the pre-split A of cuozblasDcsrmvSplitA
+        OZB_TRY(csrmv_presplit(h, m, n, alpha, val, h->nSplitA_, state(h)->splitA_ld, colind, rowptr, x, beta, y));
+        return finish(h, t0);
+    }
+    Arena ar(h);
+    const int64_t ld = splitA_ld(nnz);
+    int nA = 0;
+    OZB_TRY(split_csr_count(h, m, val, rowptr, h->splitEpsMode, 1, maxS, &nA));
+    double *As = ar.take<double>((uint64_t)nA * ld);
+    if (!ar.ok) return CUOZBLAS_STATUS_WORKSPACE;
+    OZB_TRY(split_csr_write(h, m, nnz, val, rowptr, h->splitEpsMode, 1, nA, As, ld));
+    OZB_TRY(csrmv_presplit(h, m, n, alpha, As, nA, ld, colind, rowptr, x, beta, y));
+    return finish(h, t0);
+}
+
+int cuozblasDcsrmvSplitA(cuozblasHandle_t *h, char trans, int32_t m, int32_t n, int32_t nnz, const void *descrA,
+                         const double *val, const int32_t *rowptr, double **splitA) {
+    (void)descrA;
+    (void)n;
+    OZB_TRY(counter_init(h));
+    OZB_TRY(check_flags(h));
+    if (is_trans(trans) || m < 0 || nnz < 0 || splitA == nullptr) return CUOZBLAS_STATUS_INVALID_VALUE;
+    const int maxS = h->nSplitMax > 0 ? h->nSplitMax : kMaxSplitDefault;
+    const double t0 = wall();
+    // tuning of splitShift (src/cuda/cuozblas_csrmv.cu:186-201), counts only
+    int s = 0;
+    OZB_TRY(split_csr_count(h, m, val, rowptr, h->splitEpsMode, 1, maxS, &s));
+    int shift = 1;
+    if (h->nSplitMax == 0) {
+        int sold;
+        do {
+            sold = s;
+            shift *= 2;
+            OZB_TRY(split_csr_count(h, m, val, rowptr, h->splitEpsMode, shift, maxS, &s));
+        } while (sold == s && shift < 512);
+        if (sold == s) shift = 1;
+        OZB_TRY(split_csr_count(h, m, val, rowptr, h->splitEpsMode, shift, maxS, &s));
+    }
+    // the preserved region starts at the arena base
+    State *st = state(h);
+    st->off = 0;
+    Arena ar(h);
+    const int64_t ld = splitA_ld(nnz);
+    double *As = ar.take<double>((uint64_t)s * ld);
+    if (!ar.ok) return CUOZBLAS_STATUS_WORKSPACE;
+    OZB_TRY(split_csr_write(h, m, nnz, val, rowptr, h->splitEpsMode, shift, s, As, ld));
+    h->memMaskSplitA = st->off;
+    h->splitShift = shift;
+    h->nSplitA_ = s;
+    h->nSplitA = (float)s;
+    state(h)->splitA_ld = ld;
+    *splitA = As;
+    return finish(h, t0);
+}
+
+int cuozblasDcg(cuozblasHandle_t *h, char trans, int32_t n, int32_t nnz, const void *descrA, const double *val,
+                const int32_t *colind, const int32_t *rowptr, const double *b, double *x, int32_t maxiter,
+                double tol) {
+    if (!h || !h->initialized) return CUOZBLAS_STATUS_NOT_INITIALIZED;
+    if (is_trans(trans) || n < 0 || nnz < 0 || maxiter < 0) return CUOZBLAS_STATUS_INVALID_VALUE;
+    h->t_SplitMat_total = h->t_SplitVec_total = h->t_Sum_total = 0.;
+    h->t_AXPY_SCAL_total = h->t_DOT_NRM2_total = h->t_SpMV_SpMM_total = 0.;
+    double *hist1 = reinterpret_cast<double *>(h->cg_verbose1);
+    double *hist2 = reinterpret_cast<double *>(h->cg_verbose2);
+    const double t1 = wall();
+    h->cg_numiter = 0;
+    double *As = nullptr;
+    OZB_TRY(cuozblasDcsrmvSplitA(h, trans, n, n, nnz, descrA, val, rowptr, &As));
+    // CG vectors live above the preserved split of A for the whole solve
+    State *st = state(h);
+    st->off = h->memMaskSplitA;
+    Arena ar(h);
+    const uint64_t nn = (uint64_t)(n > 0 ? n : 1);
+    double *r = ar.take<double>(nn), *p = ar.take<double>(nn), *q = ar.take<double>(nn), *tv = ar.take<double>(nn);
+    if (!ar.ok) return CUOZBLAS_STATUS_WORKSPACE;
+    const uint64_t keep = h->memMaskSplitA;
+    h->memMaskSplitA = st->off;
+    int status = CUOZBLAS_STATUS_SUCCESS;
+    auto fail = [&](int s) {
+        h->memMaskSplitA = 0;
+        h->splitShift = 1;
+        return s;
+    };
+    (void)keep;
+    double nrmb = 0.0, dold = 0.0, tmp = 0.0;
+    if ((status = cuozblasDnrm2(h, n, b, 1, &nrmb))) return fail(status);
+    if (cudaMemcpyAsync(r, b, sizeof(double) * n, cudaMemcpyDeviceToDevice, st->stream) != cudaSuccess ||
+        cudaMemsetAsync(q, 0, sizeof(double) * nn, st->stream) != cudaSuccess)
+        return fail(CUOZBLAS_STATUS_CUDA_ERROR);
+    if ((status = cuozblasDcsrmv(h, trans, n, n, nnz, -1., descrA, As, colind, rowptr, x, 1., r))) return fail(status);
+    if ((status = cuozblasDdot(h, n, r, 1, r, 1, &dold))) return fail(status);
+    double resi = sqrt(dold);
+    auto true_res = [&]() -> double {
+        // t = b - A x in plain FP64, then a plain FP64 norm (diagnostic only)
+        cudaMemcpyAsync(tv, b, sizeof(double) * n, cudaMemcpyDeviceToDevice, st->stream);
+        launch_csrmv_plain(h, n, val, colind, rowptr, x, -1., 1., tv);
+        double *hv = new double[nn];
+        cudaMemcpyAsync(hv, tv, sizeof(double) * n, cudaMemcpyDeviceToHost, st->stream);
+        cudaStreamSynchronize(st->stream);
+        double s2 = 0.0;
+        for (int i = 0; i < n; i++) s2 += hv[i] * hv[i];
+        delete[] hv;
+        return sqrt(s2);
+    };
+    if (h->verbose > 0) {
+        const double t2 = wall();
+        if (hist1) hist1[0] = resi / nrmb;
+        if (hist2) hist2[0] = h->trueresFlag ? true_res() / nrmb : t2 - t1;
+    }
+    if (cudaMemcpyAsync(p, r, sizeof(double) * n, cudaMemcpyDeviceToDevice, st->stream) != cudaSuccess)
+        return fail(CUOZBLAS_STATUS_CUDA_ERROR);
+    int verbose_cnt = 1;
+    while (h->cg_numiter < maxiter) {
+        h->cg_numiter++;
+        if ((status = cuozblasDcsrmv(h, trans, n, n, nnz, 1., descrA, As, colind, rowptr, p, 0., q)))
+            return fail(status);
+        if ((status = cuozblasDdot(h, n, p, 1, q, 1, &tmp))) return fail(status);
+        const double alpha = dold / tmp;
+        if ((status = launch_axpy(h, n, alpha, p, x))) return fail(status);
+        if ((status = launch_axpy(h, n, -alpha, q, r))) return fail(status);
+        double dnew = 0.0;
+        if ((status = cuozblasDdot(h, n, r, 1, r, 1, &dnew))) return fail(status);
+        resi = sqrt(dnew);
+        const double beta = dnew / dold;
+        dold = dnew;
+        if ((status = launch_scal(h, n, beta, p))) return fail(status);
+        if ((status = launch_axpy(h, n, 1.0, r, p))) return fail(status);
+        if (h->verbose > 0) {
+            if (resi / nrmb < tol || h->cg_numiter % h->verbose == 0) {
+                if (hist1) hist1[verbose_cnt] = resi / nrmb;
+                if (hist2) hist2[verbose_cnt] = h->trueresFlag ? true_res() / nrmb : wall() - t1;
+                verbose_cnt++;
+            }
+        }
+        if (resi / nrmb < tol) break;
+    }
+    cudaError_t e = cudaStreamSynchronize(st->stream);
+    h->memMaskSplitA = 0;  // src/cuda/cuozblas_cg.cu:124-127
+    h->splitShift = 1;
+    return e == cudaSuccess ? CUOZBLAS_STATUS_SUCCESS : CUOZBLAS_STATUS_CUDA_ERROR;
+}
+
+}  // extern "C"

@@ -1,0 +1,124 @@
+// csrmv.cu — Ozaki CSRMV (src/cuda/cuozblas_csrmv.cu:3-133, CPU
+// src/cpu/ozblas_csrmv.cpp:3-181) and the vector updates CG needs.
+//
+// The slice CSRMM of the reference CPU path accumulates each row with a
+// sequential fma chain in storage order (src/cpu/ozblas_blas_wrapper.cpp:231-255
+// and the _l2.._l5 variants), then scales by alpha = 1.  One thread per row
+// runs the same chain for every slice pair, so the products carry the CPU's
+// bits whether or not they are exact (with splitShift > 1 they need not be).
+#include "ozb_internal.h"
+#include "sum.cuh"
+
+namespace ozb {
+
+// y = fma(alpha, t, beta*y) with t the pair sum of the row (FSUM), or the
+// pair products written to pbuf[p * m + row] and NearSum-ed (sum_mode 1).
+__global__ void __launch_bounds__(256) k_csrmv_pairs(int m, const double *__restrict__ As, int64_t lda_s,
+                                                     const int *__restrict__ colind, const int *__restrict__ rowptr,
+                                                     const double *__restrict__ xs, int64_t ldx, int nA, int nB,
+                                                     int maxlevel, int sum_mode, double alpha, double beta,
+                                                     double *__restrict__ y, double *__restrict__ pbuf) {
+    const int row = blockIdx.x * blockDim.x + threadIdx.x;
+    if (row >= m) return;
+    const int lo = rowptr[row], hi = rowptr[row + 1];
+    double t = 0.0;
+    int p = 0;
+    for_each_pair(nA, nB, maxlevel, [&](int ia, int ib) {
+        const double *a = As + (size_t)ia * lda_s;
+        const double *x = xs + (size_t)ib * ldx;
+        double tr = 0.0;
+        for (int i = lo; i < hi; i++) tr = fma(a[i], x[colind[i]], tr);
+        if (sum_mode == 1)
+            pbuf[(size_t)p * m + row] = tr;
+        else
+            t += tr;
+        p++;
+    });
+    if (sum_mode == 1) t = nearsum(p, pbuf + row, m);
+    y[row] = fma(alpha, t, beta * y[row]);
+}
+
+// Plain FP64 CSRMV with a sequential fma chain (the true-residual check of CG).
+__global__ void k_csrmv_plain(int m, const double *__restrict__ val, const int *__restrict__ colind,
+                              const int *__restrict__ rowptr, const double *__restrict__ x, double alpha,
+                              double beta, double *__restrict__ y) {
+    const int row = blockIdx.x * blockDim.x + threadIdx.x;
+    if (row >= m) return;
+    double tr = 0.0;
+    for (int i = rowptr[row]; i < rowptr[row + 1]; i++) tr = fma(val[i], x[colind[i]], tr);
+    y[row] = (beta == 0.0) ? alpha * tr : fma(alpha, tr, beta * y[row]);
+}
+
+// y = fma(alpha, x, y)  (src/cuda/cuozblas_axpy.cu:5-16)
+__global__ void k_axpy(int n, double alpha, const double *__restrict__ x, double *__restrict__ y) {
+    const size_t stride = (size_t)gridDim.x * blockDim.x;
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < (size_t)n; i += stride)
+        y[i] = fma(alpha, x[i], y[i]);
+}
+
+// x = alpha * x  (the cublasDscal of src/cuda/cuozblas_cg.cu:100)
+__global__ void k_scal(int n, double alpha, double *__restrict__ x) {
+    const size_t stride = (size_t)gridDim.x * blockDim.x;
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < (size_t)n; i += stride) x[i] = alpha * x[i];
+}
+
+int launch_axpy(cuozblasHandle_t *h, int n, double alpha, const double *x, double *y) {
+    if (n <= 0) return CUOZBLAS_STATUS_SUCCESS;
+    int blocks = (n + 255) / 256;
+    if (blocks > 148 * 16) blocks = 148 * 16;
+    k_axpy<<<blocks, 256, 0, state(h)->stream>>>(n, alpha, x, y);
+    OZB_CHECK(cudaGetLastError());
+    return CUOZBLAS_STATUS_SUCCESS;
+}
+
+int launch_scal(cuozblasHandle_t *h, int n, double alpha, double *x) {
+    if (n <= 0) return CUOZBLAS_STATUS_SUCCESS;
+    int blocks = (n + 255) / 256;
+    if (blocks > 148 * 16) blocks = 148 * 16;
+    k_scal<<<blocks, 256, 0, state(h)->stream>>>(n, alpha, x);
+    OZB_CHECK(cudaGetLastError());
+    return CUOZBLAS_STATUS_SUCCESS;
+}
+
+int launch_csrmv_plain(cuozblasHandle_t *h, int m, const double *val, const int *colind, const int *rowptr,
+                       const double *x, double alpha, double beta, double *y) {
+    if (m <= 0) return CUOZBLAS_STATUS_SUCCESS;
+    k_csrmv_plain<<<(m + 255) / 256, 256, 0, state(h)->stream>>>(m, val, colind, rowptr, x, alpha, beta, y);
+    OZB_CHECK(cudaGetLastError());
+    return CUOZBLAS_STATUS_SUCCESS;
+}
+
+// Ozaki CSRMV over given A slices (nA slices of ld_s doubles).
+int csrmv_presplit(cuozblasHandle_t *h, int m, int n, double alpha, const double *As, int nA, int64_t ld_s,
+                   const int *colind, const int *rowptr, const double *x, double beta, double *y) {
+    State *st = state(h);
+    const int maxS = h->nSplitMax > 0 ? h->nSplitMax : kMaxSplitDefault;
+    Arena ar(h);
+    const int ldx = (n + 31) / 32 * 32;
+    double *xs = ar.take<double>((uint64_t)maxS * (ldx > 0 ? ldx : 32));
+    if (!ar.ok) return CUOZBLAS_STATUS_WORKSPACE;
+    int nB = 0;
+    OZB_TRY(split_vector(h, n, x, rho_rule(n, h->splitEpsMode), maxS, xs, ldx, &nB));
+    int maxlevel = (nA - 1) + (nB - 1);
+    const int mn = nA - 1 < nB - 1 ? nA - 1 : nB - 1;
+    maxlevel = (maxlevel - h->fastMode) > mn ? (maxlevel - h->fastMode) : mn;
+    int np = 0;
+    for_each_pair(nA, nB, maxlevel, [&](int, int) { np++; });
+    double *pbuf = nullptr;
+    if (h->sumMode == 1) {
+        pbuf = ar.take<double>((uint64_t)np * (m > 0 ? m : 1));
+        if (!ar.ok) return CUOZBLAS_STATUS_WORKSPACE;
+    }
+    if (m > 0)
+        k_csrmv_pairs<<<(m + 255) / 256, 256, 0, st->stream>>>(m, As, ld_s, colind, rowptr, xs, ldx, nA, nB, maxlevel,
+                                                              h->sumMode, alpha, beta, y, pbuf);
+    OZB_CHECK(cudaGetLastError());
+    int ic = 0;
+    for (int ia = 0; ia < (maxlevel + 1 < nA ? maxlevel + 1 : nA); ia++) ic += (nB < maxlevel + 1 - ia ? nB : maxlevel + 1 - ia);
+    h->nSplitA = (float)nA;
+    h->nSplitB = (float)nB;
+    h->nSplitC = (float)ic;
+    return CUOZBLAS_STATUS_SUCCESS;
+}
+
+}  // namespace ozb

@@ -1,0 +1,594 @@
+// gemm_i8.cu — INT8 precision form of the Ozaki DGEMM on tcgen05 tensor cores.
+//
+// This form has no reference implementation (the reference stubs an integer
+// path at src/cuda/cuozblas_gemm.cu:292 and src/cuda/cuozblas_common.h:53-56).
+//
+// Split: each line (row of op(A), column of op(B)) gets an exponent E with
+// max|x| < 2^E; x * 2^-E in (-1, 1) is cut into base-2^7 digits by
+// truncation, d_s = trunc(r * 128), r <- r * 128 - d_s, so every digit is an
+// int8 in [-127, 127] with the sign of x and
+//     x = 2^E * sum_s d_s 2^(-7(s+1))   (exact once enough digits are kept).
+// Products: C(i,j) = 2^(EA_i + EB_j) * sum_L 2^(-7(L+2)) V_L(i,j) with
+// V_L = sum over digit pairs ia + ib = L of the int8 dot products.  All pairs
+// of one level share the scale, so they accumulate in one INT32 tensor-memory
+// accumulator; a group holds at most floor((2^31 - 1) / (127^2)) products per
+// output, which keeps every partial sum exact (k is chunked beyond that).
+// Sum: levels are visited from the smallest (highest L) to the largest.  A
+// run of consecutive levels is first combined exactly, as an integer below
+// 2^53 held in an FP64 register (V_L shifted by 7 bits per level); each run
+// is then added once to the FP64 sum R, which lives in tensor memory.  With a
+// complete split this makes the output correctly rounded except when the
+// exact value sits within ~2^-28 ulp of a rounding boundary.  Finally
+// t = R * 2^(EA_i + EB_j) and C = fma(alpha, t, beta * C).
+//
+// Kernel: persistent, one CTA per SM, warp-specialised:
+//   warp 0      TMA producer (128 x 128-byte tiles, 128-byte swizzle)
+//   warp 1      TMEM allocator and single-thread tcgen05.mma issuer
+//   warps 2-9   epilogue: tcgen05.ld of the INT32 level sums, FP64 sum, store
+// Two 128-column TMEM accumulators let the epilogue of one level overlap the
+// MMAs of the next; the other 256 columns hold R.  Every mbarrier wait is bounded (global timer) and shares
+// an abort flag; a timeout reports CUOZBLAS_STATUS_DEVICE_TIMEOUT.
+#include <cuda.h>
+
+#include <vector>
+
+#include "ozb_device.cuh"
+#include "ozb_internal.h"
+#include "tc05.cuh"
+
+namespace ozb {
+
+constexpr int I8_BM = 128, I8_BN = 128, I8_BK = 128, I8_NST = 6;
+constexpr int I8_THREADS = 320;
+constexpr int I8_TMEM_COLS = 512;     // 2 x 128 INT32 accumulators + 128 x 128 FP64 sums
+constexpr int I8_RCOL = 2 * 128;      // first column of the FP64 sums
+constexpr int I8_TILE_A = I8_BM * I8_BK, I8_TILE_B = I8_BN * I8_BK, I8_STAGE = I8_TILE_A + I8_TILE_B;
+constexpr int I8_SMEM = I8_NST * I8_STAGE + 1024 /*align slack*/ + 256 /*barriers*/;
+constexpr int64_t I8_MAX_TERMS = 2147483647LL / (127 * 127);  // 133143 int8 products per INT32 sum
+constexpr uint64_t I8_WAIT_NS = 2000000000ull;                  // 2 s per wait
+
+enum { ERR_TIMEOUT_PRODUCER = 1, ERR_TIMEOUT_MMA = 2, ERR_TIMEOUT_EPI = 3 };
+
+struct I8Params {
+    int m, n, m_pad, n_pad, ldc;
+    int tiles_m, tiles_n, n_items, n_groups;
+    const int4 *items;   // {ia, ib, kb0, kb1} in processing order
+    const int4 *groups;  // {item_begin, item_end, flush scale exponent, meta: shift | flush<<8 | first<<9 | last<<10}
+    const int *ea, *eb;  // line exponents
+    double alpha, beta;
+    double *C;
+    int *err;
+};
+
+__global__ void __launch_bounds__(I8_THREADS, 1)
+    k_i8_gemm(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, I8Params p) {
+    extern __shared__ uint8_t smem_raw[];
+    uint8_t *smem = (uint8_t *)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+    uint64_t *bar = (uint64_t *)(smem + I8_NST * I8_STAGE);
+    uint64_t *full = bar, *empty = bar + I8_NST, *acc_full = bar + 2 * I8_NST, *acc_empty = bar + 2 * I8_NST + 2;
+    uint64_t *drain = bar + 2 * I8_NST + 4;
+    __shared__ uint32_t tmem_slot;
+    __shared__ volatile int abort_flag;
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int ntiles = p.tiles_m * p.tiles_n;
+
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < I8_NST; s++) {
+            tc::mbar_init(&full[s], 1);
+            tc::mbar_init(&empty[s], 1);
+        }
+        for (int b = 0; b < 2; b++) {
+            tc::mbar_init(&acc_full[b], 1);
+            tc::mbar_init(&acc_empty[b], 256);
+        }
+        tc::mbar_init(drain, 1);
+        abort_flag = 0;
+        tc::fence_mbar_init();
+        tc::prefetch_tmap(&tmA);
+        tc::prefetch_tmap(&tmB);
+    }
+    if (warp == 1) tc::tmem_alloc(&tmem_slot, I8_TMEM_COLS);
+    tc::fence_before_sync();
+    __syncthreads();
+    tc::fence_after_sync();
+    const uint32_t tmem_base = tmem_slot;
+
+    if (warp == 0) {
+        // ------------------------------------------------------------ producer
+        if (lane == 0) {
+            uint32_t stage = 0, phase = 0;
+            bool ok = true;
+            for (int tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x) {
+                const int tm = tile % p.tiles_m, tn = tile / p.tiles_m;
+                for (int it = 0; it < p.n_items && ok; it++) {
+                    const int4 item = p.items[it];
+                    for (int kb = item.z; kb < item.w; kb++) {
+                        if (!tc::mbar_wait(&empty[stage], phase ^ 1, &abort_flag, p.err, ERR_TIMEOUT_PRODUCER,
+                                           I8_WAIT_NS)) {
+                            ok = false;
+                            break;
+                        }
+                        uint8_t *sa = smem + stage * I8_STAGE, *sb = sa + I8_TILE_A;
+                        tc::mbar_arrive_expect_tx(&full[stage], I8_STAGE);
+                        tc::tma_load_2d(sa, &tmA, &full[stage], kb * I8_BK, item.x * p.m_pad + tm * I8_BM);
+                        tc::tma_load_2d(sb, &tmB, &full[stage], kb * I8_BK, item.y * p.n_pad + tn * I8_BN);
+                        if (++stage == I8_NST) {
+                            stage = 0;
+                            phase ^= 1;
+                        }
+                    }
+                }
+            }
+            if (!ok) {
+                // let copies already issued land before the CTA exits
+                for (int s = 0; s < I8_NST; s++) {
+                    const uint64_t t0 = tc::globaltimer();
+                    while (!tc::mbar_try_wait(&full[s], 0) && !tc::mbar_try_wait(&full[s], 1) &&
+                           tc::globaltimer() - t0 < 100000000ull) {
+                    }
+                }
+            }
+        }
+    } else if (warp == 1) {
+        // ------------------------------------------------------------ MMA issuer
+        if (lane == 0) {
+            const uint32_t idesc = tc::idesc_i8(I8_BM, I8_BN);
+            uint32_t stage = 0, phase = 0, abuf = 0, aphase = 0;
+            bool ok = true, issued = false;
+            for (int tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x) {
+                for (int g = 0; g < p.n_groups && ok; g++) {
+                    const int4 grp = p.groups[g];
+                    if (!tc::mbar_wait(&acc_empty[abuf], aphase ^ 1, &abort_flag, p.err, ERR_TIMEOUT_MMA,
+                                       I8_WAIT_NS)) {
+                        ok = false;
+                        break;
+                    }
+                    tc::fence_after_sync();
+                    const uint32_t tmem_d = tmem_base + abuf * I8_BN;
+                    uint32_t accumulate = 0;
+                    for (int it = grp.x; it < grp.y && ok; it++) {
+                        const int4 item = p.items[it];
+                        for (int kb = item.z; kb < item.w; kb++) {
+                            if (!tc::mbar_wait(&full[stage], phase, &abort_flag, p.err, ERR_TIMEOUT_MMA,
+                                               I8_WAIT_NS)) {
+                                ok = false;
+                                break;
+                            }
+                            tc::fence_after_sync();
+                            const uint32_t sa = tc::smem_u32(smem + stage * I8_STAGE), sb = sa + I8_TILE_A;
+                            const uint64_t adesc = tc::smem_desc_k_sw128(sa), bdesc = tc::smem_desc_k_sw128(sb);
+#pragma unroll
+                            for (int kk = 0; kk < I8_BK / 32; kk++) {
+                                // +32 bytes along K inside the 128-byte swizzle row = +2 in 16-byte units
+                                tc::mma_i8(tmem_d, adesc + 2 * kk, bdesc + 2 * kk, idesc, accumulate);
+                                accumulate = 1;
+                            }
+                            issued = true;
+                            tc::mma_commit(&empty[stage]);
+                            if (++stage == I8_NST) {
+                                stage = 0;
+                                phase ^= 1;
+                            }
+                        }
+                    }
+                    if (!ok) break;
+                    tc::mma_commit(&acc_full[abuf]);
+                    abuf ^= 1;
+                    if (abuf == 0) aphase ^= 1;
+                }
+            }
+            if (!ok && issued) {  // drain MMAs still in flight before TMEM is released
+                tc::mma_commit(drain);
+                const uint64_t t0 = tc::globaltimer();
+                while (!tc::mbar_try_wait(drain, 0) && tc::globaltimer() - t0 < 100000000ull) {
+                }
+            }
+        }
+    } else {
+        // ------------------------------------------------------------ epilogue
+        const int q = warp & 3, half = (warp - 2) >> 2;
+        const int row = q * 32 + lane;
+        const uint32_t lane_base = tmem_base + ((uint32_t)(q * 32) << 16);
+        const uint32_t rcol = I8_RCOL + half * 128;  // this thread's 64 FP64 sums (lo, hi word pairs)
+        uint32_t abuf = 0, aphase = 0;
+        bool ok = true;
+        for (int tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x) {
+            const int tm = tile % p.tiles_m, tn = tile / p.tiles_m;
+            const int gr = tm * I8_BM + row;
+            double acc[64];  // exact integer-valued run of levels (< 2^53)
+#pragma unroll
+            for (int c = 0; c < 64; c++) acc[c] = 0.0;
+            for (int g = 0; g < p.n_groups; g++) {
+                const int4 grp = p.groups[g];
+                const int meta = grp.w;
+                if (!tc::mbar_wait(&acc_full[abuf], aphase, &abort_flag, p.err, ERR_TIMEOUT_EPI, I8_WAIT_NS)) {
+                    ok = false;
+                    break;
+                }
+                tc::fence_after_sync();
+                const double sc = pow2(meta & 0xff);
+                const uint32_t taddr = lane_base + abuf * I8_BN + half * 64;
+                uint32_t v[32];
+                tc::tmem_ld_32x32b_x32(taddr, v);
+                tc::tmem_ld_wait();
+#pragma unroll
+                for (int c = 0; c < 32; c++) acc[c] += (double)(int32_t)v[c] * sc;
+                tc::tmem_ld_32x32b_x32(taddr + 32, v);
+                tc::tmem_ld_wait();
+#pragma unroll
+                for (int c = 0; c < 32; c++) acc[32 + c] += (double)(int32_t)v[c] * sc;
+                tc::fence_before_sync();
+                tc::mbar_arrive(&acc_empty[abuf]);
+                abuf ^= 1;
+                if (abuf == 0) aphase ^= 1;
+                if (meta & (1 << 8)) {  // end of a run: R += acc * 2^(exponent)
+                    const double fs = pow2(grp.z);
+                    const bool first = meta & (1 << 9), last = meta & (1 << 10);
+#pragma unroll
+                    for (int ch = 0; ch < 4; ch++) {
+                        const uint32_t raddr = lane_base + rcol + ch * 32;
+                        uint32_t u[32];
+                        double r[16];
+                        if (first) {
+#pragma unroll
+                            for (int e = 0; e < 16; e++) r[e] = acc[ch * 16 + e] * fs;
+                        } else {
+                            tc::tmem_ld_32x32b_x32(raddr, u);
+                            tc::tmem_ld_wait();
+#pragma unroll
+                            for (int e = 0; e < 16; e++)
+                                r[e] = __hiloint2double((int)u[2 * e + 1], (int)u[2 * e]) + acc[ch * 16 + e] * fs;
+                        }
+                        if (last) {
+                            if (gr < p.m) {
+                                const int ea = p.ea[gr];
+#pragma unroll
+                                for (int e = 0; e < 16; e++) {
+                                    const int gc = tn * I8_BN + half * 64 + ch * 16 + e;
+                                    if (gc < p.n) {
+                                        double *cp = &p.C[(size_t)gc * p.ldc + gr];
+                                        const double t = scalbn(r[e], ea + p.eb[gc]);
+                                        *cp = fma(p.alpha, t, p.beta * *cp);
+                                    }
+                                }
+                            }
+                        } else {
+#pragma unroll
+                            for (int e = 0; e < 16; e++) {
+                                u[2 * e] = (uint32_t)__double2loint(r[e]);
+                                u[2 * e + 1] = (uint32_t)__double2hiint(r[e]);
+                            }
+                            tc::tmem_st_32x32b_x32(raddr, u);
+                        }
+                    }
+                    if (!last) tc::tmem_st_wait();
+#pragma unroll
+                    for (int c = 0; c < 64; c++) acc[c] = 0.0;
+                }
+            }
+        }
+    }
+    tc::fence_before_sync();
+    __syncthreads();
+    if (warp == 1) {
+        tc::fence_after_sync();
+        tc::tmem_dealloc(tmem_base, I8_TMEM_COLS);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Digit split
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ int exp_above(double v) {  // E with v < 2^E, v > 0
+    const uint64_t b = dbits(v) & 0x7fffffffffffffffULL;
+    const int be = (int)(b >> 52);
+    if (be == 0) {
+        const uint64_t f = b & ((1ULL << 52) - 1);
+        if (f == 0) return 0;
+        return (63 - clz64(f)) - 1073;
+    }
+    return be - 1022;
+}
+
+__device__ __forceinline__ int lsb_exp(double v) {  // exponent of the lowest set bit, v != 0
+    const uint64_t b = dbits(v) & 0x7fffffffffffffffULL;
+    const int be = (int)(b >> 52);
+    uint64_t f = b & ((1ULL << 52) - 1);
+    if (be == 0) return -1074 + __ffsll((long long)f) - 1;
+    f |= (1ULL << 52);
+    return (be - 1075) + __ffsll((long long)f) - 1;
+}
+
+// One CTA per line: line exponent and the digit count that makes the line exact.
+__global__ void __launch_bounds__(256) k_digit_count(int k, int nl, const double *__restrict__ X, int ldx,
+                                                     int *__restrict__ e_out, int *__restrict__ need_max) {
+    __shared__ double red[8];
+    __shared__ int redi[8];
+    const int line = blockIdx.x;
+    const double *x = X + (size_t)line * ldx;
+    double mx = 0.0;
+    for (int i = threadIdx.x; i < k; i += blockDim.x) mx = ref_max(mx, fabs(x[i]));
+    mx = block_max_nonneg(mx, red);
+    const int E = mx > 0.0 ? exp_above(mx) : 0;
+    int need = 0;
+    if (mx > 0.0)
+        for (int i = threadIdx.x; i < k; i += blockDim.x) {
+            const double v = x[i];
+            if (v != 0.0) {
+                const int d = (E - lsb_exp(v) + 6) / 7;
+                need = need > d ? need : d;
+            }
+        }
+    for (int o = 16; o > 0; o >>= 1) {
+        const int t = __shfl_xor_sync(0xffffffffu, need, o);
+        need = need > t ? need : t;
+    }
+    __syncthreads();
+    if ((threadIdx.x & 31) == 0) redi[threadIdx.x >> 5] = need;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int r = 0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); w++) r = r > redi[w] ? r : redi[w];
+        e_out[line] = E;
+        atomicMax(need_max, r);
+    }
+}
+
+// Digits: thread handles 16 consecutive k of one line; writes S slices of
+// lines_pad x k_pad int8 (zero padded in both directions).
+__global__ void __launch_bounds__(256) k_digit_write(int k, int nl, int nl_pad, int k_pad, int S,
+                                                     const double *__restrict__ X, int ldx,
+                                                     const int *__restrict__ e_line, int8_t *__restrict__ out) {
+    const int64_t chunk = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int per_line = k_pad / 16;
+    const int64_t total = (int64_t)nl_pad * per_line;
+    if (chunk >= total) return;
+    const int line = (int)(chunk / per_line), k0 = (int)(chunk % per_line) * 16;
+    double r[16];
+    if (line < nl) {
+        const int E = e_line[line];
+        const double *x = X + (size_t)line * ldx;
+#pragma unroll
+        for (int i = 0; i < 16; i++) r[i] = (k0 + i < k) ? scalbn(x[k0 + i], -E) : 0.0;
+    } else {
+#pragma unroll
+        for (int i = 0; i < 16; i++) r[i] = 0.0;
+    }
+    for (int s = 0; s < S; s++) {
+        uint32_t w[4] = {0, 0, 0, 0};
+#pragma unroll
+        for (int i = 0; i < 16; i++) {
+            const double t = r[i] * 128.0;
+            const double d = trunc(t);
+            r[i] = t - d;
+            w[i >> 2] |= ((uint32_t)(uint8_t)(int8_t)(int)d) << (8 * (i & 3));
+        }
+        int4 *o = reinterpret_cast<int4 *>(out + ((size_t)s * nl_pad + line) * k_pad + k0);
+        *o = make_int4((int)w[0], (int)w[1], (int)w[2], (int)w[3]);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Host side
+// ---------------------------------------------------------------------------
+typedef CUresult (*PFN_TensorMapEncodeTiled)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *,
+                                             const cuuint64_t *, const cuuint64_t *, const cuuint32_t *,
+                                             const cuuint32_t *, CUtensorMapInterleave, CUtensorMapSwizzle,
+                                             CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+static PFN_TensorMapEncodeTiled get_encode() {
+    static PFN_TensorMapEncodeTiled fn = nullptr;
+    if (!fn) {
+        void *ptr = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &ptr, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = (PFN_TensorMapEncodeTiled)ptr;
+    }
+    return fn;
+}
+
+// rows x cols int8 matrix (row stride = cols bytes), box 128 (cols) x box_rows.
+static int make_map(CUtensorMap *map, const int8_t *base, uint64_t rows, uint64_t cols, uint32_t box_rows) {
+    PFN_TensorMapEncodeTiled enc = get_encode();
+    if (!enc) return CUOZBLAS_STATUS_CUDA_ERROR;
+    cuuint64_t gdim[2] = {cols, rows};
+    cuuint64_t gstride[1] = {cols};
+    cuuint32_t box[2] = {(cuuint32_t)I8_BK, box_rows};
+    cuuint32_t estr[2] = {1, 1};
+    CUresult r = enc(map, CU_TENSOR_MAP_DATA_TYPE_UINT8, 2, (void *)base, gdim, gstride, box, estr,
+                     CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                     CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    return r == CUDA_SUCCESS ? CUOZBLAS_STATUS_SUCCESS : CUOZBLAS_STATUS_CUDA_ERROR;
+}
+
+struct DigitOperand {
+    int8_t *digits = nullptr;  // S x lines_pad x k_pad
+    int *e = nullptr;          // line exponents
+    int S = 0, need = 0, lines_pad = 0;
+};
+
+// Lines of op(X): `strided` = element (line l, i) at X[i*ldx + l].
+static int split_digits(cuozblasHandle_t *h, bool strided, int nl, int k, const double *X, int ldx, int cap,
+                        int k_pad, int line_quantum, DigitOperand &op, Arena &ar) {
+    State *st = state(h);
+    const double *src = X;
+    int lds = ldx;
+    if (strided) {
+        double *tmp = ar.take<double>((uint64_t)nl * (k > 0 ? k : 1));
+        if (!ar.ok) return CUOZBLAS_STATUS_WORKSPACE;
+        OZB_TRY(transpose(h, nl, k, X, ldx, tmp, k));
+        src = tmp;
+        lds = k;
+    }
+    op.lines_pad = (nl + line_quantum - 1) / line_quantum * line_quantum;
+    op.e = ar.take<int>(nl > 0 ? nl : 1);
+    if (!ar.ok) return CUOZBLAS_STATUS_WORKSPACE;
+    OZB_CHECK(cudaMemsetAsync(st->d_ints, 0, sizeof(int), st->stream));
+    if (nl > 0) k_digit_count<<<nl, 256, 0, st->stream>>>(k, nl, src, lds, op.e, st->d_ints);
+    OZB_CHECK(cudaGetLastError());
+    OZB_CHECK(cudaMemcpyAsync(st->h_ints, st->d_ints, sizeof(int), cudaMemcpyDeviceToHost, st->stream));
+    OZB_CHECK(cudaStreamSynchronize(st->stream));
+    op.need = st->h_ints[0];
+    op.S = op.need < 1 ? 1 : op.need;
+    if (cap > 0 && op.S > cap) op.S = cap;
+    op.digits = ar.take<int8_t>((uint64_t)op.S * op.lines_pad * k_pad);
+    if (!ar.ok) return CUOZBLAS_STATUS_WORKSPACE;
+    const int64_t chunks = (int64_t)op.lines_pad * (k_pad / 16);
+    k_digit_write<<<(unsigned)((chunks + 255) / 256), 256, 0, st->stream>>>(k, nl, op.lines_pad, k_pad, op.S, src,
+                                                                             lds, op.e, op.digits);
+    OZB_CHECK(cudaGetLastError());
+    return CUOZBLAS_STATUS_SUCCESS;
+}
+
+// Default digit cap when nSplitMax is 0 (enough for an exact split of
+// values whose lines span ~2^80; larger spans are truncated).
+constexpr int kI8DefaultCap = 19;
+
+int gemm_i8_core(cuozblasHandle_t *h, char ta, char tb, int m, int n, int k, double alpha, const double *A, int lda,
+                 const double *B, int ldb, double beta, double *C, int ldc) {
+    State *st = state(h);
+    Arena ar(h);
+    const int k_pad = (k + I8_BK - 1) / I8_BK * I8_BK;
+    const int cap = h->nSplitMax > 0 ? h->nSplitMax : kI8DefaultCap;
+    DigitOperand da, db;
+    ev_record(h, 0);
+    OZB_TRY(split_digits(h, !is_trans(ta), m, k, A, lda, cap, k_pad, I8_BM, da, ar));
+    ev_record(h, 1);
+    OZB_TRY(split_digits(h, is_trans(tb), n, k, B, ldb, cap, k_pad, I8_BN, db, ar));
+    const int nA = da.S, nB = db.S;
+    // pair set: full, or the triangle ia + ib <= min(nA, nB) - 1 (fastMode, src/cuda/cuozblas_gemm.cu:138)
+    const int maxlevel = h->fastMode ? (nA < nB ? nA : nB) - 1 : nA + nB - 2;
+    const int nkb = k_pad / I8_BK;
+    // products per output in one INT32 group: (kb1 - kb0) * 128 each
+    const int64_t kb_cap = I8_MAX_TERMS / I8_BK;  // k-blocks per group
+    std::vector<int4> items, groups;
+    std::vector<int64_t> gbound;  // max |V| of each group (products x 127^2)
+    int npairs = 0;
+    for (int L = maxlevel; L >= 0; L--) {  // smallest level sums first
+        const int lo = L - (nB - 1) > 0 ? L - (nB - 1) : 0, hi = L < nA - 1 ? L : nA - 1;
+        int64_t used = 0;
+        int gbeg = (int)items.size();
+        for (int ia = lo; ia <= hi; ia++) {
+            npairs++;
+            for (int kb0 = 0; kb0 < nkb;) {
+                int64_t room = kb_cap - used;
+                if (room <= 0) {
+                    groups.push_back(make_int4(gbeg, (int)items.size(), L, 0));
+                    gbound.push_back(used * I8_BK * 127 * 127);
+                    gbeg = (int)items.size();
+                    used = 0;
+                    room = kb_cap;
+                }
+                const int kb1 = (int)((nkb - kb0) < room ? nkb : kb0 + room);
+                items.push_back(make_int4(ia, L - ia, kb0, kb1));
+                used += kb1 - kb0;
+                kb0 = kb1;
+            }
+        }
+        if ((int)items.size() > gbeg) {
+            groups.push_back(make_int4(gbeg, (int)items.size(), L, 0));
+            gbound.push_back(used * I8_BK * 127 * 127);
+        }
+    }
+    // Runs of consecutive levels whose exact combination stays below 2^53:
+    // level L of a run starting at L_hi is shifted by 7 (L_hi - L) bits; the
+    // run's last group flushes acc * 2^(-7 (L_hi + 2)) into R.
+    {
+        const unsigned __int128 lim = (unsigned __int128)1 << 53;
+        size_t i = 0;
+        bool first = true;
+        while (i < groups.size()) {
+            const int Lhi = groups[i].z;
+            unsigned __int128 sum = 0;
+            size_t j = i;
+            while (j < groups.size()) {
+                const int L = groups[j].z, d = Lhi - L;
+                size_t je = j;
+                unsigned __int128 lb = 0;
+                while (je < groups.size() && groups[je].z == L) lb += (unsigned __int128)gbound[je++];
+                lb <<= 7 * d;
+                if (j > i && sum + lb >= lim) break;
+                sum += lb;
+                for (size_t t = j; t < je; t++) groups[t].w = 7 * d;
+                j = je;
+            }
+            groups[j - 1].w |= (1 << 8) | (first ? (1 << 9) : 0);
+            groups[j - 1].z = -7 * (Lhi + 2);
+            for (size_t t = i; t + 1 < j; t++) groups[t].z = 0;
+            first = false;
+            i = j;
+        }
+        groups.back().w |= (1 << 10);
+    }
+    h->nSplitA = (float)nA;
+    h->nSplitB = (float)nB;
+    h->nSplitC = (float)npairs;
+    h->mbk = m;
+    h->nbk = n;
+    int4 *d_sched = ar.take<int4>(items.size() + groups.size());
+    int *d_err = ar.take<int>(1);
+    if (!ar.ok) return CUOZBLAS_STATUS_WORKSPACE;
+    std::vector<int4> sched(items);
+    sched.insert(sched.end(), groups.begin(), groups.end());
+    OZB_CHECK(cudaMemcpyAsync(d_sched, sched.data(), sizeof(int4) * sched.size(), cudaMemcpyHostToDevice,
+                              st->stream));
+    OZB_CHECK(cudaMemsetAsync(d_err, 0, sizeof(int), st->stream));
+
+    CUtensorMap tmA, tmB;
+    OZB_TRY(make_map(&tmA, da.digits, (uint64_t)nA * da.lines_pad, k_pad, I8_BM));
+    OZB_TRY(make_map(&tmB, db.digits, (uint64_t)nB * db.lines_pad, k_pad, I8_BN));
+    I8Params p;
+    p.m = m;
+    p.n = n;
+    p.m_pad = da.lines_pad;
+    p.n_pad = db.lines_pad;
+    p.ldc = ldc;
+    p.tiles_m = da.lines_pad / I8_BM;
+    p.tiles_n = db.lines_pad / I8_BN;
+    p.n_items = (int)items.size();
+    p.n_groups = (int)groups.size();
+    p.items = d_sched;
+    p.groups = d_sched + items.size();
+    p.ea = da.e;
+    p.eb = db.e;
+    p.alpha = alpha;
+    p.beta = beta;
+    p.C = C;
+    p.err = d_err;
+    int dev = 0, nsm = 0;
+    OZB_CHECK(cudaGetDevice(&dev));
+    OZB_CHECK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+    const int ntiles = p.tiles_m * p.tiles_n;
+    const int grid = ntiles < nsm ? ntiles : nsm;
+    OZB_CHECK(cudaFuncSetAttribute(k_i8_gemm, cudaFuncAttributeMaxDynamicSharedMemorySize, I8_SMEM));
+    ev_record(h, 2);
+    k_i8_gemm<<<grid, I8_THREADS, I8_SMEM, st->stream>>>(tmA, tmB, p);
+    OZB_CHECK(cudaGetLastError());
+    ev_record(h, 3);
+    OZB_CHECK(cudaMemcpyAsync(st->h_ints, d_err, sizeof(int), cudaMemcpyDeviceToHost, st->stream));
+    OZB_CHECK(cudaStreamSynchronize(st->stream));
+    if (st->h_ints[0] != 0) {
+        fprintf(stderr, "cuozblas: INT8 GEMM kernel wait timed out (code %d)\n", st->h_ints[0]);
+        return CUOZBLAS_STATUS_DEVICE_TIMEOUT;
+    }
+    h->t_SplitA = ev_ms(h, 0, 1) * 1e-3f;
+    h->t_SplitB = ev_ms(h, 1, 2) * 1e-3f;
+    h->t_comp = ev_ms(h, 2, 3) * 1e-3f;
+    h->t_sum = 0.f;  // fused into the product kernel
+    return CUOZBLAS_STATUS_SUCCESS;
+}
+
+}  // namespace ozb
+
+extern "C" int cuozblasDgemmI8(cuozblasHandle_t *h, char transa, char transb, int32_t m, int32_t n, int32_t k,
+                               double alpha, const double *A, int32_t lda, const double *B, int32_t ldb, double beta,
+                               double *C, int32_t ldc) {
+    using namespace ozb;
+    OZB_TRY(counter_init(h));
+    if (m < 0 || n < 0 || k < 0 || ldc < (m > 1 ? m : 1)) return CUOZBLAS_STATUS_INVALID_VALUE;
+    if (h->nSplitMax < 0 || h->nSplitMax > 64) return CUOZBLAS_STATUS_INVALID_VALUE;
+    if (m == 0 || n == 0) return CUOZBLAS_STATUS_SUCCESS;
+    return gemm_i8_core(h, transa, transb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc);
+}

@@ -1,0 +1,443 @@
+// gemm_plain.cu — the plain (FP64-slice) Ozaki GEMM and the skinny forms it
+// serves (GEMV, DOT), src/cuda/cuozblas_gemm.cu:7-284 / src/cpu/ozblas_gemm.cpp:3-315.
+//
+// Slices are exact: a slice of a line of length k carries at most 53 - rho
+// significant bits on a common grid, rho = ceil(53 - (53 - log2 k)/2), so
+// any sum of k slice products is exact in FP64 (src/cuda/cuozblas_split.cu:51-67).
+// The product of one slice pair is therefore the same in any order or
+// association, which lets the FP64 tensor pipe (DMMA) compute it.  What
+// fixes the bits is (1) the split and (2) the order of the pair sum, which
+// the fused epilogue follows exactly.
+#include "ozb_internal.h"
+#include "sum.cuh"
+
+namespace ozb {
+
+// ---------------------------------------------------------------------------
+// DMMA tile kernel.  CTA tile 64x64, k-tile 16, 4 warps (2x2), warp tile
+// 32x32 = 4x4 mma.m8n8k4.f64 fragments.  Operands are K-major slices:
+// A slice ia: m lines x ldk, B slice ib: n lines x ldk (ldk % 16 == 0, zero
+// padded).  The (pair, k-tile) sequence is one software pipeline; at each
+// pair boundary the exact pair product is added to the running FP64 sum in
+// summation order (FSUM) or stored to the pair buffer (STORE).
+// ---------------------------------------------------------------------------
+constexpr int kBM = 64, kBN = 64, kBK = 16, kLds = kBK + 4;  // row stride 20 doubles: conflict-free fragments
+
+struct PairList {
+    const int2 *pairs;  // (ia, ib) in summation order
+    int np;
+};
+
+__device__ __forceinline__ void cp_async16(void *smem, const void *gmem, bool pred) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    const int sz = pred ? 16 : 0;
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(s), "l"(gmem), "r"(sz));
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+    asm volatile("cp.async.wait_group %0;\n" ::"n"(N));
+}
+
+__device__ __forceinline__ void dmma884(double &c0, double &c1, double a, double b) {
+    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
+                 : "+d"(c0), "+d"(c1)
+                 : "d"(a), "d"(b));
+}
+
+template <bool STORE>
+__global__ void __launch_bounds__(128) k_gemm_pairs_dmma(int m, int n, int nlB, int ldk, const double *__restrict__ As,
+                                                         const double *__restrict__ Bs, const int2 *__restrict__ pairs,
+                                                         int np, double alpha, double beta, double *__restrict__ C,
+                                                         int ldc, double *__restrict__ pbuf) {
+    __shared__ __align__(16) double sA[2][kBM][kLds];
+    __shared__ __align__(16) double sB[2][kBN][kLds];
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int wm = warp >> 1, wn = warp & 1;
+    const int m0 = blockIdx.x * kBM, n0 = blockIdx.y * kBN;
+    const int nkt = ldk / kBK;
+    const int total = np * nkt;
+
+    double acc[4][4][2], t[4][4][2];
+#pragma unroll
+    for (int i = 0; i < 4; i++)
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+            acc[i][j][0] = acc[i][j][1] = 0.0;
+            t[i][j][0] = t[i][j][1] = 0.0;
+        }
+
+    // each thread copies 4 x 16B of A and of B per k-tile (64 lines x 8 chunks)
+    auto load_tile = [&](int step, int buf) {
+        const int p = step / nkt, kt = step - p * nkt;
+        const int2 pr = pairs[p];
+        const double *a = As + ((size_t)pr.x * m) * ldk + (size_t)kt * kBK;
+        const double *b = Bs + ((size_t)pr.y * nlB) * ldk + (size_t)kt * kBK;  // nlB: lines per B slice
+#pragma unroll
+        for (int c = 0; c < 4; c++) {
+            const int idx = tid + c * 128;  // 0..511
+            const int row = idx >> 3, ch = idx & 7;
+            const int gr = m0 + row, gc = n0 + row;
+            cp_async16(&sA[buf][row][ch * 2], a + (size_t)(gr < m ? gr : 0) * ldk + ch * 2, gr < m);
+            cp_async16(&sB[buf][row][ch * 2], b + (size_t)(gc < n ? gc : 0) * ldk + ch * 2, gc < n);
+        }
+    };
+
+    if (total > 0) load_tile(0, 0);
+    cp_async_commit();
+    for (int step = 0; step < total; step++) {
+        const int buf = step & 1;
+        if (step + 1 < total) load_tile(step + 1, buf ^ 1);
+        cp_async_commit();
+        cp_async_wait<1>();
+        __syncthreads();
+#pragma unroll
+        for (int kk = 0; kk < kBK; kk += 4) {
+            double af[4], bf[4];
+#pragma unroll
+            for (int i = 0; i < 4; i++) af[i] = sA[buf][wm * 32 + i * 8 + (lane >> 2)][kk + (lane & 3)];
+#pragma unroll
+            for (int j = 0; j < 4; j++) bf[j] = sB[buf][wn * 32 + j * 8 + (lane >> 2)][kk + (lane & 3)];
+#pragma unroll
+            for (int i = 0; i < 4; i++)
+#pragma unroll
+                for (int j = 0; j < 4; j++) dmma884(acc[i][j][0], acc[i][j][1], af[i], bf[j]);
+        }
+        __syncthreads();
+        const int p = step / nkt;
+        if (step - p * nkt == nkt - 1) {  // pair complete: acc is the exact product of pair p
+            if (STORE) {
+#pragma unroll
+                for (int i = 0; i < 4; i++)
+#pragma unroll
+                    for (int j = 0; j < 4; j++)
+#pragma unroll
+                        for (int h = 0; h < 2; h++) {
+                            const int r = m0 + wm * 32 + i * 8 + (lane >> 2);
+                            const int c = n0 + wn * 32 + j * 8 + (lane & 3) * 2 + h;
+                            if (r < m && c < n) pbuf[((size_t)p * n + c) * m + r] = acc[i][j][h];
+                            acc[i][j][h] = 0.0;
+                        }
+            } else {
+#pragma unroll
+                for (int i = 0; i < 4; i++)
+#pragma unroll
+                    for (int j = 0; j < 4; j++)
+#pragma unroll
+                        for (int h = 0; h < 2; h++) {
+                            t[i][j][h] += acc[i][j][h];
+                            acc[i][j][h] = 0.0;
+                        }
+            }
+        }
+    }
+    if (!STORE) {
+#pragma unroll
+        for (int i = 0; i < 4; i++)
+#pragma unroll
+            for (int j = 0; j < 4; j++)
+#pragma unroll
+                for (int h = 0; h < 2; h++) {
+                    const int r = m0 + wm * 32 + i * 8 + (lane >> 2);
+                    const int c = n0 + wn * 32 + j * 8 + (lane & 3) * 2 + h;
+                    if (r < m && c < n) {
+                        double *cp = &C[(size_t)c * ldc + r];
+                        *cp = fma(alpha, t[i][j][h], beta * *cp);
+                    }
+                }
+    }
+}
+
+// Sum a pair buffer (pair p of np at pbuf + p*ld_pair, element e at + e) in
+// summation order; output element e (row e % m, column e / m) of C.
+__global__ void k_sum_pairs(int m, int64_t count, int np, const double *__restrict__ pbuf_c, int64_t ld_pair,
+                            int sum_mode, double alpha, double beta, double *__restrict__ C, int ldc) {
+    const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= count) return;
+    double *pbuf = const_cast<double *>(pbuf_c);
+    double t = 0.0;
+    if (sum_mode == 1) {
+        t = nearsum(np, pbuf + e, ld_pair);
+    } else {
+        for (int p = 0; p < np; p++) t += pbuf[p * ld_pair + e];
+    }
+    const int64_t r = e % m, c = e / m;
+    double *cp = &C[c * ldc + r];
+    *cp = fma(alpha, t, beta * *cp);
+}
+
+// ---------------------------------------------------------------------------
+// Skinny products: P[ia][ib] over n elements for slice vectors (DOT) —
+// at most 8 x 8 pairs per launch, exact, so atomic accumulation order does
+// not change the bits.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) k_pair_dot(int n, int nA, int nB, const double *__restrict__ xs, int ldx,
+                                                  const double *__restrict__ ys, int ldy, double *__restrict__ P,
+                                                  int ldp) {
+    double acc[8][8];
+#pragma unroll
+    for (int a = 0; a < 8; a++)
+#pragma unroll
+        for (int b = 0; b < 8; b++) acc[a][b] = 0.0;
+    const size_t stride = (size_t)gridDim.x * blockDim.x;
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < (size_t)n; i += stride) {
+        double xa[8], yb[8];
+#pragma unroll
+        for (int a = 0; a < 8; a++) xa[a] = a < nA ? xs[(size_t)a * ldx + i] : 0.0;
+#pragma unroll
+        for (int b = 0; b < 8; b++) yb[b] = b < nB ? ys[(size_t)b * ldy + i] : 0.0;
+#pragma unroll
+        for (int a = 0; a < 8; a++)
+#pragma unroll
+            for (int b = 0; b < 8; b++) acc[a][b] = fma(xa[a], yb[b], acc[a][b]);
+    }
+    __shared__ double red[8][8][8];
+    const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+#pragma unroll
+    for (int a = 0; a < 8; a++)
+#pragma unroll
+        for (int b = 0; b < 8; b++) {
+            double v = acc[a][b];
+            for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+            if (l == 0) red[w][a][b] = v;
+        }
+    __syncthreads();
+    if (threadIdx.x < 64) {
+        const int a = threadIdx.x >> 3, b = threadIdx.x & 7;
+        if (a < nA && b < nB) {
+            double v = 0.0;
+            for (int i = 0; i < 8; i++) v += red[i][a][b];
+            atomicAdd(&P[a * ldp + b], v);
+        }
+    }
+}
+
+// One scalar result from a pair matrix P[ia * ldp + ib] (DOT): FSum or NearSum.
+__global__ void k_sum_pair_matrix(int nA, int nB, int maxlevel, const double *__restrict__ P, int ldp, int sum_mode,
+                                  double alpha, double beta, double *__restrict__ out, double *__restrict__ tmp) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    double t = 0.0;
+    if (sum_mode == 1) {
+        int np = 0;
+        for_each_pair(nA, nB, maxlevel, [&](int ia, int ib) { tmp[np++] = P[ia * ldp + ib]; });
+        t = nearsum(np, tmp, 1);
+    } else {
+        for_each_pair(nA, nB, maxlevel, [&](int ia, int ib) { t += P[ia * ldp + ib]; });
+    }
+    *out = fma(alpha, t, beta * *out);
+}
+
+// GEMV pairs: one warp per row i; P[p][i] = sum_k As[ia][i][k] * xs[ib][k]
+// for the pairs given (at most 8 x 8 block per launch).  Exact.
+__global__ void __launch_bounds__(256) k_pair_gemv(int m, int k, int na, int nb, int ia0, int ib0, int nBtot,
+                                                   const double *__restrict__ As, int ldk,
+                                                   const double *__restrict__ xs, int ldx, double *__restrict__ P,
+                                                   int64_t ldp) {
+    const int row = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+    if (row >= m) return;
+    double acc[8][8];
+#pragma unroll
+    for (int a = 0; a < 8; a++)
+#pragma unroll
+        for (int b = 0; b < 8; b++) acc[a][b] = 0.0;
+    for (int i = lane; i < k; i += 32) {
+        double xa[8], yb[8];
+#pragma unroll
+        for (int a = 0; a < 8; a++) xa[a] = a < na ? As[((size_t)(ia0 + a) * m + row) * ldk + i] : 0.0;
+#pragma unroll
+        for (int b = 0; b < 8; b++) yb[b] = b < nb ? xs[(size_t)(ib0 + b) * ldx + i] : 0.0;
+#pragma unroll
+        for (int a = 0; a < 8; a++)
+#pragma unroll
+            for (int b = 0; b < 8; b++) acc[a][b] = fma(xa[a], yb[b], acc[a][b]);
+    }
+#pragma unroll
+    for (int a = 0; a < 8; a++)
+#pragma unroll
+        for (int b = 0; b < 8; b++) {
+            double v = acc[a][b];
+            for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+            if (lane == 0 && a < na && b < nb) P[(size_t)((ia0 + a) * nBtot + (ib0 + b)) * ldp + row] = v;
+        }
+}
+
+// Sum a per-row pair buffer P[(ia*nB+ib)*ldp + row] in order; y = fma(alpha, t, beta*y).
+// NearSum gathers the terms in summation order into `scratch` (np x ldp).
+__global__ void k_sum_rows(int m, int nA, int nB, int maxlevel, double *__restrict__ P, int64_t ldp, int sum_mode,
+                           double alpha, double beta, double *__restrict__ y, double *__restrict__ scratch) {
+    const int row = blockIdx.x * blockDim.x + threadIdx.x;
+    if (row >= m) return;
+    double t = 0.0;
+    if (sum_mode == 1) {
+        int np = 0;
+        for_each_pair(nA, nB, maxlevel, [&](int ia, int ib) {
+            scratch[(size_t)np * ldp + row] = P[(size_t)(ia * nB + ib) * ldp + row];
+            np++;
+        });
+        t = nearsum(np, scratch + row, ldp);
+    } else {
+        for_each_pair(nA, nB, maxlevel, [&](int ia, int ib) { t += P[(size_t)(ia * nB + ib) * ldp + row]; });
+    }
+    y[row] = fma(alpha, t, beta * y[row]);
+}
+
+// ---------------------------------------------------------------------------
+// Host drivers
+// ---------------------------------------------------------------------------
+static int ceil_to(int v, int q) { return (v + q - 1) / q * q; }
+
+// Split op(A) by rows (lines of length k) into ns slices of m x ldk.  If A is
+// 'n' (m x k, column-major) it is first transposed so every line is contiguous.
+static int split_operand(cuozblasHandle_t *h, bool lines_strided, int nl, int k, const double *X, int ldx, int rho,
+                         int maxS, int ldk, double **slices, int *ns, Arena &ar) {
+    const double *src = X;
+    int lds = ldx;
+    double *tmp = nullptr;
+    const uint64_t mk = ar.mark();
+    if (lines_strided) {  // element (line l, i) at X[i * ldx + l]
+        tmp = ar.take<double>((uint64_t)nl * (k > 0 ? k : 1));
+        if (!ar.ok) return CUOZBLAS_STATUS_WORKSPACE;
+        OZB_TRY(transpose(h, nl, k, X, ldx, tmp, k));
+        src = tmp;
+        lds = k;
+    }
+    OZB_TRY(split_lines_count(h, k, nl, src, lds, rho, maxS, ns));
+    // slices go below the temporary so the temporary can be released after
+    double *out;
+    if (tmp) {
+        // place the slices after the transposed copy, then compact is unnecessary:
+        out = ar.take<double>((uint64_t)(*ns) * nl * ldk);
+    } else {
+        out = ar.take<double>((uint64_t)(*ns) * nl * ldk);
+    }
+    if (!ar.ok) return CUOZBLAS_STATUS_WORKSPACE;
+    OZB_TRY(split_lines_write(h, k, nl, src, lds, rho, *ns, out, ldk));
+    (void)mk;
+    *slices = out;
+    return CUOZBLAS_STATUS_SUCCESS;
+}
+
+int gemm_plain_core(cuozblasHandle_t *h, char ta, char tb, int m, int n, int k, double alpha, const double *A,
+                    int lda, const double *B, int ldb, double beta, double *C, int ldc, int fastMode) {
+    State *st = state(h);
+    const int maxS = h->nSplitMax > 0 ? h->nSplitMax : kMaxSplitDefault;
+    const int rho = rho_rule(k, h->splitEpsMode);
+    Arena ar(h);
+    const bool dot = (m == 1 && n == 1);
+    const bool skinny_n = (n == 1);
+    const int ldk = dot || skinny_n ? ceil_to(k > 0 ? k : 1, 2) : ceil_to(k > 0 ? k : 1, kBK);
+
+    // ---- split ----
+    double *Sa = nullptr, *Sb = nullptr;
+    int nA = 0, nB = 0;
+    if (dot) {
+        Sa = ar.take<double>((uint64_t)maxS * ldk);
+        if (!ar.ok) return CUOZBLAS_STATUS_WORKSPACE;
+        OZB_TRY(split_vector(h, k, A, rho, maxS, Sa, ldk, &nA));
+    } else {
+        // lines of op(A): 'n' -> row i of A is strided by lda
+        OZB_TRY(split_operand(h, !is_trans(ta), m, k, A, lda, rho, maxS, ldk, &Sa, &nA, ar));
+    }
+    if (skinny_n) {
+        Sb = ar.take<double>((uint64_t)maxS * ldk);
+        if (!ar.ok) return CUOZBLAS_STATUS_WORKSPACE;
+        OZB_TRY(split_vector(h, k, B, rho, maxS, Sb, ldk, &nB));
+    } else {
+        OZB_TRY(split_operand(h, is_trans(tb), n, k, B, ldb, rho, maxS, ldk, &Sb, &nB, ar));
+    }
+    const int fast = dot ? 0 : fastMode;
+    int maxlevel = (nA - 1) + (nB - 1);
+    {
+        const int mn = nA - 1 < nB - 1 ? nA - 1 : nB - 1;
+        maxlevel = (maxlevel - fast) > mn ? (maxlevel - fast) : mn;  // src/cpu/ozblas_gemm.cpp:163-164
+    }
+    int np = 0;
+    for_each_pair(nA, nB, maxlevel, [&](int, int) { np++; });
+    h->nSplitA = (float)nA;
+    h->nSplitB = (float)nB;
+    h->nSplitC = dot ? 1.f : (skinny_n && fast == 0 ? (float)(maxlevel + 1 < nA ? maxlevel + 1 : nA) : (float)np);
+    h->mbk = m;
+    h->nbk = n;
+
+    if (dot || skinny_n) {
+        // pair products into P[(ia*nB+ib)][row]
+        const int rows = dot ? 1 : m;
+        const int64_t ldp = rows;
+        double *P = ar.take<double>((uint64_t)nA * nB * ldp);
+        double *scr = ar.take<double>((uint64_t)nA * nB * ldp + 1);
+        if (!ar.ok) return CUOZBLAS_STATUS_WORKSPACE;
+        OZB_CHECK(cudaMemsetAsync(P, 0, sizeof(double) * nA * nB * ldp, st->stream));
+        for (int ia0 = 0; ia0 < nA; ia0 += 8)
+            for (int ib0 = 0; ib0 < nB; ib0 += 8) {
+                const int na = nA - ia0 < 8 ? nA - ia0 : 8, nb = nB - ib0 < 8 ? nB - ib0 : 8;
+                if (dot) {
+                    // P block at (ia0, ib0) with row stride nB
+                    int blocks = (k + 255) / 256;
+                    if (blocks > 148 * 8) blocks = 148 * 8;
+                    if (blocks < 1) blocks = 1;
+                    k_pair_dot<<<blocks, 256, 0, st->stream>>>(k, na, nb, Sa + (size_t)ia0 * ldk, ldk,
+                                                               Sb + (size_t)ib0 * ldk, ldk, P + ia0 * nB + ib0, nB);
+                } else {
+                    const int blocks = (int)(((int64_t)m * 32 + 255) / 256);
+                    k_pair_gemv<<<blocks, 256, 0, st->stream>>>(m, k, na, nb, ia0, ib0, nB, Sa, ldk, Sb, ldk, P,
+                                                                ldp);
+                }
+                OZB_CHECK(cudaGetLastError());
+            }
+        if (dot) {
+            k_sum_pair_matrix<<<1, 32, 0, st->stream>>>(nA, nB, maxlevel, P, nB, h->sumMode, alpha, beta, C, scr);
+        } else {
+            k_sum_rows<<<(m + 127) / 128, 128, 0, st->stream>>>(m, nA, nB, maxlevel, P, ldp, h->sumMode, alpha, beta,
+                                                              C, scr);
+        }
+        OZB_CHECK(cudaGetLastError());
+        return CUOZBLAS_STATUS_SUCCESS;
+    }
+
+    // ---- general GEMM ----
+    int2 *hp = new int2[np > 0 ? np : 1];
+    int q = 0;
+    for_each_pair(nA, nB, maxlevel, [&](int ia, int ib) { hp[q++] = make_int2(ia, ib); });
+    int2 *dp = ar.take<int2>(np > 0 ? np : 1);
+    if (!ar.ok) {
+        delete[] hp;
+        return CUOZBLAS_STATUS_WORKSPACE;
+    }
+    cudaError_t ce = cudaMemcpyAsync(dp, hp, sizeof(int2) * np, cudaMemcpyHostToDevice, st->stream);
+    cudaError_t ce2 = cudaStreamSynchronize(st->stream);
+    delete[] hp;
+    OZB_CHECK(ce);
+    OZB_CHECK(ce2);
+    dim3 grid((m + kBM - 1) / kBM, (n + kBN - 1) / kBN);
+    if (h->sumMode == 1) {
+        // pair products to a buffer, blocked over columns if the arena is short
+        const uint64_t avail = h->workSizeBytes - ((ar.mark() + 255) / 256 * 256);
+        int64_t ncols = (int64_t)(avail / (sizeof(double) * (uint64_t)np * (uint64_t)m));
+        if (ncols >= n) {
+            ncols = n;
+        } else {
+            ncols = ncols / kBN * kBN;
+            if (ncols == 0) return CUOZBLAS_STATUS_WORKSPACE;
+        }
+        double *pbuf = ar.take<double>((uint64_t)np * m * ncols);
+        if (!ar.ok) return CUOZBLAS_STATUS_WORKSPACE;
+        for (int64_t c0 = 0; c0 < n; c0 += ncols) {
+            const int nc = (int)((n - c0) < ncols ? (n - c0) : ncols);
+            dim3 g((m + kBM - 1) / kBM, (nc + kBN - 1) / kBN);
+            k_gemm_pairs_dmma<true><<<g, 128, 0, st->stream>>>(m, nc, n, ldk, Sa, Sb + (size_t)c0 * ldk, dp, np, alpha,
+                                                               beta, C, ldc, pbuf);
+            OZB_CHECK(cudaGetLastError());
+            const int64_t count = (int64_t)m * nc;
+            k_sum_pairs<<<(unsigned)((count + 255) / 256), 256, 0, st->stream>>>(
+                m, count, np, pbuf, count, 1, alpha, beta, C + (size_t)c0 * ldc, ldc);
+            OZB_CHECK(cudaGetLastError());
+        }
+    } else {
+        k_gemm_pairs_dmma<false><<<grid, 128, 0, st->stream>>>(m, n, n, ldk, Sa, Sb, dp, np, alpha, beta, C, ldc,
+                                                               nullptr);
+        OZB_CHECK(cudaGetLastError());
+    }
+    return CUOZBLAS_STATUS_SUCCESS;
+}
+
+}  // namespace ozb

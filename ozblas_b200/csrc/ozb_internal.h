@@ -1,0 +1,114 @@
+// ozb_internal.h — host-side state shared by the library's translation units.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <stdio.h>
+
+#include "../../include/cuozblas.h"
+#include "ozb_rules.cuh"
+
+namespace ozb {
+
+constexpr int kMaxSplitDefault = 30;  // NumSplitDefaultMax, src/cuda/cuozblas_common.h:5
+constexpr int kArenaAlign = 256;
+
+// Per-handle private state; the reference handle's hstBatchAddr field points
+// here (the batched-GEMM pointer arrays it held in the reference have no
+// counterpart in this library).
+struct State {
+    cudaStream_t stream = 0;
+    uint64_t off = 0;             // bump pointer into h->devWork
+    uint64_t high_water = 0;
+    int *d_ints = nullptr;        // small device int scratch (counters, error word)
+    int *h_ints = nullptr;        // pinned host mirror
+    double *h_dbl = nullptr;      // pinned host doubles (scalar results)
+    int last_error = 0;
+    int64_t splitA_ld = 0;        // slice stride of the pre-split A (cuozblasDcsrmvSplitA)
+    cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};  // phase timers (split A/B, products)
+};
+
+
+inline State *state(cuozblasHandle_t *h) { return reinterpret_cast<State *>(h->hstBatchAddr); }
+
+// Phase timers of the reference handle (t_SplitA, t_SplitB, t_comp), taken
+// with CUDA events on the handle's stream; read after the call's final sync.
+inline void ev_record(cuozblasHandle_t *h, int i) { cudaEventRecord(state(h)->ev[i], state(h)->stream); }
+inline float ev_ms(cuozblasHandle_t *h, int a, int b) {
+    float ms = 0.f;
+    if (cudaEventElapsedTime(&ms, state(h)->ev[a], state(h)->ev[b]) != cudaSuccess) return 0.f;
+    return ms;
+}
+
+// Bump allocation from the handle's arena (no cudaMalloc on the call path).
+struct Arena {
+    cuozblasHandle_t *h;
+    State *st;
+    bool ok = true;
+    explicit Arena(cuozblasHandle_t *hh) : h(hh), st(state(hh)) {}
+    template <typename T>
+    T *take(uint64_t count) {
+        uint64_t bytes = count * sizeof(T);
+        uint64_t start = (st->off + kArenaAlign - 1) / kArenaAlign * kArenaAlign;
+        if (start + bytes > h->workSizeBytes) {
+            ok = false;
+            return nullptr;
+        }
+        st->off = start + bytes;
+        if (st->off > st->high_water) st->high_water = st->off;
+        h->memAddr = st->off;
+        return reinterpret_cast<T *>(h->devWork + start);
+    }
+    uint64_t mark() const { return st->off; }
+    void release(uint64_t m) { st->off = m; }
+};
+
+inline int cuda_status(cudaError_t e) { return e == cudaSuccess ? CUOZBLAS_STATUS_SUCCESS : CUOZBLAS_STATUS_CUDA_ERROR; }
+
+#define OZB_CHECK(call)                                                     \
+    do {                                                                    \
+        cudaError_t _e = (call);                                            \
+        if (_e != cudaSuccess) {                                            \
+            fprintf(stderr, "cuozblas: CUDA error %s at %s:%d\n",           \
+                    cudaGetErrorString(_e), __FILE__, __LINE__);            \
+            return CUOZBLAS_STATUS_CUDA_ERROR;                              \
+        }                                                                   \
+    } while (0)
+
+#define OZB_TRY(expr)                               \
+    do {                                            \
+        int _s = (expr);                            \
+        if (_s != CUOZBLAS_STATUS_SUCCESS) return _s; \
+    } while (0)
+
+inline bool is_trans(char t) { return !(t == 'n' || t == 'N'); }
+
+// Reference counterInit (src/cuda/cuozblas.cpp:3-21): resets the exec info,
+// splitShift and the arena pointer (keeping a pre-split A below memMaskSplitA).
+int counter_init(cuozblasHandle_t *h);
+
+// ---- split (split.cu) ----
+// Lines: `nl` lines of length k, line l at X + l*ldx (contiguous).  Returns
+// the split count in *ns (reference termination rule) and, when `out` is
+// non-null, writes ns slices of nl lines of ldo doubles (zero padded).
+int split_lines_count(cuozblasHandle_t *h, int k, int nl, const double *X, int ldx, int rho, int maxS, int *ns);
+int split_lines_write(cuozblasHandle_t *h, int k, int nl, const double *X, int ldx, int rho, int ns, double *out,
+                      int ldo);
+// Transpose rows x cols (column-major, ld) into cols x rows (ldo).
+int transpose(cuozblasHandle_t *h, int rows, int cols, const double *A, int lda, double *out, int ldo);
+// Vector split with one global tau chain (n-vector).  Writes ns slices of ldo.
+int split_vector(cuozblasHandle_t *h, int n, const double *x, int rho, int maxS, double *out, int ldo, int *ns);
+// CSR row split; slices laid out ns x nnz.  shift divides sigma.
+int split_csr_count(cuozblasHandle_t *h, int m, const double *val, const int *rowptr, int epsmode, int shift,
+                    int maxS, int *ns);
+int split_csr_write(cuozblasHandle_t *h, int m, int nnz, const double *val, const int *rowptr, int epsmode,
+                    int shift, int ns, double *out, int64_t ld);
+
+// ---- sums ----
+int fsum_pairs_dot(cuozblasHandle_t *h, int nA, int nB, int maxlevel, const double *pairmat, double alpha,
+                   double beta, double *out_dev);
+
+// ---- plain GEMM core (gemm_plain.cu) ----
+int gemm_plain_core(cuozblasHandle_t *h, char ta, char tb, int m, int n, int k, double alpha, const double *A,
+                    int lda, const double *B, int ldb, double beta, double *C, int ldc, int fastMode);
+
+}  // namespace ozb

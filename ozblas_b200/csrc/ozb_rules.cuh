@@ -1,0 +1,122 @@
+// ozb_rules.cuh — the integer rules that fix the bits of the Ozaki split.
+//
+// Shared by host and device code so that one definition is tested on the CPU
+// (against glibc, through the exported ozb_rule_* functions) and used by the
+// kernels.
+#pragma once
+#include <stdint.h>
+
+#if defined(__CUDACC__)
+#define OZB_HD __host__ __device__ __forceinline__
+#else
+#define OZB_HD inline
+#endif
+
+namespace ozb {
+
+OZB_HD uint64_t dbits(double v) {
+#if defined(__CUDA_ARCH__)
+    return (uint64_t)__double_as_longlong(v);
+#else
+    uint64_t b;
+    __builtin_memcpy(&b, &v, 8);
+    return b;
+#endif
+}
+
+OZB_HD int clz64(uint64_t x) {
+#if defined(__CUDA_ARCH__)
+    return __clzll((long long)x);
+#else
+    return x ? __builtin_clzll(x) : 64;
+#endif
+}
+
+OZB_HD int clz32(uint32_t x) {
+#if defined(__CUDA_ARCH__)
+    return __clz((int)x);
+#else
+    return x ? __builtin_clz(x) : 32;
+#endif
+}
+
+// ceil(log2(d)) for an integer d >= 1, exactly.
+OZB_HD int ceil_log2_int(uint32_t d) { return d <= 1 ? 0 : 32 - clz32(d - 1u); }
+
+// The split's tau: the reference evaluates (short)ceil(log2(max)) with libm
+// (src/cpu/ozblas_split.cpp:145; src/cuda/cuozblas_split.cu:201).  For
+// v = 2^e (1 + j 2^-52), log2(v) = e + log2(1 + j 2^-52) is rounded to the
+// nearest double; it rounds down onto the integer e exactly when
+// log2(1 + j 2^-52) is below half the spacing of doubles just above e, i.e.
+// when j <= floor(ln2 * 2^(p-1)) with 2^(p-53) that half spacing.  So the
+// result is e when j is at most that threshold and e + 1 otherwise.  The
+// thresholds below are floor(ln2 * 2^(p-1)) for p = -1 .. 10.  The rule is
+// pinned against glibc's log2 over every exponent by the CPU tests.
+// Zero, infinities and NaN (undefined behaviour in the reference, where it
+// never changes a slice) return 0.
+OZB_HD int tau_rule(double v) {
+    const uint64_t b = dbits(v) & 0x7fffffffffffffffULL;
+    const int be = (int)(b >> 52);
+    uint64_t j = b & ((1ULL << 52) - 1);
+    int e;
+    if (be == 0x7ff) return 0;
+    if (be == 0) {
+        if (j == 0) return 0;
+        const int msb = 63 - clz64(j);  // 0..51
+        e = msb - 1074;
+        j = (j << (52 - msb)) & ((1ULL << 52) - 1);
+    } else {
+        e = be - 1023;
+    }
+    if (j == 0) return e;
+    const int ae = e < 0 ? -e : e;
+    int p = (ae == 0) ? -1 : (31 - clz32((uint32_t)ae));
+    if (e < 0 && (ae & (ae - 1)) == 0) p -= 1;  // just above -2^q the spacing halves
+    int J;
+    switch (p) {
+        case 2: J = 1; break;
+        case 3: J = 2; break;
+        case 4: J = 5; break;
+        case 5: J = 11; break;
+        case 6: J = 22; break;
+        case 7: J = 44; break;
+        case 8: J = 88; break;
+        case 9: J = 177; break;
+        case 10: J = 354; break;
+        default: J = 0; break;  // p <= 1
+    }
+    return ((int64_t)j <= J) ? e : e + 1;
+}
+
+// rho = ceil(53 - (53 - log2(dim)) / 2) for splitEpsMode 0
+// (src/cpu/ozblas_split.cpp:19-34) as an exact integer rule: the smallest r
+// with 2^(2r - 53) >= dim.  Mode 9 ("overflow" variant) is
+// ceil(27 + log2(dim) / 4); mode 2 (Dot2) is ceil(log2(dim) / 2).
+OZB_HD int rho_rule(int dim, int splitEpsMode) {
+    const int L = ceil_log2_int(dim < 1 ? 1u : (uint32_t)dim);
+    if (splitEpsMode == 9) return 27 + (L + 3) / 4;
+    if (splitEpsMode == 2) return (L + 1) / 2;
+    const int t = (L & 1) ? L : L + 1;
+    return (t + 53) / 2;
+}
+
+OZB_HD double from_bits(uint64_t b) {
+#if defined(__CUDA_ARCH__)
+    return __longlong_as_double((long long)b);
+#else
+    double v;
+    __builtin_memcpy(&v, &b, 8);
+    return v;
+#endif
+}
+
+// 2^e exactly as scalbn(1., e) gives it (subnormal below -1022, 0 below
+// -1074, +inf above 1023).
+OZB_HD double pow2(int e) {
+    if (e > 1023) return from_bits(0x7ff0000000000000ULL);
+    if (e >= -1022) return from_bits((uint64_t)(e + 1023) << 52);
+    if (e >= -1074) return from_bits(1ULL << (e + 1074));
+    return 0.0;
+}
+
+}  // namespace ozb

@@ -1,0 +1,111 @@
+"""INT8 precision form (tcgen05) vs the exact oracle.
+
+There is no reference implementation of this form, so its oracle is the exact
+dot product (oracle/ozoracle.c, an exact fixed-point accumulator, pinned
+against mpmath in tests/test_oracle.py).  Tolerances are written per test:
+with a complete split and the full pair set every product is exact and only
+the final FP64 level sum rounds, so the componentwise error stays within
+2 units of 2^-53 relative; the plain FP64-slice form is run on the same
+inputs as the comparison point.
+"""
+import numpy as np
+import pytest
+
+from tests.conftest import bits_equal
+
+pytestmark = pytest.mark.gpu
+
+U = 2.0 ** -53
+
+
+def dev(torch, a):
+    return torch.from_numpy(np.ascontiguousarray(a)).cuda()
+
+
+def errors(oracle, A, B, C, m, n, k, rows=None, cols=None):
+    """max |c - exact| / |exact| over the sampled entries (A m x k, B k x n column-major)."""
+    rows = range(m) if rows is None else rows
+    cols = range(n) if cols is None else cols
+    At = np.ascontiguousarray(A.reshape(k, m).T) if A.ndim == 2 else A  # A stored (k, m): row j = column j
+    worst = 0.0
+    for j in cols:
+        b = np.ascontiguousarray(B[j, :k])
+        for i in rows:
+            _, rel = oracle.exact_dot_err(np.ascontiguousarray(At[i]), b, float(C[j, i]), n=k)
+            worst = max(worst, rel)
+    return worst
+
+
+def run_i8(ozb, handle, cuda, A, B, m, n, k, ta="n", tb="n", nsplit=0, fast=0, alpha=1.0, beta=0.0, C0=None):
+    handle.nSplitMax = nsplit
+    handle.fastMode = fast
+    dC = dev(cuda, C0) if C0 is not None else cuda.zeros((n, m), dtype=cuda.float64, device="cuda")
+    lda = A.shape[1]
+    ldb = B.shape[1]
+    ozb.dgemm_i8(handle, ta, tb, m, n, k, alpha, dev(cuda, A), lda, dev(cuda, B), ldb, beta, dC, m)
+    return dC.cpu().numpy()
+
+
+@pytest.mark.parametrize("m,n,k,phi", [(128, 128, 128, 1.0), (200, 130, 300, 1.0), (1, 1, 1, 1.0),
+                                       (64, 256, 1000, 0.5), (256, 256, 512, 2.0), (300, 77, 129, 4.0)])
+def test_i8_full_pairs_accuracy(m, n, k, phi, oracle, handle, ozb, cuda):
+    A = oracle.phi_matrix(m, k, phi, 1)  # shape (k, m): column-major m x k
+    B = oracle.phi_matrix(k, n, phi, 2)  # shape (n, k)
+    C = run_i8(ozb, handle, cuda, A, B, m, n, k)
+    rows = range(m) if m <= 128 else np.linspace(0, m - 1, 64).astype(int)
+    cols = range(n) if n <= 128 else np.linspace(0, n - 1, 64).astype(int)
+    err = errors(oracle, A, B, C, m, n, k, rows, cols)
+    assert err <= 2 * U, (err, handle.nSplitA, handle.nSplitB)
+
+
+def test_i8_transposes(oracle, handle, ozb, cuda):
+    m, n, k = 150, 90, 260
+    A = oracle.phi_matrix(k, m, 1.0, 1)  # stored k x m: op(A) = A^T with ta='t'
+    B = oracle.phi_matrix(n, k, 1.0, 2)  # stored n x k: op(B) = B^T with tb='t'
+    Cn = run_i8(ozb, handle, cuda, A, B, m, n, k, ta="t", tb="t")
+    An = np.ascontiguousarray(A.T)  # m x k column-major -> shape (k, m)
+    Bn = np.ascontiguousarray(B.T)
+    Cr = run_i8(ozb, handle, cuda, An, Bn, m, n, k)
+    assert bits_equal(Cn, Cr)
+
+
+def test_i8_alpha_beta_and_repeatability(oracle, handle, ozb, cuda):
+    m, n, k = 257, 129, 384
+    A = oracle.phi_matrix(m, k, 1.0, 1)
+    B = oracle.phi_matrix(k, n, 1.0, 2)
+    C0 = oracle.phi_matrix(m, n, 1.0, 3)
+    C1 = run_i8(ozb, handle, cuda, A, B, m, n, k, alpha=-0.5, beta=2.0, C0=C0)
+    C2 = run_i8(ozb, handle, cuda, A, B, m, n, k, alpha=-0.5, beta=2.0, C0=C0)
+    assert bits_equal(C1, C2)
+    Cp = run_i8(ozb, handle, cuda, A, B, m, n, k)
+    expect = np.fma(-0.5, Cp, 2.0 * C0) if hasattr(np, "fma") else -0.5 * Cp + 2.0 * C0
+    assert np.allclose(C1, expect, rtol=4 * U, atol=0)
+
+
+@pytest.mark.parametrize("nsplit", [4, 6, 8])
+def test_i8_truncated_triangular(nsplit, oracle, handle, ozb, cuda):
+    """Fewer digits / triangular pairs: the error follows the dropped digit weight 2^-7S."""
+    m, n, k = 128, 128, 256
+    A = oracle.phi_matrix(m, k, 1.0, 1)
+    B = oracle.phi_matrix(k, n, 1.0, 2)
+    C = run_i8(ozb, handle, cuda, A, B, m, n, k, nsplit=nsplit, fast=1)
+    assert handle.nSplitA == nsplit and handle.nSplitC == nsplit * (nsplit + 1) // 2
+    err = errors(oracle, A, B, C, m, n, k, range(0, m, 8), range(0, n, 8))
+    assert err < 2.0 ** (-7 * nsplit + 24), err
+
+
+def test_i8_vs_plain_error(oracle, handle, ozb, cuda):
+    """At a complete split the INT8 form is at least as accurate as the plain FP64-slice form."""
+    m, n, k = 128, 128, 1024
+    A = oracle.phi_matrix(m, k, 1.0, 1)
+    B = oracle.phi_matrix(k, n, 1.0, 2)
+    Ci8 = run_i8(ozb, handle, cuda, A, B, m, n, k)
+    handle.nSplitMax = 0
+    handle.fastMode = 0
+    dC = cuda.zeros((n, m), dtype=cuda.float64, device="cuda")
+    ozb.dgemm(handle, "n", "n", m, n, k, 1.0, dev(cuda, A), m, dev(cuda, B), k, 0.0, dC, m)
+    Cp = dC.cpu().numpy()
+    rows, cols = range(0, m, 4), range(0, n, 4)
+    e8 = errors(oracle, A, B, Ci8, m, n, k, rows, cols)
+    ep = errors(oracle, A, B, Cp, m, n, k, rows, cols)
+    assert e8 <= max(ep, U), (e8, ep)

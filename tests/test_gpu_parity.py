@@ -1,0 +1,200 @@
+"""Plain form (FP64 slices) on the GPU vs the CPU oracle: bit-exact.
+
+Every case calls the library through its C ABI (ozblas_b200 -> ctypes ->
+libcuozblas_b200.so) with device buffers, and compares all output bits with
+the C restatement of the reference CPU path (oracle/ozoracle.c), which is
+itself pinned to the reference library by tests/test_oracle.py and the
+golden files.  Inputs come from the reference harness's phi generator
+(testing/testing_common.cpp:703-717), seeds 1 (A, x) and 2 (B, y).
+"""
+import numpy as np
+import pytest
+
+from oracle.oracle import make_flags
+from tests.conftest import bits_equal, first_diff
+
+pytestmark = pytest.mark.gpu
+
+
+def dev(torch, a):
+    return torch.from_numpy(np.ascontiguousarray(a)).cuda()
+
+
+def host(t):
+    return t.cpu().numpy()
+
+
+GEMM_CASES = [
+    # m, n, k, ta, tb, sumMode, fastMode, alpha, beta, phi
+    (1, 1, 1, "n", "n", 0, 0, 1.0, 0.0, 1.0),
+    (2, 3, 7, "n", "n", 0, 0, 1.0, 0.0, 1.0),
+    (33, 17, 100, "n", "n", 0, 0, 1.0, 0.0, 1.0),
+    (33, 17, 100, "t", "n", 1, 0, 1.0, 0.0, 1.0),
+    (7, 9, 130, "n", "t", 0, 0, -0.5, 2.0, 1.0),
+    (20, 20, 64, "t", "t", 0, 2, 1.0, 1.0, 1.0),
+    (16, 12, 77, "n", "n", 1, 1, 1.0, 0.0, 1.0),
+    (65, 129, 33, "n", "n", 0, 0, 1.5, -1.0, 2.0),
+    (130, 70, 300, "n", "n", 1, 0, 1.0, 0.0, 4.0),
+    (64, 64, 1, "n", "n", 0, 0, 1.0, 0.0, 0.5),
+    (100, 3, 512, "t", "n", 0, 0, 1.0, 0.0, 1.0),
+]
+
+
+@pytest.mark.parametrize("case", GEMM_CASES, ids=lambda c: "x".join(map(str, c[:3])) + f"-{c[3]}{c[4]}-s{c[5]}f{c[6]}")
+def test_dgemm_small(case, oracle, handle, ozb, cuda):
+    m, n, k, ta, tb, sm, fm, alpha, beta, phi = case
+    ar, ac = (m, k) if ta == "n" else (k, m)
+    br, bc = (k, n) if tb == "n" else (n, k)
+    A = oracle.phi_matrix(ar, ac, phi, 1)
+    B = oracle.phi_matrix(br, bc, phi, 2)
+    C0 = oracle.phi_matrix(m, n, 1.0, 3)
+    ref, info = oracle.dgemm(make_flags(sumMode=sm, fastMode=fm), ta, tb, m, n, k, alpha, A, ar, B, br, beta, C0, m)
+    dA, dB, dC = dev(cuda, A), dev(cuda, B), dev(cuda, C0)
+    handle.sumMode, handle.fastMode = sm, fm
+    ozb.dgemm(handle, ta, tb, m, n, k, alpha, dA, ar, dB, br, beta, dC, m)
+    out = host(dC)
+    assert bits_equal(out, ref), first_diff(out, ref)
+    assert (handle.nSplitA, handle.nSplitB, handle.nSplitC) == (info.nSplitA, info.nSplitB, info.nSplitC)
+
+
+def test_dgemm_run_to_run_identical(oracle, handle, ozb, cuda):
+    m = n = k = 256
+    A = oracle.phi_matrix(m, k, 1.0, 1)
+    B = oracle.phi_matrix(k, n, 1.0, 2)
+    dA, dB = dev(cuda, A), dev(cuda, B)
+    outs = []
+    for _ in range(3):
+        dC = cuda.zeros((n, m), dtype=cuda.float64, device="cuda")
+        ozb.dgemm(handle, "n", "n", m, n, k, 1.0, dA, m, dB, k, 0.0, dC, m)
+        outs.append(host(dC))
+    assert bits_equal(outs[0], outs[1]) and bits_equal(outs[0], outs[2])
+    ref, _ = oracle.dgemm(make_flags(), "n", "n", m, n, k, 1.0, A, m, B, k, 0.0, np.zeros((n, m)), m)
+    assert bits_equal(outs[0], ref), first_diff(outs[0], ref)
+
+
+def test_dgemm_beta0_propagates_nan(oracle, handle, ozb, cuda):
+    """C = fma(alpha, t, beta*C) with beta = 0 keeps NaN from C, as the reference does."""
+    m = n = k = 8
+    A = oracle.phi_matrix(m, k, 1.0, 1)
+    B = oracle.phi_matrix(k, n, 1.0, 2)
+    C0 = np.zeros((n, m))
+    C0[2, 3] = np.nan
+    ref, _ = oracle.dgemm(make_flags(), "n", "n", m, n, k, 1.0, A, m, B, k, 0.0, C0, m)
+    dC = dev(cuda, C0)
+    ozb.dgemm(handle, "n", "n", m, n, k, 1.0, dev(cuda, A), m, dev(cuda, B), k, 0.0, dC, m)
+    out = host(dC)
+    assert np.isnan(out[2, 3]) and bits_equal(out, ref)
+
+
+@pytest.mark.parametrize("nsplit", [1, 2, 3])
+def test_dgemm_truncated_split(nsplit, oracle, handle, ozb, cuda):
+    m, n, k = 40, 30, 200
+    A = oracle.phi_matrix(m, k, 2.0, 1)
+    B = oracle.phi_matrix(k, n, 2.0, 2)
+    ref, _ = oracle.dgemm(make_flags(nSplitMax=nsplit), "n", "n", m, n, k, 1.0, A, m, B, k, 0.0, np.zeros((n, m)), m)
+    handle.nSplitMax = nsplit
+    dC = cuda.zeros((n, m), dtype=cuda.float64, device="cuda")
+    ozb.dgemm(handle, "n", "n", m, n, k, 1.0, dev(cuda, A), m, dev(cuda, B), k, 0.0, dC, m)
+    assert bits_equal(host(dC), ref), first_diff(host(dC), ref)
+
+
+@pytest.mark.parametrize("n,phi", [(1, 1.0), (7, 1.0), (1000, 2.0), (100003, 2.0), (1 << 20, 2.0)])
+@pytest.mark.parametrize("sm", [0, 1])
+def test_ddot_dnrm2(n, phi, sm, oracle, handle, ozb, cuda):
+    x = oracle.phi_vector(n, phi, 1)
+    y = oracle.phi_vector(n, phi, 2)
+    handle.sumMode = sm
+    d = ozb.ddot(handle, n, dev(cuda, x), dev(cuda, y))
+    r, info = oracle.ddot(make_flags(sumMode=sm), x, y)
+    assert np.float64(d).view(np.int64) == np.float64(r).view(np.int64), (d, r)
+    assert (handle.nSplitA, handle.nSplitB) == (info.nSplitA, info.nSplitB)
+    nr = ozb.dnrm2(handle, n, dev(cuda, x))
+    nr_ref, _ = oracle.dnrm2(make_flags(sumMode=sm), x)
+    assert np.float64(nr).view(np.int64) == np.float64(nr_ref).view(np.int64), (nr, nr_ref)
+    if sm == 1:
+        assert d == oracle.exact_dot(x, y)  # NearSum with a complete split = correctly rounded
+
+
+@pytest.mark.parametrize("m,n,trans,sm,fm", [(50, 70, "n", 0, 0), (50, 70, "t", 1, 0), (300, 257, "n", 1, 0),
+                                              (64, 1000, "n", 0, 1), (1, 33, "t", 0, 0)])
+def test_dgemv(m, n, trans, sm, fm, oracle, handle, ozb, cuda):
+    A = oracle.phi_matrix(m, n, 1.0, 1)
+    xl = n if trans == "n" else m
+    yl = m if trans == "n" else n
+    x = oracle.phi_vector(xl, 1.0, 2)
+    y0 = oracle.phi_vector(yl, 1.0, 3)
+    ref, info = oracle.dgemv(make_flags(sumMode=sm, fastMode=fm), trans, m, n, 0.75, A, m, x, 0.5, y0)
+    handle.sumMode, handle.fastMode = sm, fm
+    dy = dev(cuda, y0)
+    ozb.dgemv(handle, trans, m, n, 0.75, dev(cuda, A), m, dev(cuda, x), 0.5, dy)
+    assert bits_equal(host(dy), ref), first_diff(host(dy), ref)
+
+
+def stencil_case(oracle, nx, ny, nz, seed=1):
+    rowptr, colind = oracle.stencil7(nx, ny, nz)
+    val = oracle.phi_vector(len(colind), 1.0, seed)
+    return rowptr, colind, val
+
+
+@pytest.mark.parametrize("grid", [(4, 3, 2), (12, 10, 9), (32, 32, 32)])
+@pytest.mark.parametrize("sm", [0, 1])
+@pytest.mark.parametrize("ab", [(1.0, 0.0), (-1.0, 1.0), (0.5, 2.0)])
+def test_dcsrmv(grid, sm, ab, oracle, handle, ozb, cuda):
+    rowptr, colind, val = stencil_case(oracle, *grid)
+    n = len(rowptr) - 1
+    x = oracle.phi_vector(n, 1.0, 2)
+    y0 = oracle.phi_vector(n, 1.0, 3)
+    ref, info = oracle.dcsrmv(make_flags(sumMode=sm), n, n, ab[0], val, colind, rowptr, x, ab[1], y0)
+    handle.sumMode = sm
+    dy = dev(cuda, y0)
+    ozb.dcsrmv(handle, "n", n, n, len(val), ab[0], dev(cuda, val), dev(cuda, colind), dev(cuda, rowptr),
+               dev(cuda, x), ab[1], dy)
+    assert bits_equal(host(dy), ref), first_diff(host(dy), ref)
+    assert (handle.nSplitA, handle.nSplitB, handle.nSplitC) == (info.nSplitA, info.nSplitB, info.nSplitC)
+
+
+def test_dcsrmv_empty_rows(oracle, handle, ozb, cuda):
+    rowptr = np.array([0, 2, 2, 5, 5, 6], dtype=np.int32)
+    colind = np.array([0, 3, 1, 2, 4, 0], dtype=np.int32)
+    val = oracle.phi_vector(6, 1.0, 5)
+    x = oracle.phi_vector(5, 1.0, 6)
+    y0 = np.zeros(5)
+    ref, _ = oracle.dcsrmv(make_flags(), 5, 5, 1.0, val, colind, rowptr, x, 0.0, y0)
+    dy = dev(cuda, y0)
+    ozb.dcsrmv(handle, "n", 5, 5, 6, 1.0, dev(cuda, val), dev(cuda, colind), dev(cuda, rowptr), dev(cuda, x), 0.0, dy)
+    assert bits_equal(host(dy), ref)
+
+
+@pytest.mark.parametrize("sm", [0, 1])
+def test_split_a_and_cg(sm, oracle, handle, ozb, cuda):
+    nx = ny = nz = 12
+    rowptr, colind = oracle.stencil7(nx, ny, nz)
+    n = len(rowptr) - 1
+    val = oracle.poisson_shift(nx, ny, nz, 3, rowptr, colind)
+    b = oracle.csrmv_fma(val, colind, rowptr, oracle.normal(n, 4))
+    iters = 60
+    xr, hr, info = oracle.dcg(make_flags(sumMode=sm), val, colind, rowptr, b, np.zeros(n), iters, 0.0)
+    handle.sumMode = sm
+    handle.verbose = 1
+    dx = cuda.zeros(n, dtype=cuda.float64, device="cuda")
+    h1 = np.zeros(iters + 1)
+    h2 = np.zeros(iters + 1)
+    it = ozb.dcg(handle, "n", n, len(val), dev(cuda, val), dev(cuda, colind), dev(cuda, rowptr), dev(cuda, b), dx,
+                 iters, 0.0, h1, h2)
+    assert it == iters
+    assert bits_equal(h1, hr), first_diff(h1, hr)
+    assert bits_equal(host(dx), xr), first_diff(host(dx), xr)
+
+
+def test_invalid_arguments(handle, ozb, cuda):
+    x = cuda.zeros(8, dtype=cuda.float64, device="cuda")
+    with pytest.raises(ozb.OzblasError) as e:
+        ozb.ddot(handle, 8, x, x, incx=2)
+    assert e.value.code == 2
+    with pytest.raises(ozb.OzblasError) as e:
+        ozb.dcsrmv(handle, "t", 1, 1, 0, 1.0, x, x, x, x, 0.0, x)
+    assert e.value.code == 2
+    handle.splitEpsMode = 2
+    with pytest.raises(ozb.OzblasError) as e:
+        ozb.ddot(handle, 8, x, x)
+    assert e.value.code == 4

@@ -1,0 +1,220 @@
+"""The oracle itself, pinned (CPU only).
+
+* The C restatement (oracle/ozoracle.c) against the golden fixtures made by
+  the reference library (tests/golden/make_golden.py): bit-exact.
+* The restatement against the live reference library (oracle/_ref) on more
+  shapes and flags, when that library is present: bit-exact, split counts
+  included.
+* The exact accumulator against mpmath.
+* The library's C ABI: loads and exports every symbol include/cuozblas.h declares.
+"""
+import json
+import os
+import re
+import subprocess
+
+import numpy as np
+import pytest
+
+from oracle.oracle import make_flags
+from tests.conftest import bits_equal, first_diff
+from tests.golden.make_golden import (CSR_GRIDS, DOT_CASES, GEMM_CASES, GEMV_CASES, case_key, gemm_inputs,
+                                      sha)
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+GOLD = os.path.join(ROOT, "tests", "golden")
+
+
+@pytest.fixture(scope="module")
+def small():
+    return np.load(os.path.join(GOLD, "small.npz"))
+
+
+@pytest.mark.parametrize("case", GEMM_CASES, ids=lambda c: case_key("g", c))
+def test_gemm_golden(case, oracle, small):
+    m, n, k, ta, tb, sm, fm, alpha, beta, phi = case
+    A, B, C0, lda, ldb = gemm_inputs(oracle, case)
+    out, info = oracle.dgemm(make_flags(sumMode=sm, fastMode=fm), ta, tb, m, n, k, alpha, A, lda, B, ldb, beta, C0,
+                             m)
+    gold = small[case_key("gemm", case)]
+    assert bits_equal(out, gold), first_diff(out, gold)
+    assert list(small[case_key("gemm", case) + "_split"]) == [info.nSplitA, info.nSplitB, info.nSplitC]
+
+
+@pytest.mark.parametrize("n,phi", DOT_CASES)
+@pytest.mark.parametrize("sm", [0, 1])
+def test_dot_golden(n, phi, sm, oracle, small):
+    x, y = oracle.phi_vector(n, phi, 1), oracle.phi_vector(n, phi, 2)
+    d, _ = oracle.ddot(make_flags(sumMode=sm), x, y)
+    r, _ = oracle.dnrm2(make_flags(sumMode=sm), x)
+    assert bits_equal(np.array([d, r]), small[f"dot_{n}_{phi}_{sm}"])
+
+
+@pytest.mark.parametrize("case", GEMV_CASES)
+def test_gemv_golden(case, oracle, small):
+    m, n, tr, sm, fm = case
+    A = oracle.phi_matrix(m, n, 1.0, 1)
+    xl, yl = (n, m) if tr == "n" else (m, n)
+    x, y0 = oracle.phi_vector(xl, 1.0, 2), oracle.phi_vector(yl, 1.0, 3)
+    out, _ = oracle.dgemv(make_flags(sumMode=sm, fastMode=fm), tr, m, n, 0.75, A, m, x, 0.5, y0)
+    assert bits_equal(out, small[f"gemv_{m}_{n}_{tr}_{sm}_{fm}"])
+
+
+@pytest.mark.parametrize("g", CSR_GRIDS)
+@pytest.mark.parametrize("sm", [0, 1])
+def test_csrmv_golden(g, sm, oracle, small):
+    rowptr, colind = oracle.stencil7(*g)
+    nn = len(rowptr) - 1
+    val = oracle.phi_vector(len(colind), 1.0, 1)
+    x, y0 = oracle.phi_vector(nn, 1.0, 2), oracle.phi_vector(nn, 1.0, 3)
+    for al, be in [(1.0, 0.0), (-1.0, 1.0), (0.5, 2.0)]:
+        out, _ = oracle.dcsrmv(make_flags(sumMode=sm), nn, nn, al, val, colind, rowptr, x, be, y0)
+        gold = small[f"csrmv_{g[0]}x{g[1]}x{g[2]}_{sm}_{al}_{be}"]
+        assert bits_equal(out, gold), first_diff(out, gold)
+
+
+@pytest.mark.parametrize("sm", [0, 1])
+def test_cg_golden(sm, oracle, small):
+    nx = 12
+    rowptr, colind = oracle.stencil7(nx, nx, nx)
+    nn = len(rowptr) - 1
+    val = oracle.poisson_shift(nx, nx, nx, 3, rowptr, colind)
+    b = oracle.csrmv_fma(val, colind, rowptr, oracle.normal(nn, 4))
+    x, h, _ = oracle.dcg(make_flags(sumMode=sm), val, colind, rowptr, b, np.zeros(nn), 60, 0.0)
+    assert bits_equal(h, small[f"cg12_{sm}_hist"]) and bits_equal(x, small[f"cg12_{sm}_x"])
+
+
+@pytest.mark.slow
+def test_gemm1024_golden_hash(oracle):
+    """BASELINE config 1 (1024^3, phi=1): the restatement reproduces the reference's output hash."""
+    with open(os.path.join(GOLD, "full.json")) as f:
+        full = json.load(f)
+    A, B = oracle.phi_matrix(1024, 1024, 1.0, 1), oracle.phi_matrix(1024, 1024, 1.0, 2)
+    # the restatement's naive triple loop is slow at 1024^3; check one 64-row block of the hash's sample
+    m = 64
+    Ab = np.ascontiguousarray(A[:, :m])  # first 64 rows of A (column-major slice)
+    out, info = oracle.dgemm(make_flags(), "n", "n", m, 1024, 1024, 1.0, Ab, m, B, 1024, 0.0,
+                             np.zeros((1024, m)), m)
+    assert float(out[0, 0]).hex() == full["gemm1024_0"]["sample"][0]
+    assert float(out[700, 5]).hex() == full["gemm1024_0"]["sample"][2]
+
+
+def test_dot_full_golden(oracle):
+    with open(os.path.join(GOLD, "full.json")) as f:
+        full = json.load(f)
+    n = 1 << 24
+    x, y = oracle.phi_vector(n, 2.0, 1), oracle.phi_vector(n, 2.0, 2)
+    for sm in (0, 1):
+        d, info = oracle.ddot(make_flags(sumMode=sm), x, y)
+        assert float(d).hex() == full[f"dot2p24_{sm}"]["dot"]
+        assert [info.nSplitA, info.nSplitB] == full[f"dot2p24_{sm}"]["nSplit"]
+
+
+# ---- live reference (only where oracle/_ref exists) ----
+
+@pytest.mark.parametrize("seed", range(6))
+def test_restatement_vs_reference_random_shapes(seed, oracle, reference):
+    rng = np.random.default_rng(100 + seed)
+    m, n, k = (int(v) for v in rng.integers(1, 90, 3))
+    k = int(rng.integers(1, 700))
+    ta, tb = rng.choice(["n", "t"]), rng.choice(["n", "t"])
+    sm, fm = int(rng.integers(0, 2)), int(rng.integers(0, 3))
+    nsplit = int(rng.choice([0, 0, 2, 5]))
+    phi = float(rng.choice([0.5, 1.0, 2.0, 4.0]))
+    case = (m, n, k, ta, tb, sm, fm, 1.25, -0.5, phi)
+    A, B, C0, lda, ldb = gemm_inputs(oracle, case)
+    out, info = oracle.dgemm(make_flags(sumMode=sm, fastMode=fm, nSplitMax=nsplit), ta, tb, m, n, k, 1.25, A, lda,
+                             B, ldb, -0.5, C0, m)
+    reference.set_flags(sumMode=sm, fastMode=fm, nSplitMax=nsplit)
+    gold = reference.dgemm(ta, tb, m, n, k, 1.25, A, lda, B, ldb, -0.5, C0, m)
+    assert bits_equal(out, gold), (case, nsplit, first_diff(out, gold))
+    inf = reference.info()
+    assert [info.nSplitA, info.nSplitB, info.nSplitC] == [inf["nSplitA"], inf["nSplitB"], inf["nSplitC"]]
+
+
+def test_split_slices_vs_reference(oracle, reference):
+    """Slice-level parity of the column-panel and CSR splits."""
+    for phi, k, ncol in [(1.0, 100, 7), (4.0, 333, 5), (2.0, 1, 3), (1.0, 64, 1)]:
+        X = oracle.phi_matrix(k, ncol, phi, 9)
+        reference.set_flags()
+        s_ref, sl_ref = reference.split_panel(X)
+        s, sl = oracle.split_cols(make_flags(), X)
+        assert s == s_ref and bits_equal(sl, sl_ref)
+    rowptr, colind = oracle.stencil7(6, 5, 4)
+    val = oracle.phi_vector(len(colind), 1.0, 3)
+    s_ref, sl_ref = reference.split_sparse(val, rowptr)
+    s, sl = oracle.split_csr(make_flags(), val, rowptr)
+    assert s == s_ref and bits_equal(sl, sl_ref)
+
+
+def test_zero_and_tiny_inputs_vs_reference(oracle, reference):
+    m, n, k = 9, 7, 40
+    A = oracle.phi_matrix(m, k, 1.0, 1)
+    A[3, :] = 0.0  # a zero column of A
+    A[:, 2] = 0.0  # a zero row
+    B = oracle.phi_matrix(k, n, 1.0, 2) * 1e-300
+    for sm in (0, 1):
+        out, _ = oracle.dgemm(make_flags(sumMode=sm), "n", "n", m, n, k, 1.0, A, m, B, k, 0.0, np.zeros((n, m)), m)
+        reference.set_flags(sumMode=sm)
+        gold = reference.dgemm("n", "n", m, n, k, 1.0, A, m, B, k, 0.0, np.zeros((n, m)), m)
+        assert bits_equal(out, gold), first_diff(out, gold)
+
+
+def test_tau_libm_matches_reference(oracle, reference):
+    for v in [1.0, 1.5, 2.0 ** 100 * (1 + 2.0 ** -52), 3.0e-310, 7.0, 2.0 ** -1000]:
+        assert oracle.tau_libm(v) == reference.tau(v)
+
+
+# ---- exact accumulator ----
+
+def test_exact_dot_vs_mpmath(oracle):
+    mpmath = pytest.importorskip("mpmath")
+    mpmath.mp.prec = 4000
+    rng = np.random.default_rng(3)
+    for trial in range(20):
+        n = int(rng.integers(1, 200))
+        x = (rng.random(n) - 0.5) * np.exp(rng.normal(0, 30, n))
+        y = (rng.random(n) - 0.5) * np.exp(rng.normal(0, 30, n))
+        if trial == 0:
+            x[0], y[0] = 1e300, 1e300
+            x[1], y[1] = 5e-324, 3.0
+        exact = mpmath.fsum(mpmath.mpf(float(a)) * mpmath.mpf(float(b)) for a, b in zip(x, y))
+        rn = oracle.exact_dot(x, y)
+        assert rn == float(exact) or (np.isinf(rn) and abs(exact) > 1.79e308), (trial, rn, exact)
+        if abs(exact) > 1e308:
+            continue
+        c = float(exact) * (1 + 2.0 ** -50)
+        _, rel = oracle.exact_dot_err(x, y, c)
+        if exact != 0:
+            ref_rel = abs((mpmath.mpf(c) - exact) / exact)
+            assert abs(rel - float(ref_rel)) <= 1e-12 * float(ref_rel)
+
+
+# ---- C ABI ----
+
+def test_c_abi_exports_every_declared_symbol():
+    lib = os.path.join(ROOT, "ozblas_b200", "libcuozblas_b200.so")
+    assert os.path.exists(lib), "libcuozblas_b200.so is not built"
+    hdr = open(os.path.join(ROOT, "include", "cuozblas.h")).read()
+    c_part = hdr.split('extern "C" {', 1)[1]
+    declared = set(re.findall(r"^\s*(?:int|const char \*)\s*(cuozblas\w+)\s*\(", c_part, re.M))
+    assert len(declared) >= 15
+    syms = subprocess.run(["nm", "-D", "--defined-only", lib], capture_output=True, text=True).stdout
+    exported = set(re.findall(r" T (\w+)$", syms, re.M))
+    assert declared <= exported, declared - exported
+    # the reference's C++ instantiations (include/cuozblas.h:66-80) for drop-in linking
+    for mangled in ["_Z14cuozblasCreateP16cuozblasHandle_tm", "_Z15cuozblasDestroyP16cuozblasHandle_t",
+                    "_Z13cuozblasRgemmIdddEiP16cuozblasHandle_tccPKiiiT_PKS3_iS5_iS3_PS3_i"[:0] or "cuozblasRgemmIdddE",
+                    "cuozblasRdotIdddE", "cuozblasRnrm2IdddE", "cuozblasRgemvIdddE", "cuozblasRaxpyIdE",
+                    "cuozblasRcsrmvIddE", "cuozblasRcsrmvSplitAIddE", "cuozblasRcgIddE", "cuozblasRgemmIdaiE"]:
+        assert any(mangled in s for s in exported), mangled
+
+
+def test_python_binding_lists_c_abi():
+    import importlib
+    # the package refuses to load without its library; the list must match the header
+    ozb = importlib.import_module("ozblas_b200")
+    hdr = open(os.path.join(ROOT, "include", "cuozblas.h")).read()
+    c_part = hdr.split('extern "C" {', 1)[1]
+    declared = set(re.findall(r"^\s*(?:int|const char \*)\s*(cuozblas\w+)\s*\(", c_part, re.M))
+    assert declared == set(ozb.C_ABI_SYMBOLS)
