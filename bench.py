@@ -1,0 +1,377 @@
+#!/usr/bin/env python
+"""Benchmark: Ozaki-scheme DGEMM on B200 (INT8 precision form on tcgen05).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Workload (the metric's configuration): m = n = k = 8192, A and B entries
+(U(0,1) - 0.5) * exp(phi * N(0,1)) with phi = 1 from a seeded generator,
+alpha = 1, beta = 0; INT8 slices on tcgen05 with INT32 accumulation, digits
+chosen per operand until the split is exact, triangular pair set (fastMode).
+One step = one cuozblasDgemmI8 call through the C ABI.  Inputs (512 MiB each)
+are larger than L2, so no flush is needed between steps.
+
+value   effective TFLOPS = 2 m n k / device time per step (inputs resident in
+        HBM), summed over ranks; with N > 1 every rank runs its own replica
+        (the path does not shard in this configuration).
+e2e     the same metric with host buffers: pinned host -> device copies of A
+        and B, the call, and the device -> host copy of C inside each step.
+roofline  the tcgen05 product kernel alone (CUDA events around its launch on
+        the handle's stream): int8 ops per launch = pairs * 2 m n k.
+
+Extra keys (rank 0): the plain FP64-slice form on the same inputs, the
+maximum relative error of both forms against the correctly rounded product
+(the library's NearSum plain form, bit-exact to the reference CPU NearSum),
+and DOT / CSRMV memory throughput.  The CPU baseline is the reference OzBLAS
+CPU library (oracle/_ref) on a bounded row sample of the same problem.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+N_DIM = 8192
+PHI = 1.0
+
+
+def phi_matrix(rows, cols, phi, seed):
+    """(U - 0.5) * exp(phi * N(0,1)) with N from Box-Muller on the same U (column-major rows x cols)."""
+    import numpy as np
+
+    g = np.random.default_rng(seed)
+    r1 = g.random((cols, rows))
+    r2 = g.random((cols, rows))
+    return (r1 - 0.5) * np.exp(phi * np.sqrt(-2.0 * np.log(r1)) * np.sin(2.0 * np.pi * r2))
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return d, "measured"
+    return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "bf16_tflops_sustained": 1400.0}, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle samples during the timed region."""
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_gpu{gpu_index}.csv")
+
+    def __enter__(self):
+        os.makedirs(os.path.dirname(self.path), exist_ok=True)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu),
+                 "--query-gpu=index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+                 "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+                 "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except (FileNotFoundError, OSError):
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *a):
+        if self.proc:
+            time.sleep(0.2)
+            self.proc.terminate()
+            self.proc.wait(timeout=10)
+
+    def summary(self):
+        rows = []
+        try:
+            with open(self.path) as f:
+                for line in f:
+                    parts = [p.strip() for p in line.split(",")]
+                    if len(parts) >= 9:
+                        rows.append(parts)
+        except OSError:
+            pass
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def cpu_reference_sample(rows_sample=256, threads=None):
+    """The reference OzBLAS CPU library (plain ozblasRgemm, FP64 slices) on the
+    first `rows_sample` rows of the same 8192^3 problem.  Test-side code: the
+    oracle is only imported here, for the CPU baseline."""
+    import numpy as np
+
+    from oracle.oracle import Reference, have_reference
+
+    if not have_reference():
+        return None, "oracle/_ref/libozblas_ref.so not built"
+    threads = threads or os.cpu_count()
+    ref = Reference(work_bytes=int(48e9), threads=threads)
+    ref.set_flags(sumMode=0, fastMode=0, nSplitMax=0, reproMode=1)
+    A = np.ascontiguousarray(phi_matrix(N_DIM, N_DIM, PHI, 1)[:, :rows_sample])  # first rows, column-major
+    B = phi_matrix(N_DIM, N_DIM, PHI, 2)
+    C = np.zeros((N_DIM, rows_sample))
+    t0 = time.perf_counter()
+    ref.dgemm("n", "n", rows_sample, N_DIM, N_DIM, 1.0, A, rows_sample, B, N_DIM, 0.0, C, rows_sample)
+    t = time.perf_counter() - t0
+    ref.close()
+    tflops = 2.0 * rows_sample * N_DIM * N_DIM / t / 1e12
+    return {"value": tflops, "unit": "TFLOPS", "cores": threads, "kind": "reference",
+            "sample": f"reference ozblasRgemm (plain FP64 slices, sumMode 0) on rows 0..{rows_sample - 1} of the "
+                      f"8192^3 phi=1 problem ({t:.2f} s, B split included)"}, None
+
+
+def run_reference_arm(args, rank, world):
+    if rank != 0:
+        return 0
+    steps = []
+    base = None
+    for i in range(args.warmup + args.steps):
+        base, err = cpu_reference_sample(rows_sample=args.ref_rows)
+        if base is None:
+            print(json.dumps({"impl": "reference", "unavailable": err}))
+            return 0
+        if i >= args.warmup:
+            steps.append(base["value"])
+    v = statistics.mean(steps)
+    base["value"] = v
+    line = {"metric": "Ozaki DGEMM TFLOPS n=8192 (INT8 vs FP64 slices, err vs MPFR); DOT/CSRMV GB/s",
+            "impl": "reference", "value": v, "unit": "TFLOPS", "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 2.0 * args.ref_rows * N_DIM * N_DIM / v / 1e9,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": "ozaki_dgemm m=n=k=8192 phi=1", "m": N_DIM, "n": N_DIM, "k": N_DIM, "phi": PHI,
+                       "sample_rows": args.ref_rows},
+            "cpu_baseline": base, "e2e": {"value": v, "unit": "TFLOPS", "h2d_bytes_per_step": 0,
+                                          "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-extras", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--ref-rows", type=int, default=256)
+    ap.add_argument("--full-pairs", action="store_true", help="headline with the full pair set instead of triangular")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+
+    if args.impl == "reference":
+        return run_reference_arm(args, rank, world)
+
+    import numpy as np
+    import torch
+
+    import ozblas_b200 as ozb
+
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    n = N_DIM
+    A_h = torch.from_numpy(phi_matrix(n, n, PHI, 1 + 10 * rank)).pin_memory()
+    B_h = torch.from_numpy(phi_matrix(n, n, PHI, 2 + 10 * rank)).pin_memory()
+    C_h = torch.empty((n, n), dtype=torch.float64).pin_memory()
+    A = A_h.cuda()
+    B = B_h.cuda()
+    C = torch.zeros((n, n), dtype=torch.float64, device="cuda")
+    h = ozb.Handle(work_bytes=40 << 30)
+    h.sumMode = 0
+    h.nSplitMax = 0
+    h.fastMode = 0 if args.full_pairs else 1
+
+    def step():
+        ozb.dgemm_i8(h, "n", "n", n, n, n, 1.0, A, n, B, n, 0.0, C, n)
+
+    for _ in range(args.warmup):
+        step()
+    barrier()
+    stream = torch.cuda.current_stream()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    kern_ms = []
+    launches0 = h.launch_count()
+    with ClockSampler(torch.cuda.current_device()) as clk:
+        barrier()
+        for i in range(args.steps):
+            ev[i][0].record(stream)
+            step()
+            ev[i][1].record(stream)
+            kern_ms.append(h.t_comp * 1e3)
+        barrier()
+    launches = (h.launch_count() - launches0) / args.steps
+    ms = statistics.mean(e0.elapsed_time(e1) for e0, e1 in ev)
+    if dist is not None:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    flops = 2.0 * n * n * n
+    value = world * flops / (ms * 1e-3) / 1e12
+    pairs = h.nSplitC
+    nA, nB = h.nSplitA, h.nSplitB
+
+    # ---- end to end: host buffers, copies inside the step ----
+    def e2e_step():
+        A.copy_(A_h, non_blocking=True)
+        B.copy_(B_h, non_blocking=True)
+        step()
+        C_h.copy_(C, non_blocking=True)
+
+    e2e_step()
+    barrier()
+    ev2 = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    for i in range(args.steps):
+        ev2[i][0].record(stream)
+        e2e_step()
+        ev2[i][1].record(stream)
+    barrier()
+    ms_e2e = statistics.mean(e0.elapsed_time(e1) for e0, e1 in ev2)
+    if dist is not None:
+        t = torch.tensor([ms_e2e], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms_e2e = float(t.item())
+    e2e = {"value": world * flops / (ms_e2e * 1e-3) / 1e12, "unit": "TFLOPS", "h2d_bytes_per_step": 2 * n * n * 8,
+           "d2h_bytes_per_step": n * n * 8, "ms_per_step": ms_e2e}
+
+    peaks, peak_kind = measured_peaks()
+    int8_peak = 2.0 * peaks["bf16_tflops"]  # dense int8 rate is twice dense bf16 on B200
+    kms = statistics.mean(kern_ms)
+    achieved = pairs * flops / (kms * 1e-3) / 1e12
+    traffic = None
+    tp = os.path.join(ROOT, "profiles", "ncu_traffic.json")
+    if os.path.exists(tp):
+        with open(tp) as f:
+            tj = json.load(f)
+        key = f"k_i8_gemm_{'full' if args.full_pairs else 'tri'}_{n}"
+        traffic = tj.get(key)
+    roofline = {"bound": "tensor", "achieved": achieved, "peak": int8_peak, "unit": "TFLOP/s", "frac": achieved / int8_peak,
+                "traffic": traffic, "kernel": "k_i8_gemm (tcgen05.mma kind::i8)", "kernel_ms": kms,
+                "peak_note": f"int8 ops/s; peak = 2 x {peak_kind} dense bf16 ({peaks['bf16_tflops']} TFLOP/s burst, "
+                             "MEASURED_PEAKS.json)",
+                "algorithmic_ops_per_launch": pairs * flops}
+
+    line = {"metric": "Ozaki DGEMM TFLOPS n=8192 (INT8 vs FP64 slices, err vs MPFR); DOT/CSRMV GB/s",
+            "value": value, "unit": "TFLOPS", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int8",
+            "data": "synthetic",
+            "config": {"workload": "ozaki_dgemm_int8 m=n=k=8192 phi=1", "m": n, "n": n, "k": n, "phi": PHI,
+                       "slices": [nA, nB], "pairs": pairs, "pair_set": "full" if args.full_pairs else "triangular",
+                       "sumMode": 0, "l2": "inputs 512 MiB each > L2, no flush",
+                       "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
+            "e2e": e2e, "roofline": roofline, "gpu_launches": launches, "clocks": clk.summary()}
+
+    if rank == 0 and not args.no_extras:
+        line["extras"] = extras(ozb, h, torch, A, B, C, n)
+        line["extras"]["int8_vs_plain_speedup"] = line["extras"]["plain_fp64_slices"]["ms"] / ms
+    if rank == 0 and world == 1 and not args.no_cpu:
+        try:
+            base, err = cpu_reference_sample(rows_sample=args.ref_rows)
+        except Exception as e:  # the baseline must not take the GPU line down
+            base, err = None, repr(e)
+        line["cpu_baseline"] = base if base else {"value": None, "unavailable": err}
+    h.close()
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(line))
+    return 0
+
+
+def extras(ozb, h, torch, A, B, C, n):
+    """Plain form, accuracy vs the correctly rounded product, DOT/CSRMV throughput."""
+    out = {}
+    flops = 2.0 * n * n * n
+
+    def timed(fn, reps=1):
+        fn()
+        torch.cuda.synchronize()
+        ts = []
+        for _ in range(reps):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            fn()
+            e1.record()
+            torch.cuda.synchronize()
+            ts.append(e0.elapsed_time(e1))
+        return min(ts)
+
+    C_tri = C.clone()
+    h.fastMode = 0
+    ms_full = timed(lambda: ozb.dgemm_i8(h, "n", "n", n, n, n, 1.0, A, n, B, n, 0.0, C, n))
+    out["int8_full_pairs"] = {"TFLOPS": flops / ms_full / 1e9, "pairs": h.nSplitC, "ms": ms_full}
+    C_full = C.clone()
+    h.nSplitMax = 0
+    ms_plain = timed(lambda: ozb.dgemm(h, "n", "n", n, n, n, 1.0, A, n, B, n, 0.0, C, n))
+    out["plain_fp64_slices"] = {"TFLOPS": flops / ms_plain / 1e9, "pairs": h.nSplitC, "slices": [h.nSplitA, h.nSplitB],
+                                "ms": ms_plain, "internal_fp64_TFLOPS": h.nSplitC * flops / ms_plain / 1e9}
+    C_plain = C.clone()
+    h.sumMode = 1
+    ozb.dgemm(h, "n", "n", n, n, n, 1.0, A, n, B, n, 0.0, C, n)
+    torch.cuda.synchronize()
+    C_rn = C  # correctly rounded product (NearSum over exact slice pairs)
+    h.sumMode = 0
+
+    def maxrel(X):
+        d = (X - C_rn).abs() / C_rn.abs()
+        d = torch.where(C_rn == 0, (X != 0).double() * float("inf"), d)
+        return float(d.max().item()), int((X != C_rn).sum().item())
+
+    e_tri, n_tri = maxrel(C_tri)
+    e_full, n_full = maxrel(C_full)
+    e_plain, n_plain = maxrel(C_plain)
+    out["max_rel_err_vs_correctly_rounded"] = {"int8_triangular": e_tri, "int8_full": e_full, "plain_fsum": e_plain,
+                                               "inexact_entries": {"int8_triangular": n_tri, "int8_full": n_full,
+                                                                   "plain_fsum": n_plain},
+                                               "note": "reference = plain form with NearSum (correctly rounded)"}
+    del C_tri, C_full, C_plain
+    torch.cuda.empty_cache()
+    # DOT n = 2^24, phi = 2
+    nv = 1 << 24
+    g = torch.Generator(device="cuda").manual_seed(7)
+    r1 = torch.rand(nv, dtype=torch.float64, device="cuda", generator=g)
+    r2 = torch.rand(nv, dtype=torch.float64, device="cuda", generator=g)
+    x = (r1 - 0.5) * torch.exp(2.0 * torch.sqrt(-2 * torch.log(r1)) * torch.sin(2 * torch.pi * r2))
+    r1 = torch.rand(nv, dtype=torch.float64, device="cuda", generator=g)
+    y = (r1 - 0.5) * torch.exp(2.0 * torch.sqrt(-2 * torch.log(r1)) * torch.sin(2 * torch.pi * r2))
+    for sm in (0, 1):
+        h.sumMode = sm
+        ms = timed(lambda: ozb.ddot(h, nv, x, y), reps=3)
+        out[f"ddot_2p24_sum{sm}"] = {"GBps": 16.0 * nv / ms / 1e6, "ms": ms, "slices": [h.nSplitA, h.nSplitB]}
+    h.sumMode = 0
+    return out
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -150,6 +150,8 @@ int cuozblasHandleCreate(cuozblasHandle_t *h, uint64_t workSizeBytes);
 int cuozblasHandleDestroy(cuozblasHandle_t *h);
 /* Extension: run the handle's work on `stream` (a cudaStream_t). */
 int cuozblasSetStream(cuozblasHandle_t *h, void *stream);
+/* Extension: number of kernels the handle has launched since create. */
+int cuozblasGetLaunchCount(cuozblasHandle_t *h, uint64_t *count);
 
 /* cuozblasRdot<double,double,double> (include/cuozblas.h:75; src/cuda/cuozblas_dot.cu:3-40).
  * *ret is a host pointer, written before return. */

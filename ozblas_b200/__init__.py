@@ -80,6 +80,7 @@ def _sig(name, args, res=C.c_int):
 _create = _sig("cuozblasHandleCreate", [_HP, C.c_uint64])
 _destroy = _sig("cuozblasHandleDestroy", [_HP])
 _setstream = _sig("cuozblasSetStream", [_HP, _vp])
+_launches = _sig("cuozblasGetLaunchCount", [_HP, C.POINTER(C.c_uint64)])
 _ddot = _sig("cuozblasDdot", [_HP, _i32, _vp, _i32, _vp, _i32, C.POINTER(_d)])
 _dnrm2 = _sig("cuozblasDnrm2", [_HP, _i32, _vp, _i32, C.POINTER(_d)])
 _daxpy = _sig("cuozblasDaxpy", [_HP, _i32, _d, _vp, _i32, _vp, _i32])
@@ -95,7 +96,7 @@ _version = _sig("cuozblasVersion", [], C.c_char_p)
 
 #: every C-ABI symbol include/cuozblas.h declares (checked by the CPU tests)
 C_ABI_SYMBOLS = [
-    "cuozblasHandleCreate", "cuozblasHandleDestroy", "cuozblasSetStream", "cuozblasDdot", "cuozblasDnrm2",
+    "cuozblasHandleCreate", "cuozblasHandleDestroy", "cuozblasSetStream", "cuozblasGetLaunchCount", "cuozblasDdot", "cuozblasDnrm2",
     "cuozblasDaxpy", "cuozblasDgemv", "cuozblasDgemm", "cuozblasDcsrmv", "cuozblasDcsrmvSplitA", "cuozblasDcg",
     "cuozblasDgemmI8", "cuozblasRuleTau", "cuozblasRuleRho", "cuozblasVersion",
 ]
@@ -134,6 +135,12 @@ class Handle:
     def set_stream(self, stream):
         s = stream if isinstance(stream, int) else getattr(stream, "cuda_stream", stream)
         _chk("cuozblasSetStream", _setstream(C.byref(self._h), s))
+
+    def launch_count(self) -> int:
+        """Kernels this handle has launched since it was created."""
+        c = C.c_uint64()
+        _chk("cuozblasGetLaunchCount", _launches(C.byref(self._h), C.byref(c)))
+        return c.value
 
     @property
     def ref(self):

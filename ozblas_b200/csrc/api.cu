@@ -133,6 +133,12 @@ int cuozblasHandleDestroy(cuozblasHandle_t *h) {
     return CUOZBLAS_STATUS_SUCCESS;
 }
 
+int cuozblasGetLaunchCount(cuozblasHandle_t *h, uint64_t *count) {
+    if (!h || !h->initialized || !count) return CUOZBLAS_STATUS_NOT_INITIALIZED;
+    *count = state(h)->launches;
+    return CUOZBLAS_STATUS_SUCCESS;
+}
+
 int cuozblasSetStream(cuozblasHandle_t *h, void *stream) {
     if (!h || !h->initialized) return CUOZBLAS_STATUS_NOT_INITIALIZED;
     state(h)->stream = reinterpret_cast<cudaStream_t>(stream);

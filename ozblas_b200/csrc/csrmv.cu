@@ -66,6 +66,7 @@ int launch_axpy(cuozblasHandle_t *h, int n, double alpha, const double *x, doubl
     if (n <= 0) return CUOZBLAS_STATUS_SUCCESS;
     int blocks = (n + 255) / 256;
     if (blocks > 148 * 16) blocks = 148 * 16;
+    counted(h);
     k_axpy<<<blocks, 256, 0, state(h)->stream>>>(n, alpha, x, y);
     OZB_CHECK(cudaGetLastError());
     return CUOZBLAS_STATUS_SUCCESS;
@@ -75,6 +76,7 @@ int launch_scal(cuozblasHandle_t *h, int n, double alpha, double *x) {
     if (n <= 0) return CUOZBLAS_STATUS_SUCCESS;
     int blocks = (n + 255) / 256;
     if (blocks > 148 * 16) blocks = 148 * 16;
+    counted(h);
     k_scal<<<blocks, 256, 0, state(h)->stream>>>(n, alpha, x);
     OZB_CHECK(cudaGetLastError());
     return CUOZBLAS_STATUS_SUCCESS;
@@ -83,6 +85,7 @@ int launch_scal(cuozblasHandle_t *h, int n, double alpha, double *x) {
 int launch_csrmv_plain(cuozblasHandle_t *h, int m, const double *val, const int *colind, const int *rowptr,
                        const double *x, double alpha, double beta, double *y) {
     if (m <= 0) return CUOZBLAS_STATUS_SUCCESS;
+    counted(h);
     k_csrmv_plain<<<(m + 255) / 256, 256, 0, state(h)->stream>>>(m, val, colind, rowptr, x, alpha, beta, y);
     OZB_CHECK(cudaGetLastError());
     return CUOZBLAS_STATUS_SUCCESS;
@@ -109,9 +112,11 @@ int csrmv_presplit(cuozblasHandle_t *h, int m, int n, double alpha, const double
         pbuf = ar.take<double>((uint64_t)np * (m > 0 ? m : 1));
         if (!ar.ok) return CUOZBLAS_STATUS_WORKSPACE;
     }
-    if (m > 0)
+    if (m > 0) {
+        counted(h);
         k_csrmv_pairs<<<(m + 255) / 256, 256, 0, st->stream>>>(m, As, ld_s, colind, rowptr, xs, ldx, nA, nB, maxlevel,
                                                               h->sumMode, alpha, beta, y, pbuf);
+    }
     OZB_CHECK(cudaGetLastError());
     int ic = 0;
     for (int ia = 0; ia < (maxlevel + 1 < nA ? maxlevel + 1 : nA); ia++) ic += (nB < maxlevel + 1 - ia ? nB : maxlevel + 1 - ia);

@@ -13,10 +13,11 @@
 // of one level share the scale, so they accumulate in one INT32 tensor-memory
 // accumulator; a group holds at most floor((2^31 - 1) / (127^2)) products per
 // output, which keeps every partial sum exact (k is chunked beyond that).
-// Sum: levels are visited from the smallest (highest L) to the largest.  A
-// run of consecutive levels is first combined exactly, as an integer below
-// 2^53 held in an FP64 register (V_L shifted by 7 bits per level); each run
-// is then added once to the FP64 sum R, which lives in tensor memory.  With a
+// Sum: levels are visited from the smallest (highest L) to the largest.  Runs
+// of consecutive levels, formed from level 0 upward, are first combined
+// exactly, as an integer below 2^53 held in an FP64 register (V_L shifted by
+// 7 bits per level); each run is then added once to the FP64 sum R, which
+// lives in tensor memory.  With a
 // complete split this makes the output correctly rounded except when the
 // exact value sits within ~2^-28 ulp of a rounding boundary.  Finally
 // t = R * 2^(EA_i + EB_j) and C = fma(alpha, t, beta * C).
@@ -426,7 +427,10 @@ static int split_digits(cuozblasHandle_t *h, bool strided, int nl, int k, const 
     op.e = ar.take<int>(nl > 0 ? nl : 1);
     if (!ar.ok) return CUOZBLAS_STATUS_WORKSPACE;
     OZB_CHECK(cudaMemsetAsync(st->d_ints, 0, sizeof(int), st->stream));
-    if (nl > 0) k_digit_count<<<nl, 256, 0, st->stream>>>(k, nl, src, lds, op.e, st->d_ints);
+    if (nl > 0) {
+        counted(h);
+        k_digit_count<<<nl, 256, 0, st->stream>>>(k, nl, src, lds, op.e, st->d_ints);
+    }
     OZB_CHECK(cudaGetLastError());
     OZB_CHECK(cudaMemcpyAsync(st->h_ints, st->d_ints, sizeof(int), cudaMemcpyDeviceToHost, st->stream));
     OZB_CHECK(cudaStreamSynchronize(st->stream));
@@ -436,6 +440,7 @@ static int split_digits(cuozblasHandle_t *h, bool strided, int nl, int k, const 
     op.digits = ar.take<int8_t>((uint64_t)op.S * op.lines_pad * k_pad);
     if (!ar.ok) return CUOZBLAS_STATUS_WORKSPACE;
     const int64_t chunks = (int64_t)op.lines_pad * (k_pad / 16);
+    counted(h);
     k_digit_write<<<(unsigned)((chunks + 255) / 256), 256, 0, st->stream>>>(k, nl, op.lines_pad, k_pad, op.S, src,
                                                                              lds, op.e, op.digits);
     OZB_CHECK(cudaGetLastError());
@@ -492,33 +497,43 @@ int gemm_i8_core(cuozblasHandle_t *h, char ta, char tb, int m, int n, int k, dou
             gbound.push_back(used * I8_BK * 127 * 127);
         }
     }
-    // Runs of consecutive levels whose exact combination stays below 2^53:
-    // level L of a run starting at L_hi is shifted by 7 (L_hi - L) bits; the
-    // run's last group flushes acc * 2^(-7 (L_hi + 2)) into R.
+    // Runs of consecutive levels whose exact combination stays below 2^53,
+    // formed from the most significant level up (levels 0..3, 4..7, ...):
+    // extending a run [L_lo, L_hi] by L_hi + 1 multiplies its bound by 2^7 and
+    // adds the new level's bound.  Groups are visited in descending level
+    // order; level L of run [L_lo, L_hi] is shifted by 7 (L_hi - L) bits and
+    // the run's last visited group (level L_lo) flushes acc * 2^(-7 (L_hi + 2)).
     {
+        std::vector<unsigned __int128> lbound(maxlevel + 1, 0);
+        for (size_t g = 0; g < groups.size(); g++) lbound[groups[g].z] += (unsigned __int128)gbound[g];
         const unsigned __int128 lim = (unsigned __int128)1 << 53;
-        size_t i = 0;
-        bool first = true;
-        while (i < groups.size()) {
-            const int Lhi = groups[i].z;
-            unsigned __int128 sum = 0;
-            size_t j = i;
-            while (j < groups.size()) {
-                const int L = groups[j].z, d = Lhi - L;
-                size_t je = j;
-                unsigned __int128 lb = 0;
-                while (je < groups.size() && groups[je].z == L) lb += (unsigned __int128)gbound[je++];
-                lb <<= 7 * d;
-                if (j > i && sum + lb >= lim) break;
-                sum += lb;
-                for (size_t t = j; t < je; t++) groups[t].w = 7 * d;
-                j = je;
+        std::vector<int> run_hi(maxlevel + 1), run_lo(maxlevel + 1);
+        for (int L0 = 0; L0 <= maxlevel;) {
+            unsigned __int128 b = lbound[L0];
+            int L1 = L0;
+            while (L1 + 1 <= maxlevel && (b << 7) + lbound[L1 + 1] < lim) {
+                b = (b << 7) + lbound[L1 + 1];
+                L1++;
             }
-            groups[j - 1].w |= (1 << 8) | (first ? (1 << 9) : 0);
-            groups[j - 1].z = -7 * (Lhi + 2);
-            for (size_t t = i; t + 1 < j; t++) groups[t].z = 0;
-            first = false;
-            i = j;
+            for (int L = L0; L <= L1; L++) {
+                run_lo[L] = L0;
+                run_hi[L] = L1;
+            }
+            L0 = L1 + 1;
+        }
+        bool first = true;
+        for (size_t g = 0; g < groups.size(); g++) {
+            const int L = groups[g].z;
+            int meta = 7 * (run_hi[L] - L);
+            const bool last_of_level = (g + 1 == groups.size()) || groups[g + 1].z != L;
+            if (last_of_level && L == run_lo[L]) {
+                meta |= (1 << 8) | (first ? (1 << 9) : 0);
+                first = false;
+                groups[g].z = -7 * (run_hi[L] + 2);
+            } else {
+                groups[g].z = 0;
+            }
+            groups[g].w = meta;
         }
         groups.back().w |= (1 << 10);
     }
@@ -564,6 +579,7 @@ int gemm_i8_core(cuozblasHandle_t *h, char ta, char tb, int m, int n, int k, dou
     const int grid = ntiles < nsm ? ntiles : nsm;
     OZB_CHECK(cudaFuncSetAttribute(k_i8_gemm, cudaFuncAttributeMaxDynamicSharedMemorySize, I8_SMEM));
     ev_record(h, 2);
+    counted(h);
     k_i8_gemm<<<grid, I8_THREADS, I8_SMEM, st->stream>>>(tmA, tmB, p);
     OZB_CHECK(cudaGetLastError());
     ev_record(h, 3);

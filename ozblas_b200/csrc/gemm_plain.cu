@@ -375,18 +375,22 @@ int gemm_plain_core(cuozblasHandle_t *h, char ta, char tb, int m, int n, int k, 
                     int blocks = (k + 255) / 256;
                     if (blocks > 148 * 8) blocks = 148 * 8;
                     if (blocks < 1) blocks = 1;
+                    counted(h);
                     k_pair_dot<<<blocks, 256, 0, st->stream>>>(k, na, nb, Sa + (size_t)ia0 * ldk, ldk,
                                                                Sb + (size_t)ib0 * ldk, ldk, P + ia0 * nB + ib0, nB);
                 } else {
                     const int blocks = (int)(((int64_t)m * 32 + 255) / 256);
+                    counted(h);
                     k_pair_gemv<<<blocks, 256, 0, st->stream>>>(m, k, na, nb, ia0, ib0, nB, Sa, ldk, Sb, ldk, P,
                                                                 ldp);
                 }
                 OZB_CHECK(cudaGetLastError());
             }
         if (dot) {
+            counted(h);
             k_sum_pair_matrix<<<1, 32, 0, st->stream>>>(nA, nB, maxlevel, P, nB, h->sumMode, alpha, beta, C, scr);
         } else {
+            counted(h);
             k_sum_rows<<<(m + 127) / 128, 128, 0, st->stream>>>(m, nA, nB, maxlevel, P, ldp, h->sumMode, alpha, beta,
                                                               C, scr);
         }
@@ -424,15 +428,18 @@ int gemm_plain_core(cuozblasHandle_t *h, char ta, char tb, int m, int n, int k, 
         for (int64_t c0 = 0; c0 < n; c0 += ncols) {
             const int nc = (int)((n - c0) < ncols ? (n - c0) : ncols);
             dim3 g((m + kBM - 1) / kBM, (nc + kBN - 1) / kBN);
+            counted(h);
             k_gemm_pairs_dmma<true><<<g, 128, 0, st->stream>>>(m, nc, n, ldk, Sa, Sb + (size_t)c0 * ldk, dp, np, alpha,
                                                                beta, C, ldc, pbuf);
             OZB_CHECK(cudaGetLastError());
             const int64_t count = (int64_t)m * nc;
+            counted(h);
             k_sum_pairs<<<(unsigned)((count + 255) / 256), 256, 0, st->stream>>>(
                 m, count, np, pbuf, count, 1, alpha, beta, C + (size_t)c0 * ldc, ldc);
             OZB_CHECK(cudaGetLastError());
         }
     } else {
+        counted(h);
         k_gemm_pairs_dmma<false><<<grid, 128, 0, st->stream>>>(m, n, n, ldk, Sa, Sb, dp, np, alpha, beta, C, ldc,
                                                                nullptr);
         OZB_CHECK(cudaGetLastError());

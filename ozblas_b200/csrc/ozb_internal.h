@@ -25,10 +25,14 @@ struct State {
     int last_error = 0;
     int64_t splitA_ld = 0;        // slice stride of the pre-split A (cuozblasDcsrmvSplitA)
     cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};  // phase timers (split A/B, products)
+    uint64_t launches = 0;        // kernels this handle has launched (cuozblasGetLaunchCount)
 };
 
 
 inline State *state(cuozblasHandle_t *h) { return reinterpret_cast<State *>(h->hstBatchAddr); }
+
+// Count one kernel launch on the handle (every <<<>>> site calls this).
+inline void counted(cuozblasHandle_t *h) { state(h)->launches++; }
 
 // Phase timers of the reference handle (t_SplitA, t_SplitB, t_comp), taken
 // with CUDA events on the handle's stream; read after the call's final sync.

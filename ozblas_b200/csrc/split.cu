@@ -82,11 +82,13 @@ static int launch_split_lines(cuozblasHandle_t *h, bool write, int k, int nl, co
     if (write) {
         OZB_CHECK(cudaFuncSetAttribute(k_split_lines<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)(kSplitSmemMaxK * sizeof(double))));
+        counted(h);
         k_split_lines<true><<<nl, kSplitThreads, smem, st->stream>>>(k, nl, X, ldx, rho, levels, out, ldo, gscratch,
                                                                      nullptr);
     } else {
         OZB_CHECK(cudaFuncSetAttribute(k_split_lines<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)(kSplitSmemMaxK * sizeof(double))));
+        counted(h);
         k_split_lines<false><<<nl, kSplitThreads, smem, st->stream>>>(k, nl, X, ldx, rho, levels, nullptr, 0,
                                                                       gscratch, zmax_dev);
     }
@@ -139,6 +141,7 @@ __global__ void k_transpose(int rows, int cols, const double *__restrict__ A, in
 int transpose(cuozblasHandle_t *h, int rows, int cols, const double *A, int lda, double *out, int ldo) {
     if (rows == 0 || cols == 0) return CUOZBLAS_STATUS_SUCCESS;
     dim3 grid((rows + 31) / 32, (cols + 31) / 32), block(32, 8);
+    counted(h);
     k_transpose<<<grid, block, 0, state(h)->stream>>>(rows, cols, A, lda, out, ldo);
     OZB_CHECK(cudaGetLastError());
     return CUOZBLAS_STATUS_SUCCESS;
@@ -204,6 +207,7 @@ int split_vector(cuozblasHandle_t *h, int n, const double *x, int rho, int maxS,
     if (blocks > need) blocks = need > 0 ? need : 1;
     int *ns_dev = st->d_ints;
     void *args[] = {&n, &x, &rho, &maxS, &out, &ldo, &rem, &slot, &ns_dev};
+    counted(h);
     OZB_CHECK(cudaLaunchCooperativeKernel((void *)k_split_vector, dim3(blocks), dim3(256), args, 0, st->stream));
     OZB_CHECK(cudaMemcpyAsync(st->h_ints, ns_dev, sizeof(int), cudaMemcpyDeviceToHost, st->stream));
     OZB_CHECK(cudaStreamSynchronize(st->stream));
@@ -276,9 +280,11 @@ int split_csr_count(cuozblasHandle_t *h, int m, const double *val, const int *ro
     if (!ar.ok) return CUOZBLAS_STATUS_WORKSPACE;
     OZB_CHECK(cudaMemsetAsync(st->d_ints, 0, sizeof(int), st->stream));
     const int blocks = (int)(((int64_t)m * 32 + 255) / 256);
-    if (m > 0)
+    if (m > 0) {
+        counted(h);
         k_split_csr<false><<<blocks, 256, 0, st->stream>>>(m, val, rowptr, epsmode, shift, maxS - 1, rem, nullptr, 0,
                                                            st->d_ints);
+    }
     OZB_CHECK(cudaGetLastError());
     OZB_CHECK(cudaMemcpyAsync(st->h_ints, st->d_ints, sizeof(int), cudaMemcpyDeviceToHost, st->stream));
     OZB_CHECK(cudaStreamSynchronize(st->stream));
@@ -297,9 +303,11 @@ int split_csr_write(cuozblasHandle_t *h, int m, int nnz, const double *val, cons
     double *rem = ar.take<double>(nnz > 0 ? nnz : 1);
     if (!ar.ok) return CUOZBLAS_STATUS_WORKSPACE;
     const int blocks = (int)(((int64_t)m * 32 + 255) / 256);
-    if (m > 0)
+    if (m > 0) {
+        counted(h);
         k_split_csr<true><<<blocks, 256, 0, st->stream>>>(m, val, rowptr, epsmode, shift, ns, rem, out, ld,
                                                           nullptr);
+    }
     OZB_CHECK(cudaGetLastError());
     ar.release(mk);
     return CUOZBLAS_STATUS_SUCCESS;
