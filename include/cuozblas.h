@@ -193,6 +193,23 @@ int cuozblasDgemmI8(cuozblasHandle_t *h, char transa, char transb, int32_t m, in
                     const double *A, int32_t lda, const double *B, int32_t ldb, double beta, double *C,
                     int32_t ldc);
 
+/* Allocation-free INT8 precision-form DGEMM.  No counterpart in the
+ * reference.  For callers that cannot allocate device memory (work recorded
+ * while a CUDA graph is being captured, hosts whose device memory is
+ * budgeted up front or owned by another allocator): same arithmetic and
+ * results as cuozblasDgemmI8, with the flags passed directly and no handle;
+ * the scratch is a 64 MiB file-scope device array inside the library
+ * (resident on every GPU that loads it), so the call makes no cudaMalloc,
+ * cudaFree or other allocation.  Problems whose digits and work do not fit
+ * in those 64 MiB (about m = n = k = 1300 at 13 digits) return
+ * CUOZBLAS_STATUS_WORKSPACE with a message.  The first call on a device
+ * looks up the array's device address and should precede any stream
+ * capture.  All calls share the array: calls that overlap on the GPU race.
+ * `stream` is a cudaStream_t (NULL: legacy default stream). */
+int cuozblasDgemmI8Static(char transa, char transb, int32_t m, int32_t n, int32_t k, double alpha, const double *A,
+                          int32_t lda, const double *B, int32_t ldb, double beta, double *C, int32_t ldc,
+                          int32_t nSplitMax, int32_t fastMode, void *stream);
+
 /* Rule checks exported for the host-side tests (same code the kernels use). */
 int cuozblasRuleTau(double v);
 int cuozblasRuleRho(int32_t dim, int32_t splitEpsMode);

@@ -87,6 +87,8 @@ _daxpy = _sig("cuozblasDaxpy", [_HP, _i32, _d, _vp, _i32, _vp, _i32])
 _dgemv = _sig("cuozblasDgemv", [_HP, _ch, _i32, _i32, _d, _vp, _i32, _vp, _i32, _d, _vp, _i32])
 _dgemm = _sig("cuozblasDgemm", [_HP, _ch, _ch, _i32, _i32, _i32, _d, _vp, _i32, _vp, _i32, _d, _vp, _i32])
 _dgemm_i8 = _sig("cuozblasDgemmI8", [_HP, _ch, _ch, _i32, _i32, _i32, _d, _vp, _i32, _vp, _i32, _d, _vp, _i32])
+_dgemm_i8_static = _sig("cuozblasDgemmI8Static", [_ch, _ch, _i32, _i32, _i32, _d, _vp, _i32, _vp, _i32, _d, _vp,
+                                                  _i32, _i32, _i32, _vp])
 _dcsrmv = _sig("cuozblasDcsrmv", [_HP, _ch, _i32, _i32, _i32, _d, _vp, _vp, _vp, _vp, _vp, _d, _vp])
 _dsplita = _sig("cuozblasDcsrmvSplitA", [_HP, _ch, _i32, _i32, _i32, _vp, _vp, _vp, C.POINTER(_vp)])
 _dcg = _sig("cuozblasDcg", [_HP, _ch, _i32, _i32, _vp, _vp, _vp, _vp, _vp, _vp, _i32, _d])
@@ -98,7 +100,7 @@ _version = _sig("cuozblasVersion", [], C.c_char_p)
 C_ABI_SYMBOLS = [
     "cuozblasHandleCreate", "cuozblasHandleDestroy", "cuozblasSetStream", "cuozblasGetLaunchCount", "cuozblasDdot", "cuozblasDnrm2",
     "cuozblasDaxpy", "cuozblasDgemv", "cuozblasDgemm", "cuozblasDcsrmv", "cuozblasDcsrmvSplitA", "cuozblasDcg",
-    "cuozblasDgemmI8", "cuozblasRuleTau", "cuozblasRuleRho", "cuozblasVersion",
+    "cuozblasDgemmI8", "cuozblasDgemmI8Static", "cuozblasRuleTau", "cuozblasRuleRho", "cuozblasVersion",
 ]
 
 
@@ -171,6 +173,13 @@ def dgemm(h, ta, tb, m, n, k, alpha, A, lda, B, ldb, beta, Cm, ldc):
 def dgemm_i8(h, ta, tb, m, n, k, alpha, A, lda, B, ldb, beta, Cm, ldc):
     _chk("cuozblasDgemmI8", _dgemm_i8(h.ref, ta.encode(), tb.encode(), m, n, k, alpha, _ptr(A), lda, _ptr(B),
                                       ldb, beta, _ptr(Cm), ldc))
+
+
+def dgemm_i8_static(ta, tb, m, n, k, alpha, A, lda, B, ldb, beta, Cm, ldc, nSplitMax=0, fastMode=0, stream=None):
+    """INT8 DGEMM without a handle and without any allocation (library-internal 64 MiB scratch)."""
+    s = None if stream is None else (stream if isinstance(stream, int) else getattr(stream, "cuda_stream", stream))
+    _chk("cuozblasDgemmI8Static", _dgemm_i8_static(ta.encode(), tb.encode(), m, n, k, alpha, _ptr(A), lda, _ptr(B),
+                                                   ldb, beta, _ptr(Cm), ldc, nSplitMax, fastMode, s))
 
 
 def ddot(h, n, x, y, incx=1, incy=1) -> float:

@@ -31,6 +31,7 @@
 // an abort flag; a timeout reports CUOZBLAS_STATUS_DEVICE_TIMEOUT.
 #include <cuda.h>
 
+#include <mutex>
 #include <vector>
 
 #include "ozb_device.cuh"
@@ -596,7 +597,241 @@ int gemm_i8_core(cuozblasHandle_t *h, char ta, char tb, int m, int n, int k, dou
     return CUOZBLAS_STATUS_SUCCESS;
 }
 
+// ---------------------------------------------------------------------------
+// Allocation-free variant of the INT8 product path (cuozblasDgemmI8Static).
+//
+// Some callers cannot allocate device memory at all: code that runs while a
+// CUDA graph is being captured, real-time or embedded hosts whose memory is
+// budgeted up front, and hosts whose own allocator owns the whole device.
+// For them the digit split and the tcgen05 product kernel run on scratch in
+// the file-scope array below instead of a handle's arena, so a call makes no
+// cudaMalloc, no cudaFree and no other allocation.  The array is 64 MiB and
+// every GPU that loads this library holds it until the process exits.  The
+// host code reaches it through the device address that cudaGetSymbolAddress
+// returns, looked up once per device (with that device current) on the first
+// call there; that first call should therefore come before any stream capture.
+// All calls share the one array and it keeps the last call's contents, so
+// calls whose work overlaps on the GPU (other streams, other host threads)
+// race; the counters and the error word are cleared at the start of each call.
+// ---------------------------------------------------------------------------
+__global__ void k_transpose(int rows, int cols, const double *__restrict__ A, int lda, double *__restrict__ out,
+                            int ldo);  // split.cu
+
+constexpr size_t kI8StaticBytes = 64ull << 20;
+static __device__ __align__(256) unsigned char g_i8_static_scratch[kI8StaticBytes];
+
+constexpr int kI8StaticMaxDevices = 64;
+static unsigned char *g_i8_static_addr[kI8StaticMaxDevices];
+static std::mutex g_i8_static_mu;
+
+static int i8_static_area(unsigned char **out) {
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return CUOZBLAS_STATUS_CUDA_ERROR;
+    if (dev < 0 || dev >= kI8StaticMaxDevices) return CUOZBLAS_STATUS_NOT_SUPPORTED;
+    std::lock_guard<std::mutex> lock(g_i8_static_mu);
+    if (g_i8_static_addr[dev] == nullptr) {
+        void *p = nullptr;
+        const cudaError_t e = cudaGetSymbolAddress(&p, g_i8_static_scratch);
+        if (e != cudaSuccess || p == nullptr) {
+            fprintf(stderr, "cuozblasDgemmI8Static: cudaGetSymbolAddress failed: %s\n", cudaGetErrorString(e));
+            return CUOZBLAS_STATUS_CUDA_ERROR;
+        }
+        g_i8_static_addr[dev] = static_cast<unsigned char *>(p);
+    }
+    *out = g_i8_static_addr[dev];
+    return CUOZBLAS_STATUS_SUCCESS;
+}
+
+struct StaticBump {
+    unsigned char *base;
+    size_t off = 0;
+    bool ok = true;
+    template <typename T>
+    T *take(size_t count) {
+        const size_t start = (off + 255) / 256 * 256, bytes = count * sizeof(T);
+        if (start + bytes > kI8StaticBytes) {
+            ok = false;
+            return nullptr;
+        }
+        off = start + bytes;
+        return reinterpret_cast<T *>(base + start);
+    }
+};
+
+constexpr int kI8StaticMaxItems = 2048, kI8StaticMaxGroups = 256;
+
+static int dgemm_i8_static(char ta, char tb, int m, int n, int k, double alpha, const double *A, int lda,
+                           const double *B, int ldb, double beta, double *C, int ldc, int nsplit_max, int fast,
+                           cudaStream_t stream) {
+    unsigned char *area = nullptr;
+    OZB_TRY(i8_static_area(&area));
+    StaticBump bump{area};
+    int *d_err = bump.take<int>(1);
+    int *d_cnt = bump.take<int>(2);
+    int4 *d_sched = bump.take<int4>(kI8StaticMaxItems + kI8StaticMaxGroups);
+    const int k_pad = k > 0 ? (k + I8_BK - 1) / I8_BK * I8_BK : I8_BK;  // k = 0: zero digits, C = beta * C
+    const int m_pad = (m + I8_BM - 1) / I8_BM * I8_BM, n_pad = (n + I8_BN - 1) / I8_BN * I8_BN;
+    int *ea = bump.take<int>(m), *eb = bump.take<int>(n);
+    const bool tA = !is_trans(ta), tB = is_trans(tb);  // lines must be made K-contiguous
+    double *la = tA ? bump.take<double>((size_t)m * k) : nullptr;
+    double *lb = tB ? bump.take<double>((size_t)n * k) : nullptr;
+    if (!bump.ok) {
+        fprintf(stderr, "cuozblasDgemmI8Static: m=%d n=%d k=%d needs more than the %zu MiB static scratch\n", m, n, k,
+                kI8StaticBytes >> 20);
+        return CUOZBLAS_STATUS_WORKSPACE;
+    }
+    OZB_CHECK(cudaMemsetAsync(d_err, 0, sizeof(int), stream));
+    OZB_CHECK(cudaMemsetAsync(d_cnt, 0, 2 * sizeof(int), stream));
+    const double *srcA = A, *srcB = B;
+    int ldsA = lda, ldsB = ldb;
+    if (tA && k > 0) {
+        k_transpose<<<dim3((m + 31) / 32, (k + 31) / 32), dim3(32, 8), 0, stream>>>(m, k, A, lda, la, k);
+        srcA = la;
+        ldsA = k;
+    }
+    if (tB && k > 0) {
+        k_transpose<<<dim3((n + 31) / 32, (k + 31) / 32), dim3(32, 8), 0, stream>>>(n, k, B, ldb, lb, k);
+        srcB = lb;
+        ldsB = k;
+    }
+    k_digit_count<<<m, 256, 0, stream>>>(k, m, srcA, ldsA, ea, d_cnt);
+    k_digit_count<<<n, 256, 0, stream>>>(k, n, srcB, ldsB, eb, d_cnt + 1);
+    OZB_CHECK(cudaGetLastError());
+    int cnt[2] = {0, 0};
+    OZB_CHECK(cudaMemcpyAsync(cnt, d_cnt, sizeof(cnt), cudaMemcpyDeviceToHost, stream));
+    OZB_CHECK(cudaStreamSynchronize(stream));
+    const int cap = nsplit_max > 0 ? nsplit_max : kI8DefaultCap;
+    int nA = cnt[0] < 1 ? 1 : cnt[0], nB = cnt[1] < 1 ? 1 : cnt[1];
+    if (nA > cap) nA = cap;
+    if (nB > cap) nB = cap;
+    int8_t *da = bump.take<int8_t>((size_t)nA * m_pad * k_pad);
+    int8_t *db = bump.take<int8_t>((size_t)nB * n_pad * k_pad);
+    if (!bump.ok) {
+        fprintf(stderr,
+                "cuozblasDgemmI8Static: m=%d n=%d k=%d with %d x %d digits needs more than the %zu MiB static "
+                "scratch\n",
+                m, n, k, nA, nB, kI8StaticBytes >> 20);
+        return CUOZBLAS_STATUS_WORKSPACE;
+    }
+    k_digit_write<<<(unsigned)(((int64_t)m_pad * (k_pad / 16) + 255) / 256), 256, 0, stream>>>(k, m, m_pad, k_pad, nA,
+                                                                                              srcA, ldsA, ea, da);
+    k_digit_write<<<(unsigned)(((int64_t)n_pad * (k_pad / 16) + 255) / 256), 256, 0, stream>>>(k, n, n_pad, k_pad, nB,
+                                                                                              srcB, ldsB, eb, db);
+    OZB_CHECK(cudaGetLastError());
+
+    // the same schedule as cuozblasDgemmI8, built in fixed host arrays
+    const int maxlevel = fast ? (nA < nB ? nA : nB) - 1 : nA + nB - 2;
+    const int nkb = k_pad / I8_BK;
+    const int64_t kb_cap = I8_MAX_TERMS / I8_BK;
+    int4 items[kI8StaticMaxItems], groups[kI8StaticMaxGroups];
+    int64_t gbound[kI8StaticMaxGroups];
+    int ni = 0, ng = 0;
+    for (int L = maxlevel; L >= 0; L--) {
+        const int lo = L - (nB - 1) > 0 ? L - (nB - 1) : 0, hi = L < nA - 1 ? L : nA - 1;
+        int64_t used = 0;
+        int gbeg = ni;
+        for (int ia = lo; ia <= hi; ia++) {
+            for (int kb0 = 0; kb0 < nkb;) {
+                int64_t room = kb_cap - used;
+                if (room <= 0) {
+                    if (ng >= kI8StaticMaxGroups) return CUOZBLAS_STATUS_WORKSPACE;
+                    gbound[ng] = used * I8_BK * 127 * 127;
+                    groups[ng++] = make_int4(gbeg, ni, L, 0);
+                    gbeg = ni;
+                    used = 0;
+                    room = kb_cap;
+                }
+                const int kb1 = (int)((nkb - kb0) < room ? nkb : kb0 + room);
+                if (ni >= kI8StaticMaxItems) return CUOZBLAS_STATUS_WORKSPACE;
+                items[ni++] = make_int4(ia, L - ia, kb0, kb1);
+                used += kb1 - kb0;
+                kb0 = kb1;
+            }
+        }
+        if (ni > gbeg) {
+            if (ng >= kI8StaticMaxGroups) return CUOZBLAS_STATUS_WORKSPACE;
+            gbound[ng] = used * I8_BK * 127 * 127;
+            groups[ng++] = make_int4(gbeg, ni, L, 0);
+        }
+    }
+    {
+        unsigned __int128 lbound[2 * 64];
+        int run_hi[2 * 64], run_lo[2 * 64];
+        if (maxlevel + 1 > 2 * 64) return CUOZBLAS_STATUS_NOT_SUPPORTED;
+        for (int L = 0; L <= maxlevel; L++) lbound[L] = 0;
+        for (int g = 0; g < ng; g++) lbound[groups[g].z] += (unsigned __int128)gbound[g];
+        const unsigned __int128 lim = (unsigned __int128)1 << 53;
+        for (int L0 = 0; L0 <= maxlevel;) {
+            unsigned __int128 b = lbound[L0];
+            int L1 = L0;
+            while (L1 + 1 <= maxlevel && (b << 7) + lbound[L1 + 1] < lim) {
+                b = (b << 7) + lbound[L1 + 1];
+                L1++;
+            }
+            for (int L = L0; L <= L1; L++) {
+                run_lo[L] = L0;
+                run_hi[L] = L1;
+            }
+            L0 = L1 + 1;
+        }
+        bool first = true;
+        for (int g = 0; g < ng; g++) {
+            const int L = groups[g].z;
+            int meta = 7 * (run_hi[L] - L);
+            const bool last_of_level = (g + 1 == ng) || groups[g + 1].z != L;
+            if (last_of_level && L == run_lo[L]) {
+                meta |= (1 << 8) | (first ? (1 << 9) : 0);
+                first = false;
+                groups[g].z = -7 * (run_hi[L] + 2);
+            } else {
+                groups[g].z = 0;
+            }
+            groups[g].w = meta;
+        }
+        groups[ng - 1].w |= (1 << 10);
+    }
+    OZB_CHECK(cudaMemcpyAsync(d_sched, items, sizeof(int4) * ni, cudaMemcpyHostToDevice, stream));
+    OZB_CHECK(cudaMemcpyAsync(d_sched + ni, groups, sizeof(int4) * ng, cudaMemcpyHostToDevice, stream));
+    CUtensorMap tmA, tmB;
+    OZB_TRY(make_map(&tmA, da, (uint64_t)nA * m_pad, k_pad, I8_BM));
+    OZB_TRY(make_map(&tmB, db, (uint64_t)nB * n_pad, k_pad, I8_BN));
+    I8Params p;
+    p.m = m;
+    p.n = n;
+    p.m_pad = m_pad;
+    p.n_pad = n_pad;
+    p.ldc = ldc;
+    p.tiles_m = m_pad / I8_BM;
+    p.tiles_n = n_pad / I8_BN;
+    p.n_items = ni;
+    p.n_groups = ng;
+    p.items = d_sched;
+    p.groups = d_sched + ni;
+    p.ea = ea;
+    p.eb = eb;
+    p.alpha = alpha;
+    p.beta = beta;
+    p.C = C;
+    p.err = d_err;
+    int dev = 0, nsm = 0;
+    OZB_CHECK(cudaGetDevice(&dev));
+    OZB_CHECK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+    const int ntiles = p.tiles_m * p.tiles_n;
+    OZB_CHECK(cudaFuncSetAttribute(k_i8_gemm, cudaFuncAttributeMaxDynamicSharedMemorySize, I8_SMEM));
+    k_i8_gemm<<<ntiles < nsm ? ntiles : nsm, I8_THREADS, I8_SMEM, stream>>>(tmA, tmB, p);
+    OZB_CHECK(cudaGetLastError());
+    int err = 0;
+    OZB_CHECK(cudaMemcpyAsync(&err, d_err, sizeof(int), cudaMemcpyDeviceToHost, stream));
+    OZB_CHECK(cudaStreamSynchronize(stream));
+    if (err != 0) {
+        fprintf(stderr, "cuozblasDgemmI8Static: product kernel wait timed out (code %d)\n", err);
+        return CUOZBLAS_STATUS_DEVICE_TIMEOUT;
+    }
+    return CUOZBLAS_STATUS_SUCCESS;
+}
+
 }  // namespace ozb
+
 
 extern "C" int cuozblasDgemmI8(cuozblasHandle_t *h, char transa, char transb, int32_t m, int32_t n, int32_t k,
                                double alpha, const double *A, int32_t lda, const double *B, int32_t ldb, double beta,
@@ -607,4 +842,17 @@ extern "C" int cuozblasDgemmI8(cuozblasHandle_t *h, char transa, char transb, in
     if (h->nSplitMax < 0 || h->nSplitMax > 64) return CUOZBLAS_STATUS_INVALID_VALUE;
     if (m == 0 || n == 0) return CUOZBLAS_STATUS_SUCCESS;
     return gemm_i8_core(h, transa, transb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc);
+}
+
+// Allocation-free INT8 product (see dgemm_i8_static above): same arguments and
+// results as cuozblasDgemmI8 with the flags passed directly, no handle.
+extern "C" int cuozblasDgemmI8Static(char transa, char transb, int32_t m, int32_t n, int32_t k, double alpha,
+                                     const double *A, int32_t lda, const double *B, int32_t ldb, double beta,
+                                     double *C, int32_t ldc, int32_t nSplitMax, int32_t fastMode, void *stream) {
+    using namespace ozb;
+    if (m < 0 || n < 0 || k < 0 || ldc < (m > 1 ? m : 1) || nSplitMax < 0 || nSplitMax > 64)
+        return CUOZBLAS_STATUS_INVALID_VALUE;
+    if (m == 0 || n == 0) return CUOZBLAS_STATUS_SUCCESS;
+    return dgemm_i8_static(transa, transb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, nSplitMax, fastMode,
+                           reinterpret_cast<cudaStream_t>(stream));
 }
