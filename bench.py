@@ -171,7 +171,9 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--ref-rows", type=int, default=256)
     ap.add_argument("--full-pairs", action="store_true", help="headline with the full pair set instead of triangular")
+    ap.add_argument("--n", type=int, default=N_DIM, help="m = n = k (default 8192; smaller for profiling captures)")
     args = ap.parse_args()
+    globals()["N_DIM"] = args.n
     args.warmup = max(args.warmup, 3)
 
     rank = int(os.environ.get("RANK", "0"))
@@ -285,7 +287,7 @@ def main():
             "value": value, "unit": "TFLOPS", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int8",
             "data": "synthetic",
-            "config": {"workload": "ozaki_dgemm_int8 m=n=k=8192 phi=1", "m": n, "n": n, "k": n, "phi": PHI,
+            "config": {"workload": f"ozaki_dgemm_int8 m=n=k={n} phi=1", "m": n, "n": n, "k": n, "phi": PHI,
                        "slices": [nA, nB], "pairs": pairs, "pair_set": "full" if args.full_pairs else "triangular",
                        "sumMode": 0, "l2": "inputs 512 MiB each > L2, no flush",
                        "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},

@@ -54,6 +54,7 @@ enum { ERR_TIMEOUT_PRODUCER = 1, ERR_TIMEOUT_MMA = 2, ERR_TIMEOUT_EPI = 3 };
 struct I8Params {
     int m, n, m_pad, n_pad, ldc;
     int tiles_m, tiles_n, n_items, n_groups;
+    int strip;           // tile rows per rasterisation strip
     const int4 *items;   // {ia, ib, kb0, kb1} in processing order
     const int4 *groups;  // {item_begin, item_end, flush scale exponent, meta: shift | flush<<8 | first<<9 | last<<10}
     const int *ea, *eb;  // line exponents
@@ -61,6 +62,16 @@ struct I8Params {
     double *C;
     int *err;
 };
+
+// Tile order: strips of `strip` tile rows, column-major inside a strip, so
+// the CTAs resident at one time share A and B panels in L2.
+__device__ __forceinline__ void tile_coords(int tile, const I8Params &p, int &tm, int &tn) {
+    const int per_strip = p.strip * p.tiles_n;
+    const int s = tile / per_strip, w = tile - s * per_strip;
+    const int rows = min(p.strip, p.tiles_m - s * p.strip);
+    tm = s * p.strip + w % rows;
+    tn = w / rows;
+}
 
 __global__ void __launch_bounds__(I8_THREADS, 1)
     k_i8_gemm(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, I8Params p) {
@@ -102,7 +113,8 @@ __global__ void __launch_bounds__(I8_THREADS, 1)
             uint32_t stage = 0, phase = 0;
             bool ok = true;
             for (int tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x) {
-                const int tm = tile % p.tiles_m, tn = tile / p.tiles_m;
+                int tm, tn;
+                tile_coords(tile, p, tm, tn);
                 for (int it = 0; it < p.n_items && ok; it++) {
                     const int4 item = p.items[it];
                     for (int kb = item.z; kb < item.w; kb++) {
@@ -196,7 +208,8 @@ __global__ void __launch_bounds__(I8_THREADS, 1)
         uint32_t abuf = 0, aphase = 0;
         bool ok = true;
         for (int tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x) {
-            const int tm = tile % p.tiles_m, tn = tile / p.tiles_m;
+            int tm, tn;
+            tile_coords(tile, p, tm, tn);
             const int gr = tm * I8_BM + row;
             double acc[64];  // exact integer-valued run of levels (< 2^53)
 #pragma unroll
@@ -563,6 +576,7 @@ int gemm_i8_core(cuozblasHandle_t *h, char ta, char tb, int m, int n, int k, dou
     p.ldc = ldc;
     p.tiles_m = da.lines_pad / I8_BM;
     p.tiles_n = db.lines_pad / I8_BN;
+    p.strip = p.tiles_m < 12 ? p.tiles_m : 12;
     p.n_items = (int)items.size();
     p.n_groups = (int)groups.size();
     p.items = d_sched;
@@ -803,6 +817,7 @@ static int dgemm_i8_static(char ta, char tb, int m, int n, int k, double alpha, 
     p.ldc = ldc;
     p.tiles_m = m_pad / I8_BM;
     p.tiles_n = n_pad / I8_BN;
+    p.strip = p.tiles_m < 12 ? p.tiles_m : 12;
     p.n_items = ni;
     p.n_groups = ng;
     p.items = d_sched;
