@@ -371,6 +371,38 @@ def extras(ozb, h, torch, A, B, C, n):
         h.sumMode = sm
         ms = timed(lambda: ozb.ddot(h, nv, x, y), reps=3)
         out[f"ddot_2p24_sum{sm}"] = {"GBps": 16.0 * nv / ms / 1e6, "ms": ms, "slices": [h.nSplitA, h.nSplitB]}
+    del x, y, r1, r2
+    # CSRMV: 7-point stencil on 128^3, values and x (U - 0.5) exp(N(0,1)), beta = 0
+    g3 = 128
+    m = g3 ** 3
+    idx = torch.arange(m, device="cuda", dtype=torch.int64)
+    xi, yi, zi = idx % g3, (idx // g3) % g3, idx // (g3 * g3)
+    offs = [(-g3 * g3, zi > 0), (-g3, yi > 0), (-1, xi > 0), (0, None), (1, xi < g3 - 1), (g3, yi < g3 - 1),
+            (g3 * g3, zi < g3 - 1)]
+    cols, masks = [], []
+    for o, msk in offs:
+        cols.append(idx + o)
+        masks.append(torch.ones(m, dtype=torch.bool, device="cuda") if msk is None else msk)
+    C7 = torch.stack(cols, 1)
+    M7 = torch.stack(masks, 1)
+    colind = C7[M7].to(torch.int32).contiguous()
+    rowptr = torch.zeros(m + 1, dtype=torch.int64, device="cuda")
+    rowptr[1:] = torch.cumsum(M7.sum(1), 0)
+    rowptr = rowptr.to(torch.int32).contiguous()
+    nnz = colind.numel()
+    r1 = torch.rand(nnz, dtype=torch.float64, device="cuda", generator=g)
+    r2 = torch.rand(nnz, dtype=torch.float64, device="cuda", generator=g)
+    val = (r1 - 0.5) * torch.exp(torch.sqrt(-2 * torch.log(r1)) * torch.sin(2 * torch.pi * r2))
+    r1 = torch.rand(m, dtype=torch.float64, device="cuda", generator=g)
+    r2 = torch.rand(m, dtype=torch.float64, device="cuda", generator=g)
+    xv = (r1 - 0.5) * torch.exp(torch.sqrt(-2 * torch.log(r1)) * torch.sin(2 * torch.pi * r2))
+    yv = torch.zeros(m, dtype=torch.float64, device="cuda")
+    nbytes = 12.0 * nnz + 4.0 * (m + 1) + 8.0 * m + 8.0 * m
+    for sm in (0, 1):
+        h.sumMode = sm
+        ms = timed(lambda: ozb.dcsrmv(h, "n", m, m, nnz, 1.0, val, colind, rowptr, xv, 0.0, yv), reps=3)
+        out[f"dcsrmv_stencil128_sum{sm}"] = {"GBps": nbytes / ms / 1e6, "ms": ms, "nnz": nnz,
+                                             "slices": [h.nSplitA, h.nSplitB]}
     h.sumMode = 0
     return out
 

@@ -15,6 +15,24 @@ int launch_csrmv_plain(cuozblasHandle_t *h, int m, const double *val, const int 
                        const double *x, double alpha, double beta, double *y);
 int csrmv_presplit(cuozblasHandle_t *h, int m, int n, double alpha, const double *As, int nA, int64_t ld_s,
                    const int *colind, const int *rowptr, const double *x, double beta, double *y);
+int dot_fused(cuozblasHandle_t *h, int n, const double *x, const double *y, double *out_dev, bool *done, int *nA,
+              int *nB);
+int csrmv_fused(cuozblasHandle_t *h, int m, int n, double alpha, const double *val, const int *colind,
+                const int *rowptr, const double *x, double beta, double *y, int shift, bool *done, int *nA_out,
+                int *nB_out);
+
+// CSRMV exec info as the reference records it (src/cpu/ozblas_csrmv.cpp:104-119)
+static void csrmv_info(cuozblasHandle_t *h, int nA, int nB) {
+    h->nSplitA = (float)nA;
+    h->nSplitB = (float)nB;
+    int maxlevel = (nA - 1) + (nB - 1);
+    const int mn = nA - 1 < nB - 1 ? nA - 1 : nB - 1;
+    maxlevel = (maxlevel - h->fastMode) > mn ? (maxlevel - h->fastMode) : mn;
+    int ic = 0;
+    for (int ia = 0; ia < (maxlevel + 1 < nA ? maxlevel + 1 : nA); ia++)
+        ic += (nB < maxlevel + 1 - ia ? nB : maxlevel + 1 - ia);
+    h->nSplitC = (float)ic;
+}
 
 static double wall() {
     struct timeval tv;
@@ -56,7 +74,16 @@ static int dot_impl(cuozblasHandle_t *h, int n, const double *x, const double *y
     State *st = state(h);
     double *d = reinterpret_cast<double *>(h->devWorkCommon);
     OZB_CHECK(cudaMemsetAsync(d, 0, sizeof(double), st->stream));
-    OZB_TRY(gemm_plain_core(h, 't', 'n', 1, 1, n, 1.0, x, n, y, n, 0.0, d, 1, 0));
+    bool done = false;
+    int nA = 0, nB = 0;
+    if (h->splitEpsMode == 0) OZB_TRY(dot_fused(h, n, x, y, d, &done, &nA, &nB));
+    if (done) {
+        h->nSplitA = (float)nA;
+        h->nSplitB = (float)nB;
+        h->nSplitC = 1.f;
+    } else {
+        OZB_TRY(gemm_plain_core(h, 't', 'n', 1, 1, n, 1.0, x, n, y, n, 0.0, d, 1, 0));
+    }
     OZB_CHECK(cudaMemcpyAsync(st->h_dbl, d, sizeof(double), cudaMemcpyDeviceToHost, st->stream));
     OZB_CHECK(cudaStreamSynchronize(st->stream));
     *ret = st->h_dbl[0];
@@ -218,6 +245,15 @@ int cuozblasDcsrmv(cuozblasHandle_t *h, char trans, int32_t m, int32_t n, int32_
         OZB_TRY(csrmv_presplit(h, m, n, alpha, val, h->nSplitA_, state(h)->splitA_ld, colind, rowptr, x, beta, y));
         return finish(h, t0);
     }
+    if (h->fastMode == 0 && h->splitEpsMode != 2) {
+        bool done = false;
+        int fa = 0, fb = 0;
+        OZB_TRY(csrmv_fused(h, m, n, alpha, val, colind, rowptr, x, beta, y, 1, &done, &fa, &fb));
+        if (done) {
+            csrmv_info(h, fa, fb);
+            return finish(h, t0);
+        }
+    }
     Arena ar(h);
     const int64_t ld = splitA_ld(nnz);
     int nA = 0;
@@ -282,6 +318,9 @@ int cuozblasDcg(cuozblasHandle_t *h, char trans, int32_t n, int32_t nnz, const v
     h->cg_numiter = 0;
     double *As = nullptr;
     OZB_TRY(cuozblasDcsrmvSplitA(h, trans, n, n, nnz, descrA, val, rowptr, &As));
+    // The pre-split rows are re-cut on the fly with the same tuned shift:
+    // identical slices (each row's chain is independent of the others).
+    const int cg_shift = h->splitShift;
     // CG vectors live above the preserved split of A for the whole solve
     State *st = state(h);
     st->off = h->memMaskSplitA;
@@ -303,7 +342,17 @@ int cuozblasDcg(cuozblasHandle_t *h, char trans, int32_t n, int32_t nnz, const v
     if (cudaMemcpyAsync(r, b, sizeof(double) * n, cudaMemcpyDeviceToDevice, st->stream) != cudaSuccess ||
         cudaMemsetAsync(q, 0, sizeof(double) * nn, st->stream) != cudaSuccess)
         return fail(CUOZBLAS_STATUS_CUDA_ERROR);
-    if ((status = cuozblasDcsrmv(h, trans, n, n, nnz, -1., descrA, As, colind, rowptr, x, 1., r))) return fail(status);
+    auto spmv = [&](double al, const double *xv, double be, double *yv) -> int {
+        if (h->fastMode == 0 && h->splitEpsMode != 2) {
+            OZB_TRY(counter_init(h));
+            bool done = false;
+            int fa = 0, fb = 0;
+            OZB_TRY(csrmv_fused(h, n, n, al, val, colind, rowptr, xv, be, yv, cg_shift, &done, &fa, &fb));
+            if (done) return CUOZBLAS_STATUS_SUCCESS;
+        }
+        return cuozblasDcsrmv(h, trans, n, n, nnz, al, descrA, As, colind, rowptr, xv, be, yv);
+    };
+    if ((status = spmv(-1., x, 1., r))) return fail(status);
     if ((status = cuozblasDdot(h, n, r, 1, r, 1, &dold))) return fail(status);
     double resi = sqrt(dold);
     auto true_res = [&]() -> double {
@@ -328,8 +377,7 @@ int cuozblasDcg(cuozblasHandle_t *h, char trans, int32_t n, int32_t nnz, const v
     int verbose_cnt = 1;
     while (h->cg_numiter < maxiter) {
         h->cg_numiter++;
-        if ((status = cuozblasDcsrmv(h, trans, n, n, nnz, 1., descrA, As, colind, rowptr, p, 0., q)))
-            return fail(status);
+        if ((status = spmv(1., p, 0., q))) return fail(status);
         if ((status = cuozblasDdot(h, n, p, 1, q, 1, &tmp))) return fail(status);
         const double alpha = dold / tmp;
         if ((status = launch_axpy(h, n, alpha, p, x))) return fail(status);

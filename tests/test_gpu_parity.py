@@ -198,3 +198,83 @@ def test_invalid_arguments(handle, ozb, cuda):
     with pytest.raises(ozb.OzblasError) as e:
         ozb.ddot(handle, 8, x, x)
     assert e.value.code == 4
+
+
+# ---- fused DOT / CSRMV: the paths that must hand over to the general algorithm ----
+
+def test_ddot_chain_prediction_fails(oracle, handle, ozb, cuda):
+    """A remainder maximum below the predicted binade: the fused DOT must fall back."""
+    n = 4096
+    x = oracle.phi_vector(n, 1.0, 1) * 2.0 ** -40
+    x[0] = 1.0  # the only large entry: after level 0 every remainder is tiny
+    y = oracle.phi_vector(n, 1.0, 2)
+    for sm in (0, 1):
+        handle.sumMode = sm
+        d = ozb.ddot(handle, n, dev(cuda, x), dev(cuda, y))
+        r, info = oracle.ddot(make_flags(sumMode=sm), x, y)
+        assert np.float64(d).view(np.int64) == np.float64(r).view(np.int64), (sm, d, r)
+        assert (handle.nSplitA, handle.nSplitB) == (info.nSplitA, info.nSplitB)
+
+
+@pytest.mark.parametrize("phi", [6.0, 10.0])
+def test_ddot_many_levels(phi, oracle, handle, ozb, cuda):
+    """More levels than the fused pass holds (wide exponent range)."""
+    n = 20000
+    x, y = oracle.phi_vector(n, phi, 1), oracle.phi_vector(n, phi, 2)
+    for sm in (0, 1):
+        handle.sumMode = sm
+        d = ozb.ddot(handle, n, dev(cuda, x), dev(cuda, y))
+        r, info = oracle.ddot(make_flags(sumMode=sm), x, y)
+        assert np.float64(d).view(np.int64) == np.float64(r).view(np.int64), (phi, sm, d, r, info.nSplitA)
+
+
+def _csr_run(oracle, handle, ozb, cuda, rowptr, colind, val, x, y0, alpha, beta, sm, fm=0):
+    n = len(rowptr) - 1
+    ref, info = oracle.dcsrmv(make_flags(sumMode=sm, fastMode=fm), n, len(x), alpha, val, colind, rowptr, x, beta, y0)
+    handle.sumMode, handle.fastMode = sm, fm
+    dy = dev(cuda, y0)
+    ozb.dcsrmv(handle, "n", n, len(x), len(val), alpha, dev(cuda, val), dev(cuda, colind), dev(cuda, rowptr),
+               dev(cuda, x), beta, dy)
+    assert bits_equal(host(dy), ref), first_diff(host(dy), ref)
+    assert (handle.nSplitA, handle.nSplitB, handle.nSplitC) == (info.nSplitA, info.nSplitB, info.nSplitC)
+
+
+@pytest.mark.parametrize("sm", [0, 1])
+def test_dcsrmv_long_rows_and_deep_rows(sm, oracle, handle, ozb, cuda):
+    """Rows longer than 8 entries and rows needing many levels go to the per-row kernel."""
+    rng = np.random.default_rng(5)
+    n = 300
+    lens = rng.integers(0, 20, n)
+    rowptr = np.concatenate([[0], np.cumsum(lens)]).astype(np.int32)
+    colind = np.concatenate([np.sort(rng.choice(n, l, replace=False)) for l in lens]).astype(np.int32)
+    val = oracle.phi_vector(len(colind), 1.0, 7)
+    for r in range(0, n, 37):  # some rows with a huge in-row exponent range
+        lo, hi = rowptr[r], rowptr[r + 1]
+        if hi - lo >= 2:
+            val[lo] *= 2.0 ** 150
+            val[hi - 1] *= 2.0 ** -150
+    x = oracle.phi_vector(n, 1.0, 8)
+    y0 = oracle.phi_vector(n, 1.0, 9)
+    _csr_run(oracle, handle, ozb, cuda, rowptr, colind, val, x, y0, 0.5, -2.0, sm)
+
+
+@pytest.mark.parametrize("sm", [0, 1])
+def test_dcsrmv_x_chain_general_path(sm, oracle, handle, ozb, cuda):
+    """x whose chain is not the predicted one, and x needing more than 8 levels."""
+    rowptr, colind, val = stencil_case(oracle, 10, 9, 8)
+    n = len(rowptr) - 1
+    y0 = oracle.phi_vector(n, 1.0, 3)
+    x = oracle.phi_vector(n, 1.0, 2) * 2.0 ** -40
+    x[5] = 1.0
+    _csr_run(oracle, handle, ozb, cuda, rowptr, colind, val, x, y0, 1.0, 0.0, sm)
+    x = oracle.phi_vector(n, 9.0, 2)
+    _csr_run(oracle, handle, ozb, cuda, rowptr, colind, val, x, y0, 1.0, 0.0, sm)
+
+
+def test_dcsrmv_fastmode_uses_general_path(oracle, handle, ozb, cuda):
+    rowptr, colind, val = stencil_case(oracle, 6, 5, 4)
+    n = len(rowptr) - 1
+    x = oracle.phi_vector(n, 1.0, 2)
+    y0 = np.zeros(n)
+    # fastMode = 1 drops only the last level: pair sets agree with the reference's storage
+    _csr_run(oracle, handle, ozb, cuda, rowptr, colind, val, x, y0, 1.0, 0.0, 0, fm=1)
