@@ -172,6 +172,8 @@ def main():
     ap.add_argument("--ref-rows", type=int, default=256)
     ap.add_argument("--full-pairs", action="store_true", help="headline with the full pair set instead of triangular")
     ap.add_argument("--n", type=int, default=N_DIM, help="m = n = k (default 8192; smaller for profiling captures)")
+    ap.add_argument("--memory-only", action="store_true",
+                    help="only the DOT / CSRMV measurements (for profiling them; prints their JSON)")
     args = ap.parse_args()
     globals()["N_DIM"] = args.n
     args.warmup = max(args.warmup, 3)
@@ -189,6 +191,13 @@ def main():
     import ozblas_b200 as ozb
 
     torch.cuda.set_device(local)
+    if args.memory_only:
+        h = ozb.Handle(work_bytes=8 << 30)
+        h.nSplitMax = 0
+        print(json.dumps({"workload": "memory-bound plain kernels", "reps": args.steps,
+                          "extras": memory_extras(ozb, h, torch, reps=args.steps)}))
+        h.close()
+        return 0
     dist = None
     if world > 1:
         import datetime
@@ -359,6 +368,27 @@ def extras(ozb, h, torch, A, B, C, n):
                                                "note": "reference = plain form with NearSum (correctly rounded)"}
     del C_tri, C_full, C_plain
     torch.cuda.empty_cache()
+    out.update(memory_extras(ozb, h, torch))
+    return out
+
+
+def memory_extras(ozb, h, torch, reps=3):
+    """DOT n = 2^24 (phi = 2) and CSRMV on the 128^3 7-point stencil, both sum modes, through the public API."""
+    out = {}
+
+    def timed(fn, reps=1):
+        fn()
+        torch.cuda.synchronize()
+        ts = []
+        for _ in range(reps):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            fn()
+            e1.record()
+            torch.cuda.synchronize()
+            ts.append(e0.elapsed_time(e1))
+        return min(ts)
+
     # DOT n = 2^24, phi = 2
     nv = 1 << 24
     g = torch.Generator(device="cuda").manual_seed(7)
@@ -369,7 +399,7 @@ def extras(ozb, h, torch, A, B, C, n):
     y = (r1 - 0.5) * torch.exp(2.0 * torch.sqrt(-2 * torch.log(r1)) * torch.sin(2 * torch.pi * r2))
     for sm in (0, 1):
         h.sumMode = sm
-        ms = timed(lambda: ozb.ddot(h, nv, x, y), reps=3)
+        ms = timed(lambda: ozb.ddot(h, nv, x, y), reps=reps)
         out[f"ddot_2p24_sum{sm}"] = {"GBps": 16.0 * nv / ms / 1e6, "ms": ms, "slices": [h.nSplitA, h.nSplitB]}
     del x, y, r1, r2
     # CSRMV: 7-point stencil on 128^3, values and x (U - 0.5) exp(N(0,1)), beta = 0
@@ -400,7 +430,7 @@ def extras(ozb, h, torch, A, B, C, n):
     nbytes = 12.0 * nnz + 4.0 * (m + 1) + 8.0 * m + 8.0 * m
     for sm in (0, 1):
         h.sumMode = sm
-        ms = timed(lambda: ozb.dcsrmv(h, "n", m, m, nnz, 1.0, val, colind, rowptr, xv, 0.0, yv), reps=3)
+        ms = timed(lambda: ozb.dcsrmv(h, "n", m, m, nnz, 1.0, val, colind, rowptr, xv, 0.0, yv), reps=reps)
         out[f"dcsrmv_stencil128_sum{sm}"] = {"GBps": nbytes / ms / 1e6, "ms": ms, "nnz": nnz,
                                              "slices": [h.nSplitA, h.nSplitB]}
     h.sumMode = 0

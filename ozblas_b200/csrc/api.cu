@@ -15,11 +15,11 @@ int launch_csrmv_plain(cuozblasHandle_t *h, int m, const double *val, const int 
                        const double *x, double alpha, double beta, double *y);
 int csrmv_presplit(cuozblasHandle_t *h, int m, int n, double alpha, const double *As, int nA, int64_t ld_s,
                    const int *colind, const int *rowptr, const double *x, double beta, double *y);
-int dot_fused(cuozblasHandle_t *h, int n, const double *x, const double *y, double *out_dev, bool *done, int *nA,
+int dot_fused(cuozblasHandle_t *h, int n, const double *x, const double *y, double *ret, bool *done, int *nA,
               int *nB);
 int csrmv_fused(cuozblasHandle_t *h, int m, int n, double alpha, const double *val, const int *colind,
-                const int *rowptr, const double *x, double beta, double *y, int shift, bool *done, int *nA_out,
-                int *nB_out);
+                const int *rowptr, const double *x, double beta, double *y, int shift, int na_hint, bool *done,
+                int *nA_out, int *nB_out);
 
 // CSRMV exec info as the reference records it (src/cpu/ozblas_csrmv.cpp:104-119)
 static void csrmv_info(cuozblasHandle_t *h, int nA, int nB) {
@@ -72,18 +72,18 @@ static int finish(cuozblasHandle_t *h, double t0) {
 // DOT into devWorkCommon[0], result to host.
 static int dot_impl(cuozblasHandle_t *h, int n, const double *x, const double *y, double *ret) {
     State *st = state(h);
-    double *d = reinterpret_cast<double *>(h->devWorkCommon);
-    OZB_CHECK(cudaMemsetAsync(d, 0, sizeof(double), st->stream));
     bool done = false;
     int nA = 0, nB = 0;
-    if (h->splitEpsMode == 0) OZB_TRY(dot_fused(h, n, x, y, d, &done, &nA, &nB));
+    if (h->splitEpsMode == 0) OZB_TRY(dot_fused(h, n, x, y, ret, &done, &nA, &nB));
     if (done) {
         h->nSplitA = (float)nA;
         h->nSplitB = (float)nB;
         h->nSplitC = 1.f;
-    } else {
-        OZB_TRY(gemm_plain_core(h, 't', 'n', 1, 1, n, 1.0, x, n, y, n, 0.0, d, 1, 0));
+        return CUOZBLAS_STATUS_SUCCESS;
     }
+    double *d = reinterpret_cast<double *>(h->devWorkCommon);
+    OZB_CHECK(cudaMemsetAsync(d, 0, sizeof(double), st->stream));
+    OZB_TRY(gemm_plain_core(h, 't', 'n', 1, 1, n, 1.0, x, n, y, n, 0.0, d, 1, 0));
     OZB_CHECK(cudaMemcpyAsync(st->h_dbl, d, sizeof(double), cudaMemcpyDeviceToHost, st->stream));
     OZB_CHECK(cudaStreamSynchronize(st->stream));
     *ret = st->h_dbl[0];
@@ -248,7 +248,7 @@ int cuozblasDcsrmv(cuozblasHandle_t *h, char trans, int32_t m, int32_t n, int32_
     if (h->fastMode == 0 && h->splitEpsMode != 2) {
         bool done = false;
         int fa = 0, fb = 0;
-        OZB_TRY(csrmv_fused(h, m, n, alpha, val, colind, rowptr, x, beta, y, 1, &done, &fa, &fb));
+        OZB_TRY(csrmv_fused(h, m, n, alpha, val, colind, rowptr, x, beta, y, 1, 4, &done, &fa, &fb));
         if (done) {
             csrmv_info(h, fa, fb);
             return finish(h, t0);
@@ -347,7 +347,8 @@ int cuozblasDcg(cuozblasHandle_t *h, char trans, int32_t n, int32_t nnz, const v
             OZB_TRY(counter_init(h));
             bool done = false;
             int fa = 0, fb = 0;
-            OZB_TRY(csrmv_fused(h, n, n, al, val, colind, rowptr, xv, be, yv, cg_shift, &done, &fa, &fb));
+            OZB_TRY(csrmv_fused(h, n, n, al, val, colind, rowptr, xv, be, yv, cg_shift, h->nSplitA_, &done, &fa,
+                                      &fb));
             if (done) return CUOZBLAS_STATUS_SUCCESS;
         }
         return cuozblasDcsrmv(h, trans, n, n, nnz, al, descrA, As, colind, rowptr, xv, be, yv);

@@ -5,243 +5,373 @@
 // sequential fma chain per row (src/cpu/ozblas_blas_wrapper.cpp:231-255) and
 // sums the pair products per row (src/cpu/ozblas_csrmv.cpp:100-160).  Here:
 //
-//  1. max|x| (and the longest row);
-//  2. x's chain is predicted (tau_{s+1} = tau_s + rho - 54) and proven by
-//     per-level flags over all of x (as in dot_fused.cu); if it does not hold,
-//     or x needs more than 8 levels, the caller uses the general path before
-//     anything is written;
+//  1. one pass over x: max, lowest set bit, Inf/NaN (chain.cuh);
+//  2. x's chain is predicted (tau_{s+1} = tau_s + rho - 54) and its slice
+//     count follows from the lowest set bit; a second pass over x proves the
+//     prediction level by level.  If it does not hold, or x needs more than
+//     8 levels, the main kernel writes nothing and the caller runs the
+//     general path;
 //  3. one thread per row: the row's own tau chain (rho from its nnz, sigma
 //     divided by the CG's splitShift) is exact per row, so it is computed in
 //     place; x's slices at the gathered columns come from the proven chain;
 //     every pair product is the CPU's sequential fma chain in storage order,
-//     summed in (ik, ia) order (FSum) or NearSum-ed.  Rows longer than 8 or
-//     needing more than 6 levels are deferred to a per-row general kernel.
+//     summed in (ik, ia) order (FSum) or NearSum-ed.  A block stages its
+//     val/colind range in shared memory with coalesced loads and issues all
+//     gathers of x before using them.  Rows longer than 8 or needing more
+//     levels than the kernel holds are deferred to a per-row general kernel.
 //
 // Pairs whose A slice is beyond a row's own exact split are zero slices in
 // the reference; they add +0 to the ordered sum and nothing to NearSum, so
 // skipping them leaves the bits unchanged.  fastMode must be 0 (the caller
 // uses the general path otherwise).
-#include "ozb_device.cuh"
+#include "chain.cuh"
 #include "ozb_internal.h"
 #include "sum.cuh"
 
 namespace ozb {
 
-constexpr int kCsrLv = 8;           // levels of x computed / checked
-constexpr int kCsrRowMax = 8;       // entries per row held on chip
-constexpr int kCsrAlv = 6;          // levels of a row held on chip
+constexpr int kCsrLv = kChainLevels;  // levels of x computed / proven
+constexpr int kCsrRowMax = 8;         // entries per row held on chip
 constexpr int kCsrThreads = 128;
 
 struct CsrScratch {
-    double xmax;
-    unsigned int nz, hi;
-    int valid, nB, maxlen, nslow, zmax;  // zmax: first zero-remainder level, max over rows
-    double sigma[kCsrLv];
+    VecStats vs;             // first pass over x
+    unsigned proven;         // levels of x's chain whose predicted tau some element proved
+    unsigned ticket;         // blocks of the proof pass that are done
+    int valid, nB, nslow, zmax;  // zmax: first zero-remainder level of A, max over rows
+    double sigma[kCsrLv];    // x's proven sigmas
 };
 
-__global__ void __launch_bounds__(256) k_csr_prep(int m, int n, const double *__restrict__ x,
-                                                  const int *__restrict__ rowptr, CsrScratch *sc) {
+template <bool ALIGNED>
+__global__ void __launch_bounds__(256) k_csr_scan(int n, const double *__restrict__ x, CsrScratch *sc) {
     __shared__ double red[8];
-    const size_t stride = (size_t)gridDim.x * blockDim.x;
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
     double mx = 0.0;
-    int ml = 0;
-    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < (size_t)n; i += stride)
-        mx = ref_max(mx, fabs(x[i]));
-    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < (size_t)m; i += stride) {
-        const int l = rowptr[i + 1] - rowptr[i];
-        ml = ml > l ? ml : l;
-    }
-    mx = block_max_nonneg(mx, red);
-    for (int o = 16; o > 0; o >>= 1) {
-        const int t = __shfl_xor_sync(0xffffffffu, ml, o);
-        ml = ml > t ? ml : t;
-    }
-    if (threadIdx.x == 0) atomic_max_nonneg(&sc->xmax, mx);
-    if ((threadIdx.x & 31) == 0) atomicMax(&sc->maxlen, ml);
-}
-
-__device__ __forceinline__ double csr_tau_threshold(int t) {
-    const int e = t - 1;
-    if (e < -1022 || e > 1023) return -1.0;
-    const int ae = e < 0 ? -e : e;
-    int p = (ae == 0) ? -1 : (31 - clz32((uint32_t)ae));
-    if (e < 0 && (ae & (ae - 1)) == 0) p -= 1;
-    int J;
-    switch (p) {
-        case 2: J = 1; break;
-        case 3: J = 2; break;
-        case 4: J = 5; break;
-        case 5: J = 11; break;
-        case 6: J = 22; break;
-        case 7: J = 44; break;
-        case 8: J = 88; break;
-        case 9: J = 177; break;
-        case 10: J = 354; break;
-        default: J = 0; break;
-    }
-    return from_bits(dbits(pow2(e)) + (uint64_t)J);
-}
-
-// Per-level flags of x's predicted chain.
-__global__ void __launch_bounds__(256) k_vec_chain_flags(int n, const double *__restrict__ x, int rho,
-                                                         CsrScratch *sc) {
-    __shared__ double sig[kCsrLv], thr[kCsrLv];
-    if (threadIdx.x == 0) {
-        int tau = tau_rule(sc->xmax);
-        for (int s = 0; s < kCsrLv; s++) {
-            sig[s] = 0.75 * pow2(rho + tau);
-            tau = tau + rho - 54;
-            thr[s] = csr_tau_threshold(tau);
+    int lx = 0, bx = 0;
+    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (ALIGNED) {
+        const int64_t np = (int64_t)n >> 1;
+        const double2 *x2 = reinterpret_cast<const double2 *>(x);
+        for (; i < np; i += stride) {
+            const double2 a = x2[i];
+            scan_elem(a.x, mx, lx, bx);
+            scan_elem(a.y, mx, lx, bx);
         }
-    }
-    __syncthreads();
-    unsigned nz = 0, hi = 0;
-    const size_t stride = (size_t)gridDim.x * blockDim.x;
-    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < (size_t)n; i += stride) {
-        double r = x[i];
-#pragma unroll
-        for (int s = 0; s < kCsrLv; s++) {
-            const double sl = (r + sig[s]) - sig[s];
-            r = r - sl;
-            const uint64_t rb = dbits(r) & 0x7fffffffffffffffULL;
-            nz |= (rb != 0) ? (1u << s) : 0u;
-            hi |= (rb > dbits(thr[s])) ? (1u << s) : 0u;
-        }
-    }
-    for (int o = 16; o > 0; o >>= 1) {
-        nz |= __shfl_xor_sync(0xffffffffu, nz, o);
-        hi |= __shfl_xor_sync(0xffffffffu, hi, o);
-    }
-    if ((threadIdx.x & 31) == 0) {
-        atomicOr(&sc->nz, nz);
-        atomicOr(&sc->hi, hi);
-    }
-}
-
-__global__ void k_vec_chain_finish(CsrScratch *sc, int rho, int maxS) {
-    if (threadIdx.x != 0 || blockIdx.x != 0) return;
-    int tau = tau_rule(sc->xmax);
-    double thr[kCsrLv];
-    for (int s = 0; s < kCsrLv; s++) {
-        sc->sigma[s] = 0.75 * pow2(rho + tau);
-        tau = tau + rho - 54;
-        thr[s] = csr_tau_threshold(tau);
-    }
-    const unsigned nz = sc->nz, hi = sc->hi;
-    int z = kCsrLv;
-    for (int s = 0; s < kCsrLv; s++)
-        if (!(nz & (1u << s))) {
-            z = s;
-            break;
-        }
-    int ns;
-    bool ok = true;
-    if (z >= kCsrLv) {
-        if (maxS > kCsrLv) ok = false;
-        ns = maxS;
+        if ((n & 1) && blockIdx.x == 0 && threadIdx.x == 0) scan_elem(x[n - 1], mx, lx, bx);
     } else {
-        ns = (z < 1 ? 1 : z) + 1;
-        if (ns > maxS) ns = maxS;
+        for (; i < n; i += stride) scan_elem(x[i], mx, lx, bx);
     }
-    for (int s = 0; ok && s + 1 < ns; s++)
-        if ((nz & (1u << s)) && (!(hi & (1u << s)) || thr[s] < 0.0)) ok = false;
-    sc->nB = ns;
-    sc->valid = ok ? 1 : 0;
+    scan_commit(&sc->vs, 0, mx, lx, bx, red);
 }
 
-// One thread per row; per-thread slices in shared memory laid out
-// [index][thread] so a warp's accesses hit distinct banks.
-template <int SUM_MODE>
-__global__ void __launch_bounds__(kCsrThreads) k_csrmv_fast(int m, const double *__restrict__ val,
-                                                            const int *__restrict__ colind,
-                                                            const int *__restrict__ rowptr,
-                                                            const double *__restrict__ x, int shift, int epsmode,
-                                                            int maxS, double alpha, double beta,
-                                                            double *__restrict__ y, CsrScratch *__restrict__ sc,
-                                                            int *__restrict__ slow_rows) {
-    extern __shared__ double sh[];
-    __shared__ double xs_sigma[kCsrLv];
-    if (!sc->valid) return;
-    const int nB = sc->nB;
-    if (threadIdx.x < kCsrLv) xs_sigma[threadIdx.x] = sc->sigma[threadIdx.x];
+template <int G, int T>
+__device__ __forceinline__ unsigned proof_body(double v, const TreePlan &pl) {
+    double q[T + 1];
+    cut_tree<G, T>(v, pl.sig[0], q);
+    unsigned hw[kCsrLv];
+#pragma unroll
+    for (int s = 0; s < T; s++) hw[s] = abs_hiword(q[s + 1]);
+    return prove_levels<T>(hw, pl.hb[0], pl.need[0]);
+}
+
+// Proof of x's predicted chain: one element per thread; the last block
+// publishes validity, slice count and sigmas.
+template <int G>
+__global__ void __launch_bounds__(256) k_csr_proof(int n, const double *__restrict__ x, int rho, int maxS,
+                                                   CsrScratch *sc) {
+    __shared__ TreePlan pl;
+    __shared__ int last;
+    const int t = threadIdx.x;
+    if (t == 0) make_plan(&sc->vs, rho, maxS, true, pl);
     __syncthreads();
-    const int row = blockIdx.x * blockDim.x + threadIdx.x;
-    if (row >= m) return;
-    const int T = blockDim.x, t = threadIdx.x;
-    double *A = sh;                                  // [kCsrAlv * kCsrRowMax][T]
-    double *X = sh + kCsrAlv * kCsrRowMax * T;      // [kCsrLv * kCsrRowMax][T]
-    double *Tm = X + kCsrLv * kCsrRowMax * T;       // [kCsrAlv * kCsrLv][T] (NearSum terms)
-    const int lo = rowptr[row], len = rowptr[row + 1] - lo;
-    if (len > kCsrRowMax) {
-        slow_rows[atomicAdd(&sc->nslow, 1)] = row;
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + t;
+    if (pl.valid && pl.need[0]) {  // uniform
+        const double v = i < n ? x[i] : 0.0;
+        int T = plan_depth(pl, 0, __reduce_min_sync(0xffffffffu, exp_key(v)));
+        if (T > pl.L - 1) T = pl.L - 1;
+        unsigned got = 0u;
+        switch (T) {
+            case 0: break;
+            case 1: got = proof_body<G, 1>(v, pl); break;
+            case 2: got = proof_body<G, 2>(v, pl); break;
+            case 3: got = proof_body<G, 3>(v, pl); break;
+            case 4: got = proof_body<G, 4>(v, pl); break;
+            case 5: got = proof_body<G, 5>(v, pl); break;
+            case 6: got = proof_body<G, 6>(v, pl); break;
+            default: got = proof_body<G, 7>(v, pl); break;
+        }
+        if ((t & 31) == 0 && got) atomicOr(&sc->proven, got);
+    }
+    __threadfence();
+    __syncthreads();
+    if (t == 0) last = atomicAdd(&sc->ticket, 1u) == gridDim.x - 1;
+    __syncthreads();
+    if (!last || t != 0) return;
+    __threadfence();
+    const int valid = pl.valid && (__ldcg(&sc->proven) & pl.need[0]) == pl.need[0];
+    for (int s = 0; s < kCsrLv; s++) sc->sigma[s] = pl.sig[0][s];
+    sc->nB = pl.ns[0];
+    sc->valid = valid;
+}
+
+// Visit the pairs (ia < na, ib < nb) of a row in summation order: ik
+// ascending, ia ascending (compile-time indices, so P stays in registers).
+template <int NA, typename F>
+__device__ __forceinline__ void for_row_pairs(int na, int nb, F f) {
+#pragma unroll
+    for (int ik = 0; ik < NA + kCsrLv - 1; ik++)
+#pragma unroll
+        for (int ia = 0; ia < NA; ia++) {
+            const int ib = ik - ia;
+            if (ib >= 0 && ib < kCsrLv)
+                if (ia < na && ib < nb) f(ia, ib);
+        }
+}
+
+// NearSum (src/cpu/ozblas_sum.cpp:10-112, as in sum.cuh) over the row's pair
+// products held in registers; same term order as sum.cuh's callers.
+template <int NA>
+__device__ __forceinline__ void ns_transform_row(double (&v)[NA][kCsrLv], int na, int nb, int n, double rho,
+                                                 double &tau1, double &tau2) {
+    const int emin = -1022, epse = 53;
+    double mu = 0.0;
+    for_row_pairs<NA>(na, nb, [&](int a, int b) {
+        const double t = fabs(v[a][b]);
+        mu = (mu > t) ? mu : t;
+    });
+    if (n == 0 || mu == 0.) {
+        tau1 = rho;
+        tau2 = 0.;
         return;
     }
-    double r[kCsrRowMax];
-    int c[kCsrRowMax];
-    double mx = 0.0;
-#pragma unroll
-    for (int e = 0; e < kCsrRowMax; e++) {
-        r[e] = e < len ? val[lo + e] : 0.0;
-        c[e] = e < len ? colind[lo + e] : 0;
-        mx = ref_max(mx, fabs(r[e]));
-    }
-    // the row's own split (src/cpu/ozblas_split.cpp:779-815, sigma / shift)
-    int na = 0, z = 0;
-    if (len > 0) {
-        const int rho = rho_rule(len, epsmode);
-        z = maxS;
-        for (int s = 0; s < kCsrAlv && s < maxS; s++) {
-            const double sigma = 0.75 * pow2(rho + tau_rule(mx)) / (double)shift;
-            double nm = 0.0;
-#pragma unroll
-            for (int e = 0; e < kCsrRowMax; e++) {
-                const double sl = (r[e] + sigma) - sigma;
-                r[e] = r[e] - sl;
-                A[(s * kCsrRowMax + e) * T + t] = sl;
-                nm = ref_max(nm, fabs(r[e]));
-            }
-            na = s + 1;
-            mx = nm;
-            if (nm == 0.0) {
-                z = s;
-                break;
-            }
-        }
-        if (mx != 0.0 && na < maxS) {  // needs more levels than held on chip
-            slow_rows[atomicAdd(&sc->nslow, 1)] = row;
+    const int M = ceil_log2_int((uint32_t)(n + 2));
+    double sigma = pow2(M + tau_rule(mu));
+    double t = rho;
+    for (;;) {
+        double tau = 0.;
+        for_row_pairs<NA>(na, nb, [&](int a, int b) {
+            const double tmp = (sigma + v[a][b]) - sigma;
+            v[a][b] -= tmp;
+            tau += tmp;
+        });
+        tau1 = t + tau;
+        if ((sigma <= pow2(emin)) || (fabs(tau1) >= pow2(2 * M + 1 - epse) * sigma)) {
+            tau2 = tau - (tau1 - t);
             return;
         }
+        sigma = pow2(M - epse) * sigma;
+        t = tau1;
     }
-    atomicMax(&sc->zmax, z);
-    // x's slices at this row's columns
+}
+
+template <int NA>
+__device__ __forceinline__ void ns_transformk_row(double (&v)[NA][kCsrLv], int na, int nb, int n, double rho,
+                                                  double &res, double &r) {
+    double tmp = 0., tau1, tau2;
+    ns_transform_row<NA>(v, na, nb, n, rho, tau1, tau2);
+    for_row_pairs<NA>(na, nb, [&](int a, int b) { tmp += v[a][b]; });
+    res = tau1 + (tau2 + tmp);
+    r = tau2 - (res - tau1);
+}
+
+template <int NA>
+__device__ __forceinline__ double nearsum_row(double (&v)[NA][kCsrLv], int na, int nb) {
+    const int n = na * nb;
+    const double eps = pow2(-53);
+    double res, r, delta, r2, res2, mu, delta2, tmp;
+    ns_transformk_row<NA>(v, na, nb, n, 0., res, r);
+    ns_transformk_row<NA>(v, na, nb, n, r, delta, r2);
+    if (delta == 0) return res;
+    res2 = res + sign1(delta) * eps * fabs(res);
+    if (res2 == res) {
+        mu = sign1(delta) * eps * fabs(res);
+        res2 = res + 2. * sign1(delta) * eps * fabs(res);
+    } else {
+        mu = (res2 - res) / 2.;
+    }
+    if (fabs(delta) < fabs(mu)) return res;
+    if (fabs(delta) > fabs(mu)) return res2;
+    ns_transformk_row<NA>(v, na, nb, n, r2, delta2, tmp);
+    if (delta2 == 0) return res + mu;
+    if (sign1(delta2) == sign1(mu)) return res2;
+    return res;
+}
+
+// One thread per row, everything in registers.  A block's val/colind range
+// is staged in shared memory with coalesced loads; each row's tau chain runs
+// over its (at most kCsrRowMax) entries, keeping only the sigmas, then every
+// entry is re-cut with them while x's slices at its column come from the
+// proven chain; the pair products P[ia][ib] are the CPU's sequential fma
+// chains in storage order.  Rows with more entries, or needing more than NA
+// levels, go to the slow list.
+template <int NA, int NB, int GX>
+__device__ __forceinline__ void row_products(const double (&a)[kCsrRowMax], const double (&xv)[kCsrRowMax], int len,
+                                             int na, const double (&sigA)[NA], const double *xsig,
+                                             double (&P)[NA][kCsrLv]) {
 #pragma unroll
     for (int e = 0; e < kCsrRowMax; e++) {
-        double xr = e < len ? x[c[e]] : 0.0;
-        for (int s = 0; s < nB; s++) {
-            const double sl = (xr + xs_sigma[s]) - xs_sigma[s];
-            xr = xr - sl;
-            X[(s * kCsrRowMax + e) * T + t] = sl;
+        if (e < len) {
+            double sa[NA];
+            double r = a[e];
+#pragma unroll
+            for (int s = 0; s < NA; s++) {
+                sa[s] = 0.0;
+                if (s < na) {
+                    const double sl = (r + sigA[s]) - sigA[s];
+                    r = r - sl;
+                    sa[s] = sl;
+                }
+            }
+            double sx[NB];
+            cut_tree<GX, NB - 1>(xv[e], xsig, sx);
+#pragma unroll
+            for (int ia = 0; ia < NA; ia++)
+                if (ia < na)
+#pragma unroll
+                    for (int ib = 0; ib < NB; ib++) P[ia][ib] = fma(sa[ia], sx[ib], P[ia][ib]);
         }
+    }
+}
+
+template <int SUM_MODE, int NA, int GX>
+__global__ void __launch_bounds__(kCsrThreads) k_csrmv_reg(int m, int n, const double *__restrict__ val,
+                                                           const int *__restrict__ colind,
+                                                           const int *__restrict__ rowptr,
+                                                           const double *__restrict__ x, int shift, int epsmode,
+                                                           int maxS, double alpha, double beta,
+                                                           double *__restrict__ y, CsrScratch *__restrict__ sc,
+                                                           int *__restrict__ slow_rows) {
+    constexpr int kStage = kCsrThreads * kCsrRowMax;
+    __shared__ double s_val[kStage];
+    __shared__ int s_col[kStage];
+    __shared__ int s_rp[kCsrThreads + 1];
+    __shared__ double xs_sigma[kCsrLv];
+    const int t = threadIdx.x;
+    const int r0 = blockIdx.x * kCsrThreads;
+    const int nrow = (m - r0 < kCsrThreads) ? m - r0 : kCsrThreads;
+    const int row = r0 + t;
+    const bool active = t < nrow;
+    // independent loads first: the block's row pointers and the old y
+    // (beta * y is formed even for beta = 0, as the reference does)
+    if (active) s_rp[t] = rowptr[r0 + t];
+    if (t == 0) s_rp[nrow] = rowptr[r0 + nrow];
+    const double yold = active ? y[row] : 0.0;
+    if (t < kCsrLv) xs_sigma[t] = sc->sigma[t];
+    const int valid = sc->valid;
+    const int nB = sc->nB;
+    __syncthreads();
+    if (!valid) return;  // uniform: the caller runs the general path
+    const int p0 = s_rp[0], p1 = s_rp[nrow];
+    const bool staged = (p1 - p0) <= kStage;
+    if (staged) {
+        const int cnt = p1 - p0;
+#pragma unroll 4
+        for (int i = t; i < cnt; i += kCsrThreads) {
+            s_val[i] = val[p0 + i];
+            s_col[i] = colind[p0 + i];
+        }
+    }
+    __syncthreads();
+    int lo = p0, len = 0;
+    if (active) {
+        lo = s_rp[t];
+        len = s_rp[t + 1] - lo;
+    }
+    bool defer = active && len > kCsrRowMax;
+    const bool work = active && !defer;
+    double a[kCsrRowMax], xv[kCsrRowMax];
+    int c[kCsrRowMax];
+#pragma unroll
+    for (int e = 0; e < kCsrRowMax; e++) {
+        const bool in = work && e < len;
+        double v = 0.0;
+        int ci = 0;
+        if (staged) {
+            const int idx = min(lo - p0 + e, kStage - 1);
+            v = s_val[idx];
+            ci = s_col[idx];
+        } else if (in) {
+            v = val[lo + e];
+            ci = colind[lo + e];
+        }
+        a[e] = in ? v : 0.0;
+        c[e] = in ? ci : -1;
+    }
+    if (n > 0) {  // all gathers in flight before any is used
+#pragma unroll
+        for (int e = 0; e < kCsrRowMax; e++) {
+            const double tx = x[c[e] >= 0 ? c[e] : 0];
+            xv[e] = c[e] >= 0 ? tx : 0.0;
+        }
+    } else {
+#pragma unroll
+        for (int e = 0; e < kCsrRowMax; e++) xv[e] = 0.0;
+    }
+    // the row's own chain (src/cpu/ozblas_split.cpp:779-815, sigma / shift)
+    double sigA[NA];
+    int na = 0, z = 0;
+#pragma unroll
+    for (int s = 0; s < NA; s++) sigA[s] = 0.0;
+    if (work && len > 0) {
+        const int rho = rho_rule(len, epsmode);
+        double rr[kCsrRowMax];
+        double mx = 0.0;
+#pragma unroll
+        for (int e = 0; e < kCsrRowMax; e++) {
+            rr[e] = a[e];
+            mx = ref_max(mx, fabs(a[e]));
+        }
+        z = maxS;
+        bool fin = false;
+#pragma unroll
+        for (int s = 0; s < NA; s++) {
+            if (!fin && s < maxS) {
+                const double sg = shift_sigma(0.75 * pow2(rho + tau_rule(mx)), shift);
+                sigA[s] = sg;
+                double nm = 0.0;
+#pragma unroll
+                for (int e = 0; e < kCsrRowMax; e++) {
+                    const double sl = (rr[e] + sg) - sg;
+                    rr[e] = rr[e] - sl;
+                    nm = ref_max(nm, fabs(rr[e]));
+                }
+                na = s + 1;
+                mx = nm;
+                if (nm == 0.0) {
+                    z = s;
+                    fin = true;
+                }
+            }
+        }
+        if (mx != 0.0 && na < maxS) defer = true;  // needs more levels than NA
+    }
+    if (defer) slow_rows[atomicAdd(&sc->nslow, 1)] = row;
+    {
+        const int zw = __reduce_max_sync(0xffffffffu, (work && !defer) ? z : 0);
+        if ((t & 31) == 0 && zw > 0) atomicMax(&sc->zmax, zw);
+    }
+    if (!work || defer) return;
+    double P[NA][kCsrLv];
+#pragma unroll
+    for (int i = 0; i < NA; i++)
+#pragma unroll
+        for (int j = 0; j < kCsrLv; j++) P[i][j] = 0.0;
+    switch (nB) {  // uniform
+        case 1: row_products<NA, 1, GX>(a, xv, len, na, sigA, xs_sigma, P); break;
+        case 2: row_products<NA, 2, GX>(a, xv, len, na, sigA, xs_sigma, P); break;
+        case 3: row_products<NA, 3, GX>(a, xv, len, na, sigA, xs_sigma, P); break;
+        case 4: row_products<NA, 4, GX>(a, xv, len, na, sigA, xs_sigma, P); break;
+        case 5: row_products<NA, 5, GX>(a, xv, len, na, sigA, xs_sigma, P); break;
+        case 6: row_products<NA, 6, GX>(a, xv, len, na, sigA, xs_sigma, P); break;
+        case 7: row_products<NA, 7, GX>(a, xv, len, na, sigA, xs_sigma, P); break;
+        default: row_products<NA, 8, GX>(a, xv, len, na, sigA, xs_sigma, P); break;
     }
     double tsum = 0.0;
-    int np = 0;
-    const int maxlevel = na + nB - 2;
-    for (int ik = 0; ik <= maxlevel; ik++) {
-        const int ia0 = ik - (nB - 1) > 0 ? ik - (nB - 1) : 0, ia1 = ik < na - 1 ? ik : na - 1;
-        for (int ia = ia0; ia <= ia1; ia++) {
-            const int ib = ik - ia;
-            double p = 0.0;
-            for (int e = 0; e < len; e++)
-                p = fma(A[(ia * kCsrRowMax + e) * T + t], X[(ib * kCsrRowMax + e) * T + t], p);
-            if (SUM_MODE == 1)
-                Tm[np * T + t] = p;
-            else
-                tsum += p;
-            np++;
-        }
-    }
-    if (SUM_MODE == 1) tsum = nearsum(np, Tm + t, T);
-    y[row] = fma(alpha, tsum, beta * y[row]);
+    if (SUM_MODE == 1)
+        tsum = nearsum_row<NA>(P, na, nB);
+    else
+        for_row_pairs<NA>(na, nB, [&](int ia, int ib) { tsum += P[ia][ib]; });
+    y[row] = fma(alpha, tsum, beta * yold);
 }
 
 // Recompute slice `lv` of v from scratch along the chain sig[0..lv].
@@ -276,7 +406,7 @@ __global__ void __launch_bounds__(128) k_csrmv_slow(int nrows, const int *__rest
         double mx = 0.0;
         for (int i = lo; i < hi; i++) mx = ref_max(mx, fabs(val[i]));
         for (int s = 0; s < maxS; s++) {
-            sa[s] = 0.75 * pow2(rho + tau_rule(mx)) / (double)shift;
+            sa[s] = shift_sigma(0.75 * pow2(rho + tau_rule(mx)), shift);
             na = s + 1;
             double nm = 0.0;
             for (int i = lo; i < hi; i++) {
@@ -317,11 +447,28 @@ __global__ void __launch_bounds__(128) k_csrmv_slow(int nrows, const int *__rest
     y[row] = fma(alpha, tsum, beta * y[row]);
 }
 
+template <int SUM_MODE, int NA>
+static void launch_reg(int gx, int rb, cudaStream_t s, int m, int n, const double *val, const int *colind,
+                       const int *rowptr, const double *x, int shift, int epsmode, int maxS, double alpha, double beta,
+                       double *y, CsrScratch *sc, int *slow) {
+    if (gx >= 3)
+        k_csrmv_reg<SUM_MODE, NA, 3><<<rb, kCsrThreads, 0, s>>>(m, n, val, colind, rowptr, x, shift, epsmode, maxS,
+                                                                 alpha, beta, y, sc, slow);
+    else if (gx == 2)
+        k_csrmv_reg<SUM_MODE, NA, 2><<<rb, kCsrThreads, 0, s>>>(m, n, val, colind, rowptr, x, shift, epsmode, maxS,
+                                                                 alpha, beta, y, sc, slow);
+    else
+        k_csrmv_reg<SUM_MODE, NA, 1><<<rb, kCsrThreads, 0, s>>>(m, n, val, colind, rowptr, x, shift, epsmode, maxS,
+                                                                 alpha, beta, y, sc, slow);
+}
+
 // Fused CSRMV.  *done = false (and y untouched) when x's chain is not proven
 // or needs more than 8 levels: the caller then runs the general path.
+// `na_hint` (levels of the rows, when the caller knows them) selects how many
+// levels per row the main kernel holds.
 int csrmv_fused(cuozblasHandle_t *h, int m, int n, double alpha, const double *val, const int *colind,
-                const int *rowptr, const double *x, double beta, double *y, int shift, bool *done, int *nA_out,
-                int *nB_out) {
+                const int *rowptr, const double *x, double beta, double *y, int shift, int na_hint, bool *done,
+                int *nA_out, int *nB_out) {
     State *st = state(h);
     *done = false;
     Arena ar(h);
@@ -331,47 +478,54 @@ int csrmv_fused(cuozblasHandle_t *h, int m, int n, double alpha, const double *v
     if (!ar.ok) return CUOZBLAS_STATUS_WORKSPACE;
     const int maxS = h->nSplitMax > 0 ? h->nSplitMax : kMaxSplitDefault;
     const int rho = rho_rule(n, h->splitEpsMode);
-    OZB_CHECK(cudaMemsetAsync(sc, 0, sizeof(CsrScratch), st->stream));
+    const int gx = chain_group(rho, 3);
+    cudaStream_t s = st->stream;
+    OZB_CHECK(cudaMemsetAsync(sc, 0, sizeof(CsrScratch), s));
     int dev = 0, nsm = 0;
     OZB_CHECK(cudaGetDevice(&dev));
     OZB_CHECK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
-    const int64_t span = m > n ? m : n;
-    int blocks = (int)((span + 255) / 256);
+    int blocks = (int)(((int64_t)n + 511) / 512);
     if (blocks > nsm * 8) blocks = nsm * 8;
     if (blocks < 1) blocks = 1;
     counted(h);
-    k_csr_prep<<<blocks, 256, 0, st->stream>>>(m, n, x, rowptr, sc);
-    int fb = (int)(((int64_t)n + 255) / 256);
-    if (fb > nsm * 8) fb = nsm * 8;
-    if (fb < 1) fb = 1;
+    if ((reinterpret_cast<uintptr_t>(x) & 15u) == 0)
+        k_csr_scan<true><<<blocks, 256, 0, s>>>(n, x, sc);
+    else
+        k_csr_scan<false><<<blocks, 256, 0, s>>>(n, x, sc);
+    const int pb = (int)(((int64_t)n + 255) / 256) > 0 ? (int)(((int64_t)n + 255) / 256) : 1;
     counted(h);
-    k_vec_chain_flags<<<fb, 256, 0, st->stream>>>(n, x, rho, sc);
-    counted(h);
-    k_vec_chain_finish<<<1, 32, 0, st->stream>>>(sc, rho, maxS);
-    const size_t sm_fsum = sizeof(double) * (kCsrAlv + kCsrLv) * kCsrRowMax * kCsrThreads;
-    const size_t sm_near = sm_fsum + sizeof(double) * kCsrAlv * kCsrLv * kCsrThreads;
+    if (gx >= 3)
+        k_csr_proof<3><<<pb, 256, 0, s>>>(n, x, rho, maxS, sc);
+    else if (gx == 2)
+        k_csr_proof<2><<<pb, 256, 0, s>>>(n, x, rho, maxS, sc);
+    else
+        k_csr_proof<1><<<pb, 256, 0, s>>>(n, x, rho, maxS, sc);
     const int rb = (m + kCsrThreads - 1) / kCsrThreads;
     if (m > 0) {
         counted(h);
+        const bool deep = na_hint > 4;
+        const int em = h->splitEpsMode;
         if (h->sumMode == 1) {
-            OZB_CHECK(cudaFuncSetAttribute(k_csrmv_fast<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_near));
-            k_csrmv_fast<1><<<rb, kCsrThreads, sm_near, st->stream>>>(m, val, colind, rowptr, x, shift,
-                                                                       h->splitEpsMode, maxS, alpha, beta, y, sc, slow);
+            if (deep)
+                launch_reg<1, 6>(gx, rb, s, m, n, val, colind, rowptr, x, shift, em, maxS, alpha, beta, y, sc, slow);
+            else
+                launch_reg<1, 4>(gx, rb, s, m, n, val, colind, rowptr, x, shift, em, maxS, alpha, beta, y, sc, slow);
         } else {
-            OZB_CHECK(cudaFuncSetAttribute(k_csrmv_fast<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_fsum));
-            k_csrmv_fast<0><<<rb, kCsrThreads, sm_fsum, st->stream>>>(m, val, colind, rowptr, x, shift,
-                                                                       h->splitEpsMode, maxS, alpha, beta, y, sc, slow);
+            if (deep)
+                launch_reg<0, 6>(gx, rb, s, m, n, val, colind, rowptr, x, shift, em, maxS, alpha, beta, y, sc, slow);
+            else
+                launch_reg<0, 4>(gx, rb, s, m, n, val, colind, rowptr, x, shift, em, maxS, alpha, beta, y, sc, slow);
         }
     }
     OZB_CHECK(cudaGetLastError());
-    int res[5];  // valid, nB, maxlen, nslow, zmax (partial until the deferred rows ran)
-    OZB_CHECK(cudaMemcpyAsync(res, &sc->valid, sizeof(res), cudaMemcpyDeviceToHost, st->stream));
-    OZB_CHECK(cudaStreamSynchronize(st->stream));
+    int res[4];  // valid, nB, nslow, zmax (partial until the deferred rows ran)
+    OZB_CHECK(cudaMemcpyAsync(res, &sc->valid, sizeof(res), cudaMemcpyDeviceToHost, s));
+    OZB_CHECK(cudaStreamSynchronize(s));
     if (!res[0]) {
         ar.release(mk);
         return CUOZBLAS_STATUS_SUCCESS;  // y untouched: general path
     }
-    const int nslow = res[3];
+    const int nslow = res[2];
     if (nslow > 0) {
         const int chunk = 8192;
         double *terms = ar.take<double>((uint64_t)chunk * kMaxSplitDefault * kCsrLv);
@@ -380,24 +534,20 @@ int csrmv_fused(cuozblasHandle_t *h, int m, int n, double alpha, const double *v
             const int nr = nslow - c0 < chunk ? nslow - c0 : chunk;
             counted(h);
             if (h->sumMode == 1)
-                k_csrmv_slow<1><<<(nr + 127) / 128, 128, 0, st->stream>>>(nr, slow + c0, val, colind, rowptr, x,
-                                                                          shift, h->splitEpsMode, maxS, alpha, beta,
-                                                                          y, sc, terms);
+                k_csrmv_slow<1><<<(nr + 127) / 128, 128, 0, s>>>(nr, slow + c0, val, colind, rowptr, x, shift,
+                                                                h->splitEpsMode, maxS, alpha, beta, y, sc, terms);
             else
-                k_csrmv_slow<0><<<(nr + 127) / 128, 128, 0, st->stream>>>(nr, slow + c0, val, colind, rowptr, x,
-                                                                          shift, h->splitEpsMode, maxS, alpha, beta,
-                                                                          y, sc, terms);
+                k_csrmv_slow<0><<<(nr + 127) / 128, 128, 0, s>>>(nr, slow + c0, val, colind, rowptr, x, shift,
+                                                                h->splitEpsMode, maxS, alpha, beta, y, sc, terms);
             OZB_CHECK(cudaGetLastError());
         }
-    }
-    if (nslow > 0) {
-        OZB_CHECK(cudaMemcpyAsync(&res[4], &sc->zmax, sizeof(int), cudaMemcpyDeviceToHost, st->stream));
-        OZB_CHECK(cudaStreamSynchronize(st->stream));
+        OZB_CHECK(cudaMemcpyAsync(&res[3], &sc->zmax, sizeof(int), cudaMemcpyDeviceToHost, s));
+        OZB_CHECK(cudaStreamSynchronize(s));
     }
     ar.release(mk);
     *done = true;
     *nB_out = res[1];
-    const int c = (res[4] < 1 ? 1 : res[4]) + 1;  // count rule, src/cpu/ozblas_split.cpp:272-289
+    const int c = (res[3] < 1 ? 1 : res[3]) + 1;  // count rule, src/cpu/ozblas_split.cpp:272-289
     *nA_out = m > 0 ? (c < maxS ? c : maxS) : (maxS < 2 ? maxS : 2);
     return CUOZBLAS_STATUS_SUCCESS;
 }

@@ -16,6 +16,15 @@ __device__ __forceinline__ double dense_sigma(int rho, double mx, int shift) {
     return 0.75 * pow2(rho + tau_rule(mx)) * (double)shift;
 }
 
+// sigma / splitShift for the sparse split (src/cpu/ozblas_split.cpp:809).
+// The tuned shift is a power of two, and dividing by 2^k is the same
+// correctly rounded scaling as multiplying by 2^-k, so no division is issued;
+// any other shift divides.
+__device__ __forceinline__ double shift_sigma(double s, int shift) {
+    if ((shift & (shift - 1)) == 0 && shift > 0) return s * pow2(-(31 - __clz(shift)));
+    return s / (double)shift;
+}
+
 // Block-wide max of non-negative doubles; every thread gets the result.
 // `red` must hold one double per warp.
 __device__ __forceinline__ double block_max_nonneg(double v, double *red) {
@@ -32,6 +41,18 @@ __device__ __forceinline__ double block_max_nonneg(double v, double *red) {
 // Non-negative doubles order like their bit patterns: atomicMax on the bits.
 __device__ __forceinline__ void atomic_max_nonneg(double *addr, double v) {
     atomicMax(reinterpret_cast<unsigned long long *>(addr), (unsigned long long)__double_as_longlong(v));
+}
+
+// 16-byte asynchronous global -> shared copy (zero fill when !pred).
+__device__ __forceinline__ void cp_async16(void *smem, const void *gmem, bool pred) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    const int sz = pred ? 16 : 0;
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(s), "l"(gmem), "r"(sz));
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+    asm volatile("cp.async.wait_group %0;\n" ::"n"(N));
 }
 
 }  // namespace ozb

@@ -43,15 +43,27 @@ OZB_HD int clz32(uint32_t x) {
 // ceil(log2(d)) for an integer d >= 1, exactly.
 OZB_HD int ceil_log2_int(uint32_t d) { return d <= 1 ? 0 : 32 - clz32(d - 1u); }
 
+// The tau rule's threshold for exponent e: floor(ln2 * 2^(p-1)), p the bit
+// length of |e| minus one (one less again just above -2^q, where the spacing
+// of doubles halves).  It is a shift of floor(ln2 * 2^40) = 762123384785
+// (the floor of a floor is the floor), so there is no table and no branch:
+// the values are 1, 2, 5, 11, 22, 44, 88, 177, 354 for p = 2..10 and 0 below.
+OZB_HD int64_t tau_threshold(int e) {
+    const int ae = e < 0 ? -e : e;
+    int p = (ae == 0) ? -1 : (31 - clz32((uint32_t)ae));
+    if (e < 0 && (ae & (ae - 1)) == 0) p -= 1;  // just above -2^q the spacing halves
+    return (int64_t)(762123384785ULL >> (41 - p));
+}
+
 // The split's tau: the reference evaluates (short)ceil(log2(max)) with libm
 // (src/cpu/ozblas_split.cpp:145; src/cuda/cuozblas_split.cu:201).  For
 // v = 2^e (1 + j 2^-52), log2(v) = e + log2(1 + j 2^-52) is rounded to the
 // nearest double; it rounds down onto the integer e exactly when
 // log2(1 + j 2^-52) is below half the spacing of doubles just above e, i.e.
 // when j <= floor(ln2 * 2^(p-1)) with 2^(p-53) that half spacing.  So the
-// result is e when j is at most that threshold and e + 1 otherwise.  The
-// thresholds below are floor(ln2 * 2^(p-1)) for p = -1 .. 10.  The rule is
-// pinned against glibc's log2 over every exponent by the CPU tests.
+// result is e when j is at most that threshold (tau_threshold) and e + 1
+// otherwise.  The rule is pinned against glibc's log2 over every exponent by
+// the CPU tests.
 // Zero, infinities and NaN (undefined behaviour in the reference, where it
 // never changes a slice) return 0.
 OZB_HD int tau_rule(double v) {
@@ -69,23 +81,7 @@ OZB_HD int tau_rule(double v) {
         e = be - 1023;
     }
     if (j == 0) return e;
-    const int ae = e < 0 ? -e : e;
-    int p = (ae == 0) ? -1 : (31 - clz32((uint32_t)ae));
-    if (e < 0 && (ae & (ae - 1)) == 0) p -= 1;  // just above -2^q the spacing halves
-    int J;
-    switch (p) {
-        case 2: J = 1; break;
-        case 3: J = 2; break;
-        case 4: J = 5; break;
-        case 5: J = 11; break;
-        case 6: J = 22; break;
-        case 7: J = 44; break;
-        case 8: J = 88; break;
-        case 9: J = 177; break;
-        case 10: J = 354; break;
-        default: J = 0; break;  // p <= 1
-    }
-    return ((int64_t)j <= J) ? e : e + 1;
+    return ((int64_t)j <= tau_threshold(e)) ? e : e + 1;
 }
 
 // rho = ceil(53 - (53 - log2(dim)) / 2) for splitEpsMode 0

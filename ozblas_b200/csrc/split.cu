@@ -240,7 +240,7 @@ __global__ void __launch_bounds__(256) k_split_csr(int m, const double *__restri
     if (hi > lo) {
         const int rho = rho_rule(hi - lo, epsmode);
         for (int s = 0; s < levels; s++) {
-            const double sigma = 0.75 * pow2(rho + tau_rule(mx)) / (double)shift;
+            const double sigma = shift_sigma(0.75 * pow2(rho + tau_rule(mx)), shift);
             double nm = 0.0;
             for (int i = lo + lane; i < hi; i += 32) {
                 double r = rem[i];

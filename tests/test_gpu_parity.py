@@ -186,6 +186,54 @@ def test_split_a_and_cg(sm, oracle, handle, ozb, cuda):
     assert bits_equal(host(dx), xr), first_diff(host(dx), xr)
 
 
+@pytest.mark.parametrize("K", [60, 120])
+@pytest.mark.parametrize("sm", [0, 1])
+def test_cg_deep_rows(K, sm, oracle, handle, ozb, cuda):
+    """Columns scaled by 2^[-K, K]: rows need 5 (K=60) or 7 (K=120) levels, so
+    the CG's SpMV runs the deep-row kernel (and defers rows beyond it); the
+    later, wide CG vectors take the general x path."""
+    nx = ny = nz = 8
+    rowptr, colind = oracle.stencil7(nx, ny, nz)
+    n = len(rowptr) - 1
+    val = oracle.poisson_shift(nx, ny, nz, 3, rowptr, colind)
+    val = val * 2.0 ** np.random.default_rng(K).integers(-K, K + 1, n)[colind]
+    b = oracle.normal(n, 4)
+    iters = 4
+    xr, hr, info = oracle.dcg(make_flags(sumMode=sm), val, colind, rowptr, b, np.zeros(n), iters, 0.0)
+    handle.sumMode = sm
+    handle.verbose = 1
+    dx = cuda.zeros(n, dtype=cuda.float64, device="cuda")
+    h1 = np.zeros(iters + 1)
+    h2 = np.zeros(iters + 1)
+    ozb.dcg(handle, "n", n, len(val), dev(cuda, val), dev(cuda, colind), dev(cuda, rowptr), dev(cuda, b), dx,
+            iters, 0.0, h1, h2)
+    assert bits_equal(h1, hr), first_diff(h1, hr)
+    assert bits_equal(host(dx), xr), first_diff(host(dx), xr)
+
+
+@pytest.mark.parametrize("n", [1, 2, 3, 4097, 100003])
+@pytest.mark.parametrize("sm", [0, 1])
+def test_ddot_unaligned_and_odd(n, sm, oracle, handle, ozb, cuda):
+    """Vectors 8 bytes off a 16-byte boundary take the scalar-load kernels;
+    odd lengths leave one element outside the paired stream."""
+    x = oracle.phi_vector(n, 2.0, 1)
+    y = oracle.phi_vector(n, 2.0, 2)
+    handle.sumMode = sm
+    r, info = oracle.ddot(make_flags(sumMode=sm), x, y)
+    bx = cuda.zeros(n + 1, dtype=cuda.float64, device="cuda")
+    by = cuda.zeros(n + 1, dtype=cuda.float64, device="cuda")
+    bx[1:] = dev(cuda, x)
+    by[1:] = dev(cuda, y)
+    for xv, yv in ((bx[1:], by[1:]), (bx[1:], dev(cuda, y)), (dev(cuda, x), dev(cuda, y))):
+        d = ozb.ddot(handle, n, xv, yv)
+        assert np.float64(d).view(np.int64) == np.float64(r).view(np.int64), (n, sm, d, r)
+        assert (handle.nSplitA, handle.nSplitB) == (info.nSplitA, info.nSplitB)
+    nr_ref, _ = oracle.dnrm2(make_flags(sumMode=sm), x)
+    for xv in (bx[1:], dev(cuda, x)):
+        nr = ozb.dnrm2(handle, n, xv)
+        assert np.float64(nr).view(np.int64) == np.float64(nr_ref).view(np.int64), (n, sm, nr, nr_ref)
+
+
 def test_invalid_arguments(handle, ozb, cuda):
     x = cuda.zeros(8, dtype=cuda.float64, device="cuda")
     with pytest.raises(ozb.OzblasError) as e:
