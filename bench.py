@@ -173,7 +173,8 @@ def main():
     ap.add_argument("--full-pairs", action="store_true", help="headline with the full pair set instead of triangular")
     ap.add_argument("--n", type=int, default=N_DIM, help="m = n = k (default 8192; smaller for profiling captures)")
     ap.add_argument("--memory-only", action="store_true",
-                    help="only the DOT / CSRMV measurements (for profiling them; prints their JSON)")
+                    help="only the DOT / CSRMV / CG measurements (for profiling them; prints their JSON)")
+    ap.add_argument("--cg-iters", type=int, default=2000, help="CG iterations of the memory-only run")
     args = ap.parse_args()
     globals()["N_DIM"] = args.n
     args.warmup = max(args.warmup, 3)
@@ -195,7 +196,7 @@ def main():
         h = ozb.Handle(work_bytes=8 << 30)
         h.nSplitMax = 0
         print(json.dumps({"workload": "memory-bound plain kernels", "reps": args.steps,
-                          "extras": memory_extras(ozb, h, torch, reps=args.steps)}))
+                          "extras": memory_extras(ozb, h, torch, reps=args.steps, cg_iters=args.cg_iters)}))
         h.close()
         return 0
     dist = None
@@ -372,8 +373,11 @@ def extras(ozb, h, torch, A, B, C, n):
     return out
 
 
-def memory_extras(ozb, h, torch, reps=3):
-    """DOT n = 2^24 (phi = 2) and CSRMV on the 128^3 7-point stencil, both sum modes, through the public API."""
+def memory_extras(ozb, h, torch, reps=3, cg_iters=2000):
+    """DOT n = 2^24 (phi = 2), CSRMV on the 128^3 7-point stencil (both sum modes) and CG on 100^3, through the
+    public API."""
+    import numpy as np
+
     out = {}
 
     def timed(fn, reps=1):
@@ -433,7 +437,44 @@ def memory_extras(ozb, h, torch, reps=3):
         ms = timed(lambda: ozb.dcsrmv(h, "n", m, m, nnz, 1.0, val, colind, rowptr, xv, 0.0, yv), reps=reps)
         out[f"dcsrmv_stencil128_sum{sm}"] = {"GBps": nbytes / ms / 1e6, "ms": ms, "nnz": nnz,
                                              "slices": [h.nSplitA, h.nSplitB]}
-    h.sumMode = 0
+    # CG: 7-point Poisson on 100^3 plus 0.01 U(0,1) on the diagonal, b = A x_true,
+    # 2000 iterations (tol 0), NearSum, history every iteration (verbose = 1)
+    del val, colind, rowptr, xv, yv, C7, M7, cols, masks, idx, xi, yi, zi
+    torch.cuda.empty_cache()
+    g3 = 100
+    m = g3 ** 3
+    idx = torch.arange(m, device="cuda", dtype=torch.int64)
+    xi, yi, zi = idx % g3, (idx // g3) % g3, idx // (g3 * g3)
+    offs = [(-g3 * g3, zi > 0), (-g3, yi > 0), (-1, xi > 0), (0, None), (1, xi < g3 - 1), (g3, yi < g3 - 1),
+            (g3 * g3, zi < g3 - 1)]
+    C7 = torch.stack([idx + o for o, _ in offs], 1)
+    M7 = torch.stack([torch.ones(m, dtype=torch.bool, device="cuda") if k is None else k for _, k in offs], 1)
+    V7 = torch.full((m, 7), -1.0, dtype=torch.float64, device="cuda")
+    V7[:, 3] = 6.0 + 0.01 * torch.rand(m, dtype=torch.float64, device="cuda", generator=g)
+    colind = C7[M7].to(torch.int32).contiguous()
+    val = V7[M7].contiguous()
+    rowptr = torch.zeros(m + 1, dtype=torch.int64, device="cuda")
+    rowptr[1:] = torch.cumsum(M7.sum(1), 0)
+    rowptr = rowptr.to(torch.int32).contiguous()
+    nnz = colind.numel()
+    xt = torch.randn(m, dtype=torch.float64, device="cuda", generator=g)
+    b = (torch.where(M7, V7 * xt[C7.clamp(0, m - 1)], torch.zeros_like(V7))).sum(1).contiguous()
+    xs = torch.zeros(m, dtype=torch.float64, device="cuda")
+    iters = cg_iters
+    h1 = np.zeros(iters + 1)
+    h2 = np.zeros(iters + 1)
+    h.sumMode, h.verbose = 1, 1
+    ms = timed(lambda: (xs.zero_(), ozb.dcg(h, "n", m, nnz, val, colind, rowptr, b, xs, iters, 0.0, h1, h2)),
+               reps=min(reps, 2))
+    l0 = h.launch_count()
+    xs.zero_()
+    ozb.dcg(h, "n", m, nnz, val, colind, rowptr, b, xs, iters, 0.0, h1, h2)
+    per_iter_bytes = 12.0 * nnz + 4.0 * (m + 1) + 116.0 * m
+    out[f"dcg_100cube_{iters}it"] = {"ms": ms, "ms_per_iter": ms / iters, "GBps": per_iter_bytes * iters / ms / 1e6,
+                                 "iterations": h.cg_numiter, "nnz": nnz, "final_rel_res": float(h1[iters]),
+                                 "launches_per_iter": (h.launch_count() - l0) / iters,
+                                 "bytes_per_iter": per_iter_bytes}
+    h.sumMode, h.verbose = 0, 0
     return out
 
 

@@ -1,6 +1,9 @@
 // api.cu — the C ABI of include/cuozblas.h: handle lifecycle and the
 // BLAS-level entry points of the plain (FP64-slice) form.
+#include <functional>
+#include <vector>
 #include <math.h>
+#include <stdlib.h>
 #include <string.h>
 #include <sys/time.h>
 
@@ -20,6 +23,11 @@ int dot_fused(cuozblasHandle_t *h, int n, const double *x, const double *y, doub
 int csrmv_fused(cuozblasHandle_t *h, int m, int n, double alpha, const double *val, const int *colind,
                 const int *rowptr, const double *x, double beta, double *y, int shift, int na_hint, bool *done,
                 int *nA_out, int *nB_out);
+int cg_graph(cuozblasHandle_t *h, int n, const double *val, const int *colind, const int *rowptr, double *x,
+             double *r, double *p, double *q, double nrmb, double tol, int maxiter, int shift, int na_hint,
+             double &dold, int &iter, bool &stop, double t1, double *res, double *when,
+             const std::function<int()> &host_head, const std::function<int(bool &)> &host_tail,
+             const std::function<double()> &wall_now);
 
 // CSRMV exec info as the reference records it (src/cpu/ozblas_csrmv.cpp:104-119)
 static void csrmv_info(cuozblasHandle_t *h, int nA, int nB) {
@@ -79,11 +87,14 @@ static int dot_impl(cuozblasHandle_t *h, int n, const double *x, const double *y
         h->nSplitA = (float)nA;
         h->nSplitB = (float)nB;
         h->nSplitC = 1.f;
+        if (getenv("OZBLAS_DOT_TRACE")) fprintf(stderr, "cuozblas: dot fused nA=%d nB=%d\n", nA, nB);
         return CUOZBLAS_STATUS_SUCCESS;
     }
     double *d = reinterpret_cast<double *>(h->devWorkCommon);
     OZB_CHECK(cudaMemsetAsync(d, 0, sizeof(double), st->stream));
     OZB_TRY(gemm_plain_core(h, 't', 'n', 1, 1, n, 1.0, x, n, y, n, 0.0, d, 1, 0));
+    if (getenv("OZBLAS_DOT_TRACE"))
+        fprintf(stderr, "cuozblas: dot general nA=%d nB=%d\n", (int)h->nSplitA, (int)h->nSplitB);
     OZB_CHECK(cudaMemcpyAsync(st->h_dbl, d, sizeof(double), cudaMemcpyDeviceToHost, st->stream));
     OZB_CHECK(cudaStreamSynchronize(st->stream));
     *ret = st->h_dbl[0];
@@ -349,9 +360,12 @@ int cuozblasDcg(cuozblasHandle_t *h, char trans, int32_t n, int32_t nnz, const v
             int fa = 0, fb = 0;
             OZB_TRY(csrmv_fused(h, n, n, al, val, colind, rowptr, xv, be, yv, cg_shift, h->nSplitA_, &done, &fa,
                                       &fb));
+            if (getenv("OZBLAS_DOT_TRACE") && done) fprintf(stderr, "cuozblas: spmv fused nB=%d\n", fb);
             if (done) return CUOZBLAS_STATUS_SUCCESS;
         }
-        return cuozblasDcsrmv(h, trans, n, n, nnz, al, descrA, As, colind, rowptr, xv, be, yv);
+        const int rs = cuozblasDcsrmv(h, trans, n, n, nnz, al, descrA, As, colind, rowptr, xv, be, yv);
+        if (getenv("OZBLAS_DOT_TRACE")) fprintf(stderr, "cuozblas: spmv general nB=%d\n", (int)h->nSplitB);
+        return rs;
     };
     if ((status = spmv(-1., x, 1., r))) return fail(status);
     if ((status = cuozblasDdot(h, n, r, 1, r, 1, &dold))) return fail(status);
@@ -375,29 +389,60 @@ int cuozblasDcg(cuozblasHandle_t *h, char trans, int32_t n, int32_t nnz, const v
     }
     if (cudaMemcpyAsync(p, r, sizeof(double) * n, cudaMemcpyDeviceToDevice, st->stream) != cudaSuccess)
         return fail(CUOZBLAS_STATUS_CUDA_ERROR);
-    int verbose_cnt = 1;
-    while (h->cg_numiter < maxiter) {
-        h->cg_numiter++;
-        if ((status = spmv(1., p, 0., q))) return fail(status);
-        if ((status = cuozblasDdot(h, n, p, 1, q, 1, &tmp))) return fail(status);
+    // per iteration: resi / nrmb and the second history value (elapsed time or
+    // the true residual); recorded by the reference's rule at the end
+    std::vector<double> res_all((size_t)maxiter + 1), when_all((size_t)maxiter + 1);
+    int it = 0;
+    bool stop = false;
+    // one iteration in two halves: up to the x and r updates, and the rest
+    auto host_head = [&]() -> int {
+        h->cg_numiter = it + 1;
+        OZB_TRY(spmv(1., p, 0., q));
+        OZB_TRY(cuozblasDdot(h, n, p, 1, q, 1, &tmp));
         const double alpha = dold / tmp;
-        if ((status = launch_axpy(h, n, alpha, p, x))) return fail(status);
-        if ((status = launch_axpy(h, n, -alpha, q, r))) return fail(status);
+        OZB_TRY(launch_axpy(h, n, alpha, p, x));
+        OZB_TRY(launch_axpy(h, n, -alpha, q, r));
+        return CUOZBLAS_STATUS_SUCCESS;
+    };
+    auto host_tail = [&](bool &stp) -> int {
+        it++;
+        h->cg_numiter = it;
         double dnew = 0.0;
-        if ((status = cuozblasDdot(h, n, r, 1, r, 1, &dnew))) return fail(status);
+        OZB_TRY(cuozblasDdot(h, n, r, 1, r, 1, &dnew));
         resi = sqrt(dnew);
         const double beta = dnew / dold;
         dold = dnew;
-        if ((status = launch_scal(h, n, beta, p))) return fail(status);
-        if ((status = launch_axpy(h, n, 1.0, r, p))) return fail(status);
-        if (h->verbose > 0) {
-            if (resi / nrmb < tol || h->cg_numiter % h->verbose == 0) {
-                if (hist1) hist1[verbose_cnt] = resi / nrmb;
-                if (hist2) hist2[verbose_cnt] = h->trueresFlag ? true_res() / nrmb : wall() - t1;
+        OZB_TRY(launch_scal(h, n, beta, p));
+        OZB_TRY(launch_axpy(h, n, 1.0, r, p));
+        res_all[(size_t)it] = resi / nrmb;
+        if (h->verbose > 0) when_all[(size_t)it] = h->trueresFlag ? true_res() / nrmb : wall() - t1;
+        if (resi / nrmb < tol) stp = true;
+        return CUOZBLAS_STATUS_SUCCESS;
+    };
+    auto host_iter = [&](bool &stp) -> int {
+        OZB_TRY(host_head());
+        return host_tail(stp);
+    };
+    // The fused steps run as captured graphs when both fused paths apply
+    // (plain split, full pair set) and the history needs no host work.
+    const bool graphs = h->fastMode == 0 && h->splitEpsMode == 0 && n > 0 &&
+                        !(h->verbose > 0 && h->trueresFlag) && getenv("OZBLAS_CG_NO_GRAPH") == nullptr;
+    if (graphs) {
+        if ((status = cg_graph(h, n, val, colind, rowptr, x, r, p, q, nrmb, tol, maxiter, cg_shift, h->nSplitA_, dold,
+                               it, stop, t1, res_all.data(), when_all.data(), host_head, host_tail, wall)))
+            return fail(status);
+    }
+    while (!stop && it < maxiter)
+        if ((status = host_iter(stop))) return fail(status);
+    h->cg_numiter = it;
+    if (h->verbose > 0) {  // src/cpu/ozblas_cg.cpp:104-115
+        int verbose_cnt = 1;
+        for (int i = 1; i <= it; i++)
+            if (res_all[(size_t)i] < tol || i % h->verbose == 0) {
+                if (hist1) hist1[verbose_cnt] = res_all[(size_t)i];
+                if (hist2) hist2[verbose_cnt] = when_all[(size_t)i];
                 verbose_cnt++;
             }
-        }
-        if (resi / nrmb < tol) break;
     }
     cudaError_t e = cudaStreamSynchronize(st->stream);
     h->memMaskSplitA = 0;  // src/cuda/cuozblas_cg.cu:124-127

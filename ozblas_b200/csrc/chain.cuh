@@ -120,6 +120,14 @@ __device__ inline void make_plan(const VecStats *vs, int rho, int maxS, bool sam
     pl.L = L;
 }
 
+// Copy a plan from global memory into shared memory (whole block).
+__device__ __forceinline__ void load_plan(const TreePlan *g, TreePlan &sh) {
+    static_assert(sizeof(TreePlan) % 4 == 0, "plan layout");
+    const unsigned *src = reinterpret_cast<const unsigned *>(g);
+    unsigned *dst = reinterpret_cast<unsigned *>(&sh);
+    for (int i = threadIdx.x; i < (int)(sizeof(TreePlan) / 4); i += blockDim.x) dst[i] = __ldcg(src + i);
+}
+
 // Deepest level that can hold a nonzero slice of an element whose exponent
 // field is `key` (0x7ff: the element is zero): its lowest set bit is at least
 // key - 1075.

@@ -24,26 +24,15 @@
 // the reference; they add +0 to the ordered sum and nothing to NearSum, so
 // skipping them leaves the bits unchanged.  fastMode must be 0 (the caller
 // uses the general path otherwise).
-#include "chain.cuh"
-#include "ozb_internal.h"
+#include "fused.h"
 #include "sum.cuh"
 
 namespace ozb {
 
-constexpr int kCsrLv = kChainLevels;  // levels of x computed / proven
-constexpr int kCsrRowMax = 8;         // entries per row held on chip
-constexpr int kCsrThreads = 128;
-
-struct CsrScratch {
-    VecStats vs;             // first pass over x
-    unsigned proven;         // levels of x's chain whose predicted tau some element proved
-    unsigned ticket;         // blocks of the proof pass that are done
-    int valid, nB, nslow, zmax;  // zmax: first zero-remainder level of A, max over rows
-    double sigma[kCsrLv];    // x's proven sigmas
-};
-
+// Max, lowest set bit and Inf/NaN of v into vs[index] (the first pass of a
+// vector's predicted chain).
 template <bool ALIGNED>
-__global__ void __launch_bounds__(256) k_csr_scan(int n, const double *__restrict__ x, CsrScratch *sc) {
+__global__ void __launch_bounds__(256) k_vec_stats(int n, const double *__restrict__ x, VecStats *vs, int index) {
     __shared__ double red[8];
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
     double mx = 0.0;
@@ -61,7 +50,7 @@ __global__ void __launch_bounds__(256) k_csr_scan(int n, const double *__restric
     } else {
         for (; i < n; i += stride) scan_elem(x[i], mx, lx, bx);
     }
-    scan_commit(&sc->vs, 0, mx, lx, bx, red);
+    scan_commit(vs, index, mx, lx, bx, red);
 }
 
 template <int G, int T>
@@ -78,11 +67,12 @@ __device__ __forceinline__ unsigned proof_body(double v, const TreePlan &pl) {
 // publishes validity, slice count and sigmas.
 template <int G>
 __global__ void __launch_bounds__(256) k_csr_proof(int n, const double *__restrict__ x, int rho, int maxS,
-                                                   CsrScratch *sc) {
+                                                   CsrScratch *sc, const int *__restrict__ gate) {
+    if (gate && *gate == 0) return;  // uniform: a captured solver step that is switched off
     __shared__ TreePlan pl;
     __shared__ int last;
     const int t = threadIdx.x;
-    if (t == 0) make_plan(&sc->vs, rho, maxS, true, pl);
+    load_plan(&sc->plan, pl);
     __syncthreads();
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + t;
     if (pl.valid && pl.need[0]) {  // uniform
@@ -112,6 +102,23 @@ __global__ void __launch_bounds__(256) k_csr_proof(int n, const double *__restri
     for (int s = 0; s < kCsrLv; s++) sc->sigma[s] = pl.sig[0][s];
     sc->nB = pl.ns[0];
     sc->valid = valid;
+    // leave the proof zeroed for the next use
+    sc->proven = 0u;
+    sc->ticket = 0u;
+}
+
+__global__ void k_make_plan(VecStats *vs, int rho, int maxS, int same, TreePlan *plan, const int *gate) {
+    if (gate && *gate == 0) return;
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    TreePlan pl;
+    make_plan(vs, rho, maxS, same != 0, pl);
+    *plan = pl;
+    *vs = VecStats{};
+}
+
+int plan_launch(cudaStream_t s, VecStats *vs, int rho, int maxS, bool same, TreePlan *plan, const int *gate) {
+    k_make_plan<<<1, 32, 0, s>>>(vs, rho, maxS, same ? 1 : 0, plan, gate);
+    return cudaGetLastError() == cudaSuccess ? CUOZBLAS_STATUS_SUCCESS : CUOZBLAS_STATUS_CUDA_ERROR;
 }
 
 // Visit the pairs (ia < na, ib < nb) of a row in summation order: ik
@@ -197,6 +204,84 @@ __device__ __forceinline__ double nearsum_row(double (&v)[NA][kCsrLv], int na, i
     return res;
 }
 
+// The row's own chain (src/cpu/ozblas_split.cpp:779-815, sigma / shift) over
+// its entries a[] (zero padded to kCsrRowMax), at most NA levels: the sigmas,
+// the level count na and the first zero-remainder level z.  Returns false
+// when the row needs more than NA levels (and nSplitMax allows more).
+template <int NA>
+__device__ __forceinline__ bool row_chain(const double (&a)[kCsrRowMax], int len, int shift, int epsmode, int maxS,
+                                          double (&sigA)[NA], int &na, int &z) {
+    na = 0;
+    z = 0;
+#pragma unroll
+    for (int s = 0; s < NA; s++) sigA[s] = 0.0;
+    if (len <= 0) return true;
+    const int rho = rho_rule(len, epsmode);
+    double rr[kCsrRowMax];
+    double mx = 0.0;
+#pragma unroll
+    for (int e = 0; e < kCsrRowMax; e++) {
+        rr[e] = a[e];
+        mx = ref_max(mx, fabs(a[e]));
+    }
+    z = maxS;
+    bool fin = false;
+#pragma unroll
+    for (int s = 0; s < NA; s++) {
+        if (!fin && s < maxS) {
+            const double sg = shift_sigma(0.75 * pow2(rho + tau_rule(mx)), shift);
+            sigA[s] = sg;
+            double nm = 0.0;
+#pragma unroll
+            for (int e = 0; e < kCsrRowMax; e++) {
+                const double sl = (rr[e] + sg) - sg;
+                rr[e] = rr[e] - sl;
+                nm = ref_max(nm, fabs(rr[e]));
+            }
+            na = s + 1;
+            mx = nm;
+            if (nm == 0.0) {
+                z = s;
+                fin = true;
+            }
+        }
+    }
+    return !(mx != 0.0 && na < maxS);
+}
+
+// The rows the row kernel defers (more than kCsrRowMax entries, or more than
+// NA levels), listed once for a matrix that is multiplied many times.
+template <int NA>
+__global__ void __launch_bounds__(128) k_csr_slow_rows(int m, const double *__restrict__ val,
+                                                       const int *__restrict__ rowptr, int shift, int epsmode,
+                                                       int maxS, int *__restrict__ list, int *__restrict__ count) {
+    const int row = blockIdx.x * blockDim.x + threadIdx.x;
+    if (row >= m) return;
+    const int lo = rowptr[row], len = rowptr[row + 1] - lo;
+    bool defer = len > kCsrRowMax;
+    if (!defer) {
+        double a[kCsrRowMax];
+#pragma unroll
+        for (int e = 0; e < kCsrRowMax; e++) a[e] = e < len ? val[lo + e] : 0.0;
+        double sigA[NA];
+        int na, z;
+        defer = !row_chain<NA>(a, len, shift, epsmode, maxS, sigA, na, z);
+    }
+    if (defer) list[atomicAdd(count, 1)] = row;
+}
+
+int csr_slow_rows_launch(cudaStream_t s, int m, const double *val, const int *rowptr, int shift, int epsmode,
+                         int maxS, int na_hint, int *list, int *count) {
+    if (m <= 0) return CUOZBLAS_STATUS_SUCCESS;
+    if (na_hint > 0 && na_hint <= 2)
+        k_csr_slow_rows<2><<<(m + 127) / 128, 128, 0, s>>>(m, val, rowptr, shift, epsmode, maxS, list, count);
+    else if (na_hint > 4)
+        k_csr_slow_rows<6><<<(m + 127) / 128, 128, 0, s>>>(m, val, rowptr, shift, epsmode, maxS, list, count);
+    else
+        k_csr_slow_rows<4><<<(m + 127) / 128, 128, 0, s>>>(m, val, rowptr, shift, epsmode, maxS, list, count);
+    return cudaGetLastError() == cudaSuccess ? CUOZBLAS_STATUS_SUCCESS : CUOZBLAS_STATUS_CUDA_ERROR;
+}
+
 // One thread per row, everything in registers.  A block's val/colind range
 // is staged in shared memory with coalesced loads; each row's tau chain runs
 // over its (at most kCsrRowMax) entries, keeping only the sigmas, then every
@@ -240,8 +325,12 @@ __global__ void __launch_bounds__(kCsrThreads) k_csrmv_reg(int m, int n, const d
                                                            const double *__restrict__ x, int shift, int epsmode,
                                                            int maxS, double alpha, double beta,
                                                            double *__restrict__ y, CsrScratch *__restrict__ sc,
-                                                           int *__restrict__ slow_rows) {
+                                                           int *__restrict__ slow_rows, int append_slow,
+                                                           VecStats *__restrict__ ystats, int ystats_index,
+                                                           const int *__restrict__ gate) {
+    if (gate && *gate == 0) return;  // uniform: a captured solver step that is switched off
     constexpr int kStage = kCsrThreads * kCsrRowMax;
+    __shared__ double red[kCsrThreads / 32];
     __shared__ double s_val[kStage];
     __shared__ int s_col[kStage];
     __shared__ int s_rp[kCsrThreads + 1];
@@ -307,71 +396,46 @@ __global__ void __launch_bounds__(kCsrThreads) k_csrmv_reg(int m, int n, const d
 #pragma unroll
         for (int e = 0; e < kCsrRowMax; e++) xv[e] = 0.0;
     }
-    // the row's own chain (src/cpu/ozblas_split.cpp:779-815, sigma / shift)
     double sigA[NA];
     int na = 0, z = 0;
-#pragma unroll
-    for (int s = 0; s < NA; s++) sigA[s] = 0.0;
-    if (work && len > 0) {
-        const int rho = rho_rule(len, epsmode);
-        double rr[kCsrRowMax];
-        double mx = 0.0;
-#pragma unroll
-        for (int e = 0; e < kCsrRowMax; e++) {
-            rr[e] = a[e];
-            mx = ref_max(mx, fabs(a[e]));
-        }
-        z = maxS;
-        bool fin = false;
-#pragma unroll
-        for (int s = 0; s < NA; s++) {
-            if (!fin && s < maxS) {
-                const double sg = shift_sigma(0.75 * pow2(rho + tau_rule(mx)), shift);
-                sigA[s] = sg;
-                double nm = 0.0;
-#pragma unroll
-                for (int e = 0; e < kCsrRowMax; e++) {
-                    const double sl = (rr[e] + sg) - sg;
-                    rr[e] = rr[e] - sl;
-                    nm = ref_max(nm, fabs(rr[e]));
-                }
-                na = s + 1;
-                mx = nm;
-                if (nm == 0.0) {
-                    z = s;
-                    fin = true;
-                }
-            }
-        }
-        if (mx != 0.0 && na < maxS) defer = true;  // needs more levels than NA
-    }
-    if (defer) slow_rows[atomicAdd(&sc->nslow, 1)] = row;
+    if (work && !row_chain<NA>(a, len, shift, epsmode, maxS, sigA, na, z)) defer = true;
+    if (defer && append_slow) slow_rows[atomicAdd(&sc->nslow, 1)] = row;
     {
         const int zw = __reduce_max_sync(0xffffffffu, (work && !defer) ? z : 0);
         if ((t & 31) == 0 && zw > 0) atomicMax(&sc->zmax, zw);
     }
-    if (!work || defer) return;
-    double P[NA][kCsrLv];
+    double ynew = 0.0;
+    const bool wrote = work && !defer;
+    if (wrote) {
+        double P[NA][kCsrLv];
 #pragma unroll
-    for (int i = 0; i < NA; i++)
+        for (int i = 0; i < NA; i++)
 #pragma unroll
-        for (int j = 0; j < kCsrLv; j++) P[i][j] = 0.0;
-    switch (nB) {  // uniform
-        case 1: row_products<NA, 1, GX>(a, xv, len, na, sigA, xs_sigma, P); break;
-        case 2: row_products<NA, 2, GX>(a, xv, len, na, sigA, xs_sigma, P); break;
-        case 3: row_products<NA, 3, GX>(a, xv, len, na, sigA, xs_sigma, P); break;
-        case 4: row_products<NA, 4, GX>(a, xv, len, na, sigA, xs_sigma, P); break;
-        case 5: row_products<NA, 5, GX>(a, xv, len, na, sigA, xs_sigma, P); break;
-        case 6: row_products<NA, 6, GX>(a, xv, len, na, sigA, xs_sigma, P); break;
-        case 7: row_products<NA, 7, GX>(a, xv, len, na, sigA, xs_sigma, P); break;
-        default: row_products<NA, 8, GX>(a, xv, len, na, sigA, xs_sigma, P); break;
+            for (int j = 0; j < kCsrLv; j++) P[i][j] = 0.0;
+        switch (nB) {  // uniform
+            case 1: row_products<NA, 1, GX>(a, xv, len, na, sigA, xs_sigma, P); break;
+            case 2: row_products<NA, 2, GX>(a, xv, len, na, sigA, xs_sigma, P); break;
+            case 3: row_products<NA, 3, GX>(a, xv, len, na, sigA, xs_sigma, P); break;
+            case 4: row_products<NA, 4, GX>(a, xv, len, na, sigA, xs_sigma, P); break;
+            case 5: row_products<NA, 5, GX>(a, xv, len, na, sigA, xs_sigma, P); break;
+            case 6: row_products<NA, 6, GX>(a, xv, len, na, sigA, xs_sigma, P); break;
+            case 7: row_products<NA, 7, GX>(a, xv, len, na, sigA, xs_sigma, P); break;
+            default: row_products<NA, 8, GX>(a, xv, len, na, sigA, xs_sigma, P); break;
+        }
+        double tsum = 0.0;
+        if (SUM_MODE == 1)
+            tsum = nearsum_row<NA>(P, na, nB);
+        else
+            for_row_pairs<NA>(na, nB, [&](int ia, int ib) { tsum += P[ia][ib]; });
+        ynew = fma(alpha, tsum, beta * yold);
+        y[row] = ynew;
     }
-    double tsum = 0.0;
-    if (SUM_MODE == 1)
-        tsum = nearsum_row<NA>(P, na, nB);
-    else
-        for_row_pairs<NA>(na, nB, [&](int ia, int ib) { tsum += P[ia][ib]; });
-    y[row] = fma(alpha, tsum, beta * yold);
+    if (ystats) {  // uniform: statistics of the written y for a following DOT
+        double mx = 0.0;
+        int lsb = 0, bad = 0;
+        if (wrote) scan_elem(ynew, mx, lsb, bad);
+        scan_commit(ystats, ystats_index, mx, lsb, bad, red);
+    }
 }
 
 // Recompute slice `lv` of v from scratch along the chain sig[0..lv].
@@ -392,74 +456,155 @@ __global__ void __launch_bounds__(128) k_csrmv_slow(int nrows, const int *__rest
                                                     const int *__restrict__ rowptr, const double *__restrict__ x,
                                                     int shift, int epsmode, int maxS, double alpha, double beta,
                                                     double *__restrict__ y, CsrScratch *__restrict__ sc,
-                                                    double *__restrict__ terms) {
+                                                    double *__restrict__ terms, VecStats *__restrict__ ystats,
+                                                    int ystats_index, const int *__restrict__ gate) {
+    if (gate && *gate == 0) return;  // uniform
+    if (!sc->valid) return;          // uniform: x's chain is not proven
+    __shared__ double red[4];
     const int slot = blockIdx.x * blockDim.x + threadIdx.x;
-    if (slot >= nrows) return;
-    const int row = rows[slot];
-    const int lo = rowptr[row], hi = rowptr[row + 1], len = hi - lo;
-    const int nB = sc->nB;
-    double sa[kMaxSplitDefault];
-    int na = 0, z = 0;
-    if (len > 0) {
-        z = maxS;
-        const int rho = rho_rule(len, epsmode);
-        double mx = 0.0;
-        for (int i = lo; i < hi; i++) mx = ref_max(mx, fabs(val[i]));
-        for (int s = 0; s < maxS; s++) {
-            sa[s] = shift_sigma(0.75 * pow2(rho + tau_rule(mx)), shift);
-            na = s + 1;
-            double nm = 0.0;
-            for (int i = lo; i < hi; i++) {
-                double v = val[i];
-                for (int q = 0; q <= s; q++) {
-                    const double sl = (v + sa[q]) - sa[q];
-                    v = v - sl;
+    double ynew = 0.0;
+    const bool wrote = slot < nrows;
+    if (wrote) {
+        const int row = rows[slot];
+        const int lo = rowptr[row], hi = rowptr[row + 1], len = hi - lo;
+        const int nB = sc->nB;
+        double sa[kMaxSplitDefault];
+        int na = 0, z = 0;
+        if (len > 0) {
+            z = maxS;
+            const int rho = rho_rule(len, epsmode);
+            double mx = 0.0;
+            for (int i = lo; i < hi; i++) mx = ref_max(mx, fabs(val[i]));
+            for (int s = 0; s < maxS; s++) {
+                sa[s] = shift_sigma(0.75 * pow2(rho + tau_rule(mx)), shift);
+                na = s + 1;
+                double nm = 0.0;
+                for (int i = lo; i < hi; i++) {
+                    double v = val[i];
+                    for (int q = 0; q <= s; q++) {
+                        const double sl = (v + sa[q]) - sa[q];
+                        v = v - sl;
+                    }
+                    nm = ref_max(nm, fabs(v));
                 }
-                nm = ref_max(nm, fabs(v));
-            }
-            mx = nm;
-            if (nm == 0.0) {
-                z = s;
-                break;
+                mx = nm;
+                if (nm == 0.0) {
+                    z = s;
+                    break;
+                }
             }
         }
-    }
-    atomicMax((int *)&sc->zmax, z);
-    double tsum = 0.0;
-    int np = 0;
-    double *tm = terms + (size_t)slot * kMaxSplitDefault * kCsrLv;
-    const int maxlevel = na + nB - 2;
-    for (int ik = 0; ik <= maxlevel; ik++) {
-        const int ia0 = ik - (nB - 1) > 0 ? ik - (nB - 1) : 0, ia1 = ik < na - 1 ? ik : na - 1;
-        for (int ia = ia0; ia <= ia1; ia++) {
-            const int ib = ik - ia;
-            double p = 0.0;
-            for (int i = lo; i < hi; i++)
-                p = fma(slice_at(val[i], sa, ia), slice_at(x[colind[i]], sc->sigma, ib), p);
-            if (SUM_MODE == 1)
-                tm[np] = p;
-            else
-                tsum += p;
-            np++;
+        atomicMax((int *)&sc->zmax, z);
+        double tsum = 0.0;
+        int np = 0;
+        double *tm = terms + (size_t)slot * kMaxSplitDefault * kCsrLv;
+        const int maxlevel = na + nB - 2;
+        for (int ik = 0; ik <= maxlevel; ik++) {
+            const int ia0 = ik - (nB - 1) > 0 ? ik - (nB - 1) : 0, ia1 = ik < na - 1 ? ik : na - 1;
+            for (int ia = ia0; ia <= ia1; ia++) {
+                const int ib = ik - ia;
+                double p = 0.0;
+                for (int i = lo; i < hi; i++)
+                    p = fma(slice_at(val[i], sa, ia), slice_at(x[colind[i]], sc->sigma, ib), p);
+                if (SUM_MODE == 1)
+                    tm[np] = p;
+                else
+                    tsum += p;
+                np++;
+            }
         }
+        if (SUM_MODE == 1) tsum = nearsum(np, tm, 1);
+        ynew = fma(alpha, tsum, beta * y[row]);
+        y[row] = ynew;
     }
-    if (SUM_MODE == 1) tsum = nearsum(np, tm, 1);
-    y[row] = fma(alpha, tsum, beta * y[row]);
+    if (ystats) {
+        double mx = 0.0;
+        int lsb = 0, bad = 0;
+        if (wrote) scan_elem(ynew, mx, lsb, bad);
+        scan_commit(ystats, ystats_index, mx, lsb, bad, red);
+    }
 }
 
 template <int SUM_MODE, int NA>
-static void launch_reg(int gx, int rb, cudaStream_t s, int m, int n, const double *val, const int *colind,
-                       const int *rowptr, const double *x, int shift, int epsmode, int maxS, double alpha, double beta,
-                       double *y, CsrScratch *sc, int *slow) {
+static void launch_reg(int gx, int rb, cudaStream_t s, const CsrmvArgs &a, CsrScratch *sc, int *slow, int append,
+                       VecStats *ys, int yi, const int *gate) {
     if (gx >= 3)
-        k_csrmv_reg<SUM_MODE, NA, 3><<<rb, kCsrThreads, 0, s>>>(m, n, val, colind, rowptr, x, shift, epsmode, maxS,
-                                                                 alpha, beta, y, sc, slow);
+        k_csrmv_reg<SUM_MODE, NA, 3><<<rb, kCsrThreads, 0, s>>>(a.m, a.n, a.val, a.colind, a.rowptr, a.x, a.shift,
+                                                                 a.epsmode, a.maxS, a.alpha, a.beta, a.y, sc, slow,
+                                                                 append, ys, yi, gate);
     else if (gx == 2)
-        k_csrmv_reg<SUM_MODE, NA, 2><<<rb, kCsrThreads, 0, s>>>(m, n, val, colind, rowptr, x, shift, epsmode, maxS,
-                                                                 alpha, beta, y, sc, slow);
+        k_csrmv_reg<SUM_MODE, NA, 2><<<rb, kCsrThreads, 0, s>>>(a.m, a.n, a.val, a.colind, a.rowptr, a.x, a.shift,
+                                                                 a.epsmode, a.maxS, a.alpha, a.beta, a.y, sc, slow,
+                                                                 append, ys, yi, gate);
     else
-        k_csrmv_reg<SUM_MODE, NA, 1><<<rb, kCsrThreads, 0, s>>>(m, n, val, colind, rowptr, x, shift, epsmode, maxS,
-                                                                 alpha, beta, y, sc, slow);
+        k_csrmv_reg<SUM_MODE, NA, 1><<<rb, kCsrThreads, 0, s>>>(a.m, a.n, a.val, a.colind, a.rowptr, a.x, a.shift,
+                                                                 a.epsmode, a.maxS, a.alpha, a.beta, a.y, sc, slow,
+                                                                 append, ys, yi, gate);
+}
+
+int vec_stats_launch(cudaStream_t s, int nsm, int n, const double *x, VecStats *vs, int index) {
+    int blocks = (int)(((int64_t)n + 511) / 512);
+    if (blocks > nsm * 8) blocks = nsm * 8;
+    if (blocks < 1) blocks = 1;
+    if ((reinterpret_cast<uintptr_t>(x) & 15u) == 0)
+        k_vec_stats<true><<<blocks, 256, 0, s>>>(n, x, vs, index);
+    else
+        k_vec_stats<false><<<blocks, 256, 0, s>>>(n, x, vs, index);
+    return cudaGetLastError() == cudaSuccess ? CUOZBLAS_STATUS_SUCCESS : CUOZBLAS_STATUS_CUDA_ERROR;
+}
+
+int csr_proof_launch(cudaStream_t s, int n, const double *x, int rho, int maxS, CsrScratch *sc, const int *gate) {
+    const int gx = chain_group(rho, 3);
+    const int pb = n > 0 ? (int)(((int64_t)n + 255) / 256) : 1;
+    if (gx >= 3)
+        k_csr_proof<3><<<pb, 256, 0, s>>>(n, x, rho, maxS, sc, gate);
+    else if (gx == 2)
+        k_csr_proof<2><<<pb, 256, 0, s>>>(n, x, rho, maxS, sc, gate);
+    else
+        k_csr_proof<1><<<pb, 256, 0, s>>>(n, x, rho, maxS, sc, gate);
+    return cudaGetLastError() == cudaSuccess ? CUOZBLAS_STATUS_SUCCESS : CUOZBLAS_STATUS_CUDA_ERROR;
+}
+
+// The row kernel, and with fixed_slow > 0 the deferred rows of that list
+// (terms: NearSum workspace of kCsrSlowChunk rows).
+constexpr int kCsrSlowChunk = 8192;
+int csr_rows_launch(cudaStream_t s, const CsrmvArgs &a, CsrScratch *sc, int *slow, int fixed_slow, VecStats *ystats,
+                    int ystats_index, double *terms, const int *gate) {
+    if (a.m <= 0) return CUOZBLAS_STATUS_SUCCESS;
+    const int rho = rho_rule(a.n, a.epsmode);
+    const int gx = chain_group(rho, 3);
+    const int rb = (a.m + kCsrThreads - 1) / kCsrThreads;
+    // levels per row held on chip: 2 when the caller knows the rows need at
+    // most 2 (the CG's pre-split count), 6 when they need more than 4, else 4
+    const int na = (a.na_hint > 0 && a.na_hint <= 2) ? 2 : (a.na_hint > 4 ? 6 : 4);
+    const int append = fixed_slow < 0 ? 1 : 0;
+    if (a.sum_mode == 1) {
+        if (na == 2)
+            launch_reg<1, 2>(gx, rb, s, a, sc, slow, append, ystats, ystats_index, gate);
+        else if (na == 6)
+            launch_reg<1, 6>(gx, rb, s, a, sc, slow, append, ystats, ystats_index, gate);
+        else
+            launch_reg<1, 4>(gx, rb, s, a, sc, slow, append, ystats, ystats_index, gate);
+    } else {
+        if (na == 2)
+            launch_reg<0, 2>(gx, rb, s, a, sc, slow, append, ystats, ystats_index, gate);
+        else if (na == 6)
+            launch_reg<0, 6>(gx, rb, s, a, sc, slow, append, ystats, ystats_index, gate);
+        else
+            launch_reg<0, 4>(gx, rb, s, a, sc, slow, append, ystats, ystats_index, gate);
+    }
+    for (int c0 = 0; c0 < fixed_slow; c0 += kCsrSlowChunk) {
+        const int nr = fixed_slow - c0 < kCsrSlowChunk ? fixed_slow - c0 : kCsrSlowChunk;
+        if (a.sum_mode == 1)
+            k_csrmv_slow<1><<<(nr + 127) / 128, 128, 0, s>>>(nr, slow + c0, a.val, a.colind, a.rowptr, a.x, a.shift,
+                                                            a.epsmode, a.maxS, a.alpha, a.beta, a.y, sc, terms,
+                                                            ystats, ystats_index, gate);
+        else
+            k_csrmv_slow<0><<<(nr + 127) / 128, 128, 0, s>>>(nr, slow + c0, a.val, a.colind, a.rowptr, a.x, a.shift,
+                                                            a.epsmode, a.maxS, a.alpha, a.beta, a.y, sc, terms,
+                                                            ystats, ystats_index, gate);
+    }
+    return cudaGetLastError() == cudaSuccess ? CUOZBLAS_STATUS_SUCCESS : CUOZBLAS_STATUS_CUDA_ERROR;
 }
 
 // Fused CSRMV.  *done = false (and y untouched) when x's chain is not proven
@@ -478,46 +623,19 @@ int csrmv_fused(cuozblasHandle_t *h, int m, int n, double alpha, const double *v
     if (!ar.ok) return CUOZBLAS_STATUS_WORKSPACE;
     const int maxS = h->nSplitMax > 0 ? h->nSplitMax : kMaxSplitDefault;
     const int rho = rho_rule(n, h->splitEpsMode);
-    const int gx = chain_group(rho, 3);
     cudaStream_t s = st->stream;
     OZB_CHECK(cudaMemsetAsync(sc, 0, sizeof(CsrScratch), s));
-    int dev = 0, nsm = 0;
-    OZB_CHECK(cudaGetDevice(&dev));
-    OZB_CHECK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
-    int blocks = (int)(((int64_t)n + 511) / 512);
-    if (blocks > nsm * 8) blocks = nsm * 8;
-    if (blocks < 1) blocks = 1;
+    const int nsm = sm_count();
     counted(h);
-    if ((reinterpret_cast<uintptr_t>(x) & 15u) == 0)
-        k_csr_scan<true><<<blocks, 256, 0, s>>>(n, x, sc);
-    else
-        k_csr_scan<false><<<blocks, 256, 0, s>>>(n, x, sc);
-    const int pb = (int)(((int64_t)n + 255) / 256) > 0 ? (int)(((int64_t)n + 255) / 256) : 1;
+    OZB_TRY(vec_stats_launch(s, nsm, n, x, &sc->vs, 0));
     counted(h);
-    if (gx >= 3)
-        k_csr_proof<3><<<pb, 256, 0, s>>>(n, x, rho, maxS, sc);
-    else if (gx == 2)
-        k_csr_proof<2><<<pb, 256, 0, s>>>(n, x, rho, maxS, sc);
-    else
-        k_csr_proof<1><<<pb, 256, 0, s>>>(n, x, rho, maxS, sc);
-    const int rb = (m + kCsrThreads - 1) / kCsrThreads;
-    if (m > 0) {
-        counted(h);
-        const bool deep = na_hint > 4;
-        const int em = h->splitEpsMode;
-        if (h->sumMode == 1) {
-            if (deep)
-                launch_reg<1, 6>(gx, rb, s, m, n, val, colind, rowptr, x, shift, em, maxS, alpha, beta, y, sc, slow);
-            else
-                launch_reg<1, 4>(gx, rb, s, m, n, val, colind, rowptr, x, shift, em, maxS, alpha, beta, y, sc, slow);
-        } else {
-            if (deep)
-                launch_reg<0, 6>(gx, rb, s, m, n, val, colind, rowptr, x, shift, em, maxS, alpha, beta, y, sc, slow);
-            else
-                launch_reg<0, 4>(gx, rb, s, m, n, val, colind, rowptr, x, shift, em, maxS, alpha, beta, y, sc, slow);
-        }
-    }
-    OZB_CHECK(cudaGetLastError());
+    OZB_TRY(plan_launch(s, &sc->vs, rho, maxS, true, &sc->plan, nullptr));
+    counted(h);
+    OZB_TRY(csr_proof_launch(s, n, x, rho, maxS, sc, nullptr));
+    const CsrmvArgs args{m, n, alpha, beta, val, colind, rowptr, x, y, shift, h->splitEpsMode, maxS, h->sumMode,
+                         na_hint};
+    if (m > 0) counted(h);
+    OZB_TRY(csr_rows_launch(s, args, sc, slow, -1, nullptr, 0, nullptr, nullptr));
     int res[4];  // valid, nB, nslow, zmax (partial until the deferred rows ran)
     OZB_CHECK(cudaMemcpyAsync(res, &sc->valid, sizeof(res), cudaMemcpyDeviceToHost, s));
     OZB_CHECK(cudaStreamSynchronize(s));
@@ -527,18 +645,19 @@ int csrmv_fused(cuozblasHandle_t *h, int m, int n, double alpha, const double *v
     }
     const int nslow = res[2];
     if (nslow > 0) {
-        const int chunk = 8192;
-        double *terms = ar.take<double>((uint64_t)chunk * kMaxSplitDefault * kCsrLv);
+        double *terms = ar.take<double>((uint64_t)kCsrSlowChunk * kMaxSplitDefault * kCsrLv);
         if (!ar.ok) return CUOZBLAS_STATUS_WORKSPACE;
-        for (int c0 = 0; c0 < nslow; c0 += chunk) {
-            const int nr = nslow - c0 < chunk ? nslow - c0 : chunk;
+        for (int c0 = 0; c0 < nslow; c0 += kCsrSlowChunk) {
+            const int nr = nslow - c0 < kCsrSlowChunk ? nslow - c0 : kCsrSlowChunk;
             counted(h);
             if (h->sumMode == 1)
                 k_csrmv_slow<1><<<(nr + 127) / 128, 128, 0, s>>>(nr, slow + c0, val, colind, rowptr, x, shift,
-                                                                h->splitEpsMode, maxS, alpha, beta, y, sc, terms);
+                                                                h->splitEpsMode, maxS, alpha, beta, y, sc, terms,
+                                                                nullptr, 0, nullptr);
             else
                 k_csrmv_slow<0><<<(nr + 127) / 128, 128, 0, s>>>(nr, slow + c0, val, colind, rowptr, x, shift,
-                                                                h->splitEpsMode, maxS, alpha, beta, y, sc, terms);
+                                                                h->splitEpsMode, maxS, alpha, beta, y, sc, terms,
+                                                                nullptr, 0, nullptr);
             OZB_CHECK(cudaGetLastError());
         }
         OZB_CHECK(cudaMemcpyAsync(&res[3], &sc->zmax, sizeof(int), cudaMemcpyDeviceToHost, s));

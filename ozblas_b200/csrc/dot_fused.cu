@@ -30,28 +30,11 @@
 // as the level-by-level chain with a dependency depth of ~3 per group.
 #include <cstring>
 
-#include "chain.cuh"
+#include "fused.h"
 #include "ozb_internal.h"
 #include "sum.cuh"
 
 namespace ozb {
-
-constexpr int kDotLevels = kChainLevels;
-constexpr int kDotThreads = 256;
-constexpr int kDotStages = 8;  // cp.async stages per thread (dynamic shared memory)
-
-struct alignas(8) DotStatus {  // copied to the host in one piece
-    int status, ns0, ns1, pad;
-    double result;
-};
-
-struct DotScratch {
-    VecStats vs;                        // first pass: max, lowest set bit, Inf/NaN of x and y
-    double P[kDotLevels * kDotLevels];  // exact slice products P[ia * 8 + ib]
-    unsigned proven[2];                 // levels whose predicted tau some element proved
-    unsigned ticket;                    // blocks of pass 2 that are done
-    DotStatus out;
-};
 
 // ---- pass 1 ---------------------------------------------------------------
 
@@ -199,14 +182,16 @@ __device__ void dot_finish(DotScratch *sc, const TreePlan &pl, int rho, bool sam
 template <int G, bool SAME, bool ALIGNED>
 __global__ void __launch_bounds__(kDotThreads, 1) k_dot_tree(int n, const double *__restrict__ x,
                                                              const double *__restrict__ y, int rho, int maxS,
-                                                             int sum_mode, DotScratch *__restrict__ sc) {
+                                                             int sum_mode, DotScratch *__restrict__ sc,
+                                                             const int *__restrict__ gate) {
+    if (gate && *gate == 0) return;  // uniform: a captured solver step that is switched off
     __shared__ TreePlan pl;
     extern __shared__ __align__(16) double2 ring_raw[];  // [kDotStages][SAME ? 1 : 2][kDotThreads]
     auto ring = reinterpret_cast<double2(*)[SAME ? 1 : 2][kDotThreads]>(ring_raw);
     __shared__ double red[kDotThreads / 32][kDotLevels * kDotLevels];
     __shared__ int last;
     const int t = threadIdx.x;
-    if (t == 0) make_plan(&sc->vs, rho, maxS, SAME, pl);
+    load_plan(&sc->plan, pl);
     __syncthreads();
     double P[kDotLevels][kDotLevels];
 #pragma unroll
@@ -297,11 +282,18 @@ __global__ void __launch_bounds__(kDotThreads, 1) k_dot_tree(int n, const double
     if (t < kDotLevels * kDotLevels) Pv[t] = __ldcg(&sc->P[t]);
     __syncthreads();
     if (t == 0) dot_finish(sc, pl, rho, SAME, sum_mode, Pv, tmp);
+    __syncthreads();
+    // leave the accumulators zeroed for the next use (replayed graphs skip the memset)
+    if (t < kDotLevels * kDotLevels) sc->P[t] = 0.0;
+    if (t == 0) {
+        sc->proven[0] = sc->proven[1] = 0u;
+        sc->ticket = 0u;
+    }
 }
 
 template <int G, bool SAME>
 static int launch_tree(bool aligned, int grid, cudaStream_t s, int n, const double *x, const double *y, int rho,
-                       int maxS, int sum_mode, DotScratch *sc) {
+                       int maxS, int sum_mode, DotScratch *sc, const int *gate) {
     if (aligned) {
         const int smem = kDotStages * (SAME ? 1 : 2) * kDotThreads * (int)sizeof(double2);
         static bool attr = false;  // once per instantiation
@@ -311,11 +303,78 @@ static int launch_tree(bool aligned, int grid, cudaStream_t s, int n, const doub
                 return CUOZBLAS_STATUS_CUDA_ERROR;
             attr = true;
         }
-        k_dot_tree<G, SAME, true><<<grid, kDotThreads, smem, s>>>(n, x, y, rho, maxS, sum_mode, sc);
+        k_dot_tree<G, SAME, true><<<grid, kDotThreads, smem, s>>>(n, x, y, rho, maxS, sum_mode, sc, gate);
     } else {
-        k_dot_tree<G, SAME, false><<<grid, kDotThreads, 0, s>>>(n, x, y, rho, maxS, sum_mode, sc);
+        k_dot_tree<G, SAME, false><<<grid, kDotThreads, 0, s>>>(n, x, y, rho, maxS, sum_mode, sc, gate);
     }
     return CUOZBLAS_STATUS_SUCCESS;
+}
+
+template <int G, bool SAME>
+static int prepare_tree() {
+    const int smem = kDotStages * (SAME ? 1 : 2) * kDotThreads * (int)sizeof(double2);
+    return cudaFuncSetAttribute(k_dot_tree<G, SAME, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) ==
+                   cudaSuccess
+               ? CUOZBLAS_STATUS_SUCCESS
+               : CUOZBLAS_STATUS_CUDA_ERROR;
+}
+
+int dot_tree_prepare() {
+    int r = 0;
+    r |= prepare_tree<1, true>() | prepare_tree<1, false>() | prepare_tree<2, true>() | prepare_tree<2, false>();
+    r |= prepare_tree<3, true>() | prepare_tree<3, false>() | prepare_tree<4, true>() | prepare_tree<4, false>();
+    return r ? CUOZBLAS_STATUS_CUDA_ERROR : CUOZBLAS_STATUS_SUCCESS;
+}
+
+int dot_scan_launch(cudaStream_t s, int nsm, int n, const double *x, const double *y, DotScratch *sc) {
+    const bool same = (x == y);
+    const bool aligned = ((reinterpret_cast<uintptr_t>(x) | reinterpret_cast<uintptr_t>(y)) & 15u) == 0;
+    int blocks = (int)(((int64_t)n + 2 * kDotThreads - 1) / (2 * kDotThreads));
+    if (blocks > nsm * 8) blocks = nsm * 8;
+    if (blocks < 1) blocks = 1;
+    if (aligned) {
+        if (same)
+            k_dot_scan<true, true><<<blocks, 256, 0, s>>>(n, x, y, sc);
+        else
+            k_dot_scan<true, false><<<blocks, 256, 0, s>>>(n, x, y, sc);
+    } else {
+        if (same)
+            k_dot_scan<false, true><<<blocks, 256, 0, s>>>(n, x, y, sc);
+        else
+            k_dot_scan<false, false><<<blocks, 256, 0, s>>>(n, x, y, sc);
+    }
+    return cudaGetLastError() == cudaSuccess ? CUOZBLAS_STATUS_SUCCESS : CUOZBLAS_STATUS_CUDA_ERROR;
+}
+
+int dot_tree_launch(cudaStream_t s, int nsm, int n, const double *x, const double *y, int rho, int maxS,
+                    int sum_mode, DotScratch *sc, const int *gate) {
+    const int G = chain_group(rho, 4);  // levels cut from one base value
+    const bool same = (x == y);
+    const bool aligned = ((reinterpret_cast<uintptr_t>(x) | reinterpret_cast<uintptr_t>(y)) & 15u) == 0;
+    int fblocks = (int)(((int64_t)n + 2 * kDotThreads - 1) / (2 * kDotThreads));
+    if (fblocks > nsm) fblocks = nsm;  // ~250 registers per thread: one 256-thread block per SM
+    if (fblocks < 1) fblocks = 1;
+    int ls;
+    switch (G) {
+        case 1:
+            ls = same ? launch_tree<1, true>(aligned, fblocks, s, n, x, y, rho, maxS, sum_mode, sc, gate)
+                      : launch_tree<1, false>(aligned, fblocks, s, n, x, y, rho, maxS, sum_mode, sc, gate);
+            break;
+        case 2:
+            ls = same ? launch_tree<2, true>(aligned, fblocks, s, n, x, y, rho, maxS, sum_mode, sc, gate)
+                      : launch_tree<2, false>(aligned, fblocks, s, n, x, y, rho, maxS, sum_mode, sc, gate);
+            break;
+        case 3:
+            ls = same ? launch_tree<3, true>(aligned, fblocks, s, n, x, y, rho, maxS, sum_mode, sc, gate)
+                      : launch_tree<3, false>(aligned, fblocks, s, n, x, y, rho, maxS, sum_mode, sc, gate);
+            break;
+        default:
+            ls = same ? launch_tree<4, true>(aligned, fblocks, s, n, x, y, rho, maxS, sum_mode, sc, gate)
+                      : launch_tree<4, false>(aligned, fblocks, s, n, x, y, rho, maxS, sum_mode, sc, gate);
+            break;
+    }
+    if (ls) return ls;
+    return cudaGetLastError() == cudaSuccess ? CUOZBLAS_STATUS_SUCCESS : CUOZBLAS_STATUS_CUDA_ERROR;
 }
 
 // Returns SUCCESS with *done = true and the result in *ret when the fused
@@ -331,54 +390,14 @@ int dot_fused(cuozblasHandle_t *h, int n, const double *x, const double *y, doub
     if (!ar.ok) return CUOZBLAS_STATUS_WORKSPACE;
     const int maxS = h->nSplitMax > 0 ? h->nSplitMax : kMaxSplitDefault;
     const int rho = rho_rule(n, h->splitEpsMode);
-    const int G = chain_group(rho, 4);  // levels cut from one base value
-    const bool same = (x == y);
-    const bool aligned = ((reinterpret_cast<uintptr_t>(x) | reinterpret_cast<uintptr_t>(y)) & 15u) == 0;
     OZB_CHECK(cudaMemsetAsync(sc, 0, sizeof(DotScratch), st->stream));
-    int dev = 0, nsm = 0;
-    OZB_CHECK(cudaGetDevice(&dev));
-    OZB_CHECK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
-    int blocks = (int)(((int64_t)n + 2 * kDotThreads - 1) / (2 * kDotThreads));
-    if (blocks > nsm * 8) blocks = nsm * 8;
-    if (blocks < 1) blocks = 1;
+    const int nsm = sm_count();
     counted(h);
-    if (aligned) {
-        if (same)
-            k_dot_scan<true, true><<<blocks, 256, 0, st->stream>>>(n, x, y, sc);
-        else
-            k_dot_scan<true, false><<<blocks, 256, 0, st->stream>>>(n, x, y, sc);
-    } else {
-        if (same)
-            k_dot_scan<false, true><<<blocks, 256, 0, st->stream>>>(n, x, y, sc);
-        else
-            k_dot_scan<false, false><<<blocks, 256, 0, st->stream>>>(n, x, y, sc);
-    }
-    int fblocks = (int)(((int64_t)n + 2 * kDotThreads - 1) / (2 * kDotThreads));
-    if (fblocks > nsm) fblocks = nsm;  // ~250 registers per thread: one 256-thread block per SM
-    if (fblocks < 1) fblocks = 1;
+    OZB_TRY(dot_scan_launch(st->stream, nsm, n, x, y, sc));
     counted(h);
-    cudaStream_t s = st->stream;
-    int ls;
-    switch (G) {
-        case 1:
-            ls = same ? launch_tree<1, true>(aligned, fblocks, s, n, x, y, rho, maxS, h->sumMode, sc)
-                      : launch_tree<1, false>(aligned, fblocks, s, n, x, y, rho, maxS, h->sumMode, sc);
-            break;
-        case 2:
-            ls = same ? launch_tree<2, true>(aligned, fblocks, s, n, x, y, rho, maxS, h->sumMode, sc)
-                      : launch_tree<2, false>(aligned, fblocks, s, n, x, y, rho, maxS, h->sumMode, sc);
-            break;
-        case 3:
-            ls = same ? launch_tree<3, true>(aligned, fblocks, s, n, x, y, rho, maxS, h->sumMode, sc)
-                      : launch_tree<3, false>(aligned, fblocks, s, n, x, y, rho, maxS, h->sumMode, sc);
-            break;
-        default:
-            ls = same ? launch_tree<4, true>(aligned, fblocks, s, n, x, y, rho, maxS, h->sumMode, sc)
-                      : launch_tree<4, false>(aligned, fblocks, s, n, x, y, rho, maxS, h->sumMode, sc);
-            break;
-    }
-    if (ls) return ls;
-    OZB_CHECK(cudaGetLastError());
+    OZB_TRY(plan_launch(st->stream, &sc->vs, rho, maxS, x == y, &sc->plan, nullptr));
+    counted(h);
+    OZB_TRY(dot_tree_launch(st->stream, nsm, n, x, y, rho, maxS, h->sumMode, sc, nullptr));
     static_assert(sizeof(DotStatus) == 24, "status block layout");
     OZB_CHECK(cudaMemcpyAsync(st->h_dbl, &sc->out, sizeof(DotStatus), cudaMemcpyDeviceToHost, st->stream));
     OZB_CHECK(cudaStreamSynchronize(st->stream));

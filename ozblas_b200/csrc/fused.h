@@ -1,0 +1,74 @@
+// fused.h — scratch layouts and launch helpers of the fused DOT and CSRMV,
+// shared by their host wrappers and the graph-captured CG.
+#pragma once
+#include "chain.cuh"
+#include "ozb_internal.h"
+
+namespace ozb {
+
+constexpr int kDotLevels = kChainLevels;
+constexpr int kDotThreads = 256;
+constexpr int kDotStages = 8;  // cp.async stages per thread (dynamic shared memory)
+
+struct alignas(8) DotStatus {  // copied to the host in one piece
+    int status, ns0, ns1, pad;
+    double result;
+};
+
+struct DotScratch {
+    VecStats vs;                        // first pass: max, lowest set bit, Inf/NaN of x and y
+    TreePlan plan;                      // the chains planned from vs (plan_launch)
+    double P[kDotLevels * kDotLevels];  // exact slice products P[ia * 8 + ib]
+    unsigned proven[2];                 // levels whose predicted tau some element proved
+    unsigned ticket;                    // blocks of pass 2 that are done
+    DotStatus out;
+};
+
+constexpr int kCsrLv = kChainLevels;  // levels of x computed / proven
+constexpr int kCsrRowMax = 8;         // entries per row held on chip
+constexpr int kCsrThreads = 128;
+
+struct CsrScratch {
+    VecStats vs;                 // first pass over x
+    TreePlan plan;               // x's chain planned from vs (plan_launch)
+    unsigned proven;             // levels of x's chain whose predicted tau some element proved
+    unsigned ticket;             // blocks of the proof pass that are done
+    int valid, nB, nslow, zmax;  // zmax: first zero-remainder level of A, max over rows
+    double sigma[kCsrLv];        // x's proven sigmas
+};
+
+// DOT: the first pass (max, lowest set bit) into sc->vs, and the second
+// pass, which leaves the result and status in sc->out and its accumulators
+// zeroed.  `gate` (device int, may be null): the kernel does nothing when 0.
+int dot_scan_launch(cudaStream_t s, int nsm, int n, const double *x, const double *y, DotScratch *sc);
+int dot_tree_launch(cudaStream_t s, int nsm, int n, const double *x, const double *y, int rho, int maxS,
+                    int sum_mode, DotScratch *sc, const int *gate);
+// Sets the kernels' shared-memory attribute up front (before a capture).
+int dot_tree_prepare();
+
+// Plans the chain(s) from the first pass's statistics once, into `plan`,
+// and zeroes the statistics for the next use (one thread; `gate` as above).
+int plan_launch(cudaStream_t s, VecStats *vs, int rho, int maxS, bool same, TreePlan *plan, const int *gate);
+
+// CSRMV pieces (csrmv_fused.cu): statistics of a vector into vs[index]; the
+// rows the row kernel defers (a property of the matrix); proof of x's chain
+// (publishes sc->valid, nB, sigma, zeroes sc->vs); the row kernel.  With
+// `fixed_slow` >= 0 the deferred rows are the given list (no appends);
+// `ystats` (may be null) collects max / lowest bit of the written y.
+struct CsrmvArgs {
+    int m, n;
+    double alpha, beta;
+    const double *val;
+    const int *colind, *rowptr;
+    const double *x;
+    double *y;
+    int shift, epsmode, maxS, sum_mode, na_hint;
+};
+int vec_stats_launch(cudaStream_t s, int nsm, int n, const double *x, VecStats *vs, int index);
+int csr_slow_rows_launch(cudaStream_t s, int m, const double *val, const int *rowptr, int shift, int epsmode,
+                         int maxS, int na_hint, int *list, int *count);
+int csr_proof_launch(cudaStream_t s, int n, const double *x, int rho, int maxS, CsrScratch *sc, const int *gate);
+int csr_rows_launch(cudaStream_t s, const CsrmvArgs &a, CsrScratch *sc, int *slow, int fixed_slow,
+                    VecStats *ystats, int ystats_index, double *terms, const int *gate);
+
+}  // namespace ozb

@@ -86,6 +86,19 @@ inline int cuda_status(cudaError_t e) { return e == cudaSuccess ? CUOZBLAS_STATU
 
 inline bool is_trans(char t) { return !(t == 'n' || t == 'N'); }
 
+// Streaming multiprocessors of the current device (cached per device).
+inline int sm_count() {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    static int cache[64] = {0};
+    if (dev >= 0 && dev < 64 && cache[dev] > 0) return cache[dev];
+    int n = 0;
+    cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+    if (n < 1) n = 1;
+    if (dev >= 0 && dev < 64) cache[dev] = n;
+    return n;
+}
+
 // Reference counterInit (src/cuda/cuozblas.cpp:3-21): resets the exec info,
 // splitShift and the arena pointer (keeping a pre-split A below memMaskSplitA).
 int counter_init(cuozblasHandle_t *h);
