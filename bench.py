@@ -175,6 +175,8 @@ def main():
     ap.add_argument("--memory-only", action="store_true",
                     help="only the DOT / CSRMV / CG measurements (for profiling them; prints their JSON)")
     ap.add_argument("--cg-iters", type=int, default=2000, help="CG iterations of the memory-only run")
+    ap.add_argument("--batched-only", action="store_true",
+                    help="only the 256-problem grouped INT8 measurement (prints its JSON)")
     args = ap.parse_args()
     globals()["N_DIM"] = args.n
     args.warmup = max(args.warmup, 3)
@@ -192,6 +194,12 @@ def main():
     import ozblas_b200 as ozb
 
     torch.cuda.set_device(local)
+    if args.batched_only:
+        h = ozb.Handle(work_bytes=24 << 30)
+        print(json.dumps({"workload": "batched uneven Ozaki DGEMM, 256 problems", "reps": args.steps,
+                          "extras": batched_extras(ozb, h, torch, reps=args.steps)}))
+        h.close()
+        return 0
     if args.memory_only:
         h = ozb.Handle(work_bytes=8 << 30)
         h.nSplitMax = 0
@@ -370,6 +378,104 @@ def extras(ozb, h, torch, A, B, C, n):
     del C_tri, C_full, C_plain
     torch.cuda.empty_cache()
     out.update(memory_extras(ozb, h, torch))
+    out["batched_uneven_256"] = batched_extras(ozb, h, torch)
+    return out
+
+
+def batched_case(count=256, seed=5):
+    """256 problems, m, n, k log-uniform in [64, 2048] (shape seed 5), phi from {0.5, 1, 2, 4}; problem i's A and B
+    use seeds 1000 + 2i and 1001 + 2i.  Host arrays (column-major, as phi_matrix)."""
+    import numpy as np
+
+    g = np.random.default_rng(seed)
+    mnk = np.exp(g.uniform(np.log(64), np.log(2048), (count, 3))).astype(int)
+    phis = g.choice([0.5, 1.0, 2.0, 4.0], count)
+    probs = []
+    for i in range(count):
+        m, n, k = (int(v) for v in mnk[i])
+        probs.append((m, n, k, float(phis[i]), phi_matrix(m, k, phis[i], 1000 + 2 * i),
+                      phi_matrix(k, n, phis[i], 1001 + 2 * i)))
+    return probs
+
+
+def batched_extras(ozb, h, torch, reps=3):
+    """Config 5: 256 uneven problems in one grouped INT8 launch vs the same problems looped through the single INT8
+    call and through the plain FP64-slice form; max relative error against the correctly rounded product."""
+    probs = batched_case()
+    flops = sum(2.0 * m * n * k for m, n, k, _, _, _ in probs)
+    As = [torch.from_numpy(A).cuda() for *_, A, _ in probs]
+    Bs = [torch.from_numpy(B).cuda() for *_, B in probs]
+    Cs = [torch.zeros((n, m), dtype=torch.float64, device="cuda") for m, n, *_ in probs]
+    ms, ns, ks = [p[0] for p in probs], [p[1] for p in probs], [p[2] for p in probs]
+    one, zero = [1.0] * len(probs), [0.0] * len(probs)
+
+    def timed(fn, reps):
+        fn()
+        torch.cuda.synchronize()
+        ts = []
+        for _ in range(reps):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            fn()
+            e1.record()
+            torch.cuda.synchronize()
+            ts.append(e0.elapsed_time(e1))
+        return min(ts)
+
+    out = {"problems": len(probs), "flops_effective": flops}
+    for fast in (0, 1):
+        h.nSplitMax, h.fastMode = 0, fast
+        l0 = h.launch_count()
+        ms_b = timed(lambda: ozb.dgemm_i8_batched(h, "n", "n", ms, ns, ks, one, As, ms, Bs, ks, zero, Cs, ms), reps)
+        launches = (h.launch_count() - l0) / (reps + 1)
+        slices = [h.nSplitA, h.nSplitB]
+        C_batched = [c.clone() for c in Cs]
+
+        def looped():
+            for i in range(len(probs)):
+                ozb.dgemm_i8(h, "n", "n", ms[i], ns[i], ks[i], 1.0, As[i], ms[i], Bs[i], ks[i], 0.0, Cs[i], ms[i])
+
+        ms_l = timed(looped, 1)
+        key = "full" if fast == 0 else "triangular"
+        out[f"int8_grouped_{key}"] = {"ms": ms_b, "TFLOPS": flops / ms_b / 1e9, "launches": launches,
+                                      "max_slices": slices}
+        out[f"int8_looped_{key}"] = {"ms": ms_l, "TFLOPS": flops / ms_l / 1e9}
+        out[f"grouped_identical_to_looped_{key}"] = all(bool(torch.equal(a, b)) for a, b in zip(C_batched, Cs))
+        if fast == 0:
+            C_full = C_batched
+    h.fastMode = 0
+
+    def plain():
+        for i in range(len(probs)):
+            ozb.dgemm(h, "n", "n", ms[i], ns[i], ks[i], 1.0, As[i], ms[i], Bs[i], ks[i], 0.0, Cs[i], ms[i])
+
+    ms_p = timed(plain, 1)
+    out["plain_fp64_slices_looped"] = {"ms": ms_p, "TFLOPS": flops / ms_p / 1e9}
+    C_fsum = [c.clone() for c in Cs]
+    h.sumMode = 1
+    plain()  # correctly rounded products
+    torch.cuda.synchronize()
+    h.sumMode = 0
+
+    def worst(X):
+        w, cnt, where = 0.0, 0, None
+        for i, (a, b) in enumerate(zip(X, Cs)):
+            d = ((a - b).abs() / b.abs()).nan_to_num(nan=0.0, posinf=float("inf"))
+            d = torch.where(b == 0, (a != 0).double() * float("inf"), d)
+            di = float(d.max().item())
+            if di > w:
+                j = int(d.argmax().item())
+                w, where = di, {"problem": i, "m": ms[i], "n": ns[i], "k": ks[i], "phi": probs[i][3],
+                                "value": float(a.flatten()[j].item()), "correctly_rounded": float(b.flatten()[j].item())}
+            cnt += int((a != b).sum().item())
+        return w, cnt, where
+
+    (e_i8, n_i8, w_i8), (e_fs, n_fs, w_fs) = worst(C_full), worst(C_fsum)
+    out["max_rel_err_vs_correctly_rounded"] = {"int8_full": e_i8, "plain_fsum": e_fs,
+                                               "inexact_entries": {"int8_full": n_i8, "plain_fsum": n_fs},
+                                               "entries": sum(m * n for m, n, *_ in probs),
+                                               "worst_int8": w_i8, "worst_fsum": w_fs}
+    out["speedup_grouped_full_vs_plain_looped"] = ms_p / out["int8_grouped_full"]["ms"]
     return out
 
 

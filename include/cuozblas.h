@@ -193,6 +193,19 @@ int cuozblasDgemmI8(cuozblasHandle_t *h, char transa, char transb, int32_t m, in
                     const double *A, int32_t lda, const double *B, int32_t ldb, double beta, double *C,
                     int32_t ldc);
 
+/* Many INT8 precision-form DGEMMs of different shapes in one persistent
+ * grouped launch.  No counterpart in the reference (its batched path,
+ * src/cuda/cuozblas_gemm.cu:165-178, batches the slice pairs of one
+ * product).  Arrays of `count` entries in host memory; A[b], B[b], C[b] are
+ * device pointers (column-major, as cuozblasDgemmI8).  Every problem's
+ * result is bit-identical to cuozblasDgemmI8 on it with the same handle
+ * flags (nSplitMax, fastMode).  nSplitA/B report the largest digit counts,
+ * nSplitC the largest pair count. */
+int cuozblasDgemmI8Batched(cuozblasHandle_t *h, char transa, char transb, int32_t count, const int32_t *m,
+                           const int32_t *n, const int32_t *k, const double *alpha, const double *const *A,
+                           const int32_t *lda, const double *const *B, const int32_t *ldb, const double *beta,
+                           double *const *C, const int32_t *ldc);
+
 /* Allocation-free INT8 precision-form DGEMM.  No counterpart in the
  * reference.  For callers that cannot allocate device memory (work recorded
  * while a CUDA graph is being captured, hosts whose device memory is

@@ -25,7 +25,7 @@ LIB_PATH = os.path.join(_HERE, "libcuozblas_b200.so")
 
 if not os.path.exists(LIB_PATH):
     raise ImportError(
-        f"{LIB_PATH} is missing: build it with `python -m ozblas_b200.build` (nvcc, sm_100a). "
+        f"{LIB_PATH} is missing: build it with `python ozblas_b200/build.py` (nvcc, sm_100a). "
         "ozblas_b200 has no CPU fallback.")
 
 _lib = C.CDLL(LIB_PATH)
@@ -89,6 +89,9 @@ _dgemm = _sig("cuozblasDgemm", [_HP, _ch, _ch, _i32, _i32, _i32, _d, _vp, _i32, 
 _dgemm_i8 = _sig("cuozblasDgemmI8", [_HP, _ch, _ch, _i32, _i32, _i32, _d, _vp, _i32, _vp, _i32, _d, _vp, _i32])
 _dgemm_i8_static = _sig("cuozblasDgemmI8Static", [_ch, _ch, _i32, _i32, _i32, _d, _vp, _i32, _vp, _i32, _d, _vp,
                                                   _i32, _i32, _i32, _vp])
+_PI32, _PD, _PVP = C.POINTER(_i32), C.POINTER(_d), C.POINTER(_vp)
+_dgemm_i8_batched = _sig("cuozblasDgemmI8Batched", [_HP, _ch, _ch, _i32, _PI32, _PI32, _PI32, _PD, _PVP, _PI32, _PVP,
+                                                    _PI32, _PD, _PVP, _PI32])
 _dcsrmv = _sig("cuozblasDcsrmv", [_HP, _ch, _i32, _i32, _i32, _d, _vp, _vp, _vp, _vp, _vp, _d, _vp])
 _dsplita = _sig("cuozblasDcsrmvSplitA", [_HP, _ch, _i32, _i32, _i32, _vp, _vp, _vp, C.POINTER(_vp)])
 _dcg = _sig("cuozblasDcg", [_HP, _ch, _i32, _i32, _vp, _vp, _vp, _vp, _vp, _vp, _i32, _d])
@@ -100,7 +103,8 @@ _version = _sig("cuozblasVersion", [], C.c_char_p)
 C_ABI_SYMBOLS = [
     "cuozblasHandleCreate", "cuozblasHandleDestroy", "cuozblasSetStream", "cuozblasGetLaunchCount", "cuozblasDdot", "cuozblasDnrm2",
     "cuozblasDaxpy", "cuozblasDgemv", "cuozblasDgemm", "cuozblasDcsrmv", "cuozblasDcsrmvSplitA", "cuozblasDcg",
-    "cuozblasDgemmI8", "cuozblasDgemmI8Static", "cuozblasRuleTau", "cuozblasRuleRho", "cuozblasVersion",
+    "cuozblasDgemmI8", "cuozblasDgemmI8Static", "cuozblasDgemmI8Batched", "cuozblasRuleTau", "cuozblasRuleRho",
+    "cuozblasVersion",
 ]
 
 
@@ -173,6 +177,16 @@ def dgemm(h, ta, tb, m, n, k, alpha, A, lda, B, ldb, beta, Cm, ldc):
 def dgemm_i8(h, ta, tb, m, n, k, alpha, A, lda, B, ldb, beta, Cm, ldc):
     _chk("cuozblasDgemmI8", _dgemm_i8(h.ref, ta.encode(), tb.encode(), m, n, k, alpha, _ptr(A), lda, _ptr(B),
                                       ldb, beta, _ptr(Cm), ldc))
+
+
+def dgemm_i8_batched(h, ta, tb, ms, ns, ks, alphas, As, ldas, Bs, ldbs, betas, Cs, ldcs):
+    """Many INT8 DGEMMs of different shapes in one grouped launch; per-problem lists (device buffers for A, B, C)."""
+    cnt = len(ms)
+    arr = lambda t, v: (t * cnt)(*v)
+    _chk("cuozblasDgemmI8Batched", _dgemm_i8_batched(
+        h.ref, ta.encode(), tb.encode(), cnt, arr(_i32, ms), arr(_i32, ns), arr(_i32, ks), arr(_d, alphas),
+        arr(_vp, [_ptr(a) for a in As]), arr(_i32, ldas), arr(_vp, [_ptr(b) for b in Bs]), arr(_i32, ldbs),
+        arr(_d, betas), arr(_vp, [_ptr(c) for c in Cs]), arr(_i32, ldcs)))
 
 
 def dgemm_i8_static(ta, tb, m, n, k, alpha, A, lda, B, ldb, beta, Cm, ldc, nSplitMax=0, fastMode=0, stream=None):

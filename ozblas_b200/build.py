@@ -1,6 +1,7 @@
 """Build libcuozblas_b200.so in-tree with nvcc for sm_100a.
 
-    python -m ozblas_b200.build            # or: python ozblas_b200/build.py
+    python ozblas_b200/build.py           (loads no package code, so it works
+                                          before the library exists)
 
 Every .cu/.cpp under ozblas_b200/csrc is compiled for
 ``-gencode arch=compute_100a,code=sm_100a`` and linked into one shared

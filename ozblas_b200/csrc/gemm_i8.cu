@@ -13,14 +13,17 @@
 // of one level share the scale, so they accumulate in one INT32 tensor-memory
 // accumulator; a group holds at most floor((2^31 - 1) / (127^2)) products per
 // output, which keeps every partial sum exact (k is chunked beyond that).
-// Sum: levels are visited from the smallest (highest L) to the largest.  Runs
-// of consecutive levels, formed from level 0 upward, are first combined
+// Sum: levels are visited from the largest (L = 0) to the smallest.  Runs of
+// consecutive levels, formed from level 0 upward, are first combined
 // exactly, as an integer below 2^53 held in an FP64 register (V_L shifted by
 // 7 bits per level); each run is then added once to the FP64 sum R, which
-// lives in tensor memory.  With a
-// complete split this makes the output correctly rounded except when the
-// exact value sits within ~2^-28 ulp of a rounding boundary.  Finally
-// t = R * 2^(EA_i + EB_j) and C = fma(alpha, t, beta * C).
+// lives in tensor memory, the most significant run first.  A cancellation
+// between runs therefore happens while R is still exact (the difference of
+// the two leading runs is representable), and each later run, 2^-28 or less
+// of R, moves it by at most one rounding: with a complete split the output
+// is within one ulp of the correctly rounded product, also when the exact
+// value is far smaller than its products.  Finally t = R * 2^(EA_i + EB_j)
+// and C = fma(alpha, t, beta * C).
 //
 // Kernel: persistent, one CTA per SM, warp-specialised:
 //   warp 0      TMA producer (128 x 128-byte tiles, 128-byte swizzle)
@@ -430,8 +433,8 @@ static int split_digits(cuozblasHandle_t *h, bool strided, int nl, int k, const 
     State *st = state(h);
     const double *src = X;
     int lds = ldx;
-    if (strided) {
-        double *tmp = ar.take<double>((uint64_t)nl * (k > 0 ? k : 1));
+    if (strided && k > 0) {
+        double *tmp = ar.take<double>((uint64_t)nl * k);
         if (!ar.ok) return CUOZBLAS_STATUS_WORKSPACE;
         OZB_TRY(transpose(h, nl, k, X, ldx, tmp, k));
         src = tmp;
@@ -461,31 +464,22 @@ static int split_digits(cuozblasHandle_t *h, bool strided, int nl, int k, const 
     return CUOZBLAS_STATUS_SUCCESS;
 }
 
-// Default digit cap when nSplitMax is 0 (enough for an exact split of
-// values whose lines span ~2^80; larger spans are truncated).
-constexpr int kI8DefaultCap = 19;
-
-int gemm_i8_core(cuozblasHandle_t *h, char ta, char tb, int m, int n, int k, double alpha, const double *A, int lda,
-                 const double *B, int ldb, double beta, double *C, int ldc) {
-    State *st = state(h);
-    Arena ar(h);
-    const int k_pad = (k + I8_BK - 1) / I8_BK * I8_BK;
-    const int cap = h->nSplitMax > 0 ? h->nSplitMax : kI8DefaultCap;
-    DigitOperand da, db;
-    ev_record(h, 0);
-    OZB_TRY(split_digits(h, !is_trans(ta), m, k, A, lda, cap, k_pad, I8_BM, da, ar));
-    ev_record(h, 1);
-    OZB_TRY(split_digits(h, is_trans(tb), n, k, B, ldb, cap, k_pad, I8_BN, db, ar));
-    const int nA = da.S, nB = db.S;
-    // pair set: full, or the triangle ia + ib <= min(nA, nB) - 1 (fastMode, src/cuda/cuozblas_gemm.cu:138)
-    const int maxlevel = h->fastMode ? (nA < nB ? nA : nB) - 1 : nA + nB - 2;
-    const int nkb = k_pad / I8_BK;
+// The schedule of one product: items {ia, ib, kb0, kb1} (a digit pair over a
+// range of 128-k blocks) grouped per level into INT32 groups of at most
+// I8_MAX_TERMS products per output, levels visited from the largest, and the
+// runs of levels that combine exactly below 2^53 (group meta: shift |
+// flush << 8 | first << 9 | last << 10, group.z the flush exponent).  Pair
+// set: full, or the triangle ia + ib <= min(nA, nB) - 1
+// (src/cuda/cuozblas_gemm.cu:138).  Returns the number of pairs.
+int i8_schedule(int nA, int nB, int nkb, bool triangular, std::vector<int4> &items, std::vector<int4> &groups) {
+    const int maxlevel = triangular ? (nA < nB ? nA : nB) - 1 : nA + nB - 2;
     // products per output in one INT32 group: (kb1 - kb0) * 128 each
     const int64_t kb_cap = I8_MAX_TERMS / I8_BK;  // k-blocks per group
-    std::vector<int4> items, groups;
+    items.clear();
+    groups.clear();
     std::vector<int64_t> gbound;  // max |V| of each group (products x 127^2)
     int npairs = 0;
-    for (int L = maxlevel; L >= 0; L--) {  // smallest level sums first
+    for (int L = 0; L <= maxlevel; L++) {  // largest level sums first
         const int lo = L - (nB - 1) > 0 ? L - (nB - 1) : 0, hi = L < nA - 1 ? L : nA - 1;
         int64_t used = 0;
         int gbeg = (int)items.size();
@@ -514,9 +508,11 @@ int gemm_i8_core(cuozblasHandle_t *h, char ta, char tb, int m, int n, int k, dou
     // Runs of consecutive levels whose exact combination stays below 2^53,
     // formed from the most significant level up (levels 0..3, 4..7, ...):
     // extending a run [L_lo, L_hi] by L_hi + 1 multiplies its bound by 2^7 and
-    // adds the new level's bound.  Groups are visited in descending level
-    // order; level L of run [L_lo, L_hi] is shifted by 7 (L_hi - L) bits and
-    // the run's last visited group (level L_lo) flushes acc * 2^(-7 (L_hi + 2)).
+    // adds the new level's bound.  Groups are visited in ascending level order
+    // (largest sums first, so a cancellation between runs happens while the
+    // FP64 sum is still exact); level L of run [L_lo, L_hi] is shifted by
+    // 7 (L_hi - L) bits and the run's last visited group (level L_hi) flushes
+    // acc * 2^(-7 (L_hi + 2)).
     {
         std::vector<unsigned __int128> lbound(maxlevel + 1, 0);
         for (size_t g = 0; g < groups.size(); g++) lbound[groups[g].z] += (unsigned __int128)gbound[g];
@@ -540,7 +536,7 @@ int gemm_i8_core(cuozblasHandle_t *h, char ta, char tb, int m, int n, int k, dou
             const int L = groups[g].z;
             int meta = 7 * (run_hi[L] - L);
             const bool last_of_level = (g + 1 == groups.size()) || groups[g + 1].z != L;
-            if (last_of_level && L == run_lo[L]) {
+            if (last_of_level && L == run_hi[L]) {
                 meta |= (1 << 8) | (first ? (1 << 9) : 0);
                 first = false;
                 groups[g].z = -7 * (run_hi[L] + 2);
@@ -549,8 +545,30 @@ int gemm_i8_core(cuozblasHandle_t *h, char ta, char tb, int m, int n, int k, dou
             }
             groups[g].w = meta;
         }
-        groups.back().w |= (1 << 10);
+        if (!groups.empty()) groups.back().w |= (1 << 10);
     }
+    return npairs;
+}
+
+// Default digit cap when nSplitMax is 0 (enough for an exact split of
+// values whose lines span ~2^80; larger spans are truncated).
+constexpr int kI8DefaultCap = 19;
+
+int gemm_i8_core(cuozblasHandle_t *h, char ta, char tb, int m, int n, int k, double alpha, const double *A, int lda,
+                 const double *B, int ldb, double beta, double *C, int ldc) {
+    State *st = state(h);
+    Arena ar(h);
+    const int k_pad = k > 0 ? (k + I8_BK - 1) / I8_BK * I8_BK : I8_BK;  // k = 0: zero digits, C = beta * C
+    const int cap = h->nSplitMax > 0 ? h->nSplitMax : kI8DefaultCap;
+    DigitOperand da, db;
+    ev_record(h, 0);
+    OZB_TRY(split_digits(h, !is_trans(ta), m, k, A, lda, cap, k_pad, I8_BM, da, ar));
+    ev_record(h, 1);
+    OZB_TRY(split_digits(h, is_trans(tb), n, k, B, ldb, cap, k_pad, I8_BN, db, ar));
+    const int nA = da.S, nB = db.S;
+    const int nkb = k_pad / I8_BK;
+    std::vector<int4> items, groups;
+    const int npairs = i8_schedule(nA, nB, nkb, h->fastMode != 0, items, groups);
     h->nSplitA = (float)nA;
     h->nSplitB = (float)nB;
     h->nSplitC = (float)npairs;
@@ -740,7 +758,7 @@ static int dgemm_i8_static(char ta, char tb, int m, int n, int k, double alpha, 
     int4 items[kI8StaticMaxItems], groups[kI8StaticMaxGroups];
     int64_t gbound[kI8StaticMaxGroups];
     int ni = 0, ng = 0;
-    for (int L = maxlevel; L >= 0; L--) {
+    for (int L = 0; L <= maxlevel; L++) {
         const int lo = L - (nB - 1) > 0 ? L - (nB - 1) : 0, hi = L < nA - 1 ? L : nA - 1;
         int64_t used = 0;
         int gbeg = ni;
@@ -793,7 +811,7 @@ static int dgemm_i8_static(char ta, char tb, int m, int n, int k, double alpha, 
             const int L = groups[g].z;
             int meta = 7 * (run_hi[L] - L);
             const bool last_of_level = (g + 1 == ng) || groups[g + 1].z != L;
-            if (last_of_level && L == run_lo[L]) {
+            if (last_of_level && L == run_hi[L]) {
                 meta |= (1 << 8) | (first ? (1 << 9) : 0);
                 first = false;
                 groups[g].z = -7 * (run_hi[L] + 2);

@@ -1,0 +1,683 @@
+// gemm_i8_grouped.cu — many INT8-form Ozaki DGEMMs of different shapes in one
+// persistent grouped launch (cuozblasDgemmI8Batched).
+//
+// The arithmetic is that of gemm_i8.cu (line exponents, truncated 7-bit
+// digits, levels, INT32 groups of at most 133143 products, exact runs of
+// levels, the FP64 sum in tensor memory), so each problem's result is
+// bit-identical to a cuozblasDgemmI8 call on it.  What changes, so that
+// problems of any shape share one kernel:
+//  * operands are split straight into tiles: every 128-line x 128-k block of
+//    a digit level is 16 KiB and is stored with the tensor core's 128-byte
+//    swizzle already applied (row r at r * 128, its 16-byte chunk c at chunk
+//    position c ^ (r & 7)), so the producer fetches it with one contiguous
+//    bulk copy and no per-problem tensor map exists;
+//  * the split reads either layout of an operand in coalesced order (lines
+//    contiguous, or k contiguous), so no transposed copy is made;
+//  * the host lists every problem's output tiles, estimates each tile's cost
+//    from its schedule (k-blocks of all pairs plus the sums) and deals the
+//    tiles longest first onto the least loaded CTA; the producer, MMA and
+//    epilogue warps of a CTA walk that same list.
+#include <cuda.h>
+
+#include <algorithm>
+#include <functional>
+#include <queue>
+#include <vector>
+
+#include "ozb_device.cuh"
+#include "ozb_internal.h"
+#include "tc05.cuh"
+
+namespace ozb {
+
+constexpr int G_T = 128;                    // lines and k per tile
+constexpr int G_TILE_BYTES = G_T * G_T;     // one digit tile
+constexpr int G_NST = 6, G_THREADS = 320, G_TMEM_COLS = 512, G_RCOL = 256;
+constexpr int G_STAGE = 2 * G_TILE_BYTES;
+constexpr int G_SMEM = G_NST * G_STAGE + 1024 + 256;
+constexpr int64_t G_MAX_TERMS = 2147483647LL / (127 * 127);
+constexpr uint64_t G_WAIT_NS = 2000000000ull;
+enum { GERR_PRODUCER = 1, GERR_MMA = 2, GERR_EPI = 3 };
+
+// One operand of one problem.  Element (line l, k index kk) of op(X) is
+// X[l + kk * ld] when lines are contiguous (kcontig = 0) or X[l * ld + kk].
+struct GOp {
+    const double *X;
+    int ld, lines, k, kcontig;
+    int tiles_l, nkb, S;
+    int *e;                  // line exponents
+    unsigned long long *mx;  // per-line max |x| (bit pattern)
+    int *lsb;                // per-line lowest set bit of a nonzero element
+    int8_t *digits;          // S x tiles_l x nkb tiles
+};
+
+struct GProb {
+    int m, n, ldc, nkb, tiles_m, tiles_n;
+    int group0, n_groups;
+    const int8_t *da, *db;
+    const int *ea, *eb;
+    double alpha, beta;
+    double *C;
+};
+
+struct GParams {
+    const GProb *probs;
+    const int4 *items;      // {ia, ib, kb0, kb1}
+    const int4 *groups;     // {item_begin, item_end, flush exponent, meta}, absolute item indices
+    const int4 *tiles;      // {problem, tm, tn, 0}
+    const int *cta_begin;   // CTA c runs tiles [cta_begin[c], cta_begin[c + 1])
+    int *err;
+};
+
+__device__ __forceinline__ int g_exp_above(double v) {  // E with v < 2^E, v > 0
+    const uint64_t b = dbits(v) & 0x7fffffffffffffffULL;
+    const int be = (int)(b >> 52);
+    if (be == 0) {
+        const uint64_t f = b & ((1ULL << 52) - 1);
+        if (f == 0) return 0;
+        return (63 - clz64(f)) - 1073;
+    }
+    return be - 1022;
+}
+
+__device__ __forceinline__ int g_lsb(double v) {  // exponent of the lowest set bit, v != 0
+    const uint64_t b = dbits(v) & 0x7fffffffffffffffULL;
+    const int be = (int)(b >> 52);
+    uint64_t f = b & ((1ULL << 52) - 1);
+    if (be == 0) return -1074 + __ffsll((long long)f) - 1;
+    f |= (1ULL << 52);
+    return (be - 1075) + __ffsll((long long)f) - 1;
+}
+
+__device__ __forceinline__ void g_stat(double v, double &mx, int &lsb) {
+    mx = ref_max(mx, fabs(v));
+    if (v != 0.0) lsb = min(lsb, g_lsb(v));
+}
+
+// Per-line max and lowest set bit of one 128 x 128 block (op, line tile, k block).
+__global__ void __launch_bounds__(256) k_g_stats(const int4 *__restrict__ blocks, const GOp *__restrict__ ops) {
+    const int4 bk = blocks[blockIdx.x];
+    const GOp o = ops[bk.x];
+    const int l0 = bk.y * G_T, k0 = bk.z * G_T;
+    const int t = threadIdx.x;
+    if (!o.kcontig) {
+        __shared__ double smx[256];
+        __shared__ int slsb[256];
+        const int l = l0 + (t & 127), kh = k0 + (t >> 7) * 64;
+        double mx = 0.0;
+        int lsb = 0x7fffffff;
+        if (l < o.lines) {
+#pragma unroll 8
+            for (int j = 0; j < 64; j++) {
+                const int kk = kh + j;
+                if (kk < o.k) g_stat(o.X[(size_t)l + (size_t)kk * o.ld], mx, lsb);
+            }
+        }
+        smx[t] = mx;
+        slsb[t] = lsb;
+        __syncthreads();
+        if (t < 128 && l < o.lines) {
+            mx = ref_max(smx[t], smx[t + 128]);
+            lsb = min(slsb[t], slsb[t + 128]);
+            if (mx > 0.0) atomicMax(&o.mx[l], (unsigned long long)__double_as_longlong(mx));
+            if (lsb != 0x7fffffff) atomicMin(&o.lsb[l], lsb);
+        }
+    } else {
+        const int w = t >> 5, lane = t & 31;
+        for (int i = 0; i < G_T / 8; i++) {
+            const int l = l0 + w + 8 * i;
+            if (l >= o.lines) break;  // uniform per warp
+            double mx = 0.0;
+            int lsb = 0x7fffffff;
+#pragma unroll
+            for (int q = 0; q < 4; q++) {
+                const int kk = k0 + 4 * lane + q;
+                if (kk < o.k) g_stat(o.X[(size_t)l * o.ld + kk], mx, lsb);
+            }
+            for (int s = 16; s > 0; s >>= 1) {
+                mx = ref_max(mx, __shfl_xor_sync(0xffffffffu, mx, s));
+                lsb = min(lsb, __shfl_xor_sync(0xffffffffu, lsb, s));
+            }
+            if (lane == 0) {
+                if (mx > 0.0) atomicMax(&o.mx[l], (unsigned long long)__double_as_longlong(mx));
+                if (lsb != 0x7fffffff) atomicMin(&o.lsb[l], lsb);
+            }
+        }
+    }
+}
+
+// Line exponent and the digit count that makes the line exact
+// (need = max over its nonzero entries of ceil((E - lsb) / 7)).
+__global__ void __launch_bounds__(256) k_g_lines(const GOp *__restrict__ ops, const int *__restrict__ line0,
+                                                 int nops, int total, int *__restrict__ need) {
+    const int g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= total) return;
+    int lo = 0, hi = nops - 1;  // op with line0[op] <= g < line0[op + 1]
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (line0[mid] <= g)
+            lo = mid;
+        else
+            hi = mid - 1;
+    }
+    const GOp &o = ops[lo];
+    const int l = g - line0[lo];
+    const double mx = __longlong_as_double((long long)o.mx[l]);
+    const int E = mx > 0.0 ? g_exp_above(mx) : 0;
+    o.e[l] = E;
+    if (mx > 0.0) atomicMax(&need[lo], (E - o.lsb[l] + 6) / 7);
+}
+
+// Digit tiles of one 128 x 128 block: S levels, truncated 7-bit digits of
+// x * 2^-E (as k_digit_write), written in the swizzled tile layout.
+__global__ void __launch_bounds__(512) k_g_digits(const int4 *__restrict__ blocks, const GOp *__restrict__ ops) {
+    const int4 bk = blocks[blockIdx.x];
+    const GOp o = ops[bk.x];
+    const int l0 = bk.y * G_T, k0 = bk.z * G_T;
+    const int t = threadIdx.x;
+    const size_t level_stride = (size_t)o.tiles_l * o.nkb * G_TILE_BYTES;
+    int8_t *tile0 = o.digits + ((size_t)bk.y * o.nkb + bk.z) * G_TILE_BYTES;
+    if (!o.kcontig) {
+        // thread: row r, k quarter q (32 values); lines contiguous across threads
+        const int r = t & 127, q = t >> 7, l = l0 + r;
+        double v[32];
+        const int E = l < o.lines ? o.e[l] : 0;
+#pragma unroll
+        for (int j = 0; j < 32; j++) {
+            const int kk = k0 + 32 * q + j;
+            v[j] = (l < o.lines && kk < o.k) ? scalbn(o.X[(size_t)l + (size_t)kk * o.ld], -E) : 0.0;
+        }
+        const int c0 = (2 * q) ^ (r & 7), c1 = (2 * q + 1) ^ (r & 7);
+        for (int s = 0; s < o.S; s++) {
+            uint32_t w[8];
+#pragma unroll
+            for (int i = 0; i < 8; i++) w[i] = 0u;
+#pragma unroll
+            for (int j = 0; j < 32; j++) {
+                const double tt = v[j] * 128.0;
+                const double d = trunc(tt);
+                v[j] = tt - d;
+                w[j >> 2] |= ((uint32_t)(uint8_t)(int8_t)(int)d) << (8 * (j & 3));
+            }
+            int8_t *row = tile0 + s * level_stride + r * 128;
+            *reinterpret_cast<int4 *>(row + c0 * 16) = make_int4((int)w[0], (int)w[1], (int)w[2], (int)w[3]);
+            *reinterpret_cast<int4 *>(row + c1 * 16) = make_int4((int)w[4], (int)w[5], (int)w[6], (int)w[7]);
+        }
+    } else {
+        // warp: rows w + 16 i; lane: k 4 lane .. 4 lane + 3 (k contiguous across lanes)
+        const int w = t >> 5, lane = t & 31;
+        double v[8][4];
+        int E[8];
+#pragma unroll
+        for (int i = 0; i < 8; i++) {
+            const int l = l0 + w + 16 * i;
+            E[i] = l < o.lines ? o.e[l] : 0;
+#pragma unroll
+            for (int q = 0; q < 4; q++) {
+                const int kk = k0 + 4 * lane + q;
+                v[i][q] = (l < o.lines && kk < o.k) ? scalbn(o.X[(size_t)l * o.ld + kk], -E[i]) : 0.0;
+            }
+        }
+        for (int s = 0; s < o.S; s++) {
+#pragma unroll
+            for (int i = 0; i < 8; i++) {
+                const int r = w + 16 * i;
+                uint32_t word = 0u;
+#pragma unroll
+                for (int q = 0; q < 4; q++) {
+                    const double tt = v[i][q] * 128.0;
+                    const double d = trunc(tt);
+                    v[i][q] = tt - d;
+                    word |= ((uint32_t)(uint8_t)(int8_t)(int)d) << (8 * q);
+                }
+                int8_t *row = tile0 + s * level_stride + r * 128;
+                *reinterpret_cast<uint32_t *>(row + (((lane >> 2) ^ (r & 7)) * 16) + (lane & 3) * 4) = word;
+            }
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// The grouped product kernel (roles and waits as k_i8_gemm)
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(G_THREADS, 1) k_i8_grouped(const GParams p) {
+    extern __shared__ uint8_t smem_raw[];
+    uint8_t *smem = (uint8_t *)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+    uint64_t *bar = (uint64_t *)(smem + G_NST * G_STAGE);
+    uint64_t *full = bar, *empty = bar + G_NST, *acc_full = bar + 2 * G_NST, *acc_empty = bar + 2 * G_NST + 2;
+    uint64_t *drain = bar + 2 * G_NST + 4;
+    __shared__ uint32_t tmem_slot;
+    __shared__ volatile int abort_flag;
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int t_begin = p.cta_begin[blockIdx.x], t_end = p.cta_begin[blockIdx.x + 1];
+
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < G_NST; s++) {
+            tc::mbar_init(&full[s], 1);
+            tc::mbar_init(&empty[s], 1);
+        }
+        for (int b = 0; b < 2; b++) {
+            tc::mbar_init(&acc_full[b], 1);
+            tc::mbar_init(&acc_empty[b], 256);
+        }
+        tc::mbar_init(drain, 1);
+        abort_flag = 0;
+        tc::fence_mbar_init();
+    }
+    if (warp == 1) tc::tmem_alloc(&tmem_slot, G_TMEM_COLS);
+    tc::fence_before_sync();
+    __syncthreads();
+    tc::fence_after_sync();
+    const uint32_t tmem_base = tmem_slot;
+
+    if (warp == 0) {
+        // ------------------------------------------------------------ producer
+        if (lane == 0) {
+            uint32_t stage = 0, phase = 0;
+            bool ok = true;
+            for (int ti = t_begin; ti < t_end && ok; ti++) {
+                const int4 tl = p.tiles[ti];
+                const GProb pr = p.probs[tl.x];
+                for (int g = 0; g < pr.n_groups && ok; g++) {
+                    const int4 grp = p.groups[pr.group0 + g];
+                    for (int it = grp.x; it < grp.y && ok; it++) {
+                        const int4 item = p.items[it];
+                        const int8_t *a0 = pr.da + ((size_t)(item.x * pr.tiles_m + tl.y) * pr.nkb) * G_TILE_BYTES;
+                        const int8_t *b0 = pr.db + ((size_t)(item.y * pr.tiles_n + tl.z) * pr.nkb) * G_TILE_BYTES;
+                        for (int kb = item.z; kb < item.w; kb++) {
+                            if (!tc::mbar_wait(&empty[stage], phase ^ 1, &abort_flag, p.err, GERR_PRODUCER,
+                                               G_WAIT_NS)) {
+                                ok = false;
+                                break;
+                            }
+                            uint8_t *sa = smem + stage * G_STAGE, *sb = sa + G_TILE_BYTES;
+                            tc::mbar_arrive_expect_tx(&full[stage], G_STAGE);
+                            tc::bulk_load(sa, a0 + (size_t)kb * G_TILE_BYTES, G_TILE_BYTES, &full[stage]);
+                            tc::bulk_load(sb, b0 + (size_t)kb * G_TILE_BYTES, G_TILE_BYTES, &full[stage]);
+                            if (++stage == G_NST) {
+                                stage = 0;
+                                phase ^= 1;
+                            }
+                        }
+                    }
+                }
+            }
+            if (!ok) {
+                for (int s = 0; s < G_NST; s++) {
+                    const uint64_t t0 = tc::globaltimer();
+                    while (!tc::mbar_try_wait(&full[s], 0) && !tc::mbar_try_wait(&full[s], 1) &&
+                           tc::globaltimer() - t0 < 100000000ull) {
+                    }
+                }
+            }
+        }
+    } else if (warp == 1) {
+        // ------------------------------------------------------------ MMA issuer
+        if (lane == 0) {
+            const uint32_t idesc = tc::idesc_i8(G_T, G_T);
+            uint32_t stage = 0, phase = 0, abuf = 0, aphase = 0;
+            bool ok = true, issued = false;
+            for (int ti = t_begin; ti < t_end && ok; ti++) {
+                const GProb pr = p.probs[p.tiles[ti].x];
+                for (int g = 0; g < pr.n_groups && ok; g++) {
+                    const int4 grp = p.groups[pr.group0 + g];
+                    if (!tc::mbar_wait(&acc_empty[abuf], aphase ^ 1, &abort_flag, p.err, GERR_MMA, G_WAIT_NS)) {
+                        ok = false;
+                        break;
+                    }
+                    tc::fence_after_sync();
+                    const uint32_t tmem_d = tmem_base + abuf * G_T;
+                    uint32_t accumulate = 0;
+                    for (int it = grp.x; it < grp.y && ok; it++) {
+                        const int4 item = p.items[it];
+                        for (int kb = item.z; kb < item.w; kb++) {
+                            if (!tc::mbar_wait(&full[stage], phase, &abort_flag, p.err, GERR_MMA, G_WAIT_NS)) {
+                                ok = false;
+                                break;
+                            }
+                            tc::fence_after_sync();
+                            const uint32_t sa = tc::smem_u32(smem + stage * G_STAGE), sb = sa + G_TILE_BYTES;
+                            const uint64_t adesc = tc::smem_desc_k_sw128(sa), bdesc = tc::smem_desc_k_sw128(sb);
+#pragma unroll
+                            for (int kk = 0; kk < G_T / 32; kk++) {
+                                tc::mma_i8(tmem_d, adesc + 2 * kk, bdesc + 2 * kk, idesc, accumulate);
+                                accumulate = 1;
+                            }
+                            issued = true;
+                            tc::mma_commit(&empty[stage]);
+                            if (++stage == G_NST) {
+                                stage = 0;
+                                phase ^= 1;
+                            }
+                        }
+                    }
+                    if (!ok) break;
+                    tc::mma_commit(&acc_full[abuf]);
+                    abuf ^= 1;
+                    if (abuf == 0) aphase ^= 1;
+                }
+            }
+            if (!ok && issued) {
+                tc::mma_commit(drain);
+                const uint64_t t0 = tc::globaltimer();
+                while (!tc::mbar_try_wait(drain, 0) && tc::globaltimer() - t0 < 100000000ull) {
+                }
+            }
+        }
+    } else {
+        // ------------------------------------------------------------ epilogue
+        const int q = warp & 3, half = (warp - 2) >> 2;
+        const int row = q * 32 + lane;
+        const uint32_t lane_base = tmem_base + ((uint32_t)(q * 32) << 16);
+        const uint32_t rcol = G_RCOL + half * 128;
+        uint32_t abuf = 0, aphase = 0;
+        bool ok = true;
+        for (int ti = t_begin; ti < t_end && ok; ti++) {
+            const int4 tl = p.tiles[ti];
+            const GProb *pr = p.probs + tl.x;  // fields read where used (registers go to the sums)
+            const int gr = tl.y * G_T + row;
+            const int ng = __ldg(&pr->n_groups), g0 = __ldg(&pr->group0);
+            double acc[64];
+#pragma unroll
+            for (int c = 0; c < 64; c++) acc[c] = 0.0;
+            for (int g = 0; g < ng; g++) {
+                const int4 grp = p.groups[g0 + g];
+                const int meta = grp.w;
+                if (!tc::mbar_wait(&acc_full[abuf], aphase, &abort_flag, p.err, GERR_EPI, G_WAIT_NS)) {
+                    ok = false;
+                    break;
+                }
+                tc::fence_after_sync();
+                const double sc = pow2(meta & 0xff);
+                const uint32_t taddr = lane_base + abuf * G_T + half * 64;
+                uint32_t v[32];
+                tc::tmem_ld_32x32b_x32(taddr, v);
+                tc::tmem_ld_wait();
+#pragma unroll
+                for (int c = 0; c < 32; c++) acc[c] += (double)(int32_t)v[c] * sc;
+                tc::tmem_ld_32x32b_x32(taddr + 32, v);
+                tc::tmem_ld_wait();
+#pragma unroll
+                for (int c = 0; c < 32; c++) acc[32 + c] += (double)(int32_t)v[c] * sc;
+                tc::fence_before_sync();
+                tc::mbar_arrive(&acc_empty[abuf]);
+                abuf ^= 1;
+                if (abuf == 0) aphase ^= 1;
+                if (meta & (1 << 8)) {
+                    const double fs = pow2(grp.z);
+                    const bool first = meta & (1 << 9), last = meta & (1 << 10);
+#pragma unroll
+                    for (int ch = 0; ch < 4; ch++) {
+                        const uint32_t raddr = lane_base + rcol + ch * 32;
+                        uint32_t u[32];
+                        double r[16];
+                        if (first) {
+#pragma unroll
+                            for (int e = 0; e < 16; e++) r[e] = acc[ch * 16 + e] * fs;
+                        } else {
+                            tc::tmem_ld_32x32b_x32(raddr, u);
+                            tc::tmem_ld_wait();
+#pragma unroll
+                            for (int e = 0; e < 16; e++)
+                                r[e] = __hiloint2double((int)u[2 * e + 1], (int)u[2 * e]) + acc[ch * 16 + e] * fs;
+                        }
+                        if (last) {
+                            const int pm = __ldg(&pr->m);
+                            if (gr < pm) {
+                                const int pn = __ldg(&pr->n), ldc = __ldg(&pr->ldc);
+                                const double al = __ldg(&pr->alpha), be = __ldg(&pr->beta);
+                                double *Cp = pr->C;
+                                const int *ebp = pr->eb;
+                                const int ea = pr->ea[gr];
+#pragma unroll
+                                for (int e = 0; e < 16; e++) {
+                                    const int gc = tl.z * G_T + half * 64 + ch * 16 + e;
+                                    if (gc < pn) {
+                                        double *cp = &Cp[(size_t)gc * ldc + gr];
+                                        const double t = scalbn(r[e], ea + ebp[gc]);
+                                        *cp = fma(al, t, be * *cp);
+                                    }
+                                }
+                            }
+                        } else {
+#pragma unroll
+                            for (int e = 0; e < 16; e++) {
+                                u[2 * e] = (uint32_t)__double2loint(r[e]);
+                                u[2 * e + 1] = (uint32_t)__double2hiint(r[e]);
+                            }
+                            tc::tmem_st_32x32b_x32(raddr, u);
+                        }
+                    }
+                    if (!last) tc::tmem_st_wait();
+#pragma unroll
+                    for (int c = 0; c < 64; c++) acc[c] = 0.0;
+                }
+            }
+        }
+    }
+    tc::fence_before_sync();
+    __syncthreads();
+    if (warp == 1) {
+        tc::fence_after_sync();
+        tc::tmem_dealloc(tmem_base, G_TMEM_COLS);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Host side
+// ---------------------------------------------------------------------------
+int i8_schedule(int nA, int nB, int nkb, bool triangular, std::vector<int4> &items, std::vector<int4> &groups);
+
+constexpr int kI8DefaultCapG = 19;  // as gemm_i8.cu's kI8DefaultCap
+
+int gemm_i8_batched(cuozblasHandle_t *h, char ta, char tb, int count, const int *m, const int *n, const int *k,
+                    const double *alpha, const double *const *A, const int *lda, const double *const *B,
+                    const int *ldb, const double *beta, double *const *C, const int *ldc) {
+    State *st = state(h);
+    cudaStream_t s = st->stream;
+    Arena ar(h);
+    const int cap = h->nSplitMax > 0 ? h->nSplitMax : kI8DefaultCapG;
+    // operands 2b (op(A) of problem b) and 2b + 1 (op(B))
+    std::vector<GOp> ops((size_t)2 * count);
+    std::vector<int> line0((size_t)2 * count + 1, 0);
+    std::vector<int4> blocks;
+    for (int b = 0; b < count; b++) {
+        const int nkb = k[b] > 0 ? (k[b] + G_T - 1) / G_T : 1;
+        GOp &oa = ops[(size_t)2 * b], &ob = ops[(size_t)2 * b + 1];
+        oa = GOp{A[b], lda[b], m[b], k[b], is_trans(ta) ? 1 : 0, (m[b] + G_T - 1) / G_T, nkb, 0,
+                 nullptr, nullptr, nullptr, nullptr};
+        ob = GOp{B[b], ldb[b], n[b], k[b], is_trans(tb) ? 0 : 1, (n[b] + G_T - 1) / G_T, nkb, 0,
+                 nullptr, nullptr, nullptr, nullptr};
+        for (int o = 0; o < 2; o++) {
+            const GOp &op = ops[(size_t)2 * b + o];
+            line0[(size_t)2 * b + o + 1] = line0[(size_t)2 * b + o] + op.lines;
+            if (k[b] > 0)
+                for (int tl = 0; tl < op.tiles_l; tl++)
+                    for (int kb = 0; kb < op.nkb; kb++) blocks.push_back(make_int4(2 * b + o, tl, kb, 0));
+        }
+    }
+    const int nops = 2 * count, total_lines = line0[(size_t)nops];
+    // per-line exponents and statistics of all operands, one array each
+    const uint64_t tl_alloc = (uint64_t)(total_lines > 0 ? total_lines : 1);
+    int *all_e = ar.take<int>(tl_alloc);
+    unsigned long long *all_mx = ar.take<unsigned long long>(tl_alloc);
+    int *all_lsb = ar.take<int>(tl_alloc);
+    GOp *d_ops = ar.take<GOp>((uint64_t)nops);
+    int *d_line0 = ar.take<int>((uint64_t)nops + 1);
+    int *d_need = ar.take<int>((uint64_t)nops);
+    int4 *d_blocks = ar.take<int4>(blocks.size() > 0 ? blocks.size() : 1);
+    if (!ar.ok) return CUOZBLAS_STATUS_WORKSPACE;
+    for (int o = 0; o < nops; o++) {
+        GOp &op = ops[(size_t)o];
+        op.e = all_e + line0[(size_t)o];
+        op.mx = all_mx + line0[(size_t)o];
+        op.lsb = all_lsb + line0[(size_t)o];
+    }
+    OZB_CHECK(cudaMemsetAsync(all_mx, 0, tl_alloc * sizeof(unsigned long long), s));
+    OZB_CHECK(cudaMemsetAsync(all_lsb, 0x7f, tl_alloc * sizeof(int), s));
+    OZB_CHECK(cudaMemsetAsync(d_need, 0, (size_t)nops * sizeof(int), s));
+    OZB_CHECK(cudaMemcpyAsync(d_ops, ops.data(), sizeof(GOp) * nops, cudaMemcpyHostToDevice, s));
+    OZB_CHECK(cudaMemcpyAsync(d_line0, line0.data(), sizeof(int) * (nops + 1), cudaMemcpyHostToDevice, s));
+    if (!blocks.empty())
+        OZB_CHECK(cudaMemcpyAsync(d_blocks, blocks.data(), sizeof(int4) * blocks.size(), cudaMemcpyHostToDevice, s));
+    ev_record(h, 0);
+    if (!blocks.empty()) {
+        counted(h);
+        k_g_stats<<<(unsigned)blocks.size(), 256, 0, s>>>(d_blocks, d_ops);
+    }
+    if (total_lines > 0) {
+        counted(h);
+        k_g_lines<<<(total_lines + 255) / 256, 256, 0, s>>>(d_ops, d_line0, nops, total_lines, d_need);
+    }
+    OZB_CHECK(cudaGetLastError());
+    std::vector<int> need((size_t)nops);
+    OZB_CHECK(cudaMemcpyAsync(need.data(), d_need, sizeof(int) * nops, cudaMemcpyDeviceToHost, s));
+    OZB_CHECK(cudaStreamSynchronize(s));
+    int maxA = 0, maxB = 0;
+    for (int o = 0; o < nops; o++) {
+        GOp &op = ops[(size_t)o];
+        op.S = need[(size_t)o] < 1 ? 1 : need[(size_t)o];
+        if (op.S > cap) op.S = cap;
+        op.digits = ar.take<int8_t>((uint64_t)op.S * op.tiles_l * op.nkb * G_TILE_BYTES + 1);
+        if (o & 1)
+            maxB = op.S > maxB ? op.S : maxB;
+        else
+            maxA = op.S > maxA ? op.S : maxA;
+    }
+    if (!ar.ok) return CUOZBLAS_STATUS_WORKSPACE;
+    for (int o = 0; o < nops; o++)  // k = 0: zero digits, so C = beta * C
+        if (ops[(size_t)o].k == 0 && ops[(size_t)o].tiles_l > 0)
+            OZB_CHECK(cudaMemsetAsync(ops[(size_t)o].digits, 0,
+                                      (size_t)ops[(size_t)o].S * ops[(size_t)o].tiles_l * G_TILE_BYTES, s));
+    OZB_CHECK(cudaMemcpyAsync(d_ops, ops.data(), sizeof(GOp) * nops, cudaMemcpyHostToDevice, s));
+    if (!blocks.empty()) {
+        counted(h);
+        k_g_digits<<<(unsigned)blocks.size(), 512, 0, s>>>(d_blocks, d_ops);
+        OZB_CHECK(cudaGetLastError());
+    }
+    ev_record(h, 1);
+    // schedules, problems and the tile deal
+    std::vector<int4> items, groups, tiles;
+    std::vector<GProb> probs((size_t)count);
+    std::vector<double> cost((size_t)count, 0.0);
+    int npairs_max = 0;
+    for (int b = 0; b < count; b++) {
+        const GOp &oa = ops[(size_t)2 * b], &ob = ops[(size_t)2 * b + 1];
+        std::vector<int4> it, gr;
+        const int np = i8_schedule(oa.S, ob.S, oa.nkb, h->fastMode != 0, it, gr);
+        npairs_max = np > npairs_max ? np : npairs_max;
+        const int ibase = (int)items.size();
+        for (auto &g : gr) {
+            g.x += ibase;
+            g.y += ibase;
+        }
+        double kbs = 0.0;
+        for (auto &i : it) kbs += i.w - i.z;
+        cost[(size_t)b] = kbs + 2.0 * gr.size();
+        GProb &pr = probs[(size_t)b];
+        pr = GProb{m[b], n[b], ldc[b], oa.nkb, oa.tiles_l, ob.tiles_l, (int)groups.size(), (int)gr.size(),
+                   oa.digits, ob.digits, oa.e, ob.e, alpha[b], beta[b], C[b]};
+        items.insert(items.end(), it.begin(), it.end());
+        groups.insert(groups.end(), gr.begin(), gr.end());
+    }
+    std::vector<int> order((size_t)count);
+    for (int b = 0; b < count; b++) order[(size_t)b] = b;
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return cost[(size_t)a] > cost[(size_t)b]; });
+    const int nsm = sm_count();
+    int ntile_total = 0;
+    for (int b = 0; b < count; b++)
+        if (m[b] > 0 && n[b] > 0) ntile_total += probs[(size_t)b].tiles_m * probs[(size_t)b].tiles_n;
+    const int grid = ntile_total < nsm ? (ntile_total > 0 ? ntile_total : 1) : nsm;
+    // longest first onto the least loaded CTA
+    std::vector<std::vector<int4>> per_cta((size_t)grid);
+    using Load = std::pair<double, int>;
+    std::priority_queue<Load, std::vector<Load>, std::greater<Load>> heap;
+    for (int c = 0; c < grid; c++) heap.push(Load(0.0, c));
+    for (int b : order) {
+        const GProb &pr = probs[(size_t)b];
+        if (pr.m <= 0 || pr.n <= 0) continue;
+        for (int tn = 0; tn < pr.tiles_n; tn++)
+            for (int tm = 0; tm < pr.tiles_m; tm++) {
+                Load l = heap.top();
+                heap.pop();
+                per_cta[(size_t)l.second].push_back(make_int4(b, tm, tn, 0));
+                l.first += cost[(size_t)b];
+                heap.push(l);
+            }
+    }
+    std::vector<int> cta_begin((size_t)grid + 1, 0);
+    for (int c = 0; c < grid; c++) {
+        cta_begin[(size_t)c + 1] = cta_begin[(size_t)c] + (int)per_cta[(size_t)c].size();
+        tiles.insert(tiles.end(), per_cta[(size_t)c].begin(), per_cta[(size_t)c].end());
+    }
+    GProb *d_probs = ar.take<GProb>((uint64_t)count);
+    int4 *d_sched = ar.take<int4>(items.size() + groups.size() + tiles.size() + 1);
+    int *d_cta = ar.take<int>((uint64_t)grid + 1);
+    int *d_err = ar.take<int>(1);
+    if (!ar.ok) return CUOZBLAS_STATUS_WORKSPACE;
+    std::vector<int4> sched(items);
+    sched.insert(sched.end(), groups.begin(), groups.end());
+    sched.insert(sched.end(), tiles.begin(), tiles.end());
+    OZB_CHECK(cudaMemcpyAsync(d_probs, probs.data(), sizeof(GProb) * count, cudaMemcpyHostToDevice, s));
+    if (!sched.empty())
+        OZB_CHECK(cudaMemcpyAsync(d_sched, sched.data(), sizeof(int4) * sched.size(), cudaMemcpyHostToDevice, s));
+    OZB_CHECK(cudaMemcpyAsync(d_cta, cta_begin.data(), sizeof(int) * (grid + 1), cudaMemcpyHostToDevice, s));
+    OZB_CHECK(cudaMemsetAsync(d_err, 0, sizeof(int), s));
+    GParams gp;
+    gp.probs = d_probs;
+    gp.items = d_sched;
+    gp.groups = d_sched + items.size();
+    gp.tiles = d_sched + items.size() + groups.size();
+    gp.cta_begin = d_cta;
+    gp.err = d_err;
+    h->nSplitA = (float)maxA;
+    h->nSplitB = (float)maxB;
+    h->nSplitC = (float)npairs_max;
+    ev_record(h, 2);
+    if (ntile_total > 0) {
+        static bool attr = false;
+        if (!attr) {
+            OZB_CHECK(cudaFuncSetAttribute(k_i8_grouped, cudaFuncAttributeMaxDynamicSharedMemorySize, G_SMEM));
+            attr = true;
+        }
+        counted(h);
+        k_i8_grouped<<<grid, G_THREADS, G_SMEM, s>>>(gp);
+        OZB_CHECK(cudaGetLastError());
+    }
+    ev_record(h, 3);
+    int herr = 0;
+    OZB_CHECK(cudaMemcpyAsync(&herr, d_err, sizeof(int), cudaMemcpyDeviceToHost, s));
+    OZB_CHECK(cudaStreamSynchronize(s));
+    if (herr != 0) {
+        fprintf(stderr, "cuozblas: grouped INT8 GEMM kernel wait timed out (code %d)\n", herr);
+        return CUOZBLAS_STATUS_DEVICE_TIMEOUT;
+    }
+    h->t_SplitA = ev_ms(h, 0, 1) * 1e-3f;
+    h->t_SplitB = 0.f;
+    h->t_comp = ev_ms(h, 2, 3) * 1e-3f;
+    h->t_sum = 0.f;
+    return CUOZBLAS_STATUS_SUCCESS;
+}
+
+}  // namespace ozb
+
+extern "C" int cuozblasDgemmI8Batched(cuozblasHandle_t *h, char transa, char transb, int32_t count, const int32_t *m,
+                                      const int32_t *n, const int32_t *k, const double *alpha,
+                                      const double *const *A, const int32_t *lda, const double *const *B,
+                                      const int32_t *ldb, const double *beta, double *const *C,
+                                      const int32_t *ldc) {
+    using namespace ozb;
+    OZB_TRY(counter_init(h));
+    if (count < 0 || h->nSplitMax < 0 || h->nSplitMax > 64) return CUOZBLAS_STATUS_INVALID_VALUE;
+    if (count == 0) return CUOZBLAS_STATUS_SUCCESS;
+    if (!m || !n || !k || !alpha || !A || !lda || !B || !ldb || !beta || !C || !ldc)
+        return CUOZBLAS_STATUS_INVALID_VALUE;
+    for (int b = 0; b < count; b++) {
+        if (m[b] < 0 || n[b] < 0 || k[b] < 0 || ldc[b] < (m[b] > 1 ? m[b] : 1)) return CUOZBLAS_STATUS_INVALID_VALUE;
+        const int rows_a = is_trans(transa) ? k[b] : m[b], rows_b = is_trans(transb) ? n[b] : k[b];
+        if (lda[b] < (rows_a > 1 ? rows_a : 1) || ldb[b] < (rows_b > 1 ? rows_b : 1))
+            return CUOZBLAS_STATUS_INVALID_VALUE;
+    }
+    return gemm_i8_batched(h, transa, transb, count, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc);
+}

@@ -109,3 +109,61 @@ def test_i8_vs_plain_error(oracle, handle, ozb, cuda):
     e8 = errors(oracle, A, B, Ci8, m, n, k, rows, cols)
     ep = errors(oracle, A, B, Cp, m, n, k, rows, cols)
     assert e8 <= max(ep, U), (e8, ep)
+
+
+# ---- grouped launch of many uneven problems (cuozblasDgemmI8Batched) ----
+
+def _batch_case(oracle, shapes, ta, tb, seed):
+    """Column-major inputs for each (m, n, k, phi); A stored for op(A) = A ('n') or A^T ('t')."""
+    rng = np.random.default_rng(seed)
+    probs = []
+    for i, (m, n, k, phi) in enumerate(shapes):
+        ar, ac = (m, k) if ta == "n" else (k, m)   # A is ar x ac column-major
+        br, bc = (k, n) if tb == "n" else (n, k)
+        A = oracle.phi_matrix(ar, ac, phi, 100 + i) if ar * ac else np.zeros((max(ac, 1), max(ar, 1)))
+        B = oracle.phi_matrix(br, bc, phi, 200 + i) if br * bc else np.zeros((max(bc, 1), max(br, 1)))
+        C0 = rng.standard_normal((max(n, 1), max(m, 1)))
+        probs.append((m, n, k, A, max(ar, 1), B, max(br, 1), C0, float(rng.choice([1.0, -0.5])),
+                      float(rng.choice([0.0, 2.0]))))
+    return probs
+
+
+@pytest.mark.parametrize("ta,tb", [("n", "n"), ("t", "n"), ("n", "t"), ("t", "t")])
+@pytest.mark.parametrize("fast", [0, 1])
+def test_i8_batched_matches_single(ta, tb, fast, oracle, handle, ozb, cuda):
+    """Every problem of a grouped launch is bit-identical to its own cuozblasDgemmI8 call."""
+    shapes = [(1, 1, 1, 1.0), (64, 300, 129, 0.5), (130, 70, 1000, 2.0), (200, 256, 512, 4.0), (7, 129, 33, 1.0),
+              (256, 3, 256, 1.0), (129, 129, 128, 2.0), (90, 40, 0, 1.0), (0, 5, 10, 1.0), (300, 200, 64, 0.5)]
+    probs = _batch_case(oracle, shapes, ta, tb, 7 + fast)
+    handle.nSplitMax, handle.fastMode = 0, fast
+    Cs = [dev(cuda, p[7]) for p in probs]
+    ozb.dgemm_i8_batched(handle, ta, tb, [p[0] for p in probs], [p[1] for p in probs], [p[2] for p in probs],
+                         [p[8] for p in probs], [dev(cuda, p[3]) for p in probs], [p[4] for p in probs],
+                         [dev(cuda, p[5]) for p in probs], [p[6] for p in probs], [p[9] for p in probs], Cs,
+                         [max(p[0], 1) for p in probs])
+    for i, p in enumerate(probs):
+        m, n, k, A, lda, B, ldb, C0, al, be = p
+        dC = dev(cuda, C0)
+        if m and n:
+            ozb.dgemm_i8(handle, ta, tb, m, n, k, al, dev(cuda, A), lda, dev(cuda, B), ldb, be, dC, max(m, 1))
+        assert bits_equal(Cs[i].cpu().numpy(), dC.cpu().numpy()), (i, m, n, k)
+
+
+def test_i8_batched_accuracy_uneven(oracle, handle, ozb, cuda):
+    """48 log-uniform shapes in [16, 400], phi from {0.5, 1, 2, 4}: within 2 units of 2^-53 of the exact product."""
+    rng = np.random.default_rng(5)
+    shapes = [(int(a), int(b), int(c), float(rng.choice([0.5, 1.0, 2.0, 4.0])))
+              for a, b, c in np.exp(rng.uniform(np.log(16), np.log(400), (48, 3))).astype(int)]
+    probs = _batch_case(oracle, shapes, "n", "n", 11)
+    handle.nSplitMax, handle.fastMode = 0, 0
+    Cs = [cuda.zeros((p[1], p[0]), dtype=cuda.float64, device="cuda") for p in probs]
+    ozb.dgemm_i8_batched(handle, "n", "n", [p[0] for p in probs], [p[1] for p in probs], [p[2] for p in probs],
+                         [1.0] * len(probs), [dev(cuda, p[3]) for p in probs], [p[4] for p in probs],
+                         [dev(cuda, p[5]) for p in probs], [p[6] for p in probs], [0.0] * len(probs), Cs,
+                         [p[0] for p in probs])
+    for i, p in enumerate(probs[:12]):
+        m, n, k, A, _, B = p[:6]
+        C = Cs[i].cpu().numpy()
+        err = errors(oracle, A, B, C, m, n, k, np.linspace(0, m - 1, min(m, 16)).astype(int),
+                     np.linspace(0, n - 1, min(n, 16)).astype(int))
+        assert err <= 2 * U, (i, m, n, k, err)
