@@ -243,6 +243,9 @@ __global__ void __launch_bounds__(I8_THREADS, 1)
                 if (meta & (1 << 8)) {  // end of a run: R += acc * 2^(exponent)
                     const double fs = pow2(grp.z);
                     const bool first = meta & (1 << 9), last = meta & (1 << 10);
+                    // the exact rounding error of R + run goes into the next run's
+                    // accumulator (scaled to its units), so R + carries stays exact
+                    const double cs = last ? 0.0 : pow2(32768 - ((meta >> 16) & 0xffff));
 #pragma unroll
                     for (int ch = 0; ch < 4; ch++) {
                         const uint32_t raddr = lane_base + rcol + ch * 32;
@@ -250,13 +253,22 @@ __global__ void __launch_bounds__(I8_THREADS, 1)
                         double r[16];
                         if (first) {
 #pragma unroll
-                            for (int e = 0; e < 16; e++) r[e] = acc[ch * 16 + e] * fs;
+                            for (int e = 0; e < 16; e++) {
+                                r[e] = acc[ch * 16 + e] * fs;
+                                acc[ch * 16 + e] = 0.0;
+                            }
                         } else {
                             tc::tmem_ld_32x32b_x32(raddr, u);
                             tc::tmem_ld_wait();
 #pragma unroll
-                            for (int e = 0; e < 16; e++)
-                                r[e] = __hiloint2double((int)u[2 * e + 1], (int)u[2 * e]) + acc[ch * 16 + e] * fs;
+                            for (int e = 0; e < 16; e++) {
+                                const double ro = __hiloint2double((int)u[2 * e + 1], (int)u[2 * e]);
+                                const double a = acc[ch * 16 + e] * fs;
+                                const double sm = ro + a;
+                                const double bb = sm - ro;
+                                acc[ch * 16 + e] = ((ro - (sm - bb)) + (a - bb)) * cs;  // TwoSum error
+                                r[e] = sm;
+                            }
                         }
                         if (last) {
                             if (gr < p.m) {
@@ -281,8 +293,6 @@ __global__ void __launch_bounds__(I8_THREADS, 1)
                         }
                     }
                     if (!last) tc::tmem_st_wait();
-#pragma unroll
-                    for (int c = 0; c < 64; c++) acc[c] = 0.0;
                 }
             }
         }
@@ -468,7 +478,8 @@ static int split_digits(cuozblasHandle_t *h, bool strided, int nl, int k, const 
 // range of 128-k blocks) grouped per level into INT32 groups of at most
 // I8_MAX_TERMS products per output, levels visited from the largest, and the
 // runs of levels that combine exactly below 2^53 (group meta: shift |
-// flush << 8 | first << 9 | last << 10, group.z the flush exponent).  Pair
+// flush << 8 | first << 9 | last << 10 | (next flush exponent + 32768) << 16,
+// group.z the flush exponent).  Pair
 // set: full, or the triangle ia + ib <= min(nA, nB) - 1
 // (src/cuda/cuozblas_gemm.cu:138).  Returns the number of pairs.
 int i8_schedule(int nA, int nB, int nkb, bool triangular, std::vector<int4> &items, std::vector<int4> &groups) {
@@ -540,6 +551,8 @@ int i8_schedule(int nA, int nB, int nkb, bool triangular, std::vector<int4> &ite
                 meta |= (1 << 8) | (first ? (1 << 9) : 0);
                 first = false;
                 groups[g].z = -7 * (run_hi[L] + 2);
+                // the next run's flush exponent: the rounding error of this flush is carried there
+                if (L < maxlevel) meta |= (-7 * (run_hi[L + 1] + 2) + 32768) << 16;
             } else {
                 groups[g].z = 0;
             }
@@ -815,6 +828,7 @@ static int dgemm_i8_static(char ta, char tb, int m, int n, int k, double alpha, 
                 meta |= (1 << 8) | (first ? (1 << 9) : 0);
                 first = false;
                 groups[g].z = -7 * (run_hi[L] + 2);
+                if (L < maxlevel) meta |= (-7 * (run_hi[L + 1] + 2) + 32768) << 16;
             } else {
                 groups[g].z = 0;
             }

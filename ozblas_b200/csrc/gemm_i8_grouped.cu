@@ -407,6 +407,9 @@ __global__ void __launch_bounds__(G_THREADS, 1) k_i8_grouped(const GParams p) {
                 if (meta & (1 << 8)) {
                     const double fs = pow2(grp.z);
                     const bool first = meta & (1 << 9), last = meta & (1 << 10);
+                    // the exact rounding error of R + run goes into the next run's
+                    // accumulator (scaled to its units), so R + carries stays exact
+                    const double cs = last ? 0.0 : pow2(32768 - ((meta >> 16) & 0xffff));
 #pragma unroll
                     for (int ch = 0; ch < 4; ch++) {
                         const uint32_t raddr = lane_base + rcol + ch * 32;
@@ -414,13 +417,22 @@ __global__ void __launch_bounds__(G_THREADS, 1) k_i8_grouped(const GParams p) {
                         double r[16];
                         if (first) {
 #pragma unroll
-                            for (int e = 0; e < 16; e++) r[e] = acc[ch * 16 + e] * fs;
+                            for (int e = 0; e < 16; e++) {
+                                r[e] = acc[ch * 16 + e] * fs;
+                                acc[ch * 16 + e] = 0.0;
+                            }
                         } else {
                             tc::tmem_ld_32x32b_x32(raddr, u);
                             tc::tmem_ld_wait();
 #pragma unroll
-                            for (int e = 0; e < 16; e++)
-                                r[e] = __hiloint2double((int)u[2 * e + 1], (int)u[2 * e]) + acc[ch * 16 + e] * fs;
+                            for (int e = 0; e < 16; e++) {
+                                const double ro = __hiloint2double((int)u[2 * e + 1], (int)u[2 * e]);
+                                const double a = acc[ch * 16 + e] * fs;
+                                const double sm = ro + a;
+                                const double bb = sm - ro;
+                                acc[ch * 16 + e] = ((ro - (sm - bb)) + (a - bb)) * cs;  // TwoSum error
+                                r[e] = sm;
+                            }
                         }
                         if (last) {
                             const int pm = __ldg(&pr->m);
@@ -450,8 +462,6 @@ __global__ void __launch_bounds__(G_THREADS, 1) k_i8_grouped(const GParams p) {
                         }
                     }
                     if (!last) tc::tmem_st_wait();
-#pragma unroll
-                    for (int c = 0; c < 64; c++) acc[c] = 0.0;
                 }
             }
         }
