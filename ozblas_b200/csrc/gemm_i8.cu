@@ -37,6 +37,9 @@
 #include <mutex>
 #include <vector>
 
+#include <algorithm>
+
+#include "autotune.h"
 #include "ozb_device.cuh"
 #include "ozb_internal.h"
 #include "tc05.cuh"
@@ -624,6 +627,38 @@ int gemm_i8_core(cuozblasHandle_t *h, char ta, char tb, int m, int n, int k, dou
     const int ntiles = p.tiles_m * p.tiles_n;
     const int grid = ntiles < nsm ? ntiles : nsm;
     OZB_CHECK(cudaFuncSetAttribute(k_i8_gemm, cudaFuncAttributeMaxDynamicSharedMemorySize, I8_SMEM));
+    // Rasterisation strip height: any value gives the same bits, the fastest is
+    // measured once per shape (candidates write a scratch product with beta = 0).
+    {
+        std::vector<int> cand;
+        for (int sv : {12, 4, 8, 16, 24}) {
+            const int v = sv < p.tiles_m ? sv : p.tiles_m;
+            if (std::find(cand.begin(), cand.end(), v) == cand.end()) cand.push_back(v);
+        }
+        int pick = 0;
+        if (cand.size() > 1) {
+            const uint64_t mk = ar.mark();
+            double *scratch = ar.take<double>((uint64_t)m * n);
+            if (ar.ok) {
+                char key[160];
+                snprintf(key, sizeof(key), "i8:%d:%d:%d:%d:%d:%d:%d", p.tiles_m, p.tiles_n, nkb, nA, nB,
+                         h->fastMode != 0 ? 1 : 0, grid);
+                I8Params pt = p;
+                pt.C = scratch;
+                pt.ldc = m;
+                pt.alpha = 1.0;
+                pt.beta = 0.0;
+                pick = tune_pick(key, (int)cand.size(), 0, st->stream, [&](int i) {
+                    pt.strip = cand[(size_t)i];
+                    k_i8_gemm<<<grid, I8_THREADS, I8_SMEM, st->stream>>>(tmA, tmB, pt);
+                    return cudaGetLastError() == cudaSuccess ? 0 : (int)CUOZBLAS_STATUS_CUDA_ERROR;
+                });
+            }
+            ar.ok = true;
+            ar.release(mk);
+        }
+        p.strip = cand[(size_t)pick];
+    }
     ev_record(h, 2);
     counted(h);
     k_i8_gemm<<<grid, I8_THREADS, I8_SMEM, st->stream>>>(tmA, tmB, p);

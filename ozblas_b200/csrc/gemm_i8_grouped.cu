@@ -24,6 +24,7 @@
 #include <queue>
 #include <vector>
 
+#include "autotune.h"
 #include "ozb_device.cuh"
 #include "ozb_internal.h"
 #include "tc05.cuh"
@@ -481,6 +482,54 @@ int i8_schedule(int nA, int nB, int nkb, bool triangular, std::vector<int4> &ite
 
 constexpr int kI8DefaultCapG = 19;  // as gemm_i8.cu's kI8DefaultCap
 
+// Output tiles of all problems to CTAs.  mode 0: problems by decreasing tile
+// cost, each tile onto the least loaded CTA (longest first); mode 1: the same
+// problem order, each problem's tiles in strips of up to 12 tile rows
+// (column-major inside a strip) dealt round-robin, so CTAs running at the same
+// time share a problem's panels in L2.
+static void deal_tiles(int mode, int grid, const std::vector<GProb> &probs, const std::vector<int> &order,
+                       const std::vector<double> &cost, std::vector<int4> &tiles, std::vector<int> &cta_begin) {
+    std::vector<std::vector<int4>> per_cta((size_t)grid);
+    if (mode == 0) {
+        using Load = std::pair<double, int>;
+        std::priority_queue<Load, std::vector<Load>, std::greater<Load>> heap;
+        for (int c = 0; c < grid; c++) heap.push(Load(0.0, c));
+        for (int b : order) {
+            const GProb &pr = probs[(size_t)b];
+            if (pr.m <= 0 || pr.n <= 0) continue;
+            for (int tn = 0; tn < pr.tiles_n; tn++)
+                for (int tm = 0; tm < pr.tiles_m; tm++) {
+                    Load l = heap.top();
+                    heap.pop();
+                    per_cta[(size_t)l.second].push_back(make_int4(b, tm, tn, 0));
+                    l.first += cost[(size_t)b];
+                    heap.push(l);
+                }
+        }
+    } else {
+        int next = 0;
+        for (int b : order) {
+            const GProb &pr = probs[(size_t)b];
+            if (pr.m <= 0 || pr.n <= 0) continue;
+            const int strip = pr.tiles_m < 12 ? pr.tiles_m : 12;
+            for (int s0 = 0; s0 < pr.tiles_m; s0 += strip) {
+                const int rows = pr.tiles_m - s0 < strip ? pr.tiles_m - s0 : strip;
+                for (int tn = 0; tn < pr.tiles_n; tn++)
+                    for (int r = 0; r < rows; r++) {
+                        per_cta[(size_t)next].push_back(make_int4(b, s0 + r, tn, 0));
+                        next = next + 1 == grid ? 0 : next + 1;
+                    }
+            }
+        }
+    }
+    tiles.clear();
+    cta_begin.assign((size_t)grid + 1, 0);
+    for (int c = 0; c < grid; c++) {
+        cta_begin[(size_t)c + 1] = cta_begin[(size_t)c] + (int)per_cta[(size_t)c].size();
+        tiles.insert(tiles.end(), per_cta[(size_t)c].begin(), per_cta[(size_t)c].end());
+    }
+}
+
 int gemm_i8_batched(cuozblasHandle_t *h, char ta, char tb, int count, const int *m, const int *n, const int *k,
                     const double *alpha, const double *const *A, const int *lda, const double *const *B,
                     const int *ldb, const double *beta, double *const *C, const int *ldc) {
@@ -599,40 +648,25 @@ int gemm_i8_batched(cuozblasHandle_t *h, char ta, char tb, int count, const int 
     for (int b = 0; b < count; b++)
         if (m[b] > 0 && n[b] > 0) ntile_total += probs[(size_t)b].tiles_m * probs[(size_t)b].tiles_n;
     const int grid = ntile_total < nsm ? (ntile_total > 0 ? ntile_total : 1) : nsm;
-    // longest first onto the least loaded CTA
-    std::vector<std::vector<int4>> per_cta((size_t)grid);
-    using Load = std::pair<double, int>;
-    std::priority_queue<Load, std::vector<Load>, std::greater<Load>> heap;
-    for (int c = 0; c < grid; c++) heap.push(Load(0.0, c));
-    for (int b : order) {
-        const GProb &pr = probs[(size_t)b];
-        if (pr.m <= 0 || pr.n <= 0) continue;
-        for (int tn = 0; tn < pr.tiles_n; tn++)
-            for (int tm = 0; tm < pr.tiles_m; tm++) {
-                Load l = heap.top();
-                heap.pop();
-                per_cta[(size_t)l.second].push_back(make_int4(b, tm, tn, 0));
-                l.first += cost[(size_t)b];
-                heap.push(l);
-            }
-    }
-    std::vector<int> cta_begin((size_t)grid + 1, 0);
-    for (int c = 0; c < grid; c++) {
-        cta_begin[(size_t)c + 1] = cta_begin[(size_t)c] + (int)per_cta[(size_t)c].size();
-        tiles.insert(tiles.end(), per_cta[(size_t)c].begin(), per_cta[(size_t)c].end());
-    }
+    std::vector<int4> tiles_m1;
+    std::vector<int> cta_begin, cta_begin_m1;
+    deal_tiles(0, grid, probs, order, cost, tiles, cta_begin);
+    deal_tiles(1, grid, probs, order, cost, tiles_m1, cta_begin_m1);
     GProb *d_probs = ar.take<GProb>((uint64_t)count);
-    int4 *d_sched = ar.take<int4>(items.size() + groups.size() + tiles.size() + 1);
-    int *d_cta = ar.take<int>((uint64_t)grid + 1);
+    int4 *d_sched = ar.take<int4>(items.size() + groups.size() + 2 * tiles.size() + 1);
+    int *d_cta = ar.take<int>(2 * ((uint64_t)grid + 1));
     int *d_err = ar.take<int>(1);
     if (!ar.ok) return CUOZBLAS_STATUS_WORKSPACE;
     std::vector<int4> sched(items);
     sched.insert(sched.end(), groups.begin(), groups.end());
     sched.insert(sched.end(), tiles.begin(), tiles.end());
+    sched.insert(sched.end(), tiles_m1.begin(), tiles_m1.end());
+    std::vector<int> ctas(cta_begin);
+    ctas.insert(ctas.end(), cta_begin_m1.begin(), cta_begin_m1.end());
     OZB_CHECK(cudaMemcpyAsync(d_probs, probs.data(), sizeof(GProb) * count, cudaMemcpyHostToDevice, s));
     if (!sched.empty())
         OZB_CHECK(cudaMemcpyAsync(d_sched, sched.data(), sizeof(int4) * sched.size(), cudaMemcpyHostToDevice, s));
-    OZB_CHECK(cudaMemcpyAsync(d_cta, cta_begin.data(), sizeof(int) * (grid + 1), cudaMemcpyHostToDevice, s));
+    OZB_CHECK(cudaMemcpyAsync(d_cta, ctas.data(), sizeof(int) * ctas.size(), cudaMemcpyHostToDevice, s));
     OZB_CHECK(cudaMemsetAsync(d_err, 0, sizeof(int), s));
     GParams gp;
     gp.probs = d_probs;
@@ -641,16 +675,59 @@ int gemm_i8_batched(cuozblasHandle_t *h, char ta, char tb, int count, const int 
     gp.tiles = d_sched + items.size() + groups.size();
     gp.cta_begin = d_cta;
     gp.err = d_err;
-    h->nSplitA = (float)maxA;
-    h->nSplitB = (float)maxB;
-    h->nSplitC = (float)npairs_max;
-    ev_record(h, 2);
     if (ntile_total > 0) {
         static bool attr = false;
         if (!attr) {
             OZB_CHECK(cudaFuncSetAttribute(k_i8_grouped, cudaFuncAttributeMaxDynamicSharedMemorySize, G_SMEM));
             attr = true;
         }
+        // dealing order: same bits either way, the faster one is measured once per
+        // problem set (candidates write scratch products with beta = 0)
+        const uint64_t mk = ar.mark();
+        size_t outs = 0;
+        for (const GProb &pr : probs) outs += (size_t)(pr.m > 0 ? pr.m : 0) * (size_t)(pr.n > 0 ? pr.n : 0);
+        double *scratch = ar.take<double>(outs + 1);
+        GProb *d_trial = ar.take<GProb>((uint64_t)count);
+        int pick = 0;
+        if (ar.ok) {
+            std::vector<GProb> trial(probs);
+            size_t off = 0;
+            for (GProb &pr : trial) {
+                pr.C = scratch + off;
+                pr.ldc = pr.m > 1 ? pr.m : 1;
+                pr.beta = 0.0;
+                off += (size_t)(pr.m > 0 ? pr.m : 0) * (size_t)(pr.n > 0 ? pr.n : 0);
+            }
+            OZB_CHECK(cudaMemcpyAsync(d_trial, trial.data(), sizeof(GProb) * count, cudaMemcpyHostToDevice, s));
+            uint64_t hk = tune_hash(&count, sizeof(count));
+            for (const GOp &o : ops) {
+                const int sig[3] = {o.lines, o.k, o.S};
+                hk = tune_hash(sig, sizeof(sig), hk);
+            }
+            char key[96];
+            snprintf(key, sizeof(key), "i8grouped:%016llx:%d:%d", (unsigned long long)hk, h->fastMode != 0 ? 1 : 0,
+                     grid);
+            pick = tune_pick(key, 2, 0, s, [&](int i) {
+                GParams gt = gp;
+                gt.probs = d_trial;
+                gt.tiles = d_sched + items.size() + groups.size() + (i ? tiles.size() : 0);
+                gt.cta_begin = d_cta + (i ? grid + 1 : 0);
+                k_i8_grouped<<<grid, G_THREADS, G_SMEM, s>>>(gt);
+                return cudaGetLastError() == cudaSuccess ? 0 : (int)CUOZBLAS_STATUS_CUDA_ERROR;
+            });
+        }
+        ar.ok = true;
+        ar.release(mk);
+        if (pick == 1) {
+            gp.tiles = d_sched + items.size() + groups.size() + tiles.size();
+            gp.cta_begin = d_cta + grid + 1;
+        }
+    }
+    h->nSplitA = (float)maxA;
+    h->nSplitB = (float)maxB;
+    h->nSplitC = (float)npairs_max;
+    ev_record(h, 2);
+    if (ntile_total > 0) {
         counted(h);
         k_i8_grouped<<<grid, G_THREADS, G_SMEM, s>>>(gp);
         OZB_CHECK(cudaGetLastError());

@@ -167,3 +167,34 @@ def test_i8_batched_accuracy_uneven(oracle, handle, ozb, cuda):
         err = errors(oracle, A, B, C, m, n, k, np.linspace(0, m - 1, min(m, 16)).astype(int),
                      np.linspace(0, n - 1, min(n, 16)).astype(int))
         assert err <= 2 * U, (i, m, n, k, err)
+
+
+# ---- autotuned launch choices: speed only, never bits ----
+
+def test_autotune_changes_no_bits(oracle, handle, ozb, cuda, tmp_path, monkeypatch):
+    """Strip height (single) and dealing order (grouped) are measured per shape; the results equal the
+    untuned defaults bit for bit, and a choice is recorded in $OZBLAS_TUNE_CACHE."""
+    m, n, k = 700, 520, 300  # a shape no other test uses (6 tile rows: two strip heights to try)
+    A = oracle.phi_matrix(m, k, 1.0, 31)
+    B = oracle.phi_matrix(k, n, 1.0, 32)
+    cache = tmp_path / "tune.txt"
+    monkeypatch.setenv("OZBLAS_TUNE_CACHE", str(cache))
+    monkeypatch.setenv("OZBLAS_TUNE", "1")
+    tuned = run_i8(ozb, handle, cuda, A, B, m, n, k, fast=1)
+    monkeypatch.setenv("OZBLAS_TUNE", "0")
+    plain = run_i8(ozb, handle, cuda, A, B, m, n, k, fast=1)
+    assert bits_equal(tuned, plain)
+    assert "i8:" in cache.read_text()
+    shapes = [(100, 260, 300, 1.0), (390, 70, 129, 2.0), (64, 64, 64, 0.5), (257, 129, 513, 4.0)]
+    probs = _batch_case(oracle, shapes, "n", "n", 3)
+    outs = []
+    for tune in ("1", "0"):
+        monkeypatch.setenv("OZBLAS_TUNE", tune)
+        Cs = [cuda.zeros((p[1], p[0]), dtype=cuda.float64, device="cuda") for p in probs]
+        ozb.dgemm_i8_batched(handle, "n", "n", [p[0] for p in probs], [p[1] for p in probs], [p[2] for p in probs],
+                             [1.0] * 4, [dev(cuda, p[3]) for p in probs], [p[4] for p in probs],
+                             [dev(cuda, p[5]) for p in probs], [p[6] for p in probs], [0.0] * 4, Cs,
+                             [p[0] for p in probs])
+        outs.append([c.cpu().numpy() for c in Cs])
+    assert all(bits_equal(a, b) for a, b in zip(*outs))
+    assert "i8grouped:" in cache.read_text()
