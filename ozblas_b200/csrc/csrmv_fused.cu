@@ -63,8 +63,10 @@ __device__ __forceinline__ unsigned proof_body(double v, const TreePlan &pl) {
     return prove_levels<T>(hw, pl.hb[0], pl.need[0]);
 }
 
-// Proof of x's predicted chain: one element per thread; the last block
-// publishes validity, slice count and sigmas.
+// Proof of x's predicted chain.  One witness per level suffices, so a warp
+// stops as soon as it has proven every level the plan needs (and all warps stop
+// once any warp has); only an unproven chain reads the whole vector.  The last
+// block publishes validity, slice count and sigmas.
 template <int G>
 __global__ void __launch_bounds__(256) k_csr_proof(int n, const double *__restrict__ x, int rho, int maxS,
                                                    CsrScratch *sc, const int *__restrict__ gate) {
@@ -74,23 +76,30 @@ __global__ void __launch_bounds__(256) k_csr_proof(int n, const double *__restri
     const int t = threadIdx.x;
     load_plan(&sc->plan, pl);
     __syncthreads();
-    const int64_t i = (int64_t)blockIdx.x * blockDim.x + t;
-    if (pl.valid && pl.need[0]) {  // uniform
-        const double v = i < n ? x[i] : 0.0;
-        int T = plan_depth(pl, 0, __reduce_min_sync(0xffffffffu, exp_key(v)));
-        if (T > pl.L - 1) T = pl.L - 1;
+    const unsigned need = pl.need[0];
+    if (pl.valid && need) {  // uniform
+        const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+        const int64_t iw = (int64_t)blockIdx.x * blockDim.x + (t & ~31);  // the warp's first element
+        const int64_t K = iw < n ? ((int64_t)n - iw + stride - 1) / stride : 0;
+        int64_t i = (int64_t)blockIdx.x * blockDim.x + t;
         unsigned got = 0u;
-        switch (T) {
-            case 0: break;
-            case 1: got = proof_body<G, 1>(v, pl); break;
-            case 2: got = proof_body<G, 2>(v, pl); break;
-            case 3: got = proof_body<G, 3>(v, pl); break;
-            case 4: got = proof_body<G, 4>(v, pl); break;
-            case 5: got = proof_body<G, 5>(v, pl); break;
-            case 6: got = proof_body<G, 6>(v, pl); break;
-            default: got = proof_body<G, 7>(v, pl); break;
+        for (int64_t k = 0; k < K; k++, i += stride) {
+            if ((got & need) == need || (k & 7) == 7 && __ldcg(&sc->proven) == need) break;  // uniform per warp
+            const double v = i < n ? x[i] : 0.0;
+            int T = plan_depth(pl, 0, __reduce_min_sync(0xffffffffu, exp_key(v)));
+            if (T > pl.L - 1) T = pl.L - 1;
+            switch (T) {
+                case 0: break;
+                case 1: got |= proof_body<G, 1>(v, pl); break;
+                case 2: got |= proof_body<G, 2>(v, pl); break;
+                case 3: got |= proof_body<G, 3>(v, pl); break;
+                case 4: got |= proof_body<G, 4>(v, pl); break;
+                case 5: got |= proof_body<G, 5>(v, pl); break;
+                case 6: got |= proof_body<G, 6>(v, pl); break;
+                default: got |= proof_body<G, 7>(v, pl); break;
+            }
         }
-        if ((t & 31) == 0 && got) atomicOr(&sc->proven, got);
+        if ((t & 31) == 0 && got) atomicOr(&sc->proven, got & need);
     }
     __threadfence();
     __syncthreads();
@@ -98,7 +107,7 @@ __global__ void __launch_bounds__(256) k_csr_proof(int n, const double *__restri
     __syncthreads();
     if (!last || t != 0) return;
     __threadfence();
-    const int valid = pl.valid && (__ldcg(&sc->proven) & pl.need[0]) == pl.need[0];
+    const int valid = pl.valid && (__ldcg(&sc->proven) & need) == need;
     for (int s = 0; s < kCsrLv; s++) sc->sigma[s] = pl.sig[0][s];
     sc->nB = pl.ns[0];
     sc->valid = valid;
@@ -282,8 +291,7 @@ int csr_slow_rows_launch(cudaStream_t s, int m, const double *val, const int *ro
     return cudaGetLastError() == cudaSuccess ? CUOZBLAS_STATUS_SUCCESS : CUOZBLAS_STATUS_CUDA_ERROR;
 }
 
-// One thread per row, everything in registers.  A block's val/colind range
-// is staged in shared memory with coalesced loads; each row's tau chain runs
+// One thread per row, everything in registers: each row's tau chain runs
 // over its (at most kCsrRowMax) entries, keeping only the sigmas, then every
 // entry is re-cut with them while x's slices at its column come from the
 // proven chain; the pair products P[ia][ib] are the CPU's sequential fma
@@ -315,126 +323,6 @@ __device__ __forceinline__ void row_products(const double (&a)[kCsrRowMax], cons
 #pragma unroll
                     for (int ib = 0; ib < NB; ib++) P[ia][ib] = fma(sa[ia], sx[ib], P[ia][ib]);
         }
-    }
-}
-
-template <int SUM_MODE, int NA, int GX>
-__global__ void __launch_bounds__(kCsrThreads) k_csrmv_reg(int m, int n, const double *__restrict__ val,
-                                                           const int *__restrict__ colind,
-                                                           const int *__restrict__ rowptr,
-                                                           const double *__restrict__ x, int shift, int epsmode,
-                                                           int maxS, double alpha, double beta,
-                                                           double *__restrict__ y, CsrScratch *__restrict__ sc,
-                                                           int *__restrict__ slow_rows, int append_slow,
-                                                           VecStats *__restrict__ ystats, int ystats_index,
-                                                           const int *__restrict__ gate) {
-    if (gate && *gate == 0) return;  // uniform: a captured solver step that is switched off
-    constexpr int kStage = kCsrThreads * kCsrRowMax;
-    __shared__ double red[kCsrThreads / 32];
-    __shared__ double s_val[kStage];
-    __shared__ int s_col[kStage];
-    __shared__ int s_rp[kCsrThreads + 1];
-    __shared__ double xs_sigma[kCsrLv];
-    const int t = threadIdx.x;
-    const int r0 = blockIdx.x * kCsrThreads;
-    const int nrow = (m - r0 < kCsrThreads) ? m - r0 : kCsrThreads;
-    const int row = r0 + t;
-    const bool active = t < nrow;
-    // independent loads first: the block's row pointers and the old y
-    // (beta * y is formed even for beta = 0, as the reference does)
-    if (active) s_rp[t] = rowptr[r0 + t];
-    if (t == 0) s_rp[nrow] = rowptr[r0 + nrow];
-    const double yold = active ? y[row] : 0.0;
-    if (t < kCsrLv) xs_sigma[t] = sc->sigma[t];
-    const int valid = sc->valid;
-    const int nB = sc->nB;
-    __syncthreads();
-    if (!valid) return;  // uniform: the caller runs the general path
-    const int p0 = s_rp[0], p1 = s_rp[nrow];
-    const bool staged = (p1 - p0) <= kStage;
-    if (staged) {
-        const int cnt = p1 - p0;
-#pragma unroll 4
-        for (int i = t; i < cnt; i += kCsrThreads) {
-            s_val[i] = val[p0 + i];
-            s_col[i] = colind[p0 + i];
-        }
-    }
-    __syncthreads();
-    int lo = p0, len = 0;
-    if (active) {
-        lo = s_rp[t];
-        len = s_rp[t + 1] - lo;
-    }
-    bool defer = active && len > kCsrRowMax;
-    const bool work = active && !defer;
-    double a[kCsrRowMax], xv[kCsrRowMax];
-    int c[kCsrRowMax];
-#pragma unroll
-    for (int e = 0; e < kCsrRowMax; e++) {
-        const bool in = work && e < len;
-        double v = 0.0;
-        int ci = 0;
-        if (staged) {
-            const int idx = min(lo - p0 + e, kStage - 1);
-            v = s_val[idx];
-            ci = s_col[idx];
-        } else if (in) {
-            v = val[lo + e];
-            ci = colind[lo + e];
-        }
-        a[e] = in ? v : 0.0;
-        c[e] = in ? ci : -1;
-    }
-    if (n > 0) {  // all gathers in flight before any is used
-#pragma unroll
-        for (int e = 0; e < kCsrRowMax; e++) {
-            const double tx = x[c[e] >= 0 ? c[e] : 0];
-            xv[e] = c[e] >= 0 ? tx : 0.0;
-        }
-    } else {
-#pragma unroll
-        for (int e = 0; e < kCsrRowMax; e++) xv[e] = 0.0;
-    }
-    double sigA[NA];
-    int na = 0, z = 0;
-    if (work && !row_chain<NA>(a, len, shift, epsmode, maxS, sigA, na, z)) defer = true;
-    if (defer && append_slow) slow_rows[atomicAdd(&sc->nslow, 1)] = row;
-    {
-        const int zw = __reduce_max_sync(0xffffffffu, (work && !defer) ? z : 0);
-        if ((t & 31) == 0 && zw > 0) atomicMax(&sc->zmax, zw);
-    }
-    double ynew = 0.0;
-    const bool wrote = work && !defer;
-    if (wrote) {
-        double P[NA][kCsrLv];
-#pragma unroll
-        for (int i = 0; i < NA; i++)
-#pragma unroll
-            for (int j = 0; j < kCsrLv; j++) P[i][j] = 0.0;
-        switch (nB) {  // uniform
-            case 1: row_products<NA, 1, GX>(a, xv, len, na, sigA, xs_sigma, P); break;
-            case 2: row_products<NA, 2, GX>(a, xv, len, na, sigA, xs_sigma, P); break;
-            case 3: row_products<NA, 3, GX>(a, xv, len, na, sigA, xs_sigma, P); break;
-            case 4: row_products<NA, 4, GX>(a, xv, len, na, sigA, xs_sigma, P); break;
-            case 5: row_products<NA, 5, GX>(a, xv, len, na, sigA, xs_sigma, P); break;
-            case 6: row_products<NA, 6, GX>(a, xv, len, na, sigA, xs_sigma, P); break;
-            case 7: row_products<NA, 7, GX>(a, xv, len, na, sigA, xs_sigma, P); break;
-            default: row_products<NA, 8, GX>(a, xv, len, na, sigA, xs_sigma, P); break;
-        }
-        double tsum = 0.0;
-        if (SUM_MODE == 1)
-            tsum = nearsum_row<NA>(P, na, nB);
-        else
-            for_row_pairs<NA>(na, nB, [&](int ia, int ib) { tsum += P[ia][ib]; });
-        ynew = fma(alpha, tsum, beta * yold);
-        y[row] = ynew;
-    }
-    if (ystats) {  // uniform: statistics of the written y for a following DOT
-        double mx = 0.0;
-        int lsb = 0, bad = 0;
-        if (wrote) scan_elem(ynew, mx, lsb, bad);
-        scan_commit(ystats, ystats_index, mx, lsb, bad, red);
     }
 }
 
@@ -525,21 +413,189 @@ __global__ void __launch_bounds__(128) k_csrmv_slow(int nrows, const int *__rest
     }
 }
 
+// Persistent, software-pipelined form of the row kernel (same arithmetic per
+// row).  A CTA walks tiles of kCsrThreads rows; while it computes tile j from
+// one shared-memory slot, cp.async fills the other with tile j+1: its val and
+// colind ranges and old y during the row chains, then the gathers of x at its
+// columns during the products, and the row pointers of tile j+2.  Tiles whose
+// entries do not fit the slot are read from global memory directly.
+struct CsrSlot {
+    int rp[kCsrThreads + 4];
+    double yold[kCsrThreads];
+    double val[kCsrThreads * kCsrRowMax];
+    double xg[kCsrThreads * kCsrRowMax];
+    int col[kCsrThreads * kCsrRowMax];
+};
+
+template <int SUM_MODE, int NA, int GX>
+__global__ void __launch_bounds__(kCsrThreads, NA > 4 ? 2 : 4)
+    k_csrmv_pipe(int m, int n, const double *__restrict__ val, const int *__restrict__ colind,
+                 const int *__restrict__ rowptr, const double *__restrict__ x, int shift, int epsmode, int maxS,
+                 double alpha, double beta, double *__restrict__ y, CsrScratch *__restrict__ sc,
+                 int *__restrict__ slow_rows, int append_slow, VecStats *__restrict__ ystats, int ystats_index,
+                 const int *__restrict__ gate) {
+    if (gate && *gate == 0) return;  // uniform: a captured solver step that is switched off
+    constexpr int kStage = kCsrThreads * kCsrRowMax;
+    __shared__ CsrSlot slot[2];
+    __shared__ double xs_sigma[kCsrLv];
+    __shared__ double red[kCsrThreads / 32];
+    const int t = threadIdx.x;
+    const int ntiles = (m + kCsrThreads - 1) / kCsrThreads;
+    if (t < kCsrLv) xs_sigma[t] = sc->sigma[t];
+    const int valid = sc->valid;
+    const int nB = sc->nB;
+    __syncthreads();
+    if (!valid) return;  // uniform: the caller runs the general path
+    int tile = blockIdx.x;
+    if (tile >= ntiles) return;  // uniform
+
+    auto rows_of = [&](int tl) { return (m - tl * kCsrThreads < kCsrThreads) ? m - tl * kCsrThreads : kCsrThreads; };
+    auto issue_rp = [&](int tl, CsrSlot &S) {
+        const int r0 = tl * kCsrThreads, nrow = rows_of(tl);
+        if (t < nrow) cp_async4(&S.rp[t], rowptr + r0 + t);
+        if (t == 0) cp_async4(&S.rp[nrow], rowptr + r0 + nrow);
+    };
+    auto issue_vals = [&](int tl, CsrSlot &S) {  // needs S.rp
+        const int r0 = tl * kCsrThreads, nrow = rows_of(tl);
+        const int p0 = S.rp[0], cnt = S.rp[nrow] - p0;
+        if (t < nrow) cp_async8(&S.yold[t], y + r0 + t);
+        if (cnt <= kStage)
+            for (int i = t; i < cnt; i += kCsrThreads) {
+                cp_async8(&S.val[i], val + p0 + i);
+                cp_async4(&S.col[i], colind + p0 + i);
+            }
+    };
+    auto issue_gathers = [&](int tl, CsrSlot &S) {  // needs S.col
+        const int nrow = rows_of(tl);
+        const int cnt = S.rp[nrow] - S.rp[0];
+        if (cnt <= kStage && n > 0)
+            for (int i = t; i < cnt; i += kCsrThreads) cp_async8(&S.xg[i], x + S.col[i]);
+    };
+
+    // prologue: the first tile complete in slot 0, the next tile's row pointers in slot 1
+    issue_rp(tile, slot[0]);
+    cp_async_commit();
+    cp_async_wait_all();
+    __syncthreads();
+    issue_vals(tile, slot[0]);
+    cp_async_commit();
+    cp_async_wait_all();
+    __syncthreads();
+    issue_gathers(tile, slot[0]);
+    if (tile + (int)gridDim.x < ntiles) issue_rp(tile + gridDim.x, slot[1]);
+    cp_async_commit();
+
+    double smx = 0.0;  // statistics of the written y, folded once at the end
+    int slsb = 0, sbad = 0, zmax = 0;
+    for (int j = 0; tile < ntiles; j++, tile += gridDim.x) {
+        CsrSlot &S = slot[j & 1], &N = slot[(j & 1) ^ 1];
+        const int nxt = tile + gridDim.x;
+        cp_async_wait_all();  // this tile's gathers and the next tile's row pointers
+        __syncthreads();
+        if (nxt < ntiles) issue_vals(nxt, N);
+        cp_async_commit();
+        // ---- phase 1: this tile's entries and row chains
+        const int r0 = tile * kCsrThreads, nrow = rows_of(tile);
+        const int row = r0 + t;
+        const bool active = t < nrow;
+        const int p0 = S.rp[0], cnt = S.rp[nrow] - p0;
+        const bool staged = cnt <= kStage;
+        int lo = p0, len = 0;
+        if (active) {
+            lo = S.rp[t];
+            len = S.rp[t + 1] - lo;
+        }
+        bool defer = active && len > kCsrRowMax;
+        const bool work = active && !defer;
+        const double yold = active ? S.yold[t] : 0.0;
+        double a[kCsrRowMax];
+#pragma unroll
+        for (int e = 0; e < kCsrRowMax; e++) {
+            const bool in = work && e < len;
+            double v = 0.0;
+            if (staged)
+                v = S.val[min(lo - p0 + e, kStage - 1)];
+            else if (in)
+                v = val[lo + e];
+            a[e] = in ? v : 0.0;
+        }
+        double sigA[NA];
+        int na = 0, z = 0;
+        if (work && !row_chain<NA>(a, len, shift, epsmode, maxS, sigA, na, z)) defer = true;
+        if (defer && append_slow) slow_rows[atomicAdd(&sc->nslow, 1)] = row;
+        if (work && !defer) zmax = z > zmax ? z : zmax;
+        cp_async_wait_all();  // the next tile's val and colind
+        __syncthreads();
+        if (nxt < ntiles) issue_gathers(nxt, N);
+        if (nxt + (int)gridDim.x < ntiles) issue_rp(nxt + gridDim.x, S);  // S.rp is no longer read
+        cp_async_commit();
+        // ---- phase 2: products and sums
+        if (work && !defer) {
+            double xv[kCsrRowMax];
+#pragma unroll
+            for (int e = 0; e < kCsrRowMax; e++) {
+                double v = 0.0;
+                if (e < len && n > 0) v = staged ? S.xg[lo - p0 + e] : x[colind[lo + e]];
+                xv[e] = v;
+            }
+            double P[NA][kCsrLv];
+#pragma unroll
+            for (int i = 0; i < NA; i++)
+#pragma unroll
+                for (int jj = 0; jj < kCsrLv; jj++) P[i][jj] = 0.0;
+            switch (nB) {  // uniform
+                case 1: row_products<NA, 1, GX>(a, xv, len, na, sigA, xs_sigma, P); break;
+                case 2: row_products<NA, 2, GX>(a, xv, len, na, sigA, xs_sigma, P); break;
+                case 3: row_products<NA, 3, GX>(a, xv, len, na, sigA, xs_sigma, P); break;
+                case 4: row_products<NA, 4, GX>(a, xv, len, na, sigA, xs_sigma, P); break;
+                case 5: row_products<NA, 5, GX>(a, xv, len, na, sigA, xs_sigma, P); break;
+                case 6: row_products<NA, 6, GX>(a, xv, len, na, sigA, xs_sigma, P); break;
+                case 7: row_products<NA, 7, GX>(a, xv, len, na, sigA, xs_sigma, P); break;
+                default: row_products<NA, 8, GX>(a, xv, len, na, sigA, xs_sigma, P); break;
+            }
+            double tsum = 0.0;
+            if (SUM_MODE == 1)
+                tsum = nearsum_row<NA>(P, na, nB);
+            else
+                for_row_pairs<NA>(na, nB, [&](int ia, int ib) { tsum += P[ia][ib]; });
+            const double ynew = fma(alpha, tsum, beta * yold);
+            y[row] = ynew;
+            if (ystats) scan_elem(ynew, smx, slsb, sbad);
+        }
+    }
+    cp_async_wait_all();
+    {
+        const int zw = __reduce_max_sync(0xffffffffu, zmax);
+        if ((t & 31) == 0 && zw > 0) atomicMax(&sc->zmax, zw);
+    }
+    if (ystats) scan_commit(ystats, ystats_index, smx, slsb, sbad, red);
+}
+
+template <int SUM_MODE, int NA, int GX>
+static void launch_pipe_g(int ntiles, cudaStream_t s, const CsrmvArgs &a, CsrScratch *sc, int *slow, int append,
+                          VecStats *ys, int yi, const int *gate) {
+    static int per_sm = 0;  // resident CTAs per SM (once per instantiation)
+    if (per_sm == 0) {
+        int v = 0;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&v, k_csrmv_pipe<SUM_MODE, NA, GX>, kCsrThreads, 0);
+        per_sm = v > 0 ? v : 1;
+    }
+    const int cap = sm_count() * per_sm;
+    const int grid = ntiles < cap ? ntiles : cap;
+    k_csrmv_pipe<SUM_MODE, NA, GX><<<grid, kCsrThreads, 0, s>>>(a.m, a.n, a.val, a.colind, a.rowptr, a.x, a.shift,
+                                                                  a.epsmode, a.maxS, a.alpha, a.beta, a.y, sc, slow,
+                                                                  append, ys, yi, gate);
+}
+
 template <int SUM_MODE, int NA>
-static void launch_reg(int gx, int rb, cudaStream_t s, const CsrmvArgs &a, CsrScratch *sc, int *slow, int append,
+static void launch_reg(int gx, int ntiles, cudaStream_t s, const CsrmvArgs &a, CsrScratch *sc, int *slow, int append,
                        VecStats *ys, int yi, const int *gate) {
     if (gx >= 3)
-        k_csrmv_reg<SUM_MODE, NA, 3><<<rb, kCsrThreads, 0, s>>>(a.m, a.n, a.val, a.colind, a.rowptr, a.x, a.shift,
-                                                                 a.epsmode, a.maxS, a.alpha, a.beta, a.y, sc, slow,
-                                                                 append, ys, yi, gate);
+        launch_pipe_g<SUM_MODE, NA, 3>(ntiles, s, a, sc, slow, append, ys, yi, gate);
     else if (gx == 2)
-        k_csrmv_reg<SUM_MODE, NA, 2><<<rb, kCsrThreads, 0, s>>>(a.m, a.n, a.val, a.colind, a.rowptr, a.x, a.shift,
-                                                                 a.epsmode, a.maxS, a.alpha, a.beta, a.y, sc, slow,
-                                                                 append, ys, yi, gate);
+        launch_pipe_g<SUM_MODE, NA, 2>(ntiles, s, a, sc, slow, append, ys, yi, gate);
     else
-        k_csrmv_reg<SUM_MODE, NA, 1><<<rb, kCsrThreads, 0, s>>>(a.m, a.n, a.val, a.colind, a.rowptr, a.x, a.shift,
-                                                                 a.epsmode, a.maxS, a.alpha, a.beta, a.y, sc, slow,
-                                                                 append, ys, yi, gate);
+        launch_pipe_g<SUM_MODE, NA, 1>(ntiles, s, a, sc, slow, append, ys, yi, gate);
 }
 
 int vec_stats_launch(cudaStream_t s, int nsm, int n, const double *x, VecStats *vs, int index) {
@@ -555,7 +611,9 @@ int vec_stats_launch(cudaStream_t s, int nsm, int n, const double *x, VecStats *
 
 int csr_proof_launch(cudaStream_t s, int n, const double *x, int rho, int maxS, CsrScratch *sc, const int *gate) {
     const int gx = chain_group(rho, 3);
-    const int pb = n > 0 ? (int)(((int64_t)n + 255) / 256) : 1;
+    int pb = n > 0 ? (int)(((int64_t)n + 255) / 256) : 1;
+    const int pcap = sm_count() * 4;
+    if (pb > pcap) pb = pcap;
     if (gx >= 3)
         k_csr_proof<3><<<pb, 256, 0, s>>>(n, x, rho, maxS, sc, gate);
     else if (gx == 2)
