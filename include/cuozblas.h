@@ -226,6 +226,9 @@ int cuozblasDgemmI8Static(char transa, char transb, int32_t m, int32_t n, int32_
 /* Rule checks exported for the host-side tests (same code the kernels use). */
 int cuozblasRuleTau(double v);
 int cuozblasRuleRho(int32_t dim, int32_t splitEpsMode);
+/* Certified fast path of the correctly rounded sum (the NearSum result when it
+ * returns 1; 0: not proven, the library then runs NearSum itself). */
+int cuozblasRuleCrSum(int32_t n, const double *terms, double *out);
 /* Library build identification ("sm_100a ..."). */
 const char *cuozblasVersion(void);
 

@@ -97,6 +97,7 @@ _dsplita = _sig("cuozblasDcsrmvSplitA", [_HP, _ch, _i32, _i32, _i32, _vp, _vp, _
 _dcg = _sig("cuozblasDcg", [_HP, _ch, _i32, _i32, _vp, _vp, _vp, _vp, _vp, _vp, _i32, _d])
 rule_tau = _sig("cuozblasRuleTau", [_d])
 rule_rho = _sig("cuozblasRuleRho", [_i32, _i32])
+rule_crsum = _sig("cuozblasRuleCrSum", [_i32, _vp, _PD])
 _version = _sig("cuozblasVersion", [], C.c_char_p)
 
 #: every C-ABI symbol include/cuozblas.h declares (checked by the CPU tests)
@@ -104,6 +105,7 @@ C_ABI_SYMBOLS = [
     "cuozblasHandleCreate", "cuozblasHandleDestroy", "cuozblasSetStream", "cuozblasGetLaunchCount", "cuozblasDdot", "cuozblasDnrm2",
     "cuozblasDaxpy", "cuozblasDgemv", "cuozblasDgemm", "cuozblasDcsrmv", "cuozblasDcsrmvSplitA", "cuozblasDcg",
     "cuozblasDgemmI8", "cuozblasDgemmI8Static", "cuozblasDgemmI8Batched", "cuozblasRuleTau", "cuozblasRuleRho",
+    "cuozblasRuleCrSum",
     "cuozblasVersion",
 ]
 

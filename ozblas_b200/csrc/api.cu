@@ -9,6 +9,7 @@
 
 #include <new>
 
+#include "crsum.h"
 #include "ozb_internal.h"
 
 namespace ozb {
@@ -111,6 +112,12 @@ const char *cuozblasVersion(void) { return "cuozblas-b200 0.1 (sm_100a; plain FP
 
 int cuozblasRuleTau(double v) { return tau_rule(v); }
 int cuozblasRuleRho(int32_t dim, int32_t mode) { return rho_rule(dim, mode); }
+
+int cuozblasRuleCrSum(int32_t n, const double *terms, double *out) {
+    CrSum cs;
+    for (int32_t i = 0; i < n; i++) cs.add(terms[i]);
+    return cs.finish(*out) ? 1 : 0;
+}
 
 int cuozblasHandleCreate(cuozblasHandle_t *h, uint64_t workSizeBytes) {
     if (!h) return CUOZBLAS_STATUS_INVALID_VALUE;

@@ -192,6 +192,12 @@ __device__ __forceinline__ void ns_transformk_row(double (&v)[NA][kCsrLv], int n
 
 template <int NA>
 __device__ __forceinline__ double nearsum_row(double (&v)[NA][kCsrLv], int na, int nb) {
+    {
+        CrSum cs;
+        for_row_pairs<NA>(na, nb, [&](int a, int b) { cs.add(v[a][b]); });
+        double out;
+        if (cs.finish(out)) return out;
+    }
     const int n = na * nb;
     const double eps = pow2(-53);
     double res, r, delta, r2, res2, mu, delta2, tmp;
@@ -571,6 +577,313 @@ __global__ void __launch_bounds__(kCsrThreads, NA > 4 ? 2 : 4)
     if (ystats) scan_commit(ystats, ystats_index, smx, slsb, sbad, red);
 }
 
+// ---------------------------------------------------------------------------
+// Lean row kernel (rows of at most NA <= 4 levels).  Same arithmetic per row
+// as k_csrmv_pipe, with less work around it:
+//  * each row is staged zero padded into kCsrRowMax slots (cp.async with zero
+//    fill), so a thread reads its entries and gathered x values with 16-byte
+//    shared loads and needs no masks;
+//  * the row chain keeps its slices (the products use them directly instead
+//    of cutting every entry again);
+//  * the row max is taken over the high words of |r| (one integer max per
+//    entry); the full value is looked at only when the high word leaves tau
+//    open (an exact power of two, zero, subnormal) — rows with Inf or NaN
+//    entries go to the general per-row kernel;
+//  * the pair products are held for exactly NA x nB pairs, so FSum and the
+//    certified correctly rounded sum run without guards (pairs beyond a
+//    row's own levels are +0 and change neither sum).
+struct LeanSlot {
+    int rp[kCsrThreads + 4];
+    double yold[kCsrThreads];
+    double val[kCsrThreads * kCsrRowMax];  // entry e of row t at lean_pos(t, e); zero padded
+    double xg[kCsrThreads * kCsrRowMax];   // x at the entry's column, same positions
+    int col[kCsrThreads * kCsrRowMax];     // row t's columns at t * kCsrRowMax + e
+};
+static_assert(kCsrRowMax == 8, "lean rows hold 8 entries as four 16-byte pairs");
+
+// Entry e of row t: the row's four 16-byte pairs are rotated by (t >> 1) & 3
+// so that the 16-byte reads of eight consecutive rows hit distinct banks.
+__device__ __forceinline__ int lean_pos(int t, int e) {
+    return t * kCsrRowMax + ((((e >> 1) ^ (t >> 1)) & 3) << 1) + (e & 1);
+}
+
+__device__ __forceinline__ void lean_read(const double *base, int t, double (&v)[kCsrRowMax]) {
+#pragma unroll
+    for (int i = 0; i < 4; i++) {
+        const double2 p = *reinterpret_cast<const double2 *>(base + t * kCsrRowMax + (((i ^ (t >> 1)) & 3) << 1));
+        v[2 * i] = p.x;
+        v[2 * i + 1] = p.y;
+    }
+}
+
+__device__ __forceinline__ unsigned hi_abs(double v) { return (unsigned)__double2hiint(v) & 0x7fffffffu; }
+
+// tau_rule(max_e |r_e|) given mh, the max of the entries' |high words| (all
+// entries finite): a normal max whose high word has mantissa bits set lies
+// above every tau threshold of its binade, so tau = exponent + 1.
+__device__ __forceinline__ int lean_tau(unsigned mh, const double (&r)[kCsrRowMax]) {
+    if ((mh & 0xfffffu) != 0u && mh >= 0x00100000u) return (int)(mh >> 20) - 1022;
+    double mx = 0.0;
+#pragma unroll
+    for (int e = 0; e < kCsrRowMax; e++) mx = fmax(mx, fabs(r[e]));
+    return tau_rule(mx);
+}
+
+// The row's own chain (src/cpu/ozblas_split.cpp:779-815) as row_chain
+// computes it, keeping the slices.  Returns false when the row needs more
+// than NA levels (and nSplitMax allows more) or holds Inf / NaN.
+template <int NA>
+__device__ __forceinline__ bool lean_chain(double (&r)[kCsrRowMax], int len, int shift, int epsmode, int maxS,
+                                           double (&sa)[kCsrRowMax][NA], int &na, int &z) {
+    na = 0;
+    z = 0;
+#pragma unroll
+    for (int e = 0; e < kCsrRowMax; e++)
+#pragma unroll
+        for (int s = 0; s < NA; s++) sa[e][s] = 0.0;
+    if (len <= 0) return true;
+    unsigned mh = 0u;
+#pragma unroll
+    for (int e = 0; e < kCsrRowMax; e++) mh = max(mh, hi_abs(r[e]));
+    if (mh >= 0x7ff00000u) return false;  // Inf or NaN: the general kernel
+    const int rho = rho_rule(len, epsmode);
+    z = maxS;
+    bool fin = false;
+#pragma unroll
+    for (int s = 0; s < NA; s++) {
+        if (!fin && s < maxS) {
+            const double sg = shift_sigma(0.75 * pow2(rho + lean_tau(mh, r)), shift);
+            unsigned nh = 0u;
+#pragma unroll
+            for (int e = 0; e < kCsrRowMax; e++) {
+                const double sl = (r[e] + sg) - sg;
+                r[e] = r[e] - sl;
+                sa[e][s] = sl;
+                nh = max(nh, hi_abs(r[e]));
+            }
+            na = s + 1;
+            mh = nh;
+            bool zero = false;
+            if (nh == 0u) {
+                unsigned lo = 0u;
+#pragma unroll
+                for (int e = 0; e < kCsrRowMax; e++) lo |= (unsigned)__double2loint(r[e]);
+                zero = lo == 0u;
+            }
+            if (zero) {
+                z = s;
+                fin = true;
+            }
+        }
+    }
+    return fin || na >= maxS;
+}
+
+template <int SUM_MODE, int NA, int NB, int GX>
+__device__ __forceinline__ double lean_products(const double (&sa)[kCsrRowMax][NA], const double (&xv)[kCsrRowMax],
+                                                int len, int na, const double *xsig) {
+    double P[NA][NB];
+#pragma unroll
+    for (int i = 0; i < NA; i++)
+#pragma unroll
+        for (int j = 0; j < NB; j++) P[i][j] = 0.0;
+#pragma unroll
+    for (int e = 0; e < kCsrRowMax; e++) {
+        if (e < len) {
+            double sx[NB];
+            cut_tree<GX, NB - 1>(xv[e], xsig, sx);
+#pragma unroll
+            for (int ia = 0; ia < NA; ia++)
+#pragma unroll
+                for (int ib = 0; ib < NB; ib++) P[ia][ib] = fma(sa[e][ia], sx[ib], P[ia][ib]);
+        }
+    }
+    if (SUM_MODE == 0) {
+        double t = 0.0;
+#pragma unroll
+        for (int ik = 0; ik < NA + NB - 1; ik++)
+#pragma unroll
+            for (int ia = 0; ia < NA; ia++)
+                if (ik - ia >= 0 && ik - ia < NB) t += P[ia][ik - ia];
+        return t;
+    } else {
+        CrSum cs;
+#pragma unroll
+        for (int ik = 0; ik < NA + NB - 1; ik++)
+#pragma unroll
+            for (int ia = 0; ia < NA; ia++)
+                if (ik - ia >= 0 && ik - ia < NB) cs.add(P[ia][ik - ia]);
+        double out;
+        if (cs.finish(out)) return out;
+        double Q[NA][kCsrLv];
+#pragma unroll
+        for (int i = 0; i < NA; i++)
+#pragma unroll
+            for (int j = 0; j < kCsrLv; j++) Q[i][j] = j < NB ? P[i][j] : 0.0;
+        return nearsum_row<NA>(Q, na, NB);
+    }
+}
+
+template <int SUM_MODE, int NA, int GX>
+__global__ void __launch_bounds__(kCsrThreads, NA >= 4 ? 3 : 4)
+    k_csrmv_lean(int m, int n, const double *__restrict__ val, const int *__restrict__ colind,
+                 const int *__restrict__ rowptr, const double *__restrict__ x, int shift, int epsmode, int maxS,
+                 double alpha, double beta, double *__restrict__ y, CsrScratch *__restrict__ sc,
+                 int *__restrict__ slow_rows, int append_slow, VecStats *__restrict__ ystats, int ystats_index,
+                 const int *__restrict__ gate) {
+    if (gate && *gate == 0) return;  // uniform: a captured solver step that is switched off
+    __shared__ __align__(16) LeanSlot slot[2];
+    __shared__ double xs_sigma[kCsrLv];
+    __shared__ double red[kCsrThreads / 32];
+    const int t = threadIdx.x;
+    const int ntiles = (m + kCsrThreads - 1) / kCsrThreads;
+    if (t < kCsrLv) xs_sigma[t] = sc->sigma[t];
+    const int valid = sc->valid;
+    const int nB = sc->nB;
+    __syncthreads();
+    if (!valid) return;  // uniform: the caller runs the general path
+    int tile = blockIdx.x;
+    if (tile >= ntiles) return;  // uniform
+
+    auto rows_of = [&](int tl) { return (m - tl * kCsrThreads < kCsrThreads) ? m - tl * kCsrThreads : kCsrThreads; };
+    auto issue_rp = [&](int tl, LeanSlot &S) {
+        const int r0 = tl * kCsrThreads, nrow = rows_of(tl);
+        if (t < nrow) cp_async4(&S.rp[t], rowptr + r0 + t);
+        if (t == 0) cp_async4(&S.rp[nrow], rowptr + r0 + nrow);
+    };
+    auto issue_vals = [&](int tl, LeanSlot &S) {  // needs S.rp
+        const int r0 = tl * kCsrThreads;
+        if (t >= rows_of(tl)) return;
+        const double *dummy = y + r0 + t;  // a valid address for copies that read nothing
+        cp_async8(&S.yold[t], dummy);
+        const int lo = S.rp[t], len = S.rp[t + 1] - lo;
+        if (len > kCsrRowMax) return;
+#pragma unroll
+        for (int e = 0; e < kCsrRowMax; e++) {
+            const bool in = e < len;
+            cp_async8_zfill(&S.val[lean_pos(t, e)], in ? (const void *)(val + lo + e) : (const void *)dummy,
+                            in ? 8u : 0u);
+            cp_async4_zfill(&S.col[t * kCsrRowMax + e], in ? (const void *)(colind + lo + e) : (const void *)dummy,
+                            in ? 4u : 0u);
+        }
+    };
+    auto issue_gathers = [&](int tl, LeanSlot &S) {  // needs S.rp and S.col
+        const int r0 = tl * kCsrThreads;
+        if (t >= rows_of(tl)) return;
+        const double *dummy = y + r0 + t;
+        const int lo = S.rp[t], len = S.rp[t + 1] - lo;
+        if (len > kCsrRowMax) return;
+        const int4 c0 = *reinterpret_cast<const int4 *>(&S.col[t * kCsrRowMax]);
+        const int4 c1 = *reinterpret_cast<const int4 *>(&S.col[t * kCsrRowMax + 4]);
+        const int cc[kCsrRowMax] = {c0.x, c0.y, c0.z, c0.w, c1.x, c1.y, c1.z, c1.w};
+#pragma unroll
+        for (int e = 0; e < kCsrRowMax; e++) {
+            const bool in = e < len && n > 0;
+            cp_async8_zfill(&S.xg[lean_pos(t, e)], in ? (const void *)(x + cc[e]) : (const void *)dummy,
+                            in ? 8u : 0u);
+        }
+    };
+
+    // prologue: the first tile complete in slot 0, the next tile's row pointers in slot 1
+    issue_rp(tile, slot[0]);
+    cp_async_commit();
+    cp_async_wait_all();
+    __syncthreads();
+    issue_vals(tile, slot[0]);
+    cp_async_commit();
+    cp_async_wait_all();
+    __syncthreads();
+    issue_gathers(tile, slot[0]);
+    if (tile + (int)gridDim.x < ntiles) issue_rp(tile + gridDim.x, slot[1]);
+    cp_async_commit();
+
+    double smx = 0.0;  // statistics of the written y, folded once at the end
+    int slsb = 0, sbad = 0, zmax = 0;
+    for (int j = 0; tile < ntiles; j++, tile += gridDim.x) {
+        LeanSlot &S = slot[j & 1], &N = slot[(j & 1) ^ 1];
+        const int nxt = tile + gridDim.x;
+        cp_async_wait_all();  // this tile's gathers and the next tile's row pointers
+        __syncthreads();
+        if (nxt < ntiles) issue_vals(nxt, N);
+        cp_async_commit();
+        // ---- phase 1: this tile's row chains
+        const int r0 = tile * kCsrThreads, nrow = rows_of(tile);
+        const int row = r0 + t;
+        const bool active = t < nrow;
+        int len = 0;
+        if (active) len = S.rp[t + 1] - S.rp[t];
+        bool defer = active && len > kCsrRowMax;
+        const bool work = active && !defer;
+        const double yold = active ? S.yold[t] : 0.0;
+        double sa[kCsrRowMax][NA];
+        int na = 0, z = 0;
+        if (work) {
+            double r[kCsrRowMax];
+            lean_read(S.val, t, r);
+            if (!lean_chain<NA>(r, len, shift, epsmode, maxS, sa, na, z)) defer = true;
+        }
+        if (defer && append_slow) slow_rows[atomicAdd(&sc->nslow, 1)] = row;
+        if (work && !defer) zmax = z > zmax ? z : zmax;
+        cp_async_wait_all();  // the next tile's val and colind
+        __syncthreads();
+        if (nxt < ntiles) issue_gathers(nxt, N);
+        if (nxt + (int)gridDim.x < ntiles) issue_rp(nxt + gridDim.x, S);  // S.rp is no longer read
+        cp_async_commit();
+        // ---- phase 2: products and sums
+        if (work && !defer) {
+            double xv[kCsrRowMax];
+            lean_read(S.xg, t, xv);
+            double tsum;
+            switch (nB) {  // uniform
+                case 1: tsum = lean_products<SUM_MODE, NA, 1, GX>(sa, xv, len, na, xs_sigma); break;
+                case 2: tsum = lean_products<SUM_MODE, NA, 2, GX>(sa, xv, len, na, xs_sigma); break;
+                case 3: tsum = lean_products<SUM_MODE, NA, 3, GX>(sa, xv, len, na, xs_sigma); break;
+                case 4: tsum = lean_products<SUM_MODE, NA, 4, GX>(sa, xv, len, na, xs_sigma); break;
+                case 5: tsum = lean_products<SUM_MODE, NA, 5, GX>(sa, xv, len, na, xs_sigma); break;
+                case 6: tsum = lean_products<SUM_MODE, NA, 6, GX>(sa, xv, len, na, xs_sigma); break;
+                case 7: tsum = lean_products<SUM_MODE, NA, 7, GX>(sa, xv, len, na, xs_sigma); break;
+                default: tsum = lean_products<SUM_MODE, NA, 8, GX>(sa, xv, len, na, xs_sigma); break;
+            }
+            const double ynew = fma(alpha, tsum, beta * yold);
+            y[row] = ynew;
+            if (ystats) scan_elem(ynew, smx, slsb, sbad);
+        }
+    }
+    cp_async_wait_all();
+    {
+        const int zw = __reduce_max_sync(0xffffffffu, zmax);
+        if ((t & 31) == 0 && zw > 0) atomicMax(&sc->zmax, zw);
+    }
+    if (ystats) scan_commit(ystats, ystats_index, smx, slsb, sbad, red);
+}
+
+template <int SUM_MODE, int NA, int GX>
+static void launch_lean_g(int ntiles, cudaStream_t s, const CsrmvArgs &a, CsrScratch *sc, int *slow, int append,
+                          VecStats *ys, int yi, const int *gate) {
+    static int per_sm = 0;  // resident CTAs per SM (once per instantiation)
+    if (per_sm == 0) {
+        int v = 0;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&v, k_csrmv_lean<SUM_MODE, NA, GX>, kCsrThreads, 0);
+        per_sm = v > 0 ? v : 1;
+    }
+    const int cap = sm_count() * per_sm;
+    const int grid = ntiles < cap ? ntiles : cap;
+    k_csrmv_lean<SUM_MODE, NA, GX><<<grid, kCsrThreads, 0, s>>>(a.m, a.n, a.val, a.colind, a.rowptr, a.x, a.shift,
+                                                                  a.epsmode, a.maxS, a.alpha, a.beta, a.y, sc, slow,
+                                                                  append, ys, yi, gate);
+}
+
+template <int SUM_MODE, int NA>
+static void launch_lean(int gx, int ntiles, cudaStream_t s, const CsrmvArgs &a, CsrScratch *sc, int *slow,
+                        int append, VecStats *ys, int yi, const int *gate) {
+    if (gx >= 3)
+        launch_lean_g<SUM_MODE, NA, 3>(ntiles, s, a, sc, slow, append, ys, yi, gate);
+    else if (gx == 2)
+        launch_lean_g<SUM_MODE, NA, 2>(ntiles, s, a, sc, slow, append, ys, yi, gate);
+    else
+        launch_lean_g<SUM_MODE, NA, 1>(ntiles, s, a, sc, slow, append, ys, yi, gate);
+}
+
 template <int SUM_MODE, int NA, int GX>
 static void launch_pipe_g(int ntiles, cudaStream_t s, const CsrmvArgs &a, CsrScratch *sc, int *slow, int append,
                           VecStats *ys, int yi, const int *gate) {
@@ -634,22 +947,26 @@ int csr_rows_launch(cudaStream_t s, const CsrmvArgs &a, CsrScratch *sc, int *slo
     const int rb = (a.m + kCsrThreads - 1) / kCsrThreads;
     // levels per row held on chip: 2 when the caller knows the rows need at
     // most 2 (the CG's pre-split count), 6 when they need more than 4, else 4
-    const int na = (a.na_hint > 0 && a.na_hint <= 2) ? 2 : (a.na_hint > 4 ? 6 : 4);
+    const int na = (a.na_hint > 0 && a.na_hint <= 2) ? 2 : a.na_hint == 3 ? 3 : (a.na_hint > 4 ? 6 : 4);
     const int append = fixed_slow < 0 ? 1 : 0;
     if (a.sum_mode == 1) {
         if (na == 2)
-            launch_reg<1, 2>(gx, rb, s, a, sc, slow, append, ystats, ystats_index, gate);
+            launch_lean<1, 2>(gx, rb, s, a, sc, slow, append, ystats, ystats_index, gate);
+        else if (na == 3)
+            launch_lean<1, 3>(gx, rb, s, a, sc, slow, append, ystats, ystats_index, gate);
         else if (na == 6)
             launch_reg<1, 6>(gx, rb, s, a, sc, slow, append, ystats, ystats_index, gate);
         else
-            launch_reg<1, 4>(gx, rb, s, a, sc, slow, append, ystats, ystats_index, gate);
+            launch_lean<1, 4>(gx, rb, s, a, sc, slow, append, ystats, ystats_index, gate);
     } else {
         if (na == 2)
-            launch_reg<0, 2>(gx, rb, s, a, sc, slow, append, ystats, ystats_index, gate);
+            launch_lean<0, 2>(gx, rb, s, a, sc, slow, append, ystats, ystats_index, gate);
+        else if (na == 3)
+            launch_lean<0, 3>(gx, rb, s, a, sc, slow, append, ystats, ystats_index, gate);
         else if (na == 6)
             launch_reg<0, 6>(gx, rb, s, a, sc, slow, append, ystats, ystats_index, gate);
         else
-            launch_reg<0, 4>(gx, rb, s, a, sc, slow, append, ystats, ystats_index, gate);
+            launch_lean<0, 4>(gx, rb, s, a, sc, slow, append, ystats, ystats_index, gate);
     }
     for (int c0 = 0; c0 < fixed_slow; c0 += kCsrSlowChunk) {
         const int nr = fixed_slow - c0 < kCsrSlowChunk ? fixed_slow - c0 : kCsrSlowChunk;

@@ -7,6 +7,7 @@
 // (src/cpu/ozblas_sum.cpp:10-112), restated below over terms at a stride.
 // Both end with C = fma(alpha, t, beta * C) (src/cpu/ozblas_sum.cpp:366).
 #pragma once
+#include "crsum.h"
 #include "ozb_device.cuh"
 
 namespace ozb {
@@ -69,8 +70,15 @@ __device__ inline void ns_transformk(int n, double *v, int64_t ld, double rho, d
     r = tau2 - (res - tau1);
 }
 
-// Correctly rounded sum of n terms at stride ld; the terms are overwritten.
+// Correctly rounded sum of n terms at stride ld; the terms are overwritten
+// when the certified fast path (crsum.h) cannot prove its result.
 __device__ inline double nearsum(int n, double *v, int64_t ld) {
+    {
+        CrSum cs;
+        for (int i = 0; i < n; i++) cs.add(v[i * ld]);
+        double out;
+        if (cs.finish(out)) return out;
+    }
     const double eps = pow2(-53);
     double res, r, delta, r2, res2, mu, delta2, tmp;
     ns_transformk(n, v, ld, 0., res, r);

@@ -307,6 +307,32 @@ def test_dcsrmv_long_rows_and_deep_rows(sm, oracle, handle, ozb, cuda):
 
 
 @pytest.mark.parametrize("sm", [0, 1])
+def test_dcsrmv_special_rows(sm, oracle, handle, ozb, cuda):
+    """Rows of exact powers of two, zero entries and rows, subnormal entries and a wide in-row range."""
+    rowptr, colind, val = stencil_case(oracle, 10, 9, 8)
+    n = len(rowptr) - 1
+    rng = np.random.default_rng(15)
+    for r in range(0, n, 7):
+        lo, hi = rowptr[r], rowptr[r + 1]
+        kind = (r // 7) % 5
+        if kind == 0:
+            val[lo:hi] = rng.choice([-1.0, 1.0], hi - lo) * 2.0 ** rng.integers(-3, 4, hi - lo)
+        elif kind == 1:
+            val[lo:hi] = 0.0
+        elif kind == 2:
+            val[lo] = 0.0
+            val[hi - 1] = -0.0
+        elif kind == 3:
+            val[lo:hi] *= 2.0 ** -1060
+        else:
+            val[lo] *= 2.0 ** 40
+    x = oracle.phi_vector(n, 1.0, 2)
+    y0 = oracle.phi_vector(n, 1.0, 3)
+    for beta in (0.0, 1.5):
+        _csr_run(oracle, handle, ozb, cuda, rowptr, colind, val, x, y0, 1.0, beta, sm)
+
+
+@pytest.mark.parametrize("sm", [0, 1])
 def test_dcsrmv_x_chain_general_path(sm, oracle, handle, ozb, cuda):
     """x whose chain is not the predicted one, and x needing more than 8 levels."""
     rowptr, colind, val = stencil_case(oracle, 10, 9, 8)
