@@ -266,8 +266,21 @@ int cuozblasDcsrmv(cuozblasHandle_t *h, char trans, int32_t m, int32_t n, int32_
     if (h->fastMode == 0 && h->splitEpsMode != 2) {
         bool done = false;
         int fa = 0, fb = 0;
-        OZB_TRY(csrmv_fused(h, m, n, alpha, val, colind, rowptr, x, beta, y, 1, 4, &done, &fa, &fb));
+        auto &memo = state(h)->csr_memo;
+        const int flags = h->splitEpsMode * 64 + maxS;
+        const bool same = memo.val == val && memo.colind == colind && memo.rowptr == rowptr && memo.m == m &&
+                          memo.n == n && memo.nnz == nnz && memo.flags == flags;
+        const int hint = same && memo.nA > 0 ? memo.nA : 4;
+        OZB_TRY(csrmv_fused(h, m, n, alpha, val, colind, rowptr, x, beta, y, 1, hint, &done, &fa, &fb));
         if (done) {
+            memo.val = val;
+            memo.colind = colind;
+            memo.rowptr = rowptr;
+            memo.m = m;
+            memo.n = n;
+            memo.nnz = nnz;
+            memo.flags = flags;
+            memo.nA = fa;
             csrmv_info(h, fa, fb);
             return finish(h, t0);
         }

@@ -637,22 +637,21 @@ __device__ __forceinline__ bool lean_chain(double (&r)[kCsrRowMax], int len, int
                                            double (&sa)[kCsrRowMax][NA], int &na, int &z) {
     na = 0;
     z = 0;
-#pragma unroll
-    for (int e = 0; e < kCsrRowMax; e++)
-#pragma unroll
-        for (int s = 0; s < NA; s++) sa[e][s] = 0.0;
-    if (len <= 0) return true;
     unsigned mh = 0u;
 #pragma unroll
     for (int e = 0; e < kCsrRowMax; e++) mh = max(mh, hi_abs(r[e]));
     if (mh >= 0x7ff00000u) return false;  // Inf or NaN: the general kernel
-    const int rho = rho_rule(len, epsmode);
-    z = maxS;
-    bool fin = false;
+    const int rho = rho_rule(len > 0 ? len : 1, epsmode);
+    z = len > 0 ? maxS : 0;
+    bool fin = len <= 0;
+    double sg = 1.0;
+    // Levels after the first zero remainder cut zeros into +0 slices (with the
+    // last sigma), which is what the products need there; only levels beyond
+    // nSplitMax are set to zero explicitly.
 #pragma unroll
     for (int s = 0; s < NA; s++) {
-        if (!fin && s < maxS) {
-            const double sg = shift_sigma(0.75 * pow2(rho + lean_tau(mh, r)), shift);
+        if (s < maxS) {  // uniform
+            if (!fin) sg = shift_sigma(0.75 * pow2(rho + lean_tau(mh, r)), shift);
             unsigned nh = 0u;
 #pragma unroll
             for (int e = 0; e < kCsrRowMax; e++) {
@@ -661,19 +660,24 @@ __device__ __forceinline__ bool lean_chain(double (&r)[kCsrRowMax], int len, int
                 sa[e][s] = sl;
                 nh = max(nh, hi_abs(r[e]));
             }
-            na = s + 1;
-            mh = nh;
-            bool zero = false;
-            if (nh == 0u) {
-                unsigned lo = 0u;
+            if (!fin) {
+                na = s + 1;
+                bool zero = false;
+                if (nh == 0u) {
+                    unsigned lo = 0u;
 #pragma unroll
-                for (int e = 0; e < kCsrRowMax; e++) lo |= (unsigned)__double2loint(r[e]);
-                zero = lo == 0u;
+                    for (int e = 0; e < kCsrRowMax; e++) lo |= (unsigned)__double2loint(r[e]);
+                    zero = lo == 0u;
+                }
+                if (zero) {
+                    z = s;
+                    fin = true;
+                }
             }
-            if (zero) {
-                z = s;
-                fin = true;
-            }
+            mh = nh;
+        } else {
+#pragma unroll
+            for (int e = 0; e < kCsrRowMax; e++) sa[e][s] = 0.0;
         }
     }
     return fin || na >= maxS;

@@ -26,6 +26,14 @@ struct State {
     int64_t splitA_ld = 0;        // slice stride of the pre-split A (cuozblasDcsrmvSplitA)
     cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};  // phase timers (split A/B, products)
     uint64_t launches = 0;        // kernels this handle has launched (cuozblasGetLaunchCount)
+    // The matrix of the last fused CSRMV and the level count its rows needed:
+    // the next call on the same matrix holds that many levels per row on chip
+    // (rows that need more go to the per-row kernel, so a stale count costs
+    // only speed).
+    struct {
+        const void *val = nullptr, *colind = nullptr, *rowptr = nullptr;
+        int m = -1, n = -1, nnz = -1, flags = 0, nA = 0;
+    } csr_memo;
 };
 
 
