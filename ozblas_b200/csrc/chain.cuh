@@ -64,6 +64,7 @@ __device__ __forceinline__ double tau_floor_threshold(int t) {
 struct TreePlan {
     double sig[2][kChainLevels];  // predicted sigma of each level
     unsigned hb[2][kChainLevels]; // level s is proven by a |slice s+1| whose high word exceeds hb
+    int ith[2][kChainLevels];     // ... or by a slice s+1 of more than ith grid units (integer form)
     unsigned need[2];             // levels whose prediction must be proven (bit s)
     int tau0[2], G0[2];           // tau of level 0, exponent of its grid
     int z[2], ns[2];              // first all-zero level, slice count (count rule)
@@ -107,6 +108,7 @@ __device__ inline void make_plan(const VecStats *vs, int rho, int maxS, bool sam
         pl.need[v] = lim > 0 ? (1u << lim) - 1u : 0u;
         for (int s = 0; s < kChainLevels; s++) {
             pl.hb[v][s] = 0xffffffffu;
+            pl.ith[v][s] = 0x7fffffff;
             if (s >= lim) continue;
             const double thr = tau_floor_threshold(tau0 + (s + 1) * (rho - 54));
             if (thr < 0.0) {
@@ -115,6 +117,9 @@ __device__ inline void make_plan(const VecStats *vs, int rho, int maxS, bool sam
             }
             const double bnd = thr + pow2(G0 - (s + 1) * d);
             pl.hb[v][s] = (unsigned)(dbits(bnd) >> 32) + 1u;
+            // |a| g > bnd  <=  |a| > floor(bnd / g), g = 2^(G0 - (s+1) d) (exact scaling, < 2^27)
+            const double q = bnd * pow2((s + 1) * d - G0);
+            pl.ith[v][s] = q < 2147483647.0 ? (int)floor(q) : 0x7fffffff;
         }
     }
     pl.L = L;

@@ -320,7 +320,7 @@ static int prepare_tree() {
 }
 
 int dot_tree_prepare() {
-    int r = 0;
+    int r = dot_i8_prepare();
     r |= prepare_tree<1, true>() | prepare_tree<1, false>() | prepare_tree<2, true>() | prepare_tree<2, false>();
     r |= prepare_tree<3, true>() | prepare_tree<3, false>() | prepare_tree<4, true>() | prepare_tree<4, false>();
     return r ? CUOZBLAS_STATUS_CUDA_ERROR : CUOZBLAS_STATUS_SUCCESS;
@@ -351,6 +351,10 @@ int dot_tree_launch(cudaStream_t s, int nsm, int n, const double *x, const doubl
     const int G = chain_group(rho, 4);  // levels cut from one base value
     const bool same = (x == y);
     const bool aligned = ((reinterpret_cast<uintptr_t>(x) | reinterpret_cast<uintptr_t>(y)) & 15u) == 0;
+    // 16-byte aligned vectors with 2 or 3 digits per level take the tensor-core
+    // pass (it holds every valid plan); the FP64 tree pass takes the rest
+    if (aligned && n > 0 && dot_i8_digits(rho) > 0 && !getenv("OZBLAS_DOT_TREE"))
+        return dot_i8_launch(s, nsm, n, x, y, rho, sum_mode, sc, gate);
     int fblocks = (int)(((int64_t)n + 2 * kDotThreads - 1) / (2 * kDotThreads));
     if (fblocks > nsm) fblocks = nsm;  // ~250 registers per thread: one 256-thread block per SM
     if (fblocks < 1) fblocks = 1;
@@ -404,6 +408,8 @@ int dot_fused(cuozblasHandle_t *h, int n, const double *x, const double *y, doub
     ar.release(mk);
     DotStatus res;
     memcpy(&res, st->h_dbl, sizeof(res));
+    if (res.status != 1 && getenv("OZBLAS_DOT_TRACE"))
+        fprintf(stderr, "cuozblas: dot fused not used (n=%d, reason bits %d)\n", n, res.pad);
     if (res.status == 1) {
         *done = true;
         *nA = res.ns0;

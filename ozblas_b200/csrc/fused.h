@@ -15,12 +15,16 @@ struct alignas(8) DotStatus {  // copied to the host in one piece
     double result;
 };
 
+constexpr int kDotDigitRows = 32;  // levels x digits per vector in the tensor-core pass (at most)
+
 struct DotScratch {
     VecStats vs;                        // first pass: max, lowest set bit, Inf/NaN of x and y
     TreePlan plan;                      // the chains planned from vs (plan_launch)
     double P[kDotLevels * kDotLevels];  // exact slice products P[ia * 8 + ib]
+    long long T[kDotDigitRows * kDotDigitRows];  // tensor-core pass: digit-pair sums T[p * 32 + q]
     unsigned proven[2];                 // levels whose predicted tau some element proved
     unsigned ticket;                    // blocks of pass 2 that are done
+    int err;                            // tensor-core pass: a bounded wait ran out
     DotStatus out;
 };
 
@@ -45,6 +49,13 @@ int dot_tree_launch(cudaStream_t s, int nsm, int n, const double *x, const doubl
                     int sum_mode, DotScratch *sc, const int *gate);
 // Sets the kernels' shared-memory attribute up front (before a capture).
 int dot_tree_prepare();
+// The tensor-core form of pass 2 (dot_i8.cu): digits per level for rho (0:
+// not applicable), its launch (every valid plan) and its shared-memory
+// attributes.
+int dot_i8_digits(int rho);
+int dot_i8_launch(cudaStream_t s, int nsm, int n, const double *x, const double *y, int rho, int sum_mode,
+                  DotScratch *sc, const int *gate);
+int dot_i8_prepare();
 
 // Plans the chain(s) from the first pass's statistics once, into `plan`,
 // and zeroes the statistics for the next use (one thread; `gate` as above).

@@ -234,6 +234,42 @@ def test_ddot_unaligned_and_odd(n, sm, oracle, handle, ozb, cuda):
         assert np.float64(nr).view(np.int64) == np.float64(nr_ref).view(np.int64), (n, sm, nr, nr_ref)
 
 
+@pytest.mark.parametrize("n,phi", [((1 << 23) + 12345, 1.0), (5000001, 1.0)])
+@pytest.mark.parametrize("sm", [0, 1])
+def test_ddot_tensor_core_pass(n, phi, sm, oracle, handle, ozb, cuda):
+    """Long vectors (2 and 3 digits per level): pass 2 runs on the INT8 tensor cores.  The chains of
+    these vectors are the predicted ones, so the fused path must be the one that answers."""
+    x = oracle.phi_vector(n, phi, 1)
+    y = oracle.phi_vector(n, phi, 2)
+    handle.sumMode = sm
+    dx, dy = dev(cuda, x), dev(cuda, y)
+    l0 = handle.launch_count()
+    d = ozb.ddot(handle, n, dx, dy)
+    assert handle.launch_count() - l0 == 3  # scan, plan, tensor-core pass: no fallback to the general path
+    r, info = oracle.ddot(make_flags(sumMode=sm), x, y)
+    assert np.float64(d).view(np.int64) == np.float64(r).view(np.int64), (d, r)
+    assert (handle.nSplitA, handle.nSplitB) == (info.nSplitA, info.nSplitB)
+    nr = ozb.dnrm2(handle, n, dx)
+    nr_ref, _ = oracle.dnrm2(make_flags(sumMode=sm), x)
+    assert np.float64(nr).view(np.int64) == np.float64(nr_ref).view(np.int64), (nr, nr_ref)
+
+
+def test_ddot_tensor_core_pass_matches_tree(oracle, handle, ozb, cuda, monkeypatch):
+    """The INT8 tensor-core pass and the FP64 tree pass give the same bits (2 and 3 digits per level)."""
+    for n, phi in ((3000, 0.5), (100003, 1.0), (1 << 20, 0.25), (1 << 20, 2.0), ((1 << 22) + 5, 1.0),
+                   ((1 << 23) + 3, 0.5)):
+        x = dev(cuda, oracle.phi_vector(n, phi, 3))
+        y = dev(cuda, oracle.phi_vector(n, phi, 4))
+        for sm in (0, 1):
+            handle.sumMode = sm
+            monkeypatch.delenv("OZBLAS_DOT_TREE", raising=False)
+            a = (ozb.ddot(handle, n, x, y), ozb.dnrm2(handle, n, x), ozb.ddot(handle, n, y, y))
+            monkeypatch.setenv("OZBLAS_DOT_TREE", "1")
+            b = (ozb.ddot(handle, n, x, y), ozb.dnrm2(handle, n, x), ozb.ddot(handle, n, y, y))
+            monkeypatch.delenv("OZBLAS_DOT_TREE", raising=False)
+            assert np.array(a).view(np.int64).tolist() == np.array(b).view(np.int64).tolist(), (n, phi, sm, a, b)
+
+
 def test_invalid_arguments(handle, ozb, cuda):
     x = cuda.zeros(8, dtype=cuda.float64, device="cuda")
     with pytest.raises(ozb.OzblasError) as e:
