@@ -46,7 +46,7 @@ constexpr int kDiQuads = 3;                      // producer groups of 4 warps
 constexpr int kDiStagesPerQuad = 2;              // each group fills its two stages in turn
 constexpr int kDiStages = kDiQuads * kDiStagesPerQuad;
 constexpr int kDiProducers = kDiQuads * 128;     // producer threads
-constexpr int kDiThreads = kDiProducers + 32;    // + the MMA warp
+constexpr int kDiThreads = kDiProducers;         // each group issues its own MMAs
 constexpr int kDiTile = 128 * 128;               // 128 rows x 128 bytes
 constexpr int kDiStage = 2 * kDiTile;            // A and B tiles
 constexpr int kDiMaxJobs = 512;                  // per CTA: 128 * 512 products of at most 2^14 each
@@ -65,73 +65,96 @@ __device__ __forceinline__ void di_transpose4(uint32_t w0, uint32_t w1, uint32_t
     }
 }
 
-// Cut E consecutive elements of vector `vi` into levels 0..L-1 and write their
-// digit rows (row RP c + s D + j, K bytes E u .. E u + E - 1 of the tile).
-// While levels of the vector wait for their proof (`pending`), the warp votes.
-template <int D, int E, int RP>
-__device__ __forceinline__ void di_digits(const double (&v)[E], const TreePlan &pl, int vi, int L, int G,
-                                          uint8_t *tile, int c, int u, unsigned pending, unsigned &prov) {
+// Cut E consecutive elements into all kDotLevels levels (levels past the
+// plan only fill rows that are never read) and write their digit rows (row
+// s D + j below `rows`, K bytes E u .. E u + E - 1; `rows` is the chunk's first
+// row plus this thread's byte offset, `ub16` its 16-byte chunk index times 16,
+// before the swizzle).  sk[s] = sigma_s + K g_s with K = 0x80808080: t = base
+// + sk[s] is rounded on the same grid, and its low word is (RN_{g_s}(base) /
+// g_s + K) mod 2^32, so w = lo(t_s) - lo(t_{s-1}) * 2^d + K * 2^d is a_s + K
+// (at a group start lo(t_{s-1}) is taken as K); the bytes of w are the
+// balanced digits of a_s plus 0x80 each, removed after the byte transpose.
+// Every G levels the base becomes the remainder.  VOTE: levels still waiting
+// for their proof (`pending`) are voted on with |a_s|.  No branch depends on
+// data or on the plan inside the level loop.
+template <int D, int E, int G, bool VOTE>
+__device__ __forceinline__ void di_digits(const double (&v)[E], const double *sk, int d, const int *ith,
+                                          uint32_t rows, unsigned pending, unsigned &prov) {
     static_assert(E == 4 || E == 8, "4 or 8 elements per thread");
-    const int d = pl.d;
+    constexpr uint32_t K = 0x80808080u;
+    const uint32_t kd = K << d;
+    // the 128-byte swizzle XORs bits 4-6 of the address with the row's low 3
+    // bits; `rows` has its own 16-byte chunk index there and row multiples of
+    // 1024 above, so row r's address is (rows ^ ((r & 7) << 4)) + r * 128
+    uint32_t bx[8];
+#pragma unroll
+    for (int k = 0; k < 8; k++) bx[k] = rows ^ (uint32_t)(k << 4);
     double base[E], tprev[E];
     uint32_t lop[E];
 #pragma unroll
-    for (int e = 0; e < E; e++) {
-        base[e] = v[e];
-        tprev[e] = 0.0;
-        lop[e] = 0u;
-    }
+    for (int e = 0; e < E; e++) base[e] = v[e];
 #pragma unroll
     for (int s = 0; s < kDotLevels; s++) {
-        if (s < L) {  // uniform
-            const double sg = pl.sig[vi][s];
-            if (s > 0 && s % G == 0) {  // uniform: the next group cuts the remainder
-                const double sp = pl.sig[vi][s - 1];
+        const double sg = sk[s];
+        if (s > 0 && s % G == 0) {  // compile-time: the next group cuts the remainder
+            const double sp = sk[s - 1];
 #pragma unroll
-                for (int e = 0; e < E; e++) {
-                    base[e] = base[e] - (tprev[e] - sp);
-                    lop[e] = 0u;
-                }
-            }
-            uint32_t w[E];
+            for (int e = 0; e < E; e++) base[e] = base[e] - (tprev[e] - sp);
+        }
+        uint32_t w[E];
 #pragma unroll
-            for (int e = 0; e < E; e++) {
-                const double tt = base[e] + sg;
-                const uint32_t lo = (uint32_t)__double2loint(tt);
-                w[e] = lo - (lop[e] << d);
-                lop[e] = lo;
-                tprev[e] = tt;
-            }
-            if (s >= 1 && (pending & (1u << (s - 1)))) {  // uniform
-                const int th = pl.ith[vi][s - 1];
-                bool hit = false;
+        for (int e = 0; e < E; e++) {
+            const double tt = base[e] + sg;
+            const uint32_t lo = (uint32_t)__double2loint(tt);
+            w[e] = (s % G == 0) ? lo : lo - (lop[e] << d) + kd;
+            lop[e] = lo;
+            tprev[e] = tt;
+        }
+        if (VOTE && s >= 1) {
+            bool hit = false;
+            const int th = ith[s - 1];
 #pragma unroll
-                for (int e = 0; e < E; e++) hit |= abs((int)w[e]) > th;
+            for (int e = 0; e < E; e++) hit |= abs((int)(w[e] - K)) > th;
+            if ((pending >> (s - 1)) & 1u)
                 if (__any_sync(0xffffffffu, hit)) prov |= 1u << (s - 1);
+        }
+        uint32_t lo4[D];
+        di_transpose4<D>(w[0], w[1], w[2], w[3], lo4);
+        if (E == 8) {
+            uint32_t hi4[D];
+            di_transpose4<D>(w[E == 8 ? 4 : 0], w[E == 8 ? 5 : 1], w[E == 8 ? 6 : 2], w[E == 8 ? 7 : 3], hi4);
+#pragma unroll
+            for (int j = 0; j < D; j++) {
+                const int r = s * D + j;
+                asm volatile("st.shared.v2.u32 [%0], {%1, %2};" ::"r"(bx[r & 7] + (uint32_t)(r * 128)),
+                             "r"(lo4[j] ^ K), "r"(hi4[j] ^ K)
+                             : "memory");
             }
+        } else {
 #pragma unroll
-            for (int e = 0; e < E; e++) w[e] = (w[e] + 0x80808080u) ^ 0x80808080u;
-            uint32_t lo4[D];
-            di_transpose4<D>(w[0], w[1], w[2], w[3], lo4);
-            if (E == 8) {
-                uint32_t hi4[D];
-                di_transpose4<D>(w[E == 8 ? 4 : 0], w[E == 8 ? 5 : 1], w[E == 8 ? 6 : 2], w[E == 8 ? 7 : 3], hi4);
-#pragma unroll
-                for (int j = 0; j < D; j++) {
-                    const int r = RP * c + s * D + j;
-                    *reinterpret_cast<uint2 *>(tile + r * 128 + (((u >> 1) ^ (r & 7)) << 4) + ((u & 1) << 3)) =
-                        make_uint2(lo4[j], hi4[j]);
-                }
-            } else {
-#pragma unroll
-                for (int j = 0; j < D; j++) {
-                    const int r = RP * c + s * D + j;
-                    *reinterpret_cast<uint32_t *>(tile + r * 128 + (((u >> 2) ^ (r & 7)) << 4) + ((u & 3) << 2)) =
-                        lo4[j];
-                }
+            for (int j = 0; j < D; j++) {
+                const int r = s * D + j;
+                asm volatile("st.shared.u32 [%0], %1;" ::"r"(bx[r & 7] + (uint32_t)(r * 128)), "r"(lo4[j] ^ K)
+                             : "memory");
             }
         }
     }
+}
+
+// Barrier of one producer group (named barrier `id`, 128 threads), and the
+// same barrier returning whether any thread of the group passed `pred`.
+__device__ __forceinline__ void di_group_sync(int id) { asm volatile("bar.sync %0, 128;" ::"r"(id) : "memory"); }
+__device__ __forceinline__ bool di_group_any(int id, bool pred) {
+    uint32_t r;
+    asm volatile(
+        "{\n\t.reg .pred p, q;\n\t"
+        "setp.ne.u32 p, %1, 0;\n\t"
+        "bar.red.or.pred q, %2, 128, p;\n\t"
+        "selp.u32 %0, 1, 0, q;\n\t}\n"
+        : "=r"(r)
+        : "r"((uint32_t)pred), "r"(id)
+        : "memory");
+    return r != 0;
 }
 
 template <int E>
@@ -192,7 +215,7 @@ __device__ void di_finish(DotScratch *sc, const TreePlan &pl, bool same, int sum
 
 // RP digit rows per chunk of 128 elements: 16 (two digits, up to 8 levels) or
 // 32 (three digits, up to 8 levels); a job is 128 / RP chunks.
-template <bool SAME, int D, int RP>
+template <bool SAME, int D, int RP, int G>
 __global__ void __launch_bounds__(kDiThreads, 1)
     k_dot_i8(int n, const double *__restrict__ x, const double *__restrict__ y, int sum_mode,
              DotScratch *__restrict__ sc, const int *__restrict__ gate) {
@@ -204,32 +227,35 @@ __global__ void __launch_bounds__(kDiThreads, 1)
     extern __shared__ uint8_t di_raw[];
     uint8_t *smem = (uint8_t *)(((uintptr_t)di_raw + 1023) & ~(uintptr_t)1023);
     __shared__ TreePlan pl;
-    __shared__ __align__(8) uint64_t full[kDiStages], empty[kDiStages], done;
+    __shared__ __align__(8) uint64_t empty[kDiStages], done;
     __shared__ uint32_t tmem_slot;
     __shared__ volatile int abort_flag;
     __shared__ unsigned long long red[RP * RP];
     __shared__ double fin[2][kDotLevels * kDotLevels];
     __shared__ int last;
     const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
+    __shared__ double sk[2][kDotLevels];
     load_plan(&sc->plan, pl);
     for (int i = t; i < RP * RP; i += kDiThreads) red[i] = 0ull;
     __syncthreads();
+    if (t < 2 * kDotLevels) {  // sigma_s + 0x80808080 g_s: exact (an integer below 2^53 times g_s)
+        const int v = t / kDotLevels, s = t % kDotLevels;
+        sk[v][s] = pl.sig[v][s] + 2155905152.0 * pow2(pl.G0[v] - s * pl.d);
+    }
+    __syncthreads();
     const int L = pl.L;
     const bool work = pl.valid != 0 && L * D <= RP;  // (L * D > RP cannot happen for a valid plan)
-    const int G = chain_group(54 - pl.d, 4);
+    // (the group size G is the plan's, chain_group(rho, 4); the launch picks it)
     const int64_t njobs = ((int64_t)n + JOB - 1) / JOB;
     const int myjobs = work && blockIdx.x < njobs ? (int)((njobs - 1 - blockIdx.x) / gridDim.x + 1) : 0;
 
     if (t == 0) {
-        for (int q = 0; q < kDiStages; q++) {
-            tc::mbar_init(&full[q], 4);
-            tc::mbar_init(&empty[q], 1);
-        }
-        tc::mbar_init(&done, 1);
+        for (int q = 0; q < kDiStages; q++) tc::mbar_init(&empty[q], 1);
+        tc::mbar_init(&done, kDiQuads);
         abort_flag = 0;
         tc::fence_mbar_init();
     }
-    if (warp == kDiQuads * 4) tc::tmem_alloc(&tmem_slot, 128);
+    if (warp == 0) tc::tmem_alloc(&tmem_slot, 512);  // one 128-column accumulator per group
     tc::fence_before_sync();
     __syncthreads();
     tc::fence_after_sync();
@@ -240,72 +266,75 @@ __global__ void __launch_bounds__(kDiThreads, 1)
         // ------------------------------------------------------------ producers
         const int quad = t >> 7, tq = t & 127;
         const int c = tq / LPC, u = tq % LPC;
+        const int rowoff = RP * c * 128 + (E == 8 ? (u & 1) << 3 : (u & 3) << 2);
+        const int ub16 = (E == 8 ? u >> 1 : u >> 2) << 4;
+        const int d = pl.d;
         auto first = [&](int i) {
             return ((int64_t)blockIdx.x + (int64_t)i * gridDim.x) * JOB + c * 128 + E * u;
         };
-        double xn[E], yn[E];  // the next job's elements, loaded one job ahead
-#pragma unroll
-        for (int e = 0; e < E; e++) xn[e] = yn[e] = 0.0;
-        if (quad < myjobs) {
-            di_load<E>(x, first(quad), n, xn);
-            if (!SAME) di_load<E>(y, first(quad), n, yn);
-        }
-        for (int k = 0, i = quad; i < myjobs; k++, i += kDiQuads) {
-            double xv[E], yv[E];
-#pragma unroll
-            for (int e = 0; e < E; e++) {
-                xv[e] = xn[e];
-                yv[e] = yn[e];
-            }
-            if (i + kDiQuads < myjobs) {
-                di_load<E>(x, first(i + kDiQuads), n, xn);
-                if (!SAME) di_load<E>(y, first(i + kDiQuads), n, yn);
-            }
-            const int st = quad * kDiStagesPerQuad + (k & 1);
-            if (!tc::mbar_wait(&empty[st], ((k >> 1) & 1) ^ 1, &abort_flag, &sc->err, 1, kDiWaitNs)) break;
-            uint8_t *tileA = smem + st * kDiStage;
-            di_digits<D, E, RP>(xv, pl, 0, L, G, tileA, c, u, pl.need[0] & ~prov[0], prov[0]);
-            if (!SAME) di_digits<D, E, RP>(yv, pl, 1, L, G, tileA + kDiTile, c, u, pl.need[1] & ~prov[1], prov[1]);
-            tc::fence_proxy_async();
-            __syncwarp();
-            if (lane == 0) tc::mbar_arrive(&full[st]);
-        }
-    } else if (lane == 0) {
-        // ------------------------------------------------------------ MMA issuer
         const uint32_t idesc = tc::idesc_i8(128, 128);
-        uint32_t ph = 0u;  // bit st: parity of the next fill of stage st
-        int consumed = 0;
-        uint64_t t_last = tc::globaltimer();
-        while (consumed < myjobs) {
-            bool any = false;
-#pragma unroll 1
-            for (int st = 0; st < kDiStages; st++) {
-                if (!tc::mbar_test_wait(&full[st], (ph >> st) & 1u)) continue;
+        const uint32_t acc = tmem_base + 128 * quad;  // this group's accumulator columns
+        // job k of this group (i = quad + k * kDiQuads), elements in xv / yv;
+        // thread 0 of the group issues the group's MMAs once all its warps
+        // have written the stage (group barrier 1 + quad)
+        auto produce = [&](int k, const double (&xv)[E], const double (&yv)[E]) -> bool {
+            const int st = quad * kDiStagesPerQuad + (k & 1);
+            const bool ok = tc::mbar_wait(&empty[st], ((k >> 1) & 1) ^ 1, &abort_flag, &sc->err, 1, kDiWaitNs);
+            if (di_group_any(1 + quad, !ok)) return false;  // the whole group leaves together
+            uint8_t *tileA = smem + st * kDiStage;
+            const uint32_t ra = tc::smem_u32(tileA) + rowoff + ub16;
+            const unsigned px = pl.need[0] & ~prov[0];
+            if (px)
+                di_digits<D, E, G, true>(xv, sk[0], d, pl.ith[0], ra, px, prov[0]);
+            else
+                di_digits<D, E, G, false>(xv, sk[0], d, pl.ith[0], ra, 0u, prov[0]);
+            if (!SAME) {
+                const unsigned py = pl.need[1] & ~prov[1];
+                if (py)
+                    di_digits<D, E, G, true>(yv, sk[1], d, pl.ith[1], ra + kDiTile, py, prov[1]);
+                else
+                    di_digits<D, E, G, false>(yv, sk[1], d, pl.ith[1], ra + kDiTile, 0u, prov[1]);
+            }
+            tc::fence_proxy_async();
+            di_group_sync(1 + quad);
+            if (tq == 0) {
                 tc::fence_after_sync();
-                const uint32_t sa = tc::smem_u32(smem + st * kDiStage), sb = SAME ? sa : sa + kDiTile;
+                const uint32_t sa = tc::smem_u32(tileA), sb = SAME ? sa : sa + kDiTile;
                 const uint64_t adesc = tc::smem_desc_k_sw128(sa), bdesc = tc::smem_desc_k_sw128(sb);
 #pragma unroll
                 for (int kk = 0; kk < 4; kk++)  // +32 bytes along K = +2 in 16-byte units
-                    tc::mma_i8(tmem_base, adesc + 2 * kk, bdesc + 2 * kk, idesc, (consumed > 0 || kk > 0) ? 1u : 0u);
+                    tc::mma_i8(acc, adesc + 2 * kk, bdesc + 2 * kk, idesc, (k > 0 || kk > 0) ? 1u : 0u);
                 tc::mma_commit(&empty[st]);
-                ph ^= 1u << st;
-                consumed++;
-                any = true;
             }
-            if (any) {
-                t_last = tc::globaltimer();
-            } else if (abort_flag) {
-                break;
-            } else if (tc::globaltimer() - t_last > kDiWaitNs) {
-                abort_flag = 1;
-                atomicExch(&sc->err, 2);
-                break;
-            }
+            return true;
+        };
+        // two register sets: the next job's elements load while this one is cut
+        double xa[E], ya[E], xb[E], yb[E];
+#pragma unroll
+        for (int e = 0; e < E; e++) xa[e] = ya[e] = xb[e] = yb[e] = 0.0;
+        if (quad < myjobs) {
+            di_load<E>(x, first(quad), n, xa);
+            if (!SAME) di_load<E>(y, first(quad), n, ya);
         }
-        tc::mma_commit(&done);  // also when nothing was issued or a wait gave up
-        // every MMA of this CTA completes before TMEM is released (bounded)
-        const uint64_t t0 = tc::globaltimer();
-        while (!tc::mbar_try_wait(&done, 0) && tc::globaltimer() - t0 < 100000000ull) {
+        for (int k = 0, i = quad; i < myjobs; k += 2, i += 2 * kDiQuads) {
+            if (i + kDiQuads < myjobs) {
+                di_load<E>(x, first(i + kDiQuads), n, xb);
+                if (!SAME) di_load<E>(y, first(i + kDiQuads), n, yb);
+            }
+            if (!produce(k, xa, ya)) break;
+            if (i + kDiQuads >= myjobs) break;
+            if (i + 2 * kDiQuads < myjobs) {
+                di_load<E>(x, first(i + 2 * kDiQuads), n, xa);
+                if (!SAME) di_load<E>(y, first(i + 2 * kDiQuads), n, ya);
+            }
+            if (!produce(k + 1, xb, yb)) break;
+        }
+        if (tq == 0) {
+            tc::mma_commit(&done);  // also when nothing was issued or the group gave up
+            // every MMA of this group completes before TMEM is released (bounded)
+            const uint64_t t0 = tc::globaltimer();
+            while (!tc::mbar_try_wait(&done, 0) && tc::globaltimer() - t0 < 100000000ull) {
+            }
         }
     }
 
@@ -313,9 +342,16 @@ __global__ void __launch_bounds__(kDiThreads, 1)
     if (warp < 4 && myjobs > 0) {
         if (tc::mbar_wait(&done, 0, &abort_flag, &sc->err, 3, kDiWaitNs) && !abort_flag) {
             tc::fence_after_sync();
-            uint32_t v[32];
-            tc::tmem_ld_32x32b_x32(tmem_base + ((uint32_t)(32 * warp) << 16) + 32 * warp, v);
-            tc::tmem_ld_wait();
+            long long sum[32];
+#pragma unroll
+            for (int q = 0; q < 32; q++) sum[q] = 0;
+            for (int g = 0; g < kDiQuads && g < myjobs; g++) {  // groups that ran a job
+                uint32_t v[32];
+                tc::tmem_ld_32x32b_x32(tmem_base + ((uint32_t)(32 * warp) << 16) + 128 * g + 32 * warp, v);
+                tc::tmem_ld_wait();
+#pragma unroll
+                for (int q = 0; q < 32; q++) sum[q] += (long long)(int)v[q];
+            }
             const int rows = L * D;
             // lane l holds TMEM row 32 warp + l: chunk c, digit row p; its
             // diagonal block starts at column RP c
@@ -323,21 +359,21 @@ __global__ void __launch_bounds__(kDiThreads, 1)
             if (p < rows) {
 #pragma unroll
                 for (int q = 0; q < RP; q++) {
-                    const int val = (int)(off ? v[(16 + q) & 31] : v[q & 31]);
-                    if (q < rows && val != 0) atomicAdd(&red[p * RP + q], (unsigned long long)(long long)val);
+                    const long long val = off ? sum[(16 + q) & 31] : sum[q & 31];
+                    if (q < rows && val != 0) atomicAdd(&red[p * RP + q], (unsigned long long)val);
                 }
             }
         }
     }
-    if (t < kDiProducers && lane == 0) {
+    if (lane == 0) {
         if (prov[0]) atomicOr(&sc->proven[0], prov[0]);
         if (!SAME && prov[1]) atomicOr(&sc->proven[1], prov[1]);
     }
     tc::fence_before_sync();
     __syncthreads();
-    if (warp == kDiQuads * 4) {
+    if (warp == 0) {
         tc::fence_after_sync();
-        tc::tmem_dealloc(tmem_base, 128);
+        tc::tmem_dealloc(tmem_base, 512);
     }
     for (int i = t; i < RP * RP; i += kDiThreads)
         if (red[i])
@@ -362,51 +398,63 @@ __global__ void __launch_bounds__(kDiThreads, 1)
 
 // Digits per level for rho (0: the tensor-core pass does not apply).
 int dot_i8_digits(int rho) {
-    const int d = 54 - rho;
-    return d <= 15 ? 2 : (d <= 23 ? 3 : 0);
+    const int d = 54 - rho, G = chain_group(rho, 4);
+    if (d <= 15) return (G == 3 || G == 4) ? 2 : 0;
+    if (d <= 23) return (G == 2 || G == 3) ? 3 : 0;
+    return 0;
 }
 
-template <bool SAME, int D>
+template <bool SAME, int D, int G>
 static int launch_i8(int grid, cudaStream_t s, int n, const double *x, const double *y, int sum_mode,
                      DotScratch *sc, const int *gate) {
     constexpr int RP = D == 2 ? 16 : 32;
     static bool attr = false;  // once per instantiation
     if (!attr) {
-        if (cudaFuncSetAttribute(k_dot_i8<SAME, D, RP>, cudaFuncAttributeMaxDynamicSharedMemorySize, kDiSmem) !=
+        if (cudaFuncSetAttribute(k_dot_i8<SAME, D, RP, G>, cudaFuncAttributeMaxDynamicSharedMemorySize, kDiSmem) !=
             cudaSuccess)
             return CUOZBLAS_STATUS_CUDA_ERROR;
         attr = true;
     }
-    k_dot_i8<SAME, D, RP><<<grid, kDiThreads, kDiSmem, s>>>(n, x, y, sum_mode, sc, gate);
+    k_dot_i8<SAME, D, RP, G><<<grid, kDiThreads, kDiSmem, s>>>(n, x, y, sum_mode, sc, gate);
     return cudaGetLastError() == cudaSuccess ? CUOZBLAS_STATUS_SUCCESS : CUOZBLAS_STATUS_CUDA_ERROR;
 }
 
-int dot_i8_prepare() {
+template <bool SAME>
+static int prepare_i8() {
     int r = 0;
-    r |= cudaFuncSetAttribute(k_dot_i8<true, 2, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize, kDiSmem);
-    r |= cudaFuncSetAttribute(k_dot_i8<false, 2, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize, kDiSmem);
-    r |= cudaFuncSetAttribute(k_dot_i8<true, 3, 32>, cudaFuncAttributeMaxDynamicSharedMemorySize, kDiSmem);
-    r |= cudaFuncSetAttribute(k_dot_i8<false, 3, 32>, cudaFuncAttributeMaxDynamicSharedMemorySize, kDiSmem);
-    return r ? CUOZBLAS_STATUS_CUDA_ERROR : CUOZBLAS_STATUS_SUCCESS;
+    r |= cudaFuncSetAttribute(k_dot_i8<SAME, 2, 16, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize, kDiSmem);
+    r |= cudaFuncSetAttribute(k_dot_i8<SAME, 2, 16, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, kDiSmem);
+    r |= cudaFuncSetAttribute(k_dot_i8<SAME, 3, 32, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, kDiSmem);
+    r |= cudaFuncSetAttribute(k_dot_i8<SAME, 3, 32, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize, kDiSmem);
+    return r;
+}
+
+int dot_i8_prepare() {
+    return (prepare_i8<true>() | prepare_i8<false>()) ? CUOZBLAS_STATUS_CUDA_ERROR : CUOZBLAS_STATUS_SUCCESS;
+}
+
+template <bool SAME>
+static int launch_i8_g(int D, int G, int grid, cudaStream_t s, int n, const double *x, const double *y,
+                       int sum_mode, DotScratch *sc, const int *gate) {
+    if (D == 2 && G == 3) return launch_i8<SAME, 2, 3>(grid, s, n, x, y, sum_mode, sc, gate);
+    if (D == 2 && G == 4) return launch_i8<SAME, 2, 4>(grid, s, n, x, y, sum_mode, sc, gate);
+    if (D == 3 && G == 2) return launch_i8<SAME, 3, 2>(grid, s, n, x, y, sum_mode, sc, gate);
+    if (D == 3 && G == 3) return launch_i8<SAME, 3, 3>(grid, s, n, x, y, sum_mode, sc, gate);
+    return CUOZBLAS_STATUS_INVALID_VALUE;
 }
 
 int dot_i8_launch(cudaStream_t s, int nsm, int n, const double *x, const double *y, int rho, int sum_mode,
                   DotScratch *sc, const int *gate) {
     const int D = dot_i8_digits(rho);
+    const int G = chain_group(rho, 4);  // levels cut from one base value, as the tree pass
     const int job = D == 2 ? 1024 : 512;
     const int64_t njobs = ((int64_t)n + job - 1) / job;
     int64_t grid = njobs < nsm ? njobs : nsm;
     const int64_t need = (njobs + kDiMaxJobs - 1) / kDiMaxJobs;
     if (grid < need) grid = need;
     if (grid < 1) grid = 1;
-    const bool same = x == y;
-    if (D == 2)
-        return same ? launch_i8<true, 2>((int)grid, s, n, x, y, sum_mode, sc, gate)
-                    : launch_i8<false, 2>((int)grid, s, n, x, y, sum_mode, sc, gate);
-    if (D == 3)
-        return same ? launch_i8<true, 3>((int)grid, s, n, x, y, sum_mode, sc, gate)
-                    : launch_i8<false, 3>((int)grid, s, n, x, y, sum_mode, sc, gate);
-    return CUOZBLAS_STATUS_INVALID_VALUE;
+    return x == y ? launch_i8_g<true>(D, G, (int)grid, s, n, x, y, sum_mode, sc, gate)
+                  : launch_i8_g<false>(D, G, (int)grid, s, n, x, y, sum_mode, sc, gate);
 }
 
 }  // namespace ozb
