@@ -351,9 +351,10 @@ int dot_tree_launch(cudaStream_t s, int nsm, int n, const double *x, const doubl
     const int G = chain_group(rho, 4);  // levels cut from one base value
     const bool same = (x == y);
     const bool aligned = ((reinterpret_cast<uintptr_t>(x) | reinterpret_cast<uintptr_t>(y)) & 15u) == 0;
-    // 16-byte aligned vectors with 2 or 3 digits per level take the tensor-core
-    // pass (it holds every valid plan); the FP64 tree pass takes the rest
-    if (aligned && n > 0 && dot_i8_digits(rho) > 0 && !getenv("OZBLAS_DOT_TREE"))
+    // 16-byte aligned vectors of at least 2^22 elements with 2 or 3 digits per
+    // level take the tensor-core pass (it holds every valid plan; below that
+    // length its fixed costs outweigh the FP64 tree pass, which takes the rest)
+    if (aligned && n >= (1 << 22) && dot_i8_digits(rho) > 0 && !getenv("OZBLAS_DOT_TREE"))
         return dot_i8_launch(s, nsm, n, x, y, rho, sum_mode, sc, gate);
     int fblocks = (int)(((int64_t)n + 2 * kDotThreads - 1) / (2 * kDotThreads));
     if (fblocks > nsm) fblocks = nsm;  // ~250 registers per thread: one 256-thread block per SM

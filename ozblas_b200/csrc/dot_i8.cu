@@ -30,11 +30,17 @@
 //  * the proof of the predicted chain is the tree pass's, on integers:
 //    level s holds if some |a_{s+1}| exceeds floor((thr_s + g_{s+1}) / g_{s+1}).
 //
-// CTA: 3 producer groups of 4 warps, two 32 KiB stages per group, and one MMA
-// warp that takes the stages in whatever order they fill (the sums commute);
-// each producer loads its next job's elements before cutting the current one.
-// The first producer group also reads the accumulator at the end.  Every wait
-// is bounded; a timeout sets DotScratch::err and the result is not used.
+// CTA (one per SM): 3 producer groups of 4 warps, two 32 KiB stages per group.
+// Each group cuts its jobs into its stages in turn, loading the next job's
+// elements before cutting the current one; one thread of the group waits for
+// its four warps (a per-stage mbarrier) and issues the group's MMAs into the
+// group's own 128-column TMEM accumulator, so no other thread touches it.
+// Proven levels are shared through DotScratch::proven at once, so warps stop
+// voting on them.  The first group sums the three accumulators at the end.
+// Every wait is bounded and every warp collective is reached by all lanes
+// (exits are agreed by a warp vote); a timeout sets DotScratch::err and the
+// result is not used.  The pass pays off from about 2^22 elements; shorter
+// vectors take the FP64 tree pass.
 #include "fused.h"
 #include "ozb_internal.h"
 #include "sum.cuh"
@@ -141,22 +147,6 @@ __device__ __forceinline__ void di_digits(const double (&v)[E], const double *sk
     }
 }
 
-// Barrier of one producer group (named barrier `id`, 128 threads), and the
-// same barrier returning whether any thread of the group passed `pred`.
-__device__ __forceinline__ void di_group_sync(int id) { asm volatile("bar.sync %0, 128;" ::"r"(id) : "memory"); }
-__device__ __forceinline__ bool di_group_any(int id, bool pred) {
-    uint32_t r;
-    asm volatile(
-        "{\n\t.reg .pred p, q;\n\t"
-        "setp.ne.u32 p, %1, 0;\n\t"
-        "bar.red.or.pred q, %2, 128, p;\n\t"
-        "selp.u32 %0, 1, 0, q;\n\t}\n"
-        : "=r"(r)
-        : "r"((uint32_t)pred), "r"(id)
-        : "memory");
-    return r != 0;
-}
-
 template <int E>
 __device__ __forceinline__ void di_load(const double *__restrict__ v, int64_t i0, int n, double (&o)[E]) {
     if (i0 + E <= n) {
@@ -227,7 +217,7 @@ __global__ void __launch_bounds__(kDiThreads, 1)
     extern __shared__ uint8_t di_raw[];
     uint8_t *smem = (uint8_t *)(((uintptr_t)di_raw + 1023) & ~(uintptr_t)1023);
     __shared__ TreePlan pl;
-    __shared__ __align__(8) uint64_t empty[kDiStages], done;
+    __shared__ __align__(8) uint64_t full[kDiStages], empty[kDiStages], done;
     __shared__ uint32_t tmem_slot;
     __shared__ volatile int abort_flag;
     __shared__ unsigned long long red[RP * RP];
@@ -250,7 +240,10 @@ __global__ void __launch_bounds__(kDiThreads, 1)
     const int myjobs = work && blockIdx.x < njobs ? (int)((njobs - 1 - blockIdx.x) / gridDim.x + 1) : 0;
 
     if (t == 0) {
-        for (int q = 0; q < kDiStages; q++) tc::mbar_init(&empty[q], 1);
+        for (int q = 0; q < kDiStages; q++) {
+            tc::mbar_init(&full[q], 4);  // one arrival per warp of the group
+            tc::mbar_init(&empty[q], 1);
+        }
         tc::mbar_init(&done, kDiQuads);
         abort_flag = 0;
         tc::fence_mbar_init();
@@ -279,25 +272,34 @@ __global__ void __launch_bounds__(kDiThreads, 1)
         // have written the stage (group barrier 1 + quad)
         auto produce = [&](int k, const double (&xv)[E], const double (&yv)[E]) -> bool {
             const int st = quad * kDiStagesPerQuad + (k & 1);
+            // every lane leaves on the same job (the warp collectives below need all lanes)
             const bool ok = tc::mbar_wait(&empty[st], ((k >> 1) & 1) ^ 1, &abort_flag, &sc->err, 1, kDiWaitNs);
-            if (di_group_any(1 + quad, !ok)) return false;  // the whole group leaves together
+            if (!__all_sync(0xffffffffu, ok)) return false;
             uint8_t *tileA = smem + st * kDiStage;
             const uint32_t ra = tc::smem_u32(tileA) + rowoff + ub16;
-            const unsigned px = pl.need[0] & ~prov[0];
-            if (px)
-                di_digits<D, E, G, true>(xv, sk[0], d, pl.ith[0], ra, px, prov[0]);
-            else
-                di_digits<D, E, G, false>(xv, sk[0], d, pl.ith[0], ra, 0u, prov[0]);
-            if (!SAME) {
-                const unsigned py = pl.need[1] & ~prov[1];
-                if (py)
-                    di_digits<D, E, G, true>(yv, sk[1], d, pl.ith[1], ra + kDiTile, py, prov[1]);
+#pragma unroll
+            for (int v = 0; v < (SAME ? 1 : 2); v++) {
+                // prov is uniform across the warp (the vote variant's __any_sync
+                // needs every lane on the same path): lane 0's read of the levels
+                // other warps proved is broadcast to all lanes
+                unsigned pend = pl.need[v] & ~prov[v];
+                if (pend) {  // uniform: levels some other warp proved need no vote here
+                    prov[v] |= __shfl_sync(0xffffffffu, __ldcg(&sc->proven[v]), 0);
+                    pend = pl.need[v] & ~prov[v];
+                }
+                const unsigned before = prov[v];
+                if (pend)
+                    di_digits<D, E, G, true>(v ? yv : xv, sk[v], d, pl.ith[v], ra + v * kDiTile, pend, prov[v]);
                 else
-                    di_digits<D, E, G, false>(yv, sk[1], d, pl.ith[1], ra + kDiTile, 0u, prov[1]);
+                    di_digits<D, E, G, false>(v ? yv : xv, sk[v], d, pl.ith[v], ra + v * kDiTile, 0u, prov[v]);
+                if (lane == 0 && prov[v] != before) atomicOr(&sc->proven[v], prov[v]);  // share at once
             }
             tc::fence_proxy_async();
-            di_group_sync(1 + quad);
-            if (tq == 0) {
+            __syncwarp();
+            if (lane == 0) tc::mbar_arrive(&full[st]);
+            // the group's issuer, once all four warps have written the stage; on a
+            // timeout it issues nothing (the abort flag then stops every wait)
+            if (tq == 0 && tc::mbar_wait(&full[st], (k >> 1) & 1, &abort_flag, &sc->err, 2, kDiWaitNs)) {
                 tc::fence_after_sync();
                 const uint32_t sa = tc::smem_u32(tileA), sb = SAME ? sa : sa + kDiTile;
                 const uint64_t adesc = tc::smem_desc_k_sw128(sa), bdesc = tc::smem_desc_k_sw128(sb);
@@ -339,8 +341,11 @@ __global__ void __launch_bounds__(kDiThreads, 1)
     }
 
     // ---------------------------------------------------------------- accumulator
+    __syncwarp();
     if (warp < 4 && myjobs > 0) {
-        if (tc::mbar_wait(&done, 0, &abort_flag, &sc->err, 3, kDiWaitNs) && !abort_flag) {
+        // tcgen05.ld is warp-collective: every lane takes the same branch
+        const bool ok = tc::mbar_wait(&done, 0, &abort_flag, &sc->err, 3, kDiWaitNs) && !abort_flag;
+        if (__all_sync(0xffffffffu, ok)) {
             tc::fence_after_sync();
             long long sum[32];
 #pragma unroll

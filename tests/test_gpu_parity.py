@@ -255,9 +255,9 @@ def test_ddot_tensor_core_pass(n, phi, sm, oracle, handle, ozb, cuda):
 
 
 def test_ddot_tensor_core_pass_matches_tree(oracle, handle, ozb, cuda, monkeypatch):
-    """The INT8 tensor-core pass and the FP64 tree pass give the same bits (2 and 3 digits per level)."""
-    for n, phi in ((3000, 0.5), (100003, 1.0), (1 << 20, 0.25), (1 << 20, 2.0), ((1 << 22) + 5, 1.0),
-                   ((1 << 23) + 3, 0.5)):
+    """The INT8 tensor-core pass (vectors of 2^22 elements and more) and the FP64 tree pass give the same
+    bits, with 3 and 2 digits per level."""
+    for n, phi in (((1 << 22) + 5, 1.0), ((1 << 23) + 3, 0.5), ((1 << 23) + 77, 2.0), ((1 << 24) + 9, 1.0)):
         x = dev(cuda, oracle.phi_vector(n, phi, 3))
         y = dev(cuda, oracle.phi_vector(n, phi, 4))
         for sm in (0, 1):
