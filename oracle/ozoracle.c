@@ -253,6 +253,82 @@ static int make_pairs(int nA, int nB, int maxlevel, int *pa, int *pb) {
     return np;
 }
 
+/* ------------------------------------------------------------------------ */
+/* Dot2 (splitEpsMode 2): error-free transformations of src/cpu/eft.h       */
+/* ------------------------------------------------------------------------ */
+
+typedef struct {
+    double x, y;
+} dd_t;
+
+static void eft_two_sum(double a, double b, double *s, double *e) { /* eft.h:11-19 */
+    const double ss = a + b;
+    const double v = ss - a;
+    *e = (a - (ss - v)) + (b - v);
+    *s = ss;
+}
+static void eft_quick_two_sum(double a, double b, double *s, double *e) { /* eft.h:51-57 */
+    const double ss = a + b;
+    *e = b - (ss - a);
+    *s = ss;
+}
+static void eft_dot2i(double a, double b, dd_t *c) { /* eft.h:99-107 with TwoProdFMA :75-81 */
+    const double h = a * b;
+    const double r = fma(a, b, -h);
+    double q;
+    eft_two_sum(c->x, h, &c->x, &q);
+    c->y = c->y + (q + r);
+}
+static dd_t eft_quad_add(dd_t a, dd_t b) { /* eft.h:129-137 */
+    dd_t t, c;
+    eft_two_sum(a.x, b.x, &t.x, &t.y);
+    t.y = t.y + (a.y + b.y);
+    eft_quick_two_sum(t.x, t.y, &c.x, &c.y);
+    return c;
+}
+static dd_t eft_quad_mul(double a, dd_t b) { /* eft.h:166-174 */
+    dd_t t, c;
+    t.x = a * b.x;
+    t.y = fma(a, b.x, -t.x);
+    t.y = fma(a, b.y, t.y);
+    eft_quick_two_sum(t.x, t.y, &c.x, &c.y);
+    return c;
+}
+
+/* Dot2 DOT: dgemm_tn_skinny_x2 (src/cpu/ozblas_blas_wrapper.cpp:109-152) run by one OpenMP
+ * thread (its result depends on the thread count: each thread's Dot2i partial is QuadAdd-ed
+ * in critical-section order), then the sum of src/cpu/ozblas_gemm.cpp:281-287 over the hi
+ * terms of every pair followed by the lo terms as B indices nB..2nB-1. */
+static double dot2_dot(const oz_flags *f, int k, const double *Sa, int nA, const double *Sb, int nB) {
+    double *hi = (double *)malloc(sizeof(double) * nA * nB * 2);
+    for (int ib = 0; ib < nB; ib++)
+        for (int ia = 0; ia < nA; ia++) {
+            dd_t L = {0., 0.}, G = {0., 0.};
+            const double *a = Sa + (size_t)ia * k, *b = Sb + (size_t)ib * k;
+            for (int l = 0; l < k; l++) eft_dot2i(a[l], b[l], &L);
+            G = eft_quad_add(G, L);
+            G = eft_quad_mul(1., G); /* beta == 0: Gr = QuadMul(alpha, Gr) */
+            hi[(size_t)ia * 2 * nB + ib] = G.x;
+            hi[(size_t)ia * 2 * nB + nB + ib] = G.y;
+        }
+    const int nB2 = 2 * nB, maxlevel = (nA - 1) + (nB2 - 1);
+    double *terms = (double *)malloc(sizeof(double) * nA * nB2);
+    int np = 0;
+    for (int ik = 0; ik <= maxlevel; ik++)
+        for (int ia = 0; ia < nA; ia++) {
+            const int ib = ik - ia;
+            if (ib >= 0 && ib < nB2) terms[np++] = hi[(size_t)ia * nB2 + ib];
+        }
+    double t = 0.;
+    if (f->sumMode == 1)
+        t = oz_nearsum(np, terms);
+    else
+        for (int p = 0; p < np; p++) t += terms[p];
+    free(hi);
+    free(terms);
+    return t;
+}
+
 int oz_dgemm(const oz_flags *f, char ta, char tb, int m, int n, int k, double alpha, const double *A, int lda,
              const double *B, int ldb, double beta, double *C, int ldc, oz_info *info) {
     if (f->reproMode != 1) return -1;
@@ -272,6 +348,27 @@ int oz_dgemm(const oz_flags *f, char ta, char tb, int m, int n, int k, double al
     double *Sb = (double *)calloc((size_t)(maxS + 1) * kk * imax(n, 1), sizeof(double));
     const int nA = oz_split_cols(f, k, m, Ap, k, 1, Sa, k);
     const int nB = oz_split_cols(f, k, n, Bp, k, 1, Sb, k);
+    if (is_dot && f->splitEpsMode == 2 && f->fastMode == 0 && f->sumMode < 2) { /* ozblas_gemm.cpp:166-172 */
+        const double t = dot2_dot(f, k, Sa, nA, Sb, nB);
+        C[0] = fma(alpha, t, (beta * C[0]));
+        if (info) {
+            info->nSplitA = (float)nA;
+            info->nSplitB = (float)nB;
+            info->nSplitC = 1.f;
+        }
+        free(Ap);
+        free(Bp);
+        free(Sa);
+        free(Sb);
+        return 0;
+    }
+    if (f->splitEpsMode == 2) { /* Dot2 products exist only for DOT and CSRMV */
+        free(Ap);
+        free(Bp);
+        free(Sa);
+        free(Sb);
+        return -1;
+    }
     int maxlevel = (nA - 1) + (nB - 1);
     maxlevel = imax(maxlevel - fast, imin(nA - 1, nB - 1)); /* src/cpu/ozblas_gemm.cpp:163-164 */
     int *pa = (int *)malloc(sizeof(int) * nA * nB), *pb = (int *)malloc(sizeof(int) * nA * nB);
@@ -348,8 +445,45 @@ int oz_dcsrmv_presplit(const oz_flags *f, int m, int n, int nnz, double alpha, c
     maxlevel = imax(maxlevel - f->fastMode, imin(nA - 1, nB - 1));
     int *pa = (int *)malloc(sizeof(int) * nA * nB), *pb = (int *)malloc(sizeof(int) * nA * nB);
     const int np = make_pairs(nA, nB, maxlevel, pa, pb);
-    double *terms = (double *)malloc(sizeof(double) * (np > 0 ? np : 1));
+    const int dot2 = f->splitEpsMode == 2;
+    if (dot2 && f->fastMode != 0) { /* the reference's storage and sum disagree there */
+        free(Sx);
+        free(pa);
+        free(pb);
+        return -1;
+    }
+    const int nB2 = 2 * nB;
+    double *pv = (double *)malloc(sizeof(double) * (nA * nB2 > 0 ? nA * nB2 : 1));
+    double *terms = (double *)malloc(sizeof(double) * (nA * nB2 > np ? nA * nB2 : (np > 0 ? np : 1)));
     for (int r = 0; r < m; r++) {
+        if (dot2) {
+            /* csrmm_n_x2 (src/cpu/ozblas_blas_wrapper.cpp:262-295): Dot2i along the row, then
+             * QuadMul(alpha = 1); hi of pair (ia, ib) at B index ib, lo at nB + ib; summed with
+             * maxlevel (nA - 1) + (2 nB - 1) (src/cpu/ozblas_csrmv.cpp:120-162) */
+            for (int ia = 0; ia < nA; ia++)
+                for (int ib = 0; ib < nB; ib++) {
+                    const double *a = aslices + (size_t)ia * lds;
+                    const double *xs = Sx + (size_t)ib * n;
+                    dd_t T = {0., 0.};
+                    for (int i = rowptr[r]; i < rowptr[r + 1]; i++) eft_dot2i(a[i], xs[colind[i]], &T);
+                    T = eft_quad_mul(1., T);
+                    pv[ia * nB2 + ib] = T.x;
+                    pv[ia * nB2 + nB + ib] = T.y;
+                }
+            int q = 0;
+            for (int ik = 0; ik <= (nA - 1) + (nB2 - 1); ik++)
+                for (int ia = 0; ia < nA; ia++) {
+                    const int ib = ik - ia;
+                    if (ib >= 0 && ib < nB2) terms[q++] = pv[ia * nB2 + ib];
+                }
+            double t = 0.;
+            if (f->sumMode == 1)
+                t = oz_nearsum(q, terms);
+            else
+                for (int p = 0; p < q; p++) t += terms[p];
+            y[r] = fma(alpha, t, (beta * y[r]));
+            continue;
+        }
         for (int p = 0; p < np; p++) {
             const double *a = aslices + (size_t)pa[p] * lds;
             const double *xs = Sx + (size_t)pb[p] * n;
@@ -374,6 +508,7 @@ int oz_dcsrmv_presplit(const oz_flags *f, int m, int n, int nnz, double alpha, c
     free(Sx);
     free(pa);
     free(pb);
+    free(pv);
     free(terms);
     (void)nnz;
     return 0;

@@ -61,8 +61,12 @@ int counter_init(cuozblasHandle_t *h) {
     return CUOZBLAS_STATUS_SUCCESS;
 }
 
-static int check_flags(cuozblasHandle_t *h) {
-    if (h->splitEpsMode != 0 && h->splitEpsMode != 9) return CUOZBLAS_STATUS_NOT_SUPPORTED;
+// splitEpsMode 2 (Dot2) exists for DOT, NRM2, CSRMV and CG only, with
+// fastMode 0 (the reference's DOT takes its Dot2 branch only then, and its
+// CSRMV stores and sums Dot2 pairs inconsistently otherwise).
+static int check_flags(cuozblasHandle_t *h, bool dot2 = false) {
+    if (h->splitEpsMode == 2 && !(dot2 && h->fastMode == 0)) return CUOZBLAS_STATUS_NOT_SUPPORTED;
+    if (h->splitEpsMode != 0 && h->splitEpsMode != 9 && h->splitEpsMode != 2) return CUOZBLAS_STATUS_NOT_SUPPORTED;
     if (h->sumMode != 0 && h->sumMode != 1) return CUOZBLAS_STATUS_NOT_SUPPORTED;
     if (h->nSplitMax < 0 || h->nSplitMax > kMaxSplitDefault) return CUOZBLAS_STATUS_INVALID_VALUE;
     return CUOZBLAS_STATUS_SUCCESS;
@@ -205,7 +209,7 @@ int cuozblasDgemm(cuozblasHandle_t *h, char transa, char transb, int32_t m, int3
 int cuozblasDdot(cuozblasHandle_t *h, int32_t n, const double *x, int32_t incx, const double *y, int32_t incy,
                  double *ret) {
     OZB_TRY(counter_init(h));
-    OZB_TRY(check_flags(h));
+    OZB_TRY(check_flags(h, true));
     if (incx != 1 || incy != 1 || n < 0 || ret == nullptr) return CUOZBLAS_STATUS_INVALID_VALUE;
     const double t0 = wall();
     OZB_TRY(dot_impl(h, n, x, y, ret));
@@ -215,7 +219,7 @@ int cuozblasDdot(cuozblasHandle_t *h, int32_t n, const double *x, int32_t incx, 
 
 int cuozblasDnrm2(cuozblasHandle_t *h, int32_t n, const double *x, int32_t incx, double *ret) {
     OZB_TRY(counter_init(h));
-    OZB_TRY(check_flags(h));
+    OZB_TRY(check_flags(h, true));
     if (incx != 1 || n < 0 || ret == nullptr) return CUOZBLAS_STATUS_INVALID_VALUE;
     const double t0 = wall();
     double d = 0.0;
@@ -255,7 +259,7 @@ int cuozblasDcsrmv(cuozblasHandle_t *h, char trans, int32_t m, int32_t n, int32_
                    const double *x, double beta, double *y) {
     (void)descrA;
     OZB_TRY(counter_init(h));
-    OZB_TRY(check_flags(h));
+    OZB_TRY(check_flags(h, true));
     if (is_trans(trans) || m < 0 || n < 0 || nnz < 0) return CUOZBLAS_STATUS_INVALID_VALUE;
     const double t0 = wall();
     const int maxS = h->nSplitMax > 0 ? h->nSplitMax : kMaxSplitDefault;
@@ -301,7 +305,7 @@ int cuozblasDcsrmvSplitA(cuozblasHandle_t *h, char trans, int32_t m, int32_t n, 
     (void)descrA;
     (void)n;
     OZB_TRY(counter_init(h));
-    OZB_TRY(check_flags(h));
+    OZB_TRY(check_flags(h, true));
     if (is_trans(trans) || m < 0 || nnz < 0 || splitA == nullptr) return CUOZBLAS_STATUS_INVALID_VALUE;
     const int maxS = h->nSplitMax > 0 ? h->nSplitMax : kMaxSplitDefault;
     const double t0 = wall();

@@ -7,6 +7,7 @@
 // runs the same chain for every slice pair, so the products carry the CPU's
 // bits whether or not they are exact (with splitShift > 1 they need not be).
 #include "ozb_internal.h"
+#include "eft.cuh"
 #include "sum.cuh"
 
 namespace ozb {
@@ -35,6 +36,45 @@ __global__ void __launch_bounds__(256) k_csrmv_pairs(int m, const double *__rest
         p++;
     });
     if (sum_mode == 1) t = nearsum(p, pbuf + row, m);
+    y[row] = fma(alpha, t, beta * y[row]);
+}
+
+// Dot2 CSRMV (splitEpsMode 2, fastMode 0): csrmm_n_x2 of the reference
+// (src/cpu/ozblas_blas_wrapper.cpp:262-295) per row and pair, Dot2i along the
+// row in storage order then QuadMul(1); pair (ia, ib)'s hi term at B index ib
+// and lo term at nB + ib, summed over levels (nA - 1) + (2 nB - 1)
+// (src/cpu/ozblas_csrmv.cpp:120-162).  tbuf: 4 nA nB terms per row, stride m.
+__global__ void __launch_bounds__(256) k_csrmv_pairs_dot2(int m, const double *__restrict__ As, int64_t lda_s,
+                                                          const int *__restrict__ colind,
+                                                          const int *__restrict__ rowptr, const double *__restrict__ xs,
+                                                          int64_t ldx, int nA, int nB, int sum_mode, double alpha,
+                                                          double beta, double *__restrict__ y,
+                                                          double *__restrict__ tbuf) {
+    const int row = blockIdx.x * blockDim.x + threadIdx.x;
+    if (row >= m) return;
+    const int lo = rowptr[row], hi = rowptr[row + 1], nB2 = 2 * nB;
+    double *pv = tbuf + row, *terms = tbuf + (size_t)nA * nB2 * m + row;
+    for (int ia = 0; ia < nA; ia++)
+        for (int ib = 0; ib < nB; ib++) {
+            const double *a = As + (size_t)ia * lda_s;
+            const double *x = xs + (size_t)ib * ldx;
+            DD t{0.0, 0.0};
+            for (int i = lo; i < hi; i++) eft_dot2i(a[i], x[colind[i]], t);
+            t = eft_quad_mul(1.0, t);
+            pv[(size_t)(ia * nB2 + ib) * m] = t.x;
+            pv[(size_t)(ia * nB2 + nB + ib) * m] = t.y;
+        }
+    int q = 0;
+    for (int ik = 0; ik <= (nA - 1) + (nB2 - 1); ik++)
+        for (int ia = 0; ia < nA; ia++) {
+            const int ib = ik - ia;
+            if (ib >= 0 && ib < nB2) terms[(size_t)(q++) * m] = pv[(size_t)(ia * nB2 + ib) * m];
+        }
+    double t = 0.0;
+    if (sum_mode == 1)
+        t = nearsum(q, terms, m);
+    else
+        for (int p = 0; p < q; p++) t += terms[(size_t)p * m];
     y[row] = fma(alpha, t, beta * y[row]);
 }
 
@@ -107,6 +147,20 @@ int csrmv_presplit(cuozblasHandle_t *h, int m, int n, double alpha, const double
     maxlevel = (maxlevel - h->fastMode) > mn ? (maxlevel - h->fastMode) : mn;
     int np = 0;
     for_each_pair(nA, nB, maxlevel, [&](int, int) { np++; });
+    if (h->splitEpsMode == 2) {  // Dot2 (the caller admits fastMode 0 only)
+        double *tbuf = ar.take<double>((uint64_t)4 * nA * nB * (m > 0 ? m : 1));
+        if (!ar.ok) return CUOZBLAS_STATUS_WORKSPACE;
+        if (m > 0) {
+            counted(h);
+            k_csrmv_pairs_dot2<<<(m + 255) / 256, 256, 0, st->stream>>>(m, As, ld_s, colind, rowptr, xs, ldx, nA, nB,
+                                                                       h->sumMode, alpha, beta, y, tbuf);
+        }
+        OZB_CHECK(cudaGetLastError());
+        h->nSplitA = (float)nA;
+        h->nSplitB = (float)nB;
+        h->nSplitC = (float)(nA * nB);
+        return CUOZBLAS_STATUS_SUCCESS;
+    }
     double *pbuf = nullptr;
     if (h->sumMode == 1) {
         pbuf = ar.take<double>((uint64_t)np * (m > 0 ? m : 1));

@@ -9,6 +9,7 @@
 // fixes the bits is (1) the split and (2) the order of the pair sum, which
 // the fused epilogue follows exactly.
 #include "ozb_internal.h"
+#include "eft.cuh"
 #include "sum.cuh"
 
 namespace ozb {
@@ -201,6 +202,62 @@ __global__ void __launch_bounds__(256) k_pair_dot(int n, int nA, int nB, const d
     }
 }
 
+// Dot2 DOT (splitEpsMode 2): the reference forms each pair with Dot2i over
+// all k and combines per-thread partials with QuadAdd in OpenMP
+// critical-section order (src/cpu/ozblas_blas_wrapper.cpp:109-152), so its bits
+// depend on its thread count.  Here the order is fixed: every thread runs
+// Dot2i over a strided share, a block combines its threads with QuadAdd in a
+// fixed tree, and one thread per pair combines the blocks in block order;
+// then QuadAdd onto (0, 0) and QuadMul(1), as the reference finishes.
+// Grid (blocks, nA * nB); partials[pair * gridDim.x + block].
+__global__ void __launch_bounds__(256) k_pair_dot2(int k, int nB, const double *__restrict__ xs, int ldx,
+                                                   const double *__restrict__ ys, int ldy, DD *__restrict__ partials) {
+    __shared__ DD red[256];
+    const int pair = blockIdx.y, ia = pair / nB, ib = pair % nB;
+    const double *x = xs + (size_t)ia * ldx, *y = ys + (size_t)ib * ldy;
+    DD c{0.0, 0.0};
+    for (int64_t i = (int64_t)blockIdx.x * 256 + threadIdx.x; i < k; i += (int64_t)gridDim.x * 256)
+        eft_dot2i(x[i], y[i], c);
+    red[threadIdx.x] = c;
+    __syncthreads();
+    for (int s = 128; s > 0; s >>= 1) {
+        if (threadIdx.x < s) red[threadIdx.x] = eft_quad_add(red[threadIdx.x], red[threadIdx.x + s]);
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) partials[(size_t)pair * gridDim.x + blockIdx.x] = red[0];
+}
+
+// The pairs' hi terms at B index ib and lo terms at nB + ib, summed over
+// levels (nA - 1) + (2 nB - 1) (src/cpu/ozblas_gemm.cpp:281-287); one block.
+__global__ void k_dot2_finish(int nA, int nB, int blocks, const DD *__restrict__ partials, int sum_mode,
+                              double alpha, double beta, double *__restrict__ out, double *__restrict__ tmp) {
+    const int nB2 = 2 * nB, np = nA * nB;
+    for (int pair = threadIdx.x; pair < np; pair += blockDim.x) {
+        DD g{0.0, 0.0};
+        for (int b = 0; b < blocks; b++) g = eft_quad_add(g, partials[(size_t)pair * blocks + b]);
+        g = eft_quad_add(DD{0.0, 0.0}, g);
+        g = eft_quad_mul(1.0, g);
+        const int ia = pair / nB, ib = pair % nB;
+        tmp[ia * nB2 + ib] = g.x;
+        tmp[ia * nB2 + nB + ib] = g.y;
+    }
+    __syncthreads();
+    if (threadIdx.x != 0) return;
+    double *terms = tmp + nA * nB2;
+    int q = 0;
+    for (int ik = 0; ik <= (nA - 1) + (nB2 - 1); ik++)
+        for (int ia = 0; ia < nA; ia++) {
+            const int ib = ik - ia;
+            if (ib >= 0 && ib < nB2) terms[q++] = tmp[ia * nB2 + ib];
+        }
+    double t = 0.0;
+    if (sum_mode == 1)
+        t = nearsum(q, terms, 1);
+    else
+        for (int p = 0; p < q; p++) t += terms[p];
+    *out = fma(alpha, t, beta * *out);
+}
+
 // One scalar result from a pair matrix P[ia * ldp + ib] (DOT): FSum or NearSum.
 __global__ void k_sum_pair_matrix(int nA, int nB, int maxlevel, const double *__restrict__ P, int ldp, int sum_mode,
                                   double alpha, double beta, double *__restrict__ out, double *__restrict__ tmp) {
@@ -348,6 +405,21 @@ int gemm_plain_core(cuozblasHandle_t *h, char ta, char tb, int m, int n, int k, 
     h->mbk = m;
     h->nbk = n;
 
+    if (dot && h->splitEpsMode == 2) {  // Dot2 DOT (the caller admits fastMode 0 only)
+        int blocks = (k + 255) / 256;
+        if (blocks > 148 * 4) blocks = 148 * 4;
+        if (blocks < 1) blocks = 1;
+        DD *partials = ar.take<DD>((uint64_t)nA * nB * blocks);
+        double *tmp = ar.take<double>((uint64_t)4 * nA * nB + 1);
+        if (!ar.ok) return CUOZBLAS_STATUS_WORKSPACE;
+        counted(h);
+        k_pair_dot2<<<dim3(blocks, nA * nB), 256, 0, st->stream>>>(k, nB, Sa, ldk, Sb, ldk, partials);
+        OZB_CHECK(cudaGetLastError());
+        counted(h);
+        k_dot2_finish<<<1, 64, 0, st->stream>>>(nA, nB, blocks, partials, h->sumMode, alpha, beta, C, tmp);
+        OZB_CHECK(cudaGetLastError());
+        return CUOZBLAS_STATUS_SUCCESS;
+    }
     if (dot || skinny_n) {
         // pair products into P[(ia*nB+ib)][row]
         const int rows = dot ? 1 : m;

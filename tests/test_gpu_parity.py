@@ -278,10 +278,78 @@ def test_invalid_arguments(handle, ozb, cuda):
     with pytest.raises(ozb.OzblasError) as e:
         ozb.dcsrmv(handle, "t", 1, 1, 0, 1.0, x, x, x, x, 0.0, x)
     assert e.value.code == 2
-    handle.splitEpsMode = 2
+    handle.splitEpsMode = 2  # Dot2 exists for DOT, NRM2, CSRMV and CG, with fastMode 0
+    with pytest.raises(ozb.OzblasError) as e:
+        ozb.dgemm(handle, "n", "n", 2, 2, 2, 1.0, x, 2, x, 2, 0.0, x, 2)
+    assert e.value.code == 4
+    handle.fastMode = 1
     with pytest.raises(ozb.OzblasError) as e:
         ozb.ddot(handle, 8, x, x)
     assert e.value.code == 4
+
+
+# ---- Dot2 (splitEpsMode 2) ----
+
+@pytest.mark.parametrize("grid", [(4, 3, 2), (12, 10, 9), (30, 20, 25)])
+@pytest.mark.parametrize("sm", [0, 1])
+def test_dcsrmv_dot2(grid, sm, oracle, handle, ozb, cuda):
+    """Dot2 CSRMV is sequential per row in the reference, so it is bit-exact here."""
+    rowptr, colind = oracle.stencil7(*grid)
+    n = len(rowptr) - 1
+    val = oracle.phi_vector(len(colind), 2.0, 1)
+    x = oracle.phi_vector(n, 2.0, 2)
+    y0 = oracle.phi_vector(n, 1.0, 3)
+    handle.sumMode, handle.splitEpsMode = sm, 2
+    for alpha, beta in ((1.0, 0.0), (-0.75, 1.5)):
+        ref, info = oracle.dcsrmv(make_flags(sumMode=sm, splitEpsMode=2), n, n, alpha, val, colind, rowptr, x, beta,
+                                  y0)
+        dy = dev(cuda, y0)
+        ozb.dcsrmv(handle, "n", n, n, len(val), alpha, dev(cuda, val), dev(cuda, colind), dev(cuda, rowptr),
+                   dev(cuda, x), beta, dy)
+        assert bits_equal(host(dy), ref), first_diff(host(dy), ref)
+        assert (handle.nSplitA, handle.nSplitB, handle.nSplitC) == (info.nSplitA, info.nSplitB, info.nSplitC)
+
+
+@pytest.mark.parametrize("n,phi", [(1, 1.0), (1000, 2.0), (100003, 1.0), (1 << 20, 2.0)])
+@pytest.mark.parametrize("sm", [0, 1])
+def test_ddot_dot2(n, phi, sm, oracle, handle, ozb, cuda):
+    """Dot2 DOT: the reference's double-double partials meet in OpenMP order, so only its one-thread
+    run is reproducible; this library uses a fixed parallel order instead.  Tolerance: the result
+    is within one unit in the last place of the one-thread reference (restatement), identical run
+    to run, and the split counts agree."""
+    x = oracle.phi_vector(n, phi, 1)
+    y = oracle.phi_vector(n, phi, 2)
+    handle.sumMode, handle.splitEpsMode = sm, 2
+    dx, dy = dev(cuda, x), dev(cuda, y)
+    d = ozb.ddot(handle, n, dx, dy)
+    assert ozb.ddot(handle, n, dx, dy) == d
+    r, info = oracle.ddot(make_flags(sumMode=sm, splitEpsMode=2), x, y)
+    assert abs(d - r) <= np.spacing(abs(r)), (d, r)
+    assert (handle.nSplitA, handle.nSplitB) == (info.nSplitA, info.nSplitB)
+    nr = ozb.dnrm2(handle, n, dx)
+    nr_ref, _ = oracle.dnrm2(make_flags(sumMode=sm, splitEpsMode=2), x)
+    assert abs(nr - nr_ref) <= np.spacing(nr_ref), (nr, nr_ref)
+
+
+def test_cg_dot2(oracle, handle, ozb, cuda):
+    """CG in Dot2 mode (host loop): CSRMV bit-exact, DOT within an ulp, so the residual history
+    follows the one-thread reference closely."""
+    nx = ny = nz = 10
+    rowptr, colind = oracle.stencil7(nx, ny, nz)
+    n = len(rowptr) - 1
+    val = oracle.poisson_shift(nx, ny, nz, 3, rowptr, colind)
+    b = oracle.csrmv_fma(val, colind, rowptr, oracle.normal(n, 4))
+    iters = 25
+    xr, hr, _ = oracle.dcg(make_flags(sumMode=1, splitEpsMode=2), val, colind, rowptr, b, np.zeros(n), iters, 0.0)
+    handle.sumMode, handle.splitEpsMode, handle.verbose = 1, 2, 1
+    dx = cuda.zeros(n, dtype=cuda.float64, device="cuda")
+    h1 = np.zeros(iters + 1)
+    h2 = np.zeros(iters + 1)
+    it = ozb.dcg(handle, "n", n, len(val), dev(cuda, val), dev(cuda, colind), dev(cuda, rowptr), dev(cuda, b), dx,
+                 iters, 0.0, h1, h2)
+    assert it == iters
+    assert np.allclose(h1, hr, rtol=1e-9, atol=0), np.max(np.abs(h1 - hr) / np.abs(hr))
+    assert np.allclose(host(dx), xr, rtol=1e-9, atol=1e-12)
 
 
 # ---- fused DOT / CSRMV: the paths that must hand over to the general algorithm ----

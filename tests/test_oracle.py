@@ -132,6 +132,46 @@ def test_restatement_vs_reference_random_shapes(seed, oracle, reference):
     assert [info.nSplitA, info.nSplitB, info.nSplitC] == [inf["nSplitA"], inf["nSplitB"], inf["nSplitC"]]
 
 
+@pytest.mark.parametrize("n,phi", [(1, 1.0), (37, 1.0), (1000, 2.0), (20000, 1.0), (65537, 4.0)])
+@pytest.mark.parametrize("sm", [0, 1])
+def test_dot2_dot_vs_reference_one_thread(n, phi, sm, oracle, reference):
+    """Dot2 (splitEpsMode 2) DOT: the restatement follows the reference run by one OpenMP thread
+    (its double-double partials are combined in critical-section order, so only one thread is
+    reproducible)."""
+    x = oracle.phi_vector(n, phi, 1)
+    y = oracle.phi_vector(n, phi, 2)
+    r, info = oracle.ddot(make_flags(sumMode=sm, splitEpsMode=2), x, y)
+    prev = reference.threads()
+    reference.threads(1)
+    try:
+        reference.set_flags(sumMode=sm, splitEpsMode=2)
+        gold = reference.ddot(x, y)
+    finally:
+        reference.threads(prev)
+    assert np.float64(r).view(np.int64) == np.float64(gold).view(np.int64), (n, phi, sm, r, gold)
+    inf = reference.info()
+    assert [info.nSplitA, info.nSplitB] == [inf["nSplitA"], inf["nSplitB"]]
+
+
+@pytest.mark.parametrize("sm", [0, 1])
+def test_dot2_csrmv_vs_reference(sm, oracle, reference):
+    """Dot2 CSRMV: Dot2i along each row (deterministic for any thread count), hi terms then lo
+    terms in the sum."""
+    rowptr, colind = oracle.stencil7(9, 8, 7)
+    n = len(rowptr) - 1
+    val = oracle.phi_vector(len(colind), 2.0, 1)
+    x = oracle.phi_vector(n, 2.0, 2)
+    y0 = oracle.phi_vector(n, 1.0, 3)
+    for alpha, beta in ((1.0, 0.0), (-0.75, 1.5)):
+        out, info = oracle.dcsrmv(make_flags(sumMode=sm, splitEpsMode=2), n, n, alpha, val, colind, rowptr, x,
+                                  beta, y0)
+        reference.set_flags(sumMode=sm, splitEpsMode=2)
+        gold = reference.dcsrmv(n, n, alpha, val, colind, rowptr, x, beta, y0)
+        assert bits_equal(out, gold), first_diff(out, gold)
+        inf = reference.info()
+        assert [info.nSplitA, info.nSplitB, info.nSplitC] == [inf["nSplitA"], inf["nSplitB"], inf["nSplitC"]]
+
+
 def test_split_slices_vs_reference(oracle, reference):
     """Slice-level parity of the column-panel and CSR splits."""
     for phi, k, ncol in [(1.0, 100, 7), (4.0, 333, 5), (2.0, 1, 3), (1.0, 64, 1)]:
