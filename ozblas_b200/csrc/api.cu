@@ -75,6 +75,14 @@ static int check_flags(cuozblasHandle_t *h, bool dot2 = false) {
 static int finish(cuozblasHandle_t *h, double t0) {
     cudaError_t e = cudaStreamSynchronize(state(h)->stream);
     h->t_total = (float)(wall() - t0);
+    State *st = state(h);
+    if (st->plain_timers && e == cudaSuccess) {  // the plain form's phases (src/cpu/ozblas_gemm.cpp timers)
+        h->t_SplitA = ev_ms(h, 0, 1) * 1e-3f;
+        h->t_SplitB = ev_ms(h, 1, 2) * 1e-3f;
+        h->t_comp = ev_ms(h, 2, 3) * 1e-3f;
+        h->t_sum = ev_ms(h, 3, 4) * 1e-3f;
+    }
+    st->plain_timers = false;
     if (e != cudaSuccess) {
         fprintf(stderr, "cuozblas: CUDA error %s\n", cudaGetErrorString(e));
         return CUOZBLAS_STATUS_CUDA_ERROR;
@@ -145,7 +153,7 @@ int cuozblasHandleCreate(cuozblasHandle_t *h, uint64_t workSizeBytes) {
     if (e == cudaSuccess) e = cudaMalloc((void **)&st->d_ints, sizeof(int) * 64);
     if (e == cudaSuccess) e = cudaMallocHost((void **)&st->h_ints, sizeof(int) * 64);
     if (e == cudaSuccess) e = cudaMallocHost((void **)&st->h_dbl, sizeof(double) * 64);
-    for (int i = 0; i < 4 && e == cudaSuccess; i++) e = cudaEventCreate(&st->ev[i]);
+    for (int i = 0; i < 5 && e == cudaSuccess; i++) e = cudaEventCreate(&st->ev[i]);
     if (e != cudaSuccess) {
         fprintf(stderr, "cuozblas: work memory allocation error (%1.3e bytes requested): %s\n",
                 (double)workSizeBytes, cudaGetErrorString(e));
@@ -173,7 +181,7 @@ int cuozblasHandleDestroy(cuozblasHandle_t *h) {
     cudaFree(st->d_ints);
     cudaFreeHost(st->h_ints);
     cudaFreeHost(st->h_dbl);
-    for (int i = 0; i < 4; i++)
+    for (int i = 0; i < 5; i++)
         if (st->ev[i]) cudaEventDestroy(st->ev[i]);
     delete st;
     h->devWork = h->devWorkCommon = nullptr;

@@ -373,7 +373,9 @@ int gemm_plain_core(cuozblasHandle_t *h, char ta, char tb, int m, int n, int k, 
     const bool skinny_n = (n == 1);
     const int ldk = dot || skinny_n ? ceil_to(k > 0 ? k : 1, 2) : ceil_to(k > 0 ? k : 1, kBK);
 
-    // ---- split ----
+    // ---- split ----  (phase events 0..4: start, A split, B split, products, sum)
+    ev_record(h, 0);
+    st->plain_timers = true;
     double *Sa = nullptr, *Sb = nullptr;
     int nA = 0, nB = 0;
     if (dot) {
@@ -384,6 +386,7 @@ int gemm_plain_core(cuozblasHandle_t *h, char ta, char tb, int m, int n, int k, 
         // lines of op(A): 'n' -> row i of A is strided by lda
         OZB_TRY(split_operand(h, !is_trans(ta), m, k, A, lda, rho, maxS, ldk, &Sa, &nA, ar));
     }
+    ev_record(h, 1);
     if (skinny_n) {
         Sb = ar.take<double>((uint64_t)maxS * ldk);
         if (!ar.ok) return CUOZBLAS_STATUS_WORKSPACE;
@@ -391,6 +394,7 @@ int gemm_plain_core(cuozblasHandle_t *h, char ta, char tb, int m, int n, int k, 
     } else {
         OZB_TRY(split_operand(h, is_trans(tb), n, k, B, ldb, rho, maxS, ldk, &Sb, &nB, ar));
     }
+    ev_record(h, 2);
     const int fast = dot ? 0 : fastMode;
     int maxlevel = (nA - 1) + (nB - 1);
     {
@@ -415,9 +419,11 @@ int gemm_plain_core(cuozblasHandle_t *h, char ta, char tb, int m, int n, int k, 
         counted(h);
         k_pair_dot2<<<dim3(blocks, nA * nB), 256, 0, st->stream>>>(k, nB, Sa, ldk, Sb, ldk, partials);
         OZB_CHECK(cudaGetLastError());
+        ev_record(h, 3);
         counted(h);
         k_dot2_finish<<<1, 64, 0, st->stream>>>(nA, nB, blocks, partials, h->sumMode, alpha, beta, C, tmp);
         OZB_CHECK(cudaGetLastError());
+        ev_record(h, 4);
         return CUOZBLAS_STATUS_SUCCESS;
     }
     if (dot || skinny_n) {
@@ -447,6 +453,7 @@ int gemm_plain_core(cuozblasHandle_t *h, char ta, char tb, int m, int n, int k, 
                 }
                 OZB_CHECK(cudaGetLastError());
             }
+        ev_record(h, 3);
         if (dot) {
             counted(h);
             k_sum_pair_matrix<<<1, 32, 0, st->stream>>>(nA, nB, maxlevel, P, nB, h->sumMode, alpha, beta, C, scr);
@@ -456,6 +463,7 @@ int gemm_plain_core(cuozblasHandle_t *h, char ta, char tb, int m, int n, int k, 
                                                               C, scr);
         }
         OZB_CHECK(cudaGetLastError());
+        ev_record(h, 4);
         return CUOZBLAS_STATUS_SUCCESS;
     }
 
@@ -505,6 +513,8 @@ int gemm_plain_core(cuozblasHandle_t *h, char ta, char tb, int m, int n, int k, 
                                                                nullptr);
         OZB_CHECK(cudaGetLastError());
     }
+    ev_record(h, 3);  // the ordered sum runs inside the product kernels here
+    ev_record(h, 4);
     return CUOZBLAS_STATUS_SUCCESS;
 }
 

@@ -24,7 +24,8 @@ struct State {
     double *h_dbl = nullptr;      // pinned host doubles (scalar results)
     int last_error = 0;
     int64_t splitA_ld = 0;        // slice stride of the pre-split A (cuozblasDcsrmvSplitA)
-    cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};  // phase timers (split A/B, products)
+    cudaEvent_t ev[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};  // phase timers (split A/B, products, sum)
+    bool plain_timers = false;    // ev[0..4] hold a plain-form call's phases, read at the call's end
     uint64_t launches = 0;        // kernels this handle has launched (cuozblasGetLaunchCount)
     // The matrix of the last fused CSRMV and the level count its rows needed:
     // the next call on the same matrix holds that many levels per row on chip

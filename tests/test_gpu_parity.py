@@ -72,6 +72,19 @@ def test_dgemm_run_to_run_identical(oracle, handle, ozb, cuda):
     assert bits_equal(outs[0], ref), first_diff(outs[0], ref)
 
 
+def test_phase_timers(oracle, handle, ozb, cuda):
+    """The exec-info phase timers (t_SplitA, t_SplitB, t_comp, t_sum) of the plain form are filled,
+    as the reference's drivers print them."""
+    m = n = k = 256
+    A = oracle.phi_matrix(m, k, 1.0, 1)
+    B = oracle.phi_matrix(k, n, 1.0, 2)
+    dC = cuda.zeros((n, m), dtype=cuda.float64, device="cuda")
+    handle.sumMode = 1
+    ozb.dgemm(handle, "n", "n", m, n, k, 1.0, dev(cuda, A), m, dev(cuda, B), k, 0.0, dC, m)
+    t = [handle.t_SplitA, handle.t_SplitB, handle.t_comp, handle.t_sum]
+    assert all(v > 0 for v in t) and sum(t) <= handle.t_total * 1.01, (t, handle.t_total)
+
+
 def test_dgemm_beta0_propagates_nan(oracle, handle, ozb, cuda):
     """C = fma(alpha, t, beta*C) with beta = 0 keeps NaN from C, as the reference does."""
     m = n = k = 8
