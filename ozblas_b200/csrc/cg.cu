@@ -215,14 +215,11 @@ int cg_graph(cuozblasHandle_t *h, int n, const double *val, const int *colind, c
     CG_CHECK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
     int cap = CUOZBLAS_STATUS_SUCCESS;
     for (int k = 0; k < K && !cap; k++) {
-        cap = plan_launch(s, &cs->vs, rho, maxS, true, &cs->plan, &d->gate);
-        if (!cap) cap = csr_proof_launch(s, n, p, rho, maxS, cs, &d->gate);
+        cap = csr_proof_launch(s, n, p, rho, maxS, cs, &d->gate);
         if (!cap) cap = csr_rows_launch(s, spmv, cs, slow, nslow, &dpq->vs, 1, terms, &d->gate);
-        if (!cap) cap = plan_launch(s, &dpq->vs, rho, maxS, false, &dpq->plan, &d->gate);
         if (!cap) cap = dot_tree_launch(s, nsm, n, p, q, rho, maxS, h->sumMode, dpq, &d->gate);
         k_cg_alpha<<<1, 1, 0, s>>>(d, dpq, cs);
         k_cg_update_xr<<<ub, 256, 0, s>>>(n, x, r, p, q, d, &drr->vs);
-        if (!cap) cap = plan_launch(s, &drr->vs, rho, maxS, true, &drr->plan, &d->gate);
         if (!cap) cap = dot_tree_launch(s, nsm, n, r, r, rho, maxS, h->sumMode, drr, &d->gate);
         k_cg_beta<<<1, 1, 0, s>>>(d, drr, res_dev, stamp_dev);
         k_cg_update_p<<<ub, 256, 0, s>>>(n, p, r, d, &cs->vs, &dpq->vs);
@@ -234,7 +231,7 @@ int cg_graph(cuozblasHandle_t *h, int n, const double *val, const int *colind, c
     }
     CG_CHECK(ce);
     CG_CHECK(cudaGraphInstantiate(&exec, graph, 0));
-    const int per_iter = 11 + (nslow > 0 ? (nslow + 8191) / 8192 : 0);
+    const int per_iter = 8 + (nslow > 0 ? (nslow + 8191) / 8192 : 0);
     // device clock against the host's, for the elapsed-time history
     k_cg_stamp<<<1, 1, 0, s>>>(stamp_dev + maxiter + 1);
     unsigned long long dev0 = 0;

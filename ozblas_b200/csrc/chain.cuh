@@ -125,6 +125,20 @@ __device__ inline void make_plan(const VecStats *vs, int rho, int maxS, bool sam
     pl.L = L;
 }
 
+// The plan straight from the first pass's statistics, computed by thread 0
+// into shared memory (the caller synchronises the block).  Every CTA of the
+// kernel that consumes the statistics does this; its last CTA zeroes them.
+__device__ __forceinline__ void plan_in_block(const VecStats *g, int rho, int maxS, bool same, TreePlan &sh) {
+    if (threadIdx.x != 0) return;
+    VecStats vs;
+    for (int v = 0; v < 2; v++) {
+        vs.mx[v] = __ldcg(&g->mx[v]);
+        vs.lsb[v] = __ldcg(&g->lsb[v]);
+        vs.bad[v] = __ldcg(&g->bad[v]);
+    }
+    make_plan(&vs, rho, maxS, same, sh);
+}
+
 // Copy a plan from global memory into shared memory (whole block).
 __device__ __forceinline__ void load_plan(const TreePlan *g, TreePlan &sh) {
     static_assert(sizeof(TreePlan) % 4 == 0, "plan layout");

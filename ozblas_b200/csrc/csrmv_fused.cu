@@ -74,7 +74,7 @@ __global__ void __launch_bounds__(256) k_csr_proof(int n, const double *__restri
     __shared__ TreePlan pl;
     __shared__ int last;
     const int t = threadIdx.x;
-    load_plan(&sc->plan, pl);
+    plan_in_block(&sc->vs, rho, maxS, true, pl);
     __syncthreads();
     const unsigned need = pl.need[0];
     if (pl.valid && need) {  // uniform
@@ -111,23 +111,11 @@ __global__ void __launch_bounds__(256) k_csr_proof(int n, const double *__restri
     for (int s = 0; s < kCsrLv; s++) sc->sigma[s] = pl.sig[0][s];
     sc->nB = pl.ns[0];
     sc->valid = valid;
-    // leave the proof zeroed for the next use
+    // leave the proof and the statistics zeroed for the next use (every block
+    // has read the statistics: the ticket comes after)
     sc->proven = 0u;
     sc->ticket = 0u;
-}
-
-__global__ void k_make_plan(VecStats *vs, int rho, int maxS, int same, TreePlan *plan, const int *gate) {
-    if (gate && *gate == 0) return;
-    if (threadIdx.x != 0 || blockIdx.x != 0) return;
-    TreePlan pl;
-    make_plan(vs, rho, maxS, same != 0, pl);
-    *plan = pl;
-    *vs = VecStats{};
-}
-
-int plan_launch(cudaStream_t s, VecStats *vs, int rho, int maxS, bool same, TreePlan *plan, const int *gate) {
-    k_make_plan<<<1, 32, 0, s>>>(vs, rho, maxS, same ? 1 : 0, plan, gate);
-    return cudaGetLastError() == cudaSuccess ? CUOZBLAS_STATUS_SUCCESS : CUOZBLAS_STATUS_CUDA_ERROR;
+    sc->vs = VecStats{};
 }
 
 // Visit the pairs (ia < na, ib < nb) of a row in summation order: ik
@@ -1007,8 +995,6 @@ int csrmv_fused(cuozblasHandle_t *h, int m, int n, double alpha, const double *v
     const int nsm = sm_count();
     counted(h);
     OZB_TRY(vec_stats_launch(s, nsm, n, x, &sc->vs, 0));
-    counted(h);
-    OZB_TRY(plan_launch(s, &sc->vs, rho, maxS, true, &sc->plan, nullptr));
     counted(h);
     OZB_TRY(csr_proof_launch(s, n, x, rho, maxS, sc, nullptr));
     const CsrmvArgs args{m, n, alpha, beta, val, colind, rowptr, x, y, shift, h->splitEpsMode, maxS, h->sumMode,

@@ -191,7 +191,7 @@ __global__ void __launch_bounds__(kDotThreads, 1) k_dot_tree(int n, const double
     __shared__ double red[kDotThreads / 32][kDotLevels * kDotLevels];
     __shared__ int last;
     const int t = threadIdx.x;
-    load_plan(&sc->plan, pl);
+    plan_in_block(&sc->vs, rho, maxS, SAME, pl);
     __syncthreads();
     double P[kDotLevels][kDotLevels];
 #pragma unroll
@@ -288,6 +288,7 @@ __global__ void __launch_bounds__(kDotThreads, 1) k_dot_tree(int n, const double
     if (t == 0) {
         sc->proven[0] = sc->proven[1] = 0u;
         sc->ticket = 0u;
+        sc->vs = VecStats{};  // every CTA has read the statistics (the ticket comes after)
     }
 }
 
@@ -355,7 +356,7 @@ int dot_tree_launch(cudaStream_t s, int nsm, int n, const double *x, const doubl
     // level take the tensor-core pass (it holds every valid plan; below that
     // length its fixed costs outweigh the FP64 tree pass, which takes the rest)
     if (aligned && n >= (1 << 22) && dot_i8_digits(rho) > 0 && !getenv("OZBLAS_DOT_TREE"))
-        return dot_i8_launch(s, nsm, n, x, y, rho, sum_mode, sc, gate);
+        return dot_i8_launch(s, nsm, n, x, y, rho, maxS, sum_mode, sc, gate);
     int fblocks = (int)(((int64_t)n + 2 * kDotThreads - 1) / (2 * kDotThreads));
     if (fblocks > nsm) fblocks = nsm;  // ~250 registers per thread: one 256-thread block per SM
     if (fblocks < 1) fblocks = 1;
@@ -399,8 +400,6 @@ int dot_fused(cuozblasHandle_t *h, int n, const double *x, const double *y, doub
     const int nsm = sm_count();
     counted(h);
     OZB_TRY(dot_scan_launch(st->stream, nsm, n, x, y, sc));
-    counted(h);
-    OZB_TRY(plan_launch(st->stream, &sc->vs, rho, maxS, x == y, &sc->plan, nullptr));
     counted(h);
     OZB_TRY(dot_tree_launch(st->stream, nsm, n, x, y, rho, maxS, h->sumMode, sc, nullptr));
     static_assert(sizeof(DotStatus) == 24, "status block layout");

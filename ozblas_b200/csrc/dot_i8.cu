@@ -207,7 +207,7 @@ __device__ void di_finish(DotScratch *sc, const TreePlan &pl, bool same, int sum
 // 32 (three digits, up to 8 levels); a job is 128 / RP chunks.
 template <bool SAME, int D, int RP, int G>
 __global__ void __launch_bounds__(kDiThreads, 1)
-    k_dot_i8(int n, const double *__restrict__ x, const double *__restrict__ y, int sum_mode,
+    k_dot_i8(int n, const double *__restrict__ x, const double *__restrict__ y, int rho, int maxS, int sum_mode,
              DotScratch *__restrict__ sc, const int *__restrict__ gate) {
     constexpr int CH = 128 / RP;   // chunks per job
     constexpr int JOB = 128 * CH;  // elements per job
@@ -225,7 +225,7 @@ __global__ void __launch_bounds__(kDiThreads, 1)
     __shared__ int last;
     const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
     __shared__ double sk[2][kDotLevels];
-    load_plan(&sc->plan, pl);
+    plan_in_block(&sc->vs, rho, maxS, SAME, pl);
     for (int i = t; i < RP * RP; i += kDiThreads) red[i] = 0ull;
     __syncthreads();
     if (t < 2 * kDotLevels) {  // sigma_s + 0x80808080 g_s: exact (an integer below 2^53 times g_s)
@@ -398,6 +398,7 @@ __global__ void __launch_bounds__(kDiThreads, 1)
         sc->proven[0] = sc->proven[1] = 0u;
         sc->ticket = 0u;
         sc->err = 0;
+        sc->vs = VecStats{};  // every CTA has read the statistics (the ticket comes after)
     }
 }
 
@@ -410,8 +411,8 @@ int dot_i8_digits(int rho) {
 }
 
 template <bool SAME, int D, int G>
-static int launch_i8(int grid, cudaStream_t s, int n, const double *x, const double *y, int sum_mode,
-                     DotScratch *sc, const int *gate) {
+static int launch_i8(int grid, cudaStream_t s, int n, const double *x, const double *y, int rho, int maxS,
+                     int sum_mode, DotScratch *sc, const int *gate) {
     constexpr int RP = D == 2 ? 16 : 32;
     static bool attr = false;  // once per instantiation
     if (!attr) {
@@ -420,7 +421,7 @@ static int launch_i8(int grid, cudaStream_t s, int n, const double *x, const dou
             return CUOZBLAS_STATUS_CUDA_ERROR;
         attr = true;
     }
-    k_dot_i8<SAME, D, RP, G><<<grid, kDiThreads, kDiSmem, s>>>(n, x, y, sum_mode, sc, gate);
+    k_dot_i8<SAME, D, RP, G><<<grid, kDiThreads, kDiSmem, s>>>(n, x, y, rho, maxS, sum_mode, sc, gate);
     return cudaGetLastError() == cudaSuccess ? CUOZBLAS_STATUS_SUCCESS : CUOZBLAS_STATUS_CUDA_ERROR;
 }
 
@@ -439,17 +440,17 @@ int dot_i8_prepare() {
 }
 
 template <bool SAME>
-static int launch_i8_g(int D, int G, int grid, cudaStream_t s, int n, const double *x, const double *y,
-                       int sum_mode, DotScratch *sc, const int *gate) {
-    if (D == 2 && G == 3) return launch_i8<SAME, 2, 3>(grid, s, n, x, y, sum_mode, sc, gate);
-    if (D == 2 && G == 4) return launch_i8<SAME, 2, 4>(grid, s, n, x, y, sum_mode, sc, gate);
-    if (D == 3 && G == 2) return launch_i8<SAME, 3, 2>(grid, s, n, x, y, sum_mode, sc, gate);
-    if (D == 3 && G == 3) return launch_i8<SAME, 3, 3>(grid, s, n, x, y, sum_mode, sc, gate);
+static int launch_i8_g(int D, int G, int grid, cudaStream_t s, int n, const double *x, const double *y, int rho,
+                       int maxS, int sum_mode, DotScratch *sc, const int *gate) {
+    if (D == 2 && G == 3) return launch_i8<SAME, 2, 3>(grid, s, n, x, y, rho, maxS, sum_mode, sc, gate);
+    if (D == 2 && G == 4) return launch_i8<SAME, 2, 4>(grid, s, n, x, y, rho, maxS, sum_mode, sc, gate);
+    if (D == 3 && G == 2) return launch_i8<SAME, 3, 2>(grid, s, n, x, y, rho, maxS, sum_mode, sc, gate);
+    if (D == 3 && G == 3) return launch_i8<SAME, 3, 3>(grid, s, n, x, y, rho, maxS, sum_mode, sc, gate);
     return CUOZBLAS_STATUS_INVALID_VALUE;
 }
 
-int dot_i8_launch(cudaStream_t s, int nsm, int n, const double *x, const double *y, int rho, int sum_mode,
-                  DotScratch *sc, const int *gate) {
+int dot_i8_launch(cudaStream_t s, int nsm, int n, const double *x, const double *y, int rho, int maxS,
+                  int sum_mode, DotScratch *sc, const int *gate) {
     const int D = dot_i8_digits(rho);
     const int G = chain_group(rho, 4);  // levels cut from one base value, as the tree pass
     const int job = D == 2 ? 1024 : 512;
@@ -458,8 +459,8 @@ int dot_i8_launch(cudaStream_t s, int nsm, int n, const double *x, const double 
     const int64_t need = (njobs + kDiMaxJobs - 1) / kDiMaxJobs;
     if (grid < need) grid = need;
     if (grid < 1) grid = 1;
-    return x == y ? launch_i8_g<true>(D, G, (int)grid, s, n, x, y, sum_mode, sc, gate)
-                  : launch_i8_g<false>(D, G, (int)grid, s, n, x, y, sum_mode, sc, gate);
+    return x == y ? launch_i8_g<true>(D, G, (int)grid, s, n, x, y, rho, maxS, sum_mode, sc, gate)
+                  : launch_i8_g<false>(D, G, (int)grid, s, n, x, y, rho, maxS, sum_mode, sc, gate);
 }
 
 }  // namespace ozb

@@ -19,7 +19,6 @@ constexpr int kDotDigitRows = 32;  // levels x digits per vector in the tensor-c
 
 struct DotScratch {
     VecStats vs;                        // first pass: max, lowest set bit, Inf/NaN of x and y
-    TreePlan plan;                      // the chains planned from vs (plan_launch)
     double P[kDotLevels * kDotLevels];  // exact slice products P[ia * 8 + ib]
     long long T[kDotDigitRows * kDotDigitRows];  // tensor-core pass: digit-pair sums T[p * 32 + q]
     unsigned proven[2];                 // levels whose predicted tau some element proved
@@ -34,7 +33,6 @@ constexpr int kCsrThreads = 128;
 
 struct CsrScratch {
     VecStats vs;                 // first pass over x
-    TreePlan plan;               // x's chain planned from vs (plan_launch)
     unsigned proven;             // levels of x's chain whose predicted tau some element proved
     unsigned ticket;             // blocks of the proof pass that are done
     int valid, nB, nslow, zmax;  // zmax: first zero-remainder level of A, max over rows
@@ -53,13 +51,10 @@ int dot_tree_prepare();
 // not applicable), its launch (every valid plan) and its shared-memory
 // attributes.
 int dot_i8_digits(int rho);
-int dot_i8_launch(cudaStream_t s, int nsm, int n, const double *x, const double *y, int rho, int sum_mode,
-                  DotScratch *sc, const int *gate);
+int dot_i8_launch(cudaStream_t s, int nsm, int n, const double *x, const double *y, int rho, int maxS,
+                  int sum_mode, DotScratch *sc, const int *gate);
 int dot_i8_prepare();
 
-// Plans the chain(s) from the first pass's statistics once, into `plan`,
-// and zeroes the statistics for the next use (one thread; `gate` as above).
-int plan_launch(cudaStream_t s, VecStats *vs, int rho, int maxS, bool same, TreePlan *plan, const int *gate);
 
 // CSRMV pieces (csrmv_fused.cu): statistics of a vector into vs[index]; the
 // rows the row kernel defers (a property of the matrix); proof of x's chain
