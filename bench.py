@@ -135,6 +135,19 @@ def cpu_reference_sample(rows_sample=256, threads=None):
                       f"8192^3 phi=1 problem ({t:.2f} s, B split included)"}, None
 
 
+def max_over_ranks(value, dist):
+    """The slowest rank's time (or any scalar's maximum) over the process group; `dist` None: one
+    process.  NCCL groups reduce on the GPU, gloo groups (CPU tests) on the host."""
+    if dist is None:
+        return value
+    import torch
+
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([float(value)], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 def run_reference_arm(args, rank, world):
     if rank != 0:
         return 0
@@ -251,11 +264,7 @@ def main():
             kern_ms.append(h.t_comp * 1e3)
         barrier()
     launches = (h.launch_count() - launches0) / args.steps
-    ms = statistics.mean(e0.elapsed_time(e1) for e0, e1 in ev)
-    if dist is not None:
-        t = torch.tensor([ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = max_over_ranks(statistics.mean(e0.elapsed_time(e1) for e0, e1 in ev), dist)
     flops = 2.0 * n * n * n
     value = world * flops / (ms * 1e-3) / 1e12
     pairs = h.nSplitC
@@ -276,11 +285,7 @@ def main():
         e2e_step()
         ev2[i][1].record(stream)
     barrier()
-    ms_e2e = statistics.mean(e0.elapsed_time(e1) for e0, e1 in ev2)
-    if dist is not None:
-        t = torch.tensor([ms_e2e], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms_e2e = float(t.item())
+    ms_e2e = max_over_ranks(statistics.mean(e0.elapsed_time(e1) for e0, e1 in ev2), dist)
     e2e = {"value": world * flops / (ms_e2e * 1e-3) / 1e12, "unit": "TFLOPS", "h2d_bytes_per_step": 2 * n * n * 8,
            "d2h_bytes_per_step": n * n * 8, "ms_per_step": ms_e2e}
 
