@@ -267,6 +267,38 @@ def test_ddot_tensor_core_pass(n, phi, sm, oracle, handle, ozb, cuda):
     assert np.float64(nr).view(np.int64) == np.float64(nr_ref).view(np.int64), (nr, nr_ref)
 
 
+@pytest.mark.parametrize("case", ["n_at_threshold", "one_element_tail", "zero_block", "same_vector", "nan_inf",
+                                  "unaligned", "wide_range"])
+def test_ddot_tensor_core_pass_edges(case, oracle, handle, ozb, cuda):
+    """Edge cases around the tensor-core pass: its length threshold, a last job holding one element,
+    jobs of zeros, x = y, Inf/NaN (the general path answers), a vector 8 bytes off a 16-byte
+    boundary (the tree pass answers) and a range too wide for 8 levels."""
+    n = (1 << 22) + (1 if case == "one_element_tail" else 0)
+    x = oracle.phi_vector(n, 1.0, 5)
+    y = oracle.phi_vector(n, 1.0, 6)
+    if case == "zero_block":
+        x[100000:900000] = 0.0
+    if case == "nan_inf":
+        x[12345] = np.inf
+        y[777] = np.nan
+    if case == "wide_range":
+        x[::1000] *= 2.0 ** 200
+    for sm in (0, 1):
+        handle.sumMode = sm
+        if case == "unaligned":
+            bx = cuda.zeros(n + 1, dtype=cuda.float64, device="cuda")
+            bx[1:] = dev(cuda, x)
+            dx = bx[1:]
+        else:
+            dx = dev(cuda, x)
+        dy = dx if case == "same_vector" else dev(cuda, y)
+        yy = x if case == "same_vector" else y
+        d = ozb.ddot(handle, n, dx, dy)
+        r, info = oracle.ddot(make_flags(sumMode=sm), x, yy)
+        assert np.float64(d).view(np.int64) == np.float64(r).view(np.int64), (case, sm, d, r)
+        assert (handle.nSplitA, handle.nSplitB) == (info.nSplitA, info.nSplitB)
+
+
 def test_ddot_tensor_core_pass_matches_tree(oracle, handle, ozb, cuda, monkeypatch):
     """The INT8 tensor-core pass (vectors of 2^22 elements and more) and the FP64 tree pass give the same
     bits, with 3 and 2 digits per level."""
