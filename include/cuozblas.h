@@ -134,7 +134,8 @@ template <typename TYPE1, typename TYPE2>
 int32_t cuozblasRcg(cuozblasHandle_t *oh, const char tranA, const int32_t dimN, const int32_t dimNNZ,
                     const cusparseMatDescr_t descrA, const TYPE1 *matA, const int32_t *matAcolind,
                     const int32_t *matArowptr, const TYPE1 *vecB, TYPE1 *vecX, int32_t maxiter, TYPE1 tol);
-/* Exported instantiations: <double,double,double> for nrm2/dot/gemv/gemm,
+/* Exported instantiations: <double,double,double> and <double,float,float>
+ * for nrm2/dot/gemv/gemm,
  * <double> for axpy, <double,double> for csrmv/csrmvSplitA/cg, and the INT8
  * precision form cuozblasRgemm<double,int8_t,int32_t> (the instantiation
  * the reference leaves commented out at src/cuda/cuozblas_gemm.cu:292). */
@@ -183,6 +184,20 @@ int cuozblasDcsrmvSplitA(cuozblasHandle_t *h, char trans, int32_t m, int32_t n, 
 int cuozblasDcg(cuozblasHandle_t *h, char trans, int32_t n, int32_t nnz, const void *descrA, const double *val,
                 const int32_t *colind, const int32_t *rowptr, const double *b, double *x, int32_t maxiter,
                 double tol);
+
+/* Mixed form <double,float,float> (include/cuozblas.h:75-77 instantiated at
+ * src/cuda/cuozblas_gemm.cu:286, src/cuda/cuozblas_dot.cu, cuozblas_nrm2.cu,
+ * cuozblas_gemv.cu): FP64 data with FP32 slices and FP32 slice products,
+ * bit-exact to the reference CPU path (src/cpu/ozblas_gemm.cpp with TYPE2 =
+ * TYPE3 = float).  sumMode 0 (FSum) only: the reference has no NearSum for
+ * mixed types (CUOZBLAS_STATUS_NOT_SUPPORTED here, exit(1) there); no Dot2. */
+int cuozblasDSgemm(cuozblasHandle_t *h, char transa, char transb, int32_t m, int32_t n, int32_t k, double alpha,
+                   const double *A, int32_t lda, const double *B, int32_t ldb, double beta, double *C, int32_t ldc);
+int cuozblasDSgemv(cuozblasHandle_t *h, char trans, int32_t m, int32_t n, double alpha, const double *A,
+                   int32_t lda, const double *x, int32_t incx, double beta, double *y, int32_t incy);
+int cuozblasDSdot(cuozblasHandle_t *h, int32_t n, const double *x, int32_t incx, const double *y, int32_t incy,
+                  double *ret);
+int cuozblasDSnrm2(cuozblasHandle_t *h, int32_t n, const double *x, int32_t incx, double *ret);
 
 /* INT8 precision form (no reference implementation; the reference stubs it
  * at src/cuda/cuozblas_gemm.cu:292 and src/cuda/cuozblas_blas_wrapper.cu:147-208):

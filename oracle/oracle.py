@@ -82,6 +82,14 @@ class Restatement:
         L.oz_tau_libm.argtypes = [C.c_double]
         L.oz_split_cols.restype = C.c_int
         L.oz_split_cols.argtypes = [F, C.c_int, C.c_int, _dp, C.c_int, C.c_int, _dp, C.c_int]
+        L.oz_rho_f32.restype = C.c_int
+        L.oz_rho_f32.argtypes = [C.c_int, C.c_int]
+        L.oz_split_cols_f32.restype = C.c_int
+        L.oz_split_cols_f32.argtypes = [F, C.c_int, C.c_int, _dp, C.c_int, C.c_int, C.POINTER(C.c_float), C.c_int,
+                                        C.POINTER(C.c_short)]
+        L.oz_dgemm_f32.restype = C.c_int
+        L.oz_dgemm_f32.argtypes = [F, C.c_char, C.c_char, C.c_int, C.c_int, C.c_int, C.c_double, _dp, C.c_int,
+                                   _dp, C.c_int, C.c_double, _dp, C.c_int, I]
         L.oz_split_rows_csr.restype = C.c_int
         L.oz_split_rows_csr.argtypes = [F, C.c_int, _dp, _ip, C.c_int, _dp, C.c_int]
         L.oz_nearsum.restype = C.c_double
@@ -171,6 +179,29 @@ class Restatement:
         out = np.zeros((maxS + 1, ncol, max(k, 1)), dtype=np.float64)
         s = self.L.oz_split_cols(C.byref(flags), k, ncol, _d(X), max(k, 1), shift, _d(out), max(k, 1))
         return s, out[:s, :, :k]
+
+    def rho_f32(self, dim, mode=0):
+        return self.L.oz_rho_f32(dim, mode)
+
+    def split_cols_f32(self, flags, X, shift=1):
+        """Mixed form: (nsplit, float slices[nsplit, ncol, k], short exps[nsplit, ncol])."""
+        X = np.ascontiguousarray(X, dtype=np.float64)
+        ncol, k = X.shape
+        maxS = flags.nSplitMax if flags.nSplitMax > 0 else 30
+        out = np.zeros((maxS + 1, ncol, max(k, 1)), dtype=np.float32)
+        ex = np.zeros((maxS + 1, max(ncol, 1)), dtype=np.int16)
+        s = self.L.oz_split_cols_f32(C.byref(flags), k, ncol, _d(X), max(k, 1), shift,
+                                     out.ctypes.data_as(C.POINTER(C.c_float)), max(k, 1),
+                                     ex.ctypes.data_as(C.POINTER(C.c_short)))
+        return s, out[:s, :, :k], ex[:s, :ncol]
+
+    def dgemm_f32(self, flags, ta, tb, m, n, k, alpha, A, lda, B, ldb, beta, C_, ldc):
+        """GEMM <double, float, float> (FSum only); (C, info), or (None, None) for unsupported flags."""
+        info = Info()
+        Cc = np.array(C_, dtype=np.float64, copy=True)
+        r = self.L.oz_dgemm_f32(C.byref(flags), ta.encode(), tb.encode(), m, n, k, alpha, _d(A), lda, _d(B), ldb,
+                                beta, _d(Cc), ldc, C.byref(info))
+        return (Cc, info) if r == 0 else (None, None)
 
     def split_csr(self, flags, val, rowptr, shift=1):
         m = len(rowptr) - 1
@@ -266,6 +297,13 @@ class Reference:
         L.ref_get_threads.restype = C.c_int
         L.ref_dgemm.argtypes = [C.c_void_p, C.c_char, C.c_char, C.c_int, C.c_int, C.c_int, C.c_double, _dp,
                                 C.c_int, _dp, C.c_int, C.c_double, _dp, C.c_int]
+        L.ref_dgemm_f32.argtypes = L.ref_dgemm.argtypes
+        L.ref_ddot_f32.restype = C.c_double
+        L.ref_ddot_f32.argtypes = [C.c_void_p, C.c_int, _dp, _dp]
+        L.ref_dnrm2_f32.restype = C.c_double
+        L.ref_dnrm2_f32.argtypes = [C.c_void_p, C.c_int, _dp]
+        L.ref_dgemv_f32.argtypes = [C.c_void_p, C.c_char, C.c_int, C.c_int, C.c_double, _dp, C.c_int, _dp,
+                                    C.c_double, _dp]
         L.ref_ddot.restype = C.c_double
         L.ref_ddot.argtypes = [C.c_void_p, C.c_int, _dp, _dp]
         L.ref_dnrm2.restype = C.c_double
@@ -320,6 +358,24 @@ class Reference:
         self.L.ref_dgemm(self.h, ta.encode(), tb.encode(), m, n, k, alpha, _d(A), lda, _d(B), ldb, beta, _d(Cc),
                          ldc)
         return Cc
+
+    def dgemm_f32(self, ta, tb, m, n, k, alpha, A, lda, B, ldb, beta, C_, ldc):
+        """ozblasRgemm<double, float, float>: double data, FP32 slices and slice products."""
+        Cc = np.array(C_, dtype=np.float64, copy=True)
+        self.L.ref_dgemm_f32(self.h, ta.encode(), tb.encode(), m, n, k, alpha, _d(A), lda, _d(B), ldb, beta,
+                             _d(Cc), ldc)
+        return Cc
+
+    def ddot_f32(self, x, y):
+        return self.L.ref_ddot_f32(self.h, len(x), _d(x), _d(y))
+
+    def dnrm2_f32(self, x):
+        return self.L.ref_dnrm2_f32(self.h, len(x), _d(x))
+
+    def dgemv_f32(self, ta, m, n, alpha, A, lda, x, beta, y):
+        yy = np.array(y, dtype=np.float64, copy=True)
+        self.L.ref_dgemv_f32(self.h, ta.encode(), m, n, alpha, _d(A), lda, _d(x), beta, _d(yy))
+        return yy
 
     def ddot(self, x, y):
         return self.L.ref_ddot(self.h, len(x), _d(x), _d(y))

@@ -24,6 +24,9 @@
 #define OZ_SPLIT_CONST 0.75    /* CONST, src/cpu/ozblas_split.cpp:9 */
 
 static int oz_max_split(const oz_flags *f) { return f->nSplitMax > 0 ? f->nSplitMax : OZ_DEFAULT_MAXSPLIT; }
+static int imax(int a, int b);
+static int imin(int a, int b);
+static int make_pairs(int nA, int nB, int maxlevel, int *pa, int *pb);
 
 /* std::max(a, b) as the reference uses it: returns a unless a < b. */
 static inline double ref_max(double a, double b) { return (a < b) ? b : a; }
@@ -101,6 +104,135 @@ int oz_split_cols(const oz_flags *f, int k, int ncol, const double *X, int ldx, 
     free(R);
     free(mx);
     return s;
+}
+
+/* ------------------------------------------------------------------------ */
+/* Mixed form <double, float, float>: FP32 slices of double data             */
+/* ------------------------------------------------------------------------ */
+
+/* getRho<double,float>, src/cpu/ozblas_split.cpp:19-34 (epse 53 and 24) */
+int oz_rho_f32(int dim, int splitEpsMode) {
+    switch (splitEpsMode) {
+    case 9: return (int)ceil((53 - (24 - log2(2. * sqrt(dim))) / 2));
+    default: return (int)ceil((53 - (24 - log2(1. * dim)) / 2));
+    }
+}
+
+/* One level, src/cpu/ozblas_split.cpp:181-221 (and the vector form :106-135): the slice is cut in
+ * double and stored as scalbn(slice, -tau) in float, tau kept per column and level. */
+static double split_level_cols_f32(int k, int ncol, int rho, double *R, int ldr, float *S, int lds, short *E,
+                                   double *mx, int shift) {
+    double check = 0.;
+    for (int j = 0; j < ncol; j++) {
+        const short tau = (short)ceil(log2(fabs(mx[j])));
+        E[j] = tau;
+        const double sigma = OZ_SPLIT_CONST * scalbn(1., rho + tau) * shift;
+        double m = 0.;
+        for (int i = 0; i < k; i++) {
+            double x = R[(size_t)j * ldr + i];
+            const double s = (x + sigma) - sigma;
+            x = x - s;
+            S[(size_t)j * lds + i] = (float)scalbn(s, -tau);
+            R[(size_t)j * ldr + i] = x;
+            m = ref_max(m, fabs(x));
+        }
+        mx[j] = m;
+        check += m;
+    }
+    return check;
+}
+
+/* Split driver as oz_split_cols (src/cpu/ozblas_split.cpp:254-289); exps holds maxS rows of ncol. */
+int oz_split_cols_f32(const oz_flags *f, int k, int ncol, const double *X, int ldx, int shift, float *slices,
+                      int lds, short *exps) {
+    const int rho = oz_rho_f32(k, f->splitEpsMode);
+    const int maxS = oz_max_split(f);
+    double *R = (double *)malloc(sizeof(double) * (size_t)(k > 0 ? k : 1) * (ncol > 0 ? ncol : 1));
+    double *mx = (double *)malloc(sizeof(double) * (ncol > 0 ? ncol : 1));
+    for (int j = 0; j < ncol; j++) {
+        double m = 0.;
+        for (int i = 0; i < k; i++) {
+            R[(size_t)j * k + i] = X[(size_t)j * ldx + i];
+            m = ref_max(m, fabs(X[(size_t)j * ldx + i]));
+        }
+        mx[j] = m;
+    }
+    split_level_cols_f32(k, ncol, rho, R, k, slices, lds, exps, mx, shift);
+    int s = 1;
+    while (s < maxS) {
+        const double c = split_level_cols_f32(k, ncol, rho, R, k, slices + (size_t)s * lds * ncol, lds,
+                                              exps + (size_t)s * ncol, mx, shift);
+        s++;
+        if (c == 0.) break;
+    }
+    free(R);
+    free(mx);
+    return s;
+}
+
+/*
+ * GEMM <double, float, float>, src/cpu/ozblas_gemm.cpp:3-315 with TYPE2 = TYPE3 = float: the
+ * slice products are FP32 GEMMs, exact by the rho rule (so any order gives these bits), and
+ * the ordered sum adds scalbn(product, tauA + tauB) in double (ozblas_sum.cpp:382-432).  The
+ * reference has no NearSum for mixed types (ozblas_sum.cpp:273-296 exits), nor Dot2.  DOT,
+ * NRM2 and GEMV of this form are this GEMM (src/cpu/ozblas_dot.cpp:25, ozblas_gemv.cpp:23-26).
+ */
+int oz_dgemm_f32(const oz_flags *f, char ta, char tb, int m, int n, int k, double alpha, const double *A, int lda,
+                 const double *B, int ldb, double beta, double *C, int ldc, oz_info *info) {
+    if (f->reproMode != 1 || f->sumMode != 0 || (f->splitEpsMode != 0 && f->splitEpsMode != 9)) return -1;
+    const int is_dot = (m == 1 && n == 1);
+    const int fast = is_dot ? 0 : f->fastMode;
+    const int maxS = oz_max_split(f);
+    const int kk = k > 0 ? k : 1;
+    double *Ap = (double *)malloc(sizeof(double) * (size_t)kk * imax(m, 1));
+    double *Bp = (double *)malloc(sizeof(double) * (size_t)kk * imax(n, 1));
+    const int tA = !(ta == 'n' || ta == 'N'), tB = !(tb == 'n' || tb == 'N');
+    for (int i = 0; i < m; i++)
+        for (int l = 0; l < k; l++) Ap[(size_t)i * k + l] = tA ? A[(size_t)i * lda + l] : A[(size_t)l * lda + i];
+    for (int j = 0; j < n; j++)
+        for (int l = 0; l < k; l++) Bp[(size_t)j * k + l] = tB ? B[(size_t)l * ldb + j] : B[(size_t)j * ldb + l];
+    float *Sa = (float *)calloc((size_t)(maxS + 1) * kk * imax(m, 1), sizeof(float));
+    float *Sb = (float *)calloc((size_t)(maxS + 1) * kk * imax(n, 1), sizeof(float));
+    short *Ea = (short *)calloc((size_t)(maxS + 1) * imax(m, 1), sizeof(short));
+    short *Eb = (short *)calloc((size_t)(maxS + 1) * imax(n, 1), sizeof(short));
+    const int nA = oz_split_cols_f32(f, k, m, Ap, k, 1, Sa, k, Ea);
+    const int nB = oz_split_cols_f32(f, k, n, Bp, k, 1, Sb, k, Eb);
+    int maxlevel = (nA - 1) + (nB - 1);
+    maxlevel = imax(maxlevel - fast, imin(nA - 1, nB - 1));
+    int *pa = (int *)malloc(sizeof(int) * nA * nB), *pb = (int *)malloc(sizeof(int) * nA * nB);
+    const int np = make_pairs(nA, nB, maxlevel, pa, pb);
+    for (int j = 0; j < n; j++)
+        for (int i = 0; i < m; i++) {
+            double t = 0.;
+            for (int p = 0; p < np; p++) {
+                const float *a = Sa + (size_t)pa[p] * k * m + (size_t)i * k;
+                const float *b = Sb + (size_t)pb[p] * k * n + (size_t)j * k;
+                float c = 0.f;
+                for (int l = 0; l < k; l++) c += a[l] * b[l]; /* exact in FP32 */
+                t += scalbn((double)c, Ea[(size_t)pa[p] * m + i] + Eb[(size_t)pb[p] * n + j]);
+            }
+            double *cc = &C[(size_t)j * ldc + i];
+            *cc = fma(alpha, t, (beta * *cc));
+        }
+    if (info) {
+        info->nSplitA = (float)nA;
+        info->nSplitB = (float)nB;
+        if (is_dot)
+            info->nSplitC = 1.f;
+        else if (n == 1 && fast == 0)
+            info->nSplitC = (float)imin(maxlevel + 1, nA);
+        else
+            info->nSplitC = (float)np;
+    }
+    free(Ap);
+    free(Bp);
+    free(Sa);
+    free(Sb);
+    free(Ea);
+    free(Eb);
+    free(pa);
+    free(pb);
+    return 0;
 }
 
 /*

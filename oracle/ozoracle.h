@@ -40,6 +40,11 @@ typedef struct {
 
 /* ---- split helpers ---- */
 int oz_rho(int dim, int splitEpsMode);
+int oz_rho_f32(int dim, int splitEpsMode);
+int oz_split_cols_f32(const oz_flags *f, int k, int ncol, const double *X, int ldx, int shift, float *slices,
+                      int lds, short *exps);
+int oz_dgemm_f32(const oz_flags *f, char ta, char tb, int m, int n, int k, double alpha, const double *A, int lda,
+                 const double *B, int ldb, double beta, double *C, int ldc, oz_info *info);
 int oz_tau_libm(double v);          /* (short)ceil(log2(v)) as the reference evaluates it */
 
 int oz_split_cols(const oz_flags *f, int k, int ncol, const double *X, int ldx, int shift, double *slices,

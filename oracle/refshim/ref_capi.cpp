@@ -68,6 +68,26 @@ int ref_dgemm(void *hp, char ta, char tb, int m, int n, int k, double alpha, con
                                                C, ldc);
 }
 
+/* the mixed form <double, float, float>: double data, FP32 slices and slice products */
+int ref_dgemm_f32(void *hp, char ta, char tb, int m, int n, int k, double alpha, const double *A, int lda,
+                  const double *B, int ldb, double beta, double *C, int ldc) {
+    return ozblasRgemm<double, float, float>((ozblasHandle_t *)hp, ta, tb, m, n, k, alpha, A, lda, B, ldb, beta, C,
+                                             ldc);
+}
+
+double ref_ddot_f32(void *hp, int n, const double *x, const double *y) {
+    return ozblasRdot<double, float, float>((ozblasHandle_t *)hp, n, x, 1, y, 1);
+}
+
+double ref_dnrm2_f32(void *hp, int n, const double *x) {
+    return ozblasRnrm2<double, float, float>((ozblasHandle_t *)hp, n, x, 1);
+}
+
+int ref_dgemv_f32(void *hp, char ta, int m, int n, double alpha, const double *A, int lda, const double *x,
+                  double beta, double *y) {
+    return ozblasRgemv<double, float, float>((ozblasHandle_t *)hp, ta, m, n, alpha, A, lda, x, 1, beta, y, 1);
+}
+
 double ref_ddot(void *hp, int n, const double *x, const double *y) {
     return ozblasRdot<double, double, double>((ozblasHandle_t *)hp, n, x, 1, y, 1);
 }

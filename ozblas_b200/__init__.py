@@ -86,6 +86,10 @@ _dnrm2 = _sig("cuozblasDnrm2", [_HP, _i32, _vp, _i32, C.POINTER(_d)])
 _daxpy = _sig("cuozblasDaxpy", [_HP, _i32, _d, _vp, _i32, _vp, _i32])
 _dgemv = _sig("cuozblasDgemv", [_HP, _ch, _i32, _i32, _d, _vp, _i32, _vp, _i32, _d, _vp, _i32])
 _dgemm = _sig("cuozblasDgemm", [_HP, _ch, _ch, _i32, _i32, _i32, _d, _vp, _i32, _vp, _i32, _d, _vp, _i32])
+_dsgemm = _sig("cuozblasDSgemm", [_HP, _ch, _ch, _i32, _i32, _i32, _d, _vp, _i32, _vp, _i32, _d, _vp, _i32])
+_dsgemv = _sig("cuozblasDSgemv", [_HP, _ch, _i32, _i32, _d, _vp, _i32, _vp, _i32, _d, _vp, _i32])
+_dsdot = _sig("cuozblasDSdot", [_HP, _i32, _vp, _i32, _vp, _i32, C.POINTER(_d)])
+_dsnrm2 = _sig("cuozblasDSnrm2", [_HP, _i32, _vp, _i32, C.POINTER(_d)])
 _dgemm_i8 = _sig("cuozblasDgemmI8", [_HP, _ch, _ch, _i32, _i32, _i32, _d, _vp, _i32, _vp, _i32, _d, _vp, _i32])
 _dgemm_i8_static = _sig("cuozblasDgemmI8Static", [_ch, _ch, _i32, _i32, _i32, _d, _vp, _i32, _vp, _i32, _d, _vp,
                                                   _i32, _i32, _i32, _vp])
@@ -105,7 +109,7 @@ C_ABI_SYMBOLS = [
     "cuozblasHandleCreate", "cuozblasHandleDestroy", "cuozblasSetStream", "cuozblasGetLaunchCount", "cuozblasDdot", "cuozblasDnrm2",
     "cuozblasDaxpy", "cuozblasDgemv", "cuozblasDgemm", "cuozblasDcsrmv", "cuozblasDcsrmvSplitA", "cuozblasDcg",
     "cuozblasDgemmI8", "cuozblasDgemmI8Static", "cuozblasDgemmI8Batched", "cuozblasRuleTau", "cuozblasRuleRho",
-    "cuozblasRuleCrSum",
+    "cuozblasRuleCrSum", "cuozblasDSgemm", "cuozblasDSgemv", "cuozblasDSdot", "cuozblasDSnrm2",
     "cuozblasVersion",
 ]
 
@@ -174,6 +178,29 @@ class Handle:
 def dgemm(h, ta, tb, m, n, k, alpha, A, lda, B, ldb, beta, Cm, ldc):
     _chk("cuozblasDgemm", _dgemm(h.ref, ta.encode(), tb.encode(), m, n, k, alpha, _ptr(A), lda, _ptr(B), ldb,
                                  beta, _ptr(Cm), ldc))
+
+
+def dsgemm(h, ta, tb, m, n, k, alpha, A, lda, B, ldb, beta, Cm, ldc):
+    """Mixed form <double, float, float>: FP64 data, FP32 slices and slice products (FSum)."""
+    _chk("cuozblasDSgemm", _dsgemm(h.ref, ta.encode(), tb.encode(), m, n, k, alpha, _ptr(A), lda, _ptr(B), ldb,
+                                   beta, _ptr(Cm), ldc))
+
+
+def dsgemv(h, trans, m, n, alpha, A, lda, x, beta, y, incx=1, incy=1):
+    _chk("cuozblasDSgemv", _dsgemv(h.ref, trans.encode(), m, n, alpha, _ptr(A), lda, _ptr(x), incx, beta, _ptr(y),
+                                   incy))
+
+
+def dsdot(h, n, x, y, incx=1, incy=1) -> float:
+    r = _d()
+    _chk("cuozblasDSdot", _dsdot(h.ref, n, _ptr(x), incx, _ptr(y), incy, C.byref(r)))
+    return r.value
+
+
+def dsnrm2(h, n, x, incx=1) -> float:
+    r = _d()
+    _chk("cuozblasDSnrm2", _dsnrm2(h.ref, n, _ptr(x), incx, C.byref(r)))
+    return r.value
 
 
 def dgemm_i8(h, ta, tb, m, n, k, alpha, A, lda, B, ldb, beta, Cm, ldc):

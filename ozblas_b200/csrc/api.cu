@@ -260,6 +260,80 @@ int cuozblasDgemv(cuozblasHandle_t *h, char trans, int32_t m, int32_t n, double 
     return finish(h, t0);
 }
 
+// Mixed form <double, float, float>: FSum only (the reference's mixed-type
+// NearSum exits, src/cpu/ozblas_sum.cpp:273-296), no Dot2.
+static int check_flags_f32(cuozblasHandle_t *h) {
+    OZB_TRY(check_flags(h));
+    if (h->sumMode != 0) return CUOZBLAS_STATUS_NOT_SUPPORTED;
+    return CUOZBLAS_STATUS_SUCCESS;
+}
+
+int cuozblasDSgemm(cuozblasHandle_t *h, char transa, char transb, int32_t m, int32_t n, int32_t k, double alpha,
+                   const double *A, int32_t lda, const double *B, int32_t ldb, double beta, double *C, int32_t ldc) {
+    OZB_TRY(counter_init(h));
+    OZB_TRY(check_flags_f32(h));
+    if (m < 0 || n < 0 || k < 0 || ldc < (m > 1 ? m : 1)) return CUOZBLAS_STATUS_INVALID_VALUE;
+    if (h->reproMode == 0 && h->nSplitMax == 1) return CUOZBLAS_STATUS_NOT_SUPPORTED;
+    if (m == 0 || n == 0) return CUOZBLAS_STATUS_SUCCESS;
+    const double t0 = wall();
+    OZB_TRY(gemm_f32_core(h, transa, transb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, h->fastMode));
+    return finish(h, t0);
+}
+
+int cuozblasDSgemv(cuozblasHandle_t *h, char trans, int32_t m, int32_t n, double alpha, const double *A,
+                   int32_t lda, const double *x, int32_t incx, double beta, double *y, int32_t incy) {
+    OZB_TRY(counter_init(h));
+    OZB_TRY(check_flags_f32(h));
+    if (incx != 1 || incy != 1 || m < 0 || n < 0) return CUOZBLAS_STATUS_INVALID_VALUE;
+    if (h->reproMode == 0 && h->nSplitMax == 1) return CUOZBLAS_STATUS_NOT_SUPPORTED;
+    const double t0 = wall();
+    if (!is_trans(trans)) {  // src/cpu/ozblas_gemv.cpp:22-26
+        if (m == 0) return CUOZBLAS_STATUS_SUCCESS;
+        OZB_TRY(gemm_f32_core(h, 'n', 'n', m, 1, n, alpha, A, lda, x, n, beta, y, m, h->fastMode));
+    } else {
+        if (n == 0) return CUOZBLAS_STATUS_SUCCESS;
+        OZB_TRY(gemm_f32_core(h, 't', 'n', n, 1, m, alpha, A, lda, x, m, beta, y, n, h->fastMode));
+    }
+    return finish(h, t0);
+}
+
+// DOT of the mixed form: the GEMM with m = n = 1 (src/cpu/ozblas_dot.cpp:25),
+// into devWorkCommon[0], result to the host.
+static int dot_f32_impl(cuozblasHandle_t *h, int n, const double *x, const double *y, double *ret) {
+    State *st = state(h);
+    double *d = reinterpret_cast<double *>(h->devWorkCommon);
+    OZB_CHECK(cudaMemsetAsync(d, 0, sizeof(double), st->stream));
+    OZB_TRY(gemm_f32_core(h, 't', 'n', 1, 1, n, 1.0, x, n, y, n, 0.0, d, 1, 0));
+    OZB_CHECK(cudaMemcpyAsync(st->h_dbl, d, sizeof(double), cudaMemcpyDeviceToHost, st->stream));
+    OZB_CHECK(cudaStreamSynchronize(st->stream));
+    *ret = st->h_dbl[0];
+    return CUOZBLAS_STATUS_SUCCESS;
+}
+
+int cuozblasDSdot(cuozblasHandle_t *h, int32_t n, const double *x, int32_t incx, const double *y, int32_t incy,
+                  double *ret) {
+    OZB_TRY(counter_init(h));
+    OZB_TRY(check_flags_f32(h));
+    if (incx != 1 || incy != 1 || n < 0 || ret == nullptr) return CUOZBLAS_STATUS_INVALID_VALUE;
+    if (h->reproMode == 0 && h->nSplitMax == 1) return CUOZBLAS_STATUS_NOT_SUPPORTED;
+    const double t0 = wall();
+    OZB_TRY(dot_f32_impl(h, n, x, y, ret));
+    h->t_SplitVec_total += h->t_SplitA + h->t_SplitB;
+    return finish(h, t0);
+}
+
+int cuozblasDSnrm2(cuozblasHandle_t *h, int32_t n, const double *x, int32_t incx, double *ret) {
+    OZB_TRY(counter_init(h));
+    OZB_TRY(check_flags_f32(h));
+    if (incx != 1 || n < 0 || ret == nullptr) return CUOZBLAS_STATUS_INVALID_VALUE;
+    if (h->reproMode == 0 && h->nSplitMax == 1) return CUOZBLAS_STATUS_NOT_SUPPORTED;
+    const double t0 = wall();
+    double d = 0.0;
+    OZB_TRY(dot_f32_impl(h, n, x, x, &d));
+    *ret = sqrt(d);  // host sqrt, src/cpu/ozblas_nrm2.cpp:24-29
+    return finish(h, t0);
+}
+
 static int64_t splitA_ld(int nnz) { return ((int64_t)(nnz > 0 ? nnz : 1) + 31) / 32 * 32; }
 
 int cuozblasDcsrmv(cuozblasHandle_t *h, char trans, int32_t m, int32_t n, int32_t nnz, double alpha,

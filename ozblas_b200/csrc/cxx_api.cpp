@@ -68,6 +68,36 @@ int32_t cuozblasRgemm<double, int8_t, int32_t>(cuozblasHandle_t *oh, const char 
 }
 
 template <>
+int32_t cuozblasRnrm2<double, float, float>(cuozblasHandle_t *oh, const int32_t n, const double *devX,
+                                            const int32_t incx, double *ret) {
+    return report("cuozblasRnrm2<float>", cuozblasDSnrm2(oh, n, devX, incx, ret));
+}
+
+template <>
+int32_t cuozblasRdot<double, float, float>(cuozblasHandle_t *oh, const int32_t n, const double *devA,
+                                           const int32_t incx, const double *devB, const int32_t incy, double *ret) {
+    return report("cuozblasRdot<float>", cuozblasDSdot(oh, n, devA, incx, devB, incy, ret));
+}
+
+template <>
+int32_t cuozblasRgemv<double, float, float>(cuozblasHandle_t *oh, const char tranA, const int32_t m, const int32_t n,
+                                            const double alpha, const double *devA, const int32_t lda,
+                                            const double *devB, const int32_t incx, const double beta, double *devC,
+                                            const int32_t incy) {
+    return report("cuozblasRgemv<float>",
+                  cuozblasDSgemv(oh, tranA, m, n, alpha, devA, lda, devB, incx, beta, devC, incy));
+}
+
+template <>
+int32_t cuozblasRgemm<double, float, float>(cuozblasHandle_t *oh, const char tranA, const char tranB, const int32_t m,
+                                            const int32_t n, const int32_t k, const double alpha, const double *devA,
+                                            const int32_t lda, const double *devB, const int32_t ldb,
+                                            const double beta, double *devC, const int32_t ldc) {
+    return report("cuozblasRgemm<float>",
+                  cuozblasDSgemm(oh, tranA, tranB, m, n, k, alpha, devA, lda, devB, ldb, beta, devC, ldc));
+}
+
+template <>
 int32_t cuozblasRcsrmv<double, double>(cuozblasHandle_t *oh, const char tranA, const int32_t m, const int32_t n,
                                        const int32_t nnz, const double alpha, const cusparseMatDescr_t descrA,
                                        const double *devA, const int32_t *devAcolind, const int32_t *devArowptr,

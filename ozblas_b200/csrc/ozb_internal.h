@@ -119,6 +119,12 @@ int counter_init(cuozblasHandle_t *h);
 int split_lines_count(cuozblasHandle_t *h, int k, int nl, const double *X, int ldx, int rho, int maxS, int *ns);
 int split_lines_write(cuozblasHandle_t *h, int k, int nl, const double *X, int ldx, int rho, int ns, double *out,
                       int ldo);
+// Mixed form <double, float, float>: FP32 slices scalbn(slice, -tau) with tau
+// per level at exps[level * nl + line] (lines) or exps[level] (vector).
+int split_lines_write_f32(cuozblasHandle_t *h, int k, int nl, const double *X, int ldx, int rho, int ns, float *out,
+                          int ldo, short *exps);
+int split_vector_f32(cuozblasHandle_t *h, int n, const double *x, int rho, int maxS, float *out, int ldo, short *exps,
+                     int *ns);
 // Transpose rows x cols (column-major, ld) into cols x rows (ldo).
 int transpose(cuozblasHandle_t *h, int rows, int cols, const double *A, int lda, double *out, int ldo);
 // Vector split with one global tau chain (n-vector).  Writes ns slices of ldo.
@@ -132,6 +138,11 @@ int split_csr_write(cuozblasHandle_t *h, int m, int nnz, const double *val, cons
 // ---- sums ----
 int fsum_pairs_dot(cuozblasHandle_t *h, int nA, int nB, int maxlevel, const double *pairmat, double alpha,
                    double beta, double *out_dev);
+
+// ---- mixed form <double, float, float> (gemm_f32.cu) ----
+int rho_rule_f32(int dim, int splitEpsMode);
+int gemm_f32_core(cuozblasHandle_t *h, char ta, char tb, int m, int n, int k, double alpha, const double *A, int lda,
+                  const double *B, int ldb, double beta, double *C, int ldc, int fastMode);
 
 // ---- plain GEMM core (gemm_plain.cu) ----
 int gemm_plain_core(cuozblasHandle_t *h, char ta, char tb, int m, int n, int k, double alpha, const double *A,

@@ -21,13 +21,30 @@ namespace ozb {
 constexpr int kSplitThreads = 256;
 constexpr int kSplitSmemMaxK = 26 * 1024;  // doubles kept on chip per line (208 KB)
 
-// One CTA per line.  COUNT: atomicMax(*zmax, z_line).  WRITE: ns slices.
+// How a slice is stored.  Plain form: the FP64 slice itself.  Mixed form
+// <double, float, float> (src/cpu/ozblas_split.cpp:181-221): scalbn(slice,
+// -tau) in FP32, exact because a slice has at most 53 - rho <= 12 significant
+// bits on the grid 2^(rho + tau - 53), with tau kept per line and level.
+template <typename SL>
+__device__ __forceinline__ SL slice_store(double sl, int tau);
+template <>
+__device__ __forceinline__ double slice_store<double>(double sl, int) {
+    return sl;
+}
+template <>
+__device__ __forceinline__ float slice_store<float>(double sl, int tau) {
+    return (float)scalbn(sl, -tau);
+}
+
+// One CTA per line.  COUNT: atomicMax(*zmax, z_line).  WRITE: ns slices
+// (and, for FP32 slices, tau of every level at exps[level * nl + line]).
 // `rem` is either dynamic shared memory (k <= kSplitSmemMaxK) or a global
 // scratch line of k doubles per CTA.
-template <bool WRITE>
+template <bool WRITE, typename SL = double>
 __global__ void __launch_bounds__(kSplitThreads) k_split_lines(int k, int nl, const double *__restrict__ X, int ldx,
-                                                               int rho, int levels, double *__restrict__ out,
-                                                               int ldo, double *__restrict__ gscratch,
+                                                               int rho, int levels, SL *__restrict__ out, int ldo,
+                                                               short *__restrict__ exps,
+                                                               double *__restrict__ gscratch,
                                                                int *__restrict__ zmax) {
     extern __shared__ double smem[];
     __shared__ double red[kSplitThreads / 32];
@@ -44,19 +61,21 @@ __global__ void __launch_bounds__(kSplitThreads) k_split_lines(int k, int nl, co
     mx = block_max_nonneg(mx, red);
     int z = levels;  // COUNT: first level leaving a zero remainder (levels = maxS-1 cap)
     for (int s = 0; s < levels; s++) {
-        const double sigma = dense_sigma(rho, mx, 1);
+        const int tau = tau_rule(mx);
+        const double sigma = 0.75 * pow2(rho + tau);  // dense_sigma(rho, mx, 1)
         double nm = 0.0;
-        double *o = WRITE ? out + ((size_t)s * nl + line) * ldo : nullptr;
+        SL *o = WRITE ? out + ((size_t)s * nl + line) * ldo : nullptr;
+        if (WRITE && exps && threadIdx.x == 0) exps[(size_t)s * nl + line] = (short)tau;
         for (int i = threadIdx.x; i < k; i += blockDim.x) {
             double r = rem[i];
             const double sl = (r + sigma) - sigma;
             r = r - sl;
             rem[i] = r;
             nm = ref_max(nm, fabs(r));
-            if (WRITE) o[i] = sl;
+            if (WRITE) o[i] = slice_store<SL>(sl, tau);
         }
         if (WRITE)
-            for (int i = k + threadIdx.x; i < ldo; i += blockDim.x) o[i] = 0.0;
+            for (int i = k + threadIdx.x; i < ldo; i += blockDim.x) o[i] = (SL)0;
         mx = block_max_nonneg(nm, red);
         if (!WRITE && mx == 0.0) {
             z = s;
@@ -66,8 +85,9 @@ __global__ void __launch_bounds__(kSplitThreads) k_split_lines(int k, int nl, co
     if (!WRITE && threadIdx.x == 0) atomicMax(zmax, z);
 }
 
+template <typename SL>
 static int launch_split_lines(cuozblasHandle_t *h, bool write, int k, int nl, const double *X, int ldx, int rho,
-                              int levels, double *out, int ldo, int *zmax_dev) {
+                              int levels, SL *out, int ldo, short *exps, int *zmax_dev) {
     State *st = state(h);
     double *gscratch = nullptr;
     size_t smem = 0;
@@ -80,17 +100,17 @@ static int launch_split_lines(cuozblasHandle_t *h, bool write, int k, int nl, co
         smem = sizeof(double) * (size_t)(k > 0 ? k : 1);
     }
     if (write) {
-        OZB_CHECK(cudaFuncSetAttribute(k_split_lines<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        OZB_CHECK(cudaFuncSetAttribute(k_split_lines<true, SL>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)(kSplitSmemMaxK * sizeof(double))));
         counted(h);
-        k_split_lines<true><<<nl, kSplitThreads, smem, st->stream>>>(k, nl, X, ldx, rho, levels, out, ldo, gscratch,
-                                                                     nullptr);
+        k_split_lines<true, SL><<<nl, kSplitThreads, smem, st->stream>>>(k, nl, X, ldx, rho, levels, out, ldo, exps,
+                                                                         gscratch, nullptr);
     } else {
-        OZB_CHECK(cudaFuncSetAttribute(k_split_lines<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        OZB_CHECK(cudaFuncSetAttribute(k_split_lines<false, double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)(kSplitSmemMaxK * sizeof(double))));
         counted(h);
-        k_split_lines<false><<<nl, kSplitThreads, smem, st->stream>>>(k, nl, X, ldx, rho, levels, nullptr, 0,
-                                                                      gscratch, zmax_dev);
+        k_split_lines<false, double><<<nl, kSplitThreads, smem, st->stream>>>(k, nl, X, ldx, rho, levels, nullptr, 0,
+                                                                      nullptr, gscratch, zmax_dev);
     }
     OZB_CHECK(cudaGetLastError());
     ar.release(mk);
@@ -105,7 +125,7 @@ int split_lines_count(cuozblasHandle_t *h, int k, int nl, const double *X, int l
         return CUOZBLAS_STATUS_SUCCESS;
     }
     OZB_CHECK(cudaMemsetAsync(st->d_ints, 0, sizeof(int), st->stream));
-    OZB_TRY(launch_split_lines(h, false, k, nl, X, ldx, rho, maxS - 1, nullptr, 0, st->d_ints));
+    OZB_TRY(launch_split_lines<double>(h, false, k, nl, X, ldx, rho, maxS - 1, nullptr, 0, nullptr, st->d_ints));
     OZB_CHECK(cudaMemcpyAsync(st->h_ints, st->d_ints, sizeof(int), cudaMemcpyDeviceToHost, st->stream));
     OZB_CHECK(cudaStreamSynchronize(st->stream));
     int zmax = st->h_ints[0];
@@ -117,7 +137,13 @@ int split_lines_count(cuozblasHandle_t *h, int k, int nl, const double *X, int l
 int split_lines_write(cuozblasHandle_t *h, int k, int nl, const double *X, int ldx, int rho, int ns, double *out,
                       int ldo) {
     if (nl == 0 || ns == 0) return CUOZBLAS_STATUS_SUCCESS;
-    return launch_split_lines(h, true, k, nl, X, ldx, rho, ns, out, ldo, nullptr);
+    return launch_split_lines<double>(h, true, k, nl, X, ldx, rho, ns, out, ldo, nullptr, nullptr);
+}
+
+int split_lines_write_f32(cuozblasHandle_t *h, int k, int nl, const double *X, int ldx, int rho, int ns, float *out,
+                          int ldo, short *exps) {
+    if (nl == 0 || ns == 0) return CUOZBLAS_STATUS_SUCCESS;
+    return launch_split_lines<float>(h, true, k, nl, X, ldx, rho, ns, out, ldo, exps, nullptr);
 }
 
 // ---------------------------------------------------------------------------
@@ -152,11 +178,13 @@ int transpose(cuozblasHandle_t *h, int rows, int cols, const double *A, int lda,
 // driver :254-289 with n = 1).  One cooperative launch runs every level; the
 // grid syncs after each level's max reduction.  rem: n doubles of scratch.
 // slot[s] = max|remainder| entering level s (slot[0] = max|x|); *ns_out is
-// written by block 0.
+// written by block 0, and for FP32 slices exps[s] = tau of level s.
 // ---------------------------------------------------------------------------
+template <typename SL>
 __global__ void __launch_bounds__(256) k_split_vector(int n, const double *__restrict__ x, int rho, int maxS,
-                                                      double *__restrict__ out, int ldo, double *__restrict__ rem,
-                                                      double *__restrict__ slot, int *__restrict__ ns_out) {
+                                                      SL *__restrict__ out, int ldo, short *__restrict__ exps,
+                                                      double *__restrict__ rem, double *__restrict__ slot,
+                                                      int *__restrict__ ns_out) {
     cg::grid_group grid = cg::this_grid();
     __shared__ double red[8];
     const size_t tid = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -170,19 +198,21 @@ __global__ void __launch_bounds__(256) k_split_vector(int n, const double *__res
     for (; s < maxS; s++) {
         const double mx = slot[s];
         if (s >= 2 && slot[s] == 0.0) break;  // previous level left nothing: the count is s
-        const double sigma = dense_sigma(rho, mx, 1);
+        const int tau = tau_rule(mx);
+        const double sigma = 0.75 * pow2(rho + tau);  // dense_sigma(rho, mx, 1)
         const double *src = (s == 0) ? x : rem;
-        double *o = out + (size_t)s * ldo;
+        SL *o = out + (size_t)s * ldo;
+        if (exps && tid == 0) exps[s] = (short)tau;
         double nm = 0.0;
         for (size_t i = tid; i < (size_t)n; i += stride) {
             double r = src[i];
             const double sl = (r + sigma) - sigma;
             r = r - sl;
             rem[i] = r;
-            o[i] = sl;
+            o[i] = slice_store<SL>(sl, tau);
             nm = ref_max(nm, fabs(r));
         }
-        for (size_t i = (size_t)n + tid; i < (size_t)ldo; i += stride) o[i] = 0.0;
+        for (size_t i = (size_t)n + tid; i < (size_t)ldo; i += stride) o[i] = (SL)0;
         nm = block_max_nonneg(nm, red);
         if (threadIdx.x == 0) atomic_max_nonneg(&slot[s + 1], nm);
         grid.sync();
@@ -190,7 +220,9 @@ __global__ void __launch_bounds__(256) k_split_vector(int n, const double *__res
     if (blockIdx.x == 0 && threadIdx.x == 0) *ns_out = s;
 }
 
-int split_vector(cuozblasHandle_t *h, int n, const double *x, int rho, int maxS, double *out, int ldo, int *ns) {
+template <typename SL>
+static int split_vector_t(cuozblasHandle_t *h, int n, const double *x, int rho, int maxS, SL *out, int ldo,
+                          short *exps, int *ns) {
     State *st = state(h);
     Arena ar(h);
     const uint64_t mk = ar.mark();
@@ -201,19 +233,28 @@ int split_vector(cuozblasHandle_t *h, int n, const double *x, int rho, int maxS,
     int dev = 0, nsm = 0, per = 0;
     OZB_CHECK(cudaGetDevice(&dev));
     OZB_CHECK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
-    OZB_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_split_vector, 256, 0));
+    OZB_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_split_vector<SL>, 256, 0));
     int blocks = nsm * (per < 4 ? per : 4);
     const int need = (n + 255) / 256;
     if (blocks > need) blocks = need > 0 ? need : 1;
     int *ns_dev = st->d_ints;
-    void *args[] = {&n, &x, &rho, &maxS, &out, &ldo, &rem, &slot, &ns_dev};
+    void *args[] = {&n, &x, &rho, &maxS, &out, &ldo, &exps, &rem, &slot, &ns_dev};
     counted(h);
-    OZB_CHECK(cudaLaunchCooperativeKernel((void *)k_split_vector, dim3(blocks), dim3(256), args, 0, st->stream));
+    OZB_CHECK(cudaLaunchCooperativeKernel((void *)k_split_vector<SL>, dim3(blocks), dim3(256), args, 0, st->stream));
     OZB_CHECK(cudaMemcpyAsync(st->h_ints, ns_dev, sizeof(int), cudaMemcpyDeviceToHost, st->stream));
     OZB_CHECK(cudaStreamSynchronize(st->stream));
     *ns = st->h_ints[0];
     ar.release(mk);
     return CUOZBLAS_STATUS_SUCCESS;
+}
+
+int split_vector(cuozblasHandle_t *h, int n, const double *x, int rho, int maxS, double *out, int ldo, int *ns) {
+    return split_vector_t<double>(h, n, x, rho, maxS, out, ldo, nullptr, ns);
+}
+
+int split_vector_f32(cuozblasHandle_t *h, int n, const double *x, int rho, int maxS, float *out, int ldo, short *exps,
+                     int *ns) {
+    return split_vector_t<float>(h, n, x, rho, maxS, out, ldo, exps, ns);
 }
 
 // ---------------------------------------------------------------------------

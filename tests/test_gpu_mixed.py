@@ -1,0 +1,158 @@
+"""Mixed form <double, float, float> on the GPU vs the CPU oracle: bit-exact.
+
+FP64 data, FP32 slices (scalbn(slice, -tau) with tau per line and level),
+exact FP32 slice products and the scaled FSum (src/cpu/ozblas_gemm.cpp with
+TYPE2 = TYPE3 = float, src/cpu/ozblas_sum.cpp:382-432).  The oracle's
+restatement of this form is pinned to ozblasRgemm/Rgemv/Rdot/Rnrm2<double,
+float, float> of the reference library by tests/test_oracle.py.  Every call
+goes through the C ABI (cuozblasDSgemm / DSgemv / DSdot / DSnrm2).
+"""
+import numpy as np
+import pytest
+
+from oracle.oracle import make_flags
+from tests.conftest import bits_equal, first_diff
+
+pytestmark = pytest.mark.gpu
+
+
+def dev(torch, a):
+    return torch.from_numpy(np.ascontiguousarray(a)).cuda()
+
+
+def host(t):
+    return t.cpu().numpy()
+
+
+CASES = [
+    # m, n, k, ta, tb, fastMode, nSplitMax, alpha, beta, phi
+    (1, 2, 1, "n", "n", 0, 0, 1.0, 0.0, 1.0),
+    (2, 3, 7, "n", "n", 0, 0, 1.0, 0.0, 1.0),
+    (33, 17, 100, "n", "n", 0, 0, 1.0, 0.0, 1.0),
+    (33, 17, 100, "t", "n", 1, 0, 1.0, 0.0, 1.0),
+    (7, 9, 130, "n", "t", 0, 0, -0.5, 2.0, 1.0),
+    (20, 20, 64, "t", "t", 2, 0, 1.0, 1.0, 2.0),
+    (130, 260, 300, "n", "n", 0, 0, 1.5, -1.0, 2.0),
+    (129, 127, 33, "t", "t", 0, 3, 1.0, 0.0, 4.0),
+    (64, 64, 1, "n", "n", 0, 0, 1.0, 0.0, 0.5),
+    (256, 200, 600, "n", "t", 0, 0, 1.0, 0.5, 1.0),
+    (40, 300, 2000, "t", "n", 1, 0, 1.0, 0.0, 1.0),
+]
+
+
+@pytest.mark.parametrize("case", CASES, ids=lambda c: "x".join(map(str, c[:3])) + f"-{c[3]}{c[4]}-f{c[5]}s{c[6]}")
+def test_dsgemm(case, oracle, handle, ozb, cuda):
+    m, n, k, ta, tb, fm, ns, alpha, beta, phi = case
+    ar, ac = (m, k) if ta == "n" else (k, m)
+    br, bc = (k, n) if tb == "n" else (n, k)
+    A = oracle.phi_matrix(ar, ac, phi, 1)
+    B = oracle.phi_matrix(br, bc, phi, 2)
+    C0 = oracle.phi_matrix(m, n, 1.0, 3)
+    ref, info = oracle.dgemm_f32(make_flags(fastMode=fm, nSplitMax=ns), ta, tb, m, n, k, alpha, A, ar, B, br, beta,
+                                 C0, m)
+    handle.fastMode, handle.nSplitMax = fm, ns
+    dC = dev(cuda, C0)
+    ozb.dsgemm(handle, ta, tb, m, n, k, alpha, dev(cuda, A), ar, dev(cuda, B), br, beta, dC, m)
+    out = host(dC)
+    assert bits_equal(out, ref), first_diff(out, ref)
+    assert (handle.nSplitA, handle.nSplitB, handle.nSplitC) == (info.nSplitA, info.nSplitB, info.nSplitC)
+
+
+def test_dsgemm_run_to_run_identical(oracle, handle, ozb, cuda):
+    m, n, k = 300, 200, 256
+    A = oracle.phi_matrix(m, k, 1.0, 1)
+    B = oracle.phi_matrix(k, n, 1.0, 2)
+    dA, dB = dev(cuda, A), dev(cuda, B)
+    outs = []
+    for _ in range(3):
+        dC = cuda.zeros((n, m), dtype=cuda.float64, device="cuda")
+        ozb.dsgemm(handle, "n", "n", m, n, k, 1.0, dA, m, dB, k, 0.0, dC, m)
+        outs.append(host(dC))
+    assert bits_equal(outs[0], outs[1]) and bits_equal(outs[0], outs[2])
+    ref, _ = oracle.dgemm_f32(make_flags(), "n", "n", m, n, k, 1.0, A, m, B, k, 0.0, np.zeros((n, m)), m)
+    assert bits_equal(outs[0], ref), first_diff(outs[0], ref)
+
+
+@pytest.mark.parametrize("n,phi", [(1, 1.0), (7, 1.0), (1000, 2.0), (100003, 2.0), (1 << 20, 1.0)])
+def test_dsdot_dsnrm2(n, phi, oracle, handle, ozb, cuda):
+    x = oracle.phi_vector(n, phi, 1)
+    y = oracle.phi_vector(n, phi, 2)
+    d = ozb.dsdot(handle, n, dev(cuda, x), dev(cuda, y))
+    r, info = oracle.dgemm_f32(make_flags(), "t", "n", 1, 1, n, 1.0, x, n, y, n, 0.0, np.zeros(1), 1)
+    assert bits_equal(np.array([d]), r), (d, r[0])
+    assert (handle.nSplitA, handle.nSplitB, handle.nSplitC) == (info.nSplitA, info.nSplitB, 1.0)
+    nr = ozb.dsnrm2(handle, n, dev(cuda, x))
+    r2, _ = oracle.dgemm_f32(make_flags(), "t", "n", 1, 1, n, 1.0, x, n, x, n, 0.0, np.zeros(1), 1)
+    assert bits_equal(np.array([nr]), np.sqrt(r2)), (nr, np.sqrt(r2[0]))
+
+
+@pytest.mark.parametrize("m,n,trans,fm", [(50, 70, "n", 0), (50, 70, "t", 0), (300, 257, "n", 1), (1, 33, "t", 0),
+                                           (700, 2000, "t", 2)])
+def test_dsgemv(m, n, trans, fm, oracle, handle, ozb, cuda):
+    A = oracle.phi_matrix(m, n, 2.0, 1)
+    xl, yl = (n, m) if trans == "n" else (m, n)
+    x = oracle.phi_vector(xl, 2.0, 2)
+    y0 = oracle.phi_vector(yl, 1.0, 3)
+    f = make_flags(fastMode=fm)
+    if trans == "n":
+        ref, info = oracle.dgemm_f32(f, "n", "n", m, 1, n, 0.75, A, m, x, n, 0.5, y0, m)
+    else:
+        ref, info = oracle.dgemm_f32(f, "t", "n", n, 1, m, 0.75, A, m, x, m, 0.5, y0, n)
+    handle.fastMode = fm
+    dy = dev(cuda, y0)
+    ozb.dsgemv(handle, trans, m, n, 0.75, dev(cuda, A), m, dev(cuda, x), 0.5, dy)
+    assert bits_equal(host(dy), ref), first_diff(host(dy), ref)
+    assert (handle.nSplitA, handle.nSplitB, handle.nSplitC) == (info.nSplitA, info.nSplitB, info.nSplitC)
+
+
+@pytest.mark.parametrize("scale", [2.0 ** -1060, 2.0 ** -540, 2.0 ** 900])
+def test_mixed_extreme_magnitudes(scale, oracle, handle, ozb, cuda):
+    """Products scaled into the subnormal range (scalbn rounds once there) and near overflow."""
+    m, n, k = 45, 37, 200
+    A = oracle.phi_matrix(m, k, 1.0, 1) * scale
+    B = oracle.phi_matrix(k, n, 1.0, 2)
+    ref, _ = oracle.dgemm_f32(make_flags(), "n", "n", m, n, k, 1.0, A, m, B, k, 0.0, np.zeros((n, m)), m)
+    dC = cuda.zeros((n, m), dtype=cuda.float64, device="cuda")
+    ozb.dsgemm(handle, "n", "n", m, n, k, 1.0, dev(cuda, A), m, dev(cuda, B), k, 0.0, dC, m)
+    assert bits_equal(host(dC), ref), first_diff(host(dC), ref)
+    x = oracle.phi_vector(5000, 1.0, 4) * scale
+    y = oracle.phi_vector(5000, 1.0, 5)
+    d = ozb.dsdot(handle, 5000, dev(cuda, x), dev(cuda, y))
+    r, _ = oracle.dgemm_f32(make_flags(), "t", "n", 1, 1, 5000, 1.0, x, 5000, y, 5000, 0.0, np.zeros(1), 1)
+    assert bits_equal(np.array([d]), r), (d, r[0])
+
+
+def test_mixed_zero_and_special_lines(oracle, handle, ozb, cuda):
+    """Zero rows / columns (tau of a zero line) and an all-zero operand."""
+    m, n, k = 70, 50, 96
+    A = oracle.phi_matrix(m, k, 2.0, 1)
+    B = oracle.phi_matrix(k, n, 2.0, 2)
+    A.reshape(k, m)[:, 5] = 0.0    # row 5 of A
+    B.reshape(n, k)[7, :] = 0.0    # column 7 of B
+    C0 = oracle.phi_matrix(m, n, 1.0, 3)
+    for a in (A, np.zeros_like(A)):
+        ref, info = oracle.dgemm_f32(make_flags(), "n", "n", m, n, k, 1.0, a, m, B, k, -1.0, C0, m)
+        dC = dev(cuda, C0)
+        ozb.dsgemm(handle, "n", "n", m, n, k, 1.0, dev(cuda, a), m, dev(cuda, B), k, -1.0, dC, m)
+        assert bits_equal(host(dC), ref), first_diff(host(dC), ref)
+        assert (handle.nSplitA, handle.nSplitB) == (info.nSplitA, info.nSplitB)
+
+
+def test_mixed_unsupported_flags(handle, ozb, cuda):
+    """NearSum (sumMode 1) and Dot2 do not exist for mixed types in the reference."""
+    x = cuda.zeros(8, dtype=cuda.float64, device="cuda")
+    handle.sumMode = 1
+    with pytest.raises(ozb.OzblasError) as e:
+        ozb.dsgemm(handle, "n", "n", 2, 2, 2, 1.0, x, 2, x, 2, 0.0, x, 2)
+    assert e.value.code == 4
+    with pytest.raises(ozb.OzblasError) as e:
+        ozb.dsdot(handle, 8, x, x)
+    assert e.value.code == 4
+    handle.sumMode, handle.splitEpsMode = 0, 2
+    with pytest.raises(ozb.OzblasError) as e:
+        ozb.dsdot(handle, 8, x, x)
+    assert e.value.code == 4
+    handle.splitEpsMode = 0
+    with pytest.raises(ozb.OzblasError) as e:
+        ozb.dsdot(handle, 8, x, x, incx=2)
+    assert e.value.code == 2

@@ -295,7 +295,13 @@ def test_ddot_tensor_core_pass_edges(case, oracle, handle, ozb, cuda):
         yy = x if case == "same_vector" else y
         d = ozb.ddot(handle, n, dx, dy)
         r, info = oracle.ddot(make_flags(sumMode=sm), x, yy)
-        assert np.float64(d).view(np.int64) == np.float64(r).view(np.int64), (case, sm, d, r)
+        if case == "nan_inf":
+            # IEEE 754 leaves the sign and payload of a NaN result open: x86 makes inf - inf a
+            # negative NaN and keeps an input NaN's sign, and which one survives depends on the
+            # order of the additions.  The result must be a NaN; its bits are not compared.
+            assert np.isnan(d) and np.isnan(r), (sm, d, r)
+        else:
+            assert np.float64(d).view(np.int64) == np.float64(r).view(np.int64), (case, sm, d, r)
         assert (handle.nSplitA, handle.nSplitB) == (info.nSplitA, info.nSplitB)
 
 

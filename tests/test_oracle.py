@@ -172,6 +172,78 @@ def test_dot2_csrmv_vs_reference(sm, oracle, reference):
         assert [info.nSplitA, info.nSplitB, info.nSplitC] == [inf["nSplitA"], inf["nSplitB"], inf["nSplitC"]]
 
 
+@pytest.mark.parametrize("seed", range(10))
+def test_mixed_f32_gemm_vs_reference(seed, oracle, reference):
+    """<double, float, float> (FP32 slices with per-line exponents, exact FP32 products, scaled FSum):
+    the restatement against ozblasRgemm<double, float, float>, bit-exact with the split counts."""
+    rng = np.random.default_rng(300 + seed)
+    m, n = (int(v) for v in rng.integers(1, 60, 2))
+    k = int(rng.integers(1, 500))
+    if seed == 0:
+        m = n = 1
+    if seed in (1, 2):
+        n = 1
+    ta, tb = rng.choice(["n", "t"]), rng.choice(["n", "t"])
+    fm = int(rng.integers(0, 3)) if seed != 2 else 0
+    nsplit = int(rng.choice([0, 0, 2, 5]))
+    phi = float(rng.choice([0.5, 1.0, 2.0, 4.0]))
+    case = (m, n, k, ta, tb, 0, fm, 1.25, -0.5, phi)
+    A, B, C0, lda, ldb = gemm_inputs(oracle, case)
+    out, info = oracle.dgemm_f32(make_flags(fastMode=fm, nSplitMax=nsplit), ta, tb, m, n, k, 1.25, A, lda, B, ldb,
+                                 -0.5, C0, m)
+    reference.set_flags(fastMode=fm, nSplitMax=nsplit)
+    gold = reference.dgemm_f32(ta, tb, m, n, k, 1.25, A, lda, B, ldb, -0.5, C0, m)
+    assert bits_equal(out, gold), (case, nsplit, first_diff(out, gold))
+    inf = reference.info()
+    assert [info.nSplitA, info.nSplitB, info.nSplitC] == [inf["nSplitA"], inf["nSplitB"], inf["nSplitC"]]
+
+
+def test_mixed_f32_skinny_vs_reference(oracle, reference):
+    """The mixed DOT, NRM2 and GEMV are the mixed GEMM with m = n = 1 / n = 1
+    (src/cpu/ozblas_dot.cpp:25, ozblas_nrm2.cpp:22-29, ozblas_gemv.cpp:22-26); long vectors and
+    tiny / huge magnitudes included."""
+    reference.set_flags()
+    f = make_flags()
+    for n, phi, scale in ((1, 1.0, 1.0), (1000, 2.0, 1.0), (100003, 1.0, 1.0), (5000, 4.0, 2.0 ** -1000),
+                          (5000, 1.0, 2.0 ** 900), (3000, 1.0, 2.0 ** -1060)):
+        x = oracle.phi_vector(n, phi, 1) * scale
+        y = oracle.phi_vector(n, phi, 2)
+        r, _ = oracle.dgemm_f32(f, "t", "n", 1, 1, n, 1.0, x, n, y, n, 0.0, np.zeros(1), 1)
+        gold = reference.ddot_f32(x, y)
+        assert bits_equal(r, np.array([gold])), (n, phi, scale, r[0], gold)
+        r2, _ = oracle.dgemm_f32(f, "t", "n", 1, 1, n, 1.0, x, n, x, n, 0.0, np.zeros(1), 1)
+        assert bits_equal(np.sqrt(r2), np.array([reference.dnrm2_f32(x)]))
+    for ta, (m, n) in (("n", (70, 300)), ("t", (300, 70))):
+        A = oracle.phi_matrix(m, n, 2.0, 3)
+        xl = n if ta == "n" else m
+        yl = m if ta == "n" else n
+        x = oracle.phi_vector(xl, 2.0, 4)
+        y0 = oracle.phi_vector(yl, 1.0, 5)
+        if ta == "n":
+            out, _ = oracle.dgemm_f32(f, "n", "n", m, 1, n, 0.75, A, m, x, n, 1.5, y0, m)
+        else:
+            out, _ = oracle.dgemm_f32(f, "t", "n", n, 1, m, 0.75, A, m, x, m, 1.5, y0, n)
+        gold = reference.dgemv_f32(ta, m, n, 0.75, A, m, x, 1.5, y0)
+        assert bits_equal(out, gold), (ta, first_diff(out, gold))
+
+
+def test_mixed_f32_split_exactness(oracle):
+    """Every FP32 slice is scalbn(FP64 slice, -tau) exactly: at most 53 - rho significant bits, so
+    a k-term slice product stays within FP32's 24 bits."""
+    for k in (1, 7, 64, 1000, 4096, 1 << 20):
+        rho = oracle.rho_f32(k)
+        assert 2 * (53 - rho) + np.log2(k) <= 24 + 1e-9, (k, rho)
+    x = oracle.phi_matrix(40, 3, 4.0, 9).reshape(3, 40)
+    ns, sl, ex = oracle.split_cols_f32(make_flags(), x)
+    ns64, sl64 = oracle.split_cols(make_flags(), x)
+    # FP64 slices differ (rho differs); the FP32 ones rebuild the input exactly
+    rec = np.zeros_like(x)
+    for s in range(ns):
+        rec += np.ldexp(sl[s].astype(np.float64), ex[s][:, None].astype(np.int64))
+    assert np.array_equal(rec, x)
+    assert ns > ns64
+
+
 def test_split_slices_vs_reference(oracle, reference):
     """Slice-level parity of the column-panel and CSR splits."""
     for phi, k, ncol in [(1.0, 100, 7), (4.0, 333, 5), (2.0, 1, 3), (1.0, 64, 1)]:
