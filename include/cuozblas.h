@@ -134,8 +134,8 @@ template <typename TYPE1, typename TYPE2>
 int32_t cuozblasRcg(cuozblasHandle_t *oh, const char tranA, const int32_t dimN, const int32_t dimNNZ,
                     const cusparseMatDescr_t descrA, const TYPE1 *matA, const int32_t *matAcolind,
                     const int32_t *matArowptr, const TYPE1 *vecB, TYPE1 *vecX, int32_t maxiter, TYPE1 tol);
-/* Exported instantiations: <double,double,double> and <double,float,float>
- * for nrm2/dot/gemv/gemm,
+/* Exported instantiations: <double,double,double>, <double,float,float> and
+ * <float,double,double> for nrm2/dot/gemv/gemm,
  * <double> for axpy, <double,double> for csrmv/csrmvSplitA/cg, and the INT8
  * precision form cuozblasRgemm<double,int8_t,int32_t> (the instantiation
  * the reference leaves commented out at src/cuda/cuozblas_gemm.cu:292). */
@@ -199,6 +199,21 @@ int cuozblasDSdot(cuozblasHandle_t *h, int32_t n, const double *x, int32_t incx,
                   double *ret);
 int cuozblasDSnrm2(cuozblasHandle_t *h, int32_t n, const double *x, int32_t incx, double *ret);
 
+/* Mixed form <float,double,double> (include/cuozblas.h:75-77 instantiated at
+ * src/cuda/cuozblas_gemm.cu:290 and the DOT/NRM2/GEMV files): float data and
+ * results with FP64 slices and exact FP64 slice products, bit-exact to the
+ * reference CPU path (src/cpu/ozblas_gemm.cpp with TYPE1 = float).  The split
+ * runs in float arithmetic; each pair product is rounded to float, scaled in
+ * float and summed in float.  sumMode 0 only, no Dot2.  *ret of SDdot/SDnrm2
+ * is a host pointer. */
+int cuozblasSDgemm(cuozblasHandle_t *h, char transa, char transb, int32_t m, int32_t n, int32_t k, float alpha,
+                   const float *A, int32_t lda, const float *B, int32_t ldb, float beta, float *C, int32_t ldc);
+int cuozblasSDgemv(cuozblasHandle_t *h, char trans, int32_t m, int32_t n, float alpha, const float *A, int32_t lda,
+                   const float *x, int32_t incx, float beta, float *y, int32_t incy);
+int cuozblasSDdot(cuozblasHandle_t *h, int32_t n, const float *x, int32_t incx, const float *y, int32_t incy,
+                  float *ret);
+int cuozblasSDnrm2(cuozblasHandle_t *h, int32_t n, const float *x, int32_t incx, float *ret);
+
 /* INT8 precision form (no reference implementation; the reference stubs it
  * at src/cuda/cuozblas_gemm.cu:292 and src/cuda/cuozblas_blas_wrapper.cu:147-208):
  * INT8 slices on tcgen05 tensor cores with INT32 accumulation.
@@ -240,6 +255,8 @@ int cuozblasDgemmI8Static(char transa, char transb, int32_t m, int32_t n, int32_
 
 /* Rule checks exported for the host-side tests (same code the kernels use). */
 int cuozblasRuleTau(double v);
+/* tau of float data for the <float,double,double> form: (short)ceil((float)log2((double)v)) */
+int cuozblasRuleTauF32(float v);
 int cuozblasRuleRho(int32_t dim, int32_t splitEpsMode);
 /* Certified fast path of the correctly rounded sum (the NearSum result when it
  * returns 1; 0: not proven, the library then runs NearSum itself). */

@@ -30,6 +30,10 @@ def _d(a):
     return a.ctypes.data_as(_dp)
 
 
+def _f(a):
+    return a.ctypes.data_as(C.POINTER(C.c_float))
+
+
 def _i(a):
     return a.ctypes.data_as(_ip)
 
@@ -90,6 +94,19 @@ class Restatement:
         L.oz_dgemm_f32.restype = C.c_int
         L.oz_dgemm_f32.argtypes = [F, C.c_char, C.c_char, C.c_int, C.c_int, C.c_int, C.c_double, _dp, C.c_int,
                                    _dp, C.c_int, C.c_double, _dp, C.c_int, I]
+        _fp = C.POINTER(C.c_float)
+        L.oz_rho_sd.restype = C.c_int
+        L.oz_rho_sd.argtypes = [C.c_int, C.c_int]
+        L.oz_tau_sd_libm.restype = C.c_short
+        L.oz_tau_sd_libm.argtypes = [C.c_float]
+        L.oz_tau_sd_sweep.restype = C.c_long
+        L.oz_tau_sd_sweep.argtypes = [C.c_void_p, C.c_uint, C.POINTER(C.c_uint)]
+        L.oz_split_cols_sd.restype = C.c_int
+        L.oz_split_cols_sd.argtypes = [F, C.c_int, C.c_int, _fp, C.c_int, C.c_int, _dp, C.c_int,
+                                       C.POINTER(C.c_short)]
+        L.oz_sgemm_d.restype = C.c_int
+        L.oz_sgemm_d.argtypes = [F, C.c_char, C.c_char, C.c_int, C.c_int, C.c_int, C.c_float, _fp, C.c_int, _fp,
+                                 C.c_int, C.c_float, _fp, C.c_int, I]
         L.oz_split_rows_csr.restype = C.c_int
         L.oz_split_rows_csr.argtypes = [F, C.c_int, _dp, _ip, C.c_int, _dp, C.c_int]
         L.oz_nearsum.restype = C.c_double
@@ -203,6 +220,39 @@ class Restatement:
                                 beta, _d(Cc), ldc, C.byref(info))
         return (Cc, info) if r == 0 else (None, None)
 
+    def rho_sd(self, dim, mode=0):
+        return self.L.oz_rho_sd(dim, mode)
+
+    def tau_sd_libm(self, v):
+        return self.L.oz_tau_sd_libm(v)
+
+    def tau_sd_sweep(self, rule_fn_addr, stride):
+        """Disagreements of a C rule int(float) with the reference's float tau over strided float bits."""
+        first = C.c_uint(0)
+        bad = self.L.oz_tau_sd_sweep(rule_fn_addr, stride, C.byref(first))
+        return bad, first.value
+
+    def split_cols_sd(self, flags, X, shift=1):
+        """<float, double, double>: (nsplit, double slices[nsplit, ncol, k], short exps[nsplit, ncol])."""
+        X = np.ascontiguousarray(X, dtype=np.float32)
+        ncol, k = X.shape
+        maxS = flags.nSplitMax if flags.nSplitMax > 0 else 30
+        out = np.zeros((maxS + 1, ncol, max(k, 1)), dtype=np.float64)
+        ex = np.zeros((maxS + 1, max(ncol, 1)), dtype=np.int16)
+        s = self.L.oz_split_cols_sd(C.byref(flags), k, ncol, _f(X), max(k, 1), shift, _d(out), max(k, 1),
+                                    ex.ctypes.data_as(C.POINTER(C.c_short)))
+        return s, out[:s, :, :k], ex[:s, :ncol]
+
+    def sgemm_d(self, flags, ta, tb, m, n, k, alpha, A, lda, B, ldb, beta, C_, ldc):
+        """GEMM <float, double, double> (FSum only); (C, info), or (None, None) for unsupported flags."""
+        info = Info()
+        A = np.ascontiguousarray(A, dtype=np.float32)
+        B = np.ascontiguousarray(B, dtype=np.float32)
+        Cc = np.array(C_, dtype=np.float32, copy=True)
+        r = self.L.oz_sgemm_d(C.byref(flags), ta.encode(), tb.encode(), m, n, k, alpha, _f(A), lda, _f(B), ldb,
+                              beta, _f(Cc), ldc, C.byref(info))
+        return (Cc, info) if r == 0 else (None, None)
+
     def split_csr(self, flags, val, rowptr, shift=1):
         m = len(rowptr) - 1
         nnz = len(val)
@@ -304,6 +354,17 @@ class Reference:
         L.ref_dnrm2_f32.argtypes = [C.c_void_p, C.c_int, _dp]
         L.ref_dgemv_f32.argtypes = [C.c_void_p, C.c_char, C.c_int, C.c_int, C.c_double, _dp, C.c_int, _dp,
                                     C.c_double, _dp]
+        _fp = C.POINTER(C.c_float)
+        L.ref_sgemm_d.argtypes = [C.c_void_p, C.c_char, C.c_char, C.c_int, C.c_int, C.c_int, C.c_float, _fp,
+                                  C.c_int, _fp, C.c_int, C.c_float, _fp, C.c_int]
+        L.ref_sdot_d.restype = C.c_float
+        L.ref_sdot_d.argtypes = [C.c_void_p, C.c_int, _fp, _fp]
+        L.ref_snrm2_d.restype = C.c_float
+        L.ref_snrm2_d.argtypes = [C.c_void_p, C.c_int, _fp]
+        L.ref_sgemv_d.argtypes = [C.c_void_p, C.c_char, C.c_int, C.c_int, C.c_float, _fp, C.c_int, _fp,
+                                  C.c_float, _fp]
+        L.ref_log21f.restype = C.c_float
+        L.ref_log21f.argtypes = [C.c_float]
         L.ref_ddot.restype = C.c_double
         L.ref_ddot.argtypes = [C.c_void_p, C.c_int, _dp, _dp]
         L.ref_dnrm2.restype = C.c_double
@@ -365,6 +426,34 @@ class Reference:
         self.L.ref_dgemm_f32(self.h, ta.encode(), tb.encode(), m, n, k, alpha, _d(A), lda, _d(B), ldb, beta,
                              _d(Cc), ldc)
         return Cc
+
+    def sgemm_d(self, ta, tb, m, n, k, alpha, A, lda, B, ldb, beta, C_, ldc):
+        """ozblasRgemm<float, double, double>: float data, FP64 slices and slice products."""
+        A = np.ascontiguousarray(A, dtype=np.float32)
+        B = np.ascontiguousarray(B, dtype=np.float32)
+        Cc = np.array(C_, dtype=np.float32, copy=True)
+        self.L.ref_sgemm_d(self.h, ta.encode(), tb.encode(), m, n, k, alpha, _f(A), lda, _f(B), ldb, beta, _f(Cc),
+                           ldc)
+        return Cc
+
+    def sdot_d(self, x, y):
+        x = np.ascontiguousarray(x, dtype=np.float32)
+        y = np.ascontiguousarray(y, dtype=np.float32)
+        return self.L.ref_sdot_d(self.h, len(x), _f(x), _f(y))
+
+    def snrm2_d(self, x):
+        x = np.ascontiguousarray(x, dtype=np.float32)
+        return self.L.ref_snrm2_d(self.h, len(x), _f(x))
+
+    def sgemv_d(self, ta, m, n, alpha, A, lda, x, beta, y):
+        A = np.ascontiguousarray(A, dtype=np.float32)
+        x = np.ascontiguousarray(x, dtype=np.float32)
+        yy = np.array(y, dtype=np.float32, copy=True)
+        self.L.ref_sgemv_d(self.h, ta.encode(), m, n, alpha, _f(A), lda, _f(x), beta, _f(yy))
+        return yy
+
+    def log21f(self, v):
+        return self.L.ref_log21f(v)
 
     def ddot_f32(self, x, y):
         return self.L.ref_ddot_f32(self.h, len(x), _d(x), _d(y))

@@ -235,6 +235,159 @@ int oz_dgemm_f32(const oz_flags *f, char ta, char tb, int m, int n, int k, doubl
     return 0;
 }
 
+/* ------------------------------------------------------------------------ */
+/* Mixed form <float, double, double>: FP64 slices of float data             */
+/* ------------------------------------------------------------------------ */
+
+/* getRho<float,double>, src/cpu/ozblas_split.cpp:19-34 (epse 24 and 53); negative for k < 32 */
+int oz_rho_sd(int dim, int splitEpsMode) {
+    switch (splitEpsMode) {
+    case 9: return (int)ceil((24 - (53 - log2(2. * sqrt(dim))) / 2));
+    default: return (int)ceil((24 - (53 - log2(1. * dim)) / 2));
+    }
+}
+
+/* The reference's float helpers call the double libm functions (src/cpu/ozblas_aux.cpp:3-47 with
+ * <cmath>, which declares no float overloads in the global namespace): log21<float> is
+ * (float)log2((double)v), scalbn1<float> is (float)scalbn((double)v, n), fma1<float> is
+ * (float)fma((double)x, (double)y, (double)z). */
+static short tau_sd(float v) { return (short)ceil((float)log2((double)v)); }
+short oz_tau_sd_libm(float v) { return tau_sd(v); }
+
+/* Count the positive finite floats (bit patterns from 1, every `stride`-th) where `rule`
+ * disagrees with tau_sd; the first disagreement's bits go to *first. */
+long oz_tau_sd_sweep(int (*rule)(float), unsigned stride, unsigned *first) {
+    long bad = 0;
+    for (unsigned long u = 1; u < 0x7f800000ul; u += stride) {
+        float v;
+        const unsigned b = (unsigned)u;
+        memcpy(&v, &b, 4);
+        if (rule(v) != tau_sd(v)) {
+            if (bad == 0 && first) *first = b;
+            bad++;
+        }
+    }
+    return bad;
+}
+static float scalbn_sd(float v, int e) { return (float)scalbn((double)v, e); }
+
+/* One level, src/cpu/ozblas_split.cpp:181-221 with TYPE1 = float: float arithmetic, the slice
+ * stored as the double scalbn(slice, -tau). */
+static float split_level_cols_sd(int k, int ncol, int rho, float *R, int ldr, double *S, int lds, short *E,
+                                 float *mx, int shift) {
+    float check = 0.f;
+    for (int j = 0; j < ncol; j++) {
+        const short tau = tau_sd(mx[j]);
+        E[j] = tau;
+        const float sigma = (float)(OZ_SPLIT_CONST * (double)scalbn_sd(1.f, rho + tau) * shift);
+        float m = 0.f;
+        for (int i = 0; i < k; i++) {
+            float x = R[(size_t)j * ldr + i];
+            const float s = (x + sigma) - sigma;
+            x = x - s;
+            S[(size_t)j * lds + i] = (double)scalbn_sd(s, -tau);
+            R[(size_t)j * ldr + i] = x;
+            const float ax = (float)fabs((double)x);
+            m = (m < ax) ? ax : m;
+        }
+        mx[j] = m;
+        check += m;
+    }
+    return check;
+}
+
+int oz_split_cols_sd(const oz_flags *f, int k, int ncol, const float *X, int ldx, int shift, double *slices, int lds,
+                     short *exps) {
+    const int rho = oz_rho_sd(k, f->splitEpsMode);
+    const int maxS = oz_max_split(f);
+    float *R = (float *)malloc(sizeof(float) * (size_t)(k > 0 ? k : 1) * (ncol > 0 ? ncol : 1));
+    float *mx = (float *)malloc(sizeof(float) * (ncol > 0 ? ncol : 1));
+    for (int j = 0; j < ncol; j++) {
+        float m = 0.f;
+        for (int i = 0; i < k; i++) {
+            R[(size_t)j * k + i] = X[(size_t)j * ldx + i];
+            const float ax = (float)fabs((double)X[(size_t)j * ldx + i]);
+            m = (m < ax) ? ax : m;
+        }
+        mx[j] = m;
+    }
+    split_level_cols_sd(k, ncol, rho, R, k, slices, lds, exps, mx, shift);
+    int s = 1;
+    while (s < maxS) {
+        const float c = split_level_cols_sd(k, ncol, rho, R, k, slices + (size_t)s * lds * ncol, lds,
+                                            exps + (size_t)s * ncol, mx, shift);
+        s++;
+        if (c == 0.f) break;
+    }
+    free(R);
+    free(mx);
+    return s;
+}
+
+/*
+ * GEMM <float, double, double>, src/cpu/ozblas_gemm.cpp:3-315 with TYPE1 = float: exact FP64
+ * slice products; the ordered sum (src/cpu/ozblas_sum.cpp:382-432) rounds each pair product to
+ * float, scales it by 2^(tauA + tauB) in float and adds it to a float t; the output is
+ * fma1(alpha, t, beta * C) in float.  FSum only, as for the other mixed form.
+ */
+int oz_sgemm_d(const oz_flags *f, char ta, char tb, int m, int n, int k, float alpha, const float *A, int lda,
+               const float *B, int ldb, float beta, float *C, int ldc, oz_info *info) {
+    if (f->reproMode != 1 || f->sumMode != 0 || (f->splitEpsMode != 0 && f->splitEpsMode != 9)) return -1;
+    const int is_dot = (m == 1 && n == 1);
+    const int fast = is_dot ? 0 : f->fastMode;
+    const int maxS = oz_max_split(f);
+    const int kk = k > 0 ? k : 1;
+    float *Ap = (float *)malloc(sizeof(float) * (size_t)kk * imax(m, 1));
+    float *Bp = (float *)malloc(sizeof(float) * (size_t)kk * imax(n, 1));
+    const int tA = !(ta == 'n' || ta == 'N'), tB = !(tb == 'n' || tb == 'N');
+    for (int i = 0; i < m; i++)
+        for (int l = 0; l < k; l++) Ap[(size_t)i * k + l] = tA ? A[(size_t)i * lda + l] : A[(size_t)l * lda + i];
+    for (int j = 0; j < n; j++)
+        for (int l = 0; l < k; l++) Bp[(size_t)j * k + l] = tB ? B[(size_t)l * ldb + j] : B[(size_t)j * ldb + l];
+    double *Sa = (double *)calloc((size_t)(maxS + 1) * kk * imax(m, 1), sizeof(double));
+    double *Sb = (double *)calloc((size_t)(maxS + 1) * kk * imax(n, 1), sizeof(double));
+    short *Ea = (short *)calloc((size_t)(maxS + 1) * imax(m, 1), sizeof(short));
+    short *Eb = (short *)calloc((size_t)(maxS + 1) * imax(n, 1), sizeof(short));
+    const int nA = oz_split_cols_sd(f, k, m, Ap, k, 1, Sa, k, Ea);
+    const int nB = oz_split_cols_sd(f, k, n, Bp, k, 1, Sb, k, Eb);
+    int maxlevel = (nA - 1) + (nB - 1);
+    maxlevel = imax(maxlevel - fast, imin(nA - 1, nB - 1));
+    int *pa = (int *)malloc(sizeof(int) * nA * nB), *pb = (int *)malloc(sizeof(int) * nA * nB);
+    const int np = make_pairs(nA, nB, maxlevel, pa, pb);
+    for (int j = 0; j < n; j++)
+        for (int i = 0; i < m; i++) {
+            float t = 0.f;
+            for (int p = 0; p < np; p++) {
+                const double *a = Sa + (size_t)pa[p] * k * m + (size_t)i * k;
+                const double *b = Sb + (size_t)pb[p] * k * n + (size_t)j * k;
+                double c = 0.;
+                for (int l = 0; l < k; l++) c += a[l] * b[l]; /* exact in FP64 */
+                t += scalbn_sd((float)c, Ea[(size_t)pa[p] * m + i] + Eb[(size_t)pb[p] * n + j]);
+            }
+            float *cc = &C[(size_t)j * ldc + i];
+            *cc = (float)fma((double)alpha, (double)t, (double)(beta * *cc));
+        }
+    if (info) {
+        info->nSplitA = (float)nA;
+        info->nSplitB = (float)nB;
+        if (is_dot)
+            info->nSplitC = 1.f;
+        else if (n == 1 && fast == 0)
+            info->nSplitC = (float)imin(maxlevel + 1, nA);
+        else
+            info->nSplitC = (float)np;
+    }
+    free(Ap);
+    free(Bp);
+    free(Sa);
+    free(Sb);
+    free(Ea);
+    free(Eb);
+    free(pa);
+    free(pb);
+    return 0;
+}
+
 /*
  * One split level over CSR rows: src/cpu/ozblas_split.cpp:779-815.
  * rho comes from the row's nnz; sigma is divided (not multiplied) by shift.

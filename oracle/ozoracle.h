@@ -41,6 +41,13 @@ typedef struct {
 /* ---- split helpers ---- */
 int oz_rho(int dim, int splitEpsMode);
 int oz_rho_f32(int dim, int splitEpsMode);
+int oz_rho_sd(int dim, int splitEpsMode);
+short oz_tau_sd_libm(float v);
+long oz_tau_sd_sweep(int (*rule)(float), unsigned stride, unsigned *first);
+int oz_split_cols_sd(const oz_flags *f, int k, int ncol, const float *X, int ldx, int shift, double *slices, int lds,
+                     short *exps);
+int oz_sgemm_d(const oz_flags *f, char ta, char tb, int m, int n, int k, float alpha, const float *A, int lda,
+               const float *B, int ldb, float beta, float *C, int ldc, oz_info *info);
 int oz_split_cols_f32(const oz_flags *f, int k, int ncol, const double *X, int ldx, int shift, float *slices,
                       int lds, short *exps);
 int oz_dgemm_f32(const oz_flags *f, char ta, char tb, int m, int n, int k, double alpha, const double *A, int lda,

@@ -75,6 +75,29 @@ int ref_dgemm_f32(void *hp, char ta, char tb, int m, int n, int k, double alpha,
                                              ldc);
 }
 
+/* the mixed form <float, double, double>: float data, FP64 slices and slice products */
+int ref_sgemm_d(void *hp, char ta, char tb, int m, int n, int k, float alpha, const float *A, int lda, const float *B,
+                int ldb, float beta, float *C, int ldc) {
+    return ozblasRgemm<float, double, double>((ozblasHandle_t *)hp, ta, tb, m, n, k, alpha, A, lda, B, ldb, beta, C,
+                                              ldc);
+}
+
+float ref_sdot_d(void *hp, int n, const float *x, const float *y) {
+    return ozblasRdot<float, double, double>((ozblasHandle_t *)hp, n, x, 1, y, 1);
+}
+
+float ref_snrm2_d(void *hp, int n, const float *x) {
+    return ozblasRnrm2<float, double, double>((ozblasHandle_t *)hp, n, x, 1);
+}
+
+int ref_sgemv_d(void *hp, char ta, int m, int n, float alpha, const float *A, int lda, const float *x, float beta,
+                float *y) {
+    return ozblasRgemv<float, double, double>((ozblasHandle_t *)hp, ta, m, n, alpha, A, lda, x, 1, beta, y, 1);
+}
+
+/* log21<float> of the reference (src/cpu/ozblas_aux.cpp:37-42), for the tau rule of float data */
+float ref_log21f(float v) { return log21<float>(v); }
+
 double ref_ddot_f32(void *hp, int n, const double *x, const double *y) {
     return ozblasRdot<double, float, float>((ozblasHandle_t *)hp, n, x, 1, y, 1);
 }

@@ -90,6 +90,11 @@ _dsgemm = _sig("cuozblasDSgemm", [_HP, _ch, _ch, _i32, _i32, _i32, _d, _vp, _i32
 _dsgemv = _sig("cuozblasDSgemv", [_HP, _ch, _i32, _i32, _d, _vp, _i32, _vp, _i32, _d, _vp, _i32])
 _dsdot = _sig("cuozblasDSdot", [_HP, _i32, _vp, _i32, _vp, _i32, C.POINTER(_d)])
 _dsnrm2 = _sig("cuozblasDSnrm2", [_HP, _i32, _vp, _i32, C.POINTER(_d)])
+_f = C.c_float
+_sdgemm = _sig("cuozblasSDgemm", [_HP, _ch, _ch, _i32, _i32, _i32, _f, _vp, _i32, _vp, _i32, _f, _vp, _i32])
+_sdgemv = _sig("cuozblasSDgemv", [_HP, _ch, _i32, _i32, _f, _vp, _i32, _vp, _i32, _f, _vp, _i32])
+_sddot = _sig("cuozblasSDdot", [_HP, _i32, _vp, _i32, _vp, _i32, C.POINTER(_f)])
+_sdnrm2 = _sig("cuozblasSDnrm2", [_HP, _i32, _vp, _i32, C.POINTER(_f)])
 _dgemm_i8 = _sig("cuozblasDgemmI8", [_HP, _ch, _ch, _i32, _i32, _i32, _d, _vp, _i32, _vp, _i32, _d, _vp, _i32])
 _dgemm_i8_static = _sig("cuozblasDgemmI8Static", [_ch, _ch, _i32, _i32, _i32, _d, _vp, _i32, _vp, _i32, _d, _vp,
                                                   _i32, _i32, _i32, _vp])
@@ -101,6 +106,7 @@ _dsplita = _sig("cuozblasDcsrmvSplitA", [_HP, _ch, _i32, _i32, _i32, _vp, _vp, _
 _dcg = _sig("cuozblasDcg", [_HP, _ch, _i32, _i32, _vp, _vp, _vp, _vp, _vp, _vp, _i32, _d])
 rule_tau = _sig("cuozblasRuleTau", [_d])
 rule_rho = _sig("cuozblasRuleRho", [_i32, _i32])
+rule_tau_f32 = _sig("cuozblasRuleTauF32", [C.c_float])
 rule_crsum = _sig("cuozblasRuleCrSum", [_i32, _vp, _PD])
 _version = _sig("cuozblasVersion", [], C.c_char_p)
 
@@ -110,6 +116,7 @@ C_ABI_SYMBOLS = [
     "cuozblasDaxpy", "cuozblasDgemv", "cuozblasDgemm", "cuozblasDcsrmv", "cuozblasDcsrmvSplitA", "cuozblasDcg",
     "cuozblasDgemmI8", "cuozblasDgemmI8Static", "cuozblasDgemmI8Batched", "cuozblasRuleTau", "cuozblasRuleRho",
     "cuozblasRuleCrSum", "cuozblasDSgemm", "cuozblasDSgemv", "cuozblasDSdot", "cuozblasDSnrm2",
+    "cuozblasRuleTauF32", "cuozblasSDgemm", "cuozblasSDgemv", "cuozblasSDdot", "cuozblasSDnrm2",
     "cuozblasVersion",
 ]
 
@@ -200,6 +207,29 @@ def dsdot(h, n, x, y, incx=1, incy=1) -> float:
 def dsnrm2(h, n, x, incx=1) -> float:
     r = _d()
     _chk("cuozblasDSnrm2", _dsnrm2(h.ref, n, _ptr(x), incx, C.byref(r)))
+    return r.value
+
+
+def sdgemm(h, ta, tb, m, n, k, alpha, A, lda, B, ldb, beta, Cm, ldc):
+    """Mixed form <float, double, double>: float data and C, FP64 slices and slice products (FSum)."""
+    _chk("cuozblasSDgemm", _sdgemm(h.ref, ta.encode(), tb.encode(), m, n, k, alpha, _ptr(A), lda, _ptr(B), ldb,
+                                   beta, _ptr(Cm), ldc))
+
+
+def sdgemv(h, trans, m, n, alpha, A, lda, x, beta, y, incx=1, incy=1):
+    _chk("cuozblasSDgemv", _sdgemv(h.ref, trans.encode(), m, n, alpha, _ptr(A), lda, _ptr(x), incx, beta, _ptr(y),
+                                   incy))
+
+
+def sddot(h, n, x, y, incx=1, incy=1) -> float:
+    r = _f()
+    _chk("cuozblasSDdot", _sddot(h.ref, n, _ptr(x), incx, _ptr(y), incy, C.byref(r)))
+    return r.value
+
+
+def sdnrm2(h, n, x, incx=1) -> float:
+    r = _f()
+    _chk("cuozblasSDnrm2", _sdnrm2(h.ref, n, _ptr(x), incx, C.byref(r)))
     return r.value
 
 

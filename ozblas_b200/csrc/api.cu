@@ -123,6 +123,8 @@ extern "C" {
 const char *cuozblasVersion(void) { return "cuozblas-b200 0.1 (sm_100a; plain FP64-slice + INT8 tcgen05 forms)"; }
 
 int cuozblasRuleTau(double v) { return tau_rule(v); }
+
+int cuozblasRuleTauF32(float v) { return tau_rule_f32(v); }
 int cuozblasRuleRho(int32_t dim, int32_t mode) { return rho_rule(dim, mode); }
 
 int cuozblasRuleCrSum(int32_t n, const double *terms, double *out) {
@@ -331,6 +333,72 @@ int cuozblasDSnrm2(cuozblasHandle_t *h, int32_t n, const double *x, int32_t incx
     double d = 0.0;
     OZB_TRY(dot_f32_impl(h, n, x, x, &d));
     *ret = sqrt(d);  // host sqrt, src/cpu/ozblas_nrm2.cpp:24-29
+    return finish(h, t0);
+}
+
+// Mixed form <float, double, double>: float data and results, FP64 slices;
+// FSum only, no Dot2, as the other mixed form.
+int cuozblasSDgemm(cuozblasHandle_t *h, char transa, char transb, int32_t m, int32_t n, int32_t k, float alpha,
+                   const float *A, int32_t lda, const float *B, int32_t ldb, float beta, float *C, int32_t ldc) {
+    OZB_TRY(counter_init(h));
+    OZB_TRY(check_flags_f32(h));
+    if (m < 0 || n < 0 || k < 0 || ldc < (m > 1 ? m : 1)) return CUOZBLAS_STATUS_INVALID_VALUE;
+    if (h->reproMode == 0 && h->nSplitMax == 1) return CUOZBLAS_STATUS_NOT_SUPPORTED;
+    if (m == 0 || n == 0) return CUOZBLAS_STATUS_SUCCESS;
+    const double t0 = wall();
+    OZB_TRY(gemm_sd_core(h, transa, transb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, h->fastMode));
+    return finish(h, t0);
+}
+
+int cuozblasSDgemv(cuozblasHandle_t *h, char trans, int32_t m, int32_t n, float alpha, const float *A, int32_t lda,
+                   const float *x, int32_t incx, float beta, float *y, int32_t incy) {
+    OZB_TRY(counter_init(h));
+    OZB_TRY(check_flags_f32(h));
+    if (incx != 1 || incy != 1 || m < 0 || n < 0) return CUOZBLAS_STATUS_INVALID_VALUE;
+    if (h->reproMode == 0 && h->nSplitMax == 1) return CUOZBLAS_STATUS_NOT_SUPPORTED;
+    const double t0 = wall();
+    if (!is_trans(trans)) {  // src/cpu/ozblas_gemv.cpp:22-26
+        if (m == 0) return CUOZBLAS_STATUS_SUCCESS;
+        OZB_TRY(gemm_sd_core(h, 'n', 'n', m, 1, n, alpha, A, lda, x, n, beta, y, m, h->fastMode));
+    } else {
+        if (n == 0) return CUOZBLAS_STATUS_SUCCESS;
+        OZB_TRY(gemm_sd_core(h, 't', 'n', n, 1, m, alpha, A, lda, x, m, beta, y, n, h->fastMode));
+    }
+    return finish(h, t0);
+}
+
+static int dot_sd_impl(cuozblasHandle_t *h, int n, const float *x, const float *y, float *ret) {
+    State *st = state(h);
+    float *d = reinterpret_cast<float *>(h->devWorkCommon);
+    OZB_CHECK(cudaMemsetAsync(d, 0, sizeof(float), st->stream));
+    OZB_TRY(gemm_sd_core(h, 't', 'n', 1, 1, n, 1.f, x, n, y, n, 0.f, d, 1, 0));
+    OZB_CHECK(cudaMemcpyAsync(st->h_dbl, d, sizeof(float), cudaMemcpyDeviceToHost, st->stream));
+    OZB_CHECK(cudaStreamSynchronize(st->stream));
+    memcpy(ret, st->h_dbl, sizeof(float));
+    return CUOZBLAS_STATUS_SUCCESS;
+}
+
+int cuozblasSDdot(cuozblasHandle_t *h, int32_t n, const float *x, int32_t incx, const float *y, int32_t incy,
+                  float *ret) {
+    OZB_TRY(counter_init(h));
+    OZB_TRY(check_flags_f32(h));
+    if (incx != 1 || incy != 1 || n < 0 || ret == nullptr) return CUOZBLAS_STATUS_INVALID_VALUE;
+    if (h->reproMode == 0 && h->nSplitMax == 1) return CUOZBLAS_STATUS_NOT_SUPPORTED;
+    const double t0 = wall();
+    OZB_TRY(dot_sd_impl(h, n, x, y, ret));
+    h->t_SplitVec_total += h->t_SplitA + h->t_SplitB;
+    return finish(h, t0);
+}
+
+int cuozblasSDnrm2(cuozblasHandle_t *h, int32_t n, const float *x, int32_t incx, float *ret) {
+    OZB_TRY(counter_init(h));
+    OZB_TRY(check_flags_f32(h));
+    if (incx != 1 || n < 0 || ret == nullptr) return CUOZBLAS_STATUS_INVALID_VALUE;
+    if (h->reproMode == 0 && h->nSplitMax == 1) return CUOZBLAS_STATUS_NOT_SUPPORTED;
+    const double t0 = wall();
+    float d = 0.f;
+    OZB_TRY(dot_sd_impl(h, n, x, x, &d));
+    *ret = (float)sqrt((double)d);  // the reference's sqrt on a float (src/cpu/ozblas_nrm2.cpp:24-29)
     return finish(h, t0);
 }
 

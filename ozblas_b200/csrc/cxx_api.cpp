@@ -98,6 +98,36 @@ int32_t cuozblasRgemm<double, float, float>(cuozblasHandle_t *oh, const char tra
 }
 
 template <>
+int32_t cuozblasRnrm2<float, double, double>(cuozblasHandle_t *oh, const int32_t n, const float *devX,
+                                             const int32_t incx, float *ret) {
+    return report("cuozblasRnrm2<float,double>", cuozblasSDnrm2(oh, n, devX, incx, ret));
+}
+
+template <>
+int32_t cuozblasRdot<float, double, double>(cuozblasHandle_t *oh, const int32_t n, const float *devA,
+                                            const int32_t incx, const float *devB, const int32_t incy, float *ret) {
+    return report("cuozblasRdot<float,double>", cuozblasSDdot(oh, n, devA, incx, devB, incy, ret));
+}
+
+template <>
+int32_t cuozblasRgemv<float, double, double>(cuozblasHandle_t *oh, const char tranA, const int32_t m, const int32_t n,
+                                             const float alpha, const float *devA, const int32_t lda,
+                                             const float *devB, const int32_t incx, const float beta, float *devC,
+                                             const int32_t incy) {
+    return report("cuozblasRgemv<float,double>",
+                  cuozblasSDgemv(oh, tranA, m, n, alpha, devA, lda, devB, incx, beta, devC, incy));
+}
+
+template <>
+int32_t cuozblasRgemm<float, double, double>(cuozblasHandle_t *oh, const char tranA, const char tranB,
+                                             const int32_t m, const int32_t n, const int32_t k, const float alpha,
+                                             const float *devA, const int32_t lda, const float *devB,
+                                             const int32_t ldb, const float beta, float *devC, const int32_t ldc) {
+    return report("cuozblasRgemm<float,double>",
+                  cuozblasSDgemm(oh, tranA, tranB, m, n, k, alpha, devA, lda, devB, ldb, beta, devC, ldc));
+}
+
+template <>
 int32_t cuozblasRcsrmv<double, double>(cuozblasHandle_t *oh, const char tranA, const int32_t m, const int32_t n,
                                        const int32_t nnz, const double alpha, const cusparseMatDescr_t descrA,
                                        const double *devA, const int32_t *devAcolind, const int32_t *devArowptr,

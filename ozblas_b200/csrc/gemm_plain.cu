@@ -35,11 +35,18 @@ __device__ __forceinline__ void dmma884(double &c0, double &c1, double a, double
                  : "d"(a), "d"(b));
 }
 
-template <bool STORE>
+// SD: the mixed form <float, double, double>.  At each pair boundary the
+// exact product is rounded to float, scaled by 2^(tauA + tauB) in float
+// ((float)scalbn, one rounding) and added to a float sum; the output is
+// (float)fma(alpha, t, beta * C) computed in double, as the reference's float
+// helpers do (src/cpu/ozblas_sum.cpp:382-432, src/cpu/ozblas_aux.cpp:3-35).
+template <bool STORE, bool SD>
 __global__ void __launch_bounds__(128) k_gemm_pairs_dmma(int m, int n, int nlB, int ldk, const double *__restrict__ As,
                                                          const double *__restrict__ Bs, const int2 *__restrict__ pairs,
                                                          int np, double alpha, double beta, double *__restrict__ C,
-                                                         int ldc, double *__restrict__ pbuf) {
+                                                         int ldc, double *__restrict__ pbuf,
+                                                         const short *__restrict__ Ea, const short *__restrict__ Eb,
+                                                         float *__restrict__ Cf) {
     __shared__ __align__(16) double sA[2][kBM][kLds];
     __shared__ __align__(16) double sB[2][kBN][kLds];
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -49,12 +56,14 @@ __global__ void __launch_bounds__(128) k_gemm_pairs_dmma(int m, int n, int nlB, 
     const int total = np * nkt;
 
     double acc[4][4][2], t[4][4][2];
+    float tf[4][4][2];
 #pragma unroll
     for (int i = 0; i < 4; i++)
 #pragma unroll
         for (int j = 0; j < 4; j++) {
             acc[i][j][0] = acc[i][j][1] = 0.0;
             t[i][j][0] = t[i][j][1] = 0.0;
+            tf[i][j][0] = tf[i][j][1] = 0.f;
         }
 
     // each thread copies 4 x 16B of A and of B per k-tile (64 lines x 8 chunks)
@@ -96,7 +105,33 @@ __global__ void __launch_bounds__(128) k_gemm_pairs_dmma(int m, int n, int nlB, 
         __syncthreads();
         const int p = step / nkt;
         if (step - p * nkt == nkt - 1) {  // pair complete: acc is the exact product of pair p
-            if (STORE) {
+            if (SD) {
+                const int2 pr = pairs[p];
+                int ea[4], eb[8];
+#pragma unroll
+                for (int i = 0; i < 4; i++) {
+                    const int r = m0 + wm * 32 + i * 8 + (lane >> 2);
+                    ea[i] = r < m ? Ea[(size_t)pr.x * m + r] : 0;
+                }
+#pragma unroll
+                for (int j = 0; j < 4; j++)
+#pragma unroll
+                    for (int h = 0; h < 2; h++) {
+                        const int c = n0 + wn * 32 + j * 8 + (lane & 3) * 2 + h;
+                        eb[j * 2 + h] = c < n ? Eb[(size_t)pr.y * nlB + c] : 0;
+                    }
+#pragma unroll
+                for (int i = 0; i < 4; i++)
+#pragma unroll
+                    for (int j = 0; j < 4; j++)
+#pragma unroll
+                        for (int h = 0; h < 2; h++) {
+                            const float c32 = __double2float_rn(acc[i][j][h]);
+                            tf[i][j][h] = __fadd_rn(tf[i][j][h],
+                                                    __double2float_rn(scalbn((double)c32, ea[i] + eb[j * 2 + h])));
+                            acc[i][j][h] = 0.0;
+                        }
+            } else if (STORE) {
 #pragma unroll
                 for (int i = 0; i < 4; i++)
 #pragma unroll
@@ -121,7 +156,22 @@ __global__ void __launch_bounds__(128) k_gemm_pairs_dmma(int m, int n, int nlB, 
             }
         }
     }
-    if (!STORE) {
+    if (SD) {
+        const float af = (float)alpha, bf = (float)beta;
+#pragma unroll
+        for (int i = 0; i < 4; i++)
+#pragma unroll
+            for (int j = 0; j < 4; j++)
+#pragma unroll
+                for (int h = 0; h < 2; h++) {
+                    const int r = m0 + wm * 32 + i * 8 + (lane >> 2);
+                    const int c = n0 + wn * 32 + j * 8 + (lane & 3) * 2 + h;
+                    if (r < m && c < n) {
+                        float *cp = &Cf[(size_t)c * ldc + r];
+                        *cp = __double2float_rn(fma((double)af, (double)tf[i][j][h], (double)__fmul_rn(bf, *cp)));
+                    }
+                }
+    } else if (!STORE) {
 #pragma unroll
         for (int i = 0; i < 4; i++)
 #pragma unroll
@@ -498,8 +548,9 @@ int gemm_plain_core(cuozblasHandle_t *h, char ta, char tb, int m, int n, int k, 
             const int nc = (int)((n - c0) < ncols ? (n - c0) : ncols);
             dim3 g((m + kBM - 1) / kBM, (nc + kBN - 1) / kBN);
             counted(h);
-            k_gemm_pairs_dmma<true><<<g, 128, 0, st->stream>>>(m, nc, n, ldk, Sa, Sb + (size_t)c0 * ldk, dp, np, alpha,
-                                                               beta, C, ldc, pbuf);
+            k_gemm_pairs_dmma<true, false><<<g, 128, 0, st->stream>>>(m, nc, n, ldk, Sa, Sb + (size_t)c0 * ldk, dp,
+                                                                      np, alpha, beta, C, ldc, pbuf, nullptr,
+                                                                      nullptr, nullptr);
             OZB_CHECK(cudaGetLastError());
             const int64_t count = (int64_t)m * nc;
             counted(h);
@@ -509,11 +560,151 @@ int gemm_plain_core(cuozblasHandle_t *h, char ta, char tb, int m, int n, int k, 
         }
     } else {
         counted(h);
-        k_gemm_pairs_dmma<false><<<grid, 128, 0, st->stream>>>(m, n, n, ldk, Sa, Sb, dp, np, alpha, beta, C, ldc,
-                                                               nullptr);
+        k_gemm_pairs_dmma<false, false><<<grid, 128, 0, st->stream>>>(m, n, n, ldk, Sa, Sb, dp, np, alpha, beta, C,
+                                                                      ldc, nullptr, nullptr, nullptr, nullptr);
         OZB_CHECK(cudaGetLastError());
     }
     ev_record(h, 3);  // the ordered sum runs inside the product kernels here
+    ev_record(h, 4);
+    return CUOZBLAS_STATUS_SUCCESS;
+}
+
+// ---------------------------------------------------------------------------
+// Mixed form <float, double, double> (src/cpu/ozblas_gemm.cpp:3-315 with
+// TYPE1 = float): float data split in float arithmetic into FP64 slices
+// (split_lines_*_sd), exact FP64 slice products on the DMMA / skinny kernels
+// above, and the float-scaled ordered sum.
+// ---------------------------------------------------------------------------
+// getRho<float, double> on the host with the reference's own expression
+// (src/cpu/ozblas_split.cpp:19-34, epse 24 and 53); negative below k = 32.
+int rho_rule_sd(int dim, int splitEpsMode) {
+    const double d = dim < 1 ? 1.0 : (double)dim;
+    if (splitEpsMode == 9) return (int)ceil((24 - (53 - log2(2. * sqrt(d))) / 2));
+    return (int)ceil((24 - (53 - log2(d)) / 2));
+}
+
+// Ordered float sum of the skinny forms: P[(ia*nB+ib)*ldp + row] exact in FP64;
+// t += (float)scalbn((float)P, tauA + tauB); y = (float)fma(alpha, t, beta*y).
+__global__ void k_sum_rows_sd(int m, int nA, int nB, int maxlevel, const double *__restrict__ P, int64_t ldp,
+                              const short *__restrict__ Ea, int ldea, const short *__restrict__ Eb, float alpha,
+                              float beta, float *__restrict__ y) {
+    const int row = blockIdx.x * blockDim.x + threadIdx.x;
+    if (row >= m) return;
+    float t = 0.f;
+    for_each_pair(nA, nB, maxlevel, [&](int ia, int ib) {
+        const float c32 = __double2float_rn(P[(size_t)(ia * nB + ib) * ldp + row]);
+        t = __fadd_rn(t, __double2float_rn(scalbn((double)c32, Ea[(size_t)ia * ldea + row] + Eb[ib])));
+    });
+    y[row] = __double2float_rn(fma((double)alpha, (double)t, (double)__fmul_rn(beta, y[row])));
+}
+
+// Split op(X) (float, nl lines of length k) into FP64 slices ns x nl x ldk
+// and exponents ns x nl; X with strided lines is transposed first.
+static int split_operand_sd(cuozblasHandle_t *h, bool lines_strided, int nl, int k, const float *X, int ldx, int rho,
+                            int maxS, int ldk, double **slices, short **exps, int *ns, Arena &ar) {
+    const float *src = X;
+    int lds = ldx;
+    if (lines_strided) {
+        float *tmp = ar.take<float>((uint64_t)nl * (k > 0 ? k : 1));
+        if (!ar.ok) return CUOZBLAS_STATUS_WORKSPACE;
+        OZB_TRY(transpose_f32(h, nl, k, X, ldx, tmp, k));
+        src = tmp;
+        lds = k;
+    }
+    OZB_TRY(split_lines_count_sd(h, k, nl, src, lds, rho, maxS, ns));
+    *slices = ar.take<double>((uint64_t)(*ns) * nl * ldk);
+    *exps = ar.take<short>((uint64_t)(*ns) * nl);
+    if (!ar.ok) return CUOZBLAS_STATUS_WORKSPACE;
+    return split_lines_write_sd(h, k, nl, src, lds, rho, *ns, *slices, ldk, *exps);
+}
+
+int gemm_sd_core(cuozblasHandle_t *h, char ta, char tb, int m, int n, int k, float alpha, const float *A, int lda,
+                 const float *B, int ldb, float beta, float *C, int ldc, int fastMode) {
+    State *st = state(h);
+    const int maxS = h->nSplitMax > 0 ? h->nSplitMax : kMaxSplitDefault;
+    const int rho = rho_rule_sd(k, h->splitEpsMode);
+    Arena ar(h);
+    const bool dot = (m == 1 && n == 1);
+    const bool skinny_n = (n == 1);
+    const int ldk = dot || skinny_n ? ceil_to(k > 0 ? k : 1, 2) : ceil_to(k > 0 ? k : 1, kBK);
+
+    ev_record(h, 0);
+    st->plain_timers = true;
+    double *Sa = nullptr, *Sb = nullptr;
+    short *Ea = nullptr, *Eb = nullptr;
+    int nA = 0, nB = 0;
+    // lines of op(A): 'n' -> row i of A is strided by lda; a vector is one line
+    OZB_TRY(split_operand_sd(h, dot ? false : !is_trans(ta), m, k, A, dot ? k : lda, rho, maxS, ldk, &Sa, &Ea, &nA,
+                             ar));
+    ev_record(h, 1);
+    OZB_TRY(split_operand_sd(h, skinny_n ? false : is_trans(tb), n, k, B, skinny_n ? k : ldb, rho, maxS, ldk, &Sb,
+                             &Eb, &nB, ar));
+    ev_record(h, 2);
+    const int fast = dot ? 0 : fastMode;
+    int maxlevel = (nA - 1) + (nB - 1);
+    {
+        const int mn = nA - 1 < nB - 1 ? nA - 1 : nB - 1;
+        maxlevel = (maxlevel - fast) > mn ? (maxlevel - fast) : mn;  // src/cpu/ozblas_gemm.cpp:163-164
+    }
+    int np = 0;
+    for_each_pair(nA, nB, maxlevel, [&](int, int) { np++; });
+    h->nSplitA = (float)nA;
+    h->nSplitB = (float)nB;
+    h->nSplitC = dot ? 1.f : (skinny_n && fast == 0 ? (float)(maxlevel + 1 < nA ? maxlevel + 1 : nA) : (float)np);
+    h->mbk = m;
+    h->nbk = n;
+
+    if (dot || skinny_n) {
+        const int rows = dot ? 1 : m;
+        const int64_t ldp = rows;
+        double *P = ar.take<double>((uint64_t)nA * nB * ldp);
+        if (!ar.ok) return CUOZBLAS_STATUS_WORKSPACE;
+        if (dot) OZB_CHECK(cudaMemsetAsync(P, 0, sizeof(double) * nA * nB, st->stream));
+        for (int ia0 = 0; ia0 < nA; ia0 += 8)
+            for (int ib0 = 0; ib0 < nB; ib0 += 8) {
+                const int na = nA - ia0 < 8 ? nA - ia0 : 8, nb = nB - ib0 < 8 ? nB - ib0 : 8;
+                counted(h);
+                if (dot) {
+                    int blocks = (k + 255) / 256;
+                    if (blocks > 148 * 8) blocks = 148 * 8;
+                    if (blocks < 1) blocks = 1;
+                    k_pair_dot<<<blocks, 256, 0, st->stream>>>(k, na, nb, Sa + (size_t)ia0 * ldk, ldk,
+                                                               Sb + (size_t)ib0 * ldk, ldk, P + ia0 * nB + ib0, nB);
+                } else {
+                    const int blocks = (int)(((int64_t)m * 32 + 255) / 256);
+                    k_pair_gemv<<<blocks, 256, 0, st->stream>>>(m, k, na, nb, ia0, ib0, nB, Sa, ldk, Sb, ldk, P,
+                                                                ldp);
+                }
+                OZB_CHECK(cudaGetLastError());
+            }
+        ev_record(h, 3);
+        counted(h);
+        k_sum_rows_sd<<<(rows + 127) / 128, 128, 0, st->stream>>>(rows, nA, nB, maxlevel, P, ldp, Ea, rows, Eb, alpha,
+                                                                  beta, C);
+        OZB_CHECK(cudaGetLastError());
+        ev_record(h, 4);
+        return CUOZBLAS_STATUS_SUCCESS;
+    }
+
+    int2 *hp = new int2[np > 0 ? np : 1];
+    int q = 0;
+    for_each_pair(nA, nB, maxlevel, [&](int ia, int ib) { hp[q++] = make_int2(ia, ib); });
+    int2 *dp = ar.take<int2>(np > 0 ? np : 1);
+    if (!ar.ok) {
+        delete[] hp;
+        return CUOZBLAS_STATUS_WORKSPACE;
+    }
+    cudaError_t ce = cudaMemcpyAsync(dp, hp, sizeof(int2) * np, cudaMemcpyHostToDevice, st->stream);
+    cudaError_t ce2 = cudaStreamSynchronize(st->stream);
+    delete[] hp;
+    OZB_CHECK(ce);
+    OZB_CHECK(ce2);
+    dim3 grid((m + kBM - 1) / kBM, (n + kBN - 1) / kBN);
+    counted(h);
+    k_gemm_pairs_dmma<false, true><<<grid, 128, 0, st->stream>>>(m, n, n, ldk, Sa, Sb, dp, np, (double)alpha,
+                                                                 (double)beta, nullptr, ldc, nullptr, Ea, Eb, C);
+    OZB_CHECK(cudaGetLastError());
+    ev_record(h, 3);
     ev_record(h, 4);
     return CUOZBLAS_STATUS_SUCCESS;
 }

@@ -125,6 +125,12 @@ int split_lines_write_f32(cuozblasHandle_t *h, int k, int nl, const double *X, i
                           int ldo, short *exps);
 int split_vector_f32(cuozblasHandle_t *h, int n, const double *x, int rho, int maxS, float *out, int ldo, short *exps,
                      int *ns);
+// Mixed form <float, double, double>: float data split in float arithmetic into
+// FP64 slices scalbn(slice, -tau), tau at exps[level * nl + line].
+int split_lines_count_sd(cuozblasHandle_t *h, int k, int nl, const float *X, int ldx, int rho, int maxS, int *ns);
+int split_lines_write_sd(cuozblasHandle_t *h, int k, int nl, const float *X, int ldx, int rho, int ns, double *out,
+                         int ldo, short *exps);
+int transpose_f32(cuozblasHandle_t *h, int rows, int cols, const float *A, int lda, float *out, int ldo);
 // Transpose rows x cols (column-major, ld) into cols x rows (ldo).
 int transpose(cuozblasHandle_t *h, int rows, int cols, const double *A, int lda, double *out, int ldo);
 // Vector split with one global tau chain (n-vector).  Writes ns slices of ldo.
@@ -143,6 +149,11 @@ int fsum_pairs_dot(cuozblasHandle_t *h, int nA, int nB, int maxlevel, const doub
 int rho_rule_f32(int dim, int splitEpsMode);
 int gemm_f32_core(cuozblasHandle_t *h, char ta, char tb, int m, int n, int k, double alpha, const double *A, int lda,
                   const double *B, int ldb, double beta, double *C, int ldc, int fastMode);
+
+// ---- mixed form <float, double, double> (gemm_plain.cu: the FP64-slice engine) ----
+int rho_rule_sd(int dim, int splitEpsMode);
+int gemm_sd_core(cuozblasHandle_t *h, char ta, char tb, int m, int n, int k, float alpha, const float *A, int lda,
+                 const float *B, int ldb, float beta, float *C, int ldc, int fastMode);
 
 // ---- plain GEMM core (gemm_plain.cu) ----
 int gemm_plain_core(cuozblasHandle_t *h, char ta, char tb, int m, int n, int k, double alpha, const double *A,

@@ -84,6 +84,40 @@ OZB_HD int tau_rule(double v) {
     return ((int64_t)j <= tau_threshold(e)) ? e : e + 1;
 }
 
+// The tau of float data, (short)ceil((float)log2((double)v)) in the reference
+// (log21<float>, src/cpu/ozblas_aux.cpp:37-42, calls the double log2).  For
+// v = 2^e (1 + j 2^-23) the float nearest to e + log2(1 + j 2^-23) is e when
+// log2(1 + j 2^-23) is at most half the spacing of floats just above e, which
+// gives the same thresholds in j as the double rule (floor(ln2 2^(p-1))): the
+// spacing and j's unit both scale by 2^29.  The double rounding of log2 before
+// the float rounding never crosses a threshold: j's nearest integers lie at
+// least 0.09 units (2^-26 in log2) from it, against a double spacing of at most
+// 2^-45 for |e| <= 149.  Pinned against the reference on every exponent by the
+// CPU tests.
+OZB_HD int tau_rule_f32(float v) {
+#if defined(__CUDA_ARCH__)
+    const uint32_t b = (uint32_t)__float_as_int(v) & 0x7fffffffu;
+#else
+    uint32_t b;
+    __builtin_memcpy(&b, &v, 4);
+    b &= 0x7fffffffu;
+#endif
+    const int be = (int)(b >> 23);
+    uint32_t j = b & ((1u << 23) - 1);
+    int e;
+    if (be == 0xff) return 0;
+    if (be == 0) {
+        if (j == 0) return 0;
+        const int msb = 31 - clz32(j);  // 0..22
+        e = msb - 149;
+        j = (j << (23 - msb)) & ((1u << 23) - 1);
+    } else {
+        e = be - 127;
+    }
+    if (j == 0) return e;
+    return ((int64_t)j <= tau_threshold(e)) ? e : e + 1;
+}
+
 // rho = ceil(53 - (53 - log2(dim)) / 2) for splitEpsMode 0
 // (src/cpu/ozblas_split.cpp:19-34) as an exact integer rule: the smallest r
 // with 2^(2r - 53) >= dim.  Mode 9 ("overflow" variant) is

@@ -149,19 +149,30 @@ int split_lines_write_f32(cuozblasHandle_t *h, int k, int nl, const double *X, i
 // ---------------------------------------------------------------------------
 // Transpose (column-major rows x cols -> cols x rows), 32x32 tiles.
 // ---------------------------------------------------------------------------
-__global__ void k_transpose(int rows, int cols, const double *__restrict__ A, int lda, double *__restrict__ out,
-                            int ldo) {
-    __shared__ double t[32][33];
+template <typename T>
+__device__ __forceinline__ void transpose_tile(int rows, int cols, const T *__restrict__ A, int lda,
+                                               T *__restrict__ out, int ldo) {
+    __shared__ T t[32][33];
     const int r0 = blockIdx.x * 32, c0 = blockIdx.y * 32;
     for (int j = threadIdx.y; j < 32; j += 8) {
         const int r = r0 + threadIdx.x, c = c0 + j;
-        t[j][threadIdx.x] = (r < rows && c < cols) ? A[(size_t)c * lda + r] : 0.0;
+        t[j][threadIdx.x] = (r < rows && c < cols) ? A[(size_t)c * lda + r] : (T)0;
     }
     __syncthreads();
     for (int j = threadIdx.y; j < 32; j += 8) {
         const int c = c0 + threadIdx.x, r = r0 + j;
         if (r < rows && c < cols) out[(size_t)r * ldo + c] = t[threadIdx.x][j];
     }
+}
+
+__global__ void k_transpose(int rows, int cols, const double *__restrict__ A, int lda, double *__restrict__ out,
+                            int ldo) {
+    transpose_tile<double>(rows, cols, A, lda, out, ldo);
+}
+
+__global__ void k_transpose_f32(int rows, int cols, const float *__restrict__ A, int lda, float *__restrict__ out,
+                                int ldo) {
+    transpose_tile<float>(rows, cols, A, lda, out, ldo);
 }
 
 int transpose(cuozblasHandle_t *h, int rows, int cols, const double *A, int lda, double *out, int ldo) {
@@ -171,6 +182,130 @@ int transpose(cuozblasHandle_t *h, int rows, int cols, const double *A, int lda,
     k_transpose<<<grid, block, 0, state(h)->stream>>>(rows, cols, A, lda, out, ldo);
     OZB_CHECK(cudaGetLastError());
     return CUOZBLAS_STATUS_SUCCESS;
+}
+
+int transpose_f32(cuozblasHandle_t *h, int rows, int cols, const float *A, int lda, float *out, int ldo) {
+    if (rows == 0 || cols == 0) return CUOZBLAS_STATUS_SUCCESS;
+    dim3 grid((rows + 31) / 32, (cols + 31) / 32), block(32, 8);
+    counted(h);
+    k_transpose_f32<<<grid, block, 0, state(h)->stream>>>(rows, cols, A, lda, out, ldo);
+    OZB_CHECK(cudaGetLastError());
+    return CUOZBLAS_STATUS_SUCCESS;
+}
+
+// ---------------------------------------------------------------------------
+// Float data, FP64 slices: the mixed form <float, double, double>
+// (src/cpu/ozblas_split.cpp:181-221 with TYPE1 = float).  The arithmetic is
+// the reference's float arithmetic: tau = ceil((float)log2((double)max))
+// (tau_rule_f32), sigma = (float)(0.75 * (float)2^(rho+tau) * shift),
+// slice = (r + sigma) - sigma and r -= slice in float, and the slice stored
+// as the double scalbn(slice, -tau) with tau at exps[level * nl + line].
+// rho may be negative (k < 32).  One CTA per line, as k_split_lines; `rem`
+// holds floats.  COUNT: atomicMax(*zmax, z_line).  WRITE: ns slices.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ float sd_sigma(int rho, int tau) {
+    const float p = (float)pow2(rho + tau);  // (float)scalbn(1., rho + tau)
+    return (float)(0.75 * (double)p);
+}
+
+template <bool WRITE>
+__global__ void __launch_bounds__(kSplitThreads) k_split_lines_sd(int k, int nl, const float *__restrict__ X, int ldx,
+                                                                  int rho, int levels, double *__restrict__ out,
+                                                                  int ldo, short *__restrict__ exps,
+                                                                  float *__restrict__ gscratch,
+                                                                  int *__restrict__ zmax) {
+    extern __shared__ float fsmem[];
+    __shared__ double red[kSplitThreads / 32];
+    const int line = blockIdx.x;
+    if (line >= nl) return;
+    float *rem = gscratch ? gscratch + (size_t)line * k : fsmem;
+    const float *x = X + (size_t)line * ldx;
+    float mx = 0.f;
+    for (int i = threadIdx.x; i < k; i += blockDim.x) {
+        const float v = x[i];
+        rem[i] = v;
+        const float av = fabsf(v);
+        mx = (mx < av) ? av : mx;
+    }
+    mx = (float)block_max_nonneg((double)mx, red);  // exact: a max of floats
+    int z = levels;
+    for (int s = 0; s < levels; s++) {
+        const int tau = tau_rule_f32(mx);
+        const float sigma = sd_sigma(rho, tau);
+        float nm = 0.f;
+        double *o = WRITE ? out + ((size_t)s * nl + line) * ldo : nullptr;
+        if (WRITE && threadIdx.x == 0) exps[(size_t)s * nl + line] = (short)tau;
+        for (int i = threadIdx.x; i < k; i += blockDim.x) {
+            float r = rem[i];
+            const float sl = __fsub_rn(__fadd_rn(r, sigma), sigma);
+            r = __fsub_rn(r, sl);
+            rem[i] = r;
+            const float ar = fabsf(r);
+            nm = (nm < ar) ? ar : nm;
+            if (WRITE) o[i] = scalbn((double)sl, -tau);  // exact, and exactly a float
+        }
+        if (WRITE)
+            for (int i = k + threadIdx.x; i < ldo; i += blockDim.x) o[i] = 0.0;
+        mx = (float)block_max_nonneg((double)nm, red);
+        if (!WRITE && mx == 0.f) {
+            z = s;
+            break;
+        }
+    }
+    if (!WRITE && threadIdx.x == 0) atomicMax(zmax, z);
+}
+
+static int launch_split_lines_sd(cuozblasHandle_t *h, bool write, int k, int nl, const float *X, int ldx, int rho,
+                                 int levels, double *out, int ldo, short *exps, int *zmax_dev) {
+    State *st = state(h);
+    float *gscratch = nullptr;
+    size_t smem = 0;
+    Arena ar(h);
+    const uint64_t mk = ar.mark();
+    if (k > 2 * kSplitSmemMaxK) {
+        gscratch = ar.take<float>((uint64_t)k * nl);
+        if (!ar.ok) return CUOZBLAS_STATUS_WORKSPACE;
+    } else {
+        smem = sizeof(float) * (size_t)(k > 0 ? k : 1);
+    }
+    const int maxsmem = (int)(2 * kSplitSmemMaxK * sizeof(float));
+    if (write) {
+        OZB_CHECK(cudaFuncSetAttribute(k_split_lines_sd<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, maxsmem));
+        counted(h);
+        k_split_lines_sd<true><<<nl, kSplitThreads, smem, st->stream>>>(k, nl, X, ldx, rho, levels, out, ldo, exps,
+                                                                         gscratch, nullptr);
+    } else {
+        OZB_CHECK(cudaFuncSetAttribute(k_split_lines_sd<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, maxsmem));
+        counted(h);
+        k_split_lines_sd<false><<<nl, kSplitThreads, smem, st->stream>>>(k, nl, X, ldx, rho, levels, nullptr, 0,
+                                                                          nullptr, gscratch, zmax_dev);
+    }
+    OZB_CHECK(cudaGetLastError());
+    ar.release(mk);
+    return CUOZBLAS_STATUS_SUCCESS;
+}
+
+int split_lines_count_sd(cuozblasHandle_t *h, int k, int nl, const float *X, int ldx, int rho, int maxS, int *ns) {
+    State *st = state(h);
+    if (maxS <= 1 || nl == 0) {
+        *ns = (nl == 0) ? (maxS < 2 ? maxS : 2) : 1;
+        if (maxS <= 1) *ns = 1;
+        return CUOZBLAS_STATUS_SUCCESS;
+    }
+    OZB_CHECK(cudaMemsetAsync(st->d_ints, 0, sizeof(int), st->stream));
+    OZB_TRY(launch_split_lines_sd(h, false, k, nl, X, ldx, rho, maxS - 1, nullptr, 0, nullptr, st->d_ints));
+    OZB_CHECK(cudaMemcpyAsync(st->h_ints, st->d_ints, sizeof(int), cudaMemcpyDeviceToHost, st->stream));
+    OZB_CHECK(cudaStreamSynchronize(st->stream));
+    const int zmax = st->h_ints[0];
+    const int c = (zmax < 1 ? 1 : zmax) + 1;
+    *ns = c < maxS ? c : maxS;
+    return CUOZBLAS_STATUS_SUCCESS;
+}
+
+int split_lines_write_sd(cuozblasHandle_t *h, int k, int nl, const float *X, int ldx, int rho, int ns, double *out,
+                         int ldo, short *exps) {
+    if (nl == 0 || ns == 0) return CUOZBLAS_STATUS_SUCCESS;
+    return launch_split_lines_sd(h, true, k, nl, X, ldx, rho, ns, out, ldo, exps, nullptr);
 }
 
 // ---------------------------------------------------------------------------

@@ -1,11 +1,16 @@
-"""Mixed form <double, float, float> on the GPU vs the CPU oracle: bit-exact.
+"""Mixed forms <double, float, float> and <float, double, double> on the GPU vs the CPU oracle: bit-exact.
 
-FP64 data, FP32 slices (scalbn(slice, -tau) with tau per line and level),
-exact FP32 slice products and the scaled FSum (src/cpu/ozblas_gemm.cpp with
-TYPE2 = TYPE3 = float, src/cpu/ozblas_sum.cpp:382-432).  The oracle's
-restatement of this form is pinned to ozblasRgemm/Rgemv/Rdot/Rnrm2<double,
-float, float> of the reference library by tests/test_oracle.py.  Every call
-goes through the C ABI (cuozblasDSgemm / DSgemv / DSdot / DSnrm2).
+<double, float, float>: FP64 data, FP32 slices (scalbn(slice, -tau) with tau
+per line and level), exact FP32 slice products and the scaled FSum
+(src/cpu/ozblas_gemm.cpp with TYPE2 = TYPE3 = float, src/cpu/ozblas_sum.cpp:382-432),
+through cuozblasDSgemm / DSgemv / DSdot / DSnrm2.
+
+<float, double, double>: float data split in float arithmetic, FP64 slices,
+exact FP64 slice products, each rounded to float, scaled and summed in float
+(TYPE1 = float), through cuozblasSDgemm / SDgemv / SDdot / SDnrm2.
+
+The oracle's restatements of both forms are pinned to the reference library's
+ozblasRgemm/Rgemv/Rdot/Rnrm2 instantiations by tests/test_oracle.py.
 """
 import numpy as np
 import pytest
@@ -156,3 +161,109 @@ def test_mixed_unsupported_flags(handle, ozb, cuda):
     with pytest.raises(ozb.OzblasError) as e:
         ozb.dsdot(handle, 8, x, x, incx=2)
     assert e.value.code == 2
+
+
+# ---- <float, double, double>: float data, FP64 slices, float-scaled sum ----
+
+def f32_bits_equal(a, b):
+    a = np.ascontiguousarray(a, dtype=np.float32)
+    b = np.ascontiguousarray(b, dtype=np.float32)
+    return a.shape == b.shape and np.array_equal(a.view(np.int32), b.view(np.int32))
+
+
+def f32_first_diff(a, b):
+    a = np.ascontiguousarray(a, dtype=np.float32).ravel()
+    b = np.ascontiguousarray(b, dtype=np.float32).ravel()
+    d = np.nonzero(a.view(np.int32) != b.view(np.int32))[0]
+    return None if len(d) == 0 else (int(d[0]), len(d), float(a[d[0]]), float(b[d[0]]))
+
+
+SD_CASES = [
+    # m, n, k, ta, tb, fastMode, nSplitMax, alpha, beta, phi
+    (1, 2, 1, "n", "n", 0, 0, 1.0, 0.0, 1.0),
+    (2, 3, 7, "n", "n", 0, 0, 1.0, 0.0, 1.0),
+    (33, 17, 100, "n", "n", 0, 0, 1.0, 0.0, 1.0),
+    (33, 17, 100, "t", "n", 1, 0, 1.0, 0.0, 4.0),
+    (7, 9, 130, "n", "t", 0, 0, -0.5, 2.0, 2.0),
+    (20, 20, 64, "t", "t", 2, 0, 1.0, 1.0, 2.0),
+    (130, 260, 300, "n", "n", 0, 0, 1.5, -1.0, 4.0),
+    (129, 127, 33, "t", "t", 0, 2, 1.0, 0.0, 4.0),
+    (64, 64, 1, "n", "n", 0, 0, 1.0, 0.0, 0.5),
+    (300, 200, 2000, "n", "t", 0, 0, 1.0, 0.5, 1.0),
+]
+
+
+@pytest.mark.parametrize("case", SD_CASES, ids=lambda c: "x".join(map(str, c[:3])) + f"-{c[3]}{c[4]}-f{c[5]}s{c[6]}")
+def test_sdgemm(case, oracle, handle, ozb, cuda):
+    m, n, k, ta, tb, fm, ns, alpha, beta, phi = case
+    ar, ac = (m, k) if ta == "n" else (k, m)
+    br, bc = (k, n) if tb == "n" else (n, k)
+    A = oracle.phi_matrix(ar, ac, phi, 1).astype(np.float32)
+    B = oracle.phi_matrix(br, bc, phi, 2).astype(np.float32)
+    C0 = oracle.phi_matrix(m, n, 1.0, 3).astype(np.float32)
+    ref, info = oracle.sgemm_d(make_flags(fastMode=fm, nSplitMax=ns), ta, tb, m, n, k, alpha, A, ar, B, br, beta,
+                               C0, m)
+    handle.fastMode, handle.nSplitMax = fm, ns
+    dC = dev(cuda, C0)
+    ozb.sdgemm(handle, ta, tb, m, n, k, alpha, dev(cuda, A), ar, dev(cuda, B), br, beta, dC, m)
+    out = host(dC)
+    assert f32_bits_equal(out, ref), f32_first_diff(out, ref)
+    assert (handle.nSplitA, handle.nSplitB, handle.nSplitC) == (info.nSplitA, info.nSplitB, info.nSplitC)
+
+
+@pytest.mark.parametrize("n,phi,scale", [(1, 1.0, 1.0), (7, 1.0, 1.0), (1000, 2.0, 1.0), (100003, 2.0, 1.0),
+                                         (1 << 20, 1.0, 1.0), (5000, 4.0, 2.0 ** -120), (5000, 1.0, 2.0 ** 60),
+                                         (3000, 1.0, 2.0 ** -140)])
+def test_sddot_sdnrm2(n, phi, scale, oracle, handle, ozb, cuda):
+    x = (oracle.phi_vector(n, phi, 1) * scale).astype(np.float32)
+    y = oracle.phi_vector(n, phi, 2).astype(np.float32)
+    d = ozb.sddot(handle, n, dev(cuda, x), dev(cuda, y))
+    r, info = oracle.sgemm_d(make_flags(), "t", "n", 1, 1, n, 1.0, x, n, y, n, 0.0, np.zeros(1, np.float32), 1)
+    assert f32_bits_equal(np.array([d], np.float32), r), (d, r[0])
+    assert (handle.nSplitA, handle.nSplitB, handle.nSplitC) == (info.nSplitA, info.nSplitB, 1.0)
+    nr = ozb.sdnrm2(handle, n, dev(cuda, x))
+    r2, _ = oracle.sgemm_d(make_flags(), "t", "n", 1, 1, n, 1.0, x, n, x, n, 0.0, np.zeros(1, np.float32), 1)
+    assert f32_bits_equal(np.array([nr], np.float32), np.array([np.sqrt(np.float64(r2[0]))], np.float32))
+
+
+@pytest.mark.parametrize("m,n,trans,fm", [(50, 70, "n", 0), (50, 70, "t", 0), (300, 257, "n", 1), (1, 33, "t", 0),
+                                           (700, 2000, "t", 2)])
+def test_sdgemv(m, n, trans, fm, oracle, handle, ozb, cuda):
+    A = oracle.phi_matrix(m, n, 2.0, 1).astype(np.float32)
+    xl, yl = (n, m) if trans == "n" else (m, n)
+    x = oracle.phi_vector(xl, 2.0, 2).astype(np.float32)
+    y0 = oracle.phi_vector(yl, 1.0, 3).astype(np.float32)
+    f = make_flags(fastMode=fm)
+    if trans == "n":
+        ref, info = oracle.sgemm_d(f, "n", "n", m, 1, n, 0.75, A, m, x, n, 0.5, y0, m)
+    else:
+        ref, info = oracle.sgemm_d(f, "t", "n", n, 1, m, 0.75, A, m, x, m, 0.5, y0, n)
+    handle.fastMode = fm
+    dy = dev(cuda, y0)
+    ozb.sdgemv(handle, trans, m, n, 0.75, dev(cuda, A), m, dev(cuda, x), 0.5, dy)
+    assert f32_bits_equal(host(dy), ref), f32_first_diff(host(dy), ref)
+    assert (handle.nSplitA, handle.nSplitB, handle.nSplitC) == (info.nSplitA, info.nSplitB, info.nSplitC)
+
+
+@pytest.mark.parametrize("scale", [2.0 ** -140, 2.0 ** -70, 2.0 ** 62])
+def test_sd_extreme_magnitudes(scale, oracle, handle, ozb, cuda):
+    """Products scaled into float's subnormal range (the float scaling rounds there) and to its top."""
+    m, n, k = 45, 37, 200
+    A = (oracle.phi_matrix(m, k, 1.0, 1) * scale).astype(np.float32)
+    B = oracle.phi_matrix(k, n, 1.0, 2).astype(np.float32)
+    ref, _ = oracle.sgemm_d(make_flags(), "n", "n", m, n, k, 1.0, A, m, B, k, 0.0, np.zeros((n, m), np.float32), m)
+    dC = cuda.zeros((n, m), dtype=cuda.float32, device="cuda")
+    ozb.sdgemm(handle, "n", "n", m, n, k, 1.0, dev(cuda, A), m, dev(cuda, B), k, 0.0, dC, m)
+    assert f32_bits_equal(host(dC), ref), f32_first_diff(host(dC), ref)
+
+
+def test_sd_unsupported_flags(handle, ozb, cuda):
+    x = cuda.zeros(8, dtype=cuda.float32, device="cuda")
+    handle.sumMode = 1
+    with pytest.raises(ozb.OzblasError) as e:
+        ozb.sdgemm(handle, "n", "n", 2, 2, 2, 1.0, x, 2, x, 2, 0.0, x, 2)
+    assert e.value.code == 4
+    handle.sumMode, handle.splitEpsMode = 0, 2
+    with pytest.raises(ozb.OzblasError) as e:
+        ozb.sddot(handle, 8, x, x)
+    assert e.value.code == 4

@@ -244,6 +244,87 @@ def test_mixed_f32_split_exactness(oracle):
     assert ns > ns64
 
 
+def f32_bits_equal(a, b):
+    a = np.ascontiguousarray(a, dtype=np.float32)
+    b = np.ascontiguousarray(b, dtype=np.float32)
+    return a.shape == b.shape and np.array_equal(a.view(np.int32), b.view(np.int32))
+
+
+@pytest.mark.parametrize("seed", range(12))
+def test_mixed_sd_gemm_vs_reference(seed, oracle, reference):
+    """<float, double, double> (float data split in float arithmetic, FP64 slices, each pair product
+    rounded and scaled in float, float sum): the restatement against ozblasRgemm<float, double,
+    double>, bit-exact with the split counts."""
+    rng = np.random.default_rng(500 + seed)
+    m, n = (int(v) for v in rng.integers(1, 50, 2))
+    k = int(rng.integers(1, 600))
+    if seed == 0:
+        m = n = 1
+    if seed in (1, 2):
+        n = 1
+    ta, tb = rng.choice(["n", "t"]), rng.choice(["n", "t"])
+    fm = int(rng.integers(0, 3))
+    nsplit = int(rng.choice([0, 0, 2, 5]))
+    phi = float(rng.choice([0.5, 1.0, 2.0, 4.0]))
+    ar, ac = (m, k) if ta == "n" else (k, m)
+    br, bc = (k, n) if tb == "n" else (n, k)
+    A = oracle.phi_matrix(ar, ac, phi, 1).astype(np.float32)
+    B = oracle.phi_matrix(br, bc, phi, 2).astype(np.float32)
+    C0 = oracle.phi_matrix(m, n, 1.0, 3).astype(np.float32)
+    out, info = oracle.sgemm_d(make_flags(fastMode=fm, nSplitMax=nsplit), ta, tb, m, n, k, 1.25, A, ar, B, br, -0.5,
+                               C0, m)
+    reference.set_flags(fastMode=fm, nSplitMax=nsplit)
+    gold = reference.sgemm_d(ta, tb, m, n, k, 1.25, A, ar, B, br, -0.5, C0, m)
+    assert f32_bits_equal(out, gold), (seed, m, n, k, ta, tb, fm, nsplit, phi)
+    inf = reference.info()
+    assert [info.nSplitA, info.nSplitB, info.nSplitC] == [inf["nSplitA"], inf["nSplitB"], inf["nSplitC"]]
+
+
+def test_mixed_sd_skinny_vs_reference(oracle, reference):
+    """The <float, double, double> DOT, NRM2 and GEMV, including data scaled near the ends of the
+    float range (the float scaling then rounds or overflows as the reference's does)."""
+    reference.set_flags()
+    f = make_flags()
+    for n, phi, scale in ((1, 1.0, 1.0), (1000, 2.0, 1.0), (100003, 1.0, 1.0), (5000, 4.0, 2.0 ** -120),
+                          (5000, 1.0, 2.0 ** 60), (3000, 1.0, 2.0 ** -140)):
+        x = (oracle.phi_vector(n, phi, 1) * scale).astype(np.float32)
+        y = oracle.phi_vector(n, phi, 2).astype(np.float32)
+        r, _ = oracle.sgemm_d(f, "t", "n", 1, 1, n, 1.0, x, n, y, n, 0.0, np.zeros(1, np.float32), 1)
+        gold = reference.sdot_d(x, y)
+        assert f32_bits_equal(r, np.array([gold], np.float32)), (n, phi, scale, r[0], gold)
+        r2, _ = oracle.sgemm_d(f, "t", "n", 1, 1, n, 1.0, x, n, x, n, 0.0, np.zeros(1, np.float32), 1)
+        nr = np.float32(np.sqrt(np.float64(r2[0])))
+        assert f32_bits_equal(np.array([nr]), np.array([reference.snrm2_d(x)], np.float32))
+    for ta, (m, n) in (("n", (70, 300)), ("t", (300, 70))):
+        A = oracle.phi_matrix(m, n, 2.0, 3).astype(np.float32)
+        xl, yl = (n, m) if ta == "n" else (m, n)
+        x = oracle.phi_vector(xl, 2.0, 4).astype(np.float32)
+        y0 = oracle.phi_vector(yl, 1.0, 5).astype(np.float32)
+        if ta == "n":
+            out, _ = oracle.sgemm_d(f, "n", "n", m, 1, n, 0.75, A, m, x, n, 1.5, y0, m)
+        else:
+            out, _ = oracle.sgemm_d(f, "t", "n", n, 1, m, 0.75, A, m, x, m, 1.5, y0, n)
+        gold = reference.sgemv_d(ta, m, n, 0.75, A, m, x, 1.5, y0)
+        assert f32_bits_equal(out, gold), ta
+
+
+def test_tau_of_float_data_vs_reference(oracle, reference):
+    """The restatement's float tau, (short)ceil((float)log2((double)v)), against the reference's
+    log21<float> on every binary exponent (mantissas 0..400 and the top ones) and random floats."""
+    import math
+    vals = []
+    for e in range(-149, 128):
+        for j in list(range(0, 400)) + [4095, (1 << 22), (1 << 23) - 1]:
+            if e >= -126:
+                vals.append(math.ldexp(1.0 + j * 2.0 ** -23, e))
+            elif j % (1 << min(-126 - e, 30)) == 0:
+                vals.append(math.ldexp(1.0 + j * 2.0 ** -23, e))
+    rng = np.random.default_rng(3)
+    vals += list(rng.integers(1, 0x7F800000, 20000, dtype=np.int64).astype(np.uint32).view(np.float32).astype(float))
+    bad = [v for v in vals if oracle.tau_sd_libm(v) != math.ceil(reference.log21f(v))]
+    assert not bad, bad[:5]
+
+
 def test_split_slices_vs_reference(oracle, reference):
     """Slice-level parity of the column-panel and CSR splits."""
     for phi, k, ncol in [(1.0, 100, 7), (4.0, 333, 5), (2.0, 1, 3), (1.0, 64, 1)]:

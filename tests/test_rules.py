@@ -69,3 +69,24 @@ def test_rho_rule(lib, oracle, mode):
     bad = [(d, lib.cuozblasRuleRho(d, mode), oracle.rho(d, mode)) for d in dims
            if lib.cuozblasRuleRho(d, mode) != oracle.rho(d, mode)]
     assert not bad, bad[:10]
+
+
+def test_tau_of_float_data_sweep(lib, oracle):
+    """The library's integer float tau rule (the device code, exported as cuozblasRuleTauF32) against
+    (short)ceil((float)log2((double)v)) on every 61st positive finite float bit pattern, plus every
+    exponent's first 400 mantissas through the per-value entry point."""
+    import ctypes
+    addr = ctypes.cast(lib.cuozblasRuleTauF32, ctypes.c_void_p).value
+    bad, first = oracle.tau_sd_sweep(addr, 61)
+    assert bad == 0, (bad, hex(first))
+    lib.cuozblasRuleTauF32.argtypes = [ctypes.c_float]
+    lib.cuozblasRuleTauF32.restype = ctypes.c_int
+    mism = []
+    for e in range(-149, 128):
+        for j in range(0, 400):
+            if e < -126 and j % (1 << min(-126 - e, 30)):
+                continue
+            v = math.ldexp(1.0 + j * 2.0 ** -23, e)
+            if lib.cuozblasRuleTauF32(v) != oracle.tau_sd_libm(v):
+                mism.append((e, j))
+    assert not mism, mism[:10]
