@@ -190,6 +190,9 @@ def main():
     ap.add_argument("--cg-iters", type=int, default=2000, help="CG iterations of the memory-only run")
     ap.add_argument("--batched-only", action="store_true",
                     help="only the 256-problem grouped INT8 measurement (prints its JSON)")
+    ap.add_argument("--mixed-only", action="store_true",
+                    help="only the mixed-precision forms <double,float,float> and <float,double,double> at m = n = k "
+                         "= --n (prints their JSON)")
     args = ap.parse_args()
     globals()["N_DIM"] = args.n
     args.warmup = max(args.warmup, 3)
@@ -211,6 +214,12 @@ def main():
         h = ozb.Handle(work_bytes=24 << 30)
         print(json.dumps({"workload": "batched uneven Ozaki DGEMM, 256 problems", "reps": args.steps,
                           "extras": batched_extras(ozb, h, torch, reps=args.steps)}))
+        h.close()
+        return 0
+    if args.mixed_only:
+        h = ozb.Handle(work_bytes=32 << 30)
+        print(json.dumps({"workload": f"mixed-precision Ozaki GEMM {args.n}^3, phi = {PHI}", "reps": args.steps,
+                          "extras": mixed_extras(ozb, h, torch, args.n, reps=args.steps)}))
         h.close()
         return 0
     if args.memory_only:
@@ -481,6 +490,42 @@ def batched_extras(ozb, h, torch, reps=3):
                                                "entries": sum(m * n for m, n, *_ in probs),
                                                "worst_int8": w_i8, "worst_fsum": w_fs}
     out["speedup_grouped_full_vs_plain_looped"] = ms_p / out["int8_grouped_full"]["ms"]
+    return out
+
+
+def mixed_extras(ozb, h, torch, n, reps=3):
+    """The two mixed forms through the public API on an n^3 phi problem: call time (CUDA events),
+    slice counts, and the slice-product throughput of the product kernel (its phase timer)."""
+    out = {}
+    A64 = torch.from_numpy(phi_matrix(n, n, PHI, 1)).cuda()
+    B64 = torch.from_numpy(phi_matrix(n, n, PHI, 2)).cuda()
+    forms = (("dsgemm", ozb.dsgemm, A64, B64, torch.float64),
+             ("sdgemm", ozb.sdgemm, A64.float(), B64.float(), torch.float32))
+    # FP32 SIMT nominal: 148 SMs x 128 lanes x 2 flops at the maximum SM clock
+    fp32_nominal = 148 * 128 * 2 * measured_peaks()[0].get("sm_max_mhz", 1965.0) * 1e6 / 1e12
+    for name, fn, A, B, dt in forms:
+        C = torch.zeros((n, n), dtype=dt, device="cuda")
+        fn(h, "n", "n", n, n, n, 1.0, A, n, B, n, 0.0, C, n)
+        torch.cuda.synchronize()
+        ts, comp = [], []
+        for _ in range(max(reps, 1)):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            fn(h, "n", "n", n, n, n, 1.0, A, n, B, n, 0.0, C, n)
+            e1.record()
+            torch.cuda.synchronize()
+            ts.append(e0.elapsed_time(e1))
+            comp.append(h.t_comp * 1e3)
+        ms, kms = min(ts), min(comp)
+        pairs = h.nSplitC
+        rec = {"ms": ms, "product_kernel_ms": kms, "slices": [h.nSplitA, h.nSplitB], "pairs": pairs,
+               "dgemm_equivalent_TFLOPS": 2.0 * n ** 3 / ms / 1e9,
+               "slice_product_TFLOPS": 2.0 * n ** 3 * pairs / kms / 1e9}
+        if name == "dsgemm":
+            rec["fp32_simt_nominal_TFLOPS"] = fp32_nominal
+            rec["fraction_of_fp32_nominal"] = rec["slice_product_TFLOPS"] / fp32_nominal
+        out[name] = rec
+        del C
     return out
 
 

@@ -214,6 +214,22 @@ int cuozblasSDdot(cuozblasHandle_t *h, int32_t n, const float *x, int32_t incx, 
                   float *ret);
 int cuozblasSDnrm2(cuozblasHandle_t *h, int32_t n, const float *x, int32_t incx, float *ret);
 
+/* Quad I/O form <__float128,double,double> (the reference's CPU instantiation,
+ * src/cpu/ozblas_gemm.cpp:316, with src/cpu/ozblas_dot.cpp, ozblas_nrm2.cpp,
+ * ozblas_gemv.cpp): binary128 data and results, FP64 slices and exact FP64
+ * slice products, the ordered sum and fmaq(alpha, t, beta C) in binary128.
+ * Arrays hold 16-byte IEEE binary128 values (the x86-64 __float128 layout);
+ * alpha, beta and *ret are host pointers to one such value.  Bit-identical to
+ * the reference CPU library; sumMode 0 only.  (The reference needs MPLAPACK
+ * to split a one-column panel, i.e. for DOT, NRM2, GEMV and m or n = 1.) */
+int cuozblasQgemm(cuozblasHandle_t *h, char transa, char transb, int32_t m, int32_t n, int32_t k, const void *alpha,
+                  const void *A, int32_t lda, const void *B, int32_t ldb, const void *beta, void *C, int32_t ldc);
+int cuozblasQgemv(cuozblasHandle_t *h, char trans, int32_t m, int32_t n, const void *alpha, const void *A,
+                  int32_t lda, const void *x, int32_t incx, const void *beta, void *y, int32_t incy);
+int cuozblasQdot(cuozblasHandle_t *h, int32_t n, const void *x, int32_t incx, const void *y, int32_t incy,
+                 void *ret);
+int cuozblasQnrm2(cuozblasHandle_t *h, int32_t n, const void *x, int32_t incx, void *ret);
+
 /* INT8 precision form (no reference implementation; the reference stubs it
  * at src/cuda/cuozblas_gemm.cu:292 and src/cuda/cuozblas_blas_wrapper.cu:147-208):
  * INT8 slices on tcgen05 tensor cores with INT32 accumulation.
@@ -257,6 +273,11 @@ int cuozblasDgemmI8Static(char transa, char transb, int32_t m, int32_t n, int32_
 int cuozblasRuleTau(double v);
 /* tau of float data for the <float,double,double> form: (short)ceil((float)log2((double)v)) */
 int cuozblasRuleTauF32(float v);
+/* The software binary128 of the quad form, on the host: op 0 *out = *a + *b,
+ * 1 *a * *b, 2 fma(*a, *b, *c), 3 (int) tau of *a, 4 the split of *a with
+ * (int) rho, tau at b (out: remainder, then the slice as a double),
+ * 5 (double)*a * 2^(int)*b.  Values are 16-byte IEEE binary128. */
+int cuozblasRuleQ128(int op, const void *a, const void *b, const void *c, void *out);
 int cuozblasRuleRho(int32_t dim, int32_t splitEpsMode);
 /* Certified fast path of the correctly rounded sum (the NearSum result when it
  * returns 1; 0: not proven, the library then runs NearSum itself). */

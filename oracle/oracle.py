@@ -107,6 +107,26 @@ class Restatement:
         L.oz_sgemm_d.restype = C.c_int
         L.oz_sgemm_d.argtypes = [F, C.c_char, C.c_char, C.c_int, C.c_int, C.c_int, C.c_float, _fp, C.c_int, _fp,
                                  C.c_int, C.c_float, _fp, C.c_int, I]
+        _vp = C.c_void_p
+        L.oz_rho_q.restype = C.c_int
+        L.oz_rho_q.argtypes = [C.c_int, C.c_int]
+        L.oz_tau_q_libm.restype = C.c_int
+        L.oz_tau_q_libm.argtypes = [_vp]
+        L.oz_split_cols_q.restype = C.c_int
+        L.oz_split_cols_q.argtypes = [F, C.c_int, C.c_int, _vp, C.c_int, _dp, C.c_int, C.POINTER(C.c_short)]
+        L.oz_qgemm_d.restype = C.c_int
+        L.oz_qgemm_d.argtypes = [F, C.c_char, C.c_char, C.c_int, C.c_int, C.c_int, _vp, _vp, C.c_int, _vp, C.c_int,
+                                 _vp, _vp, C.c_int, I]
+        L.oz_gen_phi_q.argtypes = [C.c_int, C.c_int, C.c_int, _vp, C.c_double, C.c_int]
+        for nm in ("oz_q_add", "oz_q_mul"):
+            getattr(L, nm).argtypes = [_vp, _vp, _vp]
+        L.oz_q_fma.argtypes = [_vp, _vp, _vp, _vp]
+        L.oz_q_scale.argtypes = [_vp, C.c_long, C.c_int]
+        L.oz_q_from_double.argtypes = [C.c_double, _vp]
+        L.oz_q128_check.restype = C.c_long
+        L.oz_q128_check.argtypes = [_vp, C.c_int, C.c_long, C.c_uint, _vp]
+        L.oz_q_to_double.restype = C.c_double
+        L.oz_q_to_double.argtypes = [_vp]
         L.oz_split_rows_csr.restype = C.c_int
         L.oz_split_rows_csr.argtypes = [F, C.c_int, _dp, _ip, C.c_int, _dp, C.c_int]
         L.oz_nearsum.restype = C.c_double
@@ -253,6 +273,70 @@ class Restatement:
                               beta, _f(Cc), ldc, C.byref(info))
         return (Cc, info) if r == 0 else (None, None)
 
+    # ---- quad I/O form: binary128 arrays are uint64 arrays with a last axis (lo, hi) ----
+    def rho_q(self, dim, mode=0):
+        return self.L.oz_rho_q(dim, mode)
+
+    def tau_q_libm(self, v):
+        v = np.ascontiguousarray(v, dtype=np.uint64)
+        return self.L.oz_tau_q_libm(v.ctypes.data)
+
+    def phi_matrix_q(self, m, n, phi, seed, ld=None):
+        ld = ld or m
+        a = np.zeros((n, ld, 2), dtype=np.uint64)
+        self.L.oz_gen_phi_q(m, n, ld, a.ctypes.data, phi, seed)
+        return a
+
+    def phi_vector_q(self, n, phi, seed):
+        v = np.zeros((max(n, 1), 2), dtype=np.uint64)
+        self.L.oz_gen_phi_q(n, 1, n, v.ctypes.data, phi, seed)
+        return v[:n]
+
+    def q(self, d):
+        """binary128 of a double (exact)."""
+        r = np.zeros(2, dtype=np.uint64)
+        self.L.oz_q_from_double(float(d), r.ctypes.data)
+        return r
+
+    def q_scale(self, x, e):
+        """Copy of a binary128 array scaled by 2^e (scalbnq)."""
+        y = np.array(x, dtype=np.uint64, copy=True)
+        self.L.oz_q_scale(y.ctypes.data, y.size // 2, e)
+        return y
+
+    def q_to_double(self, v):
+        v = np.ascontiguousarray(v, dtype=np.uint64)
+        return self.L.oz_q_to_double(v.ctypes.data)
+
+    def q_op(self, op, a, b, c=None):
+        a = np.ascontiguousarray(a, dtype=np.uint64)
+        b = np.ascontiguousarray(b, dtype=np.uint64)
+        r = np.zeros(2, dtype=np.uint64)
+        if op == "fma":
+            c = np.ascontiguousarray(c, dtype=np.uint64)
+            self.L.oz_q_fma(a.ctypes.data, b.ctypes.data, c.ctypes.data, r.ctypes.data)
+        else:
+            getattr(self.L, "oz_q_" + op)(a.ctypes.data, b.ctypes.data, r.ctypes.data)
+        return r
+
+    def q128_check(self, rule_addr, op, n, seed=1):
+        """Mismatches of a software binary128 rule against __float128 / libquadmath (see ozoracle.c)."""
+        first = np.zeros(10, dtype=np.uint64)
+        bad = self.L.oz_q128_check(rule_addr, op, n, seed, first.ctypes.data)
+        return bad, first
+
+    def qgemm_d(self, flags, ta, tb, m, n, k, alpha, A, lda, B, ldb, beta, C_, ldc):
+        """GEMM <__float128, double, double> (FSum only); (C, info), or (None, None) for unsupported flags."""
+        info = Info()
+        A = np.ascontiguousarray(A, dtype=np.uint64)
+        B = np.ascontiguousarray(B, dtype=np.uint64)
+        al = np.ascontiguousarray(alpha, dtype=np.uint64)
+        be = np.ascontiguousarray(beta, dtype=np.uint64)
+        Cc = np.array(C_, dtype=np.uint64, copy=True)
+        r = self.L.oz_qgemm_d(C.byref(flags), ta.encode(), tb.encode(), m, n, k, al.ctypes.data, A.ctypes.data, lda,
+                              B.ctypes.data, ldb, be.ctypes.data, Cc.ctypes.data, ldc, C.byref(info))
+        return (Cc, info) if r == 0 else (None, None)
+
     def split_csr(self, flags, val, rowptr, shift=1):
         m = len(rowptr) - 1
         nnz = len(val)
@@ -365,6 +449,12 @@ class Reference:
                                   C.c_float, _fp]
         L.ref_log21f.restype = C.c_float
         L.ref_log21f.argtypes = [C.c_float]
+        L.ref_qgemm_d.argtypes = [C.c_void_p, C.c_char, C.c_char, C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_void_p,
+                                  C.c_int, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_int]
+        L.ref_qdot_d.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p]
+        L.ref_qnrm2_d.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p]
+        L.ref_tau_q.restype = C.c_int
+        L.ref_tau_q.argtypes = [C.c_void_p]
         L.ref_ddot.restype = C.c_double
         L.ref_ddot.argtypes = [C.c_void_p, C.c_int, _dp, _dp]
         L.ref_dnrm2.restype = C.c_double
@@ -454,6 +544,34 @@ class Reference:
 
     def log21f(self, v):
         return self.L.ref_log21f(v)
+
+    def qgemm_d(self, ta, tb, m, n, k, alpha, A, lda, B, ldb, beta, C_, ldc):
+        """ozblasRgemm<__float128, double, double> on 16-byte binary128 arrays (uint64 pairs)."""
+        A = np.ascontiguousarray(A, dtype=np.uint64)
+        B = np.ascontiguousarray(B, dtype=np.uint64)
+        al = np.ascontiguousarray(alpha, dtype=np.uint64)
+        be = np.ascontiguousarray(beta, dtype=np.uint64)
+        Cc = np.array(C_, dtype=np.uint64, copy=True)
+        self.L.ref_qgemm_d(self.h, ta.encode(), tb.encode(), m, n, k, al.ctypes.data, A.ctypes.data, lda,
+                           B.ctypes.data, ldb, be.ctypes.data, Cc.ctypes.data, ldc)
+        return Cc
+
+    def qdot_d(self, x, y):
+        x = np.ascontiguousarray(x, dtype=np.uint64)
+        y = np.ascontiguousarray(y, dtype=np.uint64)
+        r = np.zeros(2, dtype=np.uint64)
+        self.L.ref_qdot_d(self.h, len(x), x.ctypes.data, y.ctypes.data, r.ctypes.data)
+        return r
+
+    def qnrm2_d(self, x):
+        x = np.ascontiguousarray(x, dtype=np.uint64)
+        r = np.zeros(2, dtype=np.uint64)
+        self.L.ref_qnrm2_d(self.h, len(x), x.ctypes.data, r.ctypes.data)
+        return r
+
+    def tau_q(self, v):
+        v = np.ascontiguousarray(v, dtype=np.uint64)
+        return self.L.ref_tau_q(v.ctypes.data)
 
     def ddot_f32(self, x, y):
         return self.L.ref_ddot_f32(self.h, len(x), _d(x), _d(y))

@@ -19,6 +19,7 @@
 #include <stdio.h>
 #include <stdlib.h>
 #include <string.h>
+#include <quadmath.h>
 
 #define OZ_DEFAULT_MAXSPLIT 30 /* NumSplitDefaultMax, src/cpu/ozblas_common.h:5 */
 #define OZ_SPLIT_CONST 0.75    /* CONST, src/cpu/ozblas_split.cpp:9 */
@@ -386,6 +387,307 @@ int oz_sgemm_d(const oz_flags *f, char ta, char tb, int m, int n, int k, float a
     free(pa);
     free(pb);
     return 0;
+}
+
+/* ------------------------------------------------------------------------ */
+/* Quad I/O form <__float128, double, double>: FP64 slices of binary128 data */
+/* ------------------------------------------------------------------------ */
+
+/* getRho<__float128,double>, src/cpu/ozblas_split.cpp:19-34 (epse 113 and 53) */
+int oz_rho_q(int dim, int splitEpsMode) {
+    switch (splitEpsMode) {
+    case 9: return (int)ceil((113 - (53 - log2(2. * sqrt(dim))) / 2));
+    default: return (int)ceil((113 - (53 - log2(1. * dim)) / 2));
+    }
+}
+
+/* tau of binary128 data: ceil(log21(max)) in the reference resolves to the double ceil of the
+ * binary128 log2q converted to double (src/cpu/ozblas_split.cpp:201, ozblas_aux.cpp:43-46) */
+static short tau_q(__float128 v) { return (short)ceil((double)log2q(v)); }
+int oz_tau_q_libm(const void *v) {
+    __float128 x;
+    memcpy(&x, v, 16);
+    return tau_q(x);
+}
+
+static double split_level_cols_q(int k, int ncol, int rho, __float128 *R, int ldr, double *S, int lds, short *E,
+                                 __float128 *mx, int shift) {
+    __float128 check = 0;
+    for (int j = 0; j < ncol; j++) {
+        const short tau = tau_q(mx[j]);
+        E[j] = tau;
+        const __float128 sigma = (__float128)OZ_SPLIT_CONST * scalbnq(1, rho + tau) * shift;
+        __float128 m = 0;
+        for (int i = 0; i < k; i++) {
+            __float128 x = R[(size_t)j * ldr + i];
+            const __float128 s = (x + sigma) - sigma;
+            x = x - s;
+            S[(size_t)j * lds + i] = (double)scalbnq(s, -tau);
+            R[(size_t)j * ldr + i] = x;
+            const __float128 ax = fabsq(x);
+            m = (m < ax) ? ax : m;
+        }
+        mx[j] = m;
+        check += m;
+    }
+    return check == 0 ? 0. : 1.;
+}
+
+int oz_split_cols_q(const oz_flags *f, int k, int ncol, const void *Xv, int ldx, double *slices, int lds,
+                    short *exps) {
+    const __float128 *X = (const __float128 *)Xv;
+    const int rho = oz_rho_q(k, f->splitEpsMode);
+    const int maxS = oz_max_split(f);
+    __float128 *R = (__float128 *)malloc(sizeof(__float128) * (size_t)(k > 0 ? k : 1) * (ncol > 0 ? ncol : 1));
+    __float128 *mx = (__float128 *)malloc(sizeof(__float128) * (ncol > 0 ? ncol : 1));
+    for (int j = 0; j < ncol; j++) {
+        __float128 m = 0;
+        for (int i = 0; i < k; i++) {
+            R[(size_t)j * k + i] = X[(size_t)j * ldx + i];
+            const __float128 ax = fabsq(X[(size_t)j * ldx + i]);
+            m = (m < ax) ? ax : m;
+        }
+        mx[j] = m;
+    }
+    split_level_cols_q(k, ncol, rho, R, k, slices, lds, exps, mx, 1);
+    int s = 1;
+    while (s < maxS) {
+        const double c = split_level_cols_q(k, ncol, rho, R, k, slices + (size_t)s * lds * ncol, lds,
+                                            exps + (size_t)s * ncol, mx, 1);
+        s++;
+        if (c == 0.) break;
+    }
+    free(R);
+    free(mx);
+    return s;
+}
+
+/*
+ * GEMM <__float128, double, double>, src/cpu/ozblas_gemm.cpp:3-316 with TYPE1 = __float128:
+ * exact FP64 slice products; the ordered sum adds scalbnq(product, tauA + tauB) in binary128
+ * (src/cpu/ozblas_sum.cpp:382-432); the output is fmaq(alpha, t, beta * C).  FSum only.
+ * A, B, C, alpha and beta are binary128 (16 bytes each, x86-64 layout).
+ */
+int oz_qgemm_d(const oz_flags *f, char ta, char tb, int m, int n, int k, const void *alphav, const void *Av, int lda,
+               const void *Bv, int ldb, const void *betav, void *Cv, int ldc, oz_info *info) {
+    if (f->reproMode != 1 || f->sumMode != 0 || (f->splitEpsMode != 0 && f->splitEpsMode != 9)) return -1;
+    const __float128 *A = (const __float128 *)Av, *B = (const __float128 *)Bv;
+    __float128 *C = (__float128 *)Cv, alpha, beta;
+    memcpy(&alpha, alphav, 16);
+    memcpy(&beta, betav, 16);
+    const int is_dot = (m == 1 && n == 1);
+    const int fast = is_dot ? 0 : f->fastMode;
+    const int maxS = oz_max_split(f);
+    const int kk = k > 0 ? k : 1;
+    __float128 *Ap = (__float128 *)malloc(sizeof(__float128) * (size_t)kk * imax(m, 1));
+    __float128 *Bp = (__float128 *)malloc(sizeof(__float128) * (size_t)kk * imax(n, 1));
+    const int tA = !(ta == 'n' || ta == 'N'), tB = !(tb == 'n' || tb == 'N');
+    for (int i = 0; i < m; i++)
+        for (int l = 0; l < k; l++) Ap[(size_t)i * k + l] = tA ? A[(size_t)i * lda + l] : A[(size_t)l * lda + i];
+    for (int j = 0; j < n; j++)
+        for (int l = 0; l < k; l++) Bp[(size_t)j * k + l] = tB ? B[(size_t)l * ldb + j] : B[(size_t)j * ldb + l];
+    double *Sa = (double *)calloc((size_t)(maxS + 1) * kk * imax(m, 1), sizeof(double));
+    double *Sb = (double *)calloc((size_t)(maxS + 1) * kk * imax(n, 1), sizeof(double));
+    short *Ea = (short *)calloc((size_t)(maxS + 1) * imax(m, 1), sizeof(short));
+    short *Eb = (short *)calloc((size_t)(maxS + 1) * imax(n, 1), sizeof(short));
+    const int nA = oz_split_cols_q(f, k, m, Ap, k, Sa, k, Ea);
+    const int nB = oz_split_cols_q(f, k, n, Bp, k, Sb, k, Eb);
+    int maxlevel = (nA - 1) + (nB - 1);
+    maxlevel = imax(maxlevel - fast, imin(nA - 1, nB - 1));
+    int *pa = (int *)malloc(sizeof(int) * nA * nB), *pb = (int *)malloc(sizeof(int) * nA * nB);
+    const int np = make_pairs(nA, nB, maxlevel, pa, pb);
+    for (int j = 0; j < n; j++)
+        for (int i = 0; i < m; i++) {
+            __float128 t = 0;
+            for (int p = 0; p < np; p++) {
+                const double *a = Sa + (size_t)pa[p] * k * m + (size_t)i * k;
+                const double *b = Sb + (size_t)pb[p] * k * n + (size_t)j * k;
+                double c = 0.;
+                for (int l = 0; l < k; l++) c += a[l] * b[l]; /* exact in FP64 */
+                t += scalbnq((__float128)c, Ea[(size_t)pa[p] * m + i] + Eb[(size_t)pb[p] * n + j]);
+            }
+            __float128 *cc = &C[(size_t)j * ldc + i];
+            *cc = fmaq(alpha, t, beta * *cc);
+        }
+    if (info) {
+        info->nSplitA = (float)nA;
+        info->nSplitB = (float)nB;
+        if (is_dot)
+            info->nSplitC = 1.f;
+        else if (n == 1 && fast == 0)
+            info->nSplitC = (float)imin(maxlevel + 1, nA);
+        else
+            info->nSplitC = (float)np;
+    }
+    free(Ap);
+    free(Bp);
+    free(Sa);
+    free(Sb);
+    free(Ea);
+    free(Eb);
+    free(pa);
+    free(pb);
+    return 0;
+}
+
+/* Binary128 test data: the harness's phi distribution in double, widened with a second draw
+ * below its last bit so that every value uses about 107 of the 113 bits. */
+void oz_gen_phi_q(int m, int n, int ld, void *outv, double phi, int seed) {
+    __float128 *out = (__float128 *)outv;
+    double *a = (double *)malloc(sizeof(double) * (size_t)(ld > 0 ? ld : 1) * (n > 0 ? n : 1));
+    double *b = (double *)malloc(sizeof(double) * (size_t)(ld > 0 ? ld : 1) * (n > 0 ? n : 1));
+    oz_gen_phi(m, n, ld, a, phi, seed);
+    oz_gen_phi(m, n, ld, b, 1.0, seed + 7919);
+    for (int j = 0; j < n; j++)
+        for (int i = 0; i < m; i++) {
+            const size_t q = (size_t)j * ld + i;
+            out[q] = (__float128)a[q] * (1 + (__float128)b[q] * 0x1p-54Q);
+        }
+    free(a);
+    free(b);
+}
+
+/* x[i] = scalbnq(x[i], e) over n binary128 values (test data near the ends of the range) */
+void oz_q_scale(void *xv, long n, int e) {
+    __float128 *x = (__float128 *)xv;
+    for (long i = 0; i < n; i++) x[i] = scalbnq(x[i], e);
+}
+
+/* Reference binary128 arithmetic for the tests of the library's software binary128 */
+void oz_q_add(const void *a, const void *b, void *r) {
+    __float128 x, y, z;
+    memcpy(&x, a, 16);
+    memcpy(&y, b, 16);
+    z = x + y;
+    memcpy(r, &z, 16);
+}
+void oz_q_mul(const void *a, const void *b, void *r) {
+    __float128 x, y, z;
+    memcpy(&x, a, 16);
+    memcpy(&y, b, 16);
+    z = x * y;
+    memcpy(r, &z, 16);
+}
+void oz_q_fma(const void *a, const void *b, const void *c, void *r) {
+    __float128 x, y, w, z;
+    memcpy(&x, a, 16);
+    memcpy(&y, b, 16);
+    memcpy(&w, c, 16);
+    z = fmaq(x, y, w);
+    memcpy(r, &z, 16);
+}
+void oz_q_from_double(double d, void *r) {
+    __float128 z = d;
+    memcpy(r, &z, 16);
+}
+double oz_q_to_double(const void *a) {
+    __float128 x;
+    memcpy(&x, a, 16);
+    return (double)x;
+}
+
+/* Bulk check of a software binary128 `rule` (the library's cuozblasRuleQ128) against gcc's
+ * __float128 and libquadmath on n random cases of operation op (0 add, 1 mul, 2 fma, 3 tau,
+ * 4 split); returns the number of mismatches, the first one's inputs and outputs in `first`
+ * (a, b, c, got, want: 5 x 16 bytes).  Operands mix random signs and exponents, close
+ * exponents (cancellation), short significands (ties), zeros and subnormals. */
+static unsigned long long q_rng_state;
+static unsigned long long q_rng(void) {
+    q_rng_state ^= q_rng_state << 13;
+    q_rng_state ^= q_rng_state >> 7;
+    q_rng_state ^= q_rng_state << 17;
+    return q_rng_state;
+}
+static __float128 q_rand(int e0, int spread) {
+    unsigned long long r = q_rng();
+    const int kind = (int)(r % 16);
+    if (kind == 0) return (r & 16) ? -0.0Q : 0.0Q;
+    unsigned __int128 m = ((unsigned __int128)q_rng() << 64) | q_rng();
+    m &= (((unsigned __int128)1) << 112) - 1;
+    if (kind <= 3) m &= ~((((unsigned __int128)1) << (int)(q_rng() % 112)) - 1); /* short significand */
+    int e = e0 + (spread ? (int)(q_rng() % (unsigned)(2 * spread + 1)) - spread : 0);
+    if (kind == 4) e = -16382 - 1 - (int)(q_rng() % 112); /* subnormal */
+    if (e < -16494) e = -16494;
+    if (e > 16383) e = 16383;
+    __float128 v;
+    if (e >= -16382) {
+        unsigned long long hi = (unsigned long long)(e + 16383) << 48 | (unsigned long long)(m >> 64);
+        unsigned long long lo = (unsigned long long)m;
+        memcpy(&v, &lo, 8);
+        memcpy((char *)&v + 8, &hi, 8);
+    } else {
+        v = scalbnq(1 + (__float128)(double)(m >> 60) * 0x1p-52Q, e);
+    }
+    return (r & 32) ? -v : v;
+}
+long oz_q128_check(int (*rule)(int, const void *, const void *, const void *, void *), int op, long n,
+                   unsigned seed, void *first) {
+    q_rng_state = 0x9E3779B97F4A7C15ULL ^ seed;
+    long bad = 0;
+    for (long t = 0; t < n; t++) {
+        const int base = (int)(q_rng() % 4) == 0 ? (int)(q_rng() % 32000) - 16000 : (int)(q_rng() % 200) - 100;
+        const int spread = (int)(q_rng() % 4) == 0 ? 200 : (int)(q_rng() % 3);
+        __float128 a = q_rand(base, spread), b = q_rand(base, spread), c = q_rand(base, spread), want = 0, got = 0;
+        int rt[2];
+        unsigned char outb[32];
+        memset(outb, 0, sizeof outb);
+        if (op == 2) c = q_rand(base + (int)(q_rng() % 200) - 100, spread); /* c near a * b's binade or not */
+        if (op == 0) want = a + b;
+        if (op == 1) want = a * b;
+        if (op == 2) want = fmaq(a, b, c);
+        if (op == 3) {
+            a = fabsq(a);
+            if (a == 0) a = 1;
+            const int w = tau_q(a);
+            memcpy(&want, &w, sizeof w);
+        }
+        if (op == 4) {
+            const __float128 mx = fabsq(a) * (1 + (__float128)(q_rng() % 4));
+            rt[0] = 87 + (int)(q_rng() % 20);
+            rt[1] = (mx == 0) ? 0 : tau_q(mx);
+            const __float128 sigma = (__float128)OZ_SPLIT_CONST * scalbnq(1, rt[0] + rt[1]);
+            const __float128 sp = (a + sigma) - sigma;
+            const __float128 rem = a - sp;
+            const double sl = (double)scalbnq(sp, -rt[1]);
+            memcpy(&want, &rem, 16);
+            b = 0;
+            memcpy(&b, rt, sizeof rt);
+            unsigned char wantb[32];
+            memcpy(wantb, &rem, 16);
+            memcpy(wantb + 16, &sl, 8);
+            memset(wantb + 24, 0, 8);
+            rule(op, &a, rt, &c, outb);
+            if (memcmp(outb, wantb, 24) != 0) {
+                if (bad == 0 && first) {
+                    memcpy(first, &a, 16);
+                    memcpy((char *)first + 16, rt, 8);
+                    memcpy((char *)first + 48, outb, 24);
+                    memcpy((char *)first + 72, wantb, 8); /* truncated record: inputs + outputs */
+                }
+                bad++;
+            }
+            continue;
+        }
+        if (op == 3) {
+            int g = 0;
+            rule(op, &a, &b, &c, &g);
+            memcpy(&got, &g, sizeof g);
+        } else {
+            rule(op, &a, &b, &c, &got);
+        }
+        const int wnan = (op <= 2) && isnanq(want), gnan = (op <= 2) && isnanq(got);
+        if (wnan ? !gnan : memcmp(&got, &want, 16) != 0) {
+            if (bad == 0 && first) {
+                memcpy(first, &a, 16);
+                memcpy((char *)first + 16, &b, 16);
+                memcpy((char *)first + 32, &c, 16);
+                memcpy((char *)first + 48, &got, 16);
+                memcpy((char *)first + 64, &want, 16);
+            }
+            bad++;
+        }
+    }
+    return bad;
 }
 
 /*

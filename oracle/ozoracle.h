@@ -42,6 +42,20 @@ typedef struct {
 int oz_rho(int dim, int splitEpsMode);
 int oz_rho_f32(int dim, int splitEpsMode);
 int oz_rho_sd(int dim, int splitEpsMode);
+int oz_rho_q(int dim, int splitEpsMode);
+int oz_tau_q_libm(const void *v);
+int oz_split_cols_q(const oz_flags *f, int k, int ncol, const void *X, int ldx, double *slices, int lds, short *exps);
+int oz_qgemm_d(const oz_flags *f, char ta, char tb, int m, int n, int k, const void *alpha, const void *A, int lda,
+               const void *B, int ldb, const void *beta, void *C, int ldc, oz_info *info);
+void oz_gen_phi_q(int m, int n, int ld, void *out, double phi, int seed);
+void oz_q_scale(void *x, long n, int e);
+void oz_q_add(const void *a, const void *b, void *r);
+void oz_q_mul(const void *a, const void *b, void *r);
+void oz_q_fma(const void *a, const void *b, const void *c, void *r);
+void oz_q_from_double(double d, void *r);
+double oz_q_to_double(const void *a);
+long oz_q128_check(int (*rule)(int, const void *, const void *, const void *, void *), int op, long n,
+                   unsigned seed, void *first);
 short oz_tau_sd_libm(float v);
 long oz_tau_sd_sweep(int (*rule)(float), unsigned stride, unsigned *first);
 int oz_split_cols_sd(const oz_flags *f, int k, int ncol, const float *X, int ldx, int shift, double *slices, int lds,

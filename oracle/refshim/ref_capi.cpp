@@ -95,6 +95,35 @@ int ref_sgemv_d(void *hp, char ta, int m, int n, float alpha, const float *A, in
     return ozblasRgemv<float, double, double>((ozblasHandle_t *)hp, ta, m, n, alpha, A, lda, x, 1, beta, y, 1);
 }
 
+/* the quad I/O form <__float128, double, double> (binary128 data as 16-byte values) */
+int ref_qgemm_d(void *hp, char ta, char tb, int m, int n, int k, const void *alpha, const void *A, int lda,
+                const void *B, int ldb, const void *beta, void *C, int ldc) {
+    __float128 al, be;
+    memcpy(&al, alpha, 16);
+    memcpy(&be, beta, 16);
+    return ozblasRgemm<__float128, double, double>((ozblasHandle_t *)hp, ta, tb, m, n, k, al, (const __float128 *)A,
+                                                   lda, (const __float128 *)B, ldb, be, (__float128 *)C, ldc);
+}
+
+void ref_qdot_d(void *hp, int n, const void *x, const void *y, void *ret) {
+    const __float128 r = ozblasRdot<__float128, double, double>((ozblasHandle_t *)hp, n, (const __float128 *)x, 1,
+                                                                (const __float128 *)y, 1);
+    memcpy(ret, &r, 16);
+}
+
+void ref_qnrm2_d(void *hp, int n, const void *x, void *ret) {
+    const __float128 r = ozblasRnrm2<__float128, double, double>((ozblasHandle_t *)hp, n, (const __float128 *)x, 1);
+    memcpy(ret, &r, 16);
+}
+
+/* the reference's tau expression for binary128 data, as its split writes it */
+int ref_tau_q(const void *v) {
+    __float128 x;
+    memcpy(&x, v, 16);
+    const short tau = ceil(log21(fabs1(x)));
+    return tau;
+}
+
 /* log21<float> of the reference (src/cpu/ozblas_aux.cpp:37-42), for the tau rule of float data */
 float ref_log21f(float v) { return log21<float>(v); }
 

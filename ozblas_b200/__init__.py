@@ -95,6 +95,10 @@ _sdgemm = _sig("cuozblasSDgemm", [_HP, _ch, _ch, _i32, _i32, _i32, _f, _vp, _i32
 _sdgemv = _sig("cuozblasSDgemv", [_HP, _ch, _i32, _i32, _f, _vp, _i32, _vp, _i32, _f, _vp, _i32])
 _sddot = _sig("cuozblasSDdot", [_HP, _i32, _vp, _i32, _vp, _i32, C.POINTER(_f)])
 _sdnrm2 = _sig("cuozblasSDnrm2", [_HP, _i32, _vp, _i32, C.POINTER(_f)])
+_qgemm = _sig("cuozblasQgemm", [_HP, _ch, _ch, _i32, _i32, _i32, _vp, _vp, _i32, _vp, _i32, _vp, _vp, _i32])
+_qgemv = _sig("cuozblasQgemv", [_HP, _ch, _i32, _i32, _vp, _vp, _i32, _vp, _i32, _vp, _vp, _i32])
+_qdot = _sig("cuozblasQdot", [_HP, _i32, _vp, _i32, _vp, _i32, _vp])
+_qnrm2 = _sig("cuozblasQnrm2", [_HP, _i32, _vp, _i32, _vp])
 _dgemm_i8 = _sig("cuozblasDgemmI8", [_HP, _ch, _ch, _i32, _i32, _i32, _d, _vp, _i32, _vp, _i32, _d, _vp, _i32])
 _dgemm_i8_static = _sig("cuozblasDgemmI8Static", [_ch, _ch, _i32, _i32, _i32, _d, _vp, _i32, _vp, _i32, _d, _vp,
                                                   _i32, _i32, _i32, _vp])
@@ -116,7 +120,8 @@ C_ABI_SYMBOLS = [
     "cuozblasDaxpy", "cuozblasDgemv", "cuozblasDgemm", "cuozblasDcsrmv", "cuozblasDcsrmvSplitA", "cuozblasDcg",
     "cuozblasDgemmI8", "cuozblasDgemmI8Static", "cuozblasDgemmI8Batched", "cuozblasRuleTau", "cuozblasRuleRho",
     "cuozblasRuleCrSum", "cuozblasDSgemm", "cuozblasDSgemv", "cuozblasDSdot", "cuozblasDSnrm2",
-    "cuozblasRuleTauF32", "cuozblasSDgemm", "cuozblasSDgemv", "cuozblasSDdot", "cuozblasSDnrm2",
+    "cuozblasRuleTauF32", "cuozblasRuleQ128", "cuozblasQgemm", "cuozblasQgemv", "cuozblasQdot", "cuozblasQnrm2",
+    "cuozblasSDgemm", "cuozblasSDgemv", "cuozblasSDdot", "cuozblasSDnrm2",
     "cuozblasVersion",
 ]
 
@@ -231,6 +236,38 @@ def sdnrm2(h, n, x, incx=1) -> float:
     r = _f()
     _chk("cuozblasSDnrm2", _sdnrm2(h.ref, n, _ptr(x), incx, C.byref(r)))
     return r.value
+
+
+def _q16(v):
+    """A host binary128 scalar (16 bytes: uint64 (lo, hi)) as a ctypes buffer."""
+    import numpy as _np
+    a = _np.ascontiguousarray(v, dtype=_np.uint64).reshape(2)
+    return (C.c_uint64 * 2)(int(a[0]), int(a[1]))
+
+
+def qgemm(h, ta, tb, m, n, k, alpha, A, lda, B, ldb, beta, Cm, ldc):
+    """Quad I/O form <__float128, double, double>: A, B, C device buffers of 16-byte binary128 values;
+    alpha, beta host binary128 scalars given as two uint64 (lo, hi)."""
+    _chk("cuozblasQgemm", _qgemm(h.ref, ta.encode(), tb.encode(), m, n, k, C.cast(_q16(alpha), _vp), _ptr(A), lda,
+                                 _ptr(B), ldb, C.cast(_q16(beta), _vp), _ptr(Cm), ldc))
+
+
+def qgemv(h, trans, m, n, alpha, A, lda, x, beta, y, incx=1, incy=1):
+    _chk("cuozblasQgemv", _qgemv(h.ref, trans.encode(), m, n, C.cast(_q16(alpha), _vp), _ptr(A), lda, _ptr(x), incx,
+                                 C.cast(_q16(beta), _vp), _ptr(y), incy))
+
+
+def qdot(h, n, x, y, incx=1, incy=1):
+    """Binary128 DOT; returns the result's two uint64 (lo, hi)."""
+    r = (C.c_uint64 * 2)()
+    _chk("cuozblasQdot", _qdot(h.ref, n, _ptr(x), incx, _ptr(y), incy, C.cast(r, _vp)))
+    return (r[0], r[1])
+
+
+def qnrm2(h, n, x, incx=1):
+    r = (C.c_uint64 * 2)()
+    _chk("cuozblasQnrm2", _qnrm2(h.ref, n, _ptr(x), incx, C.cast(r, _vp)))
+    return (r[0], r[1])
 
 
 def dgemm_i8(h, ta, tb, m, n, k, alpha, A, lda, B, ldb, beta, Cm, ldc):

@@ -10,6 +10,7 @@
 #include <new>
 
 #include "crsum.h"
+#include "q128.cuh"
 #include "ozb_internal.h"
 
 namespace ozb {
@@ -125,6 +126,49 @@ const char *cuozblasVersion(void) { return "cuozblas-b200 0.1 (sm_100a; plain FP
 int cuozblasRuleTau(double v) { return tau_rule(v); }
 
 int cuozblasRuleTauF32(float v) { return tau_rule_f32(v); }
+
+int cuozblasRuleQ128(int op, const void *a, const void *b, const void *c, void *out) {
+    Q128 x, y, z;
+    if (!a || !out) return CUOZBLAS_STATUS_INVALID_VALUE;
+    memcpy(&x, a, 16);
+    switch (op) {
+    case 0:
+    case 1:
+        memcpy(&y, b, 16);
+        x = op == 0 ? q_add(x, y) : q_mul(x, y);
+        memcpy(out, &x, 16);
+        return CUOZBLAS_STATUS_SUCCESS;
+    case 2:
+        memcpy(&y, b, 16);
+        memcpy(&z, c, 16);
+        x = q_fma(x, y, z);
+        memcpy(out, &x, 16);
+        return CUOZBLAS_STATUS_SUCCESS;
+    case 3: {
+        const int t = tau_rule_q(x);
+        memcpy(out, &t, sizeof(int));
+        return CUOZBLAS_STATUS_SUCCESS;
+    }
+    case 4: {  // b: int rho, tau; out: remainder (16 bytes) then the slice (double)
+        int rt[2];
+        memcpy(rt, b, sizeof(rt));
+        const double sl = q_split(x, rt[0], rt[1]);
+        memcpy(out, &x, 16);
+        memcpy((char *)out + 16, &sl, 8);
+        return CUOZBLAS_STATUS_SUCCESS;
+    }
+    case 5: {  // a: double, b: int k
+        double d;
+        int k;
+        memcpy(&d, a, 8);
+        memcpy(&k, b, sizeof(int));
+        x = q_from_double_scaled(d, k);
+        memcpy(out, &x, 16);
+        return CUOZBLAS_STATUS_SUCCESS;
+    }
+    }
+    return CUOZBLAS_STATUS_INVALID_VALUE;
+}
 int cuozblasRuleRho(int32_t dim, int32_t mode) { return rho_rule(dim, mode); }
 
 int cuozblasRuleCrSum(int32_t n, const double *terms, double *out) {
@@ -399,6 +443,77 @@ int cuozblasSDnrm2(cuozblasHandle_t *h, int32_t n, const float *x, int32_t incx,
     float d = 0.f;
     OZB_TRY(dot_sd_impl(h, n, x, x, &d));
     *ret = (float)sqrt((double)d);  // the reference's sqrt on a float (src/cpu/ozblas_nrm2.cpp:24-29)
+    return finish(h, t0);
+}
+
+// Quad I/O form <__float128, double, double>: binary128 data and results as
+// 16-byte values (alpha, beta and DOT/NRM2 results in host memory); FSum only.
+int cuozblasQgemm(cuozblasHandle_t *h, char transa, char transb, int32_t m, int32_t n, int32_t k, const void *alpha,
+                  const void *A, int32_t lda, const void *B, int32_t ldb, const void *beta, void *C, int32_t ldc) {
+    OZB_TRY(counter_init(h));
+    OZB_TRY(check_flags_f32(h));
+    if (m < 0 || n < 0 || k < 0 || ldc < (m > 1 ? m : 1) || !alpha || !beta) return CUOZBLAS_STATUS_INVALID_VALUE;
+    if (h->reproMode == 0 && h->nSplitMax == 1) return CUOZBLAS_STATUS_NOT_SUPPORTED;
+    if (m == 0 || n == 0) return CUOZBLAS_STATUS_SUCCESS;
+    const double t0 = wall();
+    OZB_TRY(gemm_q_core(h, transa, transb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, h->fastMode));
+    return finish(h, t0);
+}
+
+int cuozblasQgemv(cuozblasHandle_t *h, char trans, int32_t m, int32_t n, const void *alpha, const void *A,
+                  int32_t lda, const void *x, int32_t incx, const void *beta, void *y, int32_t incy) {
+    OZB_TRY(counter_init(h));
+    OZB_TRY(check_flags_f32(h));
+    if (incx != 1 || incy != 1 || m < 0 || n < 0 || !alpha || !beta) return CUOZBLAS_STATUS_INVALID_VALUE;
+    if (h->reproMode == 0 && h->nSplitMax == 1) return CUOZBLAS_STATUS_NOT_SUPPORTED;
+    const double t0 = wall();
+    if (!is_trans(trans)) {  // src/cpu/ozblas_gemv.cpp:22-26
+        if (m == 0) return CUOZBLAS_STATUS_SUCCESS;
+        OZB_TRY(gemm_q_core(h, 'n', 'n', m, 1, n, alpha, A, lda, x, n, beta, y, m, h->fastMode));
+    } else {
+        if (n == 0) return CUOZBLAS_STATUS_SUCCESS;
+        OZB_TRY(gemm_q_core(h, 't', 'n', n, 1, m, alpha, A, lda, x, m, beta, y, n, h->fastMode));
+    }
+    return finish(h, t0);
+}
+
+static int dot_q_impl(cuozblasHandle_t *h, int n, const void *x, const void *y, void *ret) {
+    State *st = state(h);
+    void *d = h->devWorkCommon;
+    static const uint64_t one[2] = {0, 0x3fff000000000000ULL}, zero[2] = {0, 0};
+    OZB_CHECK(cudaMemsetAsync(d, 0, 16, st->stream));
+    OZB_TRY(gemm_q_core(h, 't', 'n', 1, 1, n, one, x, n, y, n, zero, d, 1, 0));
+    OZB_CHECK(cudaMemcpyAsync(st->h_dbl, d, 16, cudaMemcpyDeviceToHost, st->stream));
+    OZB_CHECK(cudaStreamSynchronize(st->stream));
+    memcpy(ret, st->h_dbl, 16);
+    return CUOZBLAS_STATUS_SUCCESS;
+}
+
+int cuozblasQdot(cuozblasHandle_t *h, int32_t n, const void *x, int32_t incx, const void *y, int32_t incy,
+                 void *ret) {
+    OZB_TRY(counter_init(h));
+    OZB_TRY(check_flags_f32(h));
+    if (incx != 1 || incy != 1 || n < 0 || ret == nullptr) return CUOZBLAS_STATUS_INVALID_VALUE;
+    if (h->reproMode == 0 && h->nSplitMax == 1) return CUOZBLAS_STATUS_NOT_SUPPORTED;
+    const double t0 = wall();
+    OZB_TRY(dot_q_impl(h, n, x, y, ret));
+    h->t_SplitVec_total += h->t_SplitA + h->t_SplitB;
+    return finish(h, t0);
+}
+
+int cuozblasQnrm2(cuozblasHandle_t *h, int32_t n, const void *x, int32_t incx, void *ret) {
+    OZB_TRY(counter_init(h));
+    OZB_TRY(check_flags_f32(h));
+    if (incx != 1 || n < 0 || ret == nullptr) return CUOZBLAS_STATUS_INVALID_VALUE;
+    if (h->reproMode == 0 && h->nSplitMax == 1) return CUOZBLAS_STATUS_NOT_SUPPORTED;
+    const double t0 = wall();
+    Q128 d;
+    OZB_TRY(dot_q_impl(h, n, x, x, &d));
+    // the reference's sqrt(ret) on a __float128 resolves to the double sqrt
+    // (src/cpu/ozblas_nrm2.cpp:27): the binary128 of sqrt((double)ret)
+    const double dd = q_to_double_rn(d);
+    const Q128 r = q_from_double_scaled(sqrt(dd), 0);
+    memcpy(ret, &r, 16);
     return finish(h, t0);
 }
 

@@ -127,6 +127,43 @@ int32_t cuozblasRgemm<float, double, double>(cuozblasHandle_t *oh, const char tr
                   cuozblasSDgemm(oh, tranA, tranB, m, n, k, alpha, devA, lda, devB, ldb, beta, devC, ldc));
 }
 
+#if defined(__SIZEOF_FLOAT128__)
+// The quad I/O form: not instantiated by the reference's CUDA library (its
+// CPU library has it, src/cpu/ozblas_gemm.cpp:316); offered here with the
+// same template signature.
+template <>
+int32_t cuozblasRgemm<__float128, double, double>(cuozblasHandle_t *oh, const char tranA, const char tranB,
+                                                  const int32_t m, const int32_t n, const int32_t k,
+                                                  const __float128 alpha, const __float128 *devA, const int32_t lda,
+                                                  const __float128 *devB, const int32_t ldb, const __float128 beta,
+                                                  __float128 *devC, const int32_t ldc) {
+    return report("cuozblasRgemm<__float128>",
+                  cuozblasQgemm(oh, tranA, tranB, m, n, k, &alpha, devA, lda, devB, ldb, &beta, devC, ldc));
+}
+
+template <>
+int32_t cuozblasRgemv<__float128, double, double>(cuozblasHandle_t *oh, const char tranA, const int32_t m,
+                                                  const int32_t n, const __float128 alpha, const __float128 *devA,
+                                                  const int32_t lda, const __float128 *devB, const int32_t incx,
+                                                  const __float128 beta, __float128 *devC, const int32_t incy) {
+    return report("cuozblasRgemv<__float128>",
+                  cuozblasQgemv(oh, tranA, m, n, &alpha, devA, lda, devB, incx, &beta, devC, incy));
+}
+
+template <>
+int32_t cuozblasRdot<__float128, double, double>(cuozblasHandle_t *oh, const int32_t n, const __float128 *devA,
+                                                 const int32_t incx, const __float128 *devB, const int32_t incy,
+                                                 __float128 *ret) {
+    return report("cuozblasRdot<__float128>", cuozblasQdot(oh, n, devA, incx, devB, incy, ret));
+}
+
+template <>
+int32_t cuozblasRnrm2<__float128, double, double>(cuozblasHandle_t *oh, const int32_t n, const __float128 *devX,
+                                                  const int32_t incx, __float128 *ret) {
+    return report("cuozblasRnrm2<__float128>", cuozblasQnrm2(oh, n, devX, incx, ret));
+}
+#endif
+
 template <>
 int32_t cuozblasRcsrmv<double, double>(cuozblasHandle_t *oh, const char tranA, const int32_t m, const int32_t n,
                                        const int32_t nnz, const double alpha, const cusparseMatDescr_t descrA,

@@ -570,6 +570,46 @@ int gemm_plain_core(cuozblasHandle_t *h, char ta, char tb, int m, int n, int k, 
 }
 
 // ---------------------------------------------------------------------------
+// Exact FP64 pair products for other sums (the quad form): every pair of the
+// list to pbuf[p][col][row] for columns c0 .. c0 + nc of B's n lines, and the
+// skinny forms' pair matrices P[(ia * nB + ib) * ldp + row].
+// ---------------------------------------------------------------------------
+int gemm_pairs_store(cuozblasHandle_t *h, int m, int nc, int nlB, int ldk, const double *Sa, const double *Sb,
+                     const int2 *dp, int np, double *pbuf) {
+    State *st = state(h);
+    dim3 g((m + kBM - 1) / kBM, (nc + kBN - 1) / kBN);
+    counted(h);
+    k_gemm_pairs_dmma<true, false><<<g, 128, 0, st->stream>>>(m, nc, nlB, ldk, Sa, Sb, dp, np, 0.0, 0.0, nullptr,
+                                                              1, pbuf, nullptr, nullptr, nullptr);
+    OZB_CHECK(cudaGetLastError());
+    return CUOZBLAS_STATUS_SUCCESS;
+}
+
+int pair_products_skinny(cuozblasHandle_t *h, bool dot, int m, int k, int nA, int nB, const double *Sa,
+                         const double *Sb, int ldk, double *P) {
+    State *st = state(h);
+    const int64_t ldp = dot ? 1 : m;
+    if (dot) OZB_CHECK(cudaMemsetAsync(P, 0, sizeof(double) * nA * nB, st->stream));
+    for (int ia0 = 0; ia0 < nA; ia0 += 8)
+        for (int ib0 = 0; ib0 < nB; ib0 += 8) {
+            const int na = nA - ia0 < 8 ? nA - ia0 : 8, nb = nB - ib0 < 8 ? nB - ib0 : 8;
+            counted(h);
+            if (dot) {
+                int blocks = (k + 255) / 256;
+                if (blocks > 148 * 8) blocks = 148 * 8;
+                if (blocks < 1) blocks = 1;
+                k_pair_dot<<<blocks, 256, 0, st->stream>>>(k, na, nb, Sa + (size_t)ia0 * ldk, ldk,
+                                                           Sb + (size_t)ib0 * ldk, ldk, P + ia0 * nB + ib0, nB);
+            } else {
+                const int blocks = (int)(((int64_t)m * 32 + 255) / 256);
+                k_pair_gemv<<<blocks, 256, 0, st->stream>>>(m, k, na, nb, ia0, ib0, nB, Sa, ldk, Sb, ldk, P, ldp);
+            }
+            OZB_CHECK(cudaGetLastError());
+        }
+    return CUOZBLAS_STATUS_SUCCESS;
+}
+
+// ---------------------------------------------------------------------------
 // Mixed form <float, double, double> (src/cpu/ozblas_gemm.cpp:3-315 with
 // TYPE1 = float): float data split in float arithmetic into FP64 slices
 // (split_lines_*_sd), exact FP64 slice products on the DMMA / skinny kernels

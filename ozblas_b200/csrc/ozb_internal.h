@@ -155,6 +155,16 @@ int rho_rule_sd(int dim, int splitEpsMode);
 int gemm_sd_core(cuozblasHandle_t *h, char ta, char tb, int m, int n, int k, float alpha, const float *A, int lda,
                  const float *B, int ldb, float beta, float *C, int ldc, int fastMode);
 
+// ---- exact FP64 pair products for the quad form (gemm_plain.cu) ----
+int gemm_pairs_store(cuozblasHandle_t *h, int m, int nc, int nlB, int ldk, const double *Sa, const double *Sb,
+                     const int2 *dp, int np, double *pbuf);
+int pair_products_skinny(cuozblasHandle_t *h, bool dot, int m, int k, int nA, int nB, const double *Sa,
+                         const double *Sb, int ldk, double *P);
+
+// ---- quad I/O form <__float128, double, double> (gemm_q.cu); binary128 as 16 bytes ----
+int gemm_q_core(cuozblasHandle_t *h, char ta, char tb, int m, int n, int k, const void *alpha, const void *A, int lda,
+                const void *B, int ldb, const void *beta, void *C, int ldc, int fastMode);
+
 // ---- plain GEMM core (gemm_plain.cu) ----
 int gemm_plain_core(cuozblasHandle_t *h, char ta, char tb, int m, int n, int k, double alpha, const double *A,
                     int lda, const double *B, int ldb, double beta, double *C, int ldc, int fastMode);

@@ -1,4 +1,4 @@
-"""Mixed forms <double, float, float> and <float, double, double> on the GPU vs the CPU oracle: bit-exact.
+"""Mixed and quad I/O forms on the GPU vs the CPU oracle: bit-exact.
 
 <double, float, float>: FP64 data, FP32 slices (scalbn(slice, -tau) with tau
 per line and level), exact FP32 slice products and the scaled FSum
@@ -9,7 +9,12 @@ through cuozblasDSgemm / DSgemv / DSdot / DSnrm2.
 exact FP64 slice products, each rounded to float, scaled and summed in float
 (TYPE1 = float), through cuozblasSDgemm / SDgemv / SDdot / SDnrm2.
 
-The oracle's restatements of both forms are pinned to the reference library's
+<__float128, double, double>: binary128 data (16-byte values, held here as
+uint64 pairs) split in binary128, FP64 slices, exact FP64 products, the
+ordered sum and fmaq in binary128, through cuozblasQgemm / Qgemv / Qdot /
+Qnrm2 (the library's software binary128, q128.cuh).
+
+The oracle's restatements of these forms are pinned to the reference library's
 ozblasRgemm/Rgemv/Rdot/Rnrm2 instantiations by tests/test_oracle.py.
 """
 import numpy as np
@@ -266,4 +271,102 @@ def test_sd_unsupported_flags(handle, ozb, cuda):
     handle.sumMode, handle.splitEpsMode = 0, 2
     with pytest.raises(ozb.OzblasError) as e:
         ozb.sddot(handle, 8, x, x)
+    assert e.value.code == 4
+
+
+# ---- <__float128, double, double>: binary128 data (uint64 pairs), FP64 slices, binary128 sum ----
+
+def qdev(torch, a):
+    return torch.from_numpy(np.ascontiguousarray(a, dtype=np.uint64).view(np.int64)).cuda()
+
+
+def qhost(t):
+    return t.cpu().numpy().view(np.uint64)
+
+
+Q_CASES = [
+    # m, n, k, ta, tb, fastMode, nSplitMax, alpha, beta, phi
+    (2, 2, 1, "n", "n", 0, 0, 1.0, 0.0, 1.0),
+    (1, 5, 40, "t", "n", 0, 0, 1.0, 0.0, 1.0),
+    (33, 17, 100, "n", "n", 0, 0, 1.0, 0.0, 1.0),
+    (33, 17, 100, "t", "n", 1, 0, 1.25, -0.5, 4.0),
+    (7, 9, 130, "n", "t", 0, 0, -0.5, 2.0, 2.0),
+    (20, 20, 64, "t", "t", 2, 0, 1.0, 1.0, 2.0),
+    (130, 150, 300, "n", "n", 0, 0, 1.5, -1.0, 1.0),
+    (65, 70, 33, "t", "t", 0, 2, 1.0, 0.0, 4.0),
+]
+
+
+@pytest.mark.parametrize("case", Q_CASES, ids=lambda c: "x".join(map(str, c[:3])) + f"-{c[3]}{c[4]}-f{c[5]}s{c[6]}")
+def test_qgemm(case, oracle, handle, ozb, cuda):
+    m, n, k, ta, tb, fm, ns, alpha, beta, phi = case
+    ar, ac = (m, k) if ta == "n" else (k, m)
+    br, bc = (k, n) if tb == "n" else (n, k)
+    A = oracle.phi_matrix_q(ar, ac, phi, 1)
+    B = oracle.phi_matrix_q(br, bc, phi, 2)
+    C0 = oracle.phi_matrix_q(m, n, 1.0, 3)
+    al, be = oracle.q(alpha), oracle.q(beta)
+    ref, info = oracle.qgemm_d(make_flags(fastMode=fm, nSplitMax=ns), ta, tb, m, n, k, al, A, ar, B, br, be, C0, m)
+    handle.fastMode, handle.nSplitMax = fm, ns
+    dC = qdev(cuda, C0)
+    ozb.qgemm(handle, ta, tb, m, n, k, al, qdev(cuda, A), ar, qdev(cuda, B), br, be, dC, m)
+    out = qhost(dC)
+    assert np.array_equal(out, ref), np.argwhere(np.any(out != ref, axis=-1))[:3]
+    assert (handle.nSplitA, handle.nSplitB, handle.nSplitC) == (info.nSplitA, info.nSplitB, info.nSplitC)
+
+
+@pytest.mark.parametrize("n,phi", [(1, 1.0), (7, 1.0), (1000, 2.0), (100003, 1.0)])
+def test_qdot_qnrm2(n, phi, oracle, handle, ozb, cuda):
+    import math
+    x = oracle.phi_vector_q(n, phi, 1)
+    y = oracle.phi_vector_q(n, phi, 2)
+    d = ozb.qdot(handle, n, qdev(cuda, x), qdev(cuda, y))
+    one, zero = oracle.q(1.0), oracle.q(0.0)
+    r, info = oracle.qgemm_d(make_flags(), "t", "n", 1, 1, n, one, x, n, y, n, zero, np.zeros((1, 2), np.uint64), 1)
+    assert tuple(int(v) for v in r[0]) == tuple(int(v) for v in d)
+    assert (handle.nSplitA, handle.nSplitB, handle.nSplitC) == (info.nSplitA, info.nSplitB, 1.0)
+    nr = ozb.qnrm2(handle, n, qdev(cuda, x))
+    r2, _ = oracle.qgemm_d(make_flags(), "t", "n", 1, 1, n, one, x, n, x, n, zero, np.zeros((1, 2), np.uint64), 1)
+    want = oracle.q(math.sqrt(oracle.q_to_double(r2[0])))  # the reference's double sqrt of the binary128 dot
+    assert tuple(int(v) for v in want) == tuple(int(v) for v in nr)
+
+
+@pytest.mark.parametrize("m,n,trans,fm", [(50, 70, "n", 0), (50, 70, "t", 0), (300, 257, "n", 1), (1, 33, "t", 0)])
+def test_qgemv(m, n, trans, fm, oracle, handle, ozb, cuda):
+    A = oracle.phi_matrix_q(m, n, 2.0, 1)
+    xl, yl = (n, m) if trans == "n" else (m, n)
+    x = oracle.phi_vector_q(xl, 2.0, 2)
+    y0 = oracle.phi_vector_q(yl, 1.0, 3)
+    al, be = oracle.q(0.75), oracle.q(0.5)
+    f = make_flags(fastMode=fm)
+    if trans == "n":
+        ref, info = oracle.qgemm_d(f, "n", "n", m, 1, n, al, A, m, x, n, be, y0, m)
+    else:
+        ref, info = oracle.qgemm_d(f, "t", "n", n, 1, m, al, A, m, x, m, be, y0, n)
+    handle.fastMode = fm
+    dy = qdev(cuda, y0)
+    ozb.qgemv(handle, trans, m, n, al, qdev(cuda, A), m, qdev(cuda, x), be, dy)
+    assert np.array_equal(qhost(dy), ref)
+    assert (handle.nSplitA, handle.nSplitB, handle.nSplitC) == (info.nSplitA, info.nSplitB, info.nSplitC)
+
+
+@pytest.mark.parametrize("e", [-16350, -8000, 9000, 16200])
+def test_q_extreme_magnitudes(e, oracle, handle, ozb, cuda):
+    """Data scaled toward the ends of binary128's range: products land in its subnormal range (the
+    binary128 scaling rounds there) or near overflow."""
+    m, n, k = 20, 17, 90
+    A = oracle.q_scale(oracle.phi_matrix_q(m, k, 1.0, 1), e)
+    B = oracle.phi_matrix_q(k, n, 1.0, 2)
+    one, zero = oracle.q(1.0), oracle.q(0.0)
+    ref, _ = oracle.qgemm_d(make_flags(), "n", "n", m, n, k, one, A, m, B, k, zero, np.zeros((n, m, 2), np.uint64), m)
+    dC = qdev(cuda, np.zeros((n, m, 2), np.uint64))
+    ozb.qgemm(handle, "n", "n", m, n, k, one, qdev(cuda, A), m, qdev(cuda, B), k, zero, dC, m)
+    assert np.array_equal(qhost(dC), ref)
+
+
+def test_q_unsupported_flags(oracle, handle, ozb, cuda):
+    x = qdev(cuda, np.zeros((8, 2), np.uint64))
+    handle.sumMode = 1
+    with pytest.raises(ozb.OzblasError) as e:
+        ozb.qdot(handle, 8, x, x)
     assert e.value.code == 4

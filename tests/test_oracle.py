@@ -325,6 +325,33 @@ def test_tau_of_float_data_vs_reference(oracle, reference):
     assert not bad, bad[:5]
 
 
+@pytest.mark.parametrize("seed", range(8))
+def test_quad_gemm_vs_reference(seed, oracle, reference):
+    """<__float128, double, double> (binary128 split, FP64 slices, binary128 ordered sum and fmaq): the
+    restatement against ozblasRgemm<__float128, double, double>, bit-exact with the split counts.  The
+    reference library needs MPLAPACK (not built) to split a one-column panel, so m, n >= 2 here."""
+    rng = np.random.default_rng(700 + seed)
+    m, n = (int(v) for v in rng.integers(2, 30, 2))
+    k = int(rng.integers(1, 300))
+    ta, tb = rng.choice(["n", "t"]), rng.choice(["n", "t"])
+    fm = int(rng.integers(0, 3))
+    nsplit = int(rng.choice([0, 0, 2, 5]))
+    phi = float(rng.choice([0.5, 1.0, 2.0, 4.0]))
+    ar, ac = (m, k) if ta == "n" else (k, m)
+    br, bc = (k, n) if tb == "n" else (n, k)
+    A = oracle.phi_matrix_q(ar, ac, phi, 1)
+    B = oracle.phi_matrix_q(br, bc, phi, 2)
+    C0 = oracle.phi_matrix_q(m, n, 1.0, 3)
+    al, be = oracle.q(1.25), oracle.q(-0.5)
+    out, info = oracle.qgemm_d(make_flags(fastMode=fm, nSplitMax=nsplit), ta, tb, m, n, k, al, A, ar, B, br, be, C0,
+                               m)
+    reference.set_flags(fastMode=fm, nSplitMax=nsplit)
+    gold = reference.qgemm_d(ta, tb, m, n, k, al, A, ar, B, br, be, C0, m)
+    assert np.array_equal(out, gold), (seed, m, n, k, ta, tb, fm, nsplit, phi)
+    inf = reference.info()
+    assert [info.nSplitA, info.nSplitB, info.nSplitC] == [inf["nSplitA"], inf["nSplitB"], inf["nSplitC"]]
+
+
 def test_split_slices_vs_reference(oracle, reference):
     """Slice-level parity of the column-panel and CSR splits."""
     for phi, k, ncol in [(1.0, 100, 7), (4.0, 333, 5), (2.0, 1, 3), (1.0, 64, 1)]:

@@ -90,3 +90,72 @@ def test_tau_of_float_data_sweep(lib, oracle):
             if lib.cuozblasRuleTauF32(v) != oracle.tau_sd_libm(v):
                 mism.append((e, j))
     assert not mism, mism[:10]
+
+
+def _qrule(lib):
+    import ctypes
+    lib.cuozblasRuleQ128.argtypes = [ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                     ctypes.c_void_p]
+    lib.cuozblasRuleQ128.restype = ctypes.c_int
+    return ctypes.cast(lib.cuozblasRuleQ128, ctypes.c_void_p).value
+
+
+@pytest.mark.parametrize("op,name", [(0, "add"), (1, "mul"), (2, "fma"), (3, "tau"), (4, "split")])
+def test_software_binary128(op, name, lib, oracle):
+    """The library's binary128 (q128.cuh, the code the quad-form kernels run) against gcc's
+    __float128 and libquadmath's fmaq on 200,000 random operands per operation: random and close
+    exponents (cancellation), short significands (ties to even), signed zeros and subnormals.
+    tau is compared with the restatement's ceil((double)log2q(v)), the split with the reference's
+    (x + sigma) - sigma in binary128."""
+    addr = _qrule(lib)
+    for seed in (op + 1, op + 101):
+        bad, first = oracle.q128_check(addr, op, 100000, seed=seed)
+        assert bad == 0, (name, bad, [hex(int(v)) for v in first])
+
+
+def _q_bits(e, j):
+    be = e + 16383
+    hi = (be << 48) | (j >> 64)
+    return np.array([j & ((1 << 64) - 1), hi], dtype=np.uint64)
+
+
+def test_tau_of_binary128_every_exponent(lib, oracle, reference):
+    """The quad tau rule (threshold table) against the reference's own expression on every normal
+    binary128 exponent, at the last mantissa that keeps tau = e and the first that gives e + 1, and
+    on random subnormals."""
+    import ctypes
+    _qrule(lib)
+    out = ctypes.c_int(0)
+
+    def lib_tau(v):
+        lib.cuozblasRuleQ128(3, v.ctypes.data, None, None, ctypes.byref(out))
+        return out.value
+
+    bad = []
+    for e in range(-16382, 16384):
+        for j in (0, 1, (1 << 112) - 1):
+            v = _q_bits(e, j)
+            if lib_tau(v) != reference.tau_q(v):
+                bad.append((e, j))
+        # the switch point: tau(j) == e for j <= T, e + 1 above
+        lo, hi = 0, (1 << 112) - 1
+        if e % 97 == 0:  # bisection on a sample of exponents, every binade class included
+            while hi - lo > 1:
+                mid = (lo + hi) // 2
+                if reference.tau_q(_q_bits(e, mid)) == e:
+                    lo = mid
+                else:
+                    hi = mid
+            for j in (lo, hi):
+                if lib_tau(_q_bits(e, j)) != reference.tau_q(_q_bits(e, j)):
+                    bad.append((e, j))
+    rng = np.random.default_rng(5)
+    for _ in range(2000):
+        j = int(rng.integers(1, 1 << 62)) << int(rng.integers(0, 50))
+        j &= (1 << 112) - 1
+        if j == 0:
+            continue
+        v = np.array([j & ((1 << 64) - 1), j >> 64], dtype=np.uint64)  # subnormal
+        if lib_tau(v) != reference.tau_q(v):
+            bad.append(("sub", j))
+    assert not bad, bad[:10]
