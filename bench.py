@@ -493,6 +493,21 @@ def batched_extras(ozb, h, torch, reps=3):
     return out
 
 
+def binary128_from_phi(a, seed):
+    """Binary128 values (uint64 pairs lo, hi) with the phi distribution of the double array `a` and 113
+    significant bits: a's sign, exponent and 52 fraction bits, then 60 random low bits."""
+    import numpy as np
+    bits = np.ascontiguousarray(a, dtype=np.float64).view(np.uint64).ravel()
+    sign = bits >> np.uint64(63)
+    exp = (bits >> np.uint64(52)) & np.uint64(0x7FF)
+    frac = bits & np.uint64((1 << 52) - 1)
+    assert np.all((exp > 0) & (exp < 0x7FF)), "normal doubles only"
+    low = np.random.default_rng(seed).integers(0, 1 << 60, size=bits.size, dtype=np.uint64)
+    hi = (sign << np.uint64(63)) | ((exp - np.uint64(1023) + np.uint64(16383)) << np.uint64(48)) | (frac >> np.uint64(4))
+    lo = ((frac & np.uint64(0xF)) << np.uint64(60)) | low
+    return np.stack([lo, hi], axis=-1).reshape(a.shape + (2,))
+
+
 def mixed_extras(ozb, h, torch, n, reps=3):
     """The two mixed forms through the public API on an n^3 phi problem: call time (CUDA events),
     slice counts, and the slice-product throughput of the product kernel (its phase timer)."""
@@ -522,10 +537,41 @@ def mixed_extras(ozb, h, torch, n, reps=3):
                "dgemm_equivalent_TFLOPS": 2.0 * n ** 3 / ms / 1e9,
                "slice_product_TFLOPS": 2.0 * n ** 3 * pairs / kms / 1e9}
         if name == "dsgemm":
-            rec["fp32_simt_nominal_TFLOPS"] = fp32_nominal
-            rec["fraction_of_fp32_nominal"] = rec["slice_product_TFLOPS"] / fp32_nominal
+            if n > 1024:  # rho >= 47: the INT8 slices run on tcgen05 (kind::i8)
+                peaks, how = measured_peaks()
+                i8_peak = 2.0 * peaks["bf16_tflops"]
+                rec["path"] = "int8 tensor cores"
+                rec["int8_peak_TOPS"] = i8_peak
+                rec["fraction_of_int8_peak"] = rec["slice_product_TFLOPS"] / i8_peak
+                rec["peak_source"] = how
+            else:
+                rec["path"] = "fp32 simt"
+                rec["fp32_simt_nominal_TFLOPS"] = fp32_nominal
+                rec["fraction_of_fp32_nominal"] = rec["slice_product_TFLOPS"] / fp32_nominal
         out[name] = rec
         del C
+    # quad I/O form: binary128 data built from the same phi matrices
+    import numpy as np
+    Aq = torch.from_numpy(binary128_from_phi(phi_matrix(n, n, PHI, 1), 11).view(np.int64)).cuda()
+    Bq = torch.from_numpy(binary128_from_phi(phi_matrix(n, n, PHI, 2), 12).view(np.int64)).cuda()
+    Cq = torch.zeros((n, n, 2), dtype=torch.int64, device="cuda")
+    one = np.array([0, 0x3FFF000000000000], dtype=np.uint64)
+    zero = np.zeros(2, dtype=np.uint64)
+    ozb.qgemm(h, "n", "n", n, n, n, one, Aq, n, Bq, n, zero, Cq, n)
+    torch.cuda.synchronize()
+    ts = []
+    for _ in range(max(reps, 1)):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        ozb.qgemm(h, "n", "n", n, n, n, one, Aq, n, Bq, n, zero, Cq, n)
+        e1.record()
+        torch.cuda.synchronize()
+        ts.append(e0.elapsed_time(e1))
+    ms = min(ts)
+    out["qgemm"] = {"ms": ms, "slices": [h.nSplitA, h.nSplitB], "pairs": h.nSplitC,
+                    "split_ms": (h.t_SplitA + h.t_SplitB) * 1e3,
+                    "dgemm_equivalent_TFLOPS": 2.0 * n ** 3 / ms / 1e9,
+                    "slice_product_TFLOPS": 2.0 * n ** 3 * h.nSplitC / ms / 1e9}
     return out
 
 

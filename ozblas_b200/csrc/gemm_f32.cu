@@ -14,6 +14,7 @@
 // NearSum for mixed types (src/cpu/ozblas_sum.cpp:273-296 exits), so neither
 // does this form.
 #include <math.h>
+#include <stdlib.h>
 
 #include "ozb_internal.h"
 #include "sum.cuh"
@@ -278,6 +279,21 @@ int gemm_f32_core(cuozblasHandle_t *h, char ta, char tb, int m, int n, int k, do
     const bool dot = (m == 1 && n == 1);
     const bool skinny_n = (n == 1);
     const int ldk = dot || skinny_n ? ceil_to(k > 0 ? k : 1, 4) : ceil_to(k > 0 ? k : 1, kFK);
+
+    // rho >= 47 (k > 1024): every slice is an int8 times a power of two, and the
+    // exact slice products run on the INT8 tensor cores (same bits)
+    if (!dot && !skinny_n && rho >= 47 && !getenv("OZBLAS_DS_SIMT")) {
+        st->plain_timers = true;
+        int nA = 0, nB = 0, np = 0;
+        OZB_TRY(gemm_ds_i8_core(h, ta, tb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, rho, fastMode, &nA, &nB,
+                                &np));
+        h->nSplitA = (float)nA;
+        h->nSplitB = (float)nB;
+        h->nSplitC = (float)np;
+        h->mbk = m;
+        h->nbk = n;
+        return CUOZBLAS_STATUS_SUCCESS;
+    }
 
     // ---- split ----  (phase events 0..4: start, A split, B split, products, sum)
     ev_record(h, 0);

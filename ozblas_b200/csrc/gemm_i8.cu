@@ -64,6 +64,10 @@ struct I8Params {
     const int4 *items;   // {ia, ib, kb0, kb1} in processing order
     const int4 *groups;  // {item_begin, item_end, flush scale exponent, meta: shift | flush<<8 | first<<9 | last<<10}
     const int *ea, *eb;  // line exponents
+    // MODE 1 (the <double,float,float> form): slice exponents per level and line,
+    // [s][m] and [s][n], and the common scale 2 (rho - 53) of an INT8 slice product
+    const short *eas, *ebs;
+    int sbias;
     double alpha, beta;
     double *C;
     int *err;
@@ -79,6 +83,16 @@ __device__ __forceinline__ void tile_coords(int tile, const I8Params &p, int &tm
     tn = w / rows;
 }
 
+// v * 2^e as scalbn gives it (one rounding, in the subnormal range only).
+__device__ __forceinline__ double scale_exact(double v, int e) {
+    return (e >= -1000 && e <= 1000) ? v * pow2(e) : scalbn(v, e);
+}
+
+// MODE 0: the precision form (level groups, runs, correctly rounded sum).
+// MODE 1: the mixed form <double,float,float> with INT8 slices (each group is
+// one slice pair; its exact INT32 product V is added as scalbn(V, tauA + tauB +
+// sbias) to the FP64 sums in pair order, then C = fma(alpha, t, beta C)).
+template <int MODE>
 __global__ void __launch_bounds__(I8_THREADS, 1)
     k_i8_gemm(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, I8Params p) {
     extern __shared__ uint8_t smem_raw[];
@@ -228,9 +242,31 @@ __global__ void __launch_bounds__(I8_THREADS, 1)
                     break;
                 }
                 tc::fence_after_sync();
-                const double sc = pow2(meta & 0xff);
                 const uint32_t taddr = lane_base + abuf * I8_BN + half * 64;
                 uint32_t v[32];
+                if constexpr (MODE == 1) {
+                    const int4 pr = p.items[grp.x];
+                    const int era = (gr < p.m ? (int)p.eas[(size_t)pr.x * p.m + gr] : 0) + p.sbias;
+                    const short *ebr = p.ebs + (size_t)pr.y * p.n;
+                    const int gc0 = tn * I8_BN + half * 64;
+#pragma unroll
+                    for (int hh = 0; hh < 2; hh++) {
+                        tc::tmem_ld_32x32b_x32(taddr + 32 * hh, v);
+                        tc::tmem_ld_wait();
+#pragma unroll
+                        for (int c = 0; c < 32; c++) {
+                            const int gc = gc0 + 32 * hh + c;
+                            const int e = era + (gc < p.n ? (int)__ldg(ebr + gc) : 0);
+                            acc[32 * hh + c] += scale_exact((double)(int32_t)v[c], e);
+                        }
+                    }
+                    tc::fence_before_sync();
+                    tc::mbar_arrive(&acc_empty[abuf]);
+                    abuf ^= 1;
+                    if (abuf == 0) aphase ^= 1;
+                    continue;
+                }
+                const double sc = pow2(meta & 0xff);
                 tc::tmem_ld_32x32b_x32(taddr, v);
                 tc::tmem_ld_wait();
 #pragma unroll
@@ -296,6 +332,18 @@ __global__ void __launch_bounds__(I8_THREADS, 1)
                         }
                     }
                     if (!last) tc::tmem_st_wait();
+                }
+            }
+            if constexpr (MODE == 1) {
+                if (ok && gr < p.m) {
+#pragma unroll
+                    for (int c = 0; c < 64; c++) {
+                        const int gc = tn * I8_BN + half * 64 + c;
+                        if (gc < p.n) {
+                            double *cp = &p.C[(size_t)gc * p.ldc + gr];
+                            *cp = fma(p.alpha, acc[c], p.beta * *cp);
+                        }
+                    }
                 }
             }
         }
@@ -626,7 +674,7 @@ int gemm_i8_core(cuozblasHandle_t *h, char ta, char tb, int m, int n, int k, dou
     OZB_CHECK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
     const int ntiles = p.tiles_m * p.tiles_n;
     const int grid = ntiles < nsm ? ntiles : nsm;
-    OZB_CHECK(cudaFuncSetAttribute(k_i8_gemm, cudaFuncAttributeMaxDynamicSharedMemorySize, I8_SMEM));
+    OZB_CHECK(cudaFuncSetAttribute(k_i8_gemm<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, I8_SMEM));
     // Rasterisation strip height: any value gives the same bits, the fastest is
     // measured once per shape (candidates write a scratch product with beta = 0).
     {
@@ -650,7 +698,7 @@ int gemm_i8_core(cuozblasHandle_t *h, char ta, char tb, int m, int n, int k, dou
                 pt.beta = 0.0;
                 pick = tune_pick(key, (int)cand.size(), 0, st->stream, [&](int i) {
                     pt.strip = cand[(size_t)i];
-                    k_i8_gemm<<<grid, I8_THREADS, I8_SMEM, st->stream>>>(tmA, tmB, pt);
+                    k_i8_gemm<0><<<grid, I8_THREADS, I8_SMEM, st->stream>>>(tmA, tmB, pt);
                     return cudaGetLastError() == cudaSuccess ? 0 : (int)CUOZBLAS_STATUS_CUDA_ERROR;
                 });
             }
@@ -661,7 +709,7 @@ int gemm_i8_core(cuozblasHandle_t *h, char ta, char tb, int m, int n, int k, dou
     }
     ev_record(h, 2);
     counted(h);
-    k_i8_gemm<<<grid, I8_THREADS, I8_SMEM, st->stream>>>(tmA, tmB, p);
+    k_i8_gemm<0><<<grid, I8_THREADS, I8_SMEM, st->stream>>>(tmA, tmB, p);
     OZB_CHECK(cudaGetLastError());
     ev_record(h, 3);
     OZB_CHECK(cudaMemcpyAsync(st->h_ints, d_err, sizeof(int), cudaMemcpyDeviceToHost, st->stream));
@@ -674,6 +722,170 @@ int gemm_i8_core(cuozblasHandle_t *h, char ta, char tb, int m, int n, int k, dou
     h->t_SplitB = ev_ms(h, 1, 2) * 1e-3f;
     h->t_comp = ev_ms(h, 2, 3) * 1e-3f;
     h->t_sum = 0.f;  // fused into the product kernel
+    return CUOZBLAS_STATUS_SUCCESS;
+}
+
+// ---------------------------------------------------------------------------
+// The mixed form <double,float,float> on the INT8 tensor cores.  Its FP32
+// slice f = scalbn(s, -tau) is q 2^(rho - 53) with q an integer of magnitude at
+// most 2^(53 - rho) (src/cpu/ozblas_split.cpp:181-221), so for rho >= 47
+// (k > 1024 under splitEpsMode 0) every slice is an int8 q, and the FP32 slice
+// product sum(f_a f_b) = 2^(2 rho - 106) V with V the exact INT32 sum of the
+// q_a q_b (|V| <= 2^24 by the rho rule).  The ordered sum adds
+// scalbn(V, tauA + tauB + 2 rho - 106), the same value the reference adds.
+// ---------------------------------------------------------------------------
+// One CTA per line, the plain split arithmetic; writes q (int8) of every
+// level s at digits[(s * lines_pad + line) * k_pad + i] (the buffer is zeroed
+// before) and tau at exps[s * nl + line].  rem: k doubles per line (global).
+__global__ void __launch_bounds__(256) k_ds_digits(int k, int nl, const double *__restrict__ X, int ldx, int rho,
+                                                   int ns, int lines_pad, int k_pad, int8_t *__restrict__ digits,
+                                                   short *__restrict__ exps, double *__restrict__ rem) {
+    __shared__ double red[8];
+    const int line = blockIdx.x;
+    if (line >= nl) return;
+    const double *x = X + (size_t)line * ldx;
+    double *r = rem + (size_t)line * k;
+    double mx = 0.0;
+    for (int i = threadIdx.x; i < k; i += blockDim.x) {
+        const double v = x[i];
+        r[i] = v;
+        mx = ref_max(mx, fabs(v));
+    }
+    mx = block_max_nonneg(mx, red);
+    for (int s = 0; s < ns; s++) {
+        const int tau = tau_rule(mx);
+        const double sigma = 0.75 * pow2(rho + tau);
+        if (threadIdx.x == 0) exps[(size_t)s * nl + line] = (short)tau;
+        int8_t *o = digits + ((size_t)s * lines_pad + line) * k_pad;
+        double nm = 0.0;
+        for (int i = threadIdx.x; i < k; i += blockDim.x) {
+            double v = r[i];
+            const double sl = (v + sigma) - sigma;
+            v = v - sl;
+            r[i] = v;
+            nm = ref_max(nm, fabs(v));
+            // slices are q 2^(rho + tau - 53); scalbn is exact here and, unlike a
+            // multiplication by 2^(53 - rho - tau), cannot overflow for tiny tau
+            o[i] = (int8_t)(int)scalbn(sl, 53 - rho - tau);
+        }
+        mx = block_max_nonneg(nm, red);
+    }
+}
+
+// C = alpha op(A) op(B) + beta C in the <double,float,float> form with INT8
+// slices; the caller checks rho >= 47.  Returns the split counts in *nA, *nB.
+int gemm_ds_i8_core(cuozblasHandle_t *h, char ta, char tb, int m, int n, int k, double alpha, const double *A,
+                    int lda, const double *B, int ldb, double beta, double *C, int ldc, int rho, int fastMode,
+                    int *nA_out, int *nB_out, int *np_out) {
+    State *st = state(h);
+    Arena ar(h);
+    const int maxS = h->nSplitMax > 0 ? h->nSplitMax : kMaxSplitDefault;
+    const int k_pad = (k + I8_BK - 1) / I8_BK * I8_BK;
+    int ns[2];
+    int8_t *dig[2];
+    short *ex[2];
+    int lpad[2];
+    ev_record(h, 0);
+    for (int o = 0; o < 2; o++) {
+        const bool strided = o == 0 ? !is_trans(ta) : is_trans(tb);
+        const int nl = o == 0 ? m : n;
+        const double *X = o == 0 ? A : B;
+        const int ldx = o == 0 ? lda : ldb;
+        const double *src = X;
+        int lds = ldx;
+        const uint64_t mk = ar.mark();
+        if (strided) {
+            double *tmp = ar.take<double>((uint64_t)nl * k);
+            if (!ar.ok) return CUOZBLAS_STATUS_WORKSPACE;
+            OZB_TRY(transpose(h, nl, k, X, ldx, tmp, k));
+            src = tmp;
+            lds = k;
+        }
+        OZB_TRY(split_lines_count(h, k, nl, src, lds, rho, maxS, &ns[o]));
+        lpad[o] = (nl + I8_BM - 1) / I8_BM * I8_BM;
+        // slices and exponents stay below the temporaries
+        ar.release(mk);
+        dig[o] = ar.take<int8_t>((uint64_t)ns[o] * lpad[o] * k_pad);
+        ex[o] = ar.take<short>((uint64_t)ns[o] * nl);
+        if (!ar.ok) return CUOZBLAS_STATUS_WORKSPACE;
+        const uint64_t mk2 = ar.mark();
+        if (strided) {  // the transposed copy again, above the slices
+            double *tmp = ar.take<double>((uint64_t)nl * k);
+            if (!ar.ok) return CUOZBLAS_STATUS_WORKSPACE;
+            OZB_TRY(transpose(h, nl, k, X, ldx, tmp, k));
+            src = tmp;
+        }
+        double *rem = ar.take<double>((uint64_t)nl * k);
+        if (!ar.ok) return CUOZBLAS_STATUS_WORKSPACE;
+        OZB_CHECK(cudaMemsetAsync(dig[o], 0, (size_t)ns[o] * lpad[o] * k_pad, st->stream));
+        counted(h);
+        k_ds_digits<<<nl, 256, 0, st->stream>>>(k, nl, src, lds, rho, ns[o], lpad[o], k_pad, dig[o], ex[o], rem);
+        OZB_CHECK(cudaGetLastError());
+        ar.release(mk2);
+        ev_record(h, o + 1);
+    }
+    const int nA = ns[0], nB = ns[1];
+    int maxlevel = (nA - 1) + (nB - 1);
+    {
+        const int mn = nA - 1 < nB - 1 ? nA - 1 : nB - 1;
+        maxlevel = (maxlevel - fastMode) > mn ? (maxlevel - fastMode) : mn;  // src/cpu/ozblas_gemm.cpp:163-164
+    }
+    const int nkb = k_pad / I8_BK;
+    std::vector<int4> sched;
+    for (int ik = 0; ik <= maxlevel; ik++)  // FSum order: ik ascending, ia ascending
+        for (int ia = 0; ia < nA; ia++) {
+            const int ib = ik - ia;
+            if (ib >= 0 && ib < nB) sched.push_back(make_int4(ia, ib, 0, nkb));
+        }
+    const int np = (int)sched.size();
+    for (int g = 0; g < np; g++) sched.push_back(make_int4(g, g + 1, 0, 0));
+    int4 *d_sched = ar.take<int4>(sched.size());
+    int *d_err = ar.take<int>(1);
+    if (!ar.ok) return CUOZBLAS_STATUS_WORKSPACE;
+    OZB_CHECK(cudaMemcpyAsync(d_sched, sched.data(), sizeof(int4) * sched.size(), cudaMemcpyHostToDevice,
+                              st->stream));
+    OZB_CHECK(cudaMemsetAsync(d_err, 0, sizeof(int), st->stream));
+    CUtensorMap tmA, tmB;
+    OZB_TRY(make_map(&tmA, dig[0], (uint64_t)nA * lpad[0], k_pad, I8_BM));
+    OZB_TRY(make_map(&tmB, dig[1], (uint64_t)nB * lpad[1], k_pad, I8_BN));
+    I8Params p;
+    memset(&p, 0, sizeof(p));
+    p.m = m;
+    p.n = n;
+    p.m_pad = lpad[0];
+    p.n_pad = lpad[1];
+    p.ldc = ldc;
+    p.tiles_m = lpad[0] / I8_BM;
+    p.tiles_n = lpad[1] / I8_BN;
+    p.strip = p.tiles_m < 12 ? p.tiles_m : 12;
+    p.n_items = np;
+    p.n_groups = np;
+    p.items = d_sched;
+    p.groups = d_sched + np;
+    p.eas = ex[0];
+    p.ebs = ex[1];
+    p.sbias = 2 * (rho - 53);
+    p.alpha = alpha;
+    p.beta = beta;
+    p.C = C;
+    p.err = d_err;
+    const int nsm = sm_count();
+    const int ntiles = p.tiles_m * p.tiles_n;
+    OZB_CHECK(cudaFuncSetAttribute(k_i8_gemm<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, I8_SMEM));
+    counted(h);
+    k_i8_gemm<1><<<ntiles < nsm ? ntiles : nsm, I8_THREADS, I8_SMEM, st->stream>>>(tmA, tmB, p);
+    OZB_CHECK(cudaGetLastError());
+    ev_record(h, 3);
+    ev_record(h, 4);
+    OZB_CHECK(cudaMemcpyAsync(st->h_ints, d_err, sizeof(int), cudaMemcpyDeviceToHost, st->stream));
+    OZB_CHECK(cudaStreamSynchronize(st->stream));
+    if (st->h_ints[0] != 0) {
+        fprintf(stderr, "cuozblas: INT8 mixed-form kernel wait timed out (code %d)\n", st->h_ints[0]);
+        return CUOZBLAS_STATUS_DEVICE_TIMEOUT;
+    }
+    *nA_out = nA;
+    *nB_out = nB;
+    *np_out = np;
     return CUOZBLAS_STATUS_SUCCESS;
 }
 
@@ -899,8 +1111,8 @@ static int dgemm_i8_static(char ta, char tb, int m, int n, int k, double alpha, 
     OZB_CHECK(cudaGetDevice(&dev));
     OZB_CHECK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
     const int ntiles = p.tiles_m * p.tiles_n;
-    OZB_CHECK(cudaFuncSetAttribute(k_i8_gemm, cudaFuncAttributeMaxDynamicSharedMemorySize, I8_SMEM));
-    k_i8_gemm<<<ntiles < nsm ? ntiles : nsm, I8_THREADS, I8_SMEM, stream>>>(tmA, tmB, p);
+    OZB_CHECK(cudaFuncSetAttribute(k_i8_gemm<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, I8_SMEM));
+    k_i8_gemm<0><<<ntiles < nsm ? ntiles : nsm, I8_THREADS, I8_SMEM, stream>>>(tmA, tmB, p);
     OZB_CHECK(cudaGetLastError());
     int err = 0;
     OZB_CHECK(cudaMemcpyAsync(&err, d_err, sizeof(int), cudaMemcpyDeviceToHost, stream));

@@ -150,6 +150,11 @@ int rho_rule_f32(int dim, int splitEpsMode);
 int gemm_f32_core(cuozblasHandle_t *h, char ta, char tb, int m, int n, int k, double alpha, const double *A, int lda,
                   const double *B, int ldb, double beta, double *C, int ldc, int fastMode);
 
+// <double, float, float> with INT8 slices on tcgen05 (gemm_i8.cu), for rho >= 47
+int gemm_ds_i8_core(cuozblasHandle_t *h, char ta, char tb, int m, int n, int k, double alpha, const double *A,
+                    int lda, const double *B, int ldb, double beta, double *C, int ldc, int rho, int fastMode,
+                    int *nA, int *nB, int *np);
+
 // ---- mixed form <float, double, double> (gemm_plain.cu: the FP64-slice engine) ----
 int rho_rule_sd(int dim, int splitEpsMode);
 int gemm_sd_core(cuozblasHandle_t *h, char ta, char tb, int m, int n, int k, float alpha, const float *A, int lda,

@@ -68,6 +68,53 @@ def test_dsgemm(case, oracle, handle, ozb, cuda):
     assert (handle.nSplitA, handle.nSplitB, handle.nSplitC) == (info.nSplitA, info.nSplitB, info.nSplitC)
 
 
+DS_TC_CASES = [
+    # k > 1024: every FP32 slice is an int8 times a power of two, and the products run on tcgen05 kind::i8
+    (130, 100, 1500, "n", "n", 0, 0, 1.5, -1.0, 2.0),
+    (129, 70, 3000, "t", "t", 2, 0, 1.0, 0.5, 1.0),
+    (64, 200, 1025, "n", "t", 0, 3, -0.75, 0.0, 4.0),
+    (1, 300, 2048, "t", "n", 0, 0, 1.0, 0.0, 1.0),
+]
+
+
+@pytest.mark.parametrize("case", DS_TC_CASES, ids=lambda c: "x".join(map(str, c[:3])) + f"-{c[3]}{c[4]}-f{c[5]}")
+def test_dsgemm_tensor_core_path(case, oracle, handle, ozb, cuda):
+    m, n, k, ta, tb, fm, ns, alpha, beta, phi = case
+    ar, ac = (m, k) if ta == "n" else (k, m)
+    br, bc = (k, n) if tb == "n" else (n, k)
+    A = oracle.phi_matrix(ar, ac, phi, 1)
+    B = oracle.phi_matrix(br, bc, phi, 2)
+    C0 = oracle.phi_matrix(m, n, 1.0, 3)
+    ref, info = oracle.dgemm_f32(make_flags(fastMode=fm, nSplitMax=ns), ta, tb, m, n, k, alpha, A, ar, B, br, beta,
+                                 C0, m)
+    handle.fastMode, handle.nSplitMax = fm, ns
+    dC = dev(cuda, C0)
+    ozb.dsgemm(handle, ta, tb, m, n, k, alpha, dev(cuda, A), ar, dev(cuda, B), br, beta, dC, m)
+    out = host(dC)
+    assert bits_equal(out, ref), first_diff(out, ref)
+    assert (handle.nSplitA, handle.nSplitB, handle.nSplitC) == (info.nSplitA, info.nSplitB, info.nSplitC)
+
+
+@pytest.mark.parametrize("scale", [1.0, 2.0 ** -1040, 2.0 ** 950])
+def test_dsgemm_tensor_core_equals_simt(scale, oracle, handle, ozb, cuda, monkeypatch):
+    """At a size the oracle cannot afford, the INT8 tensor-core path gives the FP32 SIMT path's bits
+    (both are the reference's exact slice products and ordered sum), also with the scaling in the
+    subnormal range and near overflow."""
+    m, n, k = 700, 600, 4096
+    A = oracle.phi_matrix(m, k, 1.0, 1) * scale
+    B = oracle.phi_matrix(k, n, 1.0, 2)
+    dA, dB = dev(cuda, A), dev(cuda, B)
+    outs = []
+    for simt in (False, True):
+        if simt:
+            monkeypatch.setenv("OZBLAS_DS_SIMT", "1")
+        dC = cuda.zeros((n, m), dtype=cuda.float64, device="cuda")
+        ozb.dsgemm(handle, "n", "n", m, n, k, 1.0, dA, m, dB, k, 0.0, dC, m)
+        outs.append((host(dC), handle.nSplitC))
+    assert bits_equal(outs[0][0], outs[1][0]), first_diff(outs[0][0], outs[1][0])
+    assert outs[0][1] == outs[1][1]
+
+
 def test_dsgemm_run_to_run_identical(oracle, handle, ozb, cuda):
     m, n, k = 300, 200, 256
     A = oracle.phi_matrix(m, k, 1.0, 1)
