@@ -273,6 +273,8 @@ int cuozblasDgemmI8Static(char transa, char transb, int32_t m, int32_t n, int32_
 int cuozblasRuleTau(double v);
 /* tau of float data for the <float,double,double> form: (short)ceil((float)log2((double)v)) */
 int cuozblasRuleTauF32(float v);
+/* v * 2^e rounded once to nearest (the scaling of the mixed forms' ordered sums) */
+double cuozblasRuleScale2(double v, int32_t e);
 /* The software binary128 of the quad form, on the host: op 0 *out = *a + *b,
  * 1 *a * *b, 2 fma(*a, *b, *c), 3 (int) tau of *a, 4 the split of *a with
  * (int) rho, tau at b (out: remainder, then the slice as a double),

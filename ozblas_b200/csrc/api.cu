@@ -127,6 +127,8 @@ int cuozblasRuleTau(double v) { return tau_rule(v); }
 
 int cuozblasRuleTauF32(float v) { return tau_rule_f32(v); }
 
+double cuozblasRuleScale2(double v, int32_t e) { return scale2(v, e); }
+
 int cuozblasRuleQ128(int op, const void *a, const void *b, const void *c, void *out) {
     Q128 x, y, z;
     if (!a || !out) return CUOZBLAS_STATUS_INVALID_VALUE;

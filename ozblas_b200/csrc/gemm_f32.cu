@@ -16,6 +16,7 @@
 #include <math.h>
 #include <stdlib.h>
 
+#include "ozb_device.cuh"
 #include "ozb_internal.h"
 #include "sum.cuh"
 
@@ -129,7 +130,8 @@ __global__ void __launch_bounds__(kFThreads, 1)
             for (int i = 0; i < 8; i++)
 #pragma unroll
                 for (int j = 0; j < 8; j++) {
-                    tsum[(i * 8 + j) * kFThreads + tid] += scalbn((double)acc[i][j], ea[i] + eb[j]);
+                    double &ts = tsum[(i * 8 + j) * kFThreads + tid];
+                    ts = __dadd_rn(ts, scale2((double)acc[i][j], ea[i] + eb[j]));
                     acc[i][j] = 0.f;
                 }
         }
@@ -240,7 +242,7 @@ __global__ void k_sum_rows_f32(int m, int nA, int nB, int maxlevel, const float 
     if (row >= m) return;
     double t = 0.0;
     for_each_pair(nA, nB, maxlevel, [&](int ia, int ib) {
-        t += scalbn((double)P[(size_t)(ia * nB + ib) * ldp + row], Ea[(size_t)ia * ldea + row] + Eb[ib]);
+        t = __dadd_rn(t, scale2((double)P[(size_t)(ia * nB + ib) * ldp + row], Ea[(size_t)ia * ldea + row] + Eb[ib]));
     });
     y[row] = fma(alpha, t, beta * y[row]);
 }

@@ -83,11 +83,6 @@ __device__ __forceinline__ void tile_coords(int tile, const I8Params &p, int &tm
     tn = w / rows;
 }
 
-// v * 2^e as scalbn gives it (one rounding, in the subnormal range only).
-__device__ __forceinline__ double scale_exact(double v, int e) {
-    return (e >= -1000 && e <= 1000) ? v * pow2(e) : scalbn(v, e);
-}
-
 // MODE 0: the precision form (level groups, runs, correctly rounded sum).
 // MODE 1: the mixed form <double,float,float> with INT8 slices (each group is
 // one slice pair; its exact INT32 product V is added as scalbn(V, tauA + tauB +
@@ -237,7 +232,9 @@ __global__ void __launch_bounds__(I8_THREADS, 1)
             for (int g = 0; g < p.n_groups; g++) {
                 const int4 grp = p.groups[g];
                 const int meta = grp.w;
-                if (!tc::mbar_wait(&acc_full[abuf], aphase, &abort_flag, p.err, ERR_TIMEOUT_EPI, I8_WAIT_NS)) {
+                bool wok = tc::mbar_wait(&acc_full[abuf], aphase, &abort_flag, p.err, ERR_TIMEOUT_EPI, I8_WAIT_NS);
+                if constexpr (MODE == 1) wok = __all_sync(0xffffffffu, wok);  // the lanes agree before any shuffle
+                if (!wok) {
                     ok = false;
                     break;
                 }
@@ -248,16 +245,35 @@ __global__ void __launch_bounds__(I8_THREADS, 1)
                     const int4 pr = p.items[grp.x];
                     const int era = (gr < p.m ? (int)p.eas[(size_t)pr.x * p.m + gr] : 0) + p.sbias;
                     const short *ebr = p.ebs + (size_t)pr.y * p.n;
+                    // the warp's 64 columns are the same for all its lanes: lane l loads the
+                    // exponents of columns gc0 + l and gc0 + 32 + l, shuffles hand them round
                     const int gc0 = tn * I8_BN + half * 64;
+                    const int c0 = gc0 + lane, c1 = gc0 + 32 + lane;
+                    const int eb0 = c0 < p.n ? (int)__ldg(ebr + c0) : 0;
+                    const int eb1 = c1 < p.n ? (int)__ldg(ebr + c1) : 0;
+                    const int ebmin = __reduce_min_sync(0xffffffffu, eb0 < eb1 ? eb0 : eb1);
+                    const int ebmax = __reduce_max_sync(0xffffffffu, eb0 > eb1 ? eb0 : eb1);
+                    // V * 2^e is exact (normal) for |V| < 2^31 and e in [-1000, 1000]: one multiply
+                    const bool fast = __all_sync(0xffffffffu, era + ebmin >= -1000 && era + ebmax <= 1000);
 #pragma unroll
                     for (int hh = 0; hh < 2; hh++) {
                         tc::tmem_ld_32x32b_x32(taddr + 32 * hh, v);
                         tc::tmem_ld_wait();
+                        const int ebh = hh ? eb1 : eb0;
+                        if (fast) {
 #pragma unroll
-                        for (int c = 0; c < 32; c++) {
-                            const int gc = gc0 + 32 * hh + c;
-                            const int e = era + (gc < p.n ? (int)__ldg(ebr + gc) : 0);
-                            acc[32 * hh + c] += scale_exact((double)(int32_t)v[c], e);
+                            for (int c = 0; c < 32; c++) {
+                                const int e = era + __shfl_sync(0xffffffffu, ebh, c);
+                                acc[32 * hh + c] = __dadd_rn(acc[32 * hh + c],
+                                                             __dmul_rn((double)(int32_t)v[c],
+                                                                       from_bits((uint64_t)(e + 1023) << 52)));
+                            }
+                        } else {
+#pragma unroll
+                            for (int c = 0; c < 32; c++) {
+                                const int e = era + __shfl_sync(0xffffffffu, ebh, c);
+                                acc[32 * hh + c] = __dadd_rn(acc[32 * hh + c], scale2((double)(int32_t)v[c], e));
+                            }
                         }
                     }
                     tc::fence_before_sync();

@@ -128,7 +128,7 @@ __global__ void __launch_bounds__(128) k_gemm_pairs_dmma(int m, int n, int nlB, 
                         for (int h = 0; h < 2; h++) {
                             const float c32 = __double2float_rn(acc[i][j][h]);
                             tf[i][j][h] = __fadd_rn(tf[i][j][h],
-                                                    __double2float_rn(scalbn((double)c32, ea[i] + eb[j * 2 + h])));
+                                                    __double2float_rn(scale2((double)c32, ea[i] + eb[j * 2 + h])));
                             acc[i][j][h] = 0.0;
                         }
             } else if (STORE) {
@@ -633,7 +633,7 @@ __global__ void k_sum_rows_sd(int m, int nA, int nB, int maxlevel, const double 
     float t = 0.f;
     for_each_pair(nA, nB, maxlevel, [&](int ia, int ib) {
         const float c32 = __double2float_rn(P[(size_t)(ia * nB + ib) * ldp + row]);
-        t = __fadd_rn(t, __double2float_rn(scalbn((double)c32, Ea[(size_t)ia * ldea + row] + Eb[ib])));
+        t = __fadd_rn(t, __double2float_rn(scale2((double)c32, Ea[(size_t)ia * ldea + row] + Eb[ib])));
     });
     y[row] = __double2float_rn(fma((double)alpha, (double)t, (double)__fmul_rn(beta, y[row])));
 }

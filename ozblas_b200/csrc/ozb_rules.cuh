@@ -149,4 +149,33 @@ OZB_HD double pow2(int e) {
     return 0.0;
 }
 
+// v * 2^e rounded once to nearest, ties to even, as glibc's scalbn gives it
+// (exact unless the result is subnormal; overflow to infinity), in integer
+// arithmetic: no floating-point step that the compiler could fuse with the
+// caller's following addition.  Zero, infinities and NaN pass through.
+OZB_HD double scale2(double v, int e) {
+    const uint64_t b = dbits(v);
+    const uint64_t sign = b & 0x8000000000000000ULL;
+    const int be = (int)((b >> 52) & 0x7ff);
+    uint64_t M = b & ((1ULL << 52) - 1);
+    if (be == 0x7ff || (b << 1) == 0) return v;
+    int t;  // biased exponent of the result for significand M with the implicit bit at 2^52
+    if (be == 0) {  // subnormal input: normalise
+        const int msb = 63 - clz64(M);  // < 52
+        M <<= (52 - msb);
+        t = 1 - (52 - msb) + e;
+    } else {
+        M |= 1ULL << 52;
+        t = be + e;
+    }
+    if (t > 2046) return from_bits(sign | 0x7ff0000000000000ULL);
+    if (t >= 1) return from_bits(sign | ((uint64_t)t << 52) | (M & ((1ULL << 52) - 1)));
+    const int sh = 1 - t;  // onto the subnormal grid 2^-1074
+    if (sh > 54) return from_bits(sign);
+    uint64_t q = M >> sh;
+    const uint64_t rest = M & ((1ULL << sh) - 1), half = 1ULL << (sh - 1);
+    if (rest > half || (rest == half && (q & 1))) q += 1;  // q = 2^52 is the smallest normal: same bits
+    return from_bits(sign | q);
+}
+
 }  // namespace ozb

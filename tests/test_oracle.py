@@ -417,7 +417,7 @@ def test_c_abi_exports_every_declared_symbol():
     assert os.path.exists(lib), "libcuozblas_b200.so is not built"
     hdr = open(os.path.join(ROOT, "include", "cuozblas.h")).read()
     c_part = hdr.split('extern "C" {', 1)[1]
-    declared = set(re.findall(r"^\s*(?:int|const char \*)\s*(cuozblas\w+)\s*\(", c_part, re.M))
+    declared = set(re.findall(r"^\s*(?:int|double|const char \*)\s*(cuozblas\w+)\s*\(", c_part, re.M))
     assert len(declared) >= 15
     syms = subprocess.run(["nm", "-D", "--defined-only", lib], capture_output=True, text=True).stdout
     exported = set(re.findall(r" T (\w+)$", syms, re.M))
@@ -436,5 +436,5 @@ def test_python_binding_lists_c_abi():
     ozb = importlib.import_module("ozblas_b200")
     hdr = open(os.path.join(ROOT, "include", "cuozblas.h")).read()
     c_part = hdr.split('extern "C" {', 1)[1]
-    declared = set(re.findall(r"^\s*(?:int|const char \*)\s*(cuozblas\w+)\s*\(", c_part, re.M))
+    declared = set(re.findall(r"^\s*(?:int|double|const char \*)\s*(cuozblas\w+)\s*\(", c_part, re.M))
     assert declared == set(ozb.C_ABI_SYMBOLS)

@@ -159,3 +159,28 @@ def test_tau_of_binary128_every_exponent(lib, oracle, reference):
         if lib_tau(v) != reference.tau_q(v):
             bad.append(("sub", j))
     assert not bad, bad[:10]
+
+
+def test_scale2_matches_ldexp(lib):
+    """scale2 (the scaling the mixed forms add in their ordered sums, in integer arithmetic so that
+    nothing can be fused with the addition) = ldexp, correctly rounded, on integer-valued,
+    float-valued and general doubles across the normal, subnormal and overflow ranges (numpy's
+    ldexp is the C one)."""
+    import ctypes
+    lib.cuozblasRuleScale2.argtypes = [ctypes.c_double, ctypes.c_int32]
+    lib.cuozblasRuleScale2.restype = ctypes.c_double
+    rng = np.random.default_rng(9)
+    vals = list(rng.integers(-(1 << 31), 1 << 31, 3000).astype(float))
+    vals += list(rng.standard_normal(3000).astype(np.float32).astype(float) * np.exp2(rng.integers(-140, 120, 3000)))
+    vals += list(rng.standard_normal(3000) * np.exp2(rng.integers(-1070, 1020, 3000)))
+    vals += [0.0, -0.0, 1.0, -1.0, 5e-324, -5e-324, 2.0 ** -1022, 1.7976931348623157e308, float("inf")]
+    bad = []
+    for v in vals:
+        for e in (int(rng.integers(-2200, 2200)), int(rng.integers(-1100, -1000)), int(rng.integers(-60, 60)), -1074,
+                  -1075, 1023, 2000):
+            with np.errstate(over="ignore", under="ignore"):
+                want = float(np.ldexp(np.float64(v), e))
+            got = lib.cuozblasRuleScale2(v, e)
+            if np.float64(got).view(np.int64) != np.float64(want).view(np.int64):
+                bad.append((v, e, got, want))
+    assert not bad, bad[:5]
