@@ -68,6 +68,8 @@ struct I8Params {
     // [s][m] and [s][n], and the common scale 2 (rho - 53) of an INT8 slice product
     const short *eas, *ebs;
     int sbias;
+    // MODE 2 (exact FP64 pair products of digit-cut slices): output [pair][n][m]
+    double *pbuf;
     double alpha, beta;
     double *C;
     int *err;
@@ -84,6 +86,11 @@ __device__ __forceinline__ void tile_coords(int tile, const I8Params &p, int &tm
 }
 
 // MODE 0: the precision form (level groups, runs, correctly rounded sum).
+// MODE 2: exact FP64 products of slice pairs whose slices are cut into int8
+// digits: a group is one (pair, digit level L) with the INT32 products of its
+// digit pairs; the epilogue adds W 2^(group.w >> 8) to its FP64 sums (exact:
+// every partial sum of the pair is an integer below 2^53) and at the pair's
+// last level (group.w & 1) stores scalbn(sum, sbias) to pbuf[pair][col][row].
 // MODE 1: the mixed form <double,float,float> with INT8 slices (each group is
 // one slice pair; its exact INT32 product V is added as scalbn(V, tauA + tauB +
 // sbias) to the FP64 sums in pair order, then C = fma(alpha, t, beta C)).
@@ -241,6 +248,33 @@ __global__ void __launch_bounds__(I8_THREADS, 1)
                 tc::fence_after_sync();
                 const uint32_t taddr = lane_base + abuf * I8_BN + half * 64;
                 uint32_t v[32];
+                if constexpr (MODE == 2) {
+                    const double sc = pow2(grp.w >> 8);
+#pragma unroll
+                    for (int hh = 0; hh < 2; hh++) {
+                        tc::tmem_ld_32x32b_x32(taddr + 32 * hh, v);
+                        tc::tmem_ld_wait();
+#pragma unroll
+                        for (int c = 0; c < 32; c++)
+                            acc[32 * hh + c] = __dadd_rn(acc[32 * hh + c], __dmul_rn((double)(int32_t)v[c], sc));
+                    }
+                    tc::fence_before_sync();
+                    tc::mbar_arrive(&acc_empty[abuf]);
+                    abuf ^= 1;
+                    if (abuf == 0) aphase ^= 1;
+                    if (grp.w & 1) {  // the pair is complete
+                        if (gr < p.m) {
+#pragma unroll
+                            for (int c = 0; c < 64; c++) {
+                                const int gc = tn * I8_BN + half * 64 + c;
+                                if (gc < p.n) p.pbuf[((size_t)grp.z * p.n + gc) * p.m + gr] = scale2(acc[c], p.sbias);
+                            }
+                        }
+#pragma unroll
+                        for (int c = 0; c < 64; c++) acc[c] = 0.0;
+                    }
+                    continue;
+                }
                 if constexpr (MODE == 1) {
                     const int4 pr = p.items[grp.x];
                     const int era = (gr < p.m ? (int)p.eas[(size_t)pr.x * p.m + gr] : 0) + p.sbias;
@@ -902,6 +936,73 @@ int gemm_ds_i8_core(cuozblasHandle_t *h, char ta, char tb, int m, int n, int k, 
     *nA_out = nA;
     *nB_out = nB;
     *np_out = np;
+    return CUOZBLAS_STATUS_SUCCESS;
+}
+
+// Exact FP64 pair products on the INT8 tensor cores for slices cut into
+// `D` int8 digit planes (digits[(s D + d) * lines_pad + line][k_pad], most
+// significant first): for every pair of `pairs` (FSum order),
+// pbuf[pair][col][row] = 2^sbias sum_k qa qb with q = sum_d digit_d 2^(7(D-1-d)).
+// The caller guarantees D k 127^2 < 2^31 (INT32 groups) and that each pair's
+// |sum| stays below 2^53.
+int i8_exact_pairs(cuozblasHandle_t *h, int m, int n, int k_pad, const int8_t *digA, int lpadA, int planesA,
+                   const int8_t *digB, int lpadB, int planesB, int D, const std::vector<int2> &pairs, int sbias,
+                   double *pbuf) {
+    State *st = state(h);
+    Arena ar(h);
+    const uint64_t mk = ar.mark();
+    const int nkb = k_pad / I8_BK;
+    std::vector<int4> items, groups;
+    for (size_t pi = 0; pi < pairs.size(); pi++)
+        for (int L = 0; L <= 2 * D - 2; L++) {
+            const int beg = (int)items.size();
+            for (int d = 0; d < D; d++) {
+                const int e = L - d;
+                if (e >= 0 && e < D) items.push_back(make_int4(pairs[pi].x * D + d, pairs[pi].y * D + e, 0, nkb));
+            }
+            groups.push_back(make_int4(beg, (int)items.size(), (int)pi, ((7 * (2 * D - 2 - L)) << 8) | (L == 2 * D - 2)));
+        }
+    std::vector<int4> sched(items);
+    sched.insert(sched.end(), groups.begin(), groups.end());
+    int4 *d_sched = ar.take<int4>(sched.size());
+    int *d_err = ar.take<int>(1);
+    if (!ar.ok) return CUOZBLAS_STATUS_WORKSPACE;
+    OZB_CHECK(cudaMemcpyAsync(d_sched, sched.data(), sizeof(int4) * sched.size(), cudaMemcpyHostToDevice,
+                              st->stream));
+    OZB_CHECK(cudaMemsetAsync(d_err, 0, sizeof(int), st->stream));
+    CUtensorMap tmA, tmB;
+    OZB_TRY(make_map(&tmA, digA, (uint64_t)planesA * lpadA, k_pad, I8_BM));
+    OZB_TRY(make_map(&tmB, digB, (uint64_t)planesB * lpadB, k_pad, I8_BN));
+    I8Params p;
+    memset(&p, 0, sizeof(p));
+    p.m = m;
+    p.n = n;
+    p.m_pad = lpadA;
+    p.n_pad = lpadB;
+    p.ldc = m;
+    p.tiles_m = lpadA / I8_BM;
+    p.tiles_n = lpadB / I8_BN;
+    p.strip = p.tiles_m < 12 ? p.tiles_m : 12;
+    p.n_items = (int)items.size();
+    p.n_groups = (int)groups.size();
+    p.items = d_sched;
+    p.groups = d_sched + items.size();
+    p.sbias = sbias;
+    p.pbuf = pbuf;
+    p.err = d_err;
+    const int nsm = sm_count();
+    const int ntiles = p.tiles_m * p.tiles_n;
+    OZB_CHECK(cudaFuncSetAttribute(k_i8_gemm<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, I8_SMEM));
+    counted(h);
+    k_i8_gemm<2><<<ntiles < nsm ? ntiles : nsm, I8_THREADS, I8_SMEM, st->stream>>>(tmA, tmB, p);
+    OZB_CHECK(cudaGetLastError());
+    OZB_CHECK(cudaMemcpyAsync(st->h_ints, d_err, sizeof(int), cudaMemcpyDeviceToHost, st->stream));
+    OZB_CHECK(cudaStreamSynchronize(st->stream));
+    ar.release(mk);
+    if (st->h_ints[0] != 0) {
+        fprintf(stderr, "cuozblas: INT8 pair-product kernel wait timed out (code %d)\n", st->h_ints[0]);
+        return CUOZBLAS_STATUS_DEVICE_TIMEOUT;
+    }
     return CUOZBLAS_STATUS_SUCCESS;
 }
 

@@ -8,6 +8,8 @@
 // association, which lets the FP64 tensor pipe (DMMA) compute it.  What
 // fixes the bits is (1) the split and (2) the order of the pair sum, which
 // the fused epilogue follows exactly.
+#include <stdlib.h>
+
 #include "ozb_internal.h"
 #include "eft.cuh"
 #include "sum.cuh"
@@ -638,6 +640,46 @@ __global__ void k_sum_rows_sd(int m, int nA, int nB, int maxlevel, const double 
     y[row] = __double2float_rn(fma((double)alpha, (double)t, (double)__fmul_rn(beta, y[row])));
 }
 
+// FP64 slices q 2^-scale (slices [ns][nl][ldk], q an integer below 2^(7 D))
+// cut into D int8 digit planes, most significant first:
+// dig[((s D + d) lines_pad + line) k_pad + i] = sign(q) ((|q| >> 7 (D-1-d)) & 127).
+// The buffer is zeroed before (padding lines and columns stay zero).
+__global__ void k_slices_to_digits(int ns, int nl, int k, int ldk, const double *__restrict__ S, int scale, int D,
+                                   int lines_pad, int k_pad, int8_t *__restrict__ dig) {
+    const int64_t total = (int64_t)ns * nl * k;
+    for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < total; e += (int64_t)gridDim.x * blockDim.x) {
+        const int i = (int)(e % k);
+        const int64_t sl = e / k;  // s * nl + line
+        const int line = (int)(sl % nl), s = (int)(sl / nl);
+        const long long q = (long long)scale2(S[(size_t)sl * ldk + i], scale);
+        const unsigned long long aq = (unsigned long long)(q < 0 ? -q : q);
+        for (int d = 0; d < D; d++) {
+            const int dv = (int)((aq >> (7 * (D - 1 - d))) & 127);
+            dig[(((size_t)s * D + d) * lines_pad + line) * k_pad + i] = (int8_t)(q < 0 ? -dv : dv);
+        }
+    }
+}
+
+// The <float,double,double> ordered sum over a buffer of exact pair products
+// pbuf[p][col][row]: t(float) += (float)scalbn((float)P, tauA + tauB), then
+// C = (float)fma((double)alpha, t, (double)(beta * C)).
+__global__ void k_sum_pairs_sd(int m, int n, int np, const double *__restrict__ pbuf, const int2 *__restrict__ dp,
+                               const short *__restrict__ Ea, const short *__restrict__ Eb, float alpha, float beta,
+                               float *__restrict__ C, int ldc) {
+    const int64_t count = (int64_t)m * n;
+    const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= count) return;
+    const int row = (int)(e % m), col = (int)(e / m);
+    float t = 0.f;
+    for (int p = 0; p < np; p++) {
+        const int2 pr = dp[p];
+        const float c32 = __double2float_rn(pbuf[(size_t)p * count + e]);
+        t = __fadd_rn(t, __double2float_rn(scale2((double)c32, Ea[(size_t)pr.x * m + row] + Eb[(size_t)pr.y * n + col])));
+    }
+    float *cp = C + (size_t)col * ldc + row;
+    *cp = __double2float_rn(fma((double)alpha, (double)t, (double)__fmul_rn(beta, *cp)));
+}
+
 // Split op(X) (float, nl lines of length k) into FP64 slices ns x nl x ldk
 // and exponents ns x nl; X with strided lines is transposed first.
 static int split_operand_sd(cuozblasHandle_t *h, bool lines_strided, int nl, int k, const float *X, int ldx, int rho,
@@ -724,6 +766,53 @@ int gemm_sd_core(cuozblasHandle_t *h, char ta, char tb, int m, int n, int k, flo
         OZB_CHECK(cudaGetLastError());
         ev_record(h, 4);
         return CUOZBLAS_STATUS_SUCCESS;
+    }
+
+    // Pair products on the INT8 tensor cores: for rho >= 2 (k > 128) x + sigma
+    // stays in sigma's binade, so a slice is q 2^(rho - 24) with an integer
+    // |q| <= 2^(24 - rho) < 2^(7 D), cut into D <= 4 int8 digits; D k 127^2 must
+    // keep an INT32 group exact and the products of all pairs must fit.
+    {
+        const int D = (24 - rho + 1 + 6) / 7;
+        const int k_pad = (k + 127) / 128 * 128;
+        const int lpadA = (m + 127) / 128 * 128, lpadB = (n + 127) / 128 * 128;
+        const uint64_t need = (uint64_t)nA * D * lpadA * k_pad + (uint64_t)nB * D * lpadB * k_pad +
+                              sizeof(double) * (uint64_t)np * m * n + (1u << 20);
+        const uint64_t avail = h->workSizeBytes - ((ar.mark() + 255) / 256 * 256);
+        if (rho >= 2 && D <= 4 && (double)D * k * 127.0 * 127.0 < 2147483647.0 && need < avail &&
+            !getenv("OZBLAS_SD_DMMA")) {
+            std::vector<int2> pl;
+            for_each_pair(nA, nB, maxlevel, [&](int ia, int ib) { pl.push_back(make_int2(ia, ib)); });
+            int8_t *dg[2];
+            for (int o = 0; o < 2; o++) {
+                const int nl = o == 0 ? m : n, ns = o == 0 ? nA : nB, lpad = o == 0 ? lpadA : lpadB;
+                dg[o] = ar.take<int8_t>((uint64_t)ns * D * lpad * k_pad);
+                if (!ar.ok) return CUOZBLAS_STATUS_WORKSPACE;
+                OZB_CHECK(cudaMemsetAsync(dg[o], 0, (size_t)ns * D * lpad * k_pad, st->stream));
+                const int64_t total = (int64_t)ns * nl * k;
+                int blocks = (int)((total + 255) / 256);
+                if (blocks > 148 * 16) blocks = 148 * 16;
+                if (blocks < 1) blocks = 1;
+                counted(h);
+                k_slices_to_digits<<<blocks, 256, 0, st->stream>>>(ns, nl, k, ldk, o == 0 ? Sa : Sb, 24 - rho, D, lpad,
+                                                                  k_pad, dg[o]);
+                OZB_CHECK(cudaGetLastError());
+            }
+            double *pbuf = ar.take<double>((uint64_t)np * m * n);
+            int2 *dp = ar.take<int2>(np > 0 ? np : 1);
+            if (!ar.ok) return CUOZBLAS_STATUS_WORKSPACE;
+            OZB_CHECK(cudaMemcpyAsync(dp, pl.data(), sizeof(int2) * np, cudaMemcpyHostToDevice, st->stream));
+            OZB_TRY(i8_exact_pairs(h, m, n, k_pad, dg[0], lpadA, nA * D, dg[1], lpadB, nB * D, D, pl, 2 * (rho - 24),
+                                   pbuf));
+            const int64_t count = (int64_t)m * n;
+            counted(h);
+            k_sum_pairs_sd<<<(unsigned)((count + 255) / 256), 256, 0, st->stream>>>(m, n, np, pbuf, dp, Ea, Eb, alpha,
+                                                                                   beta, C, ldc);
+            OZB_CHECK(cudaGetLastError());
+            ev_record(h, 3);
+            ev_record(h, 4);
+            return CUOZBLAS_STATUS_SUCCESS;
+        }
     }
 
     int2 *hp = new int2[np > 0 ? np : 1];

@@ -15,6 +15,9 @@
 // FSum only: the reference has no NearSum for mixed types.
 #include <math.h>
 #include <string.h>
+#include <stdlib.h>
+
+#include <vector>
 
 #include "ozb_internal.h"
 #include "q128.cuh"
@@ -99,6 +102,48 @@ __global__ void __launch_bounds__(256) k_split_lines_q(int k, int nl, const Q128
         }
     }
     if (!WRITE && threadIdx.x == 0) atomicMax(zmax, z);
+}
+
+// The WRITE pass of k_split_lines_q with the slices cut into D int8 digit
+// planes instead of FP64 slices: slice = q 2^(rho - 113) with |q| < 2^(7 D),
+// digit d of level s = sign(q) ((|q| >> 7 (D - 1 - d)) & 127) at
+// dig[((s D + d) lines_pad + line) k_pad + i] (the buffer is zeroed before).
+__global__ void __launch_bounds__(256) k_split_lines_q_digits(int k, int nl, const Q128 *__restrict__ X, int64_t ls,
+                                                              int64_t es, int rho, int ns, int D, int lines_pad,
+                                                              int k_pad, int8_t *__restrict__ dig,
+                                                              short *__restrict__ exps, Q128 *__restrict__ rem) {
+    __shared__ Q128 red[8];
+    const int line = blockIdx.x;
+    if (line >= nl) return;
+    const Q128 *x = X + (size_t)line * ls;
+    Q128 *r = rem + (size_t)line * k;
+    Q128 mx = q_zero(0);
+    for (int i = threadIdx.x; i < k; i += blockDim.x) {
+        const Q128 v = q_ld(x + (size_t)i * es);
+        q_st(r + i, v);
+        const Q128 a = q_abs(v);
+        if (q_mag_less(mx, a)) mx = a;
+    }
+    mx = block_max_q(mx, red);
+    for (int s = 0; s < ns; s++) {
+        const int tau = tau_rule_q(mx);
+        if (threadIdx.x == 0) exps[(size_t)s * nl + line] = (short)tau;
+        Q128 nm = q_zero(0);
+        for (int i = threadIdx.x; i < k; i += blockDim.x) {
+            Q128 v = q_ld(r + i);
+            const double sl = q_split(v, rho, tau);
+            q_st(r + i, v);
+            const Q128 a = q_abs(v);
+            if (q_mag_less(nm, a)) nm = a;
+            const long long q = (long long)scale2(sl, 113 - rho);  // exact integer
+            const unsigned long long aq = (unsigned long long)(q < 0 ? -q : q);
+            for (int d = 0; d < D; d++) {
+                const int dv = (int)((aq >> (7 * (D - 1 - d))) & 127);
+                dig[(((size_t)s * D + d) * lines_pad + line) * k_pad + i] = (int8_t)(q < 0 ? -dv : dv);
+            }
+        }
+        mx = block_max_q(nm, red);
+    }
 }
 
 // General GEMM sum: element e = col * m + row of a block of nc columns from
@@ -227,6 +272,54 @@ int gemm_q_core(cuozblasHandle_t *h, char ta, char tb, int m, int n, int k, cons
         OZB_CHECK(cudaGetLastError());
         ev_record(h, 4);
         return CUOZBLAS_STATUS_SUCCESS;
+    }
+
+    // Pair products on the INT8 tensor cores when every slice is D <= 4 int8
+    // digits (|q| <= 2^(113 - rho) < 2^(7 D)), an INT32 group of D digit pairs
+    // over k stays exact, and the products of all pairs fit the arena at once.
+    {
+        const int D = (113 - rho + 1 + 6) / 7;
+        const int k_pad = (k + 127) / 128 * 128;
+        const int lpadA = (m + 127) / 128 * 128, lpadB = (n + 127) / 128 * 128;
+        const uint64_t need = (uint64_t)nA * D * lpadA * k_pad + (uint64_t)nB * D * lpadB * k_pad +
+                              sizeof(double) * (uint64_t)np * m * n + (uint64_t)16 * (m > n ? m : n) * k + (1u << 20);
+        const uint64_t avail = h->workSizeBytes - ((ar.mark() + 255) / 256 * 256);
+        if (D <= 4 && (double)D * k * 127.0 * 127.0 < 2147483647.0 && need < avail && !getenv("OZBLAS_Q_DMMA")) {
+            std::vector<int2> pl;
+            for_each_pair(nA, nB, maxlevel, [&](int ia, int ib) { pl.push_back(make_int2(ia, ib)); });
+            int8_t *dg[2];
+            for (int o = 0; o < 2; o++) {
+                const int nl = o == 0 ? m : n, ns = o == 0 ? nA : nB, lpad = o == 0 ? lpadA : lpadB;
+                const bool strided = o == 0 ? !is_trans(ta) : is_trans(tb);
+                const Q128 *X = o == 0 ? A : B;
+                const int ldx = o == 0 ? lda : ldb;
+                dg[o] = ar.take<int8_t>((uint64_t)ns * D * lpad * k_pad);
+                short *ex = o == 0 ? Ea : Eb;  // the FP64 split's exponents are the same taus
+                const uint64_t mk2 = ar.mark();
+                Q128 *rem = ar.take<Q128>((uint64_t)nl * (k > 0 ? k : 1));
+                if (!ar.ok) return CUOZBLAS_STATUS_WORKSPACE;
+                OZB_CHECK(cudaMemsetAsync(dg[o], 0, (size_t)ns * D * lpad * k_pad, st->stream));
+                counted(h);
+                k_split_lines_q_digits<<<nl, 256, 0, st->stream>>>(k, nl, X, strided ? 1 : ldx, strided ? ldx : 1, rho,
+                                                                   ns, D, lpad, k_pad, dg[o], ex, rem);
+                OZB_CHECK(cudaGetLastError());
+                ar.release(mk2);
+            }
+            double *pbuf = ar.take<double>((uint64_t)np * m * n);
+            int2 *dp = ar.take<int2>(np > 0 ? np : 1);
+            if (!ar.ok) return CUOZBLAS_STATUS_WORKSPACE;
+            OZB_CHECK(cudaMemcpyAsync(dp, pl.data(), sizeof(int2) * np, cudaMemcpyHostToDevice, st->stream));
+            OZB_TRY(i8_exact_pairs(h, m, n, k_pad, dg[0], lpadA, nA * D, dg[1], lpadB, nB * D, D, pl,
+                                   2 * (rho - 113), pbuf));
+            const int64_t count = (int64_t)m * n;
+            counted(h);
+            k_sum_pairs_q<<<(unsigned)((count + 255) / 256), 256, 0, st->stream>>>(m, n, count, 0, np, pbuf, dp, Ea,
+                                                                                  Eb, alpha, beta, C, ldc);
+            OZB_CHECK(cudaGetLastError());
+            ev_record(h, 3);
+            ev_record(h, 4);
+            return CUOZBLAS_STATUS_SUCCESS;
+        }
     }
 
     int2 *hp = new int2[np > 0 ? np : 1];

@@ -1,5 +1,6 @@
 // ozb_internal.h — host-side state shared by the library's translation units.
 #pragma once
+#include <vector>
 #include <cuda_runtime.h>
 #include <stdint.h>
 #include <stdio.h>
@@ -165,6 +166,11 @@ int gemm_pairs_store(cuozblasHandle_t *h, int m, int nc, int nlB, int ldk, const
                      const int2 *dp, int np, double *pbuf);
 int pair_products_skinny(cuozblasHandle_t *h, bool dot, int m, int k, int nA, int nB, const double *Sa,
                          const double *Sb, int ldk, double *P);
+
+// exact FP64 pair products of int8-digit slices on tcgen05 (gemm_i8.cu)
+int i8_exact_pairs(cuozblasHandle_t *h, int m, int n, int k_pad, const int8_t *digA, int lpadA, int planesA,
+                   const int8_t *digB, int lpadB, int planesB, int D, const std::vector<int2> &pairs, int sbias,
+                   double *pbuf);
 
 // ---- quad I/O form <__float128, double, double> (gemm_q.cu); binary128 as 16 bytes ----
 int gemm_q_core(cuozblasHandle_t *h, char ta, char tb, int m, int n, int k, const void *alpha, const void *A, int lda,

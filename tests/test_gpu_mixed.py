@@ -417,3 +417,45 @@ def test_q_unsupported_flags(oracle, handle, ozb, cuda):
     with pytest.raises(ozb.OzblasError) as e:
         ozb.qdot(handle, 8, x, x)
     assert e.value.code == 4
+
+
+@pytest.mark.parametrize("m,n,k,ta,tb", [(300, 260, 1000, "n", "n"), (129, 400, 4096, "t", "n"), (257, 130, 60, "n", "t")])
+def test_qgemm_tensor_core_equals_dmma(m, n, k, ta, tb, oracle, handle, ozb, cuda, monkeypatch):
+    """The quad form's pair products on the INT8 tensor cores (slices cut into int8 digits, exact
+    INT32 digit products combined exactly in FP64) give the DMMA kernel's bits, beta C included."""
+    ar, ac = (m, k) if ta == "n" else (k, m)
+    br, bc = (k, n) if tb == "n" else (n, k)
+    A = oracle.phi_matrix_q(ar, ac, 2.0, 1)
+    B = oracle.phi_matrix_q(br, bc, 1.0, 2)
+    C0 = oracle.phi_matrix_q(m, n, 1.0, 3)
+    al, be = oracle.q(1.25), oracle.q(-0.5)
+    outs = []
+    for dmma in (False, True):
+        if dmma:
+            monkeypatch.setenv("OZBLAS_Q_DMMA", "1")
+        dC = qdev(cuda, C0)
+        ozb.qgemm(handle, ta, tb, m, n, k, al, qdev(cuda, A), ar, qdev(cuda, B), br, be, dC, m)
+        outs.append((qhost(dC), handle.nSplitC))
+    assert np.array_equal(outs[0][0], outs[1][0])
+    assert outs[0][1] == outs[1][1]
+
+
+@pytest.mark.parametrize("m,n,k,ta,tb,scale", [(300, 260, 1000, "n", "n", 1.0), (129, 400, 4096, "t", "t", 1.0),
+                                                (257, 130, 200, "n", "t", 2.0 ** -120), (200, 200, 3000, "n", "n", 2.0 ** 60)])
+def test_sdgemm_tensor_core_equals_dmma(m, n, k, ta, tb, scale, oracle, handle, ozb, cuda, monkeypatch):
+    """The <float,double,double> pair products on the INT8 tensor cores (k > 128: FP64 slices cut into
+    int8 digits) give the DMMA kernel's bits, with products scaled near the ends of float's range."""
+    ar, ac = (m, k) if ta == "n" else (k, m)
+    br, bc = (k, n) if tb == "n" else (n, k)
+    A = (oracle.phi_matrix(ar, ac, 2.0, 1) * scale).astype(np.float32)
+    B = oracle.phi_matrix(br, bc, 1.0, 2).astype(np.float32)
+    C0 = oracle.phi_matrix(m, n, 1.0, 3).astype(np.float32)
+    outs = []
+    for dmma in (False, True):
+        if dmma:
+            monkeypatch.setenv("OZBLAS_SD_DMMA", "1")
+        dC = dev(cuda, C0)
+        ozb.sdgemm(handle, ta, tb, m, n, k, 1.25, dev(cuda, A), ar, dev(cuda, B), br, -0.5, dC, m)
+        outs.append((host(dC), handle.nSplitC))
+    assert f32_bits_equal(outs[0][0], outs[1][0]), f32_first_diff(outs[0][0], outs[1][0])
+    assert outs[0][1] == outs[1][1]
