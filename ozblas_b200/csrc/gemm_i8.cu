@@ -68,8 +68,10 @@ struct I8Params {
     // [s][m] and [s][n], and the common scale 2 (rho - 53) of an INT8 slice product
     const short *eas, *ebs;
     int sbias;
-    // MODE 2 (exact FP64 pair products of digit-cut slices): output [pair][n][m]
+    // MODE 2 (exact FP64 pair products of digit-cut slices): output [pair][n][m];
+    // digit planes per slice level; eas/ebs (or null) add tauA + tauB per element
     double *pbuf;
+    int D;
     double alpha, beta;
     double *C;
     int *err;
@@ -264,10 +266,15 @@ __global__ void __launch_bounds__(I8_THREADS, 1)
                     if (abuf == 0) aphase ^= 1;
                     if (grp.w & 1) {  // the pair is complete
                         if (gr < p.m) {
+                            const int4 it = p.items[grp.x];
+                            const short *ebr = p.ebs ? p.ebs + (size_t)(it.y / p.D) * p.n : nullptr;
+                            const int er = p.sbias + (p.eas ? (int)p.eas[(size_t)(it.x / p.D) * p.m + gr] : 0);
 #pragma unroll
                             for (int c = 0; c < 64; c++) {
                                 const int gc = tn * I8_BN + half * 64 + c;
-                                if (gc < p.n) p.pbuf[((size_t)grp.z * p.n + gc) * p.m + gr] = scale2(acc[c], p.sbias);
+                                if (gc < p.n)
+                                    p.pbuf[((size_t)grp.z * p.n + gc) * p.m + gr] =
+                                        scale2(acc[c], er + (ebr ? (int)ebr[gc] : 0));
                             }
                         }
 #pragma unroll
@@ -942,12 +949,14 @@ int gemm_ds_i8_core(cuozblasHandle_t *h, char ta, char tb, int m, int n, int k, 
 // Exact FP64 pair products on the INT8 tensor cores for slices cut into
 // `D` int8 digit planes (digits[(s D + d) * lines_pad + line][k_pad], most
 // significant first): for every pair of `pairs` (FSum order),
-// pbuf[pair][col][row] = 2^sbias sum_k qa qb with q = sum_d digit_d 2^(7(D-1-d)).
+// pbuf[pair][col][row] = 2^(sbias + tauA + tauB) sum_k qa qb with
+// q = sum_d digit_d 2^(7(D-1-d)) (tauA = eas[ia][row], tauB = ebs[ib][col], or 0
+// without them), rounded once if it is subnormal.
 // The caller guarantees D k 127^2 < 2^31 (INT32 groups) and that each pair's
 // |sum| stays below 2^53.
 int i8_exact_pairs(cuozblasHandle_t *h, int m, int n, int k_pad, const int8_t *digA, int lpadA, int planesA,
                    const int8_t *digB, int lpadB, int planesB, int D, const std::vector<int2> &pairs, int sbias,
-                   double *pbuf) {
+                   const short *eas, const short *ebs, double *pbuf) {
     State *st = state(h);
     Arena ar(h);
     const uint64_t mk = ar.mark();
@@ -989,6 +998,9 @@ int i8_exact_pairs(cuozblasHandle_t *h, int m, int n, int k_pad, const int8_t *d
     p.groups = d_sched + items.size();
     p.sbias = sbias;
     p.pbuf = pbuf;
+    p.D = D;
+    p.eas = eas;
+    p.ebs = ebs;
     p.err = d_err;
     const int nsm = sm_count();
     const int ntiles = p.tiles_m * p.tiles_n;

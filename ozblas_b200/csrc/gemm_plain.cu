@@ -10,6 +10,8 @@
 // the fused epilogue follows exactly.
 #include <stdlib.h>
 
+#include <vector>
+
 #include "ozb_internal.h"
 #include "eft.cuh"
 #include "sum.cuh"
@@ -387,7 +389,7 @@ static int ceil_to(int v, int q) { return (v + q - 1) / q * q; }
 // Split op(A) by rows (lines of length k) into ns slices of m x ldk.  If A is
 // 'n' (m x k, column-major) it is first transposed so every line is contiguous.
 static int split_operand(cuozblasHandle_t *h, bool lines_strided, int nl, int k, const double *X, int ldx, int rho,
-                         int maxS, int ldk, double **slices, int *ns, Arena &ar) {
+                         int maxS, int ldk, double **slices, int *ns, Arena &ar, short **exps = nullptr) {
     const double *src = X;
     int lds = ldx;
     double *tmp = nullptr;
@@ -408,12 +410,20 @@ static int split_operand(cuozblasHandle_t *h, bool lines_strided, int nl, int k,
     } else {
         out = ar.take<double>((uint64_t)(*ns) * nl * ldk);
     }
+    if (exps) *exps = ar.take<short>((uint64_t)(*ns) * (nl > 0 ? nl : 1));
     if (!ar.ok) return CUOZBLAS_STATUS_WORKSPACE;
-    OZB_TRY(split_lines_write(h, k, nl, src, lds, rho, *ns, out, ldk));
+    if (exps)
+        OZB_TRY(split_lines_write_e(h, k, nl, src, lds, rho, *ns, out, ldk, *exps));
+    else
+        OZB_TRY(split_lines_write(h, k, nl, src, lds, rho, *ns, out, ldk));
     (void)mk;
     *slices = out;
     return CUOZBLAS_STATUS_SUCCESS;
 }
+
+__global__ void k_slices_to_digits(int ns, int nl, int k, int ldk, const double *__restrict__ S, int scale,
+                                   const short *__restrict__ exps, int D, int lines_pad, int k_pad,
+                                   int8_t *__restrict__ dig);  // below
 
 int gemm_plain_core(cuozblasHandle_t *h, char ta, char tb, int m, int n, int k, double alpha, const double *A,
                     int lda, const double *B, int ldb, double beta, double *C, int ldc, int fastMode) {
@@ -429,6 +439,7 @@ int gemm_plain_core(cuozblasHandle_t *h, char ta, char tb, int m, int n, int k, 
     ev_record(h, 0);
     st->plain_timers = true;
     double *Sa = nullptr, *Sb = nullptr;
+    short *Ea = nullptr, *Eb = nullptr;  // taus per line and level (general GEMM: the INT8 product path)
     int nA = 0, nB = 0;
     if (dot) {
         Sa = ar.take<double>((uint64_t)maxS * ldk);
@@ -436,7 +447,7 @@ int gemm_plain_core(cuozblasHandle_t *h, char ta, char tb, int m, int n, int k, 
         OZB_TRY(split_vector(h, k, A, rho, maxS, Sa, ldk, &nA));
     } else {
         // lines of op(A): 'n' -> row i of A is strided by lda
-        OZB_TRY(split_operand(h, !is_trans(ta), m, k, A, lda, rho, maxS, ldk, &Sa, &nA, ar));
+        OZB_TRY(split_operand(h, !is_trans(ta), m, k, A, lda, rho, maxS, ldk, &Sa, &nA, ar, skinny_n ? nullptr : &Ea));
     }
     ev_record(h, 1);
     if (skinny_n) {
@@ -444,7 +455,7 @@ int gemm_plain_core(cuozblasHandle_t *h, char ta, char tb, int m, int n, int k, 
         if (!ar.ok) return CUOZBLAS_STATUS_WORKSPACE;
         OZB_TRY(split_vector(h, k, B, rho, maxS, Sb, ldk, &nB));
     } else {
-        OZB_TRY(split_operand(h, is_trans(tb), n, k, B, ldb, rho, maxS, ldk, &Sb, &nB, ar));
+        OZB_TRY(split_operand(h, is_trans(tb), n, k, B, ldb, rho, maxS, ldk, &Sb, &nB, ar, &Eb));
     }
     ev_record(h, 2);
     const int fast = dot ? 0 : fastMode;
@@ -520,6 +531,50 @@ int gemm_plain_core(cuozblasHandle_t *h, char ta, char tb, int m, int n, int k, 
     }
 
     // ---- general GEMM ----
+    // Pair products on the INT8 tensor cores: a slice is q 2^(rho + tau - 53)
+    // with an integer |q| <= 2^(53 - rho) < 2^(7 D), cut into D <= 4 int8 digits;
+    // the kernel stores the exact FP64 pair products (the DMMA kernel's values)
+    // and the ordered sum (FSum or NearSum) reads them as before.
+    {
+        const int D = (53 - rho + 1 + 6) / 7;
+        const int k_pad = (k + 127) / 128 * 128;
+        const int lpadA = (m + 127) / 128 * 128, lpadB = (n + 127) / 128 * 128;
+        const uint64_t need = (uint64_t)nA * D * lpadA * k_pad + (uint64_t)nB * D * lpadB * k_pad +
+                              sizeof(double) * (uint64_t)np * m * n + (1u << 20);
+        const uint64_t avail = h->workSizeBytes - ((ar.mark() + 255) / 256 * 256);
+        if (Ea && Eb && D <= 4 && (double)D * k * 127.0 * 127.0 < 2147483647.0 && need < avail &&
+            !getenv("OZBLAS_PLAIN_DMMA")) {
+            std::vector<int2> pl;
+            for_each_pair(nA, nB, maxlevel, [&](int ia, int ib) { pl.push_back(make_int2(ia, ib)); });
+            int8_t *dg[2];
+            for (int o = 0; o < 2; o++) {
+                const int nl = o == 0 ? m : n, ns = o == 0 ? nA : nB, lpad = o == 0 ? lpadA : lpadB;
+                dg[o] = ar.take<int8_t>((uint64_t)ns * D * lpad * k_pad);
+                if (!ar.ok) return CUOZBLAS_STATUS_WORKSPACE;
+                OZB_CHECK(cudaMemsetAsync(dg[o], 0, (size_t)ns * D * lpad * k_pad, st->stream));
+                const int64_t total = (int64_t)ns * nl * k;
+                int blocks = (int)((total + 255) / 256);
+                if (blocks > 148 * 16) blocks = 148 * 16;
+                if (blocks < 1) blocks = 1;
+                counted(h);
+                k_slices_to_digits<<<blocks, 256, 0, st->stream>>>(ns, nl, k, ldk, o == 0 ? Sa : Sb, 53 - rho,
+                                                                  o == 0 ? Ea : Eb, D, lpad, k_pad, dg[o]);
+                OZB_CHECK(cudaGetLastError());
+            }
+            double *pbuf = ar.take<double>((uint64_t)np * m * n);
+            if (!ar.ok) return CUOZBLAS_STATUS_WORKSPACE;
+            OZB_TRY(i8_exact_pairs(h, m, n, k_pad, dg[0], lpadA, nA * D, dg[1], lpadB, nB * D, D, pl, 2 * (rho - 53),
+                                   Ea, Eb, pbuf));
+            ev_record(h, 3);
+            const int64_t count = (int64_t)m * n;
+            counted(h);
+            k_sum_pairs<<<(unsigned)((count + 255) / 256), 256, 0, st->stream>>>(m, count, np, pbuf, count,
+                                                                                h->sumMode, alpha, beta, C, ldc);
+            OZB_CHECK(cudaGetLastError());
+            ev_record(h, 4);
+            return CUOZBLAS_STATUS_SUCCESS;
+        }
+    }
     int2 *hp = new int2[np > 0 ? np : 1];
     int q = 0;
     for_each_pair(nA, nB, maxlevel, [&](int ia, int ib) { hp[q++] = make_int2(ia, ib); });
@@ -640,18 +695,21 @@ __global__ void k_sum_rows_sd(int m, int nA, int nB, int maxlevel, const double 
     y[row] = __double2float_rn(fma((double)alpha, (double)t, (double)__fmul_rn(beta, y[row])));
 }
 
-// FP64 slices q 2^-scale (slices [ns][nl][ldk], q an integer below 2^(7 D))
+// FP64 slices q 2^-(scale - tau) (slices [ns][nl][ldk], tau = exps[s * nl + line] or
+// 0, q an integer below 2^(7 D))
 // cut into D int8 digit planes, most significant first:
 // dig[((s D + d) lines_pad + line) k_pad + i] = sign(q) ((|q| >> 7 (D-1-d)) & 127).
 // The buffer is zeroed before (padding lines and columns stay zero).
-__global__ void k_slices_to_digits(int ns, int nl, int k, int ldk, const double *__restrict__ S, int scale, int D,
-                                   int lines_pad, int k_pad, int8_t *__restrict__ dig) {
+__global__ void k_slices_to_digits(int ns, int nl, int k, int ldk, const double *__restrict__ S, int scale,
+                                   const short *__restrict__ exps, int D, int lines_pad, int k_pad,
+                                   int8_t *__restrict__ dig) {
     const int64_t total = (int64_t)ns * nl * k;
     for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < total; e += (int64_t)gridDim.x * blockDim.x) {
         const int i = (int)(e % k);
         const int64_t sl = e / k;  // s * nl + line
         const int line = (int)(sl % nl), s = (int)(sl / nl);
-        const long long q = (long long)scale2(S[(size_t)sl * ldk + i], scale);
+        const int sc = exps ? scale - (int)exps[sl] : scale;  // plain slices: q 2^(rho + tau - 53)
+        const long long q = (long long)scale2(S[(size_t)sl * ldk + i], sc);
         const unsigned long long aq = (unsigned long long)(q < 0 ? -q : q);
         for (int d = 0; d < D; d++) {
             const int dv = (int)((aq >> (7 * (D - 1 - d))) & 127);
@@ -794,8 +852,8 @@ int gemm_sd_core(cuozblasHandle_t *h, char ta, char tb, int m, int n, int k, flo
                 if (blocks > 148 * 16) blocks = 148 * 16;
                 if (blocks < 1) blocks = 1;
                 counted(h);
-                k_slices_to_digits<<<blocks, 256, 0, st->stream>>>(ns, nl, k, ldk, o == 0 ? Sa : Sb, 24 - rho, D, lpad,
-                                                                  k_pad, dg[o]);
+                k_slices_to_digits<<<blocks, 256, 0, st->stream>>>(ns, nl, k, ldk, o == 0 ? Sa : Sb, 24 - rho, nullptr,
+                                                                  D, lpad, k_pad, dg[o]);
                 OZB_CHECK(cudaGetLastError());
             }
             double *pbuf = ar.take<double>((uint64_t)np * m * n);
@@ -803,7 +861,7 @@ int gemm_sd_core(cuozblasHandle_t *h, char ta, char tb, int m, int n, int k, flo
             if (!ar.ok) return CUOZBLAS_STATUS_WORKSPACE;
             OZB_CHECK(cudaMemcpyAsync(dp, pl.data(), sizeof(int2) * np, cudaMemcpyHostToDevice, st->stream));
             OZB_TRY(i8_exact_pairs(h, m, n, k_pad, dg[0], lpadA, nA * D, dg[1], lpadB, nB * D, D, pl, 2 * (rho - 24),
-                                   pbuf));
+                                   nullptr, nullptr, pbuf));
             const int64_t count = (int64_t)m * n;
             counted(h);
             k_sum_pairs_sd<<<(unsigned)((count + 255) / 256), 256, 0, st->stream>>>(m, n, np, pbuf, dp, Ea, Eb, alpha,

@@ -310,7 +310,7 @@ int gemm_q_core(cuozblasHandle_t *h, char ta, char tb, int m, int n, int k, cons
             if (!ar.ok) return CUOZBLAS_STATUS_WORKSPACE;
             OZB_CHECK(cudaMemcpyAsync(dp, pl.data(), sizeof(int2) * np, cudaMemcpyHostToDevice, st->stream));
             OZB_TRY(i8_exact_pairs(h, m, n, k_pad, dg[0], lpadA, nA * D, dg[1], lpadB, nB * D, D, pl,
-                                   2 * (rho - 113), pbuf));
+                                   2 * (rho - 113), nullptr, nullptr, pbuf));
             const int64_t count = (int64_t)m * n;
             counted(h);
             k_sum_pairs_q<<<(unsigned)((count + 255) / 256), 256, 0, st->stream>>>(m, n, count, 0, np, pbuf, dp, Ea,

@@ -120,6 +120,9 @@ int counter_init(cuozblasHandle_t *h);
 int split_lines_count(cuozblasHandle_t *h, int k, int nl, const double *X, int ldx, int rho, int maxS, int *ns);
 int split_lines_write(cuozblasHandle_t *h, int k, int nl, const double *X, int ldx, int rho, int ns, double *out,
                       int ldo);
+// As split_lines_write, also recording tau of every level at exps[level * nl + line].
+int split_lines_write_e(cuozblasHandle_t *h, int k, int nl, const double *X, int ldx, int rho, int ns, double *out,
+                        int ldo, short *exps);
 // Mixed form <double, float, float>: FP32 slices scalbn(slice, -tau) with tau
 // per level at exps[level * nl + line] (lines) or exps[level] (vector).
 int split_lines_write_f32(cuozblasHandle_t *h, int k, int nl, const double *X, int ldx, int rho, int ns, float *out,
@@ -170,7 +173,7 @@ int pair_products_skinny(cuozblasHandle_t *h, bool dot, int m, int k, int nA, in
 // exact FP64 pair products of int8-digit slices on tcgen05 (gemm_i8.cu)
 int i8_exact_pairs(cuozblasHandle_t *h, int m, int n, int k_pad, const int8_t *digA, int lpadA, int planesA,
                    const int8_t *digB, int lpadB, int planesB, int D, const std::vector<int2> &pairs, int sbias,
-                   double *pbuf);
+                   const short *eas, const short *ebs, double *pbuf);
 
 // ---- quad I/O form <__float128, double, double> (gemm_q.cu); binary128 as 16 bytes ----
 int gemm_q_core(cuozblasHandle_t *h, char ta, char tb, int m, int n, int k, const void *alpha, const void *A, int lda,

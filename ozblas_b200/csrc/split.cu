@@ -140,6 +140,12 @@ int split_lines_write(cuozblasHandle_t *h, int k, int nl, const double *X, int l
     return launch_split_lines<double>(h, true, k, nl, X, ldx, rho, ns, out, ldo, nullptr, nullptr);
 }
 
+int split_lines_write_e(cuozblasHandle_t *h, int k, int nl, const double *X, int ldx, int rho, int ns, double *out,
+                        int ldo, short *exps) {
+    if (nl == 0 || ns == 0) return CUOZBLAS_STATUS_SUCCESS;
+    return launch_split_lines<double>(h, true, k, nl, X, ldx, rho, ns, out, ldo, exps, nullptr);
+}
+
 int split_lines_write_f32(cuozblasHandle_t *h, int k, int nl, const double *X, int ldx, int rho, int ns, float *out,
                           int ldo, short *exps) {
     if (nl == 0 || ns == 0) return CUOZBLAS_STATUS_SUCCESS;

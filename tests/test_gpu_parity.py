@@ -507,3 +507,27 @@ def test_dcsrmv_fastmode_uses_general_path(oracle, handle, ozb, cuda):
     y0 = np.zeros(n)
     # fastMode = 1 drops only the last level: pair sets agree with the reference's storage
     _csr_run(oracle, handle, ozb, cuda, rowptr, colind, val, x, y0, 1.0, 0.0, 0, fm=1)
+
+
+@pytest.mark.parametrize("sm", [0, 1])
+@pytest.mark.parametrize("m,n,k,ta,tb,scale", [(600, 500, 4096, "n", "n", 1.0), (257, 300, 1000, "t", "t", 2.0 ** -900),
+                                                (130, 129, 2000, "n", "t", 2.0 ** 700)])
+def test_dgemm_tensor_core_pairs_equal_dmma(sm, m, n, k, ta, tb, scale, oracle, handle, ozb, cuda, monkeypatch):
+    """The plain form's exact slice-pair products on the INT8 tensor cores (slices cut into int8
+    digits, exact INT32 digit products combined exactly in FP64, scaled by 2^(tauA + tauB)) give the
+    DMMA kernel's bits under FSum and NearSum, also for data far from 1."""
+    ar, ac = (m, k) if ta == "n" else (k, m)
+    br, bc = (k, n) if tb == "n" else (n, k)
+    A = oracle.phi_matrix(ar, ac, 2.0, 1) * scale
+    B = oracle.phi_matrix(br, bc, 1.0, 2)
+    C0 = oracle.phi_matrix(m, n, 1.0, 3)
+    handle.sumMode = sm
+    outs = []
+    for dmma in (False, True):
+        if dmma:
+            monkeypatch.setenv("OZBLAS_PLAIN_DMMA", "1")
+        dC = dev(cuda, C0)
+        ozb.dgemm(handle, ta, tb, m, n, k, 1.25, dev(cuda, A), ar, dev(cuda, B), br, -0.5, dC, m)
+        outs.append((host(dC), handle.nSplitC))
+    assert bits_equal(outs[0][0], outs[1][0]), first_diff(outs[0][0], outs[1][0])
+    assert outs[0][1] == outs[1][1]
