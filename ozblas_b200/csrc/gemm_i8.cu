@@ -68,10 +68,10 @@ struct I8Params {
     // [s][m] and [s][n], and the common scale 2 (rho - 53) of an INT8 slice product
     const short *eas, *ebs;
     int sbias;
-    // MODE 2 (exact FP64 pair products of digit-cut slices): output [pair][n][m];
-    // digit planes per slice level; eas/ebs (or null) add tauA + tauB per element
-    double *pbuf;
-    int D;
+    // MODE 2 (exact FP64 pair products of digit-cut slices) writes the pair
+    // buffer [pair][n][m] through C and reads the digit planes per slice level
+    // from ldc (no new fields: a larger parameter block makes MODE 0 spill more);
+    // eas/ebs (or null) add tauA + tauB per element
     double alpha, beta;
     double *C;
     int *err;
@@ -241,6 +241,17 @@ __global__ void __launch_bounds__(I8_THREADS, 1)
             for (int g = 0; g < p.n_groups; g++) {
                 const int4 grp = p.groups[g];
                 const int meta = grp.w;
+                // MODE 1: the pair's exponents do not depend on the MMAs, so they are
+                // loaded before the wait and arrive while the accumulator fills
+                int era = 0, eb0 = 0, eb1 = 0;
+                if constexpr (MODE == 1) {
+                    const int4 pr = p.items[grp.x];
+                    era = (gr < p.m ? (int)p.eas[(size_t)pr.x * p.m + gr] : 0) + p.sbias;
+                    const short *ebr = p.ebs + (size_t)pr.y * p.n;
+                    const int c0 = tn * I8_BN + half * 64 + lane, c1 = c0 + 32;
+                    eb0 = c0 < p.n ? (int)__ldg(ebr + c0) : 0;
+                    eb1 = c1 < p.n ? (int)__ldg(ebr + c1) : 0;
+                }
                 bool wok = tc::mbar_wait(&acc_full[abuf], aphase, &abort_flag, p.err, ERR_TIMEOUT_EPI, I8_WAIT_NS);
                 if constexpr (MODE == 1) wok = __all_sync(0xffffffffu, wok);  // the lanes agree before any shuffle
                 if (!wok) {
@@ -267,13 +278,13 @@ __global__ void __launch_bounds__(I8_THREADS, 1)
                     if (grp.w & 1) {  // the pair is complete
                         if (gr < p.m) {
                             const int4 it = p.items[grp.x];
-                            const short *ebr = p.ebs ? p.ebs + (size_t)(it.y / p.D) * p.n : nullptr;
-                            const int er = p.sbias + (p.eas ? (int)p.eas[(size_t)(it.x / p.D) * p.m + gr] : 0);
+                            const short *ebr = p.ebs ? p.ebs + (size_t)(it.y / p.ldc) * p.n : nullptr;
+                            const int er = p.sbias + (p.eas ? (int)p.eas[(size_t)(it.x / p.ldc) * p.m + gr] : 0);
 #pragma unroll
                             for (int c = 0; c < 64; c++) {
                                 const int gc = tn * I8_BN + half * 64 + c;
                                 if (gc < p.n)
-                                    p.pbuf[((size_t)grp.z * p.n + gc) * p.m + gr] =
+                                    p.C[((size_t)grp.z * p.n + gc) * p.m + gr] =
                                         scale2(acc[c], er + (ebr ? (int)ebr[gc] : 0));
                             }
                         }
@@ -283,15 +294,8 @@ __global__ void __launch_bounds__(I8_THREADS, 1)
                     continue;
                 }
                 if constexpr (MODE == 1) {
-                    const int4 pr = p.items[grp.x];
-                    const int era = (gr < p.m ? (int)p.eas[(size_t)pr.x * p.m + gr] : 0) + p.sbias;
-                    const short *ebr = p.ebs + (size_t)pr.y * p.n;
-                    // the warp's 64 columns are the same for all its lanes: lane l loads the
+                    // the warp's 64 columns are the same for all its lanes: lane l holds the
                     // exponents of columns gc0 + l and gc0 + 32 + l, shuffles hand them round
-                    const int gc0 = tn * I8_BN + half * 64;
-                    const int c0 = gc0 + lane, c1 = gc0 + 32 + lane;
-                    const int eb0 = c0 < p.n ? (int)__ldg(ebr + c0) : 0;
-                    const int eb1 = c1 < p.n ? (int)__ldg(ebr + c1) : 0;
                     const int ebmin = __reduce_min_sync(0xffffffffu, eb0 < eb1 ? eb0 : eb1);
                     const int ebmax = __reduce_max_sync(0xffffffffu, eb0 > eb1 ? eb0 : eb1);
                     // V * 2^e is exact (normal) for |V| < 2^31 and e in [-1000, 1000]: one multiply
@@ -988,7 +992,7 @@ int i8_exact_pairs(cuozblasHandle_t *h, int m, int n, int k_pad, const int8_t *d
     p.n = n;
     p.m_pad = lpadA;
     p.n_pad = lpadB;
-    p.ldc = m;
+    p.ldc = D;  // MODE 2: digit planes per slice level
     p.tiles_m = lpadA / I8_BM;
     p.tiles_n = lpadB / I8_BN;
     p.strip = p.tiles_m < 12 ? p.tiles_m : 12;
@@ -997,8 +1001,7 @@ int i8_exact_pairs(cuozblasHandle_t *h, int m, int n, int k_pad, const int8_t *d
     p.items = d_sched;
     p.groups = d_sched + items.size();
     p.sbias = sbias;
-    p.pbuf = pbuf;
-    p.D = D;
+    p.C = pbuf;  // MODE 2: the pair buffer
     p.eas = eas;
     p.ebs = ebs;
     p.err = d_err;
