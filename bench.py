@@ -328,6 +328,8 @@ def main():
     if rank == 0 and not args.no_extras:
         line["extras"] = extras(ozb, h, torch, A, B, C, n)
         line["extras"]["int8_vs_plain_speedup"] = line["extras"]["plain_fp64_slices"]["ms"] / ms
+        line["extras"]["int8_vs_plain_int8_digits_speedup"] = (
+            line["extras"]["plain_fp64_slices_int8_digits"]["ms"] / ms)
     if rank == 0 and world == 1 and not args.no_cpu:
         try:
             base, err = cpu_reference_sample(rows_sample=args.ref_rows)
@@ -367,10 +369,20 @@ def extras(ozb, h, torch, A, B, C, n):
     out["int8_full_pairs"] = {"TFLOPS": flops / ms_full / 1e9, "pairs": h.nSplitC, "ms": ms_full}
     C_full = C.clone()
     h.nSplitMax = 0
-    ms_plain = timed(lambda: ozb.dgemm(h, "n", "n", n, n, n, 1.0, A, n, B, n, 0.0, C, n))
+    # the plain form as the north star defines it: FP64 slices on the FP64 tensor pipe (DMMA)
+    os.environ["OZBLAS_PLAIN_DMMA"] = "1"
+    try:
+        ms_plain = timed(lambda: ozb.dgemm(h, "n", "n", n, n, n, 1.0, A, n, B, n, 0.0, C, n))
+    finally:
+        del os.environ["OZBLAS_PLAIN_DMMA"]
     out["plain_fp64_slices"] = {"TFLOPS": flops / ms_plain / 1e9, "pairs": h.nSplitC, "slices": [h.nSplitA, h.nSplitB],
-                                "ms": ms_plain, "internal_fp64_TFLOPS": h.nSplitC * flops / ms_plain / 1e9}
+                                "ms": ms_plain, "internal_fp64_TFLOPS": h.nSplitC * flops / ms_plain / 1e9,
+                                "pipe": "FP64 tensor (DMMA)"}
     C_plain = C.clone()
+    # the library's default plain path: the same exact slice-pair products on INT8 digits (same bits)
+    ms_plain_i8 = timed(lambda: ozb.dgemm(h, "n", "n", n, n, n, 1.0, A, n, B, n, 0.0, C, n))
+    out["plain_fp64_slices_int8_digits"] = {"TFLOPS": flops / ms_plain_i8 / 1e9, "ms": ms_plain_i8,
+                                            "bit_identical_to_dmma": bool(torch.equal(C, C_plain))}
     h.sumMode = 1
     ozb.dgemm(h, "n", "n", n, n, n, 1.0, A, n, B, n, 0.0, C, n)
     torch.cuda.synchronize()
@@ -576,8 +588,8 @@ def mixed_extras(ozb, h, torch, n, reps=3):
 
 
 def memory_extras(ozb, h, torch, reps=3, cg_iters=2000):
-    """DOT n = 2^24 (phi = 2), CSRMV on the 128^3 7-point stencil (both sum modes) and CG on 100^3, through the
-    public API."""
+    """DOT n = 2^24 (phi = 2), GEMV 8192^2 (phi = 1), CSRMV on the 128^3 7-point stencil (both sum modes) and CG
+    on 100^3, through the public API."""
     import numpy as np
 
     out = {}
@@ -608,6 +620,22 @@ def memory_extras(ozb, h, torch, reps=3, cg_iters=2000):
         ms = timed(lambda: ozb.ddot(h, nv, x, y), reps=reps)
         out[f"ddot_2p24_sum{sm}"] = {"GBps": 16.0 * nv / ms / 1e6, "ms": ms, "slices": [h.nSplitA, h.nSplitB]}
     del x, y, r1, r2
+    # GEMV 8192^2 (phi = 1), y = A x, beta = 0: algorithmic bytes 8 (mn + n + m)
+    mg = 8192
+    r1 = torch.rand(mg * mg, dtype=torch.float64, device="cuda", generator=g)
+    r2 = torch.rand(mg * mg, dtype=torch.float64, device="cuda", generator=g)
+    Ag = (r1 - 0.5) * torch.exp(torch.sqrt(-2 * torch.log(r1)) * torch.sin(2 * torch.pi * r2))
+    del r1, r2
+    r1 = torch.rand(mg, dtype=torch.float64, device="cuda", generator=g)
+    xg = (r1 - 0.5) * torch.exp(torch.sqrt(-2 * torch.log(r1)))
+    yg = torch.zeros(mg, dtype=torch.float64, device="cuda")
+    for sm in (0, 1):
+        h.sumMode = sm
+        ms = timed(lambda: ozb.dgemv(h, "n", mg, mg, 1.0, Ag, mg, xg, 0.0, yg), reps=reps)
+        out[f"dgemv_8192_sum{sm}"] = {"GBps": 8.0 * (mg * mg + 2 * mg) / ms / 1e6, "ms": ms,
+                                      "slices": [h.nSplitA, h.nSplitB]}
+    del Ag, xg, yg, r1
+    torch.cuda.empty_cache()
     # CSRMV: 7-point stencil on 128^3, values and x (U - 0.5) exp(N(0,1)), beta = 0
     g3 = 128
     m = g3 ** 3

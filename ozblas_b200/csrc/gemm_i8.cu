@@ -543,6 +543,24 @@ static int make_map(CUtensorMap *map, const int8_t *base, uint64_t rows, uint64_
     return r == CUDA_SUCCESS ? CUOZBLAS_STATUS_SUCCESS : CUOZBLAS_STATUS_CUDA_ERROR;
 }
 
+// Column-major FP64 matrix, rows x cols with leading dimension ld: boxes of
+// box_rows (inner, contiguous) x box_cols, no swizzle, zero fill outside.
+// Needs base 16-byte aligned and ld even (a stride of whole 16-byte units).
+int make_map_f64(CUtensorMap *map, const double *base, uint64_t rows, uint64_t cols, uint64_t ld, uint32_t box_rows,
+                 uint32_t box_cols) {
+    PFN_TensorMapEncodeTiled enc = get_encode();
+    if (!enc || ((uintptr_t)base & 15) != 0 || (ld & 1) != 0 || rows == 0 || cols == 0 || ld < rows)
+        return CUOZBLAS_STATUS_NOT_SUPPORTED;
+    cuuint64_t gdim[2] = {rows, cols};
+    cuuint64_t gstride[1] = {ld * sizeof(double)};
+    cuuint32_t box[2] = {box_rows, box_cols};
+    cuuint32_t estr[2] = {1, 1};
+    CUresult r = enc(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 2, (void *)base, gdim, gstride, box, estr,
+                     CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                     CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    return r == CUDA_SUCCESS ? CUOZBLAS_STATUS_SUCCESS : CUOZBLAS_STATUS_NOT_SUPPORTED;
+}
+
 struct DigitOperand {
     int8_t *digits = nullptr;  // S x lines_pad x k_pad
     int *e = nullptr;          // line exponents

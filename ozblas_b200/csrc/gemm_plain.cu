@@ -381,6 +381,16 @@ __global__ void k_sum_rows(int m, int nA, int nB, int maxlevel, double *__restri
     y[row] = fma(alpha, t, beta * y[row]);
 }
 
+// The ordered sum of a per-row pair buffer (the skinny forms), with the handle's sum mode.
+int sum_rows_launch(cuozblasHandle_t *h, int m, int nA, int nB, int maxlevel, double *P, int64_t ldp, double alpha,
+                    double beta, double *y, double *scratch) {
+    counted(h);
+    k_sum_rows<<<(m + 127) / 128, 128, 0, state(h)->stream>>>(m, nA, nB, maxlevel, P, ldp, h->sumMode, alpha, beta, y,
+                                                               scratch);
+    OZB_CHECK(cudaGetLastError());
+    return CUOZBLAS_STATUS_SUCCESS;
+}
+
 // ---------------------------------------------------------------------------
 // Host drivers
 // ---------------------------------------------------------------------------
@@ -438,6 +448,38 @@ int gemm_plain_core(cuozblasHandle_t *h, char ta, char tb, int m, int n, int k, 
     // ---- split ----  (phase events 0..4: start, A split, B split, products, sum)
     ev_record(h, 0);
     st->plain_timers = true;
+    // GEMV 'n' (rows of A strided): fused split and products, A read nA + 2 times
+    if (skinny_n && !dot && !is_trans(ta) && !getenv("OZBLAS_GEMV_SPLIT")) {
+        const uint64_t mk0 = ar.mark();
+        double *xs = ar.take<double>((uint64_t)maxS * ldk);
+        if (!ar.ok) return CUOZBLAS_STATUS_WORKSPACE;
+        int nBv = 0, nAv = 0;
+        OZB_TRY(split_vector(h, k, B, rho, maxS, xs, ldk, &nBv));
+        ev_record(h, 1);
+        const int fr = gemv_fused_n(h, m, k, A, lda, xs, ldk, nBv, rho, maxS, fastMode, alpha, beta, C, &nAv);
+        if (fr == CUOZBLAS_STATUS_SUCCESS) {
+            int ml = (nAv - 1) + (nBv - 1);
+            const int mn = nAv - 1 < nBv - 1 ? nAv - 1 : nBv - 1;
+            ml = (ml - fastMode) > mn ? (ml - fastMode) : mn;
+            h->nSplitA = (float)nAv;
+            h->nSplitB = (float)nBv;
+            h->nSplitC = fastMode == 0 ? (float)(ml + 1 < nAv ? ml + 1 : nAv) : 0.f;
+            if (fastMode != 0) {
+                int np = 0;
+                for_each_pair(nAv, nBv, ml, [&](int, int) { np++; });
+                h->nSplitC = (float)np;
+            }
+            h->mbk = m;
+            h->nbk = n;
+            ev_record(h, 2);
+            ev_record(h, 3);
+            ev_record(h, 4);
+            return CUOZBLAS_STATUS_SUCCESS;
+        }
+        if (fr != CUOZBLAS_STATUS_NOT_SUPPORTED) return fr;
+        ar.release(mk0);  // more levels than the fused kernel holds: the materialised path
+        ev_record(h, 0);
+    }
     double *Sa = nullptr, *Sb = nullptr;
     short *Ea = nullptr, *Eb = nullptr;  // taus per line and level (general GEMM: the INT8 product path)
     int nA = 0, nB = 0;

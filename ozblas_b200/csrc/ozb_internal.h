@@ -179,6 +179,12 @@ int i8_exact_pairs(cuozblasHandle_t *h, int m, int n, int k_pad, const int8_t *d
 int gemm_q_core(cuozblasHandle_t *h, char ta, char tb, int m, int n, int k, const void *alpha, const void *A, int lda,
                 const void *B, int ldb, const void *beta, void *C, int ldc, int fastMode);
 
+// ---- skinny forms (gemm_plain.cu, gemv_fused.cu) ----
+int sum_rows_launch(cuozblasHandle_t *h, int m, int nA, int nB, int maxlevel, double *P, int64_t ldp, double alpha,
+                    double beta, double *y, double *scratch);
+int gemv_fused_n(cuozblasHandle_t *h, int m, int n, const double *A, int lda, const double *xs, int ldx, int nB,
+                 int rho, int maxS, int fastMode, double alpha, double beta, double *y, int *nA_out);
+
 // ---- plain GEMM core (gemm_plain.cu) ----
 int gemm_plain_core(cuozblasHandle_t *h, char ta, char tb, int m, int n, int k, double alpha, const double *A,
                     int lda, const double *B, int ldb, double beta, double *C, int ldc, int fastMode);

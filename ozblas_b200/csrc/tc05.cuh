@@ -5,6 +5,13 @@
 #include <stdint.h>
 
 namespace ozb {
+
+// Host: tensor map of a column-major FP64 matrix (gemm_i8.cu); returns
+// CUOZBLAS_STATUS_NOT_SUPPORTED when the base or leading dimension does not
+// suit TMA.
+int make_map_f64(CUtensorMap *map, const double *base, uint64_t rows, uint64_t cols, uint64_t ld, uint32_t box_rows,
+                 uint32_t box_cols);
+
 namespace tc {
 
 __device__ __forceinline__ uint32_t smem_u32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }

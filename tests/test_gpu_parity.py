@@ -531,3 +531,64 @@ def test_dgemm_tensor_core_pairs_equal_dmma(sm, m, n, k, ta, tb, scale, oracle, 
         outs.append((host(dC), handle.nSplitC))
     assert bits_equal(outs[0][0], outs[1][0]), first_diff(outs[0][0], outs[1][0])
     assert outs[0][1] == outs[1][1]
+
+
+@pytest.mark.parametrize("sm", [0, 1])
+@pytest.mark.parametrize("m,n,fm,phi,scale", [(1000, 3000, 0, 1.0, 1.0), (777, 513, 1, 2.0, 2.0 ** -1000),
+                                               (64, 9000, 0, 4.0, 2.0 ** 900), (33, 1, 0, 1.0, 1.0),
+                                               (300, 700, 0, 0.0, 1.0), (96, 200, 0, -1.0, 1.0)])
+def test_dgemv_fused_equals_materialised(sm, m, n, fm, phi, scale, oracle, handle, ozb, cuda, monkeypatch):
+    """GEMV 'n' with the split and the slice products fused gives the bits of the path that writes
+    every slice, in both sum modes: the two-read path on predicted tau chains, the path with one read
+    of A per level, and the materialised one.  phi = 0 builds rows 1 + 2^-45 s (s = +-1), whose
+    remainders after the first level fall far below the predicted chain, so the two-read path has
+    to detect the wrong prediction and take the level passes."""
+    if phi == 0.0:
+        rng = np.random.default_rng(5)
+        A = 1.0 + 2.0 ** -45 * rng.choice([-1.0, 1.0], size=(m, n))
+        x = oracle.phi_vector(n, 1.0, 2)
+    elif phi < 0.0:  # a zero row and an infinite x entry: 0 * Inf makes NaN on every path
+        A = oracle.phi_matrix(m, n, 1.0, 1)
+        A[:, 7] = 0.0  # row 7 of the column-major m x n matrix (array rows are columns)
+        x = oracle.phi_vector(n, 1.0, 2)
+        x[n // 2] = np.inf
+    else:
+        A = oracle.phi_matrix(m, n, phi, 1) * scale
+        x = oracle.phi_vector(n, phi, 2)
+    y0 = oracle.phi_vector(m, 1.0, 3)
+    handle.sumMode, handle.fastMode = sm, fm
+    outs = []
+    for env in (None, "OZBLAS_GEMV_LEVELS", "OZBLAS_GEMV_SPLIT"):
+        if env:
+            monkeypatch.setenv(env, "1")
+        dy = dev(cuda, y0)
+        ozb.dgemv(handle, "n", m, n, 0.75, dev(cuda, A), m, dev(cuda, x), 0.5, dy)
+        outs.append((host(dy), (handle.nSplitA, handle.nSplitB, handle.nSplitC)))
+    for o in outs[1:]:
+        if phi < 0.0:  # IEEE leaves the sign of a NaN open
+            assert np.array_equal(np.isnan(outs[0][0]), np.isnan(o[0])) and np.isnan(o[0][7])
+            assert bits_equal(np.nan_to_num(outs[0][0]), np.nan_to_num(o[0]))
+        else:
+            assert bits_equal(outs[0][0], o[0]), first_diff(outs[0][0], o[0])
+        assert outs[0][1] == o[1]
+    if phi < 0.0:
+        return
+    if m * n <= 4_000_000:
+        ref, info = oracle.dgemv(make_flags(sumMode=sm, fastMode=fm), "n", m, n, 0.75, A, m, x, 0.5, y0)
+        assert bits_equal(outs[0][0], ref), first_diff(outs[0][0], ref)
+
+
+@pytest.mark.parametrize("nsplit", [2, 3])
+@pytest.mark.parametrize("m,n", [(200, 300), (64, 4096)])
+def test_dgemv_truncated_split(nsplit, m, n, oracle, handle, ozb, cuda):
+    """GEMV 'n' with the slice count capped below what the split needs (nSplitMax): the fused paths
+    keep the first levels of each row's chain, as the reference's split does."""
+    A = oracle.phi_matrix(m, n, 2.0, 1)
+    x = oracle.phi_vector(n, 2.0, 2)
+    y0 = oracle.phi_vector(m, 1.0, 3)
+    ref, info = oracle.dgemv(make_flags(nSplitMax=nsplit), "n", m, n, 1.0, A, m, x, 0.25, y0)
+    handle.nSplitMax = nsplit
+    dy = dev(cuda, y0)
+    ozb.dgemv(handle, "n", m, n, 1.0, dev(cuda, A), m, dev(cuda, x), 0.25, dy)
+    assert bits_equal(host(dy), ref), first_diff(host(dy), ref)
+    assert (handle.nSplitA, handle.nSplitB) == (info.nSplitA, info.nSplitB)
