@@ -227,11 +227,14 @@ __global__ void __launch_bounds__(256) k_gemv_tma(const __grid_constant__ CUtens
 #pragma unroll
                         for (int b = 0; b < NB; b++) {
                             xv[b] = xs[(size_t)b * ldx + jb + c];
-                            xfin = xfin && fabs(xv[b]) <= 1.7976931348623157e308;
+                            // exponent field below all-ones (integer test, off the FP64 pipe)
+                            xfin = xfin && (__double2hiint(xv[b]) & 0x7ff00000) != 0x7ff00000;
                         }
 #pragma unroll
                         for (int l = 0; l < (PRED ? kGvMaxLevels : 1); l++) {
-                            if (r != 0.0 || !xfin) {  // a zero remainder cuts zero slices from here on
+                            // a zero remainder cuts zero slices from here on (r = +-0: every bit
+                            // but the sign clear)
+                            if ((__double_as_longlong(r) << 1) != 0 || !xfin) {
                                 const double sl = (r + sig[l]) - sig[l];
                                 r = r - sl;
                                 mxl[l] = ref_max(mxl[l], fabs(r));  // max |r_{l+1}|
