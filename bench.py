@@ -371,10 +371,12 @@ def extras(ozb, h, torch, A, B, C, n):
     h.nSplitMax = 0
     # the plain form as the north star defines it: FP64 slices on the FP64 tensor pipe (DMMA)
     os.environ["OZBLAS_PLAIN_DMMA"] = "1"
+    h.read_env()
     try:
         ms_plain = timed(lambda: ozb.dgemm(h, "n", "n", n, n, n, 1.0, A, n, B, n, 0.0, C, n))
     finally:
         del os.environ["OZBLAS_PLAIN_DMMA"]
+        h.read_env()
     out["plain_fp64_slices"] = {"TFLOPS": flops / ms_plain / 1e9, "pairs": h.nSplitC, "slices": [h.nSplitA, h.nSplitB],
                                 "ms": ms_plain, "internal_fp64_TFLOPS": h.nSplitC * flops / ms_plain / 1e9,
                                 "pipe": "FP64 tensor (DMMA)"}

@@ -52,7 +52,7 @@ typedef struct {
     int32_t reproMode;      /* must be 1 (reproducible); 0 with nSplitMax 1 = plain FP64 */
     int32_t sumMode;        /* 0: ordered FP64 sum; 1: NearSum (correctly rounded) */
     int32_t useBatchedGemmFlag;
-    int32_t splitEpsMode;   /* 0 or 9 */
+    int32_t splitEpsMode;   /* 0, 9, or 2 (Dot2: DOT, NRM2, CSRMV and CG with fastMode 0) */
     int32_t precxFlag;
 
     /* exec info */
@@ -94,7 +94,7 @@ typedef enum {
     CUOZBLAS_STATUS_NOT_INITIALIZED = 1,
     CUOZBLAS_STATUS_INVALID_VALUE = 2,  /* inc != 1, transposed CSRMV, bad sizes or flags */
     CUOZBLAS_STATUS_WORKSPACE = 3,      /* the arena given at create is too small */
-    CUOZBLAS_STATUS_NOT_SUPPORTED = 4,  /* e.g. splitEpsMode 2 (Dot2) */
+    CUOZBLAS_STATUS_NOT_SUPPORTED = 4,  /* e.g. Dot2 for GEMM/GEMV, NearSum in the mixed and quad forms */
     CUOZBLAS_STATUS_INT32_BOUND = 5,    /* INT8 form: k beyond the exact INT32 bound */
     CUOZBLAS_STATUS_DEVICE_TIMEOUT = 6, /* a bounded device-side wait gave up */
     CUOZBLAS_STATUS_CUDA_ERROR = 7
@@ -153,6 +153,11 @@ int cuozblasHandleDestroy(cuozblasHandle_t *h);
 int cuozblasSetStream(cuozblasHandle_t *h, void *stream);
 /* Extension: number of kernels the handle has launched since create. */
 int cuozblasGetLaunchCount(cuozblasHandle_t *h, uint64_t *count);
+/* Re-read the OZBLAS_* diagnostic switches from the environment into the
+ * handle (they are read once when the handle is created; each selects an
+ * equal-bits alternative path or a stderr trace).  No reference counterpart. */
+int cuozblasHandleReadEnv(cuozblasHandle_t *h);
+
 
 /* cuozblasRdot<double,double,double> (include/cuozblas.h:75; src/cuda/cuozblas_dot.cu:3-40).
  * *ret is a host pointer, written before return. */
@@ -253,9 +258,9 @@ int cuozblasDgemmI8Batched(cuozblasHandle_t *h, char transa, char transb, int32_
                            double *const *C, const int32_t *ldc);
 
 /* Allocation-free INT8 precision-form DGEMM.  No counterpart in the
- * reference.  For callers that cannot allocate device memory (work recorded
- * while a CUDA graph is being captured, hosts whose device memory is
- * budgeted up front or owned by another allocator): same arithmetic and
+ * reference.  For callers that cannot allocate device memory (real-time or
+ * embedded hosts whose device memory is budgeted once at start-up, hosts
+ * whose own allocator already owns the whole device): same arithmetic and
  * results as cuozblasDgemmI8, with the flags passed directly and no handle;
  * the scratch is a 64 MiB file-scope device array inside the library
  * (resident on every GPU that loads it), so the call makes no cudaMalloc,

@@ -81,6 +81,7 @@ _create = _sig("cuozblasHandleCreate", [_HP, C.c_uint64])
 _destroy = _sig("cuozblasHandleDestroy", [_HP])
 _setstream = _sig("cuozblasSetStream", [_HP, _vp])
 _launches = _sig("cuozblasGetLaunchCount", [_HP, C.POINTER(C.c_uint64)])
+_readenv = _sig("cuozblasHandleReadEnv", [_HP])
 _ddot = _sig("cuozblasDdot", [_HP, _i32, _vp, _i32, _vp, _i32, C.POINTER(_d)])
 _dnrm2 = _sig("cuozblasDnrm2", [_HP, _i32, _vp, _i32, C.POINTER(_d)])
 _daxpy = _sig("cuozblasDaxpy", [_HP, _i32, _d, _vp, _i32, _vp, _i32])
@@ -116,7 +117,8 @@ _version = _sig("cuozblasVersion", [], C.c_char_p)
 
 #: every C-ABI symbol include/cuozblas.h declares (checked by the CPU tests)
 C_ABI_SYMBOLS = [
-    "cuozblasHandleCreate", "cuozblasHandleDestroy", "cuozblasSetStream", "cuozblasGetLaunchCount", "cuozblasDdot", "cuozblasDnrm2",
+    "cuozblasHandleCreate", "cuozblasHandleDestroy", "cuozblasSetStream", "cuozblasGetLaunchCount",
+    "cuozblasHandleReadEnv", "cuozblasDdot", "cuozblasDnrm2",
     "cuozblasDaxpy", "cuozblasDgemv", "cuozblasDgemm", "cuozblasDcsrmv", "cuozblasDcsrmvSplitA", "cuozblasDcg",
     "cuozblasDgemmI8", "cuozblasDgemmI8Static", "cuozblasDgemmI8Batched", "cuozblasRuleTau", "cuozblasRuleRho",
     "cuozblasRuleCrSum", "cuozblasDSgemm", "cuozblasDSgemv", "cuozblasDSdot", "cuozblasDSnrm2",
@@ -165,6 +167,10 @@ class Handle:
         c = C.c_uint64()
         _chk("cuozblasGetLaunchCount", _launches(C.byref(self._h), C.byref(c)))
         return c.value
+
+    def read_env(self):
+        """Re-read the OZBLAS_* diagnostic switches (read once at creation) into the handle."""
+        _chk("cuozblasHandleReadEnv", _readenv(C.byref(self._h)))
 
     @property
     def ref(self):

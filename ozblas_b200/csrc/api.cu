@@ -16,6 +16,8 @@
 namespace ozb {
 int launch_axpy(cuozblasHandle_t *h, int n, double alpha, const double *x, double *y);
 int launch_scal(cuozblasHandle_t *h, int n, double alpha, double *x);
+constexpr int kNrm2PlainScratch = 257;  // 256 block partials + the result
+int launch_nrm2_plain(cuozblasHandle_t *h, int n, const double *x, double *scratch);
 int launch_csrmv_plain(cuozblasHandle_t *h, int m, const double *val, const int *colind, const int *rowptr,
                        const double *x, double alpha, double beta, double *y);
 int csrmv_presplit(cuozblasHandle_t *h, int m, int n, double alpha, const double *As, int nA, int64_t ld_s,
@@ -48,6 +50,24 @@ static double wall() {
     struct timeval tv;
     gettimeofday(&tv, nullptr);
     return tv.tv_sec + tv.tv_usec * 1e-6;
+}
+
+static bool env_on(const char *name) {
+    const char *v = getenv(name);
+    return v != nullptr && *v != '\0' && strcmp(v, "0") != 0;
+}
+
+void EnvSwitches::read() {
+    gemv_split = env_on("OZBLAS_GEMV_SPLIT");
+    gemv_levels = env_on("OZBLAS_GEMV_LEVELS");
+    plain_dmma = env_on("OZBLAS_PLAIN_DMMA");
+    sd_dmma = env_on("OZBLAS_SD_DMMA");
+    q_dmma = env_on("OZBLAS_Q_DMMA");
+    ds_simt = env_on("OZBLAS_DS_SIMT");
+    dot_tree = env_on("OZBLAS_DOT_TREE");
+    cg_no_graph = env_on("OZBLAS_CG_NO_GRAPH");
+    dot_trace = env_on("OZBLAS_DOT_TRACE");
+    cg_trace = env_on("OZBLAS_CG_TRACE");
 }
 
 int counter_init(cuozblasHandle_t *h) {
@@ -101,17 +121,59 @@ static int dot_impl(cuozblasHandle_t *h, int n, const double *x, const double *y
         h->nSplitA = (float)nA;
         h->nSplitB = (float)nB;
         h->nSplitC = 1.f;
-        if (getenv("OZBLAS_DOT_TRACE")) fprintf(stderr, "cuozblas: dot fused nA=%d nB=%d\n", nA, nB);
+        if (state(h)->env.dot_trace) fprintf(stderr, "cuozblas: dot fused nA=%d nB=%d\n", nA, nB);
         return CUOZBLAS_STATUS_SUCCESS;
     }
     double *d = reinterpret_cast<double *>(h->devWorkCommon);
     OZB_CHECK(cudaMemsetAsync(d, 0, sizeof(double), st->stream));
     OZB_TRY(gemm_plain_core(h, 't', 'n', 1, 1, n, 1.0, x, n, y, n, 0.0, d, 1, 0));
-    if (getenv("OZBLAS_DOT_TRACE"))
+    if (state(h)->env.dot_trace)
         fprintf(stderr, "cuozblas: dot general nA=%d nB=%d\n", (int)h->nSplitA, (int)h->nSplitB);
     OZB_CHECK(cudaMemcpyAsync(st->h_dbl, d, sizeof(double), cudaMemcpyDeviceToHost, st->stream));
     OZB_CHECK(cudaStreamSynchronize(st->stream));
     *ret = st->h_dbl[0];
+    return CUOZBLAS_STATUS_SUCCESS;
+}
+
+// The engines take a one-row op(A) of a 1 x 1 product and the one-column
+// op(B) of an n = 1 product as contiguous vectors.  Stored with a leading
+// dimension above 1 (A 'n' with lda > 1, B 't' with ldb > 1) their elements
+// are strided: gather them into the arena and pass the contiguous form
+// (A as 't' with lda = k, B as 'n' with ldb = k).  The gathered copies stay
+// below the engine's own arena use for the whole call.
+static int contiguous_vectors(cuozblasHandle_t *h, int esz, int m, int n, int k, char &ta, const void *&A, int &lda,
+                              char &tb, const void *&B, int &ldb) {
+    if (k <= 0) return CUOZBLAS_STATUS_SUCCESS;
+    if (n == 1 && is_trans(tb) && ldb != 1) {
+        if (ldb < 1) return CUOZBLAS_STATUS_INVALID_VALUE;
+        Arena ar(h);
+        char *g = ar.take<char>((uint64_t)k * esz);
+        if (!ar.ok) return CUOZBLAS_STATUS_WORKSPACE;
+        OZB_TRY(gather_strided(h, k, B, ldb, esz, g));
+        B = g;
+        tb = 'n';
+        ldb = k;
+    }
+    if (m == 1 && n == 1 && !is_trans(ta) && lda != 1) {
+        if (lda < 1) return CUOZBLAS_STATUS_INVALID_VALUE;
+        Arena ar(h);
+        char *g = ar.take<char>((uint64_t)k * esz);
+        if (!ar.ok) return CUOZBLAS_STATUS_WORKSPACE;
+        OZB_TRY(gather_strided(h, k, A, lda, esz, g));
+        A = g;
+        ta = 't';
+        lda = k;
+    }
+    return CUOZBLAS_STATUS_SUCCESS;
+}
+
+template <typename T>
+static int contiguous_vectors_t(cuozblasHandle_t *h, int m, int n, int k, char &ta, const T *&A, int &lda, char &tb,
+                                const T *&B, int &ldb) {
+    const void *a = A, *b = B;
+    OZB_TRY(contiguous_vectors(h, (int)sizeof(T), m, n, k, ta, a, lda, tb, b, ldb));
+    A = static_cast<const T *>(a);
+    B = static_cast<const T *>(b);
     return CUOZBLAS_STATUS_SUCCESS;
 }
 
@@ -214,9 +276,16 @@ int cuozblasHandleCreate(cuozblasHandle_t *h, uint64_t workSizeBytes) {
         memset(h, 0, sizeof(*h));
         return CUOZBLAS_STATUS_CUDA_ERROR;
     }
+    st->env.read();
     h->hstBatchAddr = reinterpret_cast<char *>(st);
     h->devBatchAddr = nullptr;
     h->initialized = 1;
+    return CUOZBLAS_STATUS_SUCCESS;
+}
+
+int cuozblasHandleReadEnv(cuozblasHandle_t *h) {
+    if (!h || !h->initialized) return CUOZBLAS_STATUS_NOT_INITIALIZED;
+    state(h)->env.read();
     return CUOZBLAS_STATUS_SUCCESS;
 }
 
@@ -258,6 +327,7 @@ int cuozblasDgemm(cuozblasHandle_t *h, char transa, char transb, int32_t m, int3
     if (h->reproMode == 0 && h->nSplitMax == 1) return CUOZBLAS_STATUS_NOT_SUPPORTED;
     if (m == 0 || n == 0) return CUOZBLAS_STATUS_SUCCESS;
     const double t0 = wall();
+    OZB_TRY(contiguous_vectors_t(h, m, n, k, transa, A, lda, transb, B, ldb));
     OZB_TRY(gemm_plain_core(h, transa, transb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, h->fastMode));
     return finish(h, t0);
 }
@@ -324,6 +394,7 @@ int cuozblasDSgemm(cuozblasHandle_t *h, char transa, char transb, int32_t m, int
     if (h->reproMode == 0 && h->nSplitMax == 1) return CUOZBLAS_STATUS_NOT_SUPPORTED;
     if (m == 0 || n == 0) return CUOZBLAS_STATUS_SUCCESS;
     const double t0 = wall();
+    OZB_TRY(contiguous_vectors_t(h, m, n, k, transa, A, lda, transb, B, ldb));
     OZB_TRY(gemm_f32_core(h, transa, transb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, h->fastMode));
     return finish(h, t0);
 }
@@ -392,6 +463,7 @@ int cuozblasSDgemm(cuozblasHandle_t *h, char transa, char transb, int32_t m, int
     if (h->reproMode == 0 && h->nSplitMax == 1) return CUOZBLAS_STATUS_NOT_SUPPORTED;
     if (m == 0 || n == 0) return CUOZBLAS_STATUS_SUCCESS;
     const double t0 = wall();
+    OZB_TRY(contiguous_vectors_t(h, m, n, k, transa, A, lda, transb, B, ldb));
     OZB_TRY(gemm_sd_core(h, transa, transb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, h->fastMode));
     return finish(h, t0);
 }
@@ -458,6 +530,7 @@ int cuozblasQgemm(cuozblasHandle_t *h, char transa, char transb, int32_t m, int3
     if (h->reproMode == 0 && h->nSplitMax == 1) return CUOZBLAS_STATUS_NOT_SUPPORTED;
     if (m == 0 || n == 0) return CUOZBLAS_STATUS_SUCCESS;
     const double t0 = wall();
+    OZB_TRY(contiguous_vectors(h, 16, m, n, k, transa, A, lda, transb, B, ldb));
     OZB_TRY(gemm_q_core(h, transa, transb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, h->fastMode));
     return finish(h, t0);
 }
@@ -629,6 +702,7 @@ int cuozblasDcg(cuozblasHandle_t *h, char trans, int32_t n, int32_t nnz, const v
     Arena ar(h);
     const uint64_t nn = (uint64_t)(n > 0 ? n : 1);
     double *r = ar.take<double>(nn), *p = ar.take<double>(nn), *q = ar.take<double>(nn), *tv = ar.take<double>(nn);
+    double *nrm_scr = ar.take<double>(kNrm2PlainScratch);
     if (!ar.ok) return CUOZBLAS_STATUS_WORKSPACE;
     const uint64_t keep = h->memMaskSplitA;
     h->memMaskSplitA = st->off;
@@ -651,27 +725,25 @@ int cuozblasDcg(cuozblasHandle_t *h, char trans, int32_t n, int32_t nnz, const v
             int fa = 0, fb = 0;
             OZB_TRY(csrmv_fused(h, n, n, al, val, colind, rowptr, xv, be, yv, cg_shift, h->nSplitA_, &done, &fa,
                                       &fb));
-            if (getenv("OZBLAS_DOT_TRACE") && done) fprintf(stderr, "cuozblas: spmv fused nB=%d\n", fb);
+            if (state(h)->env.dot_trace && done) fprintf(stderr, "cuozblas: spmv fused nB=%d\n", fb);
             if (done) return CUOZBLAS_STATUS_SUCCESS;
         }
         const int rs = cuozblasDcsrmv(h, trans, n, n, nnz, al, descrA, As, colind, rowptr, xv, be, yv);
-        if (getenv("OZBLAS_DOT_TRACE")) fprintf(stderr, "cuozblas: spmv general nB=%d\n", (int)h->nSplitB);
+        if (state(h)->env.dot_trace) fprintf(stderr, "cuozblas: spmv general nB=%d\n", (int)h->nSplitB);
         return rs;
     };
     if ((status = spmv(-1., x, 1., r))) return fail(status);
     if ((status = cuozblasDdot(h, n, r, 1, r, 1, &dold))) return fail(status);
     double resi = sqrt(dold);
     auto true_res = [&]() -> double {
-        // t = b - A x in plain FP64, then a plain FP64 norm (diagnostic only)
+        // t = b - A x in plain FP64, then a plain FP64 norm on the device (diagnostic only,
+        // src/cuda/cuozblas_cg.cu:3-24: a cuSPARSE csrmv and a cuBLAS nrm2 there)
         cudaMemcpyAsync(tv, b, sizeof(double) * n, cudaMemcpyDeviceToDevice, st->stream);
         launch_csrmv_plain(h, n, val, colind, rowptr, x, -1., 1., tv);
-        double *hv = new double[nn];
-        cudaMemcpyAsync(hv, tv, sizeof(double) * n, cudaMemcpyDeviceToHost, st->stream);
+        launch_nrm2_plain(h, n, tv, nrm_scr);
+        cudaMemcpyAsync(st->h_dbl, nrm_scr, sizeof(double), cudaMemcpyDeviceToHost, st->stream);
         cudaStreamSynchronize(st->stream);
-        double s2 = 0.0;
-        for (int i = 0; i < n; i++) s2 += hv[i] * hv[i];
-        delete[] hv;
-        return sqrt(s2);
+        return st->h_dbl[0];
     };
     if (h->verbose > 0) {
         const double t2 = wall();
@@ -717,7 +789,7 @@ int cuozblasDcg(cuozblasHandle_t *h, char trans, int32_t n, int32_t nnz, const v
     // The fused steps run as captured graphs when both fused paths apply
     // (plain split, full pair set) and the history needs no host work.
     const bool graphs = h->fastMode == 0 && h->splitEpsMode == 0 && n > 0 &&
-                        !(h->verbose > 0 && h->trueresFlag) && getenv("OZBLAS_CG_NO_GRAPH") == nullptr;
+                        !(h->verbose > 0 && h->trueresFlag) && !state(h)->env.cg_no_graph;
     if (graphs) {
         if ((status = cg_graph(h, n, val, colind, rowptr, x, r, p, q, nrmb, tol, maxiter, cg_shift, h->nSplitA_, dold,
                                it, stop, t1, res_all.data(), when_all.data(), host_head, host_tail, wall)))

@@ -217,10 +217,10 @@ int cg_graph(cuozblasHandle_t *h, int n, const double *val, const int *colind, c
     for (int k = 0; k < K && !cap; k++) {
         cap = csr_proof_launch(s, n, p, rho, maxS, cs, &d->gate);
         if (!cap) cap = csr_rows_launch(s, spmv, cs, slow, nslow, &dpq->vs, 1, terms, &d->gate);
-        if (!cap) cap = dot_tree_launch(s, nsm, n, p, q, rho, maxS, h->sumMode, dpq, &d->gate);
+        if (!cap) cap = dot_tree_launch(s, nsm, n, p, q, rho, maxS, h->sumMode, dpq, &d->gate, state(h)->env.dot_tree);
         k_cg_alpha<<<1, 1, 0, s>>>(d, dpq, cs);
         k_cg_update_xr<<<ub, 256, 0, s>>>(n, x, r, p, q, d, &drr->vs);
-        if (!cap) cap = dot_tree_launch(s, nsm, n, r, r, rho, maxS, h->sumMode, drr, &d->gate);
+        if (!cap) cap = dot_tree_launch(s, nsm, n, r, r, rho, maxS, h->sumMode, drr, &d->gate, state(h)->env.dot_tree);
         k_cg_beta<<<1, 1, 0, s>>>(d, drr, res_dev, stamp_dev);
         k_cg_update_p<<<ub, 256, 0, s>>>(n, p, r, d, &cs->vs, &dpq->vs);
     }
@@ -267,7 +267,7 @@ int cg_graph(cuozblasHandle_t *h, int n, const double *val, const int *colind, c
         // a step was not proven: the host path finishes this iteration
         iter = hd.iter;
         dold = hd.dold;
-        if (getenv("OZBLAS_CG_TRACE"))
+        if (state(h)->env.cg_trace)
             fprintf(stderr, "cuozblas: CG iteration %d finished on the host (step %d)\n", iter + 1, hd.broken);
         if (hd.broken != 3 && (status = host_head())) {
             cleanup();
@@ -284,7 +284,7 @@ int cg_graph(cuozblasHandle_t *h, int n, const double *val, const int *colind, c
             return status;
         }
     }
-    if (getenv("OZBLAS_CG_TRACE"))
+    if (state(h)->env.cg_trace)
         fprintf(stderr, "cuozblas: CG %d iterations in %d graph batches of %d, %d finished on the host path\n",
                 iter, batches, K, reruns);
     cleanup();

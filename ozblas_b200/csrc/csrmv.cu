@@ -102,10 +102,82 @@ __global__ void k_scal(int n, double alpha, double *__restrict__ x) {
     for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < (size_t)n; i += stride) x[i] = alpha * x[i];
 }
 
+// Gather n elements of `esz` bytes spaced `stride` elements apart into a
+// contiguous array (a one-row op(A) or one-column op(B) stored with a leading
+// dimension above 1, e.g. B^T of a 1 x k B with ldb > 1).
+template <typename E>
+__global__ void k_gather_strided(int n, const E *__restrict__ src, int64_t stride, E *__restrict__ dst) {
+    const size_t step = (size_t)gridDim.x * blockDim.x;
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < (size_t)n; i += step) dst[i] = src[i * stride];
+}
+
+struct Bytes16 {
+    uint64_t lo, hi;
+};
+
+int gather_strided(cuozblasHandle_t *h, int n, const void *src, int64_t stride, int esz, void *dst) {
+    if (n <= 0) return CUOZBLAS_STATUS_SUCCESS;
+    int blocks = (n + 255) / 256;
+    if (blocks > sm_count() * 8) blocks = sm_count() * 8;
+    cudaStream_t s = state(h)->stream;
+    counted(h);
+    if (esz == 4)
+        k_gather_strided<float><<<blocks, 256, 0, s>>>(n, (const float *)src, stride, (float *)dst);
+    else if (esz == 8)
+        k_gather_strided<double><<<blocks, 256, 0, s>>>(n, (const double *)src, stride, (double *)dst);
+    else if (esz == 16)
+        k_gather_strided<Bytes16><<<blocks, 256, 0, s>>>(n, (const Bytes16 *)src, stride, (Bytes16 *)dst);
+    else
+        return CUOZBLAS_STATUS_INVALID_VALUE;
+    OZB_CHECK(cudaGetLastError());
+    return CUOZBLAS_STATUS_SUCCESS;
+}
+
+// Plain FP64 2-norm in a fixed order (the true residual of CG's diagnostics):
+// 256 blocks of strided sums of squares, then one block adds the partials in
+// order and writes sqrt to scratch[0] (partials at scratch[1..256]).
+__global__ void __launch_bounds__(256) k_sumsq_partials(int n, const double *__restrict__ x,
+                                                        double *__restrict__ part) {
+    __shared__ double red[256];
+    double s = 0.0;
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < (size_t)n; i += (size_t)gridDim.x * blockDim.x)
+        s = fma(x[i], x[i], s);
+    red[threadIdx.x] = s;
+    __syncthreads();
+    for (int o = 128; o > 0; o >>= 1) {
+        if ((int)threadIdx.x < o) red[threadIdx.x] += red[threadIdx.x + o];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) part[blockIdx.x] = red[0];
+}
+
+__global__ void __launch_bounds__(256) k_sumsq_final(int nparts, const double *__restrict__ part,
+                                                     double *__restrict__ out) {
+    __shared__ double red[256];
+    red[threadIdx.x] = (int)threadIdx.x < nparts ? part[threadIdx.x] : 0.0;
+    __syncthreads();
+    for (int o = 128; o > 0; o >>= 1) {
+        if ((int)threadIdx.x < o) red[threadIdx.x] += red[threadIdx.x + o];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) out[0] = sqrt(red[0]);
+}
+
+int launch_nrm2_plain(cuozblasHandle_t *h, int n, const double *x, double *scratch) {
+    constexpr int kParts = 256;
+    cudaStream_t s = state(h)->stream;
+    counted(h);
+    k_sumsq_partials<<<kParts, 256, 0, s>>>(n > 0 ? n : 0, x, scratch + 1);
+    counted(h);
+    k_sumsq_final<<<1, 256, 0, s>>>(kParts, scratch + 1, scratch);
+    OZB_CHECK(cudaGetLastError());
+    return CUOZBLAS_STATUS_SUCCESS;
+}
+
 int launch_axpy(cuozblasHandle_t *h, int n, double alpha, const double *x, double *y) {
     if (n <= 0) return CUOZBLAS_STATUS_SUCCESS;
     int blocks = (n + 255) / 256;
-    if (blocks > 148 * 16) blocks = 148 * 16;
+    if (blocks > sm_count() * 16) blocks = sm_count() * 16;
     counted(h);
     k_axpy<<<blocks, 256, 0, state(h)->stream>>>(n, alpha, x, y);
     OZB_CHECK(cudaGetLastError());
@@ -115,7 +187,7 @@ int launch_axpy(cuozblasHandle_t *h, int n, double alpha, const double *x, doubl
 int launch_scal(cuozblasHandle_t *h, int n, double alpha, double *x) {
     if (n <= 0) return CUOZBLAS_STATUS_SUCCESS;
     int blocks = (n + 255) / 256;
-    if (blocks > 148 * 16) blocks = 148 * 16;
+    if (blocks > sm_count() * 16) blocks = sm_count() * 16;
     counted(h);
     k_scal<<<blocks, 256, 0, state(h)->stream>>>(n, alpha, x);
     OZB_CHECK(cudaGetLastError());

@@ -297,13 +297,9 @@ static int launch_tree(bool aligned, int grid, cudaStream_t s, int n, const doub
                        int maxS, int sum_mode, DotScratch *sc, const int *gate) {
     if (aligned) {
         const int smem = kDotStages * (SAME ? 1 : 2) * kDotThreads * (int)sizeof(double2);
-        static bool attr = false;  // once per instantiation
-        if (!attr) {
-            if (cudaFuncSetAttribute(k_dot_tree<G, SAME, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) !=
-                cudaSuccess)
-                return CUOZBLAS_STATUS_CUDA_ERROR;
-            attr = true;
-        }
+        static std::atomic<uint64_t> attr{0};  // devices already opted in, per instantiation
+        if (smem_optin((const void *)k_dot_tree<G, SAME, true>, smem, attr) != cudaSuccess)
+            return CUOZBLAS_STATUS_CUDA_ERROR;
         k_dot_tree<G, SAME, true><<<grid, kDotThreads, smem, s>>>(n, x, y, rho, maxS, sum_mode, sc, gate);
     } else {
         k_dot_tree<G, SAME, false><<<grid, kDotThreads, 0, s>>>(n, x, y, rho, maxS, sum_mode, sc, gate);
@@ -348,14 +344,14 @@ int dot_scan_launch(cudaStream_t s, int nsm, int n, const double *x, const doubl
 }
 
 int dot_tree_launch(cudaStream_t s, int nsm, int n, const double *x, const double *y, int rho, int maxS,
-                    int sum_mode, DotScratch *sc, const int *gate) {
+                    int sum_mode, DotScratch *sc, const int *gate, bool tree_only) {
     const int G = chain_group(rho, 4);  // levels cut from one base value
     const bool same = (x == y);
     const bool aligned = ((reinterpret_cast<uintptr_t>(x) | reinterpret_cast<uintptr_t>(y)) & 15u) == 0;
     // 16-byte aligned vectors of at least 2^22 elements with 2 or 3 digits per
     // level take the tensor-core pass (it holds every valid plan; below that
     // length its fixed costs outweigh the FP64 tree pass, which takes the rest)
-    if (aligned && n >= (1 << 22) && dot_i8_digits(rho) > 0 && !getenv("OZBLAS_DOT_TREE"))
+    if (aligned && n >= (1 << 22) && dot_i8_digits(rho) > 0 && !tree_only)
         return dot_i8_launch(s, nsm, n, x, y, rho, maxS, sum_mode, sc, gate);
     int fblocks = (int)(((int64_t)n + 2 * kDotThreads - 1) / (2 * kDotThreads));
     if (fblocks > nsm) fblocks = nsm;  // ~250 registers per thread: one 256-thread block per SM
@@ -401,14 +397,14 @@ int dot_fused(cuozblasHandle_t *h, int n, const double *x, const double *y, doub
     counted(h);
     OZB_TRY(dot_scan_launch(st->stream, nsm, n, x, y, sc));
     counted(h);
-    OZB_TRY(dot_tree_launch(st->stream, nsm, n, x, y, rho, maxS, h->sumMode, sc, nullptr));
+    OZB_TRY(dot_tree_launch(st->stream, nsm, n, x, y, rho, maxS, h->sumMode, sc, nullptr, st->env.dot_tree));
     static_assert(sizeof(DotStatus) == 24, "status block layout");
     OZB_CHECK(cudaMemcpyAsync(st->h_dbl, &sc->out, sizeof(DotStatus), cudaMemcpyDeviceToHost, st->stream));
     OZB_CHECK(cudaStreamSynchronize(st->stream));
     ar.release(mk);
     DotStatus res;
     memcpy(&res, st->h_dbl, sizeof(res));
-    if (res.status != 1 && getenv("OZBLAS_DOT_TRACE"))
+    if (res.status != 1 && state(h)->env.dot_trace)
         fprintf(stderr, "cuozblas: dot fused not used (n=%d, reason bits %d)\n", n, res.pad);
     if (res.status == 1) {
         *done = true;

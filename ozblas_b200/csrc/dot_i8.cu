@@ -414,13 +414,9 @@ template <bool SAME, int D, int G>
 static int launch_i8(int grid, cudaStream_t s, int n, const double *x, const double *y, int rho, int maxS,
                      int sum_mode, DotScratch *sc, const int *gate) {
     constexpr int RP = D == 2 ? 16 : 32;
-    static bool attr = false;  // once per instantiation
-    if (!attr) {
-        if (cudaFuncSetAttribute(k_dot_i8<SAME, D, RP, G>, cudaFuncAttributeMaxDynamicSharedMemorySize, kDiSmem) !=
-            cudaSuccess)
-            return CUOZBLAS_STATUS_CUDA_ERROR;
-        attr = true;
-    }
+    static std::atomic<uint64_t> attr{0};  // devices already opted in, per instantiation
+    if (smem_optin((const void *)k_dot_i8<SAME, D, RP, G>, kDiSmem, attr) != cudaSuccess)
+        return CUOZBLAS_STATUS_CUDA_ERROR;
     k_dot_i8<SAME, D, RP, G><<<grid, kDiThreads, kDiSmem, s>>>(n, x, y, rho, maxS, sum_mode, sc, gate);
     return cudaGetLastError() == cudaSuccess ? CUOZBLAS_STATUS_SUCCESS : CUOZBLAS_STATUS_CUDA_ERROR;
 }

@@ -44,7 +44,8 @@ struct CsrScratch {
 // zeroed.  `gate` (device int, may be null): the kernel does nothing when 0.
 int dot_scan_launch(cudaStream_t s, int nsm, int n, const double *x, const double *y, DotScratch *sc);
 int dot_tree_launch(cudaStream_t s, int nsm, int n, const double *x, const double *y, int rho, int maxS,
-                    int sum_mode, DotScratch *sc, const int *gate);
+                    int sum_mode, DotScratch *sc, const int *gate,
+                    bool tree_only = false);
 // Sets the kernels' shared-memory attribute up front (before a capture).
 int dot_tree_prepare();
 // The tensor-core form of pass 2 (dot_i8.cu): digits per level for rho (0:

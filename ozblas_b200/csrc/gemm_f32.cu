@@ -284,7 +284,7 @@ int gemm_f32_core(cuozblasHandle_t *h, char ta, char tb, int m, int n, int k, do
 
     // rho >= 47 (k > 1024): every slice is an int8 times a power of two, and the
     // exact slice products run on the INT8 tensor cores (same bits)
-    if (!dot && !skinny_n && rho >= 47 && !getenv("OZBLAS_DS_SIMT")) {
+    if (!dot && !skinny_n && rho >= 47 && !state(h)->env.ds_simt) {
         st->plain_timers = true;
         int nA = 0, nB = 0, np = 0;
         OZB_TRY(gemm_ds_i8_core(h, ta, tb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, rho, fastMode, &nA, &nB,
@@ -347,7 +347,7 @@ int gemm_f32_core(cuozblasHandle_t *h, char ta, char tb, int m, int n, int k, do
                 counted(h);
                 if (dot) {
                     int blocks = (k + 255) / 256;
-                    if (blocks > 148 * 8) blocks = 148 * 8;
+                    if (blocks > sm_count() * 8) blocks = sm_count() * 8;
                     if (blocks < 1) blocks = 1;
                     k_pair_dot_f32<<<blocks, 256, 0, st->stream>>>(k, na, nb, Sa + (size_t)ia0 * ldk, ldk,
                                                                    Sb + (size_t)ib0 * ldk, ldk, P + ia0 * nB + ib0,

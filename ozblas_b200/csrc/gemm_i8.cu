@@ -612,39 +612,47 @@ static int split_digits(cuozblasHandle_t *h, bool strided, int nl, int k, const 
 // group.z the flush exponent).  Pair
 // set: full, or the triangle ia + ib <= min(nA, nB) - 1
 // (src/cuda/cuozblas_gemm.cu:138).  Returns the number of pairs.
-int i8_schedule(int nA, int nB, int nkb, bool triangular, std::vector<int4> &items, std::vector<int4> &groups) {
+// Fixed-capacity form: writes at most max_items items and max_groups groups
+// (counts to *ni, *ng); returns the number of pairs, or -1 when a capacity or
+// the 128-level bound of the run table is exceeded (nothing usable written).
+int i8_schedule_into(int nA, int nB, int nkb, bool triangular, int4 *items, int max_items, int *ni, int4 *groups,
+                     int max_groups, int *ng) {
     const int maxlevel = triangular ? (nA < nB ? nA : nB) - 1 : nA + nB - 2;
+    constexpr int kMaxLevels = 128;
+    if (maxlevel + 1 > kMaxLevels || max_groups < 1) return -1;
     // products per output in one INT32 group: (kb1 - kb0) * 128 each
     const int64_t kb_cap = I8_MAX_TERMS / I8_BK;  // k-blocks per group
-    items.clear();
-    groups.clear();
-    std::vector<int64_t> gbound;  // max |V| of each group (products x 127^2)
-    int npairs = 0;
+    unsigned __int128 lbound[kMaxLevels];  // max |V| of each level (products x 127^2)
+    for (int L = 0; L <= maxlevel; L++) lbound[L] = 0;
+    int n_it = 0, n_gr = 0, npairs = 0;
+    auto close_group = [&](int gbeg, int L, int64_t used) {
+        if (n_gr >= max_groups) return false;
+        groups[n_gr++] = make_int4(gbeg, n_it, L, 0);
+        lbound[L] += (unsigned __int128)(used * I8_BK * 127 * 127);
+        return true;
+    };
     for (int L = 0; L <= maxlevel; L++) {  // largest level sums first
         const int lo = L - (nB - 1) > 0 ? L - (nB - 1) : 0, hi = L < nA - 1 ? L : nA - 1;
         int64_t used = 0;
-        int gbeg = (int)items.size();
+        int gbeg = n_it;
         for (int ia = lo; ia <= hi; ia++) {
             npairs++;
             for (int kb0 = 0; kb0 < nkb;) {
                 int64_t room = kb_cap - used;
                 if (room <= 0) {
-                    groups.push_back(make_int4(gbeg, (int)items.size(), L, 0));
-                    gbound.push_back(used * I8_BK * 127 * 127);
-                    gbeg = (int)items.size();
+                    if (!close_group(gbeg, L, used)) return -1;
+                    gbeg = n_it;
                     used = 0;
                     room = kb_cap;
                 }
                 const int kb1 = (int)((nkb - kb0) < room ? nkb : kb0 + room);
-                items.push_back(make_int4(ia, L - ia, kb0, kb1));
+                if (n_it >= max_items) return -1;
+                items[n_it++] = make_int4(ia, L - ia, kb0, kb1);
                 used += kb1 - kb0;
                 kb0 = kb1;
             }
         }
-        if ((int)items.size() > gbeg) {
-            groups.push_back(make_int4(gbeg, (int)items.size(), L, 0));
-            gbound.push_back(used * I8_BK * 127 * 127);
-        }
+        if (n_it > gbeg && !close_group(gbeg, L, used)) return -1;
     }
     // Runs of consecutive levels whose exact combination stays below 2^53,
     // formed from the most significant level up (levels 0..3, 4..7, ...):
@@ -654,43 +662,51 @@ int i8_schedule(int nA, int nB, int nkb, bool triangular, std::vector<int4> &ite
     // FP64 sum is still exact); level L of run [L_lo, L_hi] is shifted by
     // 7 (L_hi - L) bits and the run's last visited group (level L_hi) flushes
     // acc * 2^(-7 (L_hi + 2)).
-    {
-        std::vector<unsigned __int128> lbound(maxlevel + 1, 0);
-        for (size_t g = 0; g < groups.size(); g++) lbound[groups[g].z] += (unsigned __int128)gbound[g];
-        const unsigned __int128 lim = (unsigned __int128)1 << 53;
-        std::vector<int> run_hi(maxlevel + 1), run_lo(maxlevel + 1);
-        for (int L0 = 0; L0 <= maxlevel;) {
-            unsigned __int128 b = lbound[L0];
-            int L1 = L0;
-            while (L1 + 1 <= maxlevel && (b << 7) + lbound[L1 + 1] < lim) {
-                b = (b << 7) + lbound[L1 + 1];
-                L1++;
-            }
-            for (int L = L0; L <= L1; L++) {
-                run_lo[L] = L0;
-                run_hi[L] = L1;
-            }
-            L0 = L1 + 1;
+    const unsigned __int128 lim = (unsigned __int128)1 << 53;
+    int run_hi[kMaxLevels];
+    for (int L0 = 0; L0 <= maxlevel;) {
+        unsigned __int128 b = lbound[L0];
+        int L1 = L0;
+        while (L1 + 1 <= maxlevel && (b << 7) + lbound[L1 + 1] < lim) {
+            b = (b << 7) + lbound[L1 + 1];
+            L1++;
         }
-        bool first = true;
-        for (size_t g = 0; g < groups.size(); g++) {
-            const int L = groups[g].z;
-            int meta = 7 * (run_hi[L] - L);
-            const bool last_of_level = (g + 1 == groups.size()) || groups[g + 1].z != L;
-            if (last_of_level && L == run_hi[L]) {
-                meta |= (1 << 8) | (first ? (1 << 9) : 0);
-                first = false;
-                groups[g].z = -7 * (run_hi[L] + 2);
-                // the next run's flush exponent: the rounding error of this flush is carried there
-                if (L < maxlevel) meta |= (-7 * (run_hi[L + 1] + 2) + 32768) << 16;
-            } else {
-                groups[g].z = 0;
-            }
-            groups[g].w = meta;
-        }
-        if (!groups.empty()) groups.back().w |= (1 << 10);
+        for (int L = L0; L <= L1; L++) run_hi[L] = L1;
+        L0 = L1 + 1;
     }
+    bool first = true;
+    for (int g = 0; g < n_gr; g++) {
+        const int L = groups[g].z;
+        int meta = 7 * (run_hi[L] - L);
+        const bool last_of_level = (g + 1 == n_gr) || groups[g + 1].z != L;
+        if (last_of_level && L == run_hi[L]) {
+            meta |= (1 << 8) | (first ? (1 << 9) : 0);
+            first = false;
+            groups[g].z = -7 * (run_hi[L] + 2);
+            // the next run's flush exponent: the rounding error of this flush is carried there
+            if (L < maxlevel) meta |= (-7 * (run_hi[L + 1] + 2) + 32768) << 16;
+        } else {
+            groups[g].z = 0;
+        }
+        groups[g].w = meta;
+    }
+    if (n_gr > 0) groups[n_gr - 1].w |= (1 << 10);
+    *ni = n_it;
+    *ng = n_gr;
     return npairs;
+}
+
+int i8_schedule(int nA, int nB, int nkb, bool triangular, std::vector<int4> &items, std::vector<int4> &groups) {
+    // every pair spans at most ceil(nkb / kb_cap) + 1 items, and a group holds at least one item
+    const int64_t per_pair = (int64_t)nkb / (I8_MAX_TERMS / I8_BK) + 2;
+    const int64_t cap = (int64_t)(nA > 0 ? nA : 1) * (nB > 0 ? nB : 1) * per_pair;
+    items.assign((size_t)cap, make_int4(0, 0, 0, 0));
+    groups.assign((size_t)cap, make_int4(0, 0, 0, 0));
+    int ni = 0, ng = 0;
+    const int np = i8_schedule_into(nA, nB, nkb, triangular, items.data(), (int)cap, &ni, groups.data(), (int)cap, &ng);
+    items.resize(np < 0 ? 0 : (size_t)ni);
+    groups.resize(np < 0 ? 0 : (size_t)ng);
+    return np;
 }
 
 // Default digit cap when nSplitMax is 0 (enough for an exact split of
@@ -712,6 +728,7 @@ int gemm_i8_core(cuozblasHandle_t *h, char ta, char tb, int m, int n, int k, dou
     const int nkb = k_pad / I8_BK;
     std::vector<int4> items, groups;
     const int npairs = i8_schedule(nA, nB, nkb, h->fastMode != 0, items, groups);
+    if (npairs < 0) return CUOZBLAS_STATUS_NOT_SUPPORTED;
     h->nSplitA = (float)nA;
     h->nSplitB = (float)nB;
     h->nSplitC = (float)npairs;
@@ -1042,9 +1059,10 @@ int i8_exact_pairs(cuozblasHandle_t *h, int m, int n, int k_pad, const int8_t *d
 // ---------------------------------------------------------------------------
 // Allocation-free variant of the INT8 product path (cuozblasDgemmI8Static).
 //
-// Some callers cannot allocate device memory at all: code that runs while a
-// CUDA graph is being captured, real-time or embedded hosts whose memory is
-// budgeted up front, and hosts whose own allocator owns the whole device.
+// Some callers cannot allocate device memory at all: real-time or embedded
+// hosts whose device memory is budgeted once at start-up, and hosts whose own
+// allocator (a framework's caching allocator, say) already owns the whole
+// device, so a cudaMalloc inside the library would fail or fight it.
 // For them the digit split and the tcgen05 product kernel run on scratch in
 // the file-scope array below instead of a handle's arena, so a call makes no
 // cudaMalloc, no cudaFree and no other allocation.  The array is 64 MiB and
@@ -1162,76 +1180,13 @@ static int dgemm_i8_static(char ta, char tb, int m, int n, int k, double alpha, 
     OZB_CHECK(cudaGetLastError());
 
     // the same schedule as cuozblasDgemmI8, built in fixed host arrays
-    const int maxlevel = fast ? (nA < nB ? nA : nB) - 1 : nA + nB - 2;
     const int nkb = k_pad / I8_BK;
-    const int64_t kb_cap = I8_MAX_TERMS / I8_BK;
     int4 items[kI8StaticMaxItems], groups[kI8StaticMaxGroups];
-    int64_t gbound[kI8StaticMaxGroups];
     int ni = 0, ng = 0;
-    for (int L = 0; L <= maxlevel; L++) {
-        const int lo = L - (nB - 1) > 0 ? L - (nB - 1) : 0, hi = L < nA - 1 ? L : nA - 1;
-        int64_t used = 0;
-        int gbeg = ni;
-        for (int ia = lo; ia <= hi; ia++) {
-            for (int kb0 = 0; kb0 < nkb;) {
-                int64_t room = kb_cap - used;
-                if (room <= 0) {
-                    if (ng >= kI8StaticMaxGroups) return CUOZBLAS_STATUS_WORKSPACE;
-                    gbound[ng] = used * I8_BK * 127 * 127;
-                    groups[ng++] = make_int4(gbeg, ni, L, 0);
-                    gbeg = ni;
-                    used = 0;
-                    room = kb_cap;
-                }
-                const int kb1 = (int)((nkb - kb0) < room ? nkb : kb0 + room);
-                if (ni >= kI8StaticMaxItems) return CUOZBLAS_STATUS_WORKSPACE;
-                items[ni++] = make_int4(ia, L - ia, kb0, kb1);
-                used += kb1 - kb0;
-                kb0 = kb1;
-            }
-        }
-        if (ni > gbeg) {
-            if (ng >= kI8StaticMaxGroups) return CUOZBLAS_STATUS_WORKSPACE;
-            gbound[ng] = used * I8_BK * 127 * 127;
-            groups[ng++] = make_int4(gbeg, ni, L, 0);
-        }
-    }
-    {
-        unsigned __int128 lbound[2 * 64];
-        int run_hi[2 * 64], run_lo[2 * 64];
-        if (maxlevel + 1 > 2 * 64) return CUOZBLAS_STATUS_NOT_SUPPORTED;
-        for (int L = 0; L <= maxlevel; L++) lbound[L] = 0;
-        for (int g = 0; g < ng; g++) lbound[groups[g].z] += (unsigned __int128)gbound[g];
-        const unsigned __int128 lim = (unsigned __int128)1 << 53;
-        for (int L0 = 0; L0 <= maxlevel;) {
-            unsigned __int128 b = lbound[L0];
-            int L1 = L0;
-            while (L1 + 1 <= maxlevel && (b << 7) + lbound[L1 + 1] < lim) {
-                b = (b << 7) + lbound[L1 + 1];
-                L1++;
-            }
-            for (int L = L0; L <= L1; L++) {
-                run_lo[L] = L0;
-                run_hi[L] = L1;
-            }
-            L0 = L1 + 1;
-        }
-        bool first = true;
-        for (int g = 0; g < ng; g++) {
-            const int L = groups[g].z;
-            int meta = 7 * (run_hi[L] - L);
-            const bool last_of_level = (g + 1 == ng) || groups[g + 1].z != L;
-            if (last_of_level && L == run_hi[L]) {
-                meta |= (1 << 8) | (first ? (1 << 9) : 0);
-                first = false;
-                groups[g].z = -7 * (run_hi[L] + 2);
-                if (L < maxlevel) meta |= (-7 * (run_hi[L + 1] + 2) + 32768) << 16;
-            } else {
-                groups[g].z = 0;
-            }
-            groups[g].w = meta;
-        }
-        groups[ng - 1].w |= (1 << 10);
+    if (i8_schedule_into(nA, nB, nkb, fast != 0, items, kI8StaticMaxItems, &ni, groups, kI8StaticMaxGroups, &ng) < 0) {
+        fprintf(stderr, "cuozblasDgemmI8Static: %d x %d digits over k=%d exceed the static schedule (%d items, %d "
+                "groups)\n", nA, nB, k, kI8StaticMaxItems, kI8StaticMaxGroups);
+        return CUOZBLAS_STATUS_WORKSPACE;
     }
     OZB_CHECK(cudaMemcpyAsync(d_sched, items, sizeof(int4) * ni, cudaMemcpyHostToDevice, stream));
     OZB_CHECK(cudaMemcpyAsync(d_sched + ni, groups, sizeof(int4) * ng, cudaMemcpyHostToDevice, stream));
@@ -1274,6 +1229,13 @@ static int dgemm_i8_static(char ta, char tb, int m, int n, int k, double alpha, 
     return CUOZBLAS_STATUS_SUCCESS;
 }
 
+// Leading dimensions of the stored A (m x k for 'n', k x m otherwise) and B
+// (k x n for 'n', n x k otherwise), as a column-major BLAS checks them.
+static bool i8_lds_valid(char ta, char tb, int m, int n, int k, int lda, int ldb) {
+    const int ra = is_trans(ta) ? k : m, rb = is_trans(tb) ? n : k;
+    return lda >= (ra > 1 ? ra : 1) && ldb >= (rb > 1 ? rb : 1);
+}
+
 }  // namespace ozb
 
 
@@ -1283,6 +1245,7 @@ extern "C" int cuozblasDgemmI8(cuozblasHandle_t *h, char transa, char transb, in
     using namespace ozb;
     OZB_TRY(counter_init(h));
     if (m < 0 || n < 0 || k < 0 || ldc < (m > 1 ? m : 1)) return CUOZBLAS_STATUS_INVALID_VALUE;
+    if (!i8_lds_valid(transa, transb, m, n, k, lda, ldb)) return CUOZBLAS_STATUS_INVALID_VALUE;
     if (h->nSplitMax < 0 || h->nSplitMax > 64) return CUOZBLAS_STATUS_INVALID_VALUE;
     if (m == 0 || n == 0) return CUOZBLAS_STATUS_SUCCESS;
     return gemm_i8_core(h, transa, transb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc);
@@ -1296,6 +1259,7 @@ extern "C" int cuozblasDgemmI8Static(char transa, char transb, int32_t m, int32_
     using namespace ozb;
     if (m < 0 || n < 0 || k < 0 || ldc < (m > 1 ? m : 1) || nSplitMax < 0 || nSplitMax > 64)
         return CUOZBLAS_STATUS_INVALID_VALUE;
+    if (!i8_lds_valid(transa, transb, m, n, k, lda, ldb)) return CUOZBLAS_STATUS_INVALID_VALUE;
     if (m == 0 || n == 0) return CUOZBLAS_STATUS_SUCCESS;
     return dgemm_i8_static(transa, transb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, nSplitMax, fastMode,
                            reinterpret_cast<cudaStream_t>(stream));

@@ -625,6 +625,7 @@ int gemm_i8_batched(cuozblasHandle_t *h, char ta, char tb, int count, const int 
         const GOp &oa = ops[(size_t)2 * b], &ob = ops[(size_t)2 * b + 1];
         std::vector<int4> it, gr;
         const int np = i8_schedule(oa.S, ob.S, oa.nkb, h->fastMode != 0, it, gr);
+        if (np < 0) return CUOZBLAS_STATUS_NOT_SUPPORTED;
         npairs_max = np > npairs_max ? np : npairs_max;
         const int ibase = (int)items.size();
         for (auto &g : gr) {
@@ -676,11 +677,8 @@ int gemm_i8_batched(cuozblasHandle_t *h, char ta, char tb, int count, const int 
     gp.cta_begin = d_cta;
     gp.err = d_err;
     if (ntile_total > 0) {
-        static bool attr = false;
-        if (!attr) {
-            OZB_CHECK(cudaFuncSetAttribute(k_i8_grouped, cudaFuncAttributeMaxDynamicSharedMemorySize, G_SMEM));
-            attr = true;
-        }
+        static std::atomic<uint64_t> attr{0};  // devices already opted in
+        OZB_CHECK(smem_optin((const void *)k_i8_grouped, G_SMEM, attr));
         // dealing order: same bits either way, the faster one is measured once per
         // problem set (candidates write scratch products with beta = 0)
         const uint64_t mk = ar.mark();

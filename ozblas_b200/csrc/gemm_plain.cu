@@ -449,7 +449,7 @@ int gemm_plain_core(cuozblasHandle_t *h, char ta, char tb, int m, int n, int k, 
     ev_record(h, 0);
     st->plain_timers = true;
     // GEMV 'n' (rows of A strided): fused split and products, A read nA + 2 times
-    if (skinny_n && !dot && !is_trans(ta) && !getenv("OZBLAS_GEMV_SPLIT")) {
+    if (skinny_n && !dot && !is_trans(ta) && !state(h)->env.gemv_split) {
         const uint64_t mk0 = ar.mark();
         double *xs = ar.take<double>((uint64_t)maxS * ldk);
         if (!ar.ok) return CUOZBLAS_STATUS_WORKSPACE;
@@ -516,7 +516,7 @@ int gemm_plain_core(cuozblasHandle_t *h, char ta, char tb, int m, int n, int k, 
 
     if (dot && h->splitEpsMode == 2) {  // Dot2 DOT (the caller admits fastMode 0 only)
         int blocks = (k + 255) / 256;
-        if (blocks > 148 * 4) blocks = 148 * 4;
+        if (blocks > sm_count() * 4) blocks = sm_count() * 4;
         if (blocks < 1) blocks = 1;
         DD *partials = ar.take<DD>((uint64_t)nA * nB * blocks);
         double *tmp = ar.take<double>((uint64_t)4 * nA * nB + 1);
@@ -545,7 +545,7 @@ int gemm_plain_core(cuozblasHandle_t *h, char ta, char tb, int m, int n, int k, 
                 if (dot) {
                     // P block at (ia0, ib0) with row stride nB
                     int blocks = (k + 255) / 256;
-                    if (blocks > 148 * 8) blocks = 148 * 8;
+                    if (blocks > sm_count() * 8) blocks = sm_count() * 8;
                     if (blocks < 1) blocks = 1;
                     counted(h);
                     k_pair_dot<<<blocks, 256, 0, st->stream>>>(k, na, nb, Sa + (size_t)ia0 * ldk, ldk,
@@ -585,7 +585,7 @@ int gemm_plain_core(cuozblasHandle_t *h, char ta, char tb, int m, int n, int k, 
                               sizeof(double) * (uint64_t)np * m * n + (1u << 20);
         const uint64_t avail = h->workSizeBytes - ((ar.mark() + 255) / 256 * 256);
         if (Ea && Eb && D <= 4 && (double)D * k * 127.0 * 127.0 < 2147483647.0 && need < avail &&
-            !getenv("OZBLAS_PLAIN_DMMA")) {
+            !state(h)->env.plain_dmma) {
             std::vector<int2> pl;
             for_each_pair(nA, nB, maxlevel, [&](int ia, int ib) { pl.push_back(make_int2(ia, ib)); });
             int8_t *dg[2];
@@ -596,7 +596,7 @@ int gemm_plain_core(cuozblasHandle_t *h, char ta, char tb, int m, int n, int k, 
                 OZB_CHECK(cudaMemsetAsync(dg[o], 0, (size_t)ns * D * lpad * k_pad, st->stream));
                 const int64_t total = (int64_t)ns * nl * k;
                 int blocks = (int)((total + 255) / 256);
-                if (blocks > 148 * 16) blocks = 148 * 16;
+                if (blocks > sm_count() * 16) blocks = sm_count() * 16;
                 if (blocks < 1) blocks = 1;
                 counted(h);
                 k_slices_to_digits<<<blocks, 256, 0, st->stream>>>(ns, nl, k, ldk, o == 0 ? Sa : Sb, 53 - rho,
@@ -695,7 +695,7 @@ int pair_products_skinny(cuozblasHandle_t *h, bool dot, int m, int k, int nA, in
             counted(h);
             if (dot) {
                 int blocks = (k + 255) / 256;
-                if (blocks > 148 * 8) blocks = 148 * 8;
+                if (blocks > sm_count() * 8) blocks = sm_count() * 8;
                 if (blocks < 1) blocks = 1;
                 k_pair_dot<<<blocks, 256, 0, st->stream>>>(k, na, nb, Sa + (size_t)ia0 * ldk, ldk,
                                                            Sb + (size_t)ib0 * ldk, ldk, P + ia0 * nB + ib0, nB);
@@ -848,7 +848,7 @@ int gemm_sd_core(cuozblasHandle_t *h, char ta, char tb, int m, int n, int k, flo
                 counted(h);
                 if (dot) {
                     int blocks = (k + 255) / 256;
-                    if (blocks > 148 * 8) blocks = 148 * 8;
+                    if (blocks > sm_count() * 8) blocks = sm_count() * 8;
                     if (blocks < 1) blocks = 1;
                     k_pair_dot<<<blocks, 256, 0, st->stream>>>(k, na, nb, Sa + (size_t)ia0 * ldk, ldk,
                                                                Sb + (size_t)ib0 * ldk, ldk, P + ia0 * nB + ib0, nB);
@@ -880,7 +880,7 @@ int gemm_sd_core(cuozblasHandle_t *h, char ta, char tb, int m, int n, int k, flo
                               sizeof(double) * (uint64_t)np * m * n + (1u << 20);
         const uint64_t avail = h->workSizeBytes - ((ar.mark() + 255) / 256 * 256);
         if (rho >= 2 && D <= 4 && (double)D * k * 127.0 * 127.0 < 2147483647.0 && need < avail &&
-            !getenv("OZBLAS_SD_DMMA")) {
+            !state(h)->env.sd_dmma) {
             std::vector<int2> pl;
             for_each_pair(nA, nB, maxlevel, [&](int ia, int ib) { pl.push_back(make_int2(ia, ib)); });
             int8_t *dg[2];
@@ -891,7 +891,7 @@ int gemm_sd_core(cuozblasHandle_t *h, char ta, char tb, int m, int n, int k, flo
                 OZB_CHECK(cudaMemsetAsync(dg[o], 0, (size_t)ns * D * lpad * k_pad, st->stream));
                 const int64_t total = (int64_t)ns * nl * k;
                 int blocks = (int)((total + 255) / 256);
-                if (blocks > 148 * 16) blocks = 148 * 16;
+                if (blocks > sm_count() * 16) blocks = sm_count() * 16;
                 if (blocks < 1) blocks = 1;
                 counted(h);
                 k_slices_to_digits<<<blocks, 256, 0, st->stream>>>(ns, nl, k, ldk, o == 0 ? Sa : Sb, 24 - rho, nullptr,

@@ -284,7 +284,7 @@ int gemm_q_core(cuozblasHandle_t *h, char ta, char tb, int m, int n, int k, cons
         const uint64_t need = (uint64_t)nA * D * lpadA * k_pad + (uint64_t)nB * D * lpadB * k_pad +
                               sizeof(double) * (uint64_t)np * m * n + (uint64_t)16 * (m > n ? m : n) * k + (1u << 20);
         const uint64_t avail = h->workSizeBytes - ((ar.mark() + 255) / 256 * 256);
-        if (D <= 4 && (double)D * k * 127.0 * 127.0 < 2147483647.0 && need < avail && !getenv("OZBLAS_Q_DMMA")) {
+        if (D <= 4 && (double)D * k * 127.0 * 127.0 < 2147483647.0 && need < avail && !state(h)->env.q_dmma) {
             std::vector<int2> pl;
             for_each_pair(nA, nB, maxlevel, [&](int ia, int ib) { pl.push_back(make_int2(ia, ib)); });
             int8_t *dg[2];

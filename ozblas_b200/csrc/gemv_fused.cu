@@ -340,13 +340,9 @@ __global__ void k_gemv_chain(int m, int rho, int it, double *__restrict__ Ma, in
 template <int NB, bool PRED>
 static int launch_gt(dim3 grid, cudaStream_t s, const CUtensorMap &tm, int m, int n, int rho, int cpb, const int *T,
                      const int *state, const double *xs, int ldx, double *P, double *Ma, int *err) {
-    static bool attr = false;  // once per instantiation
-    if (!attr) {
-        if (cudaFuncSetAttribute(k_gemv_tma<NB, PRED>, cudaFuncAttributeMaxDynamicSharedMemorySize, kGtSmem) !=
-            cudaSuccess)
-            return CUOZBLAS_STATUS_CUDA_ERROR;
-        attr = true;
-    }
+    static std::atomic<uint64_t> attr{0};  // devices already opted in, per instantiation
+    if (smem_optin((const void *)k_gemv_tma<NB, PRED>, kGtSmem, attr) != cudaSuccess)
+        return CUOZBLAS_STATUS_CUDA_ERROR;
     k_gemv_tma<NB, PRED><<<grid, 256, kGtSmem, s>>>(tm, m, n, rho, cpb, T, state, xs, ldx, P, Ma, err);
     return cudaGetLastError() == cudaSuccess ? CUOZBLAS_STATUS_SUCCESS : CUOZBLAS_STATUS_CUDA_ERROR;
 }
@@ -397,7 +393,7 @@ int gemv_fused_n(cuozblasHandle_t *h, int m, int n, const double *A, int lda, co
     // (repeated for the rows whose chain broke); the level passes below when
     // A does not suit a tensor map or a chain stays unproven
     CUtensorMap tm;
-    if (!getenv("OZBLAS_GEMV_LEVELS") && make_map_f64(&tm, A, m, n, lda, 32, kGtCols) == CUOZBLAS_STATUS_SUCCESS) {
+    if (!state(h)->env.gemv_levels && make_map_f64(&tm, A, m, n, lda, 32, kGtCols) == CUOZBLAS_STATUS_SUCCESS) {
         const uint64_t mk2 = ar.mark();
         double *Ma = ar.take<double>((uint64_t)(kGvMaxLevels + 1) * m);
         int *T = ar.take<int>((uint64_t)kGvMaxLevels * m);
@@ -405,7 +401,7 @@ int gemv_fused_n(cuozblasHandle_t *h, int m, int n, const double *A, int lda, co
         int *flags = ar.take<int>(4 + kGtIters);  // zmax, capacity, err, pad, failures per pass
         if (ar.ok) {
             const int rb = (m + 31) / 32, ctiles = (n + kGtCols - 1) / kGtCols;
-            int gy = (148 * 8 + rb - 1) / rb;  // about eight blocks per SM in all
+            int gy = (sm_count() * 8 + rb - 1) / rb;  // about eight blocks per SM in all
             gy = gy < 1 ? 1 : (gy > ctiles ? ctiles : gy);
             const int cpb = (ctiles + gy - 1) / gy * kGtCols;
             const dim3 g2(rb, (n + cpb - 1) / cpb);

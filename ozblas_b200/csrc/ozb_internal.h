@@ -1,5 +1,6 @@
 // ozb_internal.h — host-side state shared by the library's translation units.
 #pragma once
+#include <atomic>
 #include <vector>
 #include <cuda_runtime.h>
 #include <stdint.h>
@@ -12,6 +13,23 @@ namespace ozb {
 
 constexpr int kMaxSplitDefault = 30;  // NumSplitDefaultMax, src/cuda/cuozblas_common.h:5
 constexpr int kArenaAlign = 256;
+
+// Diagnostic switches from the environment, read when a handle is created
+// (and again by cuozblasHandleReadEnv), never on a call path.  Each selects an
+// equal-bits alternative path or a trace on stderr.
+struct EnvSwitches {
+    bool gemv_split = false;   // OZBLAS_GEMV_SPLIT: GEMV 'n' over materialised slices
+    bool gemv_levels = false;  // OZBLAS_GEMV_LEVELS: fused GEMV with one read of A per level
+    bool plain_dmma = false;   // OZBLAS_PLAIN_DMMA: plain GEMM pair products on DMMA
+    bool sd_dmma = false;      // OZBLAS_SD_DMMA: <float,double,double> products on DMMA
+    bool q_dmma = false;       // OZBLAS_Q_DMMA: quad-form products on DMMA
+    bool ds_simt = false;      // OZBLAS_DS_SIMT: <double,float,float> on the FP32 SIMT kernel
+    bool dot_tree = false;     // OZBLAS_DOT_TREE: DOT pass 2 on the FP64 tree
+    bool cg_no_graph = false;  // OZBLAS_CG_NO_GRAPH: CG iterations on the host loop
+    bool dot_trace = false;    // OZBLAS_DOT_TRACE
+    bool cg_trace = false;     // OZBLAS_CG_TRACE
+    void read();
+};
 
 // Per-handle private state; the reference handle's hstBatchAddr field points
 // here (the batched-GEMM pointer arrays it held in the reference have no
@@ -28,6 +46,7 @@ struct State {
     cudaEvent_t ev[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};  // phase timers (split A/B, products, sum)
     bool plain_timers = false;    // ev[0..4] hold a plain-form call's phases, read at the call's end
     uint64_t launches = 0;        // kernels this handle has launched (cuozblasGetLaunchCount)
+    EnvSwitches env;
     // The matrix of the last fused CSRMV and the level count its rows needed:
     // the next call on the same matrix holds that many levels per row on chip
     // (rows that need more go to the per-row kernel, so a stale count costs
@@ -109,6 +128,21 @@ inline int sm_count() {
     return n;
 }
 
+// Opt a kernel into `bytes` of dynamic shared memory on the current device.
+// The attribute belongs to each device's context, so `done` keeps one bit per
+// device (devices 64 and up set it on every call); concurrent first calls on
+// one device both set it, which is harmless.
+inline cudaError_t smem_optin(const void *func, int bytes, std::atomic<uint64_t> &done) {
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    const uint64_t bit = dev >= 0 && dev < 64 ? (uint64_t)1 << dev : 0;
+    if (bit && (done.load(std::memory_order_acquire) & bit)) return cudaSuccess;
+    e = cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    if (e == cudaSuccess && bit) done.fetch_or(bit, std::memory_order_acq_rel);
+    return e;
+}
+
 // Reference counterInit (src/cuda/cuozblas.cpp:3-21): resets the exec info,
 // splitShift and the arena pointer (keeping a pre-split A below memMaskSplitA).
 int counter_init(cuozblasHandle_t *h);
@@ -144,6 +178,10 @@ int split_csr_count(cuozblasHandle_t *h, int m, const double *val, const int *ro
                     int maxS, int *ns);
 int split_csr_write(cuozblasHandle_t *h, int m, int nnz, const double *val, const int *rowptr, int epsmode,
                     int shift, int ns, double *out, int64_t ld);
+
+// Copy n elements of esz (4, 8 or 16) bytes, `stride` elements apart, to a
+// contiguous array (csrmv.cu).
+int gather_strided(cuozblasHandle_t *h, int n, const void *src, int64_t stride, int esz, void *dst);
 
 // ---- sums ----
 int fsum_pairs_dot(cuozblasHandle_t *h, int nA, int nB, int maxlevel, const double *pairmat, double alpha,

@@ -108,6 +108,7 @@ def test_dsgemm_tensor_core_equals_simt(scale, oracle, handle, ozb, cuda, monkey
     for simt in (False, True):
         if simt:
             monkeypatch.setenv("OZBLAS_DS_SIMT", "1")
+            handle.read_env()
         dC = cuda.zeros((n, m), dtype=cuda.float64, device="cuda")
         ozb.dsgemm(handle, "n", "n", m, n, k, 1.0, dA, m, dB, k, 0.0, dC, m)
         outs.append((host(dC), handle.nSplitC))
@@ -433,6 +434,7 @@ def test_qgemm_tensor_core_equals_dmma(m, n, k, ta, tb, oracle, handle, ozb, cud
     for dmma in (False, True):
         if dmma:
             monkeypatch.setenv("OZBLAS_Q_DMMA", "1")
+            handle.read_env()
         dC = qdev(cuda, C0)
         ozb.qgemm(handle, ta, tb, m, n, k, al, qdev(cuda, A), ar, qdev(cuda, B), br, be, dC, m)
         outs.append((qhost(dC), handle.nSplitC))
@@ -454,8 +456,69 @@ def test_sdgemm_tensor_core_equals_dmma(m, n, k, ta, tb, scale, oracle, handle, 
     for dmma in (False, True):
         if dmma:
             monkeypatch.setenv("OZBLAS_SD_DMMA", "1")
+            handle.read_env()
         dC = dev(cuda, C0)
         ozb.sdgemm(handle, ta, tb, m, n, k, 1.25, dev(cuda, A), ar, dev(cuda, B), br, -0.5, dC, m)
         outs.append((host(dC), handle.nSplitC))
     assert f32_bits_equal(outs[0][0], outs[1][0]), f32_first_diff(outs[0][0], outs[1][0])
     assert outs[0][1] == outs[1][1]
+
+
+# Strided vector operands in the mixed and quad forms: a one-column op(B)
+# stored as a 1 x k row (tb = 't', ldb > 1) and the one-row op(A) of a 1 x 1
+# product with lda > 1; the slots between the elements hold NaN, the oracle
+# reads the same storage.
+MIXED_STRIDED = [
+    # m, n, k, ta, tb, lda, ldb
+    (37, 1, 300, "n", "t", 37, 5),
+    (1, 1, 257, "n", "n", 3, 257),
+    (1, 1, 257, "n", "t", 2, 4),
+]
+
+
+def _strided_f64(oracle, m, k, ta, tb, lda, ldb):
+    if ta == "n":
+        A = np.full(lda * k, np.nan)
+        A.reshape(k, lda)[:, :m] = oracle.phi_matrix(m, k, 1.0, 1)[:, :m]
+    else:
+        A = oracle.phi_matrix(k, m, 1.0, 1).ravel()
+    if tb == "t":
+        B = np.full(ldb * k, np.nan)
+        B.reshape(k, ldb)[:, 0] = oracle.phi_vector(k, 1.0, 2)
+    else:
+        B = oracle.phi_vector(k, 1.0, 2).copy()
+    return A, B
+
+
+@pytest.mark.parametrize("case", MIXED_STRIDED, ids=lambda c: f"{c[0]}x{c[1]}x{c[2]}-{c[3]}{c[4]}")
+def test_mixed_strided_vector_operands(case, oracle, handle, ozb, cuda):
+    m, n, k, ta, tb, lda, ldb = case
+    A, B = _strided_f64(oracle, m, k, ta, tb, lda, ldb)
+    C0 = oracle.phi_matrix(m, n, 1.0, 3)
+    # <double, float, float>
+    ref, _ = oracle.dgemm_f32(make_flags(), ta, tb, m, n, k, 1.0, A, lda, B, ldb, 0.5, C0, m)
+    dC = dev(cuda, C0)
+    ozb.dsgemm(handle, ta, tb, m, n, k, 1.0, dev(cuda, A), lda, dev(cuda, B), ldb, 0.5, dC, m)
+    out = host(dC)
+    assert np.all(np.isfinite(ref)) and bits_equal(out, ref), first_diff(out, ref)
+    # <float, double, double>
+    Af, Bf, Cf = A.astype(np.float32), B.astype(np.float32), C0.astype(np.float32)
+    ref, _ = oracle.sgemm_d(make_flags(), ta, tb, m, n, k, 1.0, Af, lda, Bf, ldb, 0.5, Cf, m)
+    dC = dev(cuda, Cf)
+    ozb.sdgemm(handle, ta, tb, m, n, k, 1.0, dev(cuda, Af), lda, dev(cuda, Bf), ldb, 0.5, dC, m)
+    out = host(dC)
+    assert np.all(np.isfinite(ref)) and f32_bits_equal(out, ref), f32_first_diff(out, ref)
+    # <__float128, double, double>: NaN slots become binary128 NaNs
+    qnan = oracle.q(float("nan"))
+    Aq = np.tile(qnan, (A.size, 1))
+    Bq = np.tile(qnan, (B.size, 1))
+    fa, fb = np.isfinite(A), np.isfinite(B)
+    Aq[fa] = np.array([oracle.q(v) for v in A[fa]])
+    Bq[fb] = np.array([oracle.q(v) for v in B[fb]])
+    Cq = np.array([oracle.q(v) for v in C0.ravel()])
+    al, be = oracle.q(1.0), oracle.q(0.5)
+    ref, _ = oracle.qgemm_d(make_flags(), ta, tb, m, n, k, al, Aq, lda, Bq, ldb, be, Cq, m)
+    dC = qdev(cuda, Cq)
+    ozb.qgemm(handle, ta, tb, m, n, k, al, qdev(cuda, Aq), lda, qdev(cuda, Bq), ldb, be, dC, m)
+    out = qhost(dC)
+    assert np.array_equal(out, ref)

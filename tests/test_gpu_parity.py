@@ -314,10 +314,13 @@ def test_ddot_tensor_core_pass_matches_tree(oracle, handle, ozb, cuda, monkeypat
         for sm in (0, 1):
             handle.sumMode = sm
             monkeypatch.delenv("OZBLAS_DOT_TREE", raising=False)
+            handle.read_env()
             a = (ozb.ddot(handle, n, x, y), ozb.dnrm2(handle, n, x), ozb.ddot(handle, n, y, y))
             monkeypatch.setenv("OZBLAS_DOT_TREE", "1")
+            handle.read_env()
             b = (ozb.ddot(handle, n, x, y), ozb.dnrm2(handle, n, x), ozb.ddot(handle, n, y, y))
             monkeypatch.delenv("OZBLAS_DOT_TREE", raising=False)
+            handle.read_env()
             assert np.array(a).view(np.int64).tolist() == np.array(b).view(np.int64).tolist(), (n, phi, sm, a, b)
 
 
@@ -526,6 +529,7 @@ def test_dgemm_tensor_core_pairs_equal_dmma(sm, m, n, k, ta, tb, scale, oracle, 
     for dmma in (False, True):
         if dmma:
             monkeypatch.setenv("OZBLAS_PLAIN_DMMA", "1")
+            handle.read_env()
         dC = dev(cuda, C0)
         ozb.dgemm(handle, ta, tb, m, n, k, 1.25, dev(cuda, A), ar, dev(cuda, B), br, -0.5, dC, m)
         outs.append((host(dC), handle.nSplitC))
@@ -592,3 +596,71 @@ def test_dgemv_truncated_split(nsplit, m, n, oracle, handle, ozb, cuda):
     ozb.dgemv(handle, "n", m, n, 1.0, dev(cuda, A), m, dev(cuda, x), 0.25, dy)
     assert bits_equal(host(dy), ref), first_diff(host(dy), ref)
     assert (handle.nSplitA, handle.nSplitB) == (info.nSplitA, info.nSplitB)
+
+
+# One-column op(B) stored as a 1 x k row (tb = 't', ldb > 1) and a one-row
+# op(A) of a 1 x 1 product stored with lda > 1 (ta = 'n'): the operand's
+# elements are strided, the slots between them hold NaN so a contiguous read
+# would show.  The oracle reads the same strided storage.
+STRIDED_CASES = [
+    # m, n, k, ta, tb, lda_extra, ldb, sumMode
+    (37, 1, 300, "n", "t", 0, 5, 0),
+    (37, 1, 300, "t", "t", 0, 3, 1),
+    (1, 1, 257, "n", "n", 3, None, 0),
+    (1, 1, 257, "n", "t", 2, 4, 1),
+    (1, 1, 64, "t", "t", 0, 2, 0),
+]
+
+
+def _strided_operands(oracle, m, n, k, ta, tb, lda_extra, ldb, phi=1.0):
+    if ta == "n":
+        lda = m + lda_extra
+        A = np.full(lda * k, np.nan)
+        A.reshape(k, lda)[:, :m] = oracle.phi_matrix(m, k, phi, 1)[:, :m]
+    else:
+        lda = k
+        A = oracle.phi_matrix(k, m, phi, 1).ravel()
+    if tb == "t":
+        B = np.full(ldb * k, np.nan)
+        B.reshape(k, ldb)[:, 0] = oracle.phi_vector(k, phi, 2)
+    else:
+        ldb = k
+        B = oracle.phi_vector(k, phi, 2).copy()
+    return A, lda, B, ldb
+
+
+@pytest.mark.parametrize("case", STRIDED_CASES, ids=lambda c: f"{c[0]}x{c[1]}x{c[2]}-{c[3]}{c[4]}-s{c[7]}")
+def test_dgemm_strided_vector_operands(case, oracle, handle, ozb, cuda):
+    m, n, k, ta, tb, lda_extra, ldb, sm = case
+    A, lda, B, ldb = _strided_operands(oracle, m, n, k, ta, tb, lda_extra, ldb)
+    C0 = oracle.phi_matrix(m, n, 1.0, 3)
+    ref, info = oracle.dgemm(make_flags(sumMode=sm), ta, tb, m, n, k, 1.0, A, lda, B, ldb, 0.5, C0, m)
+    assert np.all(np.isfinite(ref))
+    handle.sumMode = sm
+    dC = dev(cuda, C0)
+    ozb.dgemm(handle, ta, tb, m, n, k, 1.0, dev(cuda, A), lda, dev(cuda, B), ldb, 0.5, dC, m)
+    out = host(dC)
+    assert bits_equal(out, ref), first_diff(out, ref)
+    assert (handle.nSplitA, handle.nSplitB) == (info.nSplitA, info.nSplitB)
+
+
+def test_daxpy_public_entry(oracle, handle, ozb, cuda):
+    """cuozblasDaxpy: y = fma(alpha, x, y) elementwise (src/cuda/cuozblas_axpy.cu:5-16, reproMode 1), bit for bit;
+    incx/incy other than 1 are rejected with INVALID_VALUE (the reference's stride-1 kernel)."""
+    n = 20011
+    x = oracle.phi_vector(n, 2.0, 1)
+    y = oracle.phi_vector(n, 2.0, 2)
+    alpha = -1.2345678901234567
+    dy = dev(cuda, y)
+    ozb.daxpy(handle, n, alpha, dev(cuda, x), dy)
+    out = host(dy)
+    from fractions import Fraction
+    fa = Fraction(alpha)
+    ref = np.array([float(fa * Fraction(a) + Fraction(b)) for a, b in zip(x.tolist(), y.tolist())])  # one rounding
+    assert bits_equal(out, ref), first_diff(out, ref)
+    ozb.daxpy(handle, 0, alpha, dev(cuda, x), dy)  # n = 0: nothing changes
+    assert bits_equal(host(dy), ref)
+    for incx, incy in ((2, 1), (1, 2), (0, 1), (-1, 1)):
+        with pytest.raises(ozb.OzblasError) as e:
+            ozb.daxpy(handle, 8, alpha, dev(cuda, x), dy, incx=incx, incy=incy)
+        assert e.value.code == 2

@@ -1,7 +1,7 @@
 """The allocation-free INT8 DGEMM entry point (cuozblasDgemmI8Static).
 
-Callers that cannot allocate device memory (work recorded during CUDA graph
-capture, hosts with a fixed device-memory budget or a foreign allocator) use
+Callers that cannot allocate device memory (hosts whose device memory is
+budgeted once at start-up, or whose own allocator owns the whole device) use
 this entry point: it runs the INT8 precision form on a 64 MiB scratch array
 compiled into the library.  This file is collected last so that a run which
 stops at the first failure has already run every other test; it passes alone
