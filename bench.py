@@ -15,14 +15,23 @@ value   effective TFLOPS = 2 m n k / device time per step (inputs resident in
         (the path does not shard in this configuration).
 e2e     the same metric with host buffers: pinned host -> device copies of A
         and B, the call, and the device -> host copy of C inside each step.
-roofline  the tcgen05 product kernel alone (CUDA events around its launch on
-        the handle's stream): int8 ops per launch = pairs * 2 m n k.
+roofline  the tcgen05 product kernel alone (its phase timer: CUDA events
+        around its launch on the handle's stream): int8 ops per launch =
+        pairs * 2 m n k.
+cpu_baseline  the reference OzBLAS CPU library (oracle/_ref, built from the
+        reference's src/cpu) running its plain ozblasRgemm as one full
+        2048^3 call on all host cores; `--impl reference` times the same call
+        per step.
 
-Extra keys (rank 0): the plain FP64-slice form on the same inputs, the
-maximum relative error of both forms against the correctly rounded product
-(the library's NearSum plain form, bit-exact to the reference CPU NearSum),
-and DOT / CSRMV memory throughput.  The CPU baseline is the reference OzBLAS
-CPU library (oracle/_ref) on a bounded row sample of the same problem.
+extras (rank 0): full pairs and the plain FP64-slice form at the headline
+size; config 1 (plain DGEMM 1024^3, bits against the reference CPU library);
+config 2 (DOT / NRM2 / GEMV / CSRMV, both sum modes) and config 4 (CG 100^3,
+2000 iterations) with HBM rooflines, CPU baselines and bit checks; config 5
+(256 uneven problems in one grouped launch); config 3 (the INT8 form over
+m = n = k in {2048, 4096, 8192, 16384} x phi in {0.5, 1, 2, 4} x {triangular,
+full}, beside the plain form and native FP64 GEMM).  Accuracy everywhere is
+measured against the exact product (an exact accumulator of the oracle's C
+restatement) on sampled entries, outside the timed regions.
 """
 from __future__ import annotations
 
@@ -39,6 +48,7 @@ sys.path.insert(0, ROOT)
 
 N_DIM = 8192
 PHI = 1.0
+METRIC = "Ozaki DGEMM TFLOPS n=8192 (INT8 vs FP64 slices, err vs MPFR); DOT/CSRMV GB/s"
 
 
 def phi_matrix(rows, cols, phi, seed):
@@ -109,31 +119,65 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(rows)}
 
 
-def cpu_reference_sample(rows_sample=256, threads=None):
-    """The reference OzBLAS CPU library (plain ozblasRgemm, FP64 slices) on the
-    first `rows_sample` rows of the same 8192^3 problem.  Test-side code: the
-    oracle is only imported here, for the CPU baseline."""
-    import numpy as np
+# ---------------------------------------------------------------------------
+# Checker and CPU-baseline legs.  Everything below that touches oracle/ runs
+# outside every timed GPU region: the reference OzBLAS CPU library
+# (oracle/_ref, built from the reference's own src/cpu) is timed as the CPU
+# baseline and gives the bits the plain form must equal; the C restatement's
+# exact accumulator is the accuracy checker.  Neither is on the measured path.
+# ---------------------------------------------------------------------------
+REF_GEMM_N = 2048  # the reference CPU GEMM baseline: one full call at this size
 
+
+def _reference(threads=None):
     from oracle.oracle import Reference, have_reference
 
     if not have_reference():
-        return None, "oracle/_ref/libozblas_ref.so not built"
-    threads = threads or os.cpu_count()
-    ref = Reference(work_bytes=int(48e9), threads=threads)
-    ref.set_flags(sumMode=0, fastMode=0, nSplitMax=0, reproMode=1)
-    A = np.ascontiguousarray(phi_matrix(N_DIM, N_DIM, PHI, 1)[:, :rows_sample])  # first rows, column-major
-    B = phi_matrix(N_DIM, N_DIM, PHI, 2)
-    C = np.zeros((N_DIM, rows_sample))
-    t0 = time.perf_counter()
-    ref.dgemm("n", "n", rows_sample, N_DIM, N_DIM, 1.0, A, rows_sample, B, N_DIM, 0.0, C, rows_sample)
-    t = time.perf_counter() - t0
-    ref.close()
-    tflops = 2.0 * rows_sample * N_DIM * N_DIM / t / 1e12
-    return {"value": tflops, "unit": "TFLOPS", "cores": threads, "kind": "reference",
-            "sample": f"reference ozblasRgemm (plain FP64 slices, sumMode 0) on rows 0..{rows_sample - 1} of the "
-                      f"8192^3 phi=1 problem ({t:.2f} s, B split included)"}, None
+        return None
+    return Reference(work_bytes=int(48e9), threads=threads or os.cpu_count())
 
+
+def _cpu_model():
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return None
+
+
+def cpu_reference_gemm(n=REF_GEMM_N, reps=1, phi=PHI, ref=None):
+    """The reference CPU library's plain ozblasRgemm (FP64 slices, FSum) as one full n^3 call, B split included,
+    min over `reps` calls after one warm-up call (the reference harness: testing/testing_level3.cpp:184-205).
+    Returns (baseline dict, C of the last call) or (None, reason)."""
+    import numpy as np
+
+    own = ref is None
+    ref = ref or _reference()
+    if ref is None:
+        return None, "oracle/_ref/libozblas_ref.so not built"
+    ref.set_flags(sumMode=0, fastMode=0, nSplitMax=0, reproMode=1)
+    A = phi_matrix(n, n, phi, 1)
+    B = phi_matrix(n, n, phi, 2)
+    C = np.zeros((n, n))
+    out = ref.dgemm("n", "n", n, n, n, 1.0, A, n, B, n, 0.0, C, n)  # warm-up
+    ts = []
+    for _ in range(max(reps, 1)):
+        t0 = time.perf_counter()
+        out = ref.dgemm("n", "n", n, n, n, 1.0, A, n, B, n, 0.0, C, n)
+        ts.append(time.perf_counter() - t0)
+    info = ref.info()
+    cores = ref.threads()
+    if own:
+        ref.close()
+    t = min(ts)
+    return {"value": 2.0 * n ** 3 / t / 1e12, "unit": "TFLOPS", "cores": cores, "kind": "reference",
+            "cpu_model": _cpu_model(),
+            "sample": f"reference ozblasRgemm (plain FP64 slices {int(info['nSplitA'])}x{int(info['nSplitB'])}, "
+                      f"sumMode 0) as one full m=n=k={n} phi={phi} call, B split included; min of {len(ts)} after "
+                      f"1 warm-up ({t:.3f} s)"}, out
 
 def max_over_ranks(value, dist):
     """The slowest rank's time (or any scalar's maximum) over the process group; `dist` None: one
@@ -149,25 +193,40 @@ def max_over_ranks(value, dist):
 
 
 def run_reference_arm(args, rank, world):
+    """The reference's own CPU implementation (oracle/_ref) on the host cores: each step one full plain-form
+    ozblasRgemm call at m=n=k=REF_GEMM_N (the headline workload's algorithm at a CPU-bounded size)."""
     if rank != 0:
         return 0
-    steps = []
-    base = None
+    ref = _reference()
+    if ref is None:
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libozblas_ref.so not built"}))
+        return 0
+    import numpy as np
+
+    n = REF_GEMM_N
+    ref.set_flags(sumMode=0, fastMode=0, nSplitMax=0, reproMode=1)
+    A = phi_matrix(n, n, PHI, 1)
+    B = phi_matrix(n, n, PHI, 2)
+    C = np.zeros((n, n))
+    ts = []
     for i in range(args.warmup + args.steps):
-        base, err = cpu_reference_sample(rows_sample=args.ref_rows)
-        if base is None:
-            print(json.dumps({"impl": "reference", "unavailable": err}))
-            return 0
+        t0 = time.perf_counter()
+        ref.dgemm("n", "n", n, n, n, 1.0, A, n, B, n, 0.0, C, n)
         if i >= args.warmup:
-            steps.append(base["value"])
-    v = statistics.mean(steps)
-    base["value"] = v
-    line = {"metric": "Ozaki DGEMM TFLOPS n=8192 (INT8 vs FP64 slices, err vs MPFR); DOT/CSRMV GB/s",
-            "impl": "reference", "value": v, "unit": "TFLOPS", "n_gpus": args.gpus, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": 2.0 * args.ref_rows * N_DIM * N_DIM / v / 1e9,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": "ozaki_dgemm m=n=k=8192 phi=1", "m": N_DIM, "n": N_DIM, "k": N_DIM, "phi": PHI,
-                       "sample_rows": args.ref_rows},
+            ts.append(time.perf_counter() - t0)
+    info = ref.info()
+    cores = ref.threads()
+    ref.close()
+    ms = statistics.mean(ts) * 1e3
+    v = 2.0 * n ** 3 / (ms * 1e-3) / 1e12
+    base = {"value": v, "unit": "TFLOPS", "cores": cores, "kind": "reference", "cpu_model": _cpu_model(),
+            "sample": f"reference ozblasRgemm (plain FP64 slices {int(info['nSplitA'])}x{int(info['nSplitB'])}, "
+                      f"sumMode 0), one full m=n=k={n} phi={PHI} call per step, B split included"}
+    line = {"metric": METRIC, "impl": "reference", "value": v, "unit": "TFLOPS", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": f"ozaki_dgemm plain m=n=k={n} phi={PHI} (CPU-bounded size of the 8192^3 "
+                                   "workload)", "m": n, "n": n, "k": n, "phi": PHI},
             "cpu_baseline": base, "e2e": {"value": v, "unit": "TFLOPS", "h2d_bytes_per_step": 0,
                                           "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
@@ -182,7 +241,10 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-extras", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--ref-rows", type=int, default=256)
+    ap.add_argument("--sweep-sizes", default="2048,4096,8192,16384",
+                    help="m = n = k of the INT8 form sweep (comma separated; empty: no sweep)")
+    ap.add_argument("--sweep-phis", default="0.5,1,2,4")
+    ap.add_argument("--sweep-only", action="store_true", help="only the INT8 form sweep (prints its JSON)")
     ap.add_argument("--full-pairs", action="store_true", help="headline with the full pair set instead of triangular")
     ap.add_argument("--n", type=int, default=N_DIM, help="m = n = k (default 8192; smaller for profiling captures)")
     ap.add_argument("--memory-only", action="store_true",
@@ -210,10 +272,15 @@ def main():
     import ozblas_b200 as ozb
 
     torch.cuda.set_device(local)
+    sizes = [int(v) for v in args.sweep_sizes.split(",") if v.strip()]
+    phis = [float(v) for v in args.sweep_phis.split(",") if v.strip()]
+    if args.sweep_only:
+        print(json.dumps({"workload": "INT8 form sweep", "extras": sweep_extras(ozb, torch, sizes, phis)}))
+        return 0
     if args.batched_only:
         h = ozb.Handle(work_bytes=24 << 30)
         print(json.dumps({"workload": "batched uneven Ozaki DGEMM, 256 problems", "reps": args.steps,
-                          "extras": batched_extras(ozb, h, torch, reps=args.steps)}))
+                          "extras": batched_extras(ozb, h, torch, reps=args.steps, cpu=not args.no_cpu)}))
         h.close()
         return 0
     if args.mixed_only:
@@ -226,7 +293,8 @@ def main():
         h = ozb.Handle(work_bytes=8 << 30)
         h.nSplitMax = 0
         print(json.dumps({"workload": "memory-bound plain kernels", "reps": args.steps,
-                          "extras": memory_extras(ozb, h, torch, reps=args.steps, cg_iters=args.cg_iters)}))
+                          "extras": memory_extras(ozb, h, torch, reps=args.steps, cg_iters=args.cg_iters,
+                                                 cpu=not args.no_cpu)}))
         h.close()
         return 0
     dist = None
@@ -315,7 +383,7 @@ def main():
                              "MEASURED_PEAKS.json)",
                 "algorithmic_ops_per_launch": pairs * flops}
 
-    line = {"metric": "Ozaki DGEMM TFLOPS n=8192 (INT8 vs FP64 slices, err vs MPFR); DOT/CSRMV GB/s",
+    line = {"metric": METRIC,
             "value": value, "unit": "TFLOPS", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int8",
             "data": "synthetic",
@@ -325,14 +393,12 @@ def main():
                        "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
             "e2e": e2e, "roofline": roofline, "gpu_launches": launches, "clocks": clk.summary()}
 
+    cpu = rank == 0 and world == 1 and not args.no_cpu
     if rank == 0 and not args.no_extras:
-        line["extras"] = extras(ozb, h, torch, A, B, C, n)
-        line["extras"]["int8_vs_plain_speedup"] = line["extras"]["plain_fp64_slices"]["ms"] / ms
-        line["extras"]["int8_vs_plain_int8_digits_speedup"] = (
-            line["extras"]["plain_fp64_slices_int8_digits"]["ms"] / ms)
-    if rank == 0 and world == 1 and not args.no_cpu:
+        line["extras"] = extras(ozb, h, torch, A, B, C, n, ms, cpu=cpu, sizes=sizes, phis=phis)
+    if cpu:
         try:
-            base, err = cpu_reference_sample(rows_sample=args.ref_rows)
+            base, err = cpu_reference_gemm()
         except Exception as e:  # the baseline must not take the GPU line down
             base, err = None, repr(e)
         line["cpu_baseline"] = base if base else {"value": None, "unavailable": err}
@@ -345,27 +411,169 @@ def main():
     return 0
 
 
-def extras(ozb, h, torch, A, B, C, n):
-    """Plain form, accuracy vs the correctly rounded product, DOT/CSRMV throughput."""
+def timed_ms(torch, fn, reps=1, warm=1):
+    """Minimum CUDA-event time (ms) of `fn` on the current stream over `reps` runs after `warm` untimed runs."""
+    for _ in range(warm):
+        fn()
+    torch.cuda.synchronize()
+    ts = []
+    for _ in range(max(reps, 1)):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        fn()
+        e1.record()
+        torch.cuda.synchronize()
+        ts.append(e0.elapsed_time(e1))
+    return min(ts)
+
+
+def phi_device(torch, rows, cols, phi, seed):
+    """(U - 0.5) * exp(phi * N(0,1)) generated on the GPU (seeded), column-major rows x cols (tensor[j, i] = X(i, j))."""
+    g = torch.Generator(device="cuda").manual_seed(seed)
+    r1 = torch.rand((cols, rows), dtype=torch.float64, device="cuda", generator=g)
+    r2 = torch.rand((cols, rows), dtype=torch.float64, device="cuda", generator=g)
+    r2.mul_(2.0 * 3.141592653589793).sin_()
+    x = torch.log(r1).mul_(-2.0).sqrt_().mul_(r2).mul_(phi).exp_()
+    del r2
+    return x.mul_(r1.sub_(0.5))
+
+
+def exact_errors(orc, Arows, Bcols, blocks):
+    """Checker (exact accumulator of the C restatement): for each name -> computed block (column-major nr x nc,
+    shape (nc, nr)), the max componentwise relative error against the exact product and the number of entries
+    that differ from the correctly rounded value."""
+    import numpy as np
+
+    out = {}
+    for name, Cb in blocks.items():
+        rn, rel = orc.exact_gemm_block(Arows, Bcols, Cb)
+        Cb = np.ascontiguousarray(Cb, dtype=np.float64).reshape(rn.shape)
+        out[name] = {"max_rel_err": float(np.max(rel)) if rel.size else 0.0,
+                     "inexact": int(np.count_nonzero(Cb.view(np.int64) != rn.view(np.int64))), "checked": int(rn.size)}
+    return out
+
+
+def merge_errors(acc, new):
+    for name, e in new.items():
+        a = acc.setdefault(name, {"max_rel_err": 0.0, "inexact": 0, "checked": 0})
+        a["max_rel_err"] = max(a["max_rel_err"], e["max_rel_err"])
+        a["inexact"] += e["inexact"]
+        a["checked"] += e["checked"]
+    return acc
+
+
+def sampled_check(orc, torch, TA, TB, outs, nsamp=64, seed=3, full_lines=False):
+    """Exact-oracle accuracy of n x n products (tensors in column-major layout T[j, i]): a seeded 64 x 64 block of
+    sampled rows and columns (4096 entries), plus, with full_lines, every entry of row 0 and of column 0."""
+    import numpy as np
+
+    from oracle.oracle import Restatement
+
+    orc = orc or Restatement()
+    n = TA.shape[0]
+    g = np.random.default_rng(seed)
+    rows = np.sort(g.choice(n, size=min(nsamp, n), replace=False))
+    cols = np.sort(g.choice(n, size=min(nsamp, n), replace=False))
+    ri, ci = torch.as_tensor(rows, device="cuda"), torch.as_tensor(cols, device="cuda")
+    Arows = TA[:, ri].T.contiguous().cpu().numpy()
+    Bcols = TB[ci, :].contiguous().cpu().numpy()
+    acc = exact_errors(orc, Arows, Bcols, {k: v[ci][:, ri].contiguous().cpu().numpy() for k, v in outs.items()})
+    if full_lines:
+        Ball = TB.cpu().numpy()
+        merge_errors(acc, exact_errors(orc, TA[:, 0:1].T.contiguous().cpu().numpy(), Ball,
+                                       {k: v[:, 0:1].contiguous().cpu().numpy() for k, v in outs.items()}))
+        del Ball
+        Aall = TA.T.contiguous().cpu().numpy()
+        merge_errors(acc, exact_errors(orc, Aall, TB[0:1, :].contiguous().cpu().numpy(),
+                                       {k: v[0:1, :].contiguous().cpu().numpy() for k, v in outs.items()}))
+    return acc
+
+
+def i8_roofline(pairs, n, kernel_ms, peak):
+    achieved = pairs * 2.0 * n ** 3 / (kernel_ms * 1e-3) / 1e12
+    return {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak}
+
+
+def sweep_extras(ozb, torch, sizes, phis, plain_max=8192, dmma_max=4096):
+    """Config 3: the INT8 form at m = n = k in `sizes` x phi in `phis` x {triangular, full} pair sets, each timed
+    through the public API (min of 2 after a warm-up) with its product kernel's time (phase timer), against the
+    plain FP64-slice form (INT8-digit products, and DMMA up to dmma_max) and native FP64 GEMM (cuBLAS DGEMM through
+    torch, a comparison only); accuracy of every form against the exact product (oracle accumulator) on 4096
+    sampled entries, plus full row 0 and column 0 at n <= 4096."""
+    from oracle.oracle import Restatement
+
+    orc = Restatement()
+    peaks, peak_kind = measured_peaks()
+    int8_peak = 2.0 * peaks["bf16_tflops"]
+    rows = []
+    for n in sizes:
+        h = ozb.Handle(work_bytes=(110 << 30) if n > 8192 else (48 << 30))
+        for phi in phis:
+            TA = phi_device(torch, n, n, phi, 1)
+            TB = phi_device(torch, n, n, phi, 2)
+            C = torch.zeros((n, n), dtype=torch.float64, device="cuda")
+            flops = 2.0 * n ** 3
+            outs, rec = {}, {"n": n, "phi": phi}
+            h.sumMode, h.nSplitMax = 0, 0
+            for fast, key in ((1, "int8_triangular"), (0, "int8_full")):
+                h.fastMode = fast
+                kms = []
+
+                def call():
+                    ozb.dgemm_i8(h, "n", "n", n, n, n, 1.0, TA, n, TB, n, 0.0, C, n)
+                    kms.append(h.t_comp * 1e3)
+
+                ms = timed_ms(torch, call, reps=2)
+                kern = min(kms[1:])
+                rec[key] = {"ms": ms, "TFLOPS": flops / ms / 1e9, "kernel_ms": kern, "digits": [h.nSplitA, h.nSplitB],
+                            "pairs": h.nSplitC, "roofline": i8_roofline(h.nSplitC, n, kern, int8_peak)}
+                outs[key] = C.clone()
+            h.fastMode = 0
+            if n <= plain_max:
+                ms = timed_ms(torch, lambda: ozb.dgemm(h, "n", "n", n, n, n, 1.0, TA, n, TB, n, 0.0, C, n), reps=1)
+                rec["plain_int8_digits"] = {"ms": ms, "TFLOPS": flops / ms / 1e9, "slices": [h.nSplitA, h.nSplitB],
+                                            "pairs": h.nSplitC}
+                outs["plain_fsum"] = C.clone()
+            if n <= dmma_max:
+                os.environ["OZBLAS_PLAIN_DMMA"] = "1"
+                h.read_env()
+                try:
+                    ms = timed_ms(torch, lambda: ozb.dgemm(h, "n", "n", n, n, n, 1.0, TA, n, TB, n, 0.0, C, n),
+                                  reps=1)
+                finally:
+                    del os.environ["OZBLAS_PLAIN_DMMA"]
+                    h.read_env()
+                rec["plain_dmma"] = {"ms": ms, "TFLOPS": flops / ms / 1e9,
+                                     "internal_fp64_TFLOPS": h.nSplitC * flops / ms / 1e9,
+                                     "bits_equal_int8_digits": bool(torch.equal(C, outs["plain_fsum"]))}
+            ms = timed_ms(torch, lambda: torch.mm(TB, TA, out=C), reps=2)
+            rec["native_dgemm_cublas"] = {"ms": ms, "TFLOPS": flops / ms / 1e9, "note": "comparison only"}
+            outs["native_dgemm"] = C.clone()
+            del C
+            rec["accuracy_vs_exact"] = sampled_check(orc, torch, TA, TB, outs, full_lines=n <= 4096)
+            if "plain_int8_digits" in rec:
+                rec["int8_triangular_vs_plain_speedup"] = rec["plain_int8_digits"]["ms"] / rec["int8_triangular"]["ms"]
+            if "plain_dmma" in rec:
+                rec["int8_triangular_vs_plain_dmma_speedup"] = rec["plain_dmma"]["ms"] / rec["int8_triangular"]["ms"]
+            rows.append(rec)
+            del TA, TB, outs
+            torch.cuda.empty_cache()
+        h.close()
+    return {"rows": rows, "int8_peak_TOPS": int8_peak, "peak_source": peak_kind,
+            "accuracy_method": "exact accumulator of the C restatement (RN of the exact dot); 64 x 64 sampled "
+                               "entries, plus all of row 0 and column 0 at n <= 4096",
+            "inputs": "(U - 0.5) exp(phi N(0,1)) generated on the GPU, seeds 1 (A) and 2 (B)"}
+
+
+def extras(ozb, h, torch, A, B, C, n, ms_headline, cpu=True, sizes=(), phis=()):
+    """Everything the line reports beside the headline: full pairs at the headline size, the plain form, accuracy
+    against the exact product, configs 1, 2, 4 and 5, the config 3 sweep, and their CPU baselines."""
     out = {}
     flops = 2.0 * n * n * n
 
-    def timed(fn, reps=1):
-        fn()
-        torch.cuda.synchronize()
-        ts = []
-        for _ in range(reps):
-            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            e0.record()
-            fn()
-            e1.record()
-            torch.cuda.synchronize()
-            ts.append(e0.elapsed_time(e1))
-        return min(ts)
-
     C_tri = C.clone()
     h.fastMode = 0
-    ms_full = timed(lambda: ozb.dgemm_i8(h, "n", "n", n, n, n, 1.0, A, n, B, n, 0.0, C, n))
+    ms_full = timed_ms(torch, lambda: ozb.dgemm_i8(h, "n", "n", n, n, n, 1.0, A, n, B, n, 0.0, C, n))
     out["int8_full_pairs"] = {"TFLOPS": flops / ms_full / 1e9, "pairs": h.nSplitC, "ms": ms_full}
     C_full = C.clone()
     h.nSplitMax = 0
@@ -373,7 +581,7 @@ def extras(ozb, h, torch, A, B, C, n):
     os.environ["OZBLAS_PLAIN_DMMA"] = "1"
     h.read_env()
     try:
-        ms_plain = timed(lambda: ozb.dgemm(h, "n", "n", n, n, n, 1.0, A, n, B, n, 0.0, C, n))
+        ms_plain = timed_ms(torch, lambda: ozb.dgemm(h, "n", "n", n, n, n, 1.0, A, n, B, n, 0.0, C, n), warm=0)
     finally:
         del os.environ["OZBLAS_PLAIN_DMMA"]
         h.read_env()
@@ -382,32 +590,66 @@ def extras(ozb, h, torch, A, B, C, n):
                                 "pipe": "FP64 tensor (DMMA)"}
     C_plain = C.clone()
     # the library's default plain path: the same exact slice-pair products on INT8 digits (same bits)
-    ms_plain_i8 = timed(lambda: ozb.dgemm(h, "n", "n", n, n, n, 1.0, A, n, B, n, 0.0, C, n))
+    ms_plain_i8 = timed_ms(torch, lambda: ozb.dgemm(h, "n", "n", n, n, n, 1.0, A, n, B, n, 0.0, C, n))
     out["plain_fp64_slices_int8_digits"] = {"TFLOPS": flops / ms_plain_i8 / 1e9, "ms": ms_plain_i8,
                                             "bit_identical_to_dmma": bool(torch.equal(C, C_plain))}
-    h.sumMode = 1
-    ozb.dgemm(h, "n", "n", n, n, n, 1.0, A, n, B, n, 0.0, C, n)
-    torch.cuda.synchronize()
-    C_rn = C  # correctly rounded product (NearSum over exact slice pairs)
-    h.sumMode = 0
-
-    def maxrel(X):
-        d = (X - C_rn).abs() / C_rn.abs()
-        d = torch.where(C_rn == 0, (X != 0).double() * float("inf"), d)
-        return float(d.max().item()), int((X != C_rn).sum().item())
-
-    e_tri, n_tri = maxrel(C_tri)
-    e_full, n_full = maxrel(C_full)
-    e_plain, n_plain = maxrel(C_plain)
-    out["max_rel_err_vs_correctly_rounded"] = {"int8_triangular": e_tri, "int8_full": e_full, "plain_fsum": e_plain,
-                                               "inexact_entries": {"int8_triangular": n_tri, "int8_full": n_full,
-                                                                   "plain_fsum": n_plain},
-                                               "note": "reference = plain form with NearSum (correctly rounded)"}
+    out["int8_vs_plain_speedup"] = ms_plain / ms_headline
+    out["int8_vs_plain_int8_digits_speedup"] = ms_plain_i8 / ms_headline
+    out["accuracy_vs_exact"] = sampled_check(None, torch, A, B, {"int8_triangular": C_tri, "int8_full": C_full,
+                                                                 "plain_fsum": C_plain})
+    out["accuracy_vs_exact"]["method"] = "exact accumulator of the C restatement on 64 x 64 sampled entries"
     del C_tri, C_full, C_plain
     torch.cuda.empty_cache()
-    out.update(memory_extras(ozb, h, torch))
-    out["batched_uneven_256"] = batched_extras(ozb, h, torch)
+    out["config1_plain_dgemm_1024"] = config1_extras(ozb, torch, cpu=cpu)
+    out.update(memory_extras(ozb, h, torch, cpu=cpu))
+    out["batched_uneven_256"] = batched_extras(ozb, h, torch, cpu=cpu)
+    if sizes:
+        out["config3_int8_sweep"] = sweep_extras(ozb, torch, sizes, phis)
     return out
+
+
+def config1_extras(ozb, torch, cpu=True, n=1024):
+    """Config 1: plain DGEMM 1024^3, phi = 1, FSum, split until exact: time through the public API, and the bits
+    against the reference CPU library on the same host inputs (plus its time, min of 10 after a warm-up)."""
+    import numpy as np
+
+    A_h = phi_matrix(n, n, 1.0, 1)
+    B_h = phi_matrix(n, n, 1.0, 2)
+    A, B = torch.from_numpy(A_h).cuda(), torch.from_numpy(B_h).cuda()
+    C = torch.zeros((n, n), dtype=torch.float64, device="cuda")
+    h = ozb.Handle(work_bytes=8 << 30)
+    h.sumMode, h.nSplitMax, h.fastMode = 0, 0, 0
+    kms = []
+
+    def call():
+        ozb.dgemm(h, "n", "n", n, n, n, 1.0, A, n, B, n, 0.0, C, n)
+        kms.append(h.t_comp * 1e3)
+
+    ms = timed_ms(torch, call, reps=10)
+    pairs, nA, nB = h.nSplitC, h.nSplitA, h.nSplitB
+    h.close()
+    flops = 2.0 * n ** 3
+    peaks, _ = measured_peaks()
+    digits = (53 - int(ozb.rule_rho(n, 0)) + 1 + 6) // 7  # int8 digit planes per FP64 slice
+    kern = min(kms[1:])
+    i8_ops = pairs * digits * digits * flops
+    rec = {"ms": ms, "TFLOPS": flops / ms / 1e9, "slices": [nA, nB], "pairs": pairs,
+           "internal_fp64_TFLOPS": pairs * flops / ms / 1e9, "product_kernel_ms": kern,
+           "roofline": {"bound": "tensor", "unit": "TFLOP/s", "achieved": i8_ops / (kern * 1e-3) / 1e12,
+                        "peak": 2.0 * peaks["bf16_tflops"],
+                        "frac": i8_ops / (kern * 1e-3) / 1e12 / (2.0 * peaks["bf16_tflops"]),
+                        "work": f"pairs x {digits}^2 int8 digit-plane products x 2mnk"}}
+    if cpu:
+        ref = _reference()
+        if ref is None:
+            rec["cpu_baseline"] = {"value": None, "unavailable": "oracle/_ref not built"}
+        else:
+            base, C_ref = cpu_reference_gemm(n=n, reps=10, phi=1.0, ref=ref)
+            ref.close()
+            rec["cpu_baseline"] = base
+            out = C.cpu().numpy()
+            rec["bit_exact_vs_reference"] = bool(np.array_equal(out.view(np.int64), C_ref.view(np.int64)))
+    return rec
 
 
 def batched_case(count=256, seed=5):
@@ -426,9 +668,15 @@ def batched_case(count=256, seed=5):
     return probs
 
 
-def batched_extras(ozb, h, torch, reps=3):
+def batched_extras(ozb, h, torch, reps=3, cpu=True):
     """Config 5: 256 uneven problems in one grouped INT8 launch vs the same problems looped through the single INT8
-    call and through the plain FP64-slice form; max relative error against the correctly rounded product."""
+    call and through the plain FP64-slice form; accuracy of the grouped results and of the plain FSum against the
+    exact product (oracle accumulator, 16 x 16 sampled entries per problem); with cpu, the reference CPU library
+    looped over problems 0..15."""
+    import numpy as np
+
+    from oracle.oracle import Restatement
+
     probs = batched_case()
     flops = sum(2.0 * m * n * k for m, n, k, _, _, _ in probs)
     As = [torch.from_numpy(A).cuda() for *_, A, _ in probs]
@@ -437,24 +685,18 @@ def batched_extras(ozb, h, torch, reps=3):
     ms, ns, ks = [p[0] for p in probs], [p[1] for p in probs], [p[2] for p in probs]
     one, zero = [1.0] * len(probs), [0.0] * len(probs)
 
-    def timed(fn, reps):
-        fn()
-        torch.cuda.synchronize()
-        ts = []
-        for _ in range(reps):
-            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            e0.record()
-            fn()
-            e1.record()
-            torch.cuda.synchronize()
-            ts.append(e0.elapsed_time(e1))
-        return min(ts)
-
     out = {"problems": len(probs), "flops_effective": flops}
+    peaks, _ = measured_peaks()
     for fast in (0, 1):
         h.nSplitMax, h.fastMode = 0, fast
         l0 = h.launch_count()
-        ms_b = timed(lambda: ozb.dgemm_i8_batched(h, "n", "n", ms, ns, ks, one, As, ms, Bs, ks, zero, Cs, ms), reps)
+        kms = []
+
+        def grouped():
+            ozb.dgemm_i8_batched(h, "n", "n", ms, ns, ks, one, As, ms, Bs, ks, zero, Cs, ms)
+            kms.append(h.t_comp * 1e3)
+
+        ms_b = timed_ms(torch, grouped, reps)
         launches = (h.launch_count() - l0) / (reps + 1)
         slices = [h.nSplitA, h.nSplitB]
         C_batched = [c.clone() for c in Cs]
@@ -463,10 +705,10 @@ def batched_extras(ozb, h, torch, reps=3):
             for i in range(len(probs)):
                 ozb.dgemm_i8(h, "n", "n", ms[i], ns[i], ks[i], 1.0, As[i], ms[i], Bs[i], ks[i], 0.0, Cs[i], ms[i])
 
-        ms_l = timed(looped, 1)
+        ms_l = timed_ms(torch, looped, 1)
         key = "full" if fast == 0 else "triangular"
         out[f"int8_grouped_{key}"] = {"ms": ms_b, "TFLOPS": flops / ms_b / 1e9, "launches": launches,
-                                      "max_slices": slices}
+                                      "max_slices": slices, "product_kernel_ms": min(kms[1:])}
         out[f"int8_looped_{key}"] = {"ms": ms_l, "TFLOPS": flops / ms_l / 1e9}
         out[f"grouped_identical_to_looped_{key}"] = all(bool(torch.equal(a, b)) for a, b in zip(C_batched, Cs))
         if fast == 0:
@@ -477,33 +719,42 @@ def batched_extras(ozb, h, torch, reps=3):
         for i in range(len(probs)):
             ozb.dgemm(h, "n", "n", ms[i], ns[i], ks[i], 1.0, As[i], ms[i], Bs[i], ks[i], 0.0, Cs[i], ms[i])
 
-    ms_p = timed(plain, 1)
+    ms_p = timed_ms(torch, plain, 1)
     out["plain_fp64_slices_looped"] = {"ms": ms_p, "TFLOPS": flops / ms_p / 1e9}
     C_fsum = [c.clone() for c in Cs]
-    h.sumMode = 1
-    plain()  # correctly rounded products
-    torch.cuda.synchronize()
-    h.sumMode = 0
-
-    def worst(X):
-        w, cnt, where = 0.0, 0, None
-        for i, (a, b) in enumerate(zip(X, Cs)):
-            d = ((a - b).abs() / b.abs()).nan_to_num(nan=0.0, posinf=float("inf"))
-            d = torch.where(b == 0, (a != 0).double() * float("inf"), d)
-            di = float(d.max().item())
-            if di > w:
-                j = int(d.argmax().item())
-                w, where = di, {"problem": i, "m": ms[i], "n": ns[i], "k": ks[i], "phi": probs[i][3],
-                                "value": float(a.flatten()[j].item()), "correctly_rounded": float(b.flatten()[j].item())}
-            cnt += int((a != b).sum().item())
-        return w, cnt, where
-
-    (e_i8, n_i8, w_i8), (e_fs, n_fs, w_fs) = worst(C_full), worst(C_fsum)
-    out["max_rel_err_vs_correctly_rounded"] = {"int8_full": e_i8, "plain_fsum": e_fs,
-                                               "inexact_entries": {"int8_full": n_i8, "plain_fsum": n_fs},
-                                               "entries": sum(m * n for m, n, *_ in probs),
-                                               "worst_int8": w_i8, "worst_fsum": w_fs}
+    # checker: 16 x 16 sampled entries per problem against the exact product
+    orc = Restatement()
+    acc = {}
+    g = np.random.default_rng(9)
+    for i, (m, n, k, _, A_h, B_h) in enumerate(probs):
+        rows = np.sort(g.choice(m, size=min(16, m), replace=False))
+        cols = np.sort(g.choice(n, size=min(16, n), replace=False))
+        Arows = np.ascontiguousarray(A_h[:, rows].T)
+        Bcols = np.ascontiguousarray(B_h[cols, :])
+        ri, ci = torch.as_tensor(rows, device="cuda"), torch.as_tensor(cols, device="cuda")
+        blocks = {name: X[i][ci][:, ri].contiguous().cpu().numpy()
+                  for name, X in (("int8_grouped_full", C_full), ("plain_fsum", C_fsum))}
+        merge_errors(acc, exact_errors(orc, Arows, Bcols, blocks))
+    acc["method"] = "exact accumulator of the C restatement, 16 x 16 sampled entries per problem"
+    out["accuracy_vs_exact"] = acc
     out["speedup_grouped_full_vs_plain_looped"] = ms_p / out["int8_grouped_full"]["ms"]
+    if cpu:
+        ref = _reference()
+        if ref is not None:
+            ref.set_flags(sumMode=0, fastMode=0, nSplitMax=0, reproMode=1)
+            t, fl = 0.0, 0.0
+            for m, n, k, _, A_h, B_h in probs[:16]:
+                Cz = np.zeros((n, m))
+                ref.dgemm("n", "n", m, n, k, 1.0, A_h, m, B_h, k, 0.0, Cz, m)  # warm-up
+                t0 = time.perf_counter()
+                ref.dgemm("n", "n", m, n, k, 1.0, A_h, m, B_h, k, 0.0, Cz, m)
+                t += time.perf_counter() - t0
+                fl += 2.0 * m * n * k
+            out["cpu_baseline"] = {"value": fl / t / 1e12, "unit": "TFLOPS", "cores": ref.threads(),
+                                   "kind": "reference", "cpu_model": _cpu_model(),
+                                   "sample": f"reference ozblasRgemm (plain, sumMode 0) looped over problems 0..15 "
+                                             f"({fl / 1e9:.1f} GFLOP effective, {t:.2f} s, each after a warm-up)"}
+            ref.close()
     return out
 
 
@@ -589,124 +840,186 @@ def mixed_extras(ozb, h, torch, n, reps=3):
     return out
 
 
-def memory_extras(ozb, h, torch, reps=3, cg_iters=2000):
-    """DOT n = 2^24 (phi = 2), GEMV 8192^2 (phi = 1), CSRMV on the 128^3 7-point stencil (both sum modes) and CG
-    on 100^3, through the public API."""
+def stencil7(g3):
+    """7-point stencil CSR on a g3^3 grid, natural order, sorted columns (32-bit): (rowptr, colind)."""
+    import numpy as np
+
+    m = g3 ** 3
+    idx = np.arange(m, dtype=np.int64)
+    xi, yi, zi = idx % g3, (idx // g3) % g3, idx // (g3 * g3)
+    offs = [(-g3 * g3, zi > 0), (-g3, yi > 0), (-1, xi > 0), (0, np.ones(m, bool)), (1, xi < g3 - 1),
+            (g3, yi < g3 - 1), (g3 * g3, zi < g3 - 1)]
+    C7 = np.stack([idx + o for o, _ in offs], 1)
+    M7 = np.stack([k for _, k in offs], 1)
+    colind = C7[M7].astype(np.int32)
+    rowptr = np.zeros(m + 1, dtype=np.int64)
+    rowptr[1:] = np.cumsum(M7.sum(1))
+    return rowptr.astype(np.int32), colind, M7
+
+
+def hbm_roofline(nbytes, ms, traffic=None, what="whole call"):
+    peaks, kind = measured_peaks()
+    achieved = nbytes / (ms * 1e-3) / 1e9
+    return {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
+            "frac": achieved / peaks["hbm_gbs"], "traffic": traffic, "timed": what, "peak_source": kind,
+            "algorithmic_bytes": nbytes}
+
+
+def ncu_traffic(key):
+    tp = os.path.join(ROOT, "profiles", "ncu_traffic.json")
+    if os.path.exists(tp):
+        with open(tp) as f:
+            return json.load(f).get(key)
+    return None
+
+
+def cpu_mean(fn, reps):
+    """Mean wall time (s) of `fn` over `reps` calls after one warm-up call, and the last result."""
+    r = fn()
+    ts = []
+    for _ in range(reps):
+        t0 = time.perf_counter()
+        r = fn()
+        ts.append(time.perf_counter() - t0)
+    return statistics.mean(ts), r
+
+
+def memory_extras(ozb, h, torch, reps=3, cg_iters=2000, cpu=True):
+    """Config 2 (DOT / NRM2 n = 2^24 phi = 2, GEMV 8192^2 phi = 1, CSRMV on the 128^3 7-point stencil, both sum
+    modes) and config 4 (CG on 100^3, 2000 iterations), through the public API on host-generated inputs.  Each
+    carries its HBM roofline (algorithmic bytes over the call's CUDA-event time) and, with cpu, the reference CPU
+    library's time on the same inputs (mean of `cpu reps` calls after a warm-up) and whether the bits agree."""
     import numpy as np
 
     out = {}
+    ref = _reference() if cpu else None
 
-    def timed(fn, reps=1):
-        fn()
-        torch.cuda.synchronize()
-        ts = []
-        for _ in range(reps):
-            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            e0.record()
-            fn()
-            e1.record()
-            torch.cuda.synchronize()
-            ts.append(e0.elapsed_time(e1))
-        return min(ts)
+    def cpu_leg(rec, name, fn, nbytes, reps_cpu, gpu_value):
+        if ref is None:
+            return
+        t, r = cpu_mean(fn, reps_cpu)
+        rec["cpu_baseline"] = {"value": nbytes / t / 1e9, "unit": "GB/s", "ms": t * 1e3, "cores": ref.threads(),
+                               "kind": "reference", "cpu_model": _cpu_model(),
+                               "sample": f"reference {name} on the same inputs, mean of {reps_cpu} after 1 warm-up"}
+        a, b = np.asarray(gpu_value, dtype=np.float64), np.asarray(r, dtype=np.float64)
+        rec["bit_exact_vs_reference"] = bool(np.array_equal(a.view(np.int64), b.view(np.int64)))
 
-    # DOT n = 2^24, phi = 2
+    # DOT / NRM2, n = 2^24, phi = 2 (seeds 1, 2)
     nv = 1 << 24
-    g = torch.Generator(device="cuda").manual_seed(7)
-    r1 = torch.rand(nv, dtype=torch.float64, device="cuda", generator=g)
-    r2 = torch.rand(nv, dtype=torch.float64, device="cuda", generator=g)
-    x = (r1 - 0.5) * torch.exp(2.0 * torch.sqrt(-2 * torch.log(r1)) * torch.sin(2 * torch.pi * r2))
-    r1 = torch.rand(nv, dtype=torch.float64, device="cuda", generator=g)
-    y = (r1 - 0.5) * torch.exp(2.0 * torch.sqrt(-2 * torch.log(r1)) * torch.sin(2 * torch.pi * r2))
+    x_h = phi_matrix(nv, 1, 2.0, 1).ravel()
+    y_h = phi_matrix(nv, 1, 2.0, 2).ravel()
+    x, y = torch.from_numpy(x_h).cuda(), torch.from_numpy(y_h).cuda()
     for sm in (0, 1):
         h.sumMode = sm
-        ms = timed(lambda: ozb.ddot(h, nv, x, y), reps=reps)
-        out[f"ddot_2p24_sum{sm}"] = {"GBps": 16.0 * nv / ms / 1e6, "ms": ms, "slices": [h.nSplitA, h.nSplitB]}
-    del x, y, r1, r2
-    # GEMV 8192^2 (phi = 1), y = A x, beta = 0: algorithmic bytes 8 (mn + n + m)
+        if ref is not None:
+            ref.set_flags(sumMode=sm)
+        res = []
+        ms = timed_ms(torch, lambda: res.append(ozb.ddot(h, nv, x, y)), reps=reps)
+        nb = 16.0 * nv
+        rec = {"GBps": nb / ms / 1e6, "ms": ms, "slices": [h.nSplitA, h.nSplitB],
+               "roofline": hbm_roofline(nb, ms, ncu_traffic(f"ddot_2p24_sum{sm}"))}
+        cpu_leg(rec, "ozblasRdot", lambda: ref.ddot(x_h, y_h), nb, 10, res[-1])
+        out[f"ddot_2p24_sum{sm}"] = rec
+        res = []
+        ms = timed_ms(torch, lambda: res.append(ozb.dnrm2(h, nv, x)), reps=reps)
+        nb = 8.0 * nv
+        rec = {"GBps": nb / ms / 1e6, "ms": ms, "slices": [h.nSplitA, h.nSplitB],
+               "roofline": hbm_roofline(nb, ms, ncu_traffic(f"dnrm2_2p24_sum{sm}"))}
+        cpu_leg(rec, "ozblasRnrm2", lambda: ref.dnrm2(x_h), nb, 10, res[-1])
+        out[f"dnrm2_2p24_sum{sm}"] = rec
+    del x, y, x_h, y_h
+    # GEMV 8192^2, phi = 1, y = A x, beta = 0 (seeds 1, 2): algorithmic bytes 8 (mn + n + m)
     mg = 8192
-    r1 = torch.rand(mg * mg, dtype=torch.float64, device="cuda", generator=g)
-    r2 = torch.rand(mg * mg, dtype=torch.float64, device="cuda", generator=g)
-    Ag = (r1 - 0.5) * torch.exp(torch.sqrt(-2 * torch.log(r1)) * torch.sin(2 * torch.pi * r2))
-    del r1, r2
-    r1 = torch.rand(mg, dtype=torch.float64, device="cuda", generator=g)
-    xg = (r1 - 0.5) * torch.exp(torch.sqrt(-2 * torch.log(r1)))
+    A_h = phi_matrix(mg, mg, 1.0, 1)
+    xg_h = phi_matrix(mg, 1, 1.0, 2).ravel()
+    Ag, xg = torch.from_numpy(A_h).cuda(), torch.from_numpy(xg_h).cuda()
     yg = torch.zeros(mg, dtype=torch.float64, device="cuda")
     for sm in (0, 1):
         h.sumMode = sm
-        ms = timed(lambda: ozb.dgemv(h, "n", mg, mg, 1.0, Ag, mg, xg, 0.0, yg), reps=reps)
-        out[f"dgemv_8192_sum{sm}"] = {"GBps": 8.0 * (mg * mg + 2 * mg) / ms / 1e6, "ms": ms,
-                                      "slices": [h.nSplitA, h.nSplitB]}
-    del Ag, xg, yg, r1
+        if ref is not None:
+            ref.set_flags(sumMode=sm)
+        ms = timed_ms(torch, lambda: ozb.dgemv(h, "n", mg, mg, 1.0, Ag, mg, xg, 0.0, yg), reps=reps)
+        nb = 8.0 * (mg * mg + 2 * mg)
+        rec = {"GBps": nb / ms / 1e6, "ms": ms, "slices": [h.nSplitA, h.nSplitB],
+               "roofline": hbm_roofline(nb, ms, ncu_traffic(f"dgemv_8192_sum{sm}"))}
+        cpu_leg(rec, "ozblasRgemv", lambda: ref.dgemv("n", mg, mg, 1.0, A_h, mg, xg_h, 0.0, np.zeros(mg)), nb, 3,
+                yg.cpu().numpy())
+        out[f"dgemv_8192_sum{sm}"] = rec
+    del Ag, xg, yg, A_h
     torch.cuda.empty_cache()
-    # CSRMV: 7-point stencil on 128^3, values and x (U - 0.5) exp(N(0,1)), beta = 0
-    g3 = 128
-    m = g3 ** 3
-    idx = torch.arange(m, device="cuda", dtype=torch.int64)
-    xi, yi, zi = idx % g3, (idx // g3) % g3, idx // (g3 * g3)
-    offs = [(-g3 * g3, zi > 0), (-g3, yi > 0), (-1, xi > 0), (0, None), (1, xi < g3 - 1), (g3, yi < g3 - 1),
-            (g3 * g3, zi < g3 - 1)]
-    cols, masks = [], []
-    for o, msk in offs:
-        cols.append(idx + o)
-        masks.append(torch.ones(m, dtype=torch.bool, device="cuda") if msk is None else msk)
-    C7 = torch.stack(cols, 1)
-    M7 = torch.stack(masks, 1)
-    colind = C7[M7].to(torch.int32).contiguous()
-    rowptr = torch.zeros(m + 1, dtype=torch.int64, device="cuda")
-    rowptr[1:] = torch.cumsum(M7.sum(1), 0)
-    rowptr = rowptr.to(torch.int32).contiguous()
-    nnz = colind.numel()
-    r1 = torch.rand(nnz, dtype=torch.float64, device="cuda", generator=g)
-    r2 = torch.rand(nnz, dtype=torch.float64, device="cuda", generator=g)
-    val = (r1 - 0.5) * torch.exp(torch.sqrt(-2 * torch.log(r1)) * torch.sin(2 * torch.pi * r2))
-    r1 = torch.rand(m, dtype=torch.float64, device="cuda", generator=g)
-    r2 = torch.rand(m, dtype=torch.float64, device="cuda", generator=g)
-    xv = (r1 - 0.5) * torch.exp(torch.sqrt(-2 * torch.log(r1)) * torch.sin(2 * torch.pi * r2))
+    # CSRMV: 7-point stencil on 128^3, values phi = 1 (seed 3), x phi = 1 (seed 4), beta = 0
+    rp_h, ci_h, _ = stencil7(128)
+    m = len(rp_h) - 1
+    nnz = len(ci_h)
+    val_h = phi_matrix(nnz, 1, 1.0, 3).ravel()
+    xv_h = phi_matrix(m, 1, 1.0, 4).ravel()
+    val, colind, rowptr = (torch.from_numpy(a).cuda() for a in (val_h, ci_h, rp_h))
+    xv = torch.from_numpy(xv_h).cuda()
     yv = torch.zeros(m, dtype=torch.float64, device="cuda")
     nbytes = 12.0 * nnz + 4.0 * (m + 1) + 8.0 * m + 8.0 * m
     for sm in (0, 1):
         h.sumMode = sm
-        ms = timed(lambda: ozb.dcsrmv(h, "n", m, m, nnz, 1.0, val, colind, rowptr, xv, 0.0, yv), reps=reps)
-        out[f"dcsrmv_stencil128_sum{sm}"] = {"GBps": nbytes / ms / 1e6, "ms": ms, "nnz": nnz,
-                                             "slices": [h.nSplitA, h.nSplitB]}
-    # CG: 7-point Poisson on 100^3 plus 0.01 U(0,1) on the diagonal, b = A x_true,
-    # 2000 iterations (tol 0), NearSum, history every iteration (verbose = 1)
-    del val, colind, rowptr, xv, yv, C7, M7, cols, masks, idx, xi, yi, zi
+        if ref is not None:
+            ref.set_flags(sumMode=sm)
+        ms = timed_ms(torch, lambda: ozb.dcsrmv(h, "n", m, m, nnz, 1.0, val, colind, rowptr, xv, 0.0, yv), reps=reps)
+        rec = {"GBps": nbytes / ms / 1e6, "ms": ms, "nnz": nnz, "slices": [h.nSplitA, h.nSplitB],
+               "roofline": hbm_roofline(nbytes, ms, ncu_traffic(f"dcsrmv_stencil128_sum{sm}"))}
+        cpu_leg(rec, "ozblasRcsrmv", lambda: ref.dcsrmv(m, m, 1.0, val_h, ci_h, rp_h, xv_h, 0.0, np.zeros(m)),
+                nbytes, 3, yv.cpu().numpy())
+        out[f"dcsrmv_stencil128_sum{sm}"] = rec
+    del val, colind, rowptr, xv, yv, val_h, xv_h
     torch.cuda.empty_cache()
+    # CG: 7-point Poisson on 100^3 plus 0.01 U(0,1) on the diagonal (seed 5), b = A x_true (x_true ~ N(0,1),
+    # seed 6, row sums on the host), x0 = 0, NearSum, tol = 0, history every iteration (verbose = 1)
     g3 = 100
-    m = g3 ** 3
-    idx = torch.arange(m, device="cuda", dtype=torch.int64)
-    xi, yi, zi = idx % g3, (idx // g3) % g3, idx // (g3 * g3)
-    offs = [(-g3 * g3, zi > 0), (-g3, yi > 0), (-1, xi > 0), (0, None), (1, xi < g3 - 1), (g3, yi < g3 - 1),
-            (g3 * g3, zi < g3 - 1)]
-    C7 = torch.stack([idx + o for o, _ in offs], 1)
-    M7 = torch.stack([torch.ones(m, dtype=torch.bool, device="cuda") if k is None else k for _, k in offs], 1)
-    V7 = torch.full((m, 7), -1.0, dtype=torch.float64, device="cuda")
-    V7[:, 3] = 6.0 + 0.01 * torch.rand(m, dtype=torch.float64, device="cuda", generator=g)
-    colind = C7[M7].to(torch.int32).contiguous()
-    val = V7[M7].contiguous()
-    rowptr = torch.zeros(m + 1, dtype=torch.int64, device="cuda")
-    rowptr[1:] = torch.cumsum(M7.sum(1), 0)
-    rowptr = rowptr.to(torch.int32).contiguous()
-    nnz = colind.numel()
-    xt = torch.randn(m, dtype=torch.float64, device="cuda", generator=g)
-    b = (torch.where(M7, V7 * xt[C7.clamp(0, m - 1)], torch.zeros_like(V7))).sum(1).contiguous()
+    rp_h, ci_h, M7 = stencil7(g3)
+    m = len(rp_h) - 1
+    V7 = np.full((m, 7), -1.0)
+    V7[:, 3] = 6.0 + 0.01 * np.random.default_rng(5).random(m)
+    val_h = V7[M7]
+    xt = np.random.default_rng(6).standard_normal(m)
+    b_h = np.zeros(m)
+    rows_of = np.repeat(np.arange(m), np.diff(rp_h))
+    np.add.at(b_h, rows_of, val_h * xt[ci_h])
+    nnz = len(ci_h)
+    val, colind, rowptr, b = (torch.from_numpy(a).cuda() for a in (val_h, ci_h, rp_h, b_h))
     xs = torch.zeros(m, dtype=torch.float64, device="cuda")
     iters = cg_iters
     h1 = np.zeros(iters + 1)
     h2 = np.zeros(iters + 1)
     h.sumMode, h.verbose = 1, 1
-    ms = timed(lambda: (xs.zero_(), ozb.dcg(h, "n", m, nnz, val, colind, rowptr, b, xs, iters, 0.0, h1, h2)),
-               reps=min(reps, 2))
+    ms = timed_ms(torch, lambda: (xs.zero_(), ozb.dcg(h, "n", m, nnz, val, colind, rowptr, b, xs, iters, 0.0, h1, h2)),
+                  reps=min(reps, 2))
     l0 = h.launch_count()
     xs.zero_()
     ozb.dcg(h, "n", m, nnz, val, colind, rowptr, b, xs, iters, 0.0, h1, h2)
     per_iter_bytes = 12.0 * nnz + 4.0 * (m + 1) + 116.0 * m
-    out[f"dcg_100cube_{iters}it"] = {"ms": ms, "ms_per_iter": ms / iters, "GBps": per_iter_bytes * iters / ms / 1e6,
-                                 "iterations": h.cg_numiter, "nnz": nnz, "final_rel_res": float(h1[iters]),
-                                 "launches_per_iter": (h.launch_count() - l0) / iters,
-                                 "bytes_per_iter": per_iter_bytes}
+    rec = {"ms": ms, "ms_per_iter": ms / iters, "GBps": per_iter_bytes * iters / ms / 1e6,
+           "iterations": h.cg_numiter, "nnz": nnz, "final_rel_res": float(h1[iters]),
+           "launches_per_iter": (h.launch_count() - l0) / iters, "bytes_per_iter": per_iter_bytes,
+           "roofline": hbm_roofline(per_iter_bytes * iters, ms, None, "whole solve (2000 iterations)")}
+    if ref is not None:
+        # bounded sample: the reference CG at 10 and 20 iterations (same flags); per iteration = the difference
+        ref.set_flags(sumMode=1, verbose=1)
+        t0 = time.perf_counter()
+        _, hist10 = ref.dcg(val_h, ci_h, rp_h, b_h, np.zeros(m), 10, 0.0)
+        t10 = time.perf_counter() - t0
+        t0 = time.perf_counter()
+        ref.dcg(val_h, ci_h, rp_h, b_h, np.zeros(m), 20, 0.0)
+        t20 = time.perf_counter() - t0
+        per = max(t20 - t10, 1e-9) / 10
+        rec["cpu_baseline"] = {"value": per_iter_bytes / per / 1e9, "unit": "GB/s", "ms_per_iter": per * 1e3,
+                               "cores": ref.threads(), "kind": "reference", "cpu_model": _cpu_model(),
+                               "sample": f"reference ozblasRcg (NearSum, verbose 1) at 10 and 20 iterations "
+                                         f"({t10:.2f} s, {t20:.2f} s, SplitA included in both); per iteration = "
+                                         "the difference / 10"}
+        g = h1[: len(hist10)]
+        rec["history_first_10_bit_exact_vs_reference"] = bool(
+            np.array_equal(np.asarray(g).view(np.int64), np.asarray(hist10, dtype=np.float64).view(np.int64)))
+    out[f"dcg_100cube_{iters}it"] = rec
     h.sumMode, h.verbose = 0, 0
+    if ref is not None:
+        ref.close()
     return out
 
 

@@ -152,6 +152,8 @@ class Restatement:
         L.oz_exact_dot_err.argtypes = [C.c_int, _dp, C.c_int, _dp, C.c_int, C.c_double, _dp, _dp]
         L.oz_exact_sum_rn.restype = C.c_double
         L.oz_exact_sum_rn.argtypes = [C.c_int, _dp]
+        L.oz_exact_gemm_block.restype = None
+        L.oz_exact_gemm_block.argtypes = [C.c_int, C.c_int, _dp, C.c_int, _dp, _dp, _dp, _dp]
         L.oz_gen_phi.restype = None
         L.oz_gen_phi.argtypes = [C.c_int, C.c_int, C.c_int, _dp, C.c_double, C.c_int]
         L.oz_gen_normal.restype = None
@@ -408,6 +410,20 @@ class Restatement:
         rel = C.c_double()
         self.L.oz_exact_dot_err(n, _d(x), incx, _d(y), incy, c, C.byref(rn), C.byref(rel))
         return rn.value, rel.value
+
+    def exact_gemm_block(self, Arows, Bcols, Cblk):
+        """RN(exact) and the relative error of every computed entry of a GEMM block: Arows (nr x k, row i of op(A)),
+        Bcols (nc x k, column j of op(B)), Cblk (nc x nr: column-major nr x nc block of computed values)."""
+        Arows = np.ascontiguousarray(Arows, dtype=np.float64)
+        Bcols = np.ascontiguousarray(Bcols, dtype=np.float64)
+        Cblk = np.ascontiguousarray(Cblk, dtype=np.float64)
+        nr, k = Arows.shape
+        nc = Bcols.shape[0]
+        assert Bcols.shape[1] == k and Cblk.size == nr * nc
+        rn = np.zeros(nr * nc)
+        rel = np.zeros(nr * nc)
+        self.L.oz_exact_gemm_block(k, nr, _d(Arows), nc, _d(Bcols), _d(Cblk), _d(rn), _d(rel))
+        return rn.reshape(nc, nr), rel.reshape(nc, nr)
 
     def exact_sum(self, v):
         v = np.ascontiguousarray(v, dtype=np.float64)

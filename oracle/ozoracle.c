@@ -1353,6 +1353,21 @@ void oz_exact_dot_err(int n, const double *x, int incx, const double *y, int inc
     free(a);
 }
 
+/* Exact check of a block of GEMM entries: entry (i, j) of the nr x nc block is
+ * row i of op(A) (k contiguous values at Arows + i * k) times column j of op(B)
+ * (k values at Bcols + j * k).  Cblk holds the computed values (column-major,
+ * nr x nc); rn receives RN(exact) and relerr |c - exact| / |exact| per entry
+ * (0 when both are 0, inf when only the exact value is 0).  Parallel over
+ * entries (OpenMP); each entry is one exact accumulation. */
+void oz_exact_gemm_block(int k, int nr, const double *Arows, int nc, const double *Bcols, const double *Cblk,
+                         double *rn, double *relerr) {
+#pragma omp parallel for schedule(dynamic, 4)
+    for (int e = 0; e < nr * nc; e++) {
+        const int i = e % nr, j = e / nr;
+        oz_exact_dot_err(k, Arows + (size_t)i * k, 1, Bcols + (size_t)j * k, 1, Cblk[e], &rn[e], &relerr[e]);
+    }
+}
+
 double oz_exact_sum_rn(int n, const double *v) {
     acc_t *a = (acc_t *)malloc(sizeof(acc_t));
     acc_init(a);

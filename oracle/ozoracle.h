@@ -97,6 +97,8 @@ int oz_dcg(const oz_flags *f, int n, int nnz, const double *val, const int *coli
 double oz_exact_dot_rn(int n, const double *x, int incx, const double *y, int incy);
 void oz_exact_dot_err(int n, const double *x, int incx, const double *y, int incy, double c, double *rn,
                       double *relerr_exact);
+void oz_exact_gemm_block(int k, int nr, const double *Arows, int nc, const double *Bcols, const double *Cblk,
+                         double *rn, double *relerr);
 double oz_exact_sum_rn(int n, const double *v);
 
 /* ---- seeded inputs ---- */
