@@ -82,6 +82,7 @@ _destroy = _sig("cuozblasHandleDestroy", [_HP])
 _setstream = _sig("cuozblasSetStream", [_HP, _vp])
 _launches = _sig("cuozblasGetLaunchCount", [_HP, C.POINTER(C.c_uint64)])
 _readenv = _sig("cuozblasHandleReadEnv", [_HP])
+_i8_wait = _sig("cuozblasSetI8WaitLimit", [C.c_uint64])
 _ddot = _sig("cuozblasDdot", [_HP, _i32, _vp, _i32, _vp, _i32, C.POINTER(_d)])
 _dnrm2 = _sig("cuozblasDnrm2", [_HP, _i32, _vp, _i32, C.POINTER(_d)])
 _daxpy = _sig("cuozblasDaxpy", [_HP, _i32, _d, _vp, _i32, _vp, _i32])
@@ -118,7 +119,7 @@ _version = _sig("cuozblasVersion", [], C.c_char_p)
 #: every C-ABI symbol include/cuozblas.h declares (checked by the CPU tests)
 C_ABI_SYMBOLS = [
     "cuozblasHandleCreate", "cuozblasHandleDestroy", "cuozblasSetStream", "cuozblasGetLaunchCount",
-    "cuozblasHandleReadEnv", "cuozblasDdot", "cuozblasDnrm2",
+    "cuozblasHandleReadEnv", "cuozblasSetI8WaitLimit", "cuozblasDdot", "cuozblasDnrm2",
     "cuozblasDaxpy", "cuozblasDgemv", "cuozblasDgemm", "cuozblasDcsrmv", "cuozblasDcsrmvSplitA", "cuozblasDcg",
     "cuozblasDgemmI8", "cuozblasDgemmI8Static", "cuozblasDgemmI8Batched", "cuozblasRuleTau", "cuozblasRuleRho",
     "cuozblasRuleCrSum", "cuozblasDSgemm", "cuozblasDSgemv", "cuozblasDSdot", "cuozblasDSnrm2",
@@ -274,6 +275,11 @@ def qnrm2(h, n, x, incx=1):
     r = (C.c_uint64 * 2)()
     _chk("cuozblasQnrm2", _qnrm2(h.ref, n, _ptr(x), incx, C.cast(r, _vp)))
     return (r[0], r[1])
+
+
+def set_i8_wait_limit(ns: int):
+    """Testing hook: the bounded-wait limit of the INT8 product kernel on the current device (0: default 2 s)."""
+    _chk("cuozblasSetI8WaitLimit", _i8_wait(int(ns)))
 
 
 def dgemm_i8(h, ta, tb, m, n, k, alpha, A, lda, B, ldb, beta, Cm, ldc):

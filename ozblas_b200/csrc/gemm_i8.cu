@@ -57,6 +57,11 @@ constexpr uint64_t I8_WAIT_NS = 2000000000ull;                  // 2 s per wait
 
 enum { ERR_TIMEOUT_PRODUCER = 1, ERR_TIMEOUT_MMA = 2, ERR_TIMEOUT_EPI = 3 };
 
+// Limit of every bounded mbarrier wait in the INT8 product kernels (k_i8_gemm,
+// k_i8_grouped); cuozblasSetI8WaitLimit changes it (tests shorten it to make a
+// wait run out).
+__device__ uint64_t g_i8_wait_ns = I8_WAIT_NS;
+
 struct I8Params {
     int m, n, m_pad, n_pad, ldc;
     int tiles_m, tiles_n, n_items, n_groups;
@@ -109,6 +114,7 @@ __global__ void __launch_bounds__(I8_THREADS, 1)
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int ntiles = p.tiles_m * p.tiles_n;
+    const uint64_t wait_ns = g_i8_wait_ns;
 
     if (threadIdx.x == 0) {
         for (int s = 0; s < I8_NST; s++) {
@@ -135,6 +141,7 @@ __global__ void __launch_bounds__(I8_THREADS, 1)
         // ------------------------------------------------------------ producer
         if (lane == 0) {
             uint32_t stage = 0, phase = 0;
+            uint32_t issued = 0, issued_phase = 0;  // per stage: a copy was issued, and the phase it completes
             bool ok = true;
             for (int tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x) {
                 int tm, tn;
@@ -143,7 +150,7 @@ __global__ void __launch_bounds__(I8_THREADS, 1)
                     const int4 item = p.items[it];
                     for (int kb = item.z; kb < item.w; kb++) {
                         if (!tc::mbar_wait(&empty[stage], phase ^ 1, &abort_flag, p.err, ERR_TIMEOUT_PRODUCER,
-                                           I8_WAIT_NS)) {
+                                           wait_ns)) {
                             ok = false;
                             break;
                         }
@@ -151,6 +158,8 @@ __global__ void __launch_bounds__(I8_THREADS, 1)
                         tc::mbar_arrive_expect_tx(&full[stage], I8_STAGE);
                         tc::tma_load_2d(sa, &tmA, &full[stage], kb * I8_BK, item.x * p.m_pad + tm * I8_BM);
                         tc::tma_load_2d(sb, &tmB, &full[stage], kb * I8_BK, item.y * p.n_pad + tn * I8_BN);
+                        issued |= 1u << stage;
+                        issued_phase = (issued_phase & ~(1u << stage)) | (phase << stage);
                         if (++stage == I8_NST) {
                             stage = 0;
                             phase ^= 1;
@@ -158,15 +167,7 @@ __global__ void __launch_bounds__(I8_THREADS, 1)
                     }
                 }
             }
-            if (!ok) {
-                // let copies already issued land before the CTA exits
-                for (int s = 0; s < I8_NST; s++) {
-                    const uint64_t t0 = tc::globaltimer();
-                    while (!tc::mbar_try_wait(&full[s], 0) && !tc::mbar_try_wait(&full[s], 1) &&
-                           tc::globaltimer() - t0 < 100000000ull) {
-                    }
-                }
-            }
+            if (!ok) tc::drain_copies(full, I8_NST, issued, issued_phase);
         }
     } else if (warp == 1) {
         // ------------------------------------------------------------ MMA issuer
@@ -178,7 +179,7 @@ __global__ void __launch_bounds__(I8_THREADS, 1)
                 for (int g = 0; g < p.n_groups && ok; g++) {
                     const int4 grp = p.groups[g];
                     if (!tc::mbar_wait(&acc_empty[abuf], aphase ^ 1, &abort_flag, p.err, ERR_TIMEOUT_MMA,
-                                       I8_WAIT_NS)) {
+                                       wait_ns)) {
                         ok = false;
                         break;
                     }
@@ -189,7 +190,7 @@ __global__ void __launch_bounds__(I8_THREADS, 1)
                         const int4 item = p.items[it];
                         for (int kb = item.z; kb < item.w; kb++) {
                             if (!tc::mbar_wait(&full[stage], phase, &abort_flag, p.err, ERR_TIMEOUT_MMA,
-                                               I8_WAIT_NS)) {
+                                               wait_ns)) {
                                 ok = false;
                                 break;
                             }
@@ -252,7 +253,7 @@ __global__ void __launch_bounds__(I8_THREADS, 1)
                     eb0 = c0 < p.n ? (int)__ldg(ebr + c0) : 0;
                     eb1 = c1 < p.n ? (int)__ldg(ebr + c1) : 0;
                 }
-                bool wok = tc::mbar_wait(&acc_full[abuf], aphase, &abort_flag, p.err, ERR_TIMEOUT_EPI, I8_WAIT_NS);
+                bool wok = tc::mbar_wait(&acc_full[abuf], aphase, &abort_flag, p.err, ERR_TIMEOUT_EPI, wait_ns);
                 if constexpr (MODE == 1) wok = __all_sync(0xffffffffu, wok);  // the lanes agree before any shuffle
                 if (!wok) {
                     ok = false;
@@ -1238,6 +1239,18 @@ static bool i8_lds_valid(char ta, char tb, int m, int n, int k, int lda, int ldb
 
 }  // namespace ozb
 
+
+// Testing hook (no reference counterpart): the limit of every bounded wait in
+// the INT8 product kernel on the current device, in nanoseconds (0 restores
+// the default of 2 s).  A short limit makes a wait run out: the call then
+// returns CUOZBLAS_STATUS_DEVICE_TIMEOUT after the kernel has let its copies
+// and MMAs finish and released its tensor memory.
+extern "C" int cuozblasSetI8WaitLimit(uint64_t ns) {
+    using namespace ozb;
+    const uint64_t v = ns == 0 ? I8_WAIT_NS : ns;
+    OZB_CHECK(cudaMemcpyToSymbol(g_i8_wait_ns, &v, sizeof(v)));
+    return CUOZBLAS_STATUS_SUCCESS;
+}
 
 extern "C" int cuozblasDgemmI8(cuozblasHandle_t *h, char transa, char transb, int32_t m, int32_t n, int32_t k,
                                double alpha, const double *A, int32_t lda, const double *B, int32_t ldb, double beta,

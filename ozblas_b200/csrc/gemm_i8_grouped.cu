@@ -276,6 +276,7 @@ __global__ void __launch_bounds__(G_THREADS, 1) k_i8_grouped(const GParams p) {
         // ------------------------------------------------------------ producer
         if (lane == 0) {
             uint32_t stage = 0, phase = 0;
+            uint32_t issued = 0, issued_phase = 0;  // per stage: a copy was issued, and the phase it completes
             bool ok = true;
             for (int ti = t_begin; ti < t_end && ok; ti++) {
                 const int4 tl = p.tiles[ti];
@@ -296,6 +297,8 @@ __global__ void __launch_bounds__(G_THREADS, 1) k_i8_grouped(const GParams p) {
                             tc::mbar_arrive_expect_tx(&full[stage], G_STAGE);
                             tc::bulk_load(sa, a0 + (size_t)kb * G_TILE_BYTES, G_TILE_BYTES, &full[stage]);
                             tc::bulk_load(sb, b0 + (size_t)kb * G_TILE_BYTES, G_TILE_BYTES, &full[stage]);
+                            issued |= 1u << stage;
+                            issued_phase = (issued_phase & ~(1u << stage)) | (phase << stage);
                             if (++stage == G_NST) {
                                 stage = 0;
                                 phase ^= 1;
@@ -304,14 +307,7 @@ __global__ void __launch_bounds__(G_THREADS, 1) k_i8_grouped(const GParams p) {
                     }
                 }
             }
-            if (!ok) {
-                for (int s = 0; s < G_NST; s++) {
-                    const uint64_t t0 = tc::globaltimer();
-                    while (!tc::mbar_try_wait(&full[s], 0) && !tc::mbar_try_wait(&full[s], 1) &&
-                           tc::globaltimer() - t0 < 100000000ull) {
-                    }
-                }
-            }
+            if (!ok) tc::drain_copies(full, G_NST, issued, issued_phase);
         }
     } else if (warp == 1) {
         // ------------------------------------------------------------ MMA issuer

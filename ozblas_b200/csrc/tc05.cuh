@@ -81,6 +81,20 @@ __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, volati
     }
 }
 
+// After a producer gave up: wait (bounded, 100 ms each) until every copy it
+// issued has landed, so no bulk copy writes shared memory after the CTA
+// exits.  Bit s of `issued` marks a stage that received a copy, bit s of
+// `phase_bits` the parity of the phase that copy completes.
+__device__ __forceinline__ void drain_copies(uint64_t *full, int nst, uint32_t issued, uint32_t phase_bits) {
+    for (int s = 0; s < nst; s++) {
+        if (!((issued >> s) & 1u)) continue;
+        const uint32_t ph = (phase_bits >> s) & 1u;
+        const uint64_t t0 = globaltimer();
+        while (!mbar_try_wait(&full[s], ph) && globaltimer() - t0 < 100000000ull) {
+        }
+    }
+}
+
 // 2D tiled TMA load into shared memory, completing on `bar` (transaction bytes).
 __device__ __forceinline__ void tma_load_2d(void *smem_dst, const CUtensorMap *map, uint64_t *bar, int x, int y) {
     asm volatile(

@@ -198,3 +198,48 @@ def test_autotune_changes_no_bits(oracle, handle, ozb, cuda, tmp_path, monkeypat
         outs.append([c.cpu().numpy() for c in Cs])
     assert all(bits_equal(a, b) for a, b in zip(*outs))
     assert "i8grouped:" in cache.read_text()
+
+
+@pytest.mark.parametrize("fast", [0, 1], ids=["full", "triangular"])
+@pytest.mark.parametrize("phi", [1.0, 4.0])
+def test_i8_correctly_rounded_2048(fast, phi, oracle, handle, ozb, cuda):
+    """m = n = k = 2048: every checked entry equals the correctly rounded exact product (RN of the exact dot, from
+    the oracle's exact accumulator): 64 x 64 sampled entries plus all of row 0 and column 0, for the full and the
+    triangular pair set.  Tolerance: none (bit equality with RN(exact))."""
+    n = 2048
+    A = oracle.phi_matrix(n, n, phi, 1)  # (k, m): row j is column j of A
+    B = oracle.phi_matrix(n, n, phi, 2)  # (n, k): row j is column j of B
+    C = run_i8(ozb, handle, cuda, A, B, n, n, n, fast=fast)
+    assert handle.nSplitA < 19 and handle.nSplitB < 19, "split must be complete (below the default digit cap)"
+    g = np.random.default_rng(11)
+    rows = np.sort(g.choice(n, 64, replace=False))
+    cols = np.sort(g.choice(n, 64, replace=False))
+    At = np.ascontiguousarray(A.T)  # row i of A
+    checks = [(At[rows], B[cols], C[np.ix_(cols, rows)]),  # sampled block, (nc, nr) = column-major nr x nc
+              (At[0:1], B, C[:, 0:1]),                    # row 0
+              (At, B[0:1], C[0:1, :])]                    # column 0
+    for Ar, Bc, Cb in checks:
+        rn, _ = oracle.exact_gemm_block(Ar, Bc, Cb)
+        bad = np.nonzero(rn.view(np.int64) != np.ascontiguousarray(Cb).view(np.int64))
+        assert bad[0].size == 0, (bad[0].size, rn[bad][:3], np.ascontiguousarray(Cb)[bad][:3], handle.nSplitC)
+
+
+def test_i8_wait_timeout_reports_and_recovers(oracle, handle, ozb, cuda):
+    """A bounded device wait that runs out: with the INT8 kernel's wait limit cut to 1 ns, a wait gives up, the
+    call returns CUOZBLAS_STATUS_DEVICE_TIMEOUT (6) instead of hanging or faulting (the kernel lets its copies and
+    MMAs finish and frees its tensor memory first), and with the default limit restored the same call on the same
+    context returns the bits of the first call."""
+    m = n = k = 1024
+    A = oracle.phi_matrix(m, k, 1.0, 1)
+    B = oracle.phi_matrix(k, n, 1.0, 2)
+    ref = run_i8(ozb, handle, cuda, A, B, m, n, k)  # also settles the shape's launch tuning
+    ozb.set_i8_wait_limit(1)
+    try:
+        with pytest.raises(ozb.OzblasError) as e:
+            run_i8(ozb, handle, cuda, A, B, m, n, k)
+        assert e.value.code == 6
+    finally:
+        ozb.set_i8_wait_limit(0)
+    cuda.cuda.synchronize()
+    again = run_i8(ozb, handle, cuda, A, B, m, n, k)
+    assert bits_equal(again, ref)
