@@ -274,13 +274,13 @@ int cuozblasDgemmI8Static(char transa, char transb, int32_t m, int32_t n, int32_
                           int32_t lda, const double *B, int32_t ldb, double beta, double *C, int32_t ldc,
                           int32_t nSplitMax, int32_t fastMode, void *stream);
 
-/* Testing hook, no reference counterpart: the limit (ns) of every bounded
- * mbarrier wait of the INT8 product kernel on the current device (0: the
- * default 2 s).  With a short limit a wait runs out and cuozblasDgemmI8
- * returns CUOZBLAS_STATUS_DEVICE_TIMEOUT; the kernel first lets its copies and
- * tensor-core operations finish and releases its tensor memory, so the
- * context stays usable. */
-int cuozblasSetI8WaitLimit(uint64_t ns);
+/* Testing hook, no reference counterpart: on the current device, the limit
+ * (ns) of every bounded mbarrier wait of the INT8 product kernel (0: the
+ * default 2 s) and, with hold_copies != 0, a producer that issues no copies,
+ * so that the tensor-core issuer's wait runs out and cuozblasDgemmI8 returns
+ * CUOZBLAS_STATUS_DEVICE_TIMEOUT; the kernel releases its tensor memory
+ * first and the context stays usable.  Call (0, 0) to restore. */
+int cuozblasSetI8WaitTest(uint64_t ns, int32_t hold_copies);
 
 /* Rule checks exported for the host-side tests (same code the kernels use). */
 int cuozblasRuleTau(double v);

@@ -82,7 +82,7 @@ _destroy = _sig("cuozblasHandleDestroy", [_HP])
 _setstream = _sig("cuozblasSetStream", [_HP, _vp])
 _launches = _sig("cuozblasGetLaunchCount", [_HP, C.POINTER(C.c_uint64)])
 _readenv = _sig("cuozblasHandleReadEnv", [_HP])
-_i8_wait = _sig("cuozblasSetI8WaitLimit", [C.c_uint64])
+_i8_wait = _sig("cuozblasSetI8WaitTest", [C.c_uint64, _i32])
 _ddot = _sig("cuozblasDdot", [_HP, _i32, _vp, _i32, _vp, _i32, C.POINTER(_d)])
 _dnrm2 = _sig("cuozblasDnrm2", [_HP, _i32, _vp, _i32, C.POINTER(_d)])
 _daxpy = _sig("cuozblasDaxpy", [_HP, _i32, _d, _vp, _i32, _vp, _i32])
@@ -119,7 +119,7 @@ _version = _sig("cuozblasVersion", [], C.c_char_p)
 #: every C-ABI symbol include/cuozblas.h declares (checked by the CPU tests)
 C_ABI_SYMBOLS = [
     "cuozblasHandleCreate", "cuozblasHandleDestroy", "cuozblasSetStream", "cuozblasGetLaunchCount",
-    "cuozblasHandleReadEnv", "cuozblasSetI8WaitLimit", "cuozblasDdot", "cuozblasDnrm2",
+    "cuozblasHandleReadEnv", "cuozblasSetI8WaitTest", "cuozblasDdot", "cuozblasDnrm2",
     "cuozblasDaxpy", "cuozblasDgemv", "cuozblasDgemm", "cuozblasDcsrmv", "cuozblasDcsrmvSplitA", "cuozblasDcg",
     "cuozblasDgemmI8", "cuozblasDgemmI8Static", "cuozblasDgemmI8Batched", "cuozblasRuleTau", "cuozblasRuleRho",
     "cuozblasRuleCrSum", "cuozblasDSgemm", "cuozblasDSgemv", "cuozblasDSdot", "cuozblasDSnrm2",
@@ -277,9 +277,10 @@ def qnrm2(h, n, x, incx=1):
     return (r[0], r[1])
 
 
-def set_i8_wait_limit(ns: int):
-    """Testing hook: the bounded-wait limit of the INT8 product kernel on the current device (0: default 2 s)."""
-    _chk("cuozblasSetI8WaitLimit", _i8_wait(int(ns)))
+def set_i8_wait_test(ns: int, hold_copies: bool = False):
+    """Testing hook: the bounded-wait limit of the INT8 product kernel on the current device (0: default 2 s) and
+    whether its producer holds back every copy (so a wait runs out); (0, False) restores."""
+    _chk("cuozblasSetI8WaitTest", _i8_wait(int(ns), 1 if hold_copies else 0))
 
 
 def dgemm_i8(h, ta, tb, m, n, k, alpha, A, lda, B, ldb, beta, Cm, ldc):

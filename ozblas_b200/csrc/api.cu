@@ -24,6 +24,8 @@ int csrmv_presplit(cuozblasHandle_t *h, int m, int n, double alpha, const double
                    const int *colind, const int *rowptr, const double *x, double beta, double *y);
 int dot_fused(cuozblasHandle_t *h, int n, const double *x, const double *y, double *ret, bool *done, int *nA,
               int *nB);
+int dot_exact(cuozblasHandle_t *h, int n, const double *x, const double *y, double *ret, bool *done, int *nA,
+              int *nB);
 int csrmv_fused(cuozblasHandle_t *h, int m, int n, double alpha, const double *val, const int *colind,
                 const int *rowptr, const double *x, double beta, double *y, int shift, int na_hint, bool *done,
                 int *nA_out, int *nB_out);
@@ -65,6 +67,7 @@ void EnvSwitches::read() {
     q_dmma = env_on("OZBLAS_Q_DMMA");
     ds_simt = env_on("OZBLAS_DS_SIMT");
     dot_tree = env_on("OZBLAS_DOT_TREE");
+    dot_two_pass = env_on("OZBLAS_DOT_TWO_PASS");
     cg_no_graph = env_on("OZBLAS_CG_NO_GRAPH");
     dot_trace = env_on("OZBLAS_DOT_TRACE");
     cg_trace = env_on("OZBLAS_CG_TRACE");
@@ -116,7 +119,10 @@ static int dot_impl(cuozblasHandle_t *h, int n, const double *x, const double *y
     State *st = state(h);
     bool done = false;
     int nA = 0, nB = 0;
-    if (h->splitEpsMode == 0) OZB_TRY(dot_fused(h, n, x, y, ret, &done, &nA, &nB));
+    // NearSum: one pass over x and y (exact dot, certified rounding, proven split counts)
+    if (h->splitEpsMode == 0 && h->sumMode == 1 && !st->env.dot_two_pass)
+        OZB_TRY(dot_exact(h, n, x, y, ret, &done, &nA, &nB));
+    if (h->splitEpsMode == 0 && !done) OZB_TRY(dot_fused(h, n, x, y, ret, &done, &nA, &nB));
     if (done) {
         h->nSplitA = (float)nA;
         h->nSplitB = (float)nB;

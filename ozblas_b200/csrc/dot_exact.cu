@@ -1,0 +1,324 @@
+// dot_exact.cu — the NearSum DOT / NRM2 in one pass over x and y.
+//
+// With sumMode 1 and a complete split the reference's DOT is RN of the exact
+// dot product: its nA x nB slice-pair products are exact, their sum over the
+// full pair set is sum_k x_k y_k exactly, NearSum rounds that once
+// (src/cpu/ozblas_sum.cpp:10-112) and the driver's fma(1, t, 0 * 0)
+// (src/cpu/ozblas_dot.cpp:25-27, src/cpu/ozblas_sum.cpp:366) keeps it.  So
+//
+//  k_dot_exact  streams x and y once: the first-pass statistics of the split
+//               (max, lowest set bit, Inf/NaN: the split counts) and the exact
+//               dot in fixed-grid bins (xbins.cuh); its last block rounds the
+//               exact sum (certified) into the scratch.
+//  k_dot_prove  the split counts of the exec info rest on the predicted tau
+//               chain (chain.cuh): this kernel proves it like the two-pass
+//               DOT's second pass, cutting elements only until every level has
+//               its witness (blocks stop as soon as the proof is complete, so
+//               on ordinary data it reads a few thousand elements), and
+//               publishes the result only when the chain is proven, the split
+//               is complete (first all-zero level below the cap) and the
+//               rounding was certified.  Otherwise the host runs the two-pass
+//               DOT, which handles every case.
+// The result is the reference's bits whenever it is published; the exec-info
+// counts are those of the proven chain.
+#include <cstring>
+
+#include "fused.h"
+#include "ozb_internal.h"
+#include "sum.cuh"
+#include "xbins.cuh"
+
+namespace ozb {
+
+constexpr int kXThreads = 256;
+constexpr int kXMaxBlocks = 1184;  // 148 SMs x 8
+
+struct DotExactScratch {
+    XPart part[kXMaxBlocks];  // one bin set per block of k_dot_exact
+    unsigned ticket;           // blocks of k_dot_exact that are done
+    unsigned ticket2;          // blocks of k_dot_prove that are done
+    int certified;
+    int pad;
+    double result;             // certified RN(x . y)
+    unsigned proven[2];        // levels whose predicted tau some element proved
+};
+
+// ---- one pass: statistics and exact bins ----------------------------------
+
+template <bool SAME, bool ALIGNED>
+__global__ void __launch_bounds__(kXThreads) k_dot_exact(int n, const double *__restrict__ x,
+                                                         const double *__restrict__ y, DotScratch *__restrict__ sc,
+                                                         DotExactScratch *__restrict__ xs) {
+    __shared__ double red[kXThreads / 32];
+    __shared__ XPart wsh[kXThreads / 32];
+    __shared__ int last;
+    XAcc acc;
+    xacc_init(acc);
+    double mx = 0.0, my = 0.0;
+    int lx = 0, ly = 0, bx = 0, by = 0;
+    const int64_t stride = (int64_t)gridDim.x * kXThreads;
+    constexpr int U = 4;  // double2 loads per vector per step
+    if (ALIGNED) {
+        const int64_t np = (int64_t)n >> 1;
+        const double2 *x2 = reinterpret_cast<const double2 *>(x);
+        const double2 *y2 = reinterpret_cast<const double2 *>(y);
+        // every lane of a warp runs the same number of steps (the bins' B is warp-uniform)
+        const int64_t iw = (int64_t)blockIdx.x * kXThreads + (threadIdx.x & ~31);
+        const int64_t steps = iw < np ? (np - iw + U * stride - 1) / (U * stride) : 0;
+        int64_t i = (int64_t)blockIdx.x * kXThreads + threadIdx.x;
+        for (int64_t s = 0; s < steps; s++, i += U * stride) {
+            double2 a[U], b[U];
+#pragma unroll
+            for (int u = 0; u < U; u++) {
+                const int64_t k = i + u * stride;
+                a[u] = k < np ? x2[k] : make_double2(0.0, 0.0);
+                if (!SAME) b[u] = k < np ? y2[k] : make_double2(0.0, 0.0);
+            }
+            unsigned hi = 0u;
+#pragma unroll
+            for (int u = 0; u < U; u++) {
+                const double2 bb = SAME ? a[u] : b[u];
+                hi = max(hi, abs_hiword(__dmul_rn(a[u].x, bb.x)));
+                hi = max(hi, abs_hiword(__dmul_rn(a[u].y, bb.y)));
+                scan_elem(a[u].x, mx, lx, bx);
+                scan_elem(a[u].y, mx, lx, bx);
+                if (!SAME) {
+                    scan_elem(b[u].x, my, ly, by);
+                    scan_elem(b[u].y, my, ly, by);
+                }
+            }
+            xacc_fit(acc, __reduce_max_sync(0xffffffffu, hi));
+#pragma unroll
+            for (int u = 0; u < U; u++) {
+                const double2 bb = SAME ? a[u] : b[u];
+                xacc_product(acc, a[u].x, bb.x);
+                xacc_product(acc, a[u].y, bb.y);
+            }
+            if ((s & 7) == 7) xacc_normalize(acc);  // every 64 products per lane
+        }
+        if ((n & 1) && blockIdx.x == 0 && threadIdx.x < 32) {  // the odd last element, one warp
+            const double xe = threadIdx.x == 0 ? x[n - 1] : 0.0;
+            const double ye = threadIdx.x == 0 ? y[n - 1] : 0.0;
+            scan_elem(xe, mx, lx, bx);
+            if (!SAME) scan_elem(ye, my, ly, by);
+            xacc_normalize(acc);
+            xacc_fit(acc, __reduce_max_sync(0xffffffffu, abs_hiword(__dmul_rn(xe, ye))));
+            xacc_product(acc, xe, ye);
+        }
+    } else {
+        const int64_t iw = (int64_t)blockIdx.x * kXThreads + (threadIdx.x & ~31);
+        const int64_t steps = iw < n ? ((int64_t)n - iw + stride - 1) / stride : 0;
+        int64_t i = (int64_t)blockIdx.x * kXThreads + threadIdx.x;
+        for (int64_t s = 0; s < steps; s++, i += stride) {
+            const double xe = i < n ? x[i] : 0.0;
+            const double ye = SAME ? xe : (i < n ? y[i] : 0.0);
+            scan_elem(xe, mx, lx, bx);
+            if (!SAME) scan_elem(ye, my, ly, by);
+            xacc_fit(acc, __reduce_max_sync(0xffffffffu, abs_hiword(__dmul_rn(xe, ye))));
+            xacc_product(acc, xe, ye);
+            if ((s & 63) == 63) xacc_normalize(acc);
+        }
+    }
+    scan_commit(&sc->vs, 0, mx, lx, bx, red);
+    if (!SAME) scan_commit(&sc->vs, 1, my, ly, by, red);
+    xacc_block_reduce(acc, wsh, xs->part[blockIdx.x]);
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) last = atomicAdd(&xs->ticket, 1u) == gridDim.x - 1;
+    __syncthreads();
+    if (!last) return;
+    __threadfence();
+    __shared__ double sh[kXThreads * (kXK2 + 1)];
+    xparts_round(xs->part, gridDim.x, sh, &xs->result, &xs->certified);
+    if (threadIdx.x == 0) xs->ticket = 0u;
+}
+
+// ---- the chain proof, with early exit -------------------------------------
+
+template <int G, int T, bool SAME>
+__device__ __forceinline__ void prove_body(double x0, double y0, double x1, double y1, const TreePlan &pl,
+                                           unsigned (&prov)[2]) {
+    double a0[T + 1], a1[T + 1];
+    cut_tree<G, T>(x0, pl.sig[0], a0);
+    cut_tree<G, T>(x1, pl.sig[0], a1);
+    const unsigned px = pl.need[0] & ~prov[0];
+    if (px) {  // uniform
+        unsigned hw[kChainLevels];
+#pragma unroll
+        for (int s = 0; s < T; s++) hw[s] = max(abs_hiword(a0[s + 1]), abs_hiword(a1[s + 1]));
+        prov[0] |= prove_levels<T>(hw, pl.hb[0], px);
+    }
+    if (!SAME) {
+        const unsigned py = pl.need[1] & ~prov[1];
+        if (py) {
+            double b0[T + 1], b1[T + 1];
+            cut_tree<G, T>(y0, pl.sig[1], b0);
+            cut_tree<G, T>(y1, pl.sig[1], b1);
+            unsigned hw[kChainLevels];
+#pragma unroll
+            for (int s = 0; s < T; s++) hw[s] = max(abs_hiword(b0[s + 1]), abs_hiword(b1[s + 1]));
+            prov[1] |= prove_levels<T>(hw, pl.hb[1], py);
+        }
+    }
+}
+
+template <int G, bool SAME>
+__device__ __forceinline__ void prove_element(double x0, double y0, double x1, double y1, const TreePlan &pl,
+                                              unsigned (&prov)[2]) {
+    int T = plan_depth(pl, 0, __reduce_min_sync(0xffffffffu, min(exp_key(x0), exp_key(x1))));
+    if (!SAME) {
+        const int ty = plan_depth(pl, 1, __reduce_min_sync(0xffffffffu, min(exp_key(y0), exp_key(y1))));
+        T = ty > T ? ty : T;
+    }
+    if (T > pl.L - 1) T = pl.L - 1;
+    switch (T) {
+        case 0: break;  // level 0 alone proves nothing
+        case 1: prove_body<G, 1, SAME>(x0, y0, x1, y1, pl, prov); break;
+        case 2: prove_body<G, 2, SAME>(x0, y0, x1, y1, pl, prov); break;
+        case 3: prove_body<G, 3, SAME>(x0, y0, x1, y1, pl, prov); break;
+        case 4: prove_body<G, 4, SAME>(x0, y0, x1, y1, pl, prov); break;
+        case 5: prove_body<G, 5, SAME>(x0, y0, x1, y1, pl, prov); break;
+        case 6: prove_body<G, 6, SAME>(x0, y0, x1, y1, pl, prov); break;
+        default: prove_body<G, 7, SAME>(x0, y0, x1, y1, pl, prov); break;
+    }
+}
+
+template <int G, bool SAME>
+__global__ void __launch_bounds__(kXThreads) k_dot_prove(int n, const double *__restrict__ x,
+                                                         const double *__restrict__ y, int rho, int maxS,
+                                                         DotScratch *__restrict__ sc,
+                                                         DotExactScratch *__restrict__ xs) {
+    __shared__ TreePlan pl;
+    __shared__ int done_sh, last;
+    const int t = threadIdx.x;
+    plan_in_block(&sc->vs, rho, maxS, SAME, pl);
+    __syncthreads();
+    unsigned prov[2] = {0u, 0u};  // per warp (uniform)
+    const unsigned need0 = pl.need[0], need1 = SAME ? 0u : pl.need[1];
+    if (pl.valid && (need0 | need1)) {
+        const int64_t stride = (int64_t)gridDim.x * kXThreads;  // in element pairs (two per lane)
+        const int64_t npairs = ((int64_t)n + 1) >> 1;
+        for (int64_t base = (int64_t)blockIdx.x * kXThreads; base < npairs; base += stride) {
+            if (t == 0) {
+                const unsigned g0 = __ldcg(&xs->proven[0]), g1 = __ldcg(&xs->proven[1]);
+                done_sh = (g0 & need0) == need0 && (g1 & need1) == need1;
+            }
+            __syncthreads();
+            const int stop = done_sh;
+            __syncthreads();
+            if (stop) break;
+            const int64_t i = base + t, e0 = 2 * i, e1 = 2 * i + 1;
+            const double x0 = e0 < n ? x[e0] : 0.0, x1 = e1 < n ? x[e1] : 0.0;
+            const double y0 = SAME ? x0 : (e0 < n ? y[e0] : 0.0), y1 = SAME ? x1 : (e1 < n ? y[e1] : 0.0);
+            const unsigned before0 = prov[0], before1 = prov[1];
+            prove_element<G, SAME>(x0, y0, x1, y1, pl, prov);
+            if ((t & 31) == 0) {
+                if (prov[0] != before0) atomicOr(&xs->proven[0], prov[0]);
+                if (!SAME && prov[1] != before1) atomicOr(&xs->proven[1], prov[1]);
+            }
+        }
+    }
+    __threadfence();
+    __syncthreads();
+    if (t == 0) last = atomicAdd(&xs->ticket2, 1u) == gridDim.x - 1;
+    __syncthreads();
+    if (!last) return;
+    __threadfence();
+    if (t == 0) {
+        int valid = pl.valid;
+        if ((__ldcg(&xs->proven[0]) & need0) != need0 || (__ldcg(&xs->proven[1]) & need1) != need1) valid = 0;
+        const int nA = pl.ns[0], nB = SAME ? pl.ns[0] : pl.ns[1];
+        // a complete split: the first all-zero level lies within the levels the count keeps
+        const int zA = pl.z[0], zB = SAME ? pl.z[0] : pl.z[1];
+        if (zA > nA - 1 || zB > nB - 1) valid = 0;
+        if (!__ldcg(&xs->certified)) valid = 0;
+        sc->out.ns0 = nA;
+        sc->out.ns1 = nB;
+        sc->out.status = valid;
+        sc->out.pad = 0;
+        sc->out.result = fma(1.0, __ldcg(&xs->result), 0.0 * 0.0);  // alpha = 1, beta = 0 as the DOT driver passes them
+        // leave the scratch zeroed for the next use
+        xs->proven[0] = xs->proven[1] = 0u;
+        xs->ticket2 = 0u;
+        xs->certified = 0;
+        sc->vs = VecStats{};
+    }
+}
+
+// Returns SUCCESS with *done = true and the result in *ret when the one-pass
+// NearSum DOT is proven; *done = false leaves the call to the two-pass DOT.
+int dot_exact(cuozblasHandle_t *h, int n, const double *x, const double *y, double *ret, bool *done, int *nA,
+              int *nB) {
+    State *st = state(h);
+    *done = false;
+    if (n <= 0) return CUOZBLAS_STATUS_SUCCESS;
+    Arena ar(h);
+    const uint64_t mk = ar.mark();
+    DotScratch *sc = ar.take<DotScratch>(1);
+    DotExactScratch *xs = ar.take<DotExactScratch>(1);
+    if (!ar.ok) {
+        ar.release(mk);
+        return CUOZBLAS_STATUS_SUCCESS;
+    }
+    const int maxS = h->nSplitMax > 0 ? h->nSplitMax : kMaxSplitDefault;
+    const int rho = rho_rule(n, h->splitEpsMode);
+    OZB_CHECK(cudaMemsetAsync(sc, 0, sizeof(DotScratch), st->stream));
+    OZB_CHECK(cudaMemsetAsync(xs, 0, sizeof(DotExactScratch), st->stream));
+    const bool same = (x == y);
+    const bool aligned = ((reinterpret_cast<uintptr_t>(x) | reinterpret_cast<uintptr_t>(y)) & 15u) == 0;
+    const int nsm = sm_count();
+    int blocks = (int)(((int64_t)n + 8LL * kXThreads - 1) / (8LL * kXThreads));
+    if (blocks > nsm * 4) blocks = nsm * 4;
+    if (blocks > kXMaxBlocks) blocks = kXMaxBlocks;
+    if (blocks < 1) blocks = 1;
+    counted(h);
+    if (aligned) {
+        if (same)
+            k_dot_exact<true, true><<<blocks, kXThreads, 0, st->stream>>>(n, x, y, sc, xs);
+        else
+            k_dot_exact<false, true><<<blocks, kXThreads, 0, st->stream>>>(n, x, y, sc, xs);
+    } else {
+        if (same)
+            k_dot_exact<true, false><<<blocks, kXThreads, 0, st->stream>>>(n, x, y, sc, xs);
+        else
+            k_dot_exact<false, false><<<blocks, kXThreads, 0, st->stream>>>(n, x, y, sc, xs);
+    }
+    OZB_CHECK(cudaGetLastError());
+    const int G = chain_group(rho, 4);
+    int pblocks = (int)((((int64_t)n + 1) / 2 + kXThreads - 1) / kXThreads);
+    if (pblocks > nsm * 2) pblocks = nsm * 2;
+    if (pblocks < 1) pblocks = 1;
+    counted(h);
+#define OZB_PROVE(GG)                                                                                       \
+    do {                                                                                                  \
+        if (same)                                                                                         \
+            k_dot_prove<GG, true><<<pblocks, kXThreads, 0, st->stream>>>(n, x, y, rho, maxS, sc, xs);     \
+        else                                                                                              \
+            k_dot_prove<GG, false><<<pblocks, kXThreads, 0, st->stream>>>(n, x, y, rho, maxS, sc, xs);    \
+    } while (0)
+    switch (G) {
+        case 1: OZB_PROVE(1); break;
+        case 2: OZB_PROVE(2); break;
+        case 3: OZB_PROVE(3); break;
+        default: OZB_PROVE(4); break;
+    }
+#undef OZB_PROVE
+    OZB_CHECK(cudaGetLastError());
+    static_assert(sizeof(DotStatus) == 24, "status block layout");
+    OZB_CHECK(cudaMemcpyAsync(st->h_dbl, &sc->out, sizeof(DotStatus), cudaMemcpyDeviceToHost, st->stream));
+    OZB_CHECK(cudaStreamSynchronize(st->stream));
+    ar.release(mk);
+    DotStatus res;
+    memcpy(&res, st->h_dbl, sizeof(res));
+    if (res.status == 1) {
+        *done = true;
+        *nA = res.ns0;
+        *nB = res.ns1;
+        *ret = res.result;
+    } else if (st->env.dot_trace) {
+        fprintf(stderr, "cuozblas: one-pass NearSum dot not used (n=%d)\n", n);
+    }
+    return CUOZBLAS_STATUS_SUCCESS;
+}
+
+}  // namespace ozb

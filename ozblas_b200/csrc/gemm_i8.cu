@@ -57,10 +57,11 @@ constexpr uint64_t I8_WAIT_NS = 2000000000ull;                  // 2 s per wait
 
 enum { ERR_TIMEOUT_PRODUCER = 1, ERR_TIMEOUT_MMA = 2, ERR_TIMEOUT_EPI = 3 };
 
-// Limit of every bounded mbarrier wait in the INT8 product kernels (k_i8_gemm,
-// k_i8_grouped); cuozblasSetI8WaitLimit changes it (tests shorten it to make a
-// wait run out).
+// Limit of every bounded mbarrier wait in k_i8_gemm, and a test switch that
+// makes its producer issue no copies, so that the MMA issuer's first wait
+// runs out (set by cuozblasSetI8WaitTest; tests only).
 __device__ uint64_t g_i8_wait_ns = I8_WAIT_NS;
+__device__ int g_i8_hold_copies = 0;
 
 struct I8Params {
     int m, n, m_pad, n_pad, ldc;
@@ -142,7 +143,7 @@ __global__ void __launch_bounds__(I8_THREADS, 1)
         if (lane == 0) {
             uint32_t stage = 0, phase = 0;
             uint32_t issued = 0, issued_phase = 0;  // per stage: a copy was issued, and the phase it completes
-            bool ok = true;
+            bool ok = g_i8_hold_copies == 0;
             for (int tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x) {
                 int tm, tn;
                 tile_coords(tile, p, tm, tn);
@@ -1240,15 +1241,18 @@ static bool i8_lds_valid(char ta, char tb, int m, int n, int k, int lda, int ldb
 }  // namespace ozb
 
 
-// Testing hook (no reference counterpart): the limit of every bounded wait in
-// the INT8 product kernel on the current device, in nanoseconds (0 restores
-// the default of 2 s).  A short limit makes a wait run out: the call then
-// returns CUOZBLAS_STATUS_DEVICE_TIMEOUT after the kernel has let its copies
-// and MMAs finish and released its tensor memory.
-extern "C" int cuozblasSetI8WaitLimit(uint64_t ns) {
+// Testing hook (no reference counterpart), on the current device: the limit
+// of every bounded wait in the INT8 product kernel in nanoseconds (0 restores
+// the default of 2 s), and with hold_copies != 0 a producer that issues no
+// copies, so that a wait runs out: the call then returns
+// CUOZBLAS_STATUS_DEVICE_TIMEOUT after the kernel has released its tensor
+// memory, and the context stays usable.
+extern "C" int cuozblasSetI8WaitTest(uint64_t ns, int32_t hold_copies) {
     using namespace ozb;
     const uint64_t v = ns == 0 ? I8_WAIT_NS : ns;
+    const int hold = hold_copies != 0 ? 1 : 0;
     OZB_CHECK(cudaMemcpyToSymbol(g_i8_wait_ns, &v, sizeof(v)));
+    OZB_CHECK(cudaMemcpyToSymbol(g_i8_hold_copies, &hold, sizeof(hold)));
     return CUOZBLAS_STATUS_SUCCESS;
 }
 

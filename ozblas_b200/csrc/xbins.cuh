@@ -1,0 +1,258 @@
+// xbins.cuh — exact accumulation of a stream of doubles in one pass, in bins
+// of fixed absolute grids, for the correctly rounded (NearSum) reductions.
+//
+// With a complete split the reference's NearSum DOT returns RN of the exact
+// dot product (its slice-pair products are exact and NearSum rounds their
+// exact sum once), so any exact method gives its bits.  Here every product
+// x*y is the exact pair (p, e) of TwoProd (p = RN(x y), e = fma(x, y, -p)),
+// and each of p and e is cut onto the grids of K consecutive bins:
+//   bin j holds multiples of g_j = 2^((B - j) W),
+//   q_j = (r + sigma_j) - sigma_j with sigma_j = 1.5 * 2^((B - j) W + 52)
+// is r rounded to g_j (exact while |r| < 2^((B - j) W + 51)), r -= q_j is
+// exact, and the bin adds q_j exactly while it stays below 2^53 g_j.  B is
+// warp-uniform: it rises when a product reaches 2^((B + 1) W) or when a
+// lane's top bin fills (the top bin's content is then cut onto the next grid
+// up and the lowest bin leaves the window).  What a deposit leaves below the
+// lowest bin, and every bin that leaves the window, is added with upward
+// rounding to `drop`, an upper bound of everything not held exactly; the
+// final value is certified by rounding the held sum minus and plus that
+// bound (equal results: the rounding of the true sum is determined).
+#pragma once
+#include "ozb_device.cuh"
+#include "sum.cuh"
+
+namespace ozb {
+
+constexpr int kXK = 4;      // bins per lane
+constexpr int kXW = 44;     // bits per bin (a bin takes 2^(52 - 44) = 256 deposits between renormalisations)
+constexpr int kXBmin = -20; // lowest top bin: the lowest grid stays >= 2^-1012 (sigmas normal)
+constexpr int kXBmax = 21;  // highest top bin: sigmas of the next bin up stay finite
+
+struct XAcc {
+    int B;              // top bin (warp-uniform)
+    double a[kXK];      // bins, exact
+    double sig[kXK];    // sigma_j of the current B
+    double drop;        // upper bound of |everything not held| (rounded up)
+    int flags;          // 1: a product outside the range TwoProd keeps exact (tiny or huge)
+};
+
+__device__ __forceinline__ void xacc_sigmas(XAcc &x) {
+#pragma unroll
+    for (int j = 0; j < kXK; j++) x.sig[j] = 1.5 * pow2((x.B - j) * kXW + 52);
+}
+
+__device__ __forceinline__ void xacc_init(XAcc &x) {
+    x.B = kXBmin;
+#pragma unroll
+    for (int j = 0; j < kXK; j++) x.a[j] = 0.0;
+    x.drop = 0.0;
+    x.flags = 0;
+    xacc_sigmas(x);
+}
+
+// Cut v onto bins j0..K-1 (v below the top of bin j0's range).
+template <int J0>
+__device__ __forceinline__ void xacc_deposit(XAcc &x, double v) {
+    double r = v;
+#pragma unroll
+    for (int j = J0; j < kXK; j++) {
+        const double q = __dsub_rn(__dadd_rn(r, x.sig[j]), x.sig[j]);
+        r = __dsub_rn(r, q);
+        x.a[j] = __dadd_rn(x.a[j], q);
+    }
+    x.drop = __dadd_ru(x.drop, fabs(r));
+}
+
+// The exact product x * y into the bins: p into bins 0..K-1, e (at most
+// 2^-53 |p| < 2^(B W), W < 53) into bins 1..K-1.
+__device__ __forceinline__ void xacc_product(XAcc &x, double a, double b) {
+    const double p = __dmul_rn(a, b);
+    const double e = __fma_rn(a, b, -p);
+    const double ap = fabs(p);
+    // TwoProd is exact unless the product is tiny (its error term underflows)
+    // or beyond the window's top (kXBmax)
+    if ((ap < 0x1p-969 && a != 0.0 && b != 0.0) || ap >= 0x1p1012) x.flags |= 1;
+    xacc_deposit<0>(x, p);
+    xacc_deposit<1>(x, e);
+}
+
+// Raise B by one: the top bin is cut onto the new top grid, the rest move
+// down one bin, the lowest leaves the window (into drop).  Every lane of the
+// warp calls this together.
+__device__ __forceinline__ void xacc_raise(XAcc &x) {
+    if (x.B >= kXBmax) {
+        x.flags |= 1;
+        return;
+    }
+    const double s = 1.5 * pow2((x.B + 1) * kXW + 52);
+    const double c = __dsub_rn(__dadd_rn(x.a[0], s), s);
+    x.drop = __dadd_ru(x.drop, fabs(x.a[kXK - 1]));
+#pragma unroll
+    for (int j = kXK - 1; j >= 2; j--) x.a[j] = x.a[j - 1];
+    x.a[1] = __dsub_rn(x.a[0], c);
+    x.a[0] = c;
+    x.B += 1;
+    xacc_sigmas(x);
+}
+
+// Before depositing products whose largest magnitude (over the warp) has the
+// high word `hi_max` (sign cleared): raise B until they lie below 2^((B+1)W).
+__device__ __forceinline__ void xacc_fit(XAcc &x, unsigned hi_max) {
+    while (x.B < kXBmax && hi_max >= (unsigned)((x.B + 1) * kXW + 1023) << 20) xacc_raise(x);
+}
+
+// Carry every bin's part above the next bin's grid into it (exact), then keep
+// the top bin below 2^(W-1) g_0 by raising B (warp-uniform).  Afterwards
+// |a_j| <= 2^(W-1) g_j for every bin, so 2^(54 - W) such values add exactly.
+__device__ __forceinline__ void xacc_normalize(XAcc &x) {
+#pragma unroll
+    for (int j = kXK - 1; j >= 1; j--) {
+        const double c = __dsub_rn(__dadd_rn(x.a[j], x.sig[j - 1]), x.sig[j - 1]);
+        x.a[j] = __dsub_rn(x.a[j], c);
+        x.a[j - 1] = __dadd_rn(x.a[j - 1], c);
+    }
+    for (int guard = 0; guard < 4; guard++) {
+        const double lim = pow2((x.B + 1) * kXW - 1);
+        if (!__any_sync(0xffffffffu, fabs(x.a[0]) > lim)) break;
+        xacc_raise(x);
+        const double c = __dsub_rn(__dadd_rn(x.a[1], x.sig[0]), x.sig[0]);
+        x.a[1] = __dsub_rn(x.a[1], c);
+        x.a[0] = __dadd_rn(x.a[0], c);
+    }
+}
+
+// One bin set of a block or of the whole reduction: top bin B, K bins,
+// the drop bound and the flags.
+struct XPart {
+    double B, a[kXK], drop, flags;
+};
+
+// Warp sum of the lanes' bins (same B), then block sum into `out` (thread 0;
+// `wsh` holds one XPart per warp).  Exact: every lane is normalised first, a
+// warp's bins stay below 2^(W+4) g and a block of at most 8 warps below
+// 2^(W+7) g.
+__device__ __forceinline__ void xacc_block_reduce(XAcc &x, XPart *wsh, XPart &out) {
+    xacc_normalize(x);
+#pragma unroll
+    for (int j = 0; j < kXK; j++)
+        for (int o = 16; o > 0; o >>= 1) x.a[j] = __dadd_rn(x.a[j], __shfl_xor_sync(0xffffffffu, x.a[j], o));
+    for (int o = 16; o > 0; o >>= 1) x.drop = __dadd_ru(x.drop, __shfl_xor_sync(0xffffffffu, x.drop, o));
+    const int fl = (int)__reduce_or_sync(0xffffffffu, (unsigned)x.flags);
+    const int w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    if ((threadIdx.x & 31) == 0) {
+        wsh[w].B = (double)x.B;
+#pragma unroll
+        for (int j = 0; j < kXK; j++) wsh[w].a[j] = x.a[j];
+        wsh[w].drop = x.drop;
+        wsh[w].flags = (double)fl;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int Bb = kXBmin;
+        for (int i = 0; i < nw; i++) Bb = max(Bb, (int)wsh[i].B);
+        XPart r;
+        r.B = (double)Bb;
+        for (int j = 0; j < kXK; j++) r.a[j] = 0.0;
+        r.drop = 0.0;
+        int f = 0;
+        for (int i = 0; i < nw; i++) {  // <= 8 warps of bins below 2^(W+4) g: exact
+            const int d = Bb - (int)wsh[i].B;
+            for (int j = 0; j < kXK; j++) {
+                if (j + d < kXK)
+                    r.a[j + d] = __dadd_rn(r.a[j + d], wsh[i].a[j]);
+                else
+                    r.drop = __dadd_ru(r.drop, fabs(wsh[i].a[j]));
+            }
+            r.drop = __dadd_ru(r.drop, wsh[i].drop);
+            f |= (int)wsh[i].flags;
+        }
+        r.flags = (double)f;
+        out = r;
+    }
+}
+
+// Exact sum of `np` block parts into a correctly rounded double (one block
+// of 256 threads; the caller synchronises before and reads *result after).
+// Parts are shifted onto the largest top bin with two spare bins above it;
+// *certified = 0 when the drop bound leaves the rounding open or a flag is
+// set.  `sh` is shared scratch of at least 256 * (kXK + 3) doubles.
+constexpr int kXK2 = kXK + 2;
+__device__ inline void xparts_round(const XPart *parts, int np, double *sh, double *result, int *certified) {
+    __shared__ int s_B, s_flags;
+    const int t = threadIdx.x;
+    if (t == 0) {
+        int Bg = kXBmin, f = 0;
+        for (int i = 0; i < np; i++) {
+            Bg = max(Bg, (int)__ldcg(&parts[i].B));
+            f |= (int)__ldcg(&parts[i].flags);
+        }
+        s_B = Bg;
+        s_flags = f;
+    }
+    __syncthreads();
+    const int Bt = s_B + 2;  // top of the 6-bin layout
+    double c[kXK2], sig[kXK2], drop = 0.0;
+#pragma unroll
+    for (int j = 0; j < kXK2; j++) {
+        c[j] = 0.0;
+        sig[j] = 1.5 * pow2((Bt - j) * kXW + 52);
+    }
+    for (int i = t; i < np; i += blockDim.x) {
+        const int d = s_B - (int)__ldcg(&parts[i].B);
+        for (int j = 0; j < kXK; j++) {
+            const double v = __ldcg(&parts[i].a[j]);
+            const int k = j + d + 2;
+            if (k < kXK2)
+                c[k] = __dadd_rn(c[k], v);
+            else
+                drop = __dadd_ru(drop, fabs(v));
+        }
+        drop = __dadd_ru(drop, __ldcg(&parts[i].drop));
+        // a part's bins are below 2^(W+7) g (8 warps of normalised lanes) and c's
+        // below 2^(W-1) g after this carry: the next part adds exactly
+#pragma unroll
+        for (int j = kXK2 - 1; j >= 1; j--) {
+            const double q = __dsub_rn(__dadd_rn(c[j], sig[j - 1]), sig[j - 1]);
+            c[j] = __dsub_rn(c[j], q);
+            c[j - 1] = __dadd_rn(c[j - 1], q);
+        }
+    }
+    // every bin is now below 2^(W-1) g (the top two far below): 256 threads add exactly
+#pragma unroll
+    for (int j = 0; j < kXK2; j++) sh[j * blockDim.x + t] = c[j];
+    sh[kXK2 * blockDim.x + t] = drop;
+    __syncthreads();
+    for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+        if (t < s) {
+#pragma unroll
+            for (int j = 0; j < kXK2; j++)
+                sh[j * blockDim.x + t] = __dadd_rn(sh[j * blockDim.x + t], sh[j * blockDim.x + t + s]);
+            sh[kXK2 * blockDim.x + t] = __dadd_ru(sh[kXK2 * blockDim.x + t], sh[kXK2 * blockDim.x + t + s]);
+        }
+        __syncthreads();
+    }
+    if (t == 0) {
+        double terms[kXK2 + 1];
+        for (int j = 0; j < kXK2; j++) terms[j] = sh[j * blockDim.x];
+        const double D = sh[kXK2 * blockDim.x];
+        int ok = s_flags == 0;
+        double r = 0.0;
+        if (ok) {
+            if (D == 0.0) {
+                r = nearsum(kXK2, terms, 1);
+            } else {
+                double lo[kXK2 + 1], hi[kXK2 + 1];
+                for (int j = 0; j < kXK2; j++) lo[j] = hi[j] = terms[j];
+                lo[kXK2] = -D;
+                hi[kXK2] = D;
+                const double rl = nearsum(kXK2 + 1, lo, 1), rh = nearsum(kXK2 + 1, hi, 1);
+                ok = (dbits(rl) == dbits(rh));
+                r = rl;
+            }
+        }
+        *result = r;
+        *certified = ok;
+    }
+}
+
+}  // namespace ozb

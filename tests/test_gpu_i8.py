@@ -225,21 +225,22 @@ def test_i8_correctly_rounded_2048(fast, phi, oracle, handle, ozb, cuda):
 
 
 def test_i8_wait_timeout_reports_and_recovers(oracle, handle, ozb, cuda):
-    """A bounded device wait that runs out: with the INT8 kernel's wait limit cut to 1 ns, a wait gives up, the
-    call returns CUOZBLAS_STATUS_DEVICE_TIMEOUT (6) instead of hanging or faulting (the kernel lets its copies and
-    MMAs finish and frees its tensor memory first), and with the default limit restored the same call on the same
-    context returns the bits of the first call."""
+    """A bounded device wait that runs out: the INT8 kernel's producer holds back its copies (a test switch) and
+    the wait limit is 20 ms, so the tensor-core issuer's wait for its first stage gives up; the call returns
+    CUOZBLAS_STATUS_DEVICE_TIMEOUT (6) instead of hanging or faulting (the kernel frees its tensor memory first),
+    and with the switch and the default limit restored the same call on the same context returns the bits of the
+    first call."""
     m = n = k = 1024
     A = oracle.phi_matrix(m, k, 1.0, 1)
     B = oracle.phi_matrix(k, n, 1.0, 2)
     ref = run_i8(ozb, handle, cuda, A, B, m, n, k)  # also settles the shape's launch tuning
-    ozb.set_i8_wait_limit(1)
+    ozb.set_i8_wait_test(20_000_000, hold_copies=True)
     try:
         with pytest.raises(ozb.OzblasError) as e:
             run_i8(ozb, handle, cuda, A, B, m, n, k)
         assert e.value.code == 6
     finally:
-        ozb.set_i8_wait_limit(0)
+        ozb.set_i8_wait_test(0, hold_copies=False)
     cuda.cuda.synchronize()
     again = run_i8(ozb, handle, cuda, A, B, m, n, k)
     assert bits_equal(again, ref)

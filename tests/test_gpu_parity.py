@@ -664,3 +664,48 @@ def test_daxpy_public_entry(oracle, handle, ozb, cuda):
         with pytest.raises(ozb.OzblasError) as e:
             ozb.daxpy(handle, 8, alpha, dev(cuda, x), dy, incx=incx, incy=incy)
         assert e.value.code == 2
+
+
+# ---- the one-pass NearSum DOT (exact bins, certified rounding, proven counts) ----
+
+ONE_PASS_CASES = [
+    # name, n, builder(oracle, n) -> (x, y)
+    ("phi1", 1 << 20, lambda o, n: (o.phi_vector(n, 1.0, 1), o.phi_vector(n, 1.0, 2))),
+    ("phi4_wide", 300001, lambda o, n: (o.phi_vector(n, 4.0, 1), o.phi_vector(n, 4.0, 2))),
+    ("odd_tiny", 7, lambda o, n: (o.phi_vector(n, 2.0, 1), o.phi_vector(n, 2.0, 2))),
+    ("cancel", 100000, lambda o, n: (np.concatenate([o.phi_vector(n // 2, 1.0, 1)] * 2),
+                                      np.concatenate([o.phi_vector(n // 2, 1.0, 2), -o.phi_vector(n // 2, 1.0, 2)]))),
+    ("zeros_and_scale", 65536, lambda o, n: (np.where(np.arange(n) % 3 == 0, 0.0, o.phi_vector(n, 2.0, 1) * 2.0 ** 300),
+                                             o.phi_vector(n, 2.0, 2) * 2.0 ** -350)),
+    ("huge", 4096, lambda o, n: (o.phi_vector(n, 1.0, 1) * 2.0 ** 500, o.phi_vector(n, 1.0, 2) * 2.0 ** 510)),
+    ("tiny", 4096, lambda o, n: (o.phi_vector(n, 1.0, 1) * 2.0 ** -500, o.phi_vector(n, 1.0, 2) * 2.0 ** -480)),
+]
+
+
+@pytest.mark.parametrize("case", ONE_PASS_CASES, ids=lambda c: c[0])
+def test_ddot_nearsum_one_pass(case, oracle, handle, ozb, cuda, monkeypatch):
+    """NearSum DOT and NRM2: the one-pass path (2 launches when it answers) gives the oracle's bits and exec-info
+    counts, equal to the two-pass DOT's; wide ranges, cancellation, zeros, and products beyond the bins' range
+    (which hand the call to the two-pass DOT) included."""
+    name, n, build = case
+    x, y = build(oracle, n)
+    x, y = np.ascontiguousarray(x), np.ascontiguousarray(y)
+    dx, dy = dev(cuda, x), dev(cuda, y)
+    handle.sumMode = 1
+    l0 = handle.launch_count()
+    d = ozb.ddot(handle, n, dx, dy)
+    launches = handle.launch_count() - l0
+    r, info = oracle.ddot(make_flags(sumMode=1), x, y)
+    assert np.float64(d).view(np.int64) == np.float64(r).view(np.int64), (name, d, r)
+    assert (handle.nSplitA, handle.nSplitB) == (info.nSplitA, info.nSplitB)
+    nr = ozb.dnrm2(handle, n, dx)
+    nr_ref, _ = oracle.dnrm2(make_flags(sumMode=1), x)
+    assert np.float64(nr).view(np.int64) == np.float64(nr_ref).view(np.int64), (name, nr, nr_ref)
+    monkeypatch.setenv("OZBLAS_DOT_TWO_PASS", "1")
+    handle.read_env()
+    d2 = ozb.ddot(handle, n, dx, dy)
+    monkeypatch.delenv("OZBLAS_DOT_TWO_PASS")
+    handle.read_env()
+    assert np.float64(d2).view(np.int64) == np.float64(d).view(np.int64)
+    if name in ("phi1", "cancel", "odd_tiny"):
+        assert launches == 2, launches  # answered by the one-pass kernels
