@@ -9,8 +9,8 @@
 // the host's bits), every DOT's first pass (max and lowest set bit of its
 // vectors) is folded into the kernel that writes the vector (the p and r
 // updates, the SpMV's epilogue), and the scratch areas clean themselves, so
-// an iteration is eleven kernels with no host round trip.  K iterations are
-// captured once into a graph and replayed.
+// an iteration is eight kernels (five with NearSum, below) with no host round
+// trip.  K iterations are captured once into a graph and replayed.
 //
 // Every kernel reads a device gate: the iterations after convergence or
 // maxiter do nothing.  A fused step whose predicted chain is not proven
@@ -26,6 +26,7 @@
 
 #include "fused.h"
 #include "tc05.cuh"
+#include "xbins.cuh"
 
 namespace ozb {
 
@@ -108,6 +109,169 @@ __global__ void __launch_bounds__(256) k_cg_update_p(int n, double *__restrict__
 
 __global__ void k_cg_stamp(unsigned long long *t) { *t = tc::globaltimer(); }
 
+// ---- NearSum: the dots fused into their producers ----------------------------
+// With sumMode 1 each DOT of the iteration is RN of the exact dot product
+// whenever the reference's split of both vectors is complete
+// (split_complete, from the statistics the producers already gather), so
+// <p, q> is one exact pass over p and q that ends in alpha, and <r, r> rides
+// in the x / r update, whose last block computes beta, the history and the
+// gate: five kernels per iteration (proof, SpMV, <p, q> + alpha,
+// x / r + <r, r> + beta, p update) and no separate DOT passes.
+
+// Exact p . q of n elements into bins, U double2 pairs per lane per step.
+template <bool ALIGNED>
+__device__ __forceinline__ void cg_dot_stream(int n, const double *__restrict__ a, const double *__restrict__ b,
+                                              XAcc &acc) {
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    const int64_t iw = (int64_t)blockIdx.x * blockDim.x + (threadIdx.x & ~31);
+    if (ALIGNED) {
+        constexpr int U = 2;
+        const int64_t np = (int64_t)n >> 1;
+        const double2 *a2 = reinterpret_cast<const double2 *>(a);
+        const double2 *b2 = reinterpret_cast<const double2 *>(b);
+        const int64_t steps = iw < np ? (np - iw + U * stride - 1) / (U * stride) : 0;
+        int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+        for (int64_t s = 0; s < steps; s++, i += U * stride) {
+            double2 u[U], v[U];
+#pragma unroll
+            for (int k = 0; k < U; k++) {
+                const int64_t e = i + k * stride;
+                u[k] = e < np ? a2[e] : make_double2(0.0, 0.0);
+                v[k] = e < np ? b2[e] : make_double2(0.0, 0.0);
+            }
+            unsigned hi = 0u;
+#pragma unroll
+            for (int k = 0; k < U; k++) {
+                hi = max(hi, abs_hiword(__dmul_rn(u[k].x, v[k].x)));
+                hi = max(hi, abs_hiword(__dmul_rn(u[k].y, v[k].y)));
+            }
+            xacc_fit(acc, __reduce_max_sync(0xffffffffu, hi));
+#pragma unroll
+            for (int k = 0; k < U; k++) {
+                xacc_product(acc, u[k].x, v[k].x);
+                xacc_product(acc, u[k].y, v[k].y);
+            }
+            if ((s & 15) == 15) xacc_normalize(acc);  // every 64 products per lane
+        }
+        if ((n & 1) && blockIdx.x == 0 && threadIdx.x < 32) {  // the odd last element, one warp
+            const double ae = threadIdx.x == 0 ? a[n - 1] : 0.0, be = threadIdx.x == 0 ? b[n - 1] : 0.0;
+            xacc_normalize(acc);
+            xacc_fit(acc, __reduce_max_sync(0xffffffffu, abs_hiword(__dmul_rn(ae, be))));
+            xacc_product(acc, ae, be);
+        }
+    } else {
+        const int64_t steps = iw < n ? ((int64_t)n - iw + stride - 1) / stride : 0;
+        int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+        for (int64_t s = 0; s < steps; s++, i += stride) {
+            const double ae = i < n ? a[i] : 0.0, be = i < n ? b[i] : 0.0;
+            xacc_fit(acc, __reduce_max_sync(0xffffffffu, abs_hiword(__dmul_rn(ae, be))));
+            xacc_product(acc, ae, be);
+            if ((s & 63) == 63) xacc_normalize(acc);
+        }
+    }
+}
+
+__device__ __forceinline__ VecStats load_stats(const VecStats *g) {
+    VecStats v;
+    for (int i = 0; i < 2; i++) {
+        v.mx[i] = __ldcg(&g->mx[i]);
+        v.lsb[i] = __ldcg(&g->lsb[i]);
+        v.bad[i] = __ldcg(&g->bad[i]);
+    }
+    return v;
+}
+
+// tmp = <p, q> and alpha = dold / tmp.  The statistics of p (from the p
+// update) and of q (from the SpMV) are in dpq->vs; they are consumed here.
+template <bool ALIGNED>
+__global__ void __launch_bounds__(256) k_cg_pq(int n, const double *__restrict__ p, const double *__restrict__ q,
+                                               CgDev *d, DotScratch *dpq, const CsrScratch *cs, XReduce *xr, int rho,
+                                               int maxS) {
+    __shared__ double res_sh;
+    __shared__ int cert_sh;
+    if (!d->gate) return;  // uniform
+    if (!cs->valid) {      // the SpMV did not run: the host path takes this iteration
+        if (blockIdx.x == 0 && threadIdx.x == 0) {
+            d->broken = 2;
+            d->gate = 0;
+        }
+        return;
+    }
+    XAcc acc;
+    xacc_init(acc);
+    cg_dot_stream<ALIGNED>(n, p, q, acc);
+    if (!xreduce_finish(acc, xr, &res_sh, &cert_sh)) return;
+    if (threadIdx.x == 0) {
+        const VecStats vs = load_stats(&dpq->vs);
+        if (cert_sh && split_complete(vs, 0, rho, maxS) && split_complete(vs, 1, rho, maxS)) {
+            d->alpha = d->dold / fma(1.0, res_sh, 0.0 * 0.0);
+        } else {
+            d->broken = 1;
+            d->gate = 0;
+        }
+        dpq->vs = VecStats{};
+    }
+}
+
+// x = fma(alpha, p, x), r = fma(-alpha, q, r), dnew = <r, r> (exact, in the
+// same pass), then k_cg_beta's step in the last block.
+__global__ void __launch_bounds__(256) k_cg_xr_rr(int n, double *__restrict__ x, double *__restrict__ r,
+                                                  const double *__restrict__ p, const double *__restrict__ q,
+                                                  CgDev *d, VecStats *rs, XReduce *xr, int rho, int maxS,
+                                                  double *res, unsigned long long *stamp) {
+    __shared__ double red[8];
+    __shared__ double res_sh;
+    __shared__ int cert_sh;
+    if (!d->gate) {  // uniform
+        if (blockIdx.x == 0 && threadIdx.x == 0) d->ran = 0;
+        return;
+    }
+    const double al = d->alpha;
+    double mx = 0.0;
+    int lsb = 0, bad = 0;
+    XAcc acc;
+    xacc_init(acc);
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    const int64_t iw = (int64_t)blockIdx.x * blockDim.x + (threadIdx.x & ~31);
+    const int64_t steps = iw < n ? ((int64_t)n - iw + stride - 1) / stride : 0;
+    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    for (int64_t s = 0; s < steps; s++, i += stride) {
+        double ri = 0.0;
+        if (i < n) {
+            x[i] = fma(al, p[i], x[i]);
+            ri = fma(-al, q[i], r[i]);
+            r[i] = ri;
+            scan_elem(ri, mx, lsb, bad);
+        }
+        xacc_fit(acc, __reduce_max_sync(0xffffffffu, abs_hiword(__dmul_rn(ri, ri))));
+        xacc_product(acc, ri, ri);
+        if ((s & 63) == 63) xacc_normalize(acc);
+    }
+    scan_commit(rs, 0, mx, lsb, bad, red);
+    if (!xreduce_finish(acc, xr, &res_sh, &cert_sh)) return;
+    if (threadIdx.x == 0) {
+        const VecStats vs = load_stats(rs);
+        *rs = VecStats{};
+        if (!(cert_sh && split_complete(vs, 0, rho, maxS))) {
+            d->broken = 3;  // <r, r> not certified
+            d->gate = 0;
+            d->ran = 0;
+            return;
+        }
+        const double dnew = fma(1.0, res_sh, 0.0 * 0.0);
+        const double resi = sqrt(dnew);
+        d->beta = dnew / d->dold;
+        d->dold = dnew;
+        d->iter += 1;
+        const double rel = resi / d->nrmb;
+        res[d->iter] = rel;
+        stamp[d->iter] = tc::globaltimer();
+        d->ran = 1;
+        if (rel < d->tol) d->stop = 1;
+        d->gate = (!d->stop && d->iter < d->maxiter) ? 1 : 0;
+    }
+}
+
 // Run the CG iterations from the state (x, r, p, dold) after `iter`
 // iterations.  `host_head` runs an iteration's SpMV, <p, q> and x, r updates
 // through the host path, `host_tail` the rest (it reports convergence);
@@ -130,6 +294,8 @@ int cg_graph(cuozblasHandle_t *h, int n, const double *val, const int *colind, c
     CgDev *d = ar.take<CgDev>(1);
     DotScratch *dpq = ar.take<DotScratch>(1), *drr = ar.take<DotScratch>(1);
     CsrScratch *cs = ar.take<CsrScratch>(1);
+    const bool fused_dots = h->sumMode == 1 && !st->env.dot_two_pass;
+    XReduce *xpq = fused_dots ? ar.take<XReduce>(1) : nullptr, *xrr = fused_dots ? ar.take<XReduce>(1) : nullptr;
     int *slow = ar.take<int>(nn + 1);
     double *res_dev = ar.take<double>((uint64_t)maxiter + 1);
     unsigned long long *stamp_dev = ar.take<unsigned long long>((uint64_t)maxiter + 2);
@@ -201,6 +367,10 @@ int cg_graph(cuozblasHandle_t *h, int n, const double *val, const int *colind, c
         OZB_CHECK(cudaMemsetAsync(dpq, 0, sizeof(DotScratch), s));
         OZB_CHECK(cudaMemsetAsync(drr, 0, sizeof(DotScratch), s));
         OZB_CHECK(cudaMemsetAsync(cs, 0, sizeof(CsrScratch), s));
+        if (fused_dots) {
+            OZB_CHECK(cudaMemsetAsync(xpq, 0, sizeof(XReduce), s));
+            OZB_CHECK(cudaMemsetAsync(xrr, 0, sizeof(XReduce), s));
+        }
         OZB_TRY(vec_stats_launch(s, nsm, n, p, &cs->vs, 0));
         OZB_TRY(vec_stats_launch(s, nsm, n, p, &dpq->vs, 0));
         OZB_CHECK(cudaStreamSynchronize(s));
@@ -214,14 +384,26 @@ int cg_graph(cuozblasHandle_t *h, int n, const double *val, const int *colind, c
     const int ub = (int)((nn + 255) / 256) < nsm * 8 ? (int)((nn + 255) / 256) : nsm * 8;
     CG_CHECK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
     int cap = CUOZBLAS_STATUS_SUCCESS;
+    const bool aligned_pq = ((reinterpret_cast<uintptr_t>(p) | reinterpret_cast<uintptr_t>(q)) & 15u) == 0;
+    const int xb = ub < kXMaxBlocks ? ub : kXMaxBlocks;  // blocks of the fused dot kernels
     for (int k = 0; k < K && !cap; k++) {
         cap = csr_proof_launch(s, n, p, rho, maxS, cs, &d->gate);
         if (!cap) cap = csr_rows_launch(s, spmv, cs, slow, nslow, &dpq->vs, 1, terms, &d->gate);
-        if (!cap) cap = dot_tree_launch(s, nsm, n, p, q, rho, maxS, h->sumMode, dpq, &d->gate, state(h)->env.dot_tree);
-        k_cg_alpha<<<1, 1, 0, s>>>(d, dpq, cs);
-        k_cg_update_xr<<<ub, 256, 0, s>>>(n, x, r, p, q, d, &drr->vs);
-        if (!cap) cap = dot_tree_launch(s, nsm, n, r, r, rho, maxS, h->sumMode, drr, &d->gate, state(h)->env.dot_tree);
-        k_cg_beta<<<1, 1, 0, s>>>(d, drr, res_dev, stamp_dev);
+        if (fused_dots) {
+            if (aligned_pq)
+                k_cg_pq<true><<<xb, 256, 0, s>>>(n, p, q, d, dpq, cs, xpq, rho, maxS);
+            else
+                k_cg_pq<false><<<xb, 256, 0, s>>>(n, p, q, d, dpq, cs, xpq, rho, maxS);
+            k_cg_xr_rr<<<xb, 256, 0, s>>>(n, x, r, p, q, d, &drr->vs, xrr, rho, maxS, res_dev, stamp_dev);
+        } else {
+            if (!cap)
+                cap = dot_tree_launch(s, nsm, n, p, q, rho, maxS, h->sumMode, dpq, &d->gate, state(h)->env.dot_tree);
+            k_cg_alpha<<<1, 1, 0, s>>>(d, dpq, cs);
+            k_cg_update_xr<<<ub, 256, 0, s>>>(n, x, r, p, q, d, &drr->vs);
+            if (!cap)
+                cap = dot_tree_launch(s, nsm, n, r, r, rho, maxS, h->sumMode, drr, &d->gate, state(h)->env.dot_tree);
+            k_cg_beta<<<1, 1, 0, s>>>(d, drr, res_dev, stamp_dev);
+        }
         k_cg_update_p<<<ub, 256, 0, s>>>(n, p, r, d, &cs->vs, &dpq->vs);
     }
     const cudaError_t ce = cudaStreamEndCapture(s, &graph);
@@ -231,7 +413,7 @@ int cg_graph(cuozblasHandle_t *h, int n, const double *val, const int *colind, c
     }
     CG_CHECK(ce);
     CG_CHECK(cudaGraphInstantiate(&exec, graph, 0));
-    const int per_iter = 8 + (nslow > 0 ? (nslow + 8191) / 8192 : 0);
+    const int per_iter = (fused_dots ? 5 : 8) + (nslow > 0 ? (nslow + 8191) / 8192 : 0);
     // device clock against the host's, for the elapsed-time history
     k_cg_stamp<<<1, 1, 0, s>>>(stamp_dev + maxiter + 1);
     unsigned long long dev0 = 0;

@@ -125,6 +125,27 @@ __device__ inline void make_plan(const VecStats *vs, int rho, int maxS, bool sam
     pl.L = L;
 }
 
+// Whether the reference's split of a vector with these statistics is complete
+// (the remainder after its last level is zero), from the predicted chain
+// tau_{s+1} = tau_s + rho - 54.  The actual chain descends no slower (the
+// remainder after level s is at most g_s / 2), so its grids are no coarser
+// and its first all-zero level is at most the predicted z: z <= maxS - 1
+// makes the split complete whatever the actual chain.  False for Inf / NaN,
+// a sigma beyond the double range, or a grid below the normal range (the
+// caller then takes a path that follows the reference step by step).
+__device__ __forceinline__ bool split_complete(const VecStats &vs, int v, int rho, int maxS) {
+    if (vs.bad[v]) return false;
+    const double mx = vs.mx[v];
+    if (!(mx <= 1.7976931348623157e308)) return false;
+    if (vs.lsb[v] == 0) return true;  // every element is zero
+    const int tau0 = tau_rule(mx);
+    if (rho + tau0 > 1023) return false;
+    const int d = 54 - rho, G0 = rho + tau0 - 53;
+    const int num = G0 - (kLsbBias - vs.lsb[v]);
+    const int z = num <= 0 ? 0 : (num + d - 1) / d;
+    return z <= maxS - 1 && G0 - z * d >= -1022;
+}
+
 // The plan straight from the first pass's statistics, computed by thread 0
 // into shared memory (the caller synchronises the block).  Every CTA of the
 // kernel that consumes the statistics does this; its last CTA zeroes them.

@@ -31,14 +31,11 @@
 namespace ozb {
 
 constexpr int kXThreads = 256;
-constexpr int kXMaxBlocks = 1184;  // 148 SMs x 8
 
 struct DotExactScratch {
-    XPart part[kXMaxBlocks];  // one bin set per block of k_dot_exact
-    unsigned ticket;           // blocks of k_dot_exact that are done
+    XReduce xr;                // the blocks' bins of k_dot_exact
     unsigned ticket2;          // blocks of k_dot_prove that are done
     int certified;
-    int pad;
     double result;             // certified RN(x . y)
     unsigned proven[2];        // levels whose predicted tau some element proved
 };
@@ -50,8 +47,8 @@ __global__ void __launch_bounds__(kXThreads) k_dot_exact(int n, const double *__
                                                          const double *__restrict__ y, DotScratch *__restrict__ sc,
                                                          DotExactScratch *__restrict__ xs) {
     __shared__ double red[kXThreads / 32];
-    __shared__ XPart wsh[kXThreads / 32];
-    __shared__ int last;
+    __shared__ double res_sh;
+    __shared__ int cert_sh;
     XAcc acc;
     xacc_init(acc);
     double mx = 0.0, my = 0.0;
@@ -121,16 +118,11 @@ __global__ void __launch_bounds__(kXThreads) k_dot_exact(int n, const double *__
     }
     scan_commit(&sc->vs, 0, mx, lx, bx, red);
     if (!SAME) scan_commit(&sc->vs, 1, my, ly, by, red);
-    xacc_block_reduce(acc, wsh, xs->part[blockIdx.x]);
-    __threadfence();
-    __syncthreads();
-    if (threadIdx.x == 0) last = atomicAdd(&xs->ticket, 1u) == gridDim.x - 1;
-    __syncthreads();
-    if (!last) return;
-    __threadfence();
-    __shared__ double sh[kXThreads * (kXK2 + 1)];
-    xparts_round(xs->part, gridDim.x, sh, &xs->result, &xs->certified);
-    if (threadIdx.x == 0) xs->ticket = 0u;
+    if (!xreduce_finish(acc, &xs->xr, &res_sh, &cert_sh)) return;
+    if (threadIdx.x == 0) {
+        xs->result = res_sh;
+        xs->certified = cert_sh;
+    }
 }
 
 // ---- the chain proof, with early exit -------------------------------------

@@ -255,4 +255,36 @@ __device__ inline void xparts_round(const XPart *parts, int np, double *sh, doub
     }
 }
 
+constexpr int kXMaxBlocks = 1184;  // block parts a reduction holds (148 SMs x 8)
+
+// Scratch of one one-pass exact reduction: the blocks' parts and the ticket
+// that finds the last block (self-cleaning: the last block resets it).
+struct XReduce {
+    XPart part[kXMaxBlocks];
+    unsigned ticket;
+    int pad;
+};
+
+// End of a one-pass exact reduction over gridDim.x <= kXMaxBlocks blocks of
+// 256 threads (every thread calls this): each block folds its lanes' bins
+// into its part; returns true, in every thread of the last block only, with
+// the certified rounding of the total in *result and *certified (shared
+// memory, valid for all threads of that block).
+__device__ inline bool xreduce_finish(XAcc &acc, XReduce *xr, double *result, int *certified) {
+    __shared__ XPart wsh[8];
+    __shared__ int last;
+    __shared__ double sh[256 * (kXK2 + 1)];
+    xacc_block_reduce(acc, wsh, xr->part[blockIdx.x]);
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) last = atomicAdd(&xr->ticket, 1u) == gridDim.x - 1;
+    __syncthreads();
+    if (!last) return false;
+    __threadfence();
+    xparts_round(xr->part, gridDim.x, sh, result, certified);
+    if (threadIdx.x == 0) xr->ticket = 0u;
+    __syncthreads();
+    return true;
+}
+
 }  // namespace ozb

@@ -707,5 +707,7 @@ def test_ddot_nearsum_one_pass(case, oracle, handle, ozb, cuda, monkeypatch):
     monkeypatch.delenv("OZBLAS_DOT_TWO_PASS")
     handle.read_env()
     assert np.float64(d2).view(np.int64) == np.float64(d).view(np.int64)
-    if name in ("phi1", "cancel", "odd_tiny"):
+    if name in ("phi1", "odd_tiny"):
         assert launches == 2, launches  # answered by the one-pass kernels
+    # "cancel" sums to exactly zero while the bins hold the products' lowest bits only up to a bound: the
+    # rounding of a sum within that bound of zero is not certified, so the two-pass DOT answers (same bits)
