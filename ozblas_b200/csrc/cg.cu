@@ -190,7 +190,7 @@ __global__ void __launch_bounds__(256) k_cg_pq(int n, const double *__restrict__
     __shared__ double res_sh;
     __shared__ int cert_sh;
     if (!d->gate) return;  // uniform
-    if (!cs->valid) {      // the SpMV did not run: the host path takes this iteration
+    if (!cs->valid || cs->rn_declined) {  // the SpMV did not run: the host path takes this iteration
         if (blockIdx.x == 0 && threadIdx.x == 0) {
             d->broken = 2;
             d->gate = 0;
@@ -385,10 +385,14 @@ int cg_graph(cuozblasHandle_t *h, int n, const double *val, const int *colind, c
     CG_CHECK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
     int cap = CUOZBLAS_STATUS_SUCCESS;
     const bool aligned_pq = ((reinterpret_cast<uintptr_t>(p) | reinterpret_cast<uintptr_t>(q)) & 15u) == 0;
-    const int xb = ub < kXMaxBlocks ? ub : kXMaxBlocks;  // blocks of the fused dot kernels
+    int xb = ub < nsm * 4 ? ub : nsm * 4;  // blocks of the fused dot kernels (one part each)
+    if (xb > kXMaxBlocks) xb = kXMaxBlocks;
+    const bool rn_rows = fused_dots && csr_rn_applies(spmv) && !st->env.csr_slices;
     for (int k = 0; k < K && !cap; k++) {
         cap = csr_proof_launch(s, n, p, rho, maxS, cs, &d->gate);
-        if (!cap) cap = csr_rows_launch(s, spmv, cs, slow, nslow, &dpq->vs, 1, terms, &d->gate);
+        if (!cap)
+            cap = rn_rows ? csr_rn_launch(s, spmv, cs, slow, nslow, &dpq->vs, 1, terms, &d->gate)
+                          : csr_rows_launch(s, spmv, cs, slow, nslow, &dpq->vs, 1, terms, &d->gate);
         if (fused_dots) {
             if (aligned_pq)
                 k_cg_pq<true><<<xb, 256, 0, s>>>(n, p, q, d, dpq, cs, xpq, rho, maxS);

@@ -110,6 +110,8 @@ __global__ void __launch_bounds__(256) k_csr_proof(int n, const double *__restri
     const int valid = pl.valid && (__ldcg(&sc->proven) & need) == need;
     for (int s = 0; s < kCsrLv; s++) sc->sigma[s] = pl.sig[0][s];
     sc->nB = pl.ns[0];
+    sc->xcomplete = valid && pl.z[0] <= pl.ns[0] - 1;
+    sc->rn_declined = 0;
     sc->valid = valid;
     // leave the proof and the statistics zeroed for the next use (every block
     // has read the statistics: the ticket comes after)
@@ -849,6 +851,235 @@ __global__ void __launch_bounds__(kCsrThreads, NA >= 4 ? 3 : 4)
     if (ystats) scan_commit(ystats, ystats_index, smx, slsb, sbad, red);
 }
 
+// ---------------------------------------------------------------------------
+// NearSum rows, correctly rounded.  With sumMode 1 the reference's row result
+// is NearSum over the row's slice-pair products (src/cpu/ozblas_csrmv.cpp:
+// 100-160, src/cpu/ozblas_sum.cpp:10-112).  Each pair product is exact when
+// its slices' bits fit: an A slice is at most 2^(53 - rho_A) grid units
+// (times the shift), an x slice at most 2^(53 - rho_x), so a row of len
+// entries sums to at most len 2^(106 - rho_A - rho_x + log2 shift) units of
+// the product grid, exact below 2^53.  With both splits complete the pair
+// products then add up to the exact row dot product, and NearSum returns its
+// correct rounding.  So a row that meets both conditions is computed as
+// RN(sum_j a_j x_j) directly: TwoProd of each entry gives exact terms, the
+// certified TwoSum cascade (crsum.h) rounds them, NearSum when it cannot
+// certify.  Rows that do not meet them (or whose products leave the range
+// TwoProd keeps exact) are deferred to the per-row general kernel.
+// ---------------------------------------------------------------------------
+constexpr int kCsrSlowChunk = 8192;  // rows per launch of the per-row general kernel
+
+__device__ __forceinline__ bool rn_row_dot(const double (&v)[kCsrRowMax], const double (&xv)[kCsrRowMax], int len,
+                                           double &out) {
+    double t[2 * kCsrRowMax];
+    CrSum cs;
+    bool ok = true;
+#pragma unroll
+    for (int e = 0; e < kCsrRowMax; e++) {
+        const double p = e < len ? __dmul_rn(v[e], xv[e]) : 0.0;
+        const double er = e < len ? __fma_rn(v[e], xv[e], -p) : 0.0;
+        const double ap = fabs(p);
+        if (e < len && ((ap < 0x1p-969 && v[e] != 0.0 && xv[e] != 0.0) || !(ap < 0x1p1023))) ok = false;
+        t[2 * e] = p;
+        t[2 * e + 1] = er;
+        cs.add(p);
+        cs.add(er);
+    }
+    if (!ok) return false;
+    if (cs.finish(out)) return true;
+    out = nearsum(2 * kCsrRowMax, t, 1);
+    return true;
+}
+
+__host__ __device__ __forceinline__ int ceil_log2_small(int v) {
+    int c = 0;
+    while ((1 << c) < v) c++;
+    return c;
+}
+
+template <int NA>
+__global__ void __launch_bounds__(kCsrThreads, 4)
+    k_csrmv_rn(int m, int n, const double *__restrict__ val, const int *__restrict__ colind,
+               const int *__restrict__ rowptr, const double *__restrict__ x, int shift, int lg_shift, int rho_x,
+               int epsmode, int maxS, double alpha, double beta, double *__restrict__ y, CsrScratch *__restrict__ sc,
+               int *__restrict__ slow_rows, int append_slow, VecStats *__restrict__ ystats, int ystats_index,
+               const int *__restrict__ gate) {
+    if (gate && *gate == 0) return;  // uniform: a captured solver step that is switched off
+    __shared__ __align__(16) LeanSlot slot[2];
+    __shared__ double red[kCsrThreads / 32];
+    const int t = threadIdx.x;
+    const int ntiles = (m + kCsrThreads - 1) / kCsrThreads;
+    if (!sc->valid) return;  // uniform: the caller runs the general path
+    if (!sc->xcomplete) {    // uniform: the lean kernel computes the slices instead
+        if (blockIdx.x == 0 && t == 0) sc->rn_declined = 1;
+        return;
+    }
+    int tile = blockIdx.x;
+    if (tile >= ntiles) return;  // uniform
+
+    auto rows_of = [&](int tl) { return (m - tl * kCsrThreads < kCsrThreads) ? m - tl * kCsrThreads : kCsrThreads; };
+    auto issue_rp = [&](int tl, LeanSlot &S) {
+        const int r0 = tl * kCsrThreads, nrow = rows_of(tl);
+        if (t < nrow) cp_async4(&S.rp[t], rowptr + r0 + t);
+        if (t == 0) cp_async4(&S.rp[nrow], rowptr + r0 + nrow);
+    };
+    auto issue_vals = [&](int tl, LeanSlot &S) {  // needs S.rp
+        const int r0 = tl * kCsrThreads;
+        if (t >= rows_of(tl)) return;
+        const double *dummy = y + r0 + t;  // a valid address for copies that read nothing
+        cp_async8(&S.yold[t], dummy);
+        const int lo = S.rp[t], len = S.rp[t + 1] - lo;
+        if (len > kCsrRowMax) return;
+#pragma unroll
+        for (int e = 0; e < kCsrRowMax; e++) {
+            const bool in = e < len;
+            cp_async8_zfill(&S.val[lean_pos(t, e)], in ? (const void *)(val + lo + e) : (const void *)dummy,
+                            in ? 8u : 0u);
+            cp_async4_zfill(&S.col[t * kCsrRowMax + e], in ? (const void *)(colind + lo + e) : (const void *)dummy,
+                            in ? 4u : 0u);
+        }
+    };
+    auto issue_gathers = [&](int tl, LeanSlot &S) {  // needs S.rp and S.col
+        const int r0 = tl * kCsrThreads;
+        if (t >= rows_of(tl)) return;
+        const double *dummy = y + r0 + t;
+        const int lo = S.rp[t], len = S.rp[t + 1] - lo;
+        if (len > kCsrRowMax) return;
+        const int4 c0 = *reinterpret_cast<const int4 *>(&S.col[t * kCsrRowMax]);
+        const int4 c1 = *reinterpret_cast<const int4 *>(&S.col[t * kCsrRowMax + 4]);
+        const int cc[kCsrRowMax] = {c0.x, c0.y, c0.z, c0.w, c1.x, c1.y, c1.z, c1.w};
+#pragma unroll
+        for (int e = 0; e < kCsrRowMax; e++) {
+            const bool in = e < len && n > 0;
+            cp_async8_zfill(&S.xg[lean_pos(t, e)], in ? (const void *)(x + cc[e]) : (const void *)dummy,
+                            in ? 8u : 0u);
+        }
+    };
+
+    issue_rp(tile, slot[0]);
+    cp_async_commit();
+    cp_async_wait_all();
+    __syncthreads();
+    issue_vals(tile, slot[0]);
+    cp_async_commit();
+    cp_async_wait_all();
+    __syncthreads();
+    issue_gathers(tile, slot[0]);
+    if (tile + (int)gridDim.x < ntiles) issue_rp(tile + gridDim.x, slot[1]);
+    cp_async_commit();
+
+    double smx = 0.0;
+    int slsb = 0, sbad = 0, zmax = 0;
+    for (int j = 0; tile < ntiles; j++, tile += gridDim.x) {
+        LeanSlot &S = slot[j & 1], &N = slot[(j & 1) ^ 1];
+        const int nxt = tile + gridDim.x;
+        cp_async_wait_all();
+        __syncthreads();
+        if (nxt < ntiles) issue_vals(nxt, N);
+        cp_async_commit();
+        // ---- phase 1: the row's own split: complete, and exact slice products
+        const int r0 = tile * kCsrThreads, nrow = rows_of(tile);
+        const int row = r0 + t;
+        const bool active = t < nrow;
+        int len = 0;
+        if (active) len = S.rp[t + 1] - S.rp[t];
+        // `listed`: a row the slice kernel defers too (longer than 8, more than NA
+        // levels, Inf / NaN); with a fixed list (append_slow = 0) its caller
+        // computes it.  `defer`: a row this kernel cannot give the reference's
+        // bits (incomplete split, possibly inexact slice products, TwoProd out of
+        // range): appended, or with a fixed list the whole product is declined.
+        bool listed = active && len > kCsrRowMax, defer = false;
+        bool work = active && !listed;
+        const double yold = active ? S.yold[t] : 0.0;
+        if (work) {
+            // len 2^(106 - rho_A - rho_x + log2 shift) < 2^53 in product-grid units
+            if (len > 0 && ceil_log2_small(len) + 106 - rho_rule(len, epsmode) - rho_x + lg_shift > 53) defer = true;
+            double r[kCsrRowMax], sa[kCsrRowMax][NA];
+            lean_read(S.val, t, r);
+            int na = 0, z = 0;
+            if (!lean_chain<NA>(r, len, shift, epsmode, maxS, sa, na, z))
+                listed = true;  // more levels than held, or Inf / NaN
+            else if (len > 0 && z >= maxS)
+                defer = true;   // an incomplete split
+            if (!listed && !defer) zmax = z > zmax ? z : zmax;
+        }
+        cp_async_wait_all();
+        __syncthreads();
+        if (nxt < ntiles) issue_gathers(nxt, N);
+        if (nxt + (int)gridDim.x < ntiles) issue_rp(nxt + gridDim.x, S);
+        cp_async_commit();
+        // ---- phase 2: the correctly rounded row dot
+        work = work && !listed && !defer;
+        if (work) {
+            double v[kCsrRowMax], xv[kCsrRowMax], tsum = 0.0;
+            lean_read(S.val, t, v);
+            lean_read(S.xg, t, xv);
+            if (rn_row_dot(v, xv, len, tsum)) {
+                const double ynew = fma(alpha, tsum, beta * yold);
+                y[row] = ynew;
+                if (ystats) scan_elem(ynew, smx, slsb, sbad);
+            } else {
+                defer = true;
+            }
+        }
+        if (append_slow) {
+            if (listed || defer) slow_rows[atomicAdd(&sc->nslow, 1)] = row;
+        } else if (defer) {
+            sc->rn_declined = 1;
+        }
+    }
+    cp_async_wait_all();
+    {
+        const int zw = __reduce_max_sync(0xffffffffu, zmax);
+        if ((t & 31) == 0 && zw > 0) atomicMax(&sc->zmax, zw);
+    }
+    if (ystats) scan_commit(ystats, ystats_index, smx, slsb, sbad, red);
+}
+
+bool csr_rn_applies(const CsrmvArgs &a) {
+    return a.sum_mode == 1 && a.epsmode == 0 && a.shift > 0 && (a.shift & (a.shift - 1)) == 0;
+}
+
+template <int NA>
+static void launch_rn(const CsrmvArgs &a, cudaStream_t s, CsrScratch *sc, int *slow, int append, VecStats *ystats,
+                      int ystats_index, const int *gate) {
+    static std::atomic<int> per_sm{0};  // resident CTAs per SM (once per instantiation)
+    int ps = per_sm.load();
+    if (ps == 0) {
+        int v = 0;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&v, k_csrmv_rn<NA>, kCsrThreads, 0);
+        ps = v > 0 ? v : 1;
+        per_sm.store(ps);
+    }
+    const int rb = (a.m + kCsrThreads - 1) / kCsrThreads;
+    const int cap = sm_count() * ps;
+    const int grid = rb < cap ? rb : cap;
+    const int lg_shift = 31 - __builtin_clz((unsigned)a.shift);
+    const int rho_x = rho_rule(a.n > 0 ? a.n : 1, a.epsmode);
+    k_csrmv_rn<NA><<<grid, kCsrThreads, 0, s>>>(a.m, a.n, a.val, a.colind, a.rowptr, a.x, a.shift, lg_shift, rho_x,
+                                                 a.epsmode, a.maxS, a.alpha, a.beta, a.y, sc, slow, append, ystats,
+                                                 ystats_index, gate);
+}
+
+int csr_rn_launch(cudaStream_t s, const CsrmvArgs &a, CsrScratch *sc, int *slow, int fixed_slow, VecStats *ystats,
+                  int ystats_index, double *terms, const int *gate) {
+    if (a.m <= 0) return CUOZBLAS_STATUS_SUCCESS;
+    const int append = fixed_slow < 0 ? 1 : 0;
+    // the levels per row held on chip match the slow-row list's (csr_slow_rows_launch)
+    if (a.na_hint > 0 && a.na_hint <= 2)
+        launch_rn<2>(a, s, sc, slow, append, ystats, ystats_index, gate);
+    else if (a.na_hint > 4)
+        launch_rn<6>(a, s, sc, slow, append, ystats, ystats_index, gate);
+    else
+        launch_rn<4>(a, s, sc, slow, append, ystats, ystats_index, gate);
+    for (int c0 = 0; c0 < fixed_slow; c0 += kCsrSlowChunk) {  // the listed rows (general per-row kernel)
+        const int nr = fixed_slow - c0 < kCsrSlowChunk ? fixed_slow - c0 : kCsrSlowChunk;
+        k_csrmv_slow<1><<<(nr + 127) / 128, 128, 0, s>>>(nr, slow + c0, a.val, a.colind, a.rowptr, a.x, a.shift,
+                                                        a.epsmode, a.maxS, a.alpha, a.beta, a.y, sc, terms, ystats,
+                                                        ystats_index, gate);
+    }
+    return cudaGetLastError() == cudaSuccess ? CUOZBLAS_STATUS_SUCCESS : CUOZBLAS_STATUS_CUDA_ERROR;
+}
+
 template <int SUM_MODE, int NA, int GX>
 static void launch_lean_g(int ntiles, cudaStream_t s, const CsrmvArgs &a, CsrScratch *sc, int *slow, int append,
                           VecStats *ys, int yi, const int *gate) {
@@ -930,7 +1161,6 @@ int csr_proof_launch(cudaStream_t s, int n, const double *x, int rho, int maxS, 
 
 // The row kernel, and with fixed_slow > 0 the deferred rows of that list
 // (terms: NearSum workspace of kCsrSlowChunk rows).
-constexpr int kCsrSlowChunk = 8192;
 int csr_rows_launch(cudaStream_t s, const CsrmvArgs &a, CsrScratch *sc, int *slow, int fixed_slow, VecStats *ystats,
                     int ystats_index, double *terms, const int *gate) {
     if (a.m <= 0) return CUOZBLAS_STATUS_SUCCESS;
@@ -999,14 +1229,26 @@ int csrmv_fused(cuozblasHandle_t *h, int m, int n, double alpha, const double *v
     OZB_TRY(csr_proof_launch(s, n, x, rho, maxS, sc, nullptr));
     const CsrmvArgs args{m, n, alpha, beta, val, colind, rowptr, x, y, shift, h->splitEpsMode, maxS, h->sumMode,
                          na_hint};
+    // NearSum: correctly rounded exact row dots where the splits allow (the
+    // slices otherwise, and when x's split turns out incomplete)
+    const bool rn = csr_rn_applies(args) && !st->env.csr_slices;
     if (m > 0) counted(h);
-    OZB_TRY(csr_rows_launch(s, args, sc, slow, -1, nullptr, 0, nullptr, nullptr));
-    int res[4];  // valid, nB, nslow, zmax (partial until the deferred rows ran)
+    if (rn)
+        OZB_TRY(csr_rn_launch(s, args, sc, slow, -1, nullptr, 0, nullptr, nullptr));
+    else
+        OZB_TRY(csr_rows_launch(s, args, sc, slow, -1, nullptr, 0, nullptr, nullptr));
+    int res[6];  // valid, nB, nslow, zmax (partial until the deferred rows ran), xcomplete, rn_declined
     OZB_CHECK(cudaMemcpyAsync(res, &sc->valid, sizeof(res), cudaMemcpyDeviceToHost, s));
     OZB_CHECK(cudaStreamSynchronize(s));
     if (!res[0]) {
         ar.release(mk);
         return CUOZBLAS_STATUS_SUCCESS;  // y untouched: general path
+    }
+    if (rn && res[5]) {  // the row kernel declined: the slice kernel computes every row
+        if (m > 0) counted(h);
+        OZB_TRY(csr_rows_launch(s, args, sc, slow, -1, nullptr, 0, nullptr, nullptr));
+        OZB_CHECK(cudaMemcpyAsync(res, &sc->valid, sizeof(res), cudaMemcpyDeviceToHost, s));
+        OZB_CHECK(cudaStreamSynchronize(s));
     }
     const int nslow = res[2];
     if (nslow > 0) {

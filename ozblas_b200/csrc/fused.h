@@ -36,6 +36,8 @@ struct CsrScratch {
     unsigned proven;             // levels of x's chain whose predicted tau some element proved
     unsigned ticket;             // blocks of the proof pass that are done
     int valid, nB, nslow, zmax;  // zmax: first zero-remainder level of A, max over rows
+    int xcomplete;               // x's (proven) split is complete: its last remainder is zero
+    int rn_declined;             // the correctly rounded row kernel wrote nothing (x's split incomplete)
     double sigma[kCsrLv];        // x's proven sigmas
 };
 
@@ -77,5 +79,15 @@ int csr_slow_rows_launch(cudaStream_t s, int m, const double *val, const int *ro
 int csr_proof_launch(cudaStream_t s, int n, const double *x, int rho, int maxS, CsrScratch *sc, const int *gate);
 int csr_rows_launch(cudaStream_t s, const CsrmvArgs &a, CsrScratch *sc, int *slow, int fixed_slow,
                     VecStats *ystats, int ystats_index, double *terms, const int *gate);
+// NearSum rows as the correctly rounded exact row dots (csrmv_fused.cu): true
+// when the arguments allow it (sum mode 1, splitEpsMode 0, a power-of-two
+// shift).  The kernel writes nothing when x's split is incomplete
+// (sc->rn_declined); rows whose split is incomplete or whose slice products
+// could be inexact are appended to the slow list, or with a fixed list
+// (fixed_slow >= 0, whose rows the call computes afterwards) they decline the
+// whole product (sc->rn_declined).
+bool csr_rn_applies(const CsrmvArgs &a);
+int csr_rn_launch(cudaStream_t s, const CsrmvArgs &a, CsrScratch *sc, int *slow, int fixed_slow, VecStats *ystats,
+                  int ystats_index, double *terms, const int *gate);
 
 }  // namespace ozb

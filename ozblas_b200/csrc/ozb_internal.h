@@ -26,6 +26,7 @@ struct EnvSwitches {
     bool ds_simt = false;      // OZBLAS_DS_SIMT: <double,float,float> on the FP32 SIMT kernel
     bool dot_tree = false;     // OZBLAS_DOT_TREE: DOT pass 2 on the FP64 tree
     bool dot_two_pass = false; // OZBLAS_DOT_TWO_PASS: NearSum DOT on the two-pass path
+    bool csr_slices = false;   // OZBLAS_CSR_SLICES: NearSum CSRMV rows through their slices
     bool cg_no_graph = false;  // OZBLAS_CG_NO_GRAPH: CG iterations on the host loop
     bool dot_trace = false;    // OZBLAS_DOT_TRACE
     bool cg_trace = false;     // OZBLAS_CG_TRACE

@@ -181,13 +181,22 @@ __device__ inline void xparts_round(const XPart *parts, int np, double *sh, doub
     __shared__ int s_B, s_flags;
     const int t = threadIdx.x;
     if (t == 0) {
+        s_B = kXBmin;
+        s_flags = 0;
+    }
+    __syncthreads();
+    {  // the largest top bin and the flags, every thread over its parts
         int Bg = kXBmin, f = 0;
-        for (int i = 0; i < np; i++) {
+        for (int i = t; i < np; i += blockDim.x) {
             Bg = max(Bg, (int)__ldcg(&parts[i].B));
             f |= (int)__ldcg(&parts[i].flags);
         }
-        s_B = Bg;
-        s_flags = f;
+        Bg = __reduce_max_sync(0xffffffffu, Bg);
+        f = (int)__reduce_or_sync(0xffffffffu, (unsigned)f);
+        if ((t & 31) == 0) {
+            atomicMax(&s_B, Bg);
+            atomicOr(&s_flags, f);
+        }
     }
     __syncthreads();
     const int Bt = s_B + 2;  // top of the 6-bin layout

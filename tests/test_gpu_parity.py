@@ -711,3 +711,28 @@ def test_ddot_nearsum_one_pass(case, oracle, handle, ozb, cuda, monkeypatch):
         assert launches == 2, launches  # answered by the one-pass kernels
     # "cancel" sums to exactly zero while the bins hold the products' lowest bits only up to a bound: the
     # rounding of a sum within that bound of zero is not certified, so the two-pass DOT answers (same bits)
+
+
+@pytest.mark.parametrize("phi", [1.0, 4.0])
+def test_dcsrmv_nearsum_rows_equal_slices(phi, oracle, handle, ozb, cuda, monkeypatch):
+    """NearSum CSRMV: the correctly rounded exact row dots give the bits of the slice-pair path (and of the
+    oracle), with rows that the kernel must defer (longer than 8, deep splits) mixed in."""
+    g = 24
+    rowptr, colind = oracle.stencil7(g, g, g)
+    m = len(rowptr) - 1
+    val = oracle.phi_vector(len(colind), phi, 3)
+    val[::97] *= 2.0 ** -600  # rows spanning many levels
+    x = oracle.phi_vector(m, phi, 4)
+    y0 = oracle.phi_vector(m, 1.0, 5)
+    _csr_run(oracle, handle, ozb, cuda, rowptr, colind, val, x, y0, 1.5, -0.5, 1)
+    a = (handle.nSplitA, handle.nSplitB, handle.nSplitC)
+    dy = dev(cuda, y0)
+    monkeypatch.setenv("OZBLAS_CSR_SLICES", "1")
+    handle.read_env()
+    ozb.dcsrmv(handle, "n", m, m, len(val), 1.5, dev(cuda, val), dev(cuda, colind), dev(cuda, rowptr), dev(cuda, x),
+               -0.5, dy)
+    monkeypatch.delenv("OZBLAS_CSR_SLICES")
+    handle.read_env()
+    ref, _ = oracle.dcsrmv(make_flags(sumMode=1), m, m, 1.5, val, colind, rowptr, x, -0.5, y0)
+    assert bits_equal(host(dy), ref), first_diff(host(dy), ref)
+    assert (handle.nSplitA, handle.nSplitB, handle.nSplitC) == a
