@@ -448,6 +448,26 @@ int gemm_plain_core(cuozblasHandle_t *h, char ta, char tb, int m, int n, int k, 
     // ---- split ----  (phase events 0..4: start, A split, B split, products, sum)
     ev_record(h, 0);
     st->plain_timers = true;
+    // GEMV 'n' with NearSum: correctly rounded exact row dots, A read once
+    if (skinny_n && !dot && !is_trans(ta) && h->sumMode == 1 && fastMode == 0 && h->splitEpsMode == 0 &&
+        !state(h)->env.gemv_split && !state(h)->env.gemv_slices) {
+        bool done = false;
+        int nAv = 0, nBv = 0;
+        OZB_TRY(gemv_rn_n(h, m, k, A, lda, B, alpha, beta, C, &done, &nAv, &nBv));
+        if (done) {
+            const int ml = (nAv - 1) + (nBv - 1);
+            h->nSplitA = (float)nAv;
+            h->nSplitB = (float)nBv;
+            h->nSplitC = (float)(ml + 1 < nAv ? ml + 1 : nAv);
+            h->mbk = m;
+            h->nbk = n;
+            ev_record(h, 1);
+            ev_record(h, 2);
+            ev_record(h, 3);
+            ev_record(h, 4);
+            return CUOZBLAS_STATUS_SUCCESS;
+        }
+    }
     // GEMV 'n' (rows of A strided): fused split and products, A read nA + 2 times
     if (skinny_n && !dot && !is_trans(ta) && !state(h)->env.gemv_split) {
         const uint64_t mk0 = ar.mark();

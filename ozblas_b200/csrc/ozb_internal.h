@@ -27,6 +27,7 @@ struct EnvSwitches {
     bool dot_tree = false;     // OZBLAS_DOT_TREE: DOT pass 2 on the FP64 tree
     bool dot_two_pass = false; // OZBLAS_DOT_TWO_PASS: NearSum DOT on the two-pass path
     bool csr_slices = false;   // OZBLAS_CSR_SLICES: NearSum CSRMV rows through their slices
+    bool gemv_slices = false;  // OZBLAS_GEMV_SLICES: NearSum GEMV 'n' through its slices
     bool cg_no_graph = false;  // OZBLAS_CG_NO_GRAPH: CG iterations on the host loop
     bool dot_trace = false;    // OZBLAS_DOT_TRACE
     bool cg_trace = false;     // OZBLAS_CG_TRACE
@@ -224,6 +225,8 @@ int sum_rows_launch(cuozblasHandle_t *h, int m, int nA, int nB, int maxlevel, do
                     double beta, double *y, double *scratch);
 int gemv_fused_n(cuozblasHandle_t *h, int m, int n, const double *A, int lda, const double *xs, int ldx, int nB,
                  int rho, int maxS, int fastMode, double alpha, double beta, double *y, int *nA_out);
+int gemv_rn_n(cuozblasHandle_t *h, int m, int n, const double *A, int lda, const double *x, double alpha, double beta,
+              double *y, bool *done, int *nA, int *nB);
 
 // ---- plain GEMM core (gemm_plain.cu) ----
 int gemm_plain_core(cuozblasHandle_t *h, char ta, char tb, int m, int n, int k, double alpha, const double *A,

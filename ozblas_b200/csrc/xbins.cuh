@@ -4,8 +4,11 @@
 // With a complete split the reference's NearSum DOT returns RN of the exact
 // dot product (its slice-pair products are exact and NearSum rounds their
 // exact sum once), so any exact method gives its bits.  Here every product
-// x*y is the exact pair (p, e) of TwoProd (p = RN(x y), e = fma(x, y, -p)),
-// and each of p and e is cut onto the grids of K consecutive bins:
+// x*y is the exact pair (p, e) of TwoProd (p = RN(x y), e = fma(x, y, -p)).
+// The e are at most 2^-53 |p|: they are added in plain FP64 (es) next to a
+// rounded-up sum of their magnitudes (ea), and es's error is bounded by
+// 2^-28 ea (at most 2^22 additions on any path).  Each p is cut onto the
+// grids of K consecutive bins:
 //   bin j holds multiples of g_j = 2^((B - j) W),
 //   q_j = (r + sigma_j) - sigma_j with sigma_j = 1.5 * 2^((B - j) W + 52)
 // is r rounded to g_j (exact while |r| < 2^((B - j) W + 51)), r -= q_j is
@@ -15,8 +18,9 @@
 // up and the lowest bin leaves the window).  What a deposit leaves below the
 // lowest bin, and every bin that leaves the window, is added with upward
 // rounding to `drop`, an upper bound of everything not held exactly; the
-// final value is certified by rounding the held sum minus and plus that
-// bound (equal results: the rounding of the true sum is determined).
+// final value is certified by rounding the held sum (bins and es) minus and
+// plus the total bound (equal results: the rounding of the true sum is
+// determined).
 #pragma once
 #include "ozb_device.cuh"
 #include "sum.cuh"
@@ -33,6 +37,7 @@ struct XAcc {
     double a[kXK];      // bins, exact
     double sig[kXK];    // sigma_j of the current B
     double drop;        // upper bound of |everything not held| (rounded up)
+    double es, ea;      // sum of the TwoProd error terms, sum of their magnitudes (rounded up)
     int flags;          // 1: a product outside the range TwoProd keeps exact (tiny or huge)
 };
 
@@ -46,6 +51,7 @@ __device__ __forceinline__ void xacc_init(XAcc &x) {
 #pragma unroll
     for (int j = 0; j < kXK; j++) x.a[j] = 0.0;
     x.drop = 0.0;
+    x.es = x.ea = 0.0;
     x.flags = 0;
     xacc_sigmas(x);
 }
@@ -63,8 +69,7 @@ __device__ __forceinline__ void xacc_deposit(XAcc &x, double v) {
     x.drop = __dadd_ru(x.drop, fabs(r));
 }
 
-// The exact product x * y into the bins: p into bins 0..K-1, e (at most
-// 2^-53 |p| < 2^(B W), W < 53) into bins 1..K-1.
+// The product x * y: p into the bins, its exact error term into es / ea.
 __device__ __forceinline__ void xacc_product(XAcc &x, double a, double b) {
     const double p = __dmul_rn(a, b);
     const double e = __fma_rn(a, b, -p);
@@ -73,7 +78,8 @@ __device__ __forceinline__ void xacc_product(XAcc &x, double a, double b) {
     // or beyond the window's top (kXBmax)
     if ((ap < 0x1p-969 && a != 0.0 && b != 0.0) || ap >= 0x1p1012) x.flags |= 1;
     xacc_deposit<0>(x, p);
-    xacc_deposit<1>(x, e);
+    x.es = __dadd_rn(x.es, e);
+    x.ea = __dadd_ru(x.ea, fabs(e));
 }
 
 // Raise B by one: the top bin is cut onto the new top grid, the rest move
@@ -121,11 +127,80 @@ __device__ __forceinline__ void xacc_normalize(XAcc &x) {
     }
 }
 
+// Per-lane forms, for lanes that accumulate different reductions (the rows of
+// a matrix): every lane keeps its own B, and the decisions diverge.
+__device__ __forceinline__ void xacc_fit1(XAcc &x, unsigned hi) {
+    while (x.B < kXBmax && hi >= (unsigned)((x.B + 1) * kXW + 1023) << 20) xacc_raise(x);
+}
+
+__device__ __forceinline__ void xacc_normalize1(XAcc &x) {
+#pragma unroll
+    for (int j = kXK - 1; j >= 1; j--) {
+        const double c = __dsub_rn(__dadd_rn(x.a[j], x.sig[j - 1]), x.sig[j - 1]);
+        x.a[j] = __dsub_rn(x.a[j], c);
+        x.a[j - 1] = __dadd_rn(x.a[j - 1], c);
+    }
+    for (int guard = 0; guard < 4 && fabs(x.a[0]) > pow2((x.B + 1) * kXW - 1); guard++) {
+        xacc_raise(x);
+        const double c = __dsub_rn(__dadd_rn(x.a[1], x.sig[0]), x.sig[0]);
+        x.a[1] = __dsub_rn(x.a[1], c);
+        x.a[0] = __dadd_rn(x.a[0], c);
+    }
+}
+
 // One bin set of a block or of the whole reduction: top bin B, K bins,
 // the drop bound and the flags.
 struct XPart {
-    double B, a[kXK], drop, flags;
+    double B, a[kXK], drop, es, ea, flags;
 };
+
+// Bound of |es - (exact sum of the error terms)| for a total magnitude ea.
+__device__ __forceinline__ double xes_bound(double ea) { return __dmul_ru(ea, 0x1p-28); }
+
+// The certified correct rounding of the exact sum of `np` normalised bin
+// sets, part(i) returning the i-th (one thread; np <= 2^(54 - W) / 2 so the
+// bins add exactly).
+template <typename Get>
+__device__ inline bool xparts_round1(int np, Get part, double &out) {
+    int Bg = kXBmin, f = 0;
+    for (int i = 0; i < np; i++) {
+        Bg = max(Bg, (int)part(i).B);
+        f |= (int)part(i).flags;
+    }
+    if (f) return false;
+    double c[kXK + 1], drop = 0.0, es = 0.0, ea = 0.0;
+#pragma unroll
+    for (int j = 0; j < kXK; j++) c[j] = 0.0;
+    for (int i = 0; i < np; i++) {
+        const XPart &q = part(i);
+        const int d = Bg - (int)q.B;
+#pragma unroll
+        for (int j = 0; j < kXK; j++) {
+            if (j + d < kXK)
+                c[j + d] = __dadd_rn(c[j + d], q.a[j]);
+            else
+                drop = __dadd_ru(drop, fabs(q.a[j]));
+        }
+        drop = __dadd_ru(drop, q.drop);
+        es = __dadd_rn(es, q.es);
+        ea = __dadd_ru(ea, q.ea);
+    }
+    c[kXK] = es;
+    drop = __dadd_ru(drop, xes_bound(ea));
+    if (drop == 0.0) {
+        out = nearsum(kXK + 1, c, 1);
+        return true;
+    }
+    double lo[kXK + 2], hi[kXK + 2];
+#pragma unroll
+    for (int j = 0; j <= kXK; j++) lo[j] = hi[j] = c[j];
+    lo[kXK + 1] = -drop;
+    hi[kXK + 1] = drop;
+    const double rl = nearsum(kXK + 2, lo, 1), rh = nearsum(kXK + 2, hi, 1);
+    out = rl;
+    return dbits(rl) == dbits(rh);
+}
+
 
 // Warp sum of the lanes' bins (same B), then block sum into `out` (thread 0;
 // `wsh` holds one XPart per warp).  Exact: every lane is normalised first, a
@@ -136,7 +211,11 @@ __device__ __forceinline__ void xacc_block_reduce(XAcc &x, XPart *wsh, XPart &ou
 #pragma unroll
     for (int j = 0; j < kXK; j++)
         for (int o = 16; o > 0; o >>= 1) x.a[j] = __dadd_rn(x.a[j], __shfl_xor_sync(0xffffffffu, x.a[j], o));
-    for (int o = 16; o > 0; o >>= 1) x.drop = __dadd_ru(x.drop, __shfl_xor_sync(0xffffffffu, x.drop, o));
+    for (int o = 16; o > 0; o >>= 1) {
+        x.drop = __dadd_ru(x.drop, __shfl_xor_sync(0xffffffffu, x.drop, o));
+        x.es = __dadd_rn(x.es, __shfl_xor_sync(0xffffffffu, x.es, o));
+        x.ea = __dadd_ru(x.ea, __shfl_xor_sync(0xffffffffu, x.ea, o));
+    }
     const int fl = (int)__reduce_or_sync(0xffffffffu, (unsigned)x.flags);
     const int w = threadIdx.x >> 5, nw = blockDim.x >> 5;
     if ((threadIdx.x & 31) == 0) {
@@ -144,6 +223,8 @@ __device__ __forceinline__ void xacc_block_reduce(XAcc &x, XPart *wsh, XPart &ou
 #pragma unroll
         for (int j = 0; j < kXK; j++) wsh[w].a[j] = x.a[j];
         wsh[w].drop = x.drop;
+        wsh[w].es = x.es;
+        wsh[w].ea = x.ea;
         wsh[w].flags = (double)fl;
     }
     __syncthreads();
@@ -153,7 +234,7 @@ __device__ __forceinline__ void xacc_block_reduce(XAcc &x, XPart *wsh, XPart &ou
         XPart r;
         r.B = (double)Bb;
         for (int j = 0; j < kXK; j++) r.a[j] = 0.0;
-        r.drop = 0.0;
+        r.drop = r.es = r.ea = 0.0;
         int f = 0;
         for (int i = 0; i < nw; i++) {  // <= 8 warps of bins below 2^(W+4) g: exact
             const int d = Bb - (int)wsh[i].B;
@@ -164,6 +245,8 @@ __device__ __forceinline__ void xacc_block_reduce(XAcc &x, XPart *wsh, XPart &ou
                     r.drop = __dadd_ru(r.drop, fabs(wsh[i].a[j]));
             }
             r.drop = __dadd_ru(r.drop, wsh[i].drop);
+            r.es = __dadd_rn(r.es, wsh[i].es);
+            r.ea = __dadd_ru(r.ea, wsh[i].ea);
             f |= (int)wsh[i].flags;
         }
         r.flags = (double)f;
@@ -175,7 +258,7 @@ __device__ __forceinline__ void xacc_block_reduce(XAcc &x, XPart *wsh, XPart &ou
 // of 256 threads; the caller synchronises before and reads *result after).
 // Parts are shifted onto the largest top bin with two spare bins above it;
 // *certified = 0 when the drop bound leaves the rounding open or a flag is
-// set.  `sh` is shared scratch of at least 256 * (kXK + 3) doubles.
+// set.  `sh` is shared scratch of at least 256 * (kXK2 + 3) doubles.
 constexpr int kXK2 = kXK + 2;
 __device__ inline void xparts_round(const XPart *parts, int np, double *sh, double *result, int *certified) {
     __shared__ int s_B, s_flags;
@@ -200,7 +283,7 @@ __device__ inline void xparts_round(const XPart *parts, int np, double *sh, doub
     }
     __syncthreads();
     const int Bt = s_B + 2;  // top of the 6-bin layout
-    double c[kXK2], sig[kXK2], drop = 0.0;
+    double c[kXK2], sig[kXK2], drop = 0.0, es = 0.0, ea = 0.0;
 #pragma unroll
     for (int j = 0; j < kXK2; j++) {
         c[j] = 0.0;
@@ -217,6 +300,8 @@ __device__ inline void xparts_round(const XPart *parts, int np, double *sh, doub
                 drop = __dadd_ru(drop, fabs(v));
         }
         drop = __dadd_ru(drop, __ldcg(&parts[i].drop));
+        es = __dadd_rn(es, __ldcg(&parts[i].es));
+        ea = __dadd_ru(ea, __ldcg(&parts[i].ea));
         // a part's bins are below 2^(W+7) g (8 warps of normalised lanes) and c's
         // below 2^(W-1) g after this carry: the next part adds exactly
 #pragma unroll
@@ -227,34 +312,40 @@ __device__ inline void xparts_round(const XPart *parts, int np, double *sh, doub
         }
     }
     // every bin is now below 2^(W-1) g (the top two far below): 256 threads add exactly
+    // slots: the kXK2 bins, es, drop, ea
 #pragma unroll
     for (int j = 0; j < kXK2; j++) sh[j * blockDim.x + t] = c[j];
-    sh[kXK2 * blockDim.x + t] = drop;
+    sh[kXK2 * blockDim.x + t] = es;
+    sh[(kXK2 + 1) * blockDim.x + t] = drop;
+    sh[(kXK2 + 2) * blockDim.x + t] = ea;
     __syncthreads();
     for (int s = blockDim.x / 2; s > 0; s >>= 1) {
         if (t < s) {
 #pragma unroll
-            for (int j = 0; j < kXK2; j++)
+            for (int j = 0; j <= kXK2; j++)
                 sh[j * blockDim.x + t] = __dadd_rn(sh[j * blockDim.x + t], sh[j * blockDim.x + t + s]);
-            sh[kXK2 * blockDim.x + t] = __dadd_ru(sh[kXK2 * blockDim.x + t], sh[kXK2 * blockDim.x + t + s]);
+            sh[(kXK2 + 1) * blockDim.x + t] =
+                __dadd_ru(sh[(kXK2 + 1) * blockDim.x + t], sh[(kXK2 + 1) * blockDim.x + t + s]);
+            sh[(kXK2 + 2) * blockDim.x + t] =
+                __dadd_ru(sh[(kXK2 + 2) * blockDim.x + t], sh[(kXK2 + 2) * blockDim.x + t + s]);
         }
         __syncthreads();
     }
     if (t == 0) {
-        double terms[kXK2 + 1];
-        for (int j = 0; j < kXK2; j++) terms[j] = sh[j * blockDim.x];
-        const double D = sh[kXK2 * blockDim.x];
+        double terms[kXK2 + 2];
+        for (int j = 0; j <= kXK2; j++) terms[j] = sh[j * blockDim.x];
+        const double D = __dadd_ru(sh[(kXK2 + 1) * blockDim.x], xes_bound(sh[(kXK2 + 2) * blockDim.x]));
         int ok = s_flags == 0;
         double r = 0.0;
         if (ok) {
             if (D == 0.0) {
-                r = nearsum(kXK2, terms, 1);
+                r = nearsum(kXK2 + 1, terms, 1);
             } else {
-                double lo[kXK2 + 1], hi[kXK2 + 1];
-                for (int j = 0; j < kXK2; j++) lo[j] = hi[j] = terms[j];
-                lo[kXK2] = -D;
-                hi[kXK2] = D;
-                const double rl = nearsum(kXK2 + 1, lo, 1), rh = nearsum(kXK2 + 1, hi, 1);
+                double lo[kXK2 + 2], hi[kXK2 + 2];
+                for (int j = 0; j <= kXK2; j++) lo[j] = hi[j] = terms[j];
+                lo[kXK2 + 1] = -D;
+                hi[kXK2 + 1] = D;
+                const double rl = nearsum(kXK2 + 2, lo, 1), rh = nearsum(kXK2 + 2, hi, 1);
                 ok = (dbits(rl) == dbits(rh));
                 r = rl;
             }
@@ -282,7 +373,7 @@ struct XReduce {
 __device__ inline bool xreduce_finish(XAcc &acc, XReduce *xr, double *result, int *certified) {
     __shared__ XPart wsh[8];
     __shared__ int last;
-    __shared__ double sh[256 * (kXK2 + 1)];
+    __shared__ double sh[256 * (kXK2 + 3)];
     xacc_block_reduce(acc, wsh, xr->part[blockIdx.x]);
     __threadfence();
     __syncthreads();

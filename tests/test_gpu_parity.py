@@ -736,3 +736,27 @@ def test_dcsrmv_nearsum_rows_equal_slices(phi, oracle, handle, ozb, cuda, monkey
     ref, _ = oracle.dcsrmv(make_flags(sumMode=1), m, m, 1.5, val, colind, rowptr, x, -0.5, y0)
     assert bits_equal(host(dy), ref), first_diff(host(dy), ref)
     assert (handle.nSplitA, handle.nSplitB, handle.nSplitC) == a
+
+
+@pytest.mark.parametrize("m,n,phi", [(300, 1000, 1.0), (1024, 8192, 2.0), (77, 513, 4.0)])
+def test_dgemv_nearsum_rows_equal_slices(m, n, phi, oracle, handle, ozb, cuda, monkeypatch):
+    """NearSum GEMV 'n': the correctly rounded exact row dots give the oracle's bits and exec-info counts, and the
+    bits of the slice path; rows spanning many levels (which hand the call back to the slice path) included."""
+    A = oracle.phi_matrix(m, n, phi, 1)
+    x = oracle.phi_vector(n, phi, 2)
+    y0 = oracle.phi_vector(m, 1.0, 3)
+    if phi == 4.0:
+        A[5, 3] *= 2.0 ** -700  # a deep row: its split needs more levels than the cap allows
+    ref, info = oracle.dgemv(make_flags(sumMode=1), "n", m, n, 0.75, A, m, x, -1.5, y0)
+    handle.sumMode = 1
+    dy = dev(cuda, y0)
+    ozb.dgemv(handle, "n", m, n, 0.75, dev(cuda, A), m, dev(cuda, x), -1.5, dy)
+    assert bits_equal(host(dy), ref), first_diff(host(dy), ref)
+    assert (handle.nSplitA, handle.nSplitB, handle.nSplitC) == (info.nSplitA, info.nSplitB, info.nSplitC)
+    monkeypatch.setenv("OZBLAS_GEMV_SLICES", "1")
+    handle.read_env()
+    dy2 = dev(cuda, y0)
+    ozb.dgemv(handle, "n", m, n, 0.75, dev(cuda, A), m, dev(cuda, x), -1.5, dy2)
+    monkeypatch.delenv("OZBLAS_GEMV_SLICES")
+    handle.read_env()
+    assert bits_equal(host(dy2), host(dy))
