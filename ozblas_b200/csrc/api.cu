@@ -269,6 +269,8 @@ int cuozblasHandleCreate(cuozblasHandle_t *h, uint64_t workSizeBytes) {
     cudaError_t e = cudaMalloc((void **)&h->devWorkCommon, sizeof(double) * 512);
     if (e == cudaSuccess) e = cudaMalloc((void **)&h->devWork, workSizeBytes > 0 ? workSizeBytes : 256);
     if (e == cudaSuccess) e = cudaMalloc((void **)&st->d_ints, sizeof(int) * 64);
+    if (e == cudaSuccess) e = cudaMalloc(&st->d_persist, kPersistBytes);
+    if (e == cudaSuccess) e = cudaMemset(st->d_persist, 0, kPersistBytes);
     if (e == cudaSuccess) e = cudaMallocHost((void **)&st->h_ints, sizeof(int) * 64);
     if (e == cudaSuccess) e = cudaMallocHost((void **)&st->h_dbl, sizeof(double) * 64);
     for (int i = 0; i < 5 && e == cudaSuccess; i++) e = cudaEventCreate(&st->ev[i]);
@@ -278,6 +280,7 @@ int cuozblasHandleCreate(cuozblasHandle_t *h, uint64_t workSizeBytes) {
         if (h->devWork) cudaFree(h->devWork);
         if (h->devWorkCommon) cudaFree(h->devWorkCommon);
         if (st->d_ints) cudaFree(st->d_ints);
+        if (st->d_persist) cudaFree(st->d_persist);
         if (st->h_ints) cudaFreeHost(st->h_ints);
         if (st->h_dbl) cudaFreeHost(st->h_dbl);
         delete st;
@@ -304,6 +307,7 @@ int cuozblasHandleDestroy(cuozblasHandle_t *h) {
     cudaFree(h->devWork);
     cudaFree(h->devWorkCommon);
     cudaFree(st->d_ints);
+    cudaFree(st->d_persist);
     cudaFreeHost(st->h_ints);
     cudaFreeHost(st->h_dbl);
     for (int i = 0; i < 5; i++)

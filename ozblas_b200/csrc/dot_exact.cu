@@ -54,7 +54,7 @@ __global__ void __launch_bounds__(kXThreads) k_dot_exact(int n, const double *__
     double mx = 0.0, my = 0.0;
     int lx = 0, ly = 0, bx = 0, by = 0;
     const int64_t stride = (int64_t)gridDim.x * kXThreads;
-    constexpr int U = 4;  // double2 loads per vector per step
+    constexpr int U = 2;  // double2 loads per vector per step
     if (ALIGNED) {
         const int64_t np = (int64_t)n >> 1;
         const double2 *x2 = reinterpret_cast<const double2 *>(x);
@@ -91,7 +91,7 @@ __global__ void __launch_bounds__(kXThreads) k_dot_exact(int n, const double *__
                 xacc_product(acc, a[u].x, bb.x);
                 xacc_product(acc, a[u].y, bb.y);
             }
-            if ((s & 7) == 7) xacc_normalize(acc);  // every 64 products per lane
+            if ((s & 15) == 15) xacc_normalize(acc);  // every 64 products per lane
         }
         if ((n & 1) && blockIdx.x == 0 && threadIdx.x < 32) {  // the odd last element, one warp
             const double xe = threadIdx.x == 0 ? x[n - 1] : 0.0;
@@ -244,18 +244,13 @@ int dot_exact(cuozblasHandle_t *h, int n, const double *x, const double *y, doub
     State *st = state(h);
     *done = false;
     if (n <= 0) return CUOZBLAS_STATUS_SUCCESS;
-    Arena ar(h);
-    const uint64_t mk = ar.mark();
-    DotScratch *sc = ar.take<DotScratch>(1);
-    DotExactScratch *xs = ar.take<DotExactScratch>(1);
-    if (!ar.ok) {
-        ar.release(mk);
-        return CUOZBLAS_STATUS_SUCCESS;
-    }
+    // the handle's persistent scratch: zeroed at create, left zeroed by the kernels below
+    static_assert(sizeof(DotScratch) + 256 + sizeof(DotExactScratch) <= kPersistBytes, "persistent scratch size");
+    DotScratch *sc = reinterpret_cast<DotScratch *>(st->d_persist);
+    DotExactScratch *xs = reinterpret_cast<DotExactScratch *>(reinterpret_cast<char *>(st->d_persist) +
+                                                              (sizeof(DotScratch) + 255) / 256 * 256);
     const int maxS = h->nSplitMax > 0 ? h->nSplitMax : kMaxSplitDefault;
     const int rho = rho_rule(n, h->splitEpsMode);
-    OZB_CHECK(cudaMemsetAsync(sc, 0, sizeof(DotScratch), st->stream));
-    OZB_CHECK(cudaMemsetAsync(xs, 0, sizeof(DotExactScratch), st->stream));
     const bool same = (x == y);
     const bool aligned = ((reinterpret_cast<uintptr_t>(x) | reinterpret_cast<uintptr_t>(y)) & 15u) == 0;
     const int nsm = sm_count();
@@ -299,7 +294,6 @@ int dot_exact(cuozblasHandle_t *h, int n, const double *x, const double *y, doub
     static_assert(sizeof(DotStatus) == 24, "status block layout");
     OZB_CHECK(cudaMemcpyAsync(st->h_dbl, &sc->out, sizeof(DotStatus), cudaMemcpyDeviceToHost, st->stream));
     OZB_CHECK(cudaStreamSynchronize(st->stream));
-    ar.release(mk);
     DotStatus res;
     memcpy(&res, st->h_dbl, sizeof(res));
     if (res.status == 1) {

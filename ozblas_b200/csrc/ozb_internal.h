@@ -12,6 +12,7 @@
 namespace ozb {
 
 constexpr int kMaxSplitDefault = 30;  // NumSplitDefaultMax, src/cuda/cuozblas_common.h:5
+constexpr size_t kPersistBytes = 256 << 10;  // State::d_persist
 constexpr int kArenaAlign = 256;
 
 // Diagnostic switches from the environment, read when a handle is created
@@ -49,6 +50,10 @@ struct State {
     cudaEvent_t ev[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};  // phase timers (split A/B, products, sum)
     bool plain_timers = false;    // ev[0..4] hold a plain-form call's phases, read at the call's end
     uint64_t launches = 0;        // kernels this handle has launched (cuozblasGetLaunchCount)
+    // Device scratch that lives as long as the handle (zeroed at create; every
+    // kernel that uses it leaves it zeroed): the one-pass DOT's statistics,
+    // block parts and tickets, so a call needs no memset.
+    void *d_persist = nullptr;
     EnvSwitches env;
     // The matrix of the last fused CSRMV and the level count its rows needed:
     // the next call on the same matrix holds that many levels per row on chip
