@@ -116,7 +116,10 @@ __global__ void k_cg_stamp(unsigned long long *t) { *t = tc::globaltimer(); }
 // <p, q> is one exact pass over p and q that ends in alpha, and <r, r> rides
 // in the x / r update, whose last block computes beta, the history and the
 // gate: five kernels per iteration (proof, SpMV, <p, q> + alpha,
-// x / r + <r, r> + beta, p update) and no separate DOT passes.
+// x / r + <r, r> + beta, p update) and no separate DOT passes.  The SpMV's
+// rows are then correctly rounded exact row dots (csrmv_fused.cu), which need
+// only p's split to be complete, not its proven chain: without listed rows
+// the proof kernel is left out too (four kernels).
 
 // Exact p . q of n elements into bins, U double2 pairs per lane per step.
 template <bool ALIGNED>
@@ -185,12 +188,12 @@ __device__ __forceinline__ VecStats load_stats(const VecStats *g) {
 // update) and of q (from the SpMV) are in dpq->vs; they are consumed here.
 template <bool ALIGNED>
 __global__ void __launch_bounds__(256) k_cg_pq(int n, const double *__restrict__ p, const double *__restrict__ q,
-                                               CgDev *d, DotScratch *dpq, const CsrScratch *cs, XReduce *xr, int rho,
-                                               int maxS) {
+                                               CgDev *d, DotScratch *dpq, CsrScratch *cs, XReduce *xr, int rho,
+                                               int maxS, int proof_ran) {
     __shared__ double res_sh;
     __shared__ int cert_sh;
     if (!d->gate) return;  // uniform
-    if (!cs->valid || cs->rn_declined) {  // the SpMV did not run: the host path takes this iteration
+    if ((proof_ran && !cs->valid) || cs->rn_declined) {  // the SpMV did not run: the host path takes this iteration
         if (blockIdx.x == 0 && threadIdx.x == 0) {
             d->broken = 2;
             d->gate = 0;
@@ -210,6 +213,7 @@ __global__ void __launch_bounds__(256) k_cg_pq(int n, const double *__restrict__
             d->gate = 0;
         }
         dpq->vs = VecStats{};
+        cs->rn_declined = 0;  // every block has read it (the ticket comes after)
     }
 }
 
@@ -388,16 +392,21 @@ int cg_graph(cuozblasHandle_t *h, int n, const double *val, const int *colind, c
     int xb = ub < nsm * 4 ? ub : nsm * 4;  // blocks of the fused dot kernels (one part each)
     if (xb > kXMaxBlocks) xb = kXMaxBlocks;
     const bool rn_rows = fused_dots && csr_rn_applies(spmv) && !st->env.csr_slices;
+    // correctly rounded rows need only p's completeness (its statistics from the p
+    // update, dpq->vs[0]), not its proven chain: no proof kernel unless listed rows
+    // (computed through p's slices) need one
+    const bool no_proof = rn_rows && nslow == 0;
     for (int k = 0; k < K && !cap; k++) {
-        cap = csr_proof_launch(s, n, p, rho, maxS, cs, &d->gate);
+        if (!no_proof) cap = csr_proof_launch(s, n, p, rho, maxS, cs, &d->gate);
         if (!cap)
-            cap = rn_rows ? csr_rn_launch(s, spmv, cs, slow, nslow, &dpq->vs, 1, terms, &d->gate)
+            cap = rn_rows ? csr_rn_launch(s, spmv, cs, slow, nslow, &dpq->vs, 1, terms, &d->gate,
+                                          no_proof ? &dpq->vs : nullptr)
                           : csr_rows_launch(s, spmv, cs, slow, nslow, &dpq->vs, 1, terms, &d->gate);
         if (fused_dots) {
             if (aligned_pq)
-                k_cg_pq<true><<<xb, 256, 0, s>>>(n, p, q, d, dpq, cs, xpq, rho, maxS);
+                k_cg_pq<true><<<xb, 256, 0, s>>>(n, p, q, d, dpq, cs, xpq, rho, maxS, no_proof ? 0 : 1);
             else
-                k_cg_pq<false><<<xb, 256, 0, s>>>(n, p, q, d, dpq, cs, xpq, rho, maxS);
+                k_cg_pq<false><<<xb, 256, 0, s>>>(n, p, q, d, dpq, cs, xpq, rho, maxS, no_proof ? 0 : 1);
             k_cg_xr_rr<<<xb, 256, 0, s>>>(n, x, r, p, q, d, &drr->vs, xrr, rho, maxS, res_dev, stamp_dev);
         } else {
             if (!cap)
@@ -417,7 +426,7 @@ int cg_graph(cuozblasHandle_t *h, int n, const double *val, const int *colind, c
     }
     CG_CHECK(ce);
     CG_CHECK(cudaGraphInstantiate(&exec, graph, 0));
-    const int per_iter = (fused_dots ? 5 : 8) + (nslow > 0 ? (nslow + 8191) / 8192 : 0);
+    const int per_iter = (fused_dots ? (no_proof ? 4 : 5) : 8) + (nslow > 0 ? (nslow + 8191) / 8192 : 0);
     // device clock against the host's, for the elapsed-time history
     k_cg_stamp<<<1, 1, 0, s>>>(stamp_dev + maxiter + 1);
     unsigned long long dev0 = 0;

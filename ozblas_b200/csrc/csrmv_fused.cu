@@ -902,14 +902,29 @@ __global__ void __launch_bounds__(kCsrThreads, 4)
                const int *__restrict__ rowptr, const double *__restrict__ x, int shift, int lg_shift, int rho_x,
                int epsmode, int maxS, double alpha, double beta, double *__restrict__ y, CsrScratch *__restrict__ sc,
                int *__restrict__ slow_rows, int append_slow, VecStats *__restrict__ ystats, int ystats_index,
-               const int *__restrict__ gate) {
+               const VecStats *__restrict__ xstats, const int *__restrict__ gate) {
     if (gate && *gate == 0) return;  // uniform: a captured solver step that is switched off
     __shared__ __align__(16) LeanSlot slot[2];
     __shared__ double red[kCsrThreads / 32];
+    __shared__ int xok;
     const int t = threadIdx.x;
     const int ntiles = (m + kCsrThreads - 1) / kCsrThreads;
-    if (!sc->valid) return;  // uniform: the caller runs the general path
-    if (!sc->xcomplete) {    // uniform: the lean kernel computes the slices instead
+    // x's split must be complete: from the proof kernel (sc), or with `xstats`
+    // (no proof ran) straight from x's statistics
+    if (t == 0) {
+        if (xstats) {
+            VecStats vs;
+            vs.mx[0] = __ldcg(&xstats->mx[0]);
+            vs.lsb[0] = __ldcg(&xstats->lsb[0]);
+            vs.bad[0] = __ldcg(&xstats->bad[0]);
+            xok = split_complete(vs, 0, rho_x, maxS) ? 1 : 0;
+        } else {
+            xok = !sc->valid ? -1 : (sc->xcomplete ? 1 : 0);
+        }
+    }
+    __syncthreads();
+    if (xok < 0) return;  // uniform: the caller runs the general path
+    if (xok == 0) {       // uniform: the lean kernel computes the slices instead
         if (blockIdx.x == 0 && t == 0) sc->rn_declined = 1;
         return;
     }
@@ -1041,7 +1056,7 @@ bool csr_rn_applies(const CsrmvArgs &a) {
 
 template <int NA>
 static void launch_rn(const CsrmvArgs &a, cudaStream_t s, CsrScratch *sc, int *slow, int append, VecStats *ystats,
-                      int ystats_index, const int *gate) {
+                      int ystats_index, const VecStats *xstats, const int *gate) {
     static std::atomic<int> per_sm{0};  // resident CTAs per SM (once per instantiation)
     int ps = per_sm.load();
     if (ps == 0) {
@@ -1057,20 +1072,20 @@ static void launch_rn(const CsrmvArgs &a, cudaStream_t s, CsrScratch *sc, int *s
     const int rho_x = rho_rule(a.n > 0 ? a.n : 1, a.epsmode);
     k_csrmv_rn<NA><<<grid, kCsrThreads, 0, s>>>(a.m, a.n, a.val, a.colind, a.rowptr, a.x, a.shift, lg_shift, rho_x,
                                                  a.epsmode, a.maxS, a.alpha, a.beta, a.y, sc, slow, append, ystats,
-                                                 ystats_index, gate);
+                                                 ystats_index, xstats, gate);
 }
 
 int csr_rn_launch(cudaStream_t s, const CsrmvArgs &a, CsrScratch *sc, int *slow, int fixed_slow, VecStats *ystats,
-                  int ystats_index, double *terms, const int *gate) {
+                  int ystats_index, double *terms, const int *gate, const VecStats *xstats) {
     if (a.m <= 0) return CUOZBLAS_STATUS_SUCCESS;
     const int append = fixed_slow < 0 ? 1 : 0;
     // the levels per row held on chip match the slow-row list's (csr_slow_rows_launch)
     if (a.na_hint > 0 && a.na_hint <= 2)
-        launch_rn<2>(a, s, sc, slow, append, ystats, ystats_index, gate);
+        launch_rn<2>(a, s, sc, slow, append, ystats, ystats_index, xstats, gate);
     else if (a.na_hint > 4)
-        launch_rn<6>(a, s, sc, slow, append, ystats, ystats_index, gate);
+        launch_rn<6>(a, s, sc, slow, append, ystats, ystats_index, xstats, gate);
     else
-        launch_rn<4>(a, s, sc, slow, append, ystats, ystats_index, gate);
+        launch_rn<4>(a, s, sc, slow, append, ystats, ystats_index, xstats, gate);
     for (int c0 = 0; c0 < fixed_slow; c0 += kCsrSlowChunk) {  // the listed rows (general per-row kernel)
         const int nr = fixed_slow - c0 < kCsrSlowChunk ? fixed_slow - c0 : kCsrSlowChunk;
         k_csrmv_slow<1><<<(nr + 127) / 128, 128, 0, s>>>(nr, slow + c0, a.val, a.colind, a.rowptr, a.x, a.shift,

@@ -87,7 +87,9 @@ int csr_rows_launch(cudaStream_t s, const CsrmvArgs &a, CsrScratch *sc, int *slo
 // (fixed_slow >= 0, whose rows the call computes afterwards) they decline the
 // whole product (sc->rn_declined).
 bool csr_rn_applies(const CsrmvArgs &a);
+// With `xstats` (x's statistics at index 0) the kernel decides x's completeness
+// itself and needs no proof (no fixed list then: its rows need x's proven chain).
 int csr_rn_launch(cudaStream_t s, const CsrmvArgs &a, CsrScratch *sc, int *slow, int fixed_slow, VecStats *ystats,
-                  int ystats_index, double *terms, const int *gate);
+                  int ystats_index, double *terms, const int *gate, const VecStats *xstats = nullptr);
 
 }  // namespace ozb
