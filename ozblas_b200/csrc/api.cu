@@ -70,6 +70,7 @@ void EnvSwitches::read() {
     dot_two_pass = env_on("OZBLAS_DOT_TWO_PASS");
     csr_slices = env_on("OZBLAS_CSR_SLICES");
     gemv_slices = env_on("OZBLAS_GEMV_SLICES");
+    i8_levelwise = env_on("OZBLAS_I8_LEVELWISE");
     cg_no_graph = env_on("OZBLAS_CG_NO_GRAPH");
     dot_trace = env_on("OZBLAS_DOT_TRACE");
     cg_trace = env_on("OZBLAS_CG_TRACE");

@@ -711,6 +711,10 @@ int i8_schedule(int nA, int nB, int nkb, bool triangular, std::vector<int4> &ite
     return np;
 }
 
+int i8_blk_launch(cuozblasHandle_t *h, const CUtensorMap &tmA, const CUtensorMap &tmB, int m, int n, int m_pad,
+                  int n_pad, int k_pad, int nA, int nB, bool triangular, const int *ea, const int *eb, double alpha,
+                  double beta, double *C, int ldc, int strip, int *d_err, Arena &ar);  // gemm_i8_blk.cu
+
 // Default digit cap when nSplitMax is 0 (enough for an exact split of
 // values whose lines span ~2^80; larger spans are truncated).
 constexpr int kI8DefaultCap = 19;
@@ -806,9 +810,18 @@ int gemm_i8_core(cuozblasHandle_t *h, char ta, char tb, int m, int n, int k, dou
         p.strip = cand[(size_t)pick];
     }
     ev_record(h, 2);
-    counted(h);
-    k_i8_gemm<0><<<grid, I8_THREADS, I8_SMEM, st->stream>>>(tmA, tmB, p);
-    OZB_CHECK(cudaGetLastError());
+    // the level-blocked kernel (same bits, a quarter of the operand traffic) unless switched off
+    int blk = CUOZBLAS_STATUS_NOT_SUPPORTED;
+    if (!st->env.i8_levelwise)
+        blk = i8_blk_launch(h, tmA, tmB, m, n, p.m_pad, p.n_pad, k_pad, nA, nB, h->fastMode != 0, da.e, db.e, alpha,
+                            beta, C, ldc, p.strip, d_err, ar);
+    if (blk == CUOZBLAS_STATUS_NOT_SUPPORTED) {
+        counted(h);
+        k_i8_gemm<0><<<grid, I8_THREADS, I8_SMEM, st->stream>>>(tmA, tmB, p);
+        OZB_CHECK(cudaGetLastError());
+    } else if (blk != CUOZBLAS_STATUS_SUCCESS) {
+        return blk;
+    }
     ev_record(h, 3);
     OZB_CHECK(cudaMemcpyAsync(st->h_ints, d_err, sizeof(int), cudaMemcpyDeviceToHost, st->stream));
     OZB_CHECK(cudaStreamSynchronize(st->stream));

@@ -244,3 +244,26 @@ def test_i8_wait_timeout_reports_and_recovers(oracle, handle, ozb, cuda):
     cuda.cuda.synchronize()
     again = run_i8(ozb, handle, cuda, A, B, m, n, k)
     assert bits_equal(again, ref)
+
+
+@pytest.mark.parametrize("m,n,k,phi,fast,ta,tb", [
+    (300, 260, 1000, 1.0, 0, "n", "n"),
+    (300, 260, 1000, 1.0, 1, "t", "n"),
+    (129, 513, 4096, 4.0, 0, "n", "t"),
+    (256, 128, 20000, 1.0, 0, "n", "n"),   # K chunks: a level's INT32 sum is split over K
+    (130, 200, 20000, 2.0, 1, "t", "t"),
+    (1, 1, 7, 1.0, 0, "n", "n"),
+])
+def test_i8_level_blocked_equals_levelwise(m, n, k, phi, fast, ta, tb, oracle, handle, ozb, cuda, monkeypatch):
+    """The level-blocked product kernel (k_i8_blk) gives the bits of the level-wise one (k_i8_gemm): the same
+    products and sums, in another order of the exact INT32 accumulations."""
+    A = oracle.phi_matrix(m, k, phi, 1) if ta == "n" else oracle.phi_matrix(k, m, phi, 1)
+    B = oracle.phi_matrix(k, n, phi, 2) if tb == "n" else oracle.phi_matrix(n, k, phi, 2)
+    C0 = oracle.phi_matrix(m, n, 1.0, 3)
+    a = run_i8(ozb, handle, cuda, A, B, m, n, k, ta=ta, tb=tb, fast=fast, alpha=-0.75, beta=0.5, C0=C0)
+    monkeypatch.setenv("OZBLAS_I8_LEVELWISE", "1")
+    handle.read_env()
+    b = run_i8(ozb, handle, cuda, A, B, m, n, k, ta=ta, tb=tb, fast=fast, alpha=-0.75, beta=0.5, C0=C0)
+    monkeypatch.delenv("OZBLAS_I8_LEVELWISE")
+    handle.read_env()
+    assert bits_equal(a, b)
