@@ -62,6 +62,11 @@ enum { ERR_TIMEOUT_PRODUCER = 1, ERR_TIMEOUT_MMA = 2, ERR_TIMEOUT_EPI = 3 };
 // runs out (set by cuozblasSetI8WaitTest; tests only).
 __device__ uint64_t g_i8_wait_ns = I8_WAIT_NS;
 __device__ int g_i8_hold_copies = 0;
+// host copies, passed to the level-blocked kernel (gemm_i8_blk.cu) as parameters
+static std::atomic<uint64_t> h_i8_wait_ns{I8_WAIT_NS};
+static std::atomic<int> h_i8_hold_copies{0};
+uint64_t i8_test_wait_ns() { return h_i8_wait_ns.load(); }
+int i8_test_hold_copies() { return h_i8_hold_copies.load(); }
 
 struct I8Params {
     int m, n, m_pad, n_pad, ldc;
@@ -1266,6 +1271,8 @@ extern "C" int cuozblasSetI8WaitTest(uint64_t ns, int32_t hold_copies) {
     const int hold = hold_copies != 0 ? 1 : 0;
     OZB_CHECK(cudaMemcpyToSymbol(g_i8_wait_ns, &v, sizeof(v)));
     OZB_CHECK(cudaMemcpyToSymbol(g_i8_hold_copies, &hold, sizeof(hold)));
+    h_i8_wait_ns.store(v);
+    h_i8_hold_copies.store(hold);
     return CUOZBLAS_STATUS_SUCCESS;
 }
 

@@ -75,7 +75,7 @@ __device__ __forceinline__ int blk_whi(int L1, int ia, int nB) { return L1 - ia 
 
 __global__ void __launch_bounds__(KB_THREADS, 1)
     k_i8_blk(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, BlkParams p,
-             uint64_t wait_ns) {
+             uint64_t wait_ns, int hold_copies) {
     extern __shared__ uint8_t smem_raw[];
     uint8_t *smem = (uint8_t *)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
     uint8_t *ringA = smem, *ringB = smem + KB_RA * KB_TILE;
@@ -116,7 +116,7 @@ __global__ void __launch_bounds__(KB_THREADS, 1)
         if (lane == 0) {
             uint32_t na = 0, nb = 0;  // planes loaded into each ring
             uint32_t issuedA = 0, phaseA = 0, issuedB = 0, phaseB = 0;  // per slot: copy issued / its phase
-            bool ok = true;
+            bool ok = hold_copies == 0;  // a test switch holds back every copy (a wait then runs out)
             auto loadA = [&](int ia, int kb, int tm) {
                 const uint32_t s = na % KB_RA, ph = (na / KB_RA) & 1u;
                 if (!tc::mbar_wait(&emptyA[s], ph ^ 1u, &abort_flag, p.err, 1, wait_ns)) return false;
@@ -385,6 +385,9 @@ static bool blk_schedule(int nA, int nB, int nkb, bool triangular, std::vector<B
 
 static std::atomic<uint64_t> g_blk_attr{0};
 
+uint64_t i8_test_wait_ns();  // gemm_i8.cu: the wait limit and copy switch of cuozblasSetI8WaitTest
+int i8_test_hold_copies();
+
 // The level-blocked product kernel over digit operands laid out as for
 // k_i8_gemm (tensor maps over [S * lines_pad][k_pad], 128 x 128-byte boxes).
 // Returns NOT_SUPPORTED (nothing launched) when the schedule does not apply.
@@ -424,7 +427,7 @@ int i8_blk_launch(cuozblasHandle_t *h, const CUtensorMap &tmA, const CUtensorMap
     p.err = d_err;
     OZB_CHECK(smem_optin((const void *)k_i8_blk, KB_SMEM, g_blk_attr));
     counted(h);
-    k_i8_blk<<<grid, KB_THREADS, KB_SMEM, st->stream>>>(tmA, tmB, p, 2000000000ull);
+    k_i8_blk<<<grid, KB_THREADS, KB_SMEM, st->stream>>>(tmA, tmB, p, i8_test_wait_ns(), i8_test_hold_copies());
     OZB_CHECK(cudaGetLastError());
     return CUOZBLAS_STATUS_SUCCESS;
 }
