@@ -247,6 +247,7 @@ def main():
     ap.add_argument("--sweep-only", action="store_true", help="only the INT8 form sweep (prints its JSON)")
     ap.add_argument("--full-pairs", action="store_true", help="headline with the full pair set instead of triangular")
     ap.add_argument("--n", type=int, default=N_DIM, help="m = n = k (default 8192; smaller for profiling captures)")
+    ap.add_argument("--work-gb", type=int, default=40, help="arena of the headline handle (GB)")
     ap.add_argument("--memory-only", action="store_true",
                     help="only the DOT / CSRMV / CG measurements (for profiling them; prints their JSON)")
     ap.add_argument("--cg-iters", type=int, default=2000, help="CG iterations of the memory-only run")
@@ -317,7 +318,7 @@ def main():
     A = A_h.cuda()
     B = B_h.cuda()
     C = torch.zeros((n, n), dtype=torch.float64, device="cuda")
-    h = ozb.Handle(work_bytes=40 << 30)
+    h = ozb.Handle(work_bytes=args.work_gb << 30)
     h.sumMode = 0
     h.nSplitMax = 0
     h.fastMode = 0 if args.full_pairs else 1
