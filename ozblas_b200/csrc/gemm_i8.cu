@@ -795,9 +795,11 @@ int gemm_i8_core(cuozblasHandle_t *h, char ta, char tb, int m, int n, int k, dou
             const uint64_t mk = ar.mark();
             double *scratch = ar.take<double>((uint64_t)m * n);
             if (ar.ok) {
+                // the kernel the call will run: level-blocked unless switched off
+                const bool blk = !st->env.i8_levelwise;
                 char key[160];
-                snprintf(key, sizeof(key), "i8:%d:%d:%d:%d:%d:%d:%d", p.tiles_m, p.tiles_n, nkb, nA, nB,
-                         h->fastMode != 0 ? 1 : 0, grid);
+                snprintf(key, sizeof(key), "%s:%d:%d:%d:%d:%d:%d:%d", blk ? "i8b" : "i8", p.tiles_m, p.tiles_n, nkb,
+                         nA, nB, h->fastMode != 0 ? 1 : 0, grid);
                 I8Params pt = p;
                 pt.C = scratch;
                 pt.ldc = m;
@@ -805,6 +807,14 @@ int gemm_i8_core(cuozblasHandle_t *h, char ta, char tb, int m, int n, int k, dou
                 pt.beta = 0.0;
                 pick = tune_pick(key, (int)cand.size(), 0, st->stream, [&](int i) {
                     pt.strip = cand[(size_t)i];
+                    if (blk) {
+                        const uint64_t mk2 = ar.mark();
+                        const int r = i8_blk_launch(h, tmA, tmB, m, n, p.m_pad, p.n_pad, k_pad, nA, nB,
+                                                    h->fastMode != 0, da.e, db.e, 1.0, 0.0, scratch, m, pt.strip,
+                                                    d_err, ar);
+                        ar.release(mk2);
+                        if (r != CUOZBLAS_STATUS_NOT_SUPPORTED) return r;
+                    }
                     k_i8_gemm<0><<<grid, I8_THREADS, I8_SMEM, st->stream>>>(tmA, tmB, pt);
                     return cudaGetLastError() == cudaSuccess ? 0 : (int)CUOZBLAS_STATUS_CUDA_ERROR;
                 });
