@@ -372,14 +372,16 @@ def main():
     kms = statistics.mean(kern_ms)
     achieved = pairs * flops / (kms * 1e-3) / 1e12
     traffic = None
+    # the level-blocked kernel unless the handle was switched to the level-wise one
+    kname = "k_i8_gemm" if os.environ.get("OZBLAS_I8_LEVELWISE", "0") not in ("", "0") else "k_i8_blk"
     tp = os.path.join(ROOT, "profiles", "ncu_traffic.json")
     if os.path.exists(tp):
         with open(tp) as f:
             tj = json.load(f)
-        key = f"k_i8_gemm_{'full' if args.full_pairs else 'tri'}_{n}"
+        key = f"{kname}_{'full' if args.full_pairs else 'tri'}_{n}"
         traffic = tj.get(key)
     roofline = {"bound": "tensor", "achieved": achieved, "peak": int8_peak, "unit": "TFLOP/s", "frac": achieved / int8_peak,
-                "traffic": traffic, "kernel": "k_i8_gemm (tcgen05.mma kind::i8)", "kernel_ms": kms,
+                "traffic": traffic, "kernel": f"{kname} (tcgen05.mma kind::i8)", "kernel_ms": kms,
                 "peak_note": f"int8 ops/s; peak = 2 x {peak_kind} dense bf16 ({peaks['bf16_tflops']} TFLOP/s burst, "
                              "MEASURED_PEAKS.json)",
                 "algorithmic_ops_per_launch": pairs * flops}
@@ -866,6 +868,27 @@ def hbm_roofline(nbytes, ms, traffic=None, what="whole call"):
             "algorithmic_bytes": nbytes}
 
 
+def span_ms(h, fn, reps=3):
+    """Minimum device span (ms) of a call's kernels over `reps` calls, from the exec info's t_comp (CUDA events
+    the library records on its stream before the call's first kernel and after its last)."""
+    ts = []
+    for _ in range(max(reps, 1)):
+        fn()
+        ts.append(float(h.t_comp) * 1e3)
+    return min(ts)
+
+
+def mem_record(h, fn, nb, ms, traffic, reps, **kw):
+    """A memory-bound call's record: whole-call GB/s (CUDA events around the API call, host work included) and
+    the HBM roofline of the call's kernels (algorithmic bytes over their device span)."""
+    kms = span_ms(h, fn, reps)
+    rec = {"GBps": nb / ms / 1e6, "ms": ms, "kernel_ms": kms, "slices": [h.nSplitA, h.nSplitB], **kw}
+    if kms > 0:
+        rec["roofline"] = hbm_roofline(nb, kms, traffic, what="device span of the call's kernels")
+    rec["roofline_whole_call"] = hbm_roofline(nb, ms, None)
+    return rec
+
+
 def ncu_traffic(key):
     tp = os.path.join(ROOT, "profiles", "ncu_traffic.json")
     if os.path.exists(tp):
@@ -888,7 +911,8 @@ def cpu_mean(fn, reps):
 def memory_extras(ozb, h, torch, reps=3, cg_iters=2000, cpu=True):
     """Config 2 (DOT / NRM2 n = 2^24 phi = 2, GEMV 8192^2 phi = 1, CSRMV on the 128^3 7-point stencil, both sum
     modes) and config 4 (CG on 100^3, 2000 iterations), through the public API on host-generated inputs.  Each
-    carries its HBM roofline (algorithmic bytes over the call's CUDA-event time) and, with cpu, the reference CPU
+    carries its HBM roofline (algorithmic bytes over the device span of the call's kernels; roofline_whole_call: over
+    the call's CUDA-event time, host work included) and, with cpu, the reference CPU
     library's time on the same inputs (mean of `cpu reps` calls after a warm-up) and whether the bits agree."""
     import numpy as np
 
@@ -917,15 +941,13 @@ def memory_extras(ozb, h, torch, reps=3, cg_iters=2000, cpu=True):
         res = []
         ms = timed_ms(torch, lambda: res.append(ozb.ddot(h, nv, x, y)), reps=reps)
         nb = 16.0 * nv
-        rec = {"GBps": nb / ms / 1e6, "ms": ms, "slices": [h.nSplitA, h.nSplitB],
-               "roofline": hbm_roofline(nb, ms, ncu_traffic(f"ddot_2p24_sum{sm}"))}
+        rec = mem_record(h, lambda: ozb.ddot(h, nv, x, y), nb, ms, ncu_traffic(f"ddot_2p24_sum{sm}"), reps)
         cpu_leg(rec, "ozblasRdot", lambda: ref.ddot(x_h, y_h), nb, 10, res[-1])
         out[f"ddot_2p24_sum{sm}"] = rec
         res = []
         ms = timed_ms(torch, lambda: res.append(ozb.dnrm2(h, nv, x)), reps=reps)
         nb = 8.0 * nv
-        rec = {"GBps": nb / ms / 1e6, "ms": ms, "slices": [h.nSplitA, h.nSplitB],
-               "roofline": hbm_roofline(nb, ms, ncu_traffic(f"dnrm2_2p24_sum{sm}"))}
+        rec = mem_record(h, lambda: ozb.dnrm2(h, nv, x), nb, ms, ncu_traffic(f"dnrm2_2p24_sum{sm}"), reps)
         cpu_leg(rec, "ozblasRnrm2", lambda: ref.dnrm2(x_h), nb, 10, res[-1])
         out[f"dnrm2_2p24_sum{sm}"] = rec
     del x, y, x_h, y_h
@@ -939,10 +961,10 @@ def memory_extras(ozb, h, torch, reps=3, cg_iters=2000, cpu=True):
         h.sumMode = sm
         if ref is not None:
             ref.set_flags(sumMode=sm)
-        ms = timed_ms(torch, lambda: ozb.dgemv(h, "n", mg, mg, 1.0, Ag, mg, xg, 0.0, yg), reps=reps)
+        gv = lambda: ozb.dgemv(h, "n", mg, mg, 1.0, Ag, mg, xg, 0.0, yg)
+        ms = timed_ms(torch, gv, reps=reps)
         nb = 8.0 * (mg * mg + 2 * mg)
-        rec = {"GBps": nb / ms / 1e6, "ms": ms, "slices": [h.nSplitA, h.nSplitB],
-               "roofline": hbm_roofline(nb, ms, ncu_traffic(f"dgemv_8192_sum{sm}"))}
+        rec = mem_record(h, gv, nb, ms, ncu_traffic(f"dgemv_8192_sum{sm}"), reps)
         cpu_leg(rec, "ozblasRgemv", lambda: ref.dgemv("n", mg, mg, 1.0, A_h, mg, xg_h, 0.0, np.zeros(mg)), nb, 3,
                 yg.cpu().numpy())
         out[f"dgemv_8192_sum{sm}"] = rec
@@ -962,9 +984,9 @@ def memory_extras(ozb, h, torch, reps=3, cg_iters=2000, cpu=True):
         h.sumMode = sm
         if ref is not None:
             ref.set_flags(sumMode=sm)
-        ms = timed_ms(torch, lambda: ozb.dcsrmv(h, "n", m, m, nnz, 1.0, val, colind, rowptr, xv, 0.0, yv), reps=reps)
-        rec = {"GBps": nbytes / ms / 1e6, "ms": ms, "nnz": nnz, "slices": [h.nSplitA, h.nSplitB],
-               "roofline": hbm_roofline(nbytes, ms, ncu_traffic(f"dcsrmv_stencil128_sum{sm}"))}
+        cv = lambda: ozb.dcsrmv(h, "n", m, m, nnz, 1.0, val, colind, rowptr, xv, 0.0, yv)
+        ms = timed_ms(torch, cv, reps=reps)
+        rec = mem_record(h, cv, nbytes, ms, ncu_traffic(f"dcsrmv_stencil128_sum{sm}"), reps, nnz=nnz)
         cpu_leg(rec, "ozblasRcsrmv", lambda: ref.dcsrmv(m, m, 1.0, val_h, ci_h, rp_h, xv_h, 0.0, np.zeros(m)),
                 nbytes, 3, yv.cpu().numpy())
         out[f"dcsrmv_stencil128_sum{sm}"] = rec

@@ -1238,6 +1238,7 @@ int csrmv_fused(cuozblasHandle_t *h, int m, int n, double alpha, const double *v
     cudaStream_t s = st->stream;
     OZB_CHECK(cudaMemsetAsync(sc, 0, sizeof(CsrScratch), s));
     const int nsm = sm_count();
+    span_begin(h);
     counted(h);
     OZB_TRY(vec_stats_launch(s, nsm, n, x, &sc->vs, 0));
     counted(h);
@@ -1252,6 +1253,7 @@ int csrmv_fused(cuozblasHandle_t *h, int m, int n, double alpha, const double *v
         OZB_TRY(csr_rn_launch(s, args, sc, slow, -1, nullptr, 0, nullptr, nullptr));
     else
         OZB_TRY(csr_rows_launch(s, args, sc, slow, -1, nullptr, 0, nullptr, nullptr));
+    span_end(h);
     int res[6];  // valid, nB, nslow, zmax (partial until the deferred rows ran), xcomplete, rn_declined
     OZB_CHECK(cudaMemcpyAsync(res, &sc->valid, sizeof(res), cudaMemcpyDeviceToHost, s));
     OZB_CHECK(cudaStreamSynchronize(s));
@@ -1262,6 +1264,7 @@ int csrmv_fused(cuozblasHandle_t *h, int m, int n, double alpha, const double *v
     if (rn && res[5]) {  // the row kernel declined: the slice kernel computes every row
         if (m > 0) counted(h);
         OZB_TRY(csr_rows_launch(s, args, sc, slow, -1, nullptr, 0, nullptr, nullptr));
+        span_end(h);
         OZB_CHECK(cudaMemcpyAsync(res, &sc->valid, sizeof(res), cudaMemcpyDeviceToHost, s));
         OZB_CHECK(cudaStreamSynchronize(s));
     }

@@ -254,6 +254,7 @@ int dot_exact(cuozblasHandle_t *h, int n, const double *x, const double *y, doub
     const bool same = (x == y);
     const bool aligned = ((reinterpret_cast<uintptr_t>(x) | reinterpret_cast<uintptr_t>(y)) & 15u) == 0;
     const int nsm = sm_count();
+    span_begin(h);
     int blocks = (int)(((int64_t)n + 8LL * kXThreads - 1) / (8LL * kXThreads));
     if (blocks > nsm * 4) blocks = nsm * 4;
     if (blocks > kXMaxBlocks) blocks = kXMaxBlocks;
@@ -291,6 +292,7 @@ int dot_exact(cuozblasHandle_t *h, int n, const double *x, const double *y, doub
     }
 #undef OZB_PROVE
     OZB_CHECK(cudaGetLastError());
+    span_end(h);
     static_assert(sizeof(DotStatus) == 24, "status block layout");
     OZB_CHECK(cudaMemcpyAsync(st->h_dbl, &sc->out, sizeof(DotStatus), cudaMemcpyDeviceToHost, st->stream));
     OZB_CHECK(cudaStreamSynchronize(st->stream));

@@ -394,10 +394,12 @@ int dot_fused(cuozblasHandle_t *h, int n, const double *x, const double *y, doub
     const int rho = rho_rule(n, h->splitEpsMode);
     OZB_CHECK(cudaMemsetAsync(sc, 0, sizeof(DotScratch), st->stream));
     const int nsm = sm_count();
+    span_begin(h);
     counted(h);
     OZB_TRY(dot_scan_launch(st->stream, nsm, n, x, y, sc));
     counted(h);
     OZB_TRY(dot_tree_launch(st->stream, nsm, n, x, y, rho, maxS, h->sumMode, sc, nullptr, st->env.dot_tree));
+    span_end(h);
     static_assert(sizeof(DotStatus) == 24, "status block layout");
     OZB_CHECK(cudaMemcpyAsync(st->h_dbl, &sc->out, sizeof(DotStatus), cudaMemcpyDeviceToHost, st->stream));
     OZB_CHECK(cudaStreamSynchronize(st->stream));

@@ -461,12 +461,9 @@ int gemm_plain_core(cuozblasHandle_t *h, char ta, char tb, int m, int n, int k, 
             h->nSplitC = (float)(ml + 1 < nAv ? ml + 1 : nAv);
             h->mbk = m;
             h->nbk = n;
-            ev_record(h, 1);
-            ev_record(h, 2);
-            ev_record(h, 3);
-            ev_record(h, 4);
-            return CUOZBLAS_STATUS_SUCCESS;
+            return CUOZBLAS_STATUS_SUCCESS;  // gemv_rn_n recorded the span of its kernels (t_comp)
         }
+        ev_record(h, 0);
     }
     // GEMV 'n' (rows of A strided): fused split and products, A read nA + 2 times
     if (skinny_n && !dot && !is_trans(ta) && !state(h)->env.gemv_split) {

@@ -210,6 +210,7 @@ int gemv_rn_n(cuozblasHandle_t *h, int m, int n, const double *A, int lda, const
     OZB_CHECK(cudaMemsetAsync(gs, 0, sizeof(GemvRnStatus), s));
     OZB_CHECK(cudaMemsetAsync(xs, 0, sizeof(CsrScratch), s));
     const int nsm = sm_count();
+    span_begin(h);
     // x: statistics, then the proof of its predicted chain (count and completeness)
     counted(h);
     OZB_TRY(vec_stats_launch(s, nsm, n, x, &xs->vs, 0));
@@ -228,6 +229,7 @@ int gemv_rn_n(cuozblasHandle_t *h, int m, int n, const double *A, int lda, const
     counted(h);
     k_gemv_rn_done<<<1, 1, 0, s>>>(gs, xs);
     OZB_CHECK(cudaGetLastError());
+    span_end(h);
     int res[5];  // done, nA (from the status), nB
     OZB_CHECK(cudaMemcpyAsync(&res[0], &gs->done, sizeof(int) * 2, cudaMemcpyDeviceToHost, s));
     OZB_CHECK(cudaMemcpyAsync(&res[2], &xs->nB, sizeof(int), cudaMemcpyDeviceToHost, s));

@@ -81,6 +81,17 @@ inline float ev_ms(cuozblasHandle_t *h, int a, int b) {
     return ms;
 }
 
+// The device span of a call's kernels as the exec info's t_comp (events 0-2
+// before the first launch, 3-4 after the last, read at the call's end).
+inline void span_begin(cuozblasHandle_t *h) {
+    for (int i = 0; i < 3; i++) ev_record(h, i);
+}
+inline void span_end(cuozblasHandle_t *h) {
+    ev_record(h, 3);
+    ev_record(h, 4);
+    state(h)->plain_timers = true;
+}
+
 // Bump allocation from the handle's arena (no cudaMalloc on the call path).
 struct Arena {
     cuozblasHandle_t *h;
