@@ -40,6 +40,74 @@ __device__ __forceinline__ void scan_elem(double v, double &mx, int &lsb, int &b
     }
 }
 
+// scan_elem with fewer integer operations: the maximum by fmax (a NaN only
+// matters together with `bad`, which every consumer checks first), the
+// lowest set bit from the 32-bit halves.
+__device__ __forceinline__ void scan_elem_fast(double v, double &mx, int &lsb, int &bad) {
+    mx = fmax(mx, fabs(v));
+    const unsigned hw = (unsigned)__double2hiint(v) & 0x7fffffffu, lw = (unsigned)__double2loint(v);
+    const int be = (int)(hw >> 20);
+    bad |= be == 0x7ff;
+    // lowest set bit: the exponent of the last significand bit (the implicit
+    // bit stands in for an all-zero fraction; subnormals use exponent -1074)
+    const int c = lw ? __ffs(lw) - 1 : 31 + __ffs((hw & 0xfffffu) | 0x100000u);
+    const int l = max(be, 1) - 1075 + c;
+    if ((hw | lw) != 0u && be != 0x7ff) lsb = max(lsb, kLsbBias - l);
+}
+
+// The statistics of one vector in a streaming kernel, with the lowest set bit
+// computed lazily: an element can lower the lowest set bit exponent `lb` only
+// if its ulp exponent max(be, 1) - 1075 is below it, which a warp-uniform
+// threshold (the warp's lowest lb, + 1075 in biased-exponent units) tests in
+// a few integer operations; the exact exponent (and the candidate element)
+// is computed only when some lane passes.  Inf / NaN show in the largest
+// high word.
+struct LazyStats {
+    double mx = 0.0;    // max |v| (fmax: NaN shows in hmax instead)
+    unsigned hmax = 0;  // largest high word of |v|
+    int lb = 4000;      // lowest set-bit exponent (4000: no nonzero element yet)
+    int thr = 5075;     // warp-uniform: a nonzero element with max(be, 1) >= thr cannot lower lb
+    double cand = 0.0;  // an element whose lowest set bit is lb
+};
+
+__device__ __forceinline__ void lazy_elem(LazyStats &st, double v) {
+    st.mx = fmax(st.mx, fabs(v));
+    const unsigned hw = (unsigned)__double2hiint(v) & 0x7fffffffu, lw = (unsigned)__double2loint(v);
+    st.hmax = max(st.hmax, hw);
+    const int mb = max((int)(hw >> 20), 1);
+    const bool pass = mb < st.thr && (hw | lw) != 0u && mb != 0x7ff;
+    if (__any_sync(0xffffffffu, pass)) {  // uniform
+        const int c = lw ? __ffs(lw) - 1 : 31 + __ffs((hw & 0xfffffu) | 0x100000u);
+        const int l = mb - 1075 + c;
+        if (pass && l < st.lb) {
+            st.lb = l;
+            st.cand = v;
+        }
+    }
+}
+
+// After each step: the warp's threshold from its lowest lb.
+__device__ __forceinline__ void lazy_sync(LazyStats &st) { st.thr = __reduce_min_sync(0xffffffffu, st.lb) + 1075; }
+
+__device__ __forceinline__ int lazy_key(const LazyStats &st) { return st.lb < 4000 ? kLsbBias - st.lb : 0; }
+__device__ __forceinline__ int lazy_bad(const LazyStats &st) { return st.hmax >= 0x7ff00000u; }
+
+// The per-lane form (lanes that scan different vectors, e.g. the rows of a
+// matrix): the threshold is the lane's own, the exact exponent is computed
+// when some lane of the warp passes.
+__device__ __forceinline__ void lazy_elem1(LazyStats &st, double v) {
+    st.mx = fmax(st.mx, fabs(v));
+    const unsigned hw = (unsigned)__double2hiint(v) & 0x7fffffffu, lw = (unsigned)__double2loint(v);
+    st.hmax = max(st.hmax, hw);
+    const int mb = max((int)(hw >> 20), 1);
+    const bool pass = mb < st.lb + 1075 && (hw | lw) != 0u && mb != 0x7ff;
+    if (__any_sync(0xffffffffu, pass)) {  // uniform
+        const int c = lw ? __ffs(lw) - 1 : 31 + __ffs((hw & 0xfffffu) | 0x100000u);
+        const int l = mb - 1075 + c;
+        if (pass && l < st.lb) st.lb = l;
+    }
+}
+
 // Fold one thread's statistics of vector v into `vs` (every thread of the
 // block calls this; `red` holds one double per warp).
 __device__ __forceinline__ void scan_commit(VecStats *vs, int v, double mx, int lsb, int bad, double *red) {

@@ -32,12 +32,20 @@ namespace ozb {
 
 constexpr int kXThreads = 256;
 
+// Witness candidates of one block of the ring kernel: its largest |x| and the
+// x element with the lowest set bit (the same for y).  Large elements carry
+// the bits of the first levels, the lowest-bit ones those of the deepest.
+struct DotCand {
+    double mx, cx, my, cy;
+};
+
 struct DotExactScratch {
     XReduce xr;                // the blocks' bins of k_dot_exact
     unsigned ticket2;          // blocks of k_dot_prove that are done
     int certified;
     double result;             // certified RN(x . y)
     unsigned proven[2];        // levels whose predicted tau some element proved
+    DotCand cand[kXMaxBlocks];
 };
 
 // ---- one pass: statistics and exact bins ----------------------------------
@@ -175,10 +183,153 @@ __device__ __forceinline__ void prove_element(double x0, double y0, double x1, d
     }
 }
 
+// The aligned form: each thread streams its double2 pairs of x and y through
+// a private cp.async ring (kXStages groups of kXU pairs per vector; a thread
+// reads back only its own copies, so no barrier), four products per group
+// with one warp-wide fit and lean deposits (bounds per group).  The ring is
+// reused as the last block's scratch.
+constexpr int kXU = 2;
+constexpr int kXStages = 4;
+constexpr int kXLeanKD = 4;
+
+template <bool SAME>
+__host__ __device__ constexpr int dot_ring_bytes() {
+    return kXStages * (SAME ? 1 : 2) * kXU * kXThreads * (int)sizeof(double2);
+}
+
+template <bool SAME>
+__global__ void __launch_bounds__(kXThreads) k_dot_exact_ring(int n, const double *__restrict__ x,
+                                                              const double *__restrict__ y, DotScratch *__restrict__ sc,
+                                                              DotExactScratch *__restrict__ xs) {
+    constexpr int V = SAME ? 1 : 2;
+    static_assert(dot_ring_bytes<SAME>() >= 256 * (kXK2 + 3) * (int)sizeof(double), "ring too small for the scratch");
+    extern __shared__ __align__(16) double2 dring[];
+    auto ring = reinterpret_cast<double2(*)[V][kXU][kXThreads]>(dring);
+    __shared__ double red[kXThreads / 32];
+    __shared__ double res_sh;
+    __shared__ int cert_sh;
+    const int t = threadIdx.x;
+    XAcc acc;
+    xacc_init(acc);
+    LazyStats sx, sy;
+    const int64_t np = (int64_t)n >> 1;
+    const int64_t stride = (int64_t)gridDim.x * kXThreads;
+    const double2 *x2 = reinterpret_cast<const double2 *>(x);
+    const double2 *y2 = reinterpret_cast<const double2 *>(y);
+    // every lane of a warp runs the same number of steps (the bins' B is warp-uniform)
+    const int64_t iw = (int64_t)blockIdx.x * kXThreads + (t & ~31);
+    const int64_t steps = iw < np ? (np - iw + kXU * stride - 1) / (kXU * stride) : 0;
+    const int64_t i0 = (int64_t)blockIdx.x * kXThreads + t;
+    auto issue = [&](int64_t s) {
+        if (s < steps) {
+#pragma unroll
+            for (int u = 0; u < kXU; u++) {
+                const int64_t k = i0 + (s * kXU + u) * stride;
+                const bool ok = k < np;
+                cp_async16(&ring[s % kXStages][0][u][t], x2 + (ok ? k : 0), ok);
+                if (!SAME) cp_async16(&ring[s % kXStages][V - 1][u][t], y2 + (ok ? k : 0), ok);
+            }
+        }
+        cp_async_commit();
+    };
+#pragma unroll
+    for (int s = 0; s < kXStages - 1; s++) issue(s);
+    for (int64_t s = 0; s < steps; s++) {
+        cp_async_wait<kXStages - 2>();
+        double2 a[kXU], b[kXU];
+#pragma unroll
+        for (int u = 0; u < kXU; u++) {
+            a[u] = ring[s % kXStages][0][u][t];
+            b[u] = SAME ? a[u] : ring[s % kXStages][V - 1][u][t];
+        }
+        issue(s + kXStages - 1);  // into the slot read in the previous step (this thread's own)
+        unsigned hi = 0u;
+#pragma unroll
+        for (int u = 0; u < kXU; u++) {
+            hi = max(hi, abs_hiword(__dmul_rn(a[u].x, b[u].x)));
+            hi = max(hi, abs_hiword(__dmul_rn(a[u].y, b[u].y)));
+            lazy_elem(sx, a[u].x);
+            lazy_elem(sx, a[u].y);
+            if (!SAME) {
+                lazy_elem(sy, b[u].x);
+                lazy_elem(sy, b[u].y);
+            }
+        }
+        lazy_sync(sx);
+        if (!SAME) lazy_sync(sy);
+        xacc_fit(acc, __reduce_max_sync(0xffffffffu, hi));
+#pragma unroll
+        for (int u = 0; u < kXU; u++) {
+            xacc_product_lean<kXLeanKD>(acc, a[u].x, b[u].x);
+            xacc_product_lean<kXLeanKD>(acc, a[u].y, b[u].y);
+        }
+        xacc_lean_bounds<kXLeanKD>(acc, hi, 2 * kXU);
+        if ((s & 15) == 15) xacc_normalize(acc);  // every 64 products per lane
+    }
+    cp_async_wait<0>();
+    if ((n & 1) && blockIdx.x == 0 && t < 32) {  // the odd last element, one warp
+        const double xe = t == 0 ? x[n - 1] : 0.0;
+        const double ye = t == 0 ? y[n - 1] : 0.0;
+        lazy_elem(sx, xe);
+        if (!SAME) lazy_elem(sy, ye);
+        xacc_normalize(acc);
+        xacc_fit(acc, __reduce_max_sync(0xffffffffu, abs_hiword(__dmul_rn(xe, ye))));
+        xacc_product(acc, xe, ye);
+    }
+    {  // the block's candidates: per warp, then warp 0 over the warps
+        __shared__ double cw[kXThreads / 32][4];
+        __shared__ int kw[kXThreads / 32][2];
+        double m0 = sx.mx, m1 = sy.mx;
+        for (int o = 16; o > 0; o >>= 1) {
+            m0 = fmax(m0, __shfl_xor_sync(0xffffffffu, m0, o));
+            if (!SAME) m1 = fmax(m1, __shfl_xor_sync(0xffffffffu, m1, o));
+        }
+        const int lk0 = lazy_key(sx), lk1 = lazy_key(sy);
+        const int k0 = __reduce_max_sync(0xffffffffu, lk0), k1 = SAME ? 0 : __reduce_max_sync(0xffffffffu, lk1);
+        const double c0 = __shfl_sync(0xffffffffu, sx.cand, __ffs(__ballot_sync(0xffffffffu, lk0 == k0)) - 1);
+        const double c1 =
+            SAME ? 0.0 : __shfl_sync(0xffffffffu, sy.cand, __ffs(__ballot_sync(0xffffffffu, lk1 == k1)) - 1);
+        if ((t & 31) == 0) {
+            cw[t >> 5][0] = m0;
+            cw[t >> 5][1] = c0;
+            cw[t >> 5][2] = m1;
+            cw[t >> 5][3] = c1;
+            kw[t >> 5][0] = k0;
+            kw[t >> 5][1] = k1;
+        }
+        __syncthreads();
+        if (t == 0) {
+            DotCand c{cw[0][0], cw[0][1], cw[0][2], cw[0][3]};
+            int b0 = kw[0][0], b1 = kw[0][1];
+            for (int w = 1; w < kXThreads / 32; w++) {
+                c.mx = fmax(c.mx, cw[w][0]);
+                c.my = fmax(c.my, cw[w][2]);
+                if (kw[w][0] > b0) {
+                    b0 = kw[w][0];
+                    c.cx = cw[w][1];
+                }
+                if (kw[w][1] > b1) {
+                    b1 = kw[w][1];
+                    c.cy = cw[w][3];
+                }
+            }
+            xs->cand[blockIdx.x] = c;
+        }
+    }
+    scan_commit(&sc->vs, 0, sx.mx, lazy_key(sx), lazy_bad(sx), red);
+    if (!SAME) scan_commit(&sc->vs, 1, sy.mx, lazy_key(sy), lazy_bad(sy), red);
+    __syncthreads();  // every thread is done with the ring before it becomes the scratch
+    if (!xreduce_finish_sh(acc, &xs->xr, &res_sh, &cert_sh, reinterpret_cast<double *>(dring))) return;
+    if (t == 0) {
+        xs->result = res_sh;
+        xs->certified = cert_sh;
+    }
+}
+
 template <int G, bool SAME>
 __global__ void __launch_bounds__(kXThreads) k_dot_prove(int n, const double *__restrict__ x,
                                                          const double *__restrict__ y, int rho, int maxS,
-                                                         DotScratch *__restrict__ sc,
+                                                         int ncand, DotScratch *__restrict__ sc,
                                                          DotExactScratch *__restrict__ xs) {
     __shared__ TreePlan pl;
     __shared__ int done_sh, last;
@@ -187,10 +338,30 @@ __global__ void __launch_bounds__(kXThreads) k_dot_prove(int n, const double *__
     __syncthreads();
     unsigned prov[2] = {0u, 0u};  // per warp (uniform)
     const unsigned need0 = pl.need[0], need1 = SAME ? 0u : pl.need[1];
+    if (pl.valid && (need0 | need1) && (int)blockIdx.x * kXThreads < ncand) {
+        // first the ring kernel's per-block candidates (its largest and its
+        // lowest-bit elements), one per thread: on ordinary data they prove
+        // every level, deep ones included, in this single round
+        const int i = (int)blockIdx.x * kXThreads + t;
+        DotCand c{0.0, 0.0, 0.0, 0.0};
+        if (i < ncand)
+            c = DotCand{__ldcg(&xs->cand[i].mx), __ldcg(&xs->cand[i].cx), __ldcg(&xs->cand[i].my),
+                        __ldcg(&xs->cand[i].cy)};
+        prove_element<G, SAME>(c.mx, c.my, c.cx, c.cy, pl, prov);
+        if ((t & 31) == 0) {
+            if (prov[0]) atomicOr(&xs->proven[0], prov[0]);
+            if (!SAME && prov[1]) atomicOr(&xs->proven[1], prov[1]);
+        }
+        __threadfence();
+        __syncthreads();  // the block's own witnesses are published before its first check
+    }
     if (pl.valid && (need0 | need1)) {
-        const int64_t stride = (int64_t)gridDim.x * kXThreads;  // in element pairs (two per lane)
+        // kPP pairs per lane per round (their loads in flight together), then
+        // the global proof state decides whether the block goes on
+        constexpr int kPP = 4;
+        const int64_t stride = (int64_t)gridDim.x * kXThreads * kPP;  // in element pairs (two per lane)
         const int64_t npairs = ((int64_t)n + 1) >> 1;
-        for (int64_t base = (int64_t)blockIdx.x * kXThreads; base < npairs; base += stride) {
+        for (int64_t base = (int64_t)blockIdx.x * kXThreads * kPP; base < npairs; base += stride) {
             if (t == 0) {
                 const unsigned g0 = __ldcg(&xs->proven[0]), g1 = __ldcg(&xs->proven[1]);
                 done_sh = (g0 & need0) == need0 && (g1 & need1) == need1;
@@ -199,11 +370,18 @@ __global__ void __launch_bounds__(kXThreads) k_dot_prove(int n, const double *__
             const int stop = done_sh;
             __syncthreads();
             if (stop) break;
-            const int64_t i = base + t, e0 = 2 * i, e1 = 2 * i + 1;
-            const double x0 = e0 < n ? x[e0] : 0.0, x1 = e1 < n ? x[e1] : 0.0;
-            const double y0 = SAME ? x0 : (e0 < n ? y[e0] : 0.0), y1 = SAME ? x1 : (e1 < n ? y[e1] : 0.0);
+            double xv[kPP][2], yv[kPP][2];
+#pragma unroll
+            for (int q = 0; q < kPP; q++) {
+                const int64_t i = base + q * kXThreads + t, e0 = 2 * i, e1 = 2 * i + 1;
+                xv[q][0] = e0 < n ? x[e0] : 0.0;
+                xv[q][1] = e1 < n ? x[e1] : 0.0;
+                yv[q][0] = SAME ? xv[q][0] : (e0 < n ? y[e0] : 0.0);
+                yv[q][1] = SAME ? xv[q][1] : (e1 < n ? y[e1] : 0.0);
+            }
             const unsigned before0 = prov[0], before1 = prov[1];
-            prove_element<G, SAME>(x0, y0, x1, y1, pl, prov);
+#pragma unroll
+            for (int q = 0; q < kPP; q++) prove_element<G, SAME>(xv[q][0], yv[q][0], xv[q][1], yv[q][1], pl, prov);
             if ((t & 31) == 0) {
                 if (prov[0] != before0) atomicOr(&xs->proven[0], prov[0]);
                 if (!SAME && prov[1] != before1) atomicOr(&xs->proven[1], prov[1]);
@@ -260,11 +438,30 @@ int dot_exact(cuozblasHandle_t *h, int n, const double *x, const double *y, doub
     if (blocks > kXMaxBlocks) blocks = kXMaxBlocks;
     if (blocks < 1) blocks = 1;
     counted(h);
+    int ncand = 0;  // blocks of the ring kernel, each leaving its witness candidates
     if (aligned) {
+        // one wave of the ring kernel: its resident blocks per SM x SMs
+        static std::atomic<uint64_t> attr_s{0}, attr_d{0};
+        static std::atomic<int> occ_s{0}, occ_d{0};
+        const void *fn = same ? (const void *)k_dot_exact_ring<true> : (const void *)k_dot_exact_ring<false>;
+        const int smem = same ? dot_ring_bytes<true>() : dot_ring_bytes<false>();
+        if (smem_optin(fn, smem, same ? attr_s : attr_d) != cudaSuccess) return CUOZBLAS_STATUS_CUDA_ERROR;
+        std::atomic<int> &oc = same ? occ_s : occ_d;
+        int occ = oc.load();
+        if (occ == 0) {
+            if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, kXThreads, smem) != cudaSuccess || occ < 1)
+                occ = 1;
+            oc.store(occ);
+        }
+        int rb = (int)(((int64_t)n / 2 + (int64_t)kXU * kXThreads - 1) / ((int64_t)kXU * kXThreads));
+        if (rb > nsm * occ) rb = nsm * occ;
+        if (rb > kXMaxBlocks) rb = kXMaxBlocks;
+        if (rb < 1) rb = 1;
+        ncand = rb;
         if (same)
-            k_dot_exact<true, true><<<blocks, kXThreads, 0, st->stream>>>(n, x, y, sc, xs);
+            k_dot_exact_ring<true><<<rb, kXThreads, smem, st->stream>>>(n, x, y, sc, xs);
         else
-            k_dot_exact<false, true><<<blocks, kXThreads, 0, st->stream>>>(n, x, y, sc, xs);
+            k_dot_exact_ring<false><<<rb, kXThreads, smem, st->stream>>>(n, x, y, sc, xs);
     } else {
         if (same)
             k_dot_exact<true, false><<<blocks, kXThreads, 0, st->stream>>>(n, x, y, sc, xs);
@@ -273,16 +470,17 @@ int dot_exact(cuozblasHandle_t *h, int n, const double *x, const double *y, doub
     }
     OZB_CHECK(cudaGetLastError());
     const int G = chain_group(rho, 4);
-    int pblocks = (int)((((int64_t)n + 1) / 2 + kXThreads - 1) / kXThreads);
+    int pblocks = (int)((((int64_t)n + 1) / 2 + 4 * kXThreads - 1) / (4 * kXThreads));  // kPP = 4 pairs per lane
     if (pblocks > nsm * 2) pblocks = nsm * 2;
+    if (pblocks < (ncand + kXThreads - 1) / kXThreads) pblocks = (ncand + kXThreads - 1) / kXThreads;
     if (pblocks < 1) pblocks = 1;
     counted(h);
 #define OZB_PROVE(GG)                                                                                       \
     do {                                                                                                  \
         if (same)                                                                                         \
-            k_dot_prove<GG, true><<<pblocks, kXThreads, 0, st->stream>>>(n, x, y, rho, maxS, sc, xs);     \
+            k_dot_prove<GG, true><<<pblocks, kXThreads, 0, st->stream>>>(n, x, y, rho, maxS, ncand, sc, xs); \
         else                                                                                              \
-            k_dot_prove<GG, false><<<pblocks, kXThreads, 0, st->stream>>>(n, x, y, rho, maxS, sc, xs);    \
+            k_dot_prove<GG, false><<<pblocks, kXThreads, 0, st->stream>>>(n, x, y, rho, maxS, ncand, sc, xs); \
     } while (0)
     switch (G) {
         case 1: OZB_PROVE(1); break;

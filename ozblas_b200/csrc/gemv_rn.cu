@@ -7,23 +7,25 @@
 // its grid), so when the row's split and x's split are complete their sum is
 // the exact row dot and NearSum returns its correct rounding.  Here:
 //
-//  k_gemv_rn_part   one thread per (row, chunk of columns): the exact dot of
-//                   that chunk in fixed-grid bins (xbins.cuh), plus the chunk's
+//  k_gemv_rn_part   one thread per (row, range of columns): the exact dot of
+//                   that range in fixed-grid bins (xbins.cuh), plus the range's
 //                   statistics of the row (max, lowest set bit, Inf/NaN); A is
-//                   read once, in its column-major order (lanes = rows).
+//                   read once, in its column-major order (lanes = rows), through
+//                   a per-thread cp.async ring; rows x ranges fill one wave.
 //  k_gemv_rn_merge  one thread per row: the certified rounding of the row's
-//                   chunks, the row's predicted split count and whether its
+//                   ranges, the row's predicted split count and whether its
 //                   split is complete (chain.cuh's argument: the actual chain
 //                   descends no slower than the predicted one); the largest
 //                   predicted count and one row holding it.
-//  k_gemv_rn_count  the reference's own split of that one row (level by level)
-//                   gives its actual count: equal to the predicted maximum, it
-//                   is the maximum over all rows (every actual count is at
-//                   most its prediction), which the exec info reports.
 //  k_gemv_rn_write  y = fma(alpha, t, beta y) when every row is complete and
-//                   certified, x's split is proven complete and the count
-//                   holds; otherwise nothing is written and the caller runs
-//                   the fused slice path.
+//                   certified and x's split is proven complete (otherwise
+//                   nothing is written and the caller runs the fused slice
+//                   path).  Its last block splits the row with the largest
+//                   predicted count the reference's way: equal to the
+//                   prediction, that count is the maximum over all rows (every
+//                   actual count is at most its prediction), which the exec
+//                   info reports; otherwise every row's count is taken
+//                   (k_gemv_rn_count_rows, rare).
 #include "fused.h"
 #include "ozb_internal.h"
 #include "sum.cuh"
@@ -31,8 +33,10 @@
 
 namespace ozb {
 
-constexpr int kGrRows = 256;   // rows per block, one per thread
-constexpr int kGrChunk = 512;  // columns per block
+constexpr int kGrRows = 256;  // rows per block, one per thread
+constexpr int kGrGroup = 8;   // columns per group: one cp.async stage, one bin fit
+constexpr int kGrStages = 3;  // cp.async ring depth (48 KB per block: groups in flight per thread)
+constexpr int kGrKD = 3;      // bins a product is cut onto (the window below is bounded per group)
 
 struct GRowPart {
     XPart p;
@@ -48,58 +52,83 @@ struct GemvRnStatus {
     int nA;                   // the rows' split count (exec info)
 };
 
-__global__ void __launch_bounds__(kGrRows) k_gemv_rn_part(int m, int n, const double *__restrict__ A, int lda,
-                                                          const double *__restrict__ x, GRowPart *__restrict__ parts) {
-    __shared__ double xs[kGrChunk];
-    const int row = blockIdx.x * kGrRows + threadIdx.x;
-    const int c0 = blockIdx.y * kGrChunk;
-    const int len = n - c0 < kGrChunk ? n - c0 : kGrChunk;
-    for (int j = threadIdx.x; j < len; j += kGrRows) xs[j] = x[c0 + j];
-    __syncthreads();
-    if (row >= m) return;
+// One thread per (row, range of `cols` columns): each thread streams its own
+// row segment through a private cp.async ring in shared memory (a warp's 32
+// rows are 256 contiguous bytes of a column, so the copies coalesce; a
+// thread reads back only what it copied, so no block barrier is needed),
+// and cuts 8 products per group onto its bins with one fit and one bound.
+__global__ void __launch_bounds__(kGrRows, 3) k_gemv_rn_part(int m, int n, const double *__restrict__ A, int lda,
+                                                          const double *__restrict__ x, int cols,
+                                                          GRowPart *__restrict__ parts) {
+    __shared__ __align__(16) double ring[kGrStages][kGrGroup][kGrRows];
+    const int t = threadIdx.x;
+    const int row = blockIdx.x * kGrRows + t;
+    const int c0 = blockIdx.y * cols;
+    const int len = n - c0 < cols ? n - c0 : cols;
+    if (len <= 0) return;  // uniform
+    // lanes past the last row read that row again (warp votes need every
+    // lane) and write nothing
+    const bool live = row < m;
+    const double *a = A + (live ? row : m - 1) + (size_t)c0 * lda;
+    const double *xc = x + c0;
+    const int ng = len / kGrGroup;
+    auto issue = [&](int g) {
+        if (g < ng) {
+            double(*st)[kGrRows] = ring[g % kGrStages];
+#pragma unroll
+            for (int u = 0; u < kGrGroup; u++) cp_async8(&st[u][t], a + (size_t)(g * kGrGroup + u) * lda);
+        }
+        cp_async_commit();
+    };
+#pragma unroll
+    for (int g = 0; g < kGrStages - 1; g++) issue(g);
     XAcc acc;
     xacc_init(acc);
-    double mx = 0.0;
-    int lsb = 0, bad = 0;
-    const double *a = A + row + (size_t)c0 * lda;
-    int j = 0;
-    for (int blk = 0; j + 8 <= len; j += 8, blk++) {
-        double v[8];
+    LazyStats rs;  // the row's statistics (per lane)
+    for (int g = 0; g < ng; g++) {
+        cp_async_wait<kGrStages - 2>();
+        double v[kGrGroup], w[kGrGroup];
 #pragma unroll
-        for (int u = 0; u < 8; u++) v[u] = __ldg(a + (size_t)(j + u) * lda);
+        for (int u = 0; u < kGrGroup; u++) {
+            v[u] = ring[g % kGrStages][u][t];
+            w[u] = __ldg(xc + g * kGrGroup + u);
+        }
+        issue(g + kGrStages - 1);  // into the slot read in the previous group (this thread's own)
         unsigned hi = 0u;
 #pragma unroll
-        for (int u = 0; u < 8; u++) {
-            scan_elem(v[u], mx, lsb, bad);
-            hi = max(hi, abs_hiword(__dmul_rn(v[u], xs[j + u])));
+        for (int u = 0; u < kGrGroup; u++) {
+            lazy_elem1(rs, v[u]);
+            hi = max(hi, abs_hiword(__dmul_rn(v[u], w[u])));
         }
         xacc_fit1(acc, hi);
 #pragma unroll
-        for (int u = 0; u < 8; u++) xacc_product(acc, v[u], xs[j + u]);
-        if ((blk & 7) == 7) xacc_normalize1(acc);  // every 64 products
+        for (int u = 0; u < kGrGroup; u++) xacc_product_lean<kGrKD>(acc, v[u], w[u]);
+        xacc_lean_bounds<kGrKD>(acc, hi, kGrGroup);
+        if ((g & 7) == 7) xacc_normalize1(acc);  // every 64 products
     }
-    for (; j < len; j++) {
+    cp_async_wait<0>();
+    for (int j = ng * kGrGroup; j < len; j++) {
         const double v = a[(size_t)j * lda];
-        scan_elem(v, mx, lsb, bad);
-        xacc_fit1(acc, abs_hiword(__dmul_rn(v, xs[j])));
-        xacc_product(acc, v, xs[j]);
+        lazy_elem1(rs, v);
+        xacc_fit1(acc, abs_hiword(__dmul_rn(v, xc[j])));
+        xacc_product(acc, v, xc[j]);
     }
     xacc_normalize1(acc);
-    GRowPart g;
-    g.p.B = (double)acc.B;
+    GRowPart gp;
+    gp.p.B = (double)acc.B;
 #pragma unroll
-    for (int k = 0; k < kXK; k++) g.p.a[k] = acc.a[k];
-    g.p.drop = acc.drop;
-    g.p.es = acc.es;
-    g.p.ea = acc.ea;
-    g.p.flags = (double)acc.flags;
-    g.mx = mx;
-    g.lsb = lsb;
-    g.bad = bad;
-    parts[(size_t)blockIdx.y * m + row] = g;
+    for (int k = 0; k < kXK; k++) gp.p.a[k] = acc.a[k];
+    gp.p.drop = acc.drop;
+    gp.p.es = acc.es;
+    gp.p.ea = acc.ea;
+    gp.p.flags = (double)acc.flags;
+    gp.mx = rs.mx;
+    gp.lsb = lazy_key(rs);
+    gp.bad = lazy_bad(rs);
+    if (live) parts[(size_t)blockIdx.y * m + row] = gp;
 }
 
-__global__ void __launch_bounds__(256) k_gemv_rn_merge(int m, int nchunks, const GRowPart *__restrict__ parts, int rho,
+__global__ void __launch_bounds__(64) k_gemv_rn_merge(int m, int nchunks, const GRowPart *__restrict__ parts, int rho,
                                                        int maxS, double *__restrict__ t, GemvRnStatus *st) {
     const int row = blockIdx.x * blockDim.x + threadIdx.x;
     if (row >= m) return;
@@ -132,13 +161,10 @@ __global__ void __launch_bounds__(256) k_gemv_rn_merge(int m, int nchunks, const
 
 // The reference's dense split of one row (src/cpu/ozblas_split.cpp:36-289 on
 // the transposed operand: one line of length n), level by level, for its
-// count.  One block; the row's elements stay in registers.
+// count.  One block of 256 threads; the row's elements stay in registers.
 constexpr int kGrCountPer = 32;  // elements per thread: rows up to 256 * 32 = 8192 entries
-__global__ void __launch_bounds__(256) k_gemv_rn_count(int m, int n, const double *__restrict__ A, int lda, int rho,
-                                                       int maxS, GemvRnStatus *st) {
+__device__ int gemv_row_count(int row, int n, const double *__restrict__ A, int lda, int rho, int maxS) {
     __shared__ double red[8];
-    if (st->incomplete) return;  // uniform
-    const int row = (int)(st->best & 0xffffffffu), pred = (int)(st->best >> 32);
     double r[kGrCountPer];
 #pragma unroll
     for (int e = 0; e < kGrCountPer; e++) {
@@ -166,23 +192,39 @@ __global__ void __launch_bounds__(256) k_gemv_rn_count(int m, int n, const doubl
         }
     }
     int ns = s >= maxS ? maxS : (z < 1 ? 1 : z) + 1;
-    if (ns > maxS) ns = maxS;
-    if (threadIdx.x == 0) {
-        st->count_ok = ns == pred;
-        st->nA = ns;
-    }
+    return ns > maxS ? maxS : ns;
 }
 
-__global__ void __launch_bounds__(256) k_gemv_rn_write(int m, const double *__restrict__ t, double alpha, double beta,
-                                                       double *__restrict__ y, const GemvRnStatus *st,
+// y = fma(alpha, t, beta y) when every row is complete and certified and x's
+// split is proven complete (otherwise nothing is written and the caller runs
+// the fused slice path).  The last block instead splits the row that holds
+// the largest predicted count: equal to the prediction, that count is the
+// maximum over all rows (each actual count is at most its prediction).
+__global__ void __launch_bounds__(256) k_gemv_rn_write(int m, int n, const double *__restrict__ A, int lda, int rho,
+                                                       int maxS, const double *__restrict__ t, double alpha,
+                                                       double beta, double *__restrict__ y, GemvRnStatus *st,
                                                        const CsrScratch *xs) {
-    if (st->incomplete || !st->count_ok || !xs->valid || !xs->xcomplete) return;  // uniform
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < m; i += gridDim.x * blockDim.x)
+    if (st->incomplete || !xs->valid || !xs->xcomplete) return;  // uniform
+    if (blockIdx.x == gridDim.x - 1) {
+        const int row = (int)(st->best & 0xffffffffu), pred = (int)(st->best >> 32);
+        const int ns = gemv_row_count(row, n, A, lda, rho, maxS);
+        if (threadIdx.x == 0) {
+            st->count_ok = ns == pred;
+            st->nA = ns;
+        }
+        return;
+    }
+    const int nb = gridDim.x - 1;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < m; i += nb * blockDim.x)
         y[i] = fma(alpha, t[i], beta * y[i]);
 }
 
-__global__ void k_gemv_rn_done(GemvRnStatus *st, const CsrScratch *xs) {
-    st->done = !st->incomplete && st->count_ok && xs->valid && xs->xcomplete;
+// The rare case of a row whose split has fewer levels than predicted: the
+// actual count of every row (one block per row), the maximum into st->nA.
+__global__ void __launch_bounds__(256) k_gemv_rn_count_rows(int n, const double *__restrict__ A, int lda, int rho,
+                                                            int maxS, GemvRnStatus *st) {
+    const int ns = gemv_row_count(blockIdx.x, n, A, lda, rho, maxS);
+    if (threadIdx.x == 0) atomicMax(&st->nA, ns);
 }
 
 // NearSum GEMV 'n' (fastMode 0) through the exact row dots.  *done = false:
@@ -196,7 +238,24 @@ int gemv_rn_n(cuozblasHandle_t *h, int m, int n, const double *A, int lda, const
     cudaStream_t s = st->stream;
     Arena ar(h);
     const uint64_t mk = ar.mark();
-    const int nchunks = (n + kGrChunk - 1) / kGrChunk;
+    // one wave: row blocks x column ranges ~ the resident blocks of the device
+    // (a range of at least 64 columns, at most 512 ranges: the merge's exact bin sum)
+    const int nsm = sm_count();
+    static std::atomic<int> occ_cached{0};
+    int occ = occ_cached.load();
+    if (occ == 0) {
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_gemv_rn_part, kGrRows, 0) != cudaSuccess || occ < 1)
+            occ = 1;
+        occ_cached.store(occ);
+    }
+    const int rblocks = (m + kGrRows - 1) / kGrRows;
+    int nsplit = nsm * occ / rblocks;
+    const int max_split = (n + 63) / 64 < 512 ? (n + 63) / 64 : 512;
+    if (nsplit > max_split) nsplit = max_split;
+    if (nsplit < 1) nsplit = 1;
+    int cols = (n + nsplit - 1) / nsplit;
+    cols = (cols + kGrGroup - 1) / kGrGroup * kGrGroup;
+    const int nchunks = (n + cols - 1) / cols;
     GRowPart *parts = ar.take<GRowPart>((uint64_t)nchunks * m);
     double *t = ar.take<double>((uint64_t)m);
     GemvRnStatus *gs = ar.take<GemvRnStatus>(1);
@@ -209,7 +268,6 @@ int gemv_rn_n(cuozblasHandle_t *h, int m, int n, const double *A, int lda, const
     const int rho = rho_rule(n, h->splitEpsMode);
     OZB_CHECK(cudaMemsetAsync(gs, 0, sizeof(GemvRnStatus), s));
     OZB_CHECK(cudaMemsetAsync(xs, 0, sizeof(CsrScratch), s));
-    const int nsm = sm_count();
     span_begin(h);
     // x: statistics, then the proof of its predicted chain (count and completeness)
     counted(h);
@@ -217,23 +275,29 @@ int gemv_rn_n(cuozblasHandle_t *h, int m, int n, const double *A, int lda, const
     counted(h);
     OZB_TRY(csr_proof_launch(s, n, x, rho, maxS, xs, nullptr));
     counted(h);
-    k_gemv_rn_part<<<dim3((m + kGrRows - 1) / kGrRows, nchunks), kGrRows, 0, s>>>(m, n, A, lda, x, parts);
+    k_gemv_rn_part<<<dim3(rblocks, nchunks), kGrRows, 0, s>>>(m, n, A, lda, x, cols, parts);
     counted(h);
-    k_gemv_rn_merge<<<(m + 255) / 256, 256, 0, s>>>(m, nchunks, parts, rho, maxS, t, gs);
-    counted(h);
-    k_gemv_rn_count<<<1, 256, 0, s>>>(m, n, A, lda, rho, maxS, gs);
+    k_gemv_rn_merge<<<(m + 63) / 64, 64, 0, s>>>(m, nchunks, parts, rho, maxS, t, gs);
     int wb = (m + 255) / 256;
     if (wb > nsm * 8) wb = nsm * 8;
     counted(h);
-    k_gemv_rn_write<<<wb, 256, 0, s>>>(m, t, alpha, beta, y, gs, xs);
-    counted(h);
-    k_gemv_rn_done<<<1, 1, 0, s>>>(gs, xs);
+    k_gemv_rn_write<<<wb + 1, 256, 0, s>>>(m, n, A, lda, rho, maxS, t, alpha, beta, y, gs, xs);
     OZB_CHECK(cudaGetLastError());
     span_end(h);
-    int res[5];  // done, nA (from the status), nB
-    OZB_CHECK(cudaMemcpyAsync(&res[0], &gs->done, sizeof(int) * 2, cudaMemcpyDeviceToHost, s));
-    OZB_CHECK(cudaMemcpyAsync(&res[2], &xs->nB, sizeof(int), cudaMemcpyDeviceToHost, s));
+    GemvRnStatus gst;
+    CsrScratch xst;
+    OZB_CHECK(cudaMemcpyAsync(&gst, gs, sizeof(gst), cudaMemcpyDeviceToHost, s));
+    OZB_CHECK(cudaMemcpyAsync(&xst, xs, sizeof(xst), cudaMemcpyDeviceToHost, s));
     OZB_CHECK(cudaStreamSynchronize(s));
+    int res[3] = {!gst.incomplete && xst.valid && xst.xcomplete, gst.nA, xst.nB};
+    if (res[0] && !gst.count_ok) {  // y is written; the exec info needs every row's actual count
+        OZB_CHECK(cudaMemsetAsync(&gs->nA, 0, sizeof(int), s));
+        counted(h);
+        k_gemv_rn_count_rows<<<m, 256, 0, s>>>(n, A, lda, rho, maxS, gs);
+        OZB_CHECK(cudaGetLastError());
+        OZB_CHECK(cudaMemcpyAsync(&res[1], &gs->nA, sizeof(int), cudaMemcpyDeviceToHost, s));
+        OZB_CHECK(cudaStreamSynchronize(s));
+    }
     ar.release(mk);
     if (res[0]) {
         *done = true;

@@ -22,6 +22,7 @@
 // plus the total bound (equal results: the rounding of the true sum is
 // determined).
 #pragma once
+#include "chain.cuh"
 #include "ozb_device.cuh"
 #include "sum.cuh"
 
@@ -80,6 +81,44 @@ __device__ __forceinline__ void xacc_product(XAcc &x, double a, double b) {
     xacc_deposit<0>(x, p);
     x.es = __dadd_rn(x.es, e);
     x.ea = __dadd_ru(x.ea, fabs(e));
+}
+
+// Lean form for a group of products fitted together (xacc_fit / xacc_fit1 on
+// their largest high word): p goes into bins 0..KD-1 only, and neither the
+// remainder below bin KD-1 nor |e| is accumulated per product; instead
+// xacc_lean_bounds adds, once per group, bounds that hold for every member:
+// the remainder after bin KD-1 is at most g_{KD-1} / 2 and |e| <= ulp(p) / 2.
+// The flags collect the products TwoProd cannot keep exact (xacc_product):
+// tiny ones here, huge ones in xacc_lean_bounds.
+constexpr unsigned kXTinyHi = (unsigned)(-969 + 1023) << 20;  // high word of 2^-969
+constexpr unsigned kXHugeHi = (unsigned)(1012 + 1023) << 20;  // high word of 2^1012
+
+template <int KD>
+__device__ __forceinline__ void xacc_product_lean(XAcc &x, double a, double b) {
+    const double p = __dmul_rn(a, b);
+    const double e = __fma_rn(a, b, -p);
+    if (abs_hiword(p) < kXTinyHi)  // p tiny or zero: an issue only when both factors are nonzero
+        if (a != 0.0 && b != 0.0) x.flags |= 1;
+    double r = p;
+#pragma unroll
+    for (int j = 0; j < KD; j++) {
+        const double q = __dsub_rn(__dadd_rn(r, x.sig[j]), x.sig[j]);
+        if (j + 1 < KD) r = __dsub_rn(r, q);
+        x.a[j] = __dadd_rn(x.a[j], q);
+    }
+    x.es = __dadd_rn(x.es, e);
+}
+
+// Bounds of a group of `cnt` lean products whose largest |p| has the high
+// word `hi`: drop += cnt g_{KD-1} / 2, ea += cnt 2^(E - 53) (E the exponent of
+// the largest |p|; smaller products have smaller error terms).  Call after
+// the group's deposits with the B they used.
+template <int KD>
+__device__ __forceinline__ void xacc_lean_bounds(XAcc &x, unsigned hi, int cnt) {
+    if (hi >= kXHugeHi) x.flags |= 1;
+    x.drop = __dadd_ru(x.drop, (double)cnt * pow2((x.B - (KD - 1)) * kXW - 1));
+    const int E = (int)(hi >> 20) - 1023;
+    if (hi >= kXTinyHi) x.ea = __dadd_ru(x.ea, (double)cnt * pow2(E - 53));
 }
 
 // Raise B by one: the top bin is cut onto the new top grid, the rest move
@@ -311,30 +350,39 @@ __device__ inline void xparts_round(const XPart *parts, int np, double *sh, doub
             c[j - 1] = __dadd_rn(c[j - 1], q);
         }
     }
-    // every bin is now below 2^(W-1) g (the top two far below): 256 threads add exactly
+    // every bin is now below 2^(W-1) g (the top two far below): 256 threads add
+    // exactly in any order; warps first (shuffles), then the 8 warp sums
     // slots: the kXK2 bins, es, drop, ea
 #pragma unroll
-    for (int j = 0; j < kXK2; j++) sh[j * blockDim.x + t] = c[j];
-    sh[kXK2 * blockDim.x + t] = es;
-    sh[(kXK2 + 1) * blockDim.x + t] = drop;
-    sh[(kXK2 + 2) * blockDim.x + t] = ea;
-    __syncthreads();
-    for (int s = blockDim.x / 2; s > 0; s >>= 1) {
-        if (t < s) {
+    for (int o = 16; o > 0; o >>= 1) {
 #pragma unroll
-            for (int j = 0; j <= kXK2; j++)
-                sh[j * blockDim.x + t] = __dadd_rn(sh[j * blockDim.x + t], sh[j * blockDim.x + t + s]);
-            sh[(kXK2 + 1) * blockDim.x + t] =
-                __dadd_ru(sh[(kXK2 + 1) * blockDim.x + t], sh[(kXK2 + 1) * blockDim.x + t + s]);
-            sh[(kXK2 + 2) * blockDim.x + t] =
-                __dadd_ru(sh[(kXK2 + 2) * blockDim.x + t], sh[(kXK2 + 2) * blockDim.x + t + s]);
+        for (int j = 0; j < kXK2; j++) c[j] = __dadd_rn(c[j], __shfl_xor_sync(0xffffffffu, c[j], o));
+        es = __dadd_rn(es, __shfl_xor_sync(0xffffffffu, es, o));
+        drop = __dadd_ru(drop, __shfl_xor_sync(0xffffffffu, drop, o));
+        ea = __dadd_ru(ea, __shfl_xor_sync(0xffffffffu, ea, o));
+    }
+    const int nw = blockDim.x >> 5;
+    if ((t & 31) == 0) {
+        const int w = t >> 5;
+#pragma unroll
+        for (int j = 0; j < kXK2; j++) sh[j * nw + w] = c[j];
+        sh[kXK2 * nw + w] = es;
+        sh[(kXK2 + 1) * nw + w] = drop;
+        sh[(kXK2 + 2) * nw + w] = ea;
+    }
+    __syncthreads();
+    if (t == 0) {
+        for (int j = 0; j < kXK2 + 3; j++) {
+            double v = sh[j * nw];
+            for (int w = 1; w < nw; w++)
+                v = j == kXK2 + 1 || j == kXK2 + 2 ? __dadd_ru(v, sh[j * nw + w]) : __dadd_rn(v, sh[j * nw + w]);
+            sh[j * nw] = v;
         }
-        __syncthreads();
     }
     if (t == 0) {
         double terms[kXK2 + 2];
-        for (int j = 0; j <= kXK2; j++) terms[j] = sh[j * blockDim.x];
-        const double D = __dadd_ru(sh[(kXK2 + 1) * blockDim.x], xes_bound(sh[(kXK2 + 2) * blockDim.x]));
+        for (int j = 0; j <= kXK2; j++) terms[j] = sh[j * nw];
+        const double D = __dadd_ru(sh[(kXK2 + 1) * nw], xes_bound(sh[(kXK2 + 2) * nw]));
         int ok = s_flags == 0;
         double r = 0.0;
         if (ok) {
@@ -370,10 +418,11 @@ struct XReduce {
 // into its part; returns true, in every thread of the last block only, with
 // the certified rounding of the total in *result and *certified (shared
 // memory, valid for all threads of that block).
-__device__ inline bool xreduce_finish(XAcc &acc, XReduce *xr, double *result, int *certified) {
+// `sh`: shared scratch of 256 * (kXK2 + 3) doubles (the caller's, e.g. a
+// streaming ring that is no longer in use).
+__device__ inline bool xreduce_finish_sh(XAcc &acc, XReduce *xr, double *result, int *certified, double *sh) {
     __shared__ XPart wsh[8];
     __shared__ int last;
-    __shared__ double sh[256 * (kXK2 + 3)];
     xacc_block_reduce(acc, wsh, xr->part[blockIdx.x]);
     __threadfence();
     __syncthreads();
@@ -385,6 +434,11 @@ __device__ inline bool xreduce_finish(XAcc &acc, XReduce *xr, double *result, in
     if (threadIdx.x == 0) xr->ticket = 0u;
     __syncthreads();
     return true;
+}
+
+__device__ inline bool xreduce_finish(XAcc &acc, XReduce *xr, double *result, int *certified) {
+    __shared__ double sh[256 * (kXK2 + 3)];
+    return xreduce_finish_sh(acc, xr, result, certified, sh);
 }
 
 }  // namespace ozb

@@ -760,3 +760,21 @@ def test_dgemv_nearsum_rows_equal_slices(m, n, phi, oracle, handle, ozb, cuda, m
     monkeypatch.delenv("OZBLAS_GEMV_SLICES")
     handle.read_env()
     assert bits_equal(host(dy2), host(dy))
+
+
+def test_dgemv_nearsum_rows_steep_chain(oracle, handle, ozb, cuda):
+    """NearSum GEMV 'n' where the row with the largest predicted split count splits in fewer levels (its second
+    level already takes the tiny element): the rows' correctly rounded dots are written and the exec-info count
+    comes from every row's own split; both equal the oracle's."""
+    m, n = 300, 64
+    A = oracle.phi_matrix(m, n, 1.0, 11)
+    A[7, :] = 0.0
+    A[7, 0], A[7, 1] = 1.0, 2.0 ** -100
+    x = oracle.phi_vector(n, 1.0, 12)
+    y0 = oracle.phi_vector(m, 1.0, 13)
+    ref, info = oracle.dgemv(make_flags(sumMode=1), "n", m, n, 0.75, A, m, x, -1.5, y0)
+    handle.sumMode = 1
+    dy = dev(cuda, y0)
+    ozb.dgemv(handle, "n", m, n, 0.75, dev(cuda, A), m, dev(cuda, x), -1.5, dy)
+    assert bits_equal(host(dy), ref), first_diff(host(dy), ref)
+    assert (handle.nSplitA, handle.nSplitB, handle.nSplitC) == (info.nSplitA, info.nSplitB, info.nSplitC)
