@@ -50,6 +50,23 @@ N_DIM = 8192
 PHI = 1.0
 METRIC = "Ozaki DGEMM TFLOPS n=8192 (INT8 vs FP64 slices, err vs MPFR); DOT/CSRMV GB/s"
 
+_JSON_FD = None
+
+
+def claim_stdout():
+    """Send everything written to file descriptor 1 from here on (the reference CPU library's own printf
+    included) to stderr, so that standard output carries the JSON line alone."""
+    global _JSON_FD
+    if _JSON_FD is None:
+        sys.stdout.flush()
+        _JSON_FD = os.dup(1)
+        os.dup2(2, 1)
+
+
+def emit(obj):
+    """Write one JSON line to the original standard output."""
+    os.write(_JSON_FD if _JSON_FD is not None else 1, (json.dumps(obj) + "\n").encode())
+
 
 def phi_matrix(rows, cols, phi, seed):
     """(U - 0.5) * exp(phi * N(0,1)) with N from Box-Muller on the same U (column-major rows x cols)."""
@@ -199,7 +216,7 @@ def run_reference_arm(args, rank, world):
         return 0
     ref = _reference()
     if ref is None:
-        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libozblas_ref.so not built"}))
+        emit({"impl": "reference", "unavailable": "oracle/_ref/libozblas_ref.so not built"})
         return 0
     import numpy as np
 
@@ -229,7 +246,7 @@ def run_reference_arm(args, rank, world):
                                    "workload)", "m": n, "n": n, "k": n, "phi": PHI},
             "cpu_baseline": base, "e2e": {"value": v, "unit": "TFLOPS", "h2d_bytes_per_step": 0,
                                           "d2h_bytes_per_step": 0}}
-    print(json.dumps(line))
+    emit(line)
     return 0
 
 
@@ -257,6 +274,7 @@ def main():
                     help="only the mixed-precision forms <double,float,float> and <float,double,double> at m = n = k "
                          "= --n (prints their JSON)")
     args = ap.parse_args()
+    claim_stdout()
     globals()["N_DIM"] = args.n
     args.warmup = max(args.warmup, 3)
 
@@ -276,26 +294,26 @@ def main():
     sizes = [int(v) for v in args.sweep_sizes.split(",") if v.strip()]
     phis = [float(v) for v in args.sweep_phis.split(",") if v.strip()]
     if args.sweep_only:
-        print(json.dumps({"workload": "INT8 form sweep", "extras": sweep_extras(ozb, torch, sizes, phis)}))
+        emit({"workload": "INT8 form sweep", "extras": sweep_extras(ozb, torch, sizes, phis)})
         return 0
     if args.batched_only:
         h = ozb.Handle(work_bytes=24 << 30)
-        print(json.dumps({"workload": "batched uneven Ozaki DGEMM, 256 problems", "reps": args.steps,
-                          "extras": batched_extras(ozb, h, torch, reps=args.steps, cpu=not args.no_cpu)}))
+        emit({"workload": "batched uneven Ozaki DGEMM, 256 problems", "reps": args.steps,
+              "extras": batched_extras(ozb, h, torch, reps=args.steps, cpu=not args.no_cpu)})
         h.close()
         return 0
     if args.mixed_only:
         h = ozb.Handle(work_bytes=32 << 30)
-        print(json.dumps({"workload": f"mixed-precision Ozaki GEMM {args.n}^3, phi = {PHI}", "reps": args.steps,
-                          "extras": mixed_extras(ozb, h, torch, args.n, reps=args.steps)}))
+        emit({"workload": f"mixed-precision Ozaki GEMM {args.n}^3, phi = {PHI}", "reps": args.steps,
+              "extras": mixed_extras(ozb, h, torch, args.n, reps=args.steps)})
         h.close()
         return 0
     if args.memory_only:
         h = ozb.Handle(work_bytes=8 << 30)
         h.nSplitMax = 0
-        print(json.dumps({"workload": "memory-bound plain kernels", "reps": args.steps,
-                          "extras": memory_extras(ozb, h, torch, reps=args.steps, cg_iters=args.cg_iters,
-                                                 cpu=not args.no_cpu)}))
+        emit({"workload": "memory-bound plain kernels", "reps": args.steps,
+              "extras": memory_extras(ozb, h, torch, reps=args.steps, cg_iters=args.cg_iters,
+                                      cpu=not args.no_cpu)})
         h.close()
         return 0
     dist = None
@@ -410,7 +428,7 @@ def main():
         dist.barrier()
         dist.destroy_process_group()
     if rank == 0:
-        print(json.dumps(line))
+        emit(line)
     return 0
 
 
