@@ -471,8 +471,8 @@ int gemm_plain_core(cuozblasHandle_t *h, char ta, char tb, int m, int n, int k, 
         double *xs = ar.take<double>((uint64_t)maxS * ldk);
         if (!ar.ok) return CUOZBLAS_STATUS_WORKSPACE;
         int nBv = 0, nAv = 0;
+        span_begin(h);  // t_comp: the device span of the vector split and the fused kernels
         OZB_TRY(split_vector(h, k, B, rho, maxS, xs, ldk, &nBv));
-        ev_record(h, 1);
         const int fr = gemv_fused_n(h, m, k, A, lda, xs, ldk, nBv, rho, maxS, fastMode, alpha, beta, C, &nAv);
         if (fr == CUOZBLAS_STATUS_SUCCESS) {
             int ml = (nAv - 1) + (nBv - 1);
@@ -488,9 +488,7 @@ int gemm_plain_core(cuozblasHandle_t *h, char ta, char tb, int m, int n, int k, 
             }
             h->mbk = m;
             h->nbk = n;
-            ev_record(h, 2);
-            ev_record(h, 3);
-            ev_record(h, 4);
+            span_end(h);
             return CUOZBLAS_STATUS_SUCCESS;
         }
         if (fr != CUOZBLAS_STATUS_NOT_SUPPORTED) return fr;

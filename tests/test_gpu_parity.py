@@ -85,6 +85,24 @@ def test_phase_timers(oracle, handle, ozb, cuda):
     assert all(v > 0 for v in t) and sum(t) <= handle.t_total * 1.01, (t, handle.t_total)
 
 
+@pytest.mark.parametrize("sum_mode", [0, 1])
+def test_kernel_span_timer(oracle, handle, ozb, cuda, sum_mode):
+    """t_comp holds the device span of the call's kernels on every DOT and GEMV path: positive and no longer
+    than the whole call."""
+    handle.sumMode = sum_mode
+    n = 1 << 16
+    x = dev(cuda, oracle.phi_vector(n, 2.0, 1))
+    y = dev(cuda, oracle.phi_vector(n, 2.0, 2))
+    ozb.ddot(handle, n, x, y)
+    assert 0 < handle.t_comp <= handle.t_total * 1.01, (handle.t_comp, handle.t_total)
+    m = k = 512
+    A = dev(cuda, oracle.phi_matrix(m, k, 1.0, 3))
+    xv = dev(cuda, oracle.phi_vector(k, 1.0, 4))
+    yv = cuda.zeros(m, dtype=cuda.float64, device="cuda")
+    ozb.dgemv(handle, "n", m, k, 1.0, A, m, xv, 0.0, yv)
+    assert 0 < handle.t_comp <= handle.t_total * 1.01, (handle.t_comp, handle.t_total)
+
+
 def test_dgemm_beta0_propagates_nan(oracle, handle, ozb, cuda):
     """C = fma(alpha, t, beta*C) with beta = 0 keeps NaN from C, as the reference does."""
     m = n = k = 8
