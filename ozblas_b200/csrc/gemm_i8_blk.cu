@@ -18,7 +18,7 @@
 //
 // Roles (one CTA per SM, persistent): warp 0 lane 0 loads planes by TMA into
 // two rings (A: 4 slots, B: 8 slots of 16 KB, 128-byte swizzle); warp 1 holds
-// the tensor memory and lane 0 issues tcgen05.mma.kind::i8; warps 2-9 read the
+// the tensor memory and lane 0 issues tcgen05.mma.kind::i8; warps 4-11 read the
 // accumulators after each (block, K chunk), combine the block's levels into
 // the run accumulator in registers, and at a run's end add the run into R,
 // which lives in a per-CTA buffer in global memory (128 KB, L2-resident).
@@ -37,7 +37,12 @@ constexpr int KB_BM = 128, KB_BN = 128, KB_BK = 128;
 constexpr int KB_W = 4;                       // levels per block (tensor-memory accumulators)
 constexpr int KB_RA = 4, KB_RB = 8;           // ring slots for A and B planes
 constexpr int KB_TILE = KB_BM * KB_BK;        // 16 KB plane tile
-constexpr int KB_THREADS = 320;
+constexpr int KB_THREADS = 384;  // warp 0 producer, warp 1 MMA issuer, warps 2-3 idle, warps 4-11 epilogue
+// Registers per thread: 168 at launch (65536 / 384, rounded down to 8); the
+// producer warpgroup drops to KB_REG_LO and the two epilogue warpgroups rise to
+// KB_REG_HI: 4 x 56 + 8 x 224 = 12 x 168, and per SM sub-partition (one warp of
+// each warpgroup) 56 + 2 x 224 <= 512.
+constexpr uint32_t KB_REG_LO = 56, KB_REG_HI = 224;
 constexpr int KB_SMEM = (KB_RA + KB_RB) * KB_TILE + 1024 /*align*/ + 512 /*barriers*/;
 constexpr int64_t KB_MAX_TERMS = 2147483647LL / (127 * 127);
 
@@ -111,7 +116,9 @@ __global__ void __launch_bounds__(KB_THREADS, 1)
     tc::fence_after_sync();
     const uint32_t tmem_base = tmem_slot;
 
-    if (warp == 0) {
+    if (warp < 4) {
+      tc::reg_dealloc<KB_REG_LO>();
+      if (warp == 0) {
         // ---------------------------------------------------------------- producer
         if (lane == 0) {
             uint32_t na = 0, nb = 0;  // planes loaded into each ring
@@ -161,7 +168,7 @@ __global__ void __launch_bounds__(KB_THREADS, 1)
                 tc::drain_copies(fullB, KB_RB, issuedB, phaseB);
             }
         }
-    } else if (warp == 1) {
+      } else if (warp == 1) {
         // ---------------------------------------------------------------- MMA issuer
         if (lane == 0) {
             const uint32_t idesc = tc::idesc_i8(KB_BM, KB_BN);
@@ -240,9 +247,11 @@ __global__ void __launch_bounds__(KB_THREADS, 1)
                 }
             }
         }
+      }
     } else {
+        tc::reg_alloc<KB_REG_HI>();
         // ---------------------------------------------------------------- epilogue
-        const int q = warp & 3, half = (warp - 2) >> 2;
+        const int q = warp & 3, half = (warp - 4) >> 2;
         const int row = q * 32 + lane;
         const uint32_t lane_base = tmem_base + ((uint32_t)(q * 32) << 16);
         double *R = p.rbuf + (size_t)blockIdx.x * (KB_BM * KB_BN);  // [col][row]
