@@ -711,11 +711,12 @@ def batched_extras(ozb, h, torch, reps=3, cpu=True):
     for fast in (0, 1):
         h.nSplitMax, h.fastMode = 0, fast
         l0 = h.launch_count()
-        kms = []
+        kms, sms = [], []
 
         def grouped():
             ozb.dgemm_i8_batched(h, "n", "n", ms, ns, ks, one, As, ms, Bs, ks, zero, Cs, ms)
             kms.append(h.t_comp * 1e3)
+            sms.append(h.t_SplitA * 1e3)
 
         ms_b = timed_ms(torch, grouped, reps)
         launches = (h.launch_count() - l0) / (reps + 1)
@@ -729,7 +730,8 @@ def batched_extras(ozb, h, torch, reps=3, cpu=True):
         ms_l = timed_ms(torch, looped, 1)
         key = "full" if fast == 0 else "triangular"
         out[f"int8_grouped_{key}"] = {"ms": ms_b, "TFLOPS": flops / ms_b / 1e9, "launches": launches,
-                                      "max_slices": slices, "product_kernel_ms": min(kms[1:])}
+                                      "max_slices": slices, "product_kernel_ms": min(kms[1:]),
+                                      "split_ms": min(sms[1:])}
         out[f"int8_looped_{key}"] = {"ms": ms_l, "TFLOPS": flops / ms_l / 1e9}
         out[f"grouped_identical_to_looped_{key}"] = all(bool(torch.equal(a, b)) for a, b in zip(C_batched, Cs))
         if fast == 0:

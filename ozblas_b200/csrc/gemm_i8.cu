@@ -447,7 +447,19 @@ __device__ __forceinline__ int lsb_exp(double v) {  // exponent of the lowest se
     return (be - 1075) + __ffsll((long long)f) - 1;
 }
 
-// One CTA per line: line exponent and the digit count that makes the line exact.
+// Line exponent E (max|x| < 2^E) and the digit count that makes the line
+// exact, need = max over its nonzero x of ceil((E - lsb(x)) / 7) =
+// ceil((E - min lsb) / 7): both statistics in one pass.
+__device__ __forceinline__ void line_stat(double v, double &mx, int &lsb) {
+    mx = ref_max(mx, fabs(v));
+    if (v != 0.0) lsb = min(lsb, lsb_exp(v));
+}
+__device__ __forceinline__ int line_need(double mx, int lsb, int &E) {
+    E = mx > 0.0 ? exp_above(mx) : 0;
+    return mx > 0.0 ? (E - lsb + 6) / 7 : 0;
+}
+
+// k contiguous (element i of line l at X[l * ldx + i]): one CTA per line.
 __global__ void __launch_bounds__(256) k_digit_count(int k, int nl, const double *__restrict__ X, int ldx,
                                                      int *__restrict__ e_out, int *__restrict__ need_max) {
     __shared__ double red[8];
@@ -455,35 +467,81 @@ __global__ void __launch_bounds__(256) k_digit_count(int k, int nl, const double
     const int line = blockIdx.x;
     const double *x = X + (size_t)line * ldx;
     double mx = 0.0;
-    for (int i = threadIdx.x; i < k; i += blockDim.x) mx = ref_max(mx, fabs(x[i]));
-    mx = block_max_nonneg(mx, red);
-    const int E = mx > 0.0 ? exp_above(mx) : 0;
-    int need = 0;
-    if (mx > 0.0)
-        for (int i = threadIdx.x; i < k; i += blockDim.x) {
-            const double v = x[i];
-            if (v != 0.0) {
-                const int d = (E - lsb_exp(v) + 6) / 7;
-                need = need > d ? need : d;
-            }
+    int lsb = 0x7fffffff;
+    if ((reinterpret_cast<uintptr_t>(x) & 15) == 0) {
+        const double2 *x2 = reinterpret_cast<const double2 *>(x);
+        for (int i = threadIdx.x; i < (k >> 1); i += blockDim.x) {
+            const double2 v = x2[i];
+            line_stat(v.x, mx, lsb);
+            line_stat(v.y, mx, lsb);
         }
-    for (int o = 16; o > 0; o >>= 1) {
-        const int t = __shfl_xor_sync(0xffffffffu, need, o);
-        need = need > t ? need : t;
+        if ((k & 1) && threadIdx.x == 0) line_stat(x[k - 1], mx, lsb);
+    } else {
+        for (int i = threadIdx.x; i < k; i += blockDim.x) line_stat(x[i], mx, lsb);
     }
-    __syncthreads();
-    if ((threadIdx.x & 31) == 0) redi[threadIdx.x >> 5] = need;
+    mx = block_max_nonneg(mx, red);
+    lsb = __reduce_min_sync(0xffffffffu, lsb);
+    if ((threadIdx.x & 31) == 0) redi[threadIdx.x >> 5] = lsb;
     __syncthreads();
     if (threadIdx.x == 0) {
-        int r = 0;
-        for (int w = 0; w < (int)(blockDim.x >> 5); w++) r = r > redi[w] ? r : redi[w];
+        for (int w = 1; w < (int)(blockDim.x >> 5); w++) lsb = min(lsb, redi[w]);
+        int E;
+        const int need = line_need(mx, lsb, E);
         e_out[line] = E;
-        atomicMax(need_max, r);
+        atomicMax(need_max, need);
     }
 }
 
+// Lines contiguous (element i of line l at X[i * ldx + l], op(A) = A with A
+// column-major): blocks of 128 lines x a slice of k, per-line partial results
+// merged by atomics; the block that finishes last computes every line's E and
+// the largest need.  mxb / lsbm / ticket start at 0 / above every exponent / 0.
+__global__ void __launch_bounds__(256) k_digit_count_rows(int k, int nl, const double *__restrict__ X, int ldx,
+                                                          unsigned long long *__restrict__ mxb, int *__restrict__ lsbm,
+                                                          unsigned *__restrict__ ticket, int *__restrict__ e_out,
+                                                          int *__restrict__ need_max) {
+    __shared__ double smx[256];
+    __shared__ int slsb[256];
+    __shared__ int last;
+    const int t = threadIdx.x, r = t & 127, l = blockIdx.x * 128 + r;
+    const int kper = (k + gridDim.y - 1) / gridDim.y;
+    const int kb = blockIdx.y * kper, ke = min(k, kb + kper);
+    double mx = 0.0;
+    int lsb = 0x7fffffff;
+    if (l < nl) {
+#pragma unroll 4
+        for (int i = kb + (t >> 7); i < ke; i += 2) line_stat(X[(size_t)i * ldx + l], mx, lsb);
+    }
+    smx[t] = mx;
+    slsb[t] = lsb;
+    __syncthreads();
+    if (t < 128 && l < nl) {
+        mx = ref_max(smx[t], smx[t + 128]);
+        lsb = min(slsb[t], slsb[t + 128]);
+        if (mx > 0.0) atomicMax(&mxb[l], (unsigned long long)__double_as_longlong(mx));
+        if (lsb != 0x7fffffff) atomicMin(&lsbm[l], lsb);
+    }
+    __threadfence();
+    __syncthreads();
+    if (t == 0) last = atomicAdd(ticket, 1u) == gridDim.x * gridDim.y - 1;
+    __syncthreads();
+    if (!last) return;
+    __threadfence();
+    int nmax = 0;
+    for (int i = t; i < nl; i += blockDim.x) {
+        const double m = __longlong_as_double((long long)__ldcg(&mxb[i]));
+        int E;
+        const int nd = line_need(m, __ldcg(&lsbm[i]), E);
+        e_out[i] = E;
+        nmax = max(nmax, nd);
+    }
+    nmax = __reduce_max_sync(0xffffffffu, nmax);
+    if ((t & 31) == 0) atomicMax(need_max, nmax);
+}
+
 // Digits: thread handles 16 consecutive k of one line; writes S slices of
-// lines_pad x k_pad int8 (zero padded in both directions).
+// lines_pad x k_pad int8 (zero padded in both directions).  The digits are cut
+// with integer operations (digit_cut), one 16-byte store per level.
 __global__ void __launch_bounds__(256) k_digit_write(int k, int nl, int nl_pad, int k_pad, int S,
                                                      const double *__restrict__ X, int ldx,
                                                      const int *__restrict__ e_line, int8_t *__restrict__ out) {
@@ -492,27 +550,77 @@ __global__ void __launch_bounds__(256) k_digit_write(int k, int nl, int nl_pad, 
     const int64_t total = (int64_t)nl_pad * per_line;
     if (chunk >= total) return;
     const int line = (int)(chunk / per_line), k0 = (int)(chunk % per_line) * 16;
-    double r[16];
-    if (line < nl) {
-        const int E = e_line[line];
-        const double *x = X + (size_t)line * ldx;
+    uint64_t m7[16];
+    int f[16];
+    uint32_t neg[4] = {0u, 0u, 0u, 0u};  // 0xff in the bytes of negative elements
+    const int E = line < nl ? e_line[line] : 0;
+    const double *x = X + (size_t)(line < nl ? line : 0) * ldx;
+    if (line < nl && k0 + 16 <= k && ((reinterpret_cast<uintptr_t>(x + k0) & 15) == 0)) {
 #pragma unroll
-        for (int i = 0; i < 16; i++) r[i] = (k0 + i < k) ? scalbn(x[k0 + i], -E) : 0.0;
+        for (int i = 0; i < 16; i += 2) {
+            const double2 v = *reinterpret_cast<const double2 *>(x + k0 + i);
+            const DigitCut c0 = digit_cut(v.x, E), c1 = digit_cut(v.y, E);
+            m7[i] = c0.m7;
+            f[i] = c0.f;
+            m7[i + 1] = c1.m7;
+            f[i + 1] = c1.f;
+            if (v.x < 0.0) neg[i >> 2] |= 0xffu << (8 * (i & 3));
+            if (v.y < 0.0) neg[i >> 2] |= 0xffu << (8 * ((i + 1) & 3));
+        }
     } else {
 #pragma unroll
-        for (int i = 0; i < 16; i++) r[i] = 0.0;
+        for (int i = 0; i < 16; i++) {
+            const double v = (line < nl && k0 + i < k) ? x[k0 + i] : 0.0;
+            const DigitCut c = digit_cut(v, E);
+            m7[i] = c.m7;
+            f[i] = c.f;
+            if (v < 0.0) neg[i >> 2] |= 0xffu << (8 * (i & 3));
+        }
     }
     for (int s = 0; s < S; s++) {
-        uint32_t w[4] = {0, 0, 0, 0};
+        uint32_t w[4] = {0u, 0u, 0u, 0u};
 #pragma unroll
         for (int i = 0; i < 16; i++) {
-            const double t = r[i] * 128.0;
-            const double d = trunc(t);
-            r[i] = t - d;
-            w[i >> 2] |= ((uint32_t)(uint8_t)(int8_t)(int)d) << (8 * (i & 3));
+            w[i >> 2] |= digit_mag(m7[i], f[i]) << (8 * (i & 3));
+            f[i] -= 7;
         }
         int4 *o = reinterpret_cast<int4 *>(out + ((size_t)s * nl_pad + line) * k_pad + k0);
-        *o = make_int4((int)w[0], (int)w[1], (int)w[2], (int)w[3]);
+        *o = make_int4((int)digits_signed(w[0], neg[0]), (int)digits_signed(w[1], neg[1]),
+                       (int)digits_signed(w[2], neg[2]), (int)digits_signed(w[3], neg[3]));
+    }
+}
+
+// Digits of lines contiguous in memory (element i of line l at X[i * ldx + l]):
+// thread (line r of a 128-line tile, 16 consecutive k), loads coalesced across
+// the lines, the same digits and layout as k_digit_write (no transposed copy).
+__global__ void __launch_bounds__(256) k_digit_write_rows(int k, int nl, int nl_pad, int k_pad, int S,
+                                                          const double *__restrict__ X, int ldx,
+                                                          const int *__restrict__ e_line, int8_t *__restrict__ out) {
+    const int t = threadIdx.x, line = blockIdx.x * 128 + (t & 127);
+    const int k0 = (blockIdx.y * 2 + (t >> 7)) * 16;
+    if (line >= nl_pad || k0 >= k_pad) return;
+    uint64_t m7[16];
+    int f[16];
+    uint32_t neg[4] = {0u, 0u, 0u, 0u};
+    const int E = line < nl ? e_line[line] : 0;
+#pragma unroll
+    for (int i = 0; i < 16; i++) {
+        const double v = (line < nl && k0 + i < k) ? X[(size_t)(k0 + i) * ldx + line] : 0.0;
+        const DigitCut c = digit_cut(v, E);
+        m7[i] = c.m7;
+        f[i] = c.f;
+        if (v < 0.0) neg[i >> 2] |= 0xffu << (8 * (i & 3));
+    }
+    for (int s = 0; s < S; s++) {
+        uint32_t w[4] = {0u, 0u, 0u, 0u};
+#pragma unroll
+        for (int i = 0; i < 16; i++) {
+            w[i >> 2] |= digit_mag(m7[i], f[i]) << (8 * (i & 3));
+            f[i] -= 7;
+        }
+        int4 *o = reinterpret_cast<int4 *>(out + ((size_t)s * nl_pad + line) * k_pad + k0);
+        *o = make_int4((int)digits_signed(w[0], neg[0]), (int)digits_signed(w[1], neg[1]),
+                       (int)digits_signed(w[2], neg[2]), (int)digits_signed(w[3], neg[3]));
     }
 }
 
@@ -578,22 +686,36 @@ struct DigitOperand {
 static int split_digits(cuozblasHandle_t *h, bool strided, int nl, int k, const double *X, int ldx, int cap,
                         int k_pad, int line_quantum, DigitOperand &op, Arena &ar) {
     State *st = state(h);
-    const double *src = X;
-    int lds = ldx;
-    if (strided && k > 0) {
-        double *tmp = ar.take<double>((uint64_t)nl * k);
-        if (!ar.ok) return CUOZBLAS_STATUS_WORKSPACE;
-        OZB_TRY(transpose(h, nl, k, X, ldx, tmp, k));
-        src = tmp;
-        lds = k;
-    }
     op.lines_pad = (nl + line_quantum - 1) / line_quantum * line_quantum;
     op.e = ar.take<int>(nl > 0 ? nl : 1);
+    unsigned long long *mxb = nullptr;
+    int *lsbm = nullptr;
+    unsigned *ticket = nullptr;
+    if (strided) {  // lines contiguous: per-line statistics merged across blocks
+        mxb = ar.take<unsigned long long>(nl > 0 ? nl : 1);
+        lsbm = ar.take<int>(nl > 0 ? nl : 1);
+        ticket = ar.take<unsigned>(1);
+    }
     if (!ar.ok) return CUOZBLAS_STATUS_WORKSPACE;
     OZB_CHECK(cudaMemsetAsync(st->d_ints, 0, sizeof(int), st->stream));
-    if (nl > 0) {
-        counted(h);
-        k_digit_count<<<nl, 256, 0, st->stream>>>(k, nl, src, lds, op.e, st->d_ints);
+    if (nl > 0 && k > 0) {
+        if (strided) {
+            OZB_CHECK(cudaMemsetAsync(mxb, 0, sizeof(unsigned long long) * nl, st->stream));
+            OZB_CHECK(cudaMemsetAsync(lsbm, 0x7f, sizeof(int) * nl, st->stream));  // above every exponent
+            OZB_CHECK(cudaMemsetAsync(ticket, 0, sizeof(unsigned), st->stream));
+            const int tiles = (nl + 127) / 128;
+            int ky = (4 * sm_count() + tiles - 1) / tiles;
+            const int kmax = (k + 63) / 64;
+            ky = ky < 1 ? 1 : (ky > kmax ? kmax : ky);
+            counted(h);
+            k_digit_count_rows<<<dim3(tiles, ky), 256, 0, st->stream>>>(k, nl, X, ldx, mxb, lsbm, ticket, op.e,
+                                                                        st->d_ints);
+        } else {
+            counted(h);
+            k_digit_count<<<nl, 256, 0, st->stream>>>(k, nl, X, ldx, op.e, st->d_ints);
+        }
+    } else if (nl > 0) {
+        OZB_CHECK(cudaMemsetAsync(op.e, 0, sizeof(int) * nl, st->stream));  // k = 0: zero digits
     }
     OZB_CHECK(cudaGetLastError());
     OZB_CHECK(cudaMemcpyAsync(st->h_ints, st->d_ints, sizeof(int), cudaMemcpyDeviceToHost, st->stream));
@@ -603,10 +725,17 @@ static int split_digits(cuozblasHandle_t *h, bool strided, int nl, int k, const 
     if (cap > 0 && op.S > cap) op.S = cap;
     op.digits = ar.take<int8_t>((uint64_t)op.S * op.lines_pad * k_pad);
     if (!ar.ok) return CUOZBLAS_STATUS_WORKSPACE;
-    const int64_t chunks = (int64_t)op.lines_pad * (k_pad / 16);
+    if (op.lines_pad == 0) return CUOZBLAS_STATUS_SUCCESS;
     counted(h);
-    k_digit_write<<<(unsigned)((chunks + 255) / 256), 256, 0, st->stream>>>(k, nl, op.lines_pad, k_pad, op.S, src,
-                                                                             lds, op.e, op.digits);
+    if (strided) {
+        k_digit_write_rows<<<dim3(op.lines_pad / 128, k_pad / 32), 256, 0, st->stream>>>(k, nl, op.lines_pad, k_pad,
+                                                                                         op.S, X, ldx, op.e,
+                                                                                         op.digits);
+    } else {
+        const int64_t chunks = (int64_t)op.lines_pad * (k_pad / 16);
+        k_digit_write<<<(unsigned)((chunks + 255) / 256), 256, 0, st->stream>>>(k, nl, op.lines_pad, k_pad, op.S, X,
+                                                                                 ldx, op.e, op.digits);
+    }
     OZB_CHECK(cudaGetLastError());
     return CUOZBLAS_STATUS_SUCCESS;
 }

@@ -170,7 +170,8 @@ __global__ void __launch_bounds__(256) k_g_lines(const GOp *__restrict__ ops, co
 }
 
 // Digit tiles of one 128 x 128 block: S levels, truncated 7-bit digits of
-// x * 2^-E (as k_digit_write), written in the swizzled tile layout.
+// x * 2^-E (as k_digit_write, cut with integer operations), written in the
+// swizzled tile layout.  Each thread holds 16 elements at a time.
 __global__ void __launch_bounds__(512) k_g_digits(const int4 *__restrict__ blocks, const GOp *__restrict__ ops) {
     const int4 bk = blocks[blockIdx.x];
     const GOp o = ops[bk.x];
@@ -178,61 +179,72 @@ __global__ void __launch_bounds__(512) k_g_digits(const int4 *__restrict__ block
     const int t = threadIdx.x;
     const size_t level_stride = (size_t)o.tiles_l * o.nkb * G_TILE_BYTES;
     int8_t *tile0 = o.digits + ((size_t)bk.y * o.nkb + bk.z) * G_TILE_BYTES;
+    uint64_t m7[16];
+    int f[16];
+    uint32_t neg[4];
     if (!o.kcontig) {
-        // thread: row r, k quarter q (32 values); lines contiguous across threads
+        // thread: row r, k quarter q (two halves of 16 values); lines contiguous across threads
         const int r = t & 127, q = t >> 7, l = l0 + r;
-        double v[32];
         const int E = l < o.lines ? o.e[l] : 0;
+        for (int hh = 0; hh < 2; hh++) {
+            neg[0] = neg[1] = neg[2] = neg[3] = 0u;
 #pragma unroll
-        for (int j = 0; j < 32; j++) {
-            const int kk = k0 + 32 * q + j;
-            v[j] = (l < o.lines && kk < o.k) ? scalbn(o.X[(size_t)l + (size_t)kk * o.ld], -E) : 0.0;
-        }
-        const int c0 = (2 * q) ^ (r & 7), c1 = (2 * q + 1) ^ (r & 7);
-        for (int s = 0; s < o.S; s++) {
-            uint32_t w[8];
-#pragma unroll
-            for (int i = 0; i < 8; i++) w[i] = 0u;
-#pragma unroll
-            for (int j = 0; j < 32; j++) {
-                const double tt = v[j] * 128.0;
-                const double d = trunc(tt);
-                v[j] = tt - d;
-                w[j >> 2] |= ((uint32_t)(uint8_t)(int8_t)(int)d) << (8 * (j & 3));
+            for (int j = 0; j < 16; j++) {
+                const int kk = k0 + 32 * q + 16 * hh + j;
+                const double v = (l < o.lines && kk < o.k) ? o.X[(size_t)l + (size_t)kk * o.ld] : 0.0;
+                const DigitCut c = digit_cut(v, E);
+                m7[j] = c.m7;
+                f[j] = c.f;
+                if (v < 0.0) neg[j >> 2] |= 0xffu << (8 * (j & 3));
             }
-            int8_t *row = tile0 + s * level_stride + r * 128;
-            *reinterpret_cast<int4 *>(row + c0 * 16) = make_int4((int)w[0], (int)w[1], (int)w[2], (int)w[3]);
-            *reinterpret_cast<int4 *>(row + c1 * 16) = make_int4((int)w[4], (int)w[5], (int)w[6], (int)w[7]);
-        }
-    } else {
-        // warp: rows w + 16 i; lane: k 4 lane .. 4 lane + 3 (k contiguous across lanes)
-        const int w = t >> 5, lane = t & 31;
-        double v[8][4];
-        int E[8];
+            const int ch = (2 * q + hh) ^ (r & 7);
+            for (int s = 0; s < o.S; s++) {
+                uint32_t w[4] = {0u, 0u, 0u, 0u};
 #pragma unroll
-        for (int i = 0; i < 8; i++) {
-            const int l = l0 + w + 16 * i;
-            E[i] = l < o.lines ? o.e[l] : 0;
-#pragma unroll
-            for (int q = 0; q < 4; q++) {
-                const int kk = k0 + 4 * lane + q;
-                v[i][q] = (l < o.lines && kk < o.k) ? scalbn(o.X[(size_t)l * o.ld + kk], -E[i]) : 0.0;
-            }
-        }
-        for (int s = 0; s < o.S; s++) {
-#pragma unroll
-            for (int i = 0; i < 8; i++) {
-                const int r = w + 16 * i;
-                uint32_t word = 0u;
-#pragma unroll
-                for (int q = 0; q < 4; q++) {
-                    const double tt = v[i][q] * 128.0;
-                    const double d = trunc(tt);
-                    v[i][q] = tt - d;
-                    word |= ((uint32_t)(uint8_t)(int8_t)(int)d) << (8 * q);
+                for (int j = 0; j < 16; j++) {
+                    w[j >> 2] |= digit_mag(m7[j], f[j]) << (8 * (j & 3));
+                    f[j] -= 7;
                 }
                 int8_t *row = tile0 + s * level_stride + r * 128;
-                *reinterpret_cast<uint32_t *>(row + (((lane >> 2) ^ (r & 7)) * 16) + (lane & 3) * 4) = word;
+                *reinterpret_cast<int4 *>(row + ch * 16) =
+                    make_int4((int)digits_signed(w[0], neg[0]), (int)digits_signed(w[1], neg[1]),
+                              (int)digits_signed(w[2], neg[2]), (int)digits_signed(w[3], neg[3]));
+            }
+        }
+    } else {
+        // warp: rows w + 16 i (two passes of four rows); lane: k 4 lane .. 4 lane + 3 (k contiguous)
+        const int w = t >> 5, lane = t & 31;
+        for (int pass = 0; pass < 2; pass++) {
+            int E[4];
+            neg[0] = neg[1] = neg[2] = neg[3] = 0u;
+#pragma unroll
+            for (int i = 0; i < 4; i++) {
+                const int l = l0 + w + 16 * (4 * pass + i);
+                E[i] = l < o.lines ? o.e[l] : 0;
+#pragma unroll
+                for (int qq = 0; qq < 4; qq++) {
+                    const int kk = k0 + 4 * lane + qq;
+                    const double v = (l < o.lines && kk < o.k) ? o.X[(size_t)l * o.ld + kk] : 0.0;
+                    const DigitCut c = digit_cut(v, E[i]);
+                    m7[4 * i + qq] = c.m7;
+                    f[4 * i + qq] = c.f;
+                    if (v < 0.0) neg[i] |= 0xffu << (8 * qq);
+                }
+            }
+            for (int s = 0; s < o.S; s++) {
+#pragma unroll
+                for (int i = 0; i < 4; i++) {
+                    const int r = w + 16 * (4 * pass + i);
+                    uint32_t word = 0u;
+#pragma unroll
+                    for (int qq = 0; qq < 4; qq++) {
+                        word |= digit_mag(m7[4 * i + qq], f[4 * i + qq]) << (8 * qq);
+                        f[4 * i + qq] -= 7;
+                    }
+                    int8_t *row = tile0 + s * level_stride + r * 128;
+                    *reinterpret_cast<uint32_t *>(row + (((lane >> 2) ^ (r & 7)) * 16) + (lane & 3) * 4) =
+                        digits_signed(word, neg[i]);
+                }
             }
         }
     }

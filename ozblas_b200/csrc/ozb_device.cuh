@@ -76,4 +76,40 @@ __device__ __forceinline__ void cp_async_wait() {
     asm volatile("cp.async.wait_group %0;\n" ::"n"(N));
 }
 
+// ---- the INT8 form's digits, cut with integer operations ----
+// With |x| < 2^E, the digits are the 7-bit groups of |x| 2^-E below the binary
+// point, each carrying x's sign: d_s = trunc(x 2^(7(s+1) - E)) - 128 trunc(x 2^(7s - E)).
+// |x| 2^-E = M / 2^f exactly, M the 53-bit significand (implicit bit included)
+// and f = 1075 + E - (biased exponent, 1 for subnormals), so
+// |d_s| = ((M << 7) >> (f - 7 s)) mod 128, which is 0 once f - 7 s leaves
+// [0, 64).  These are the digits of the repeated t = 128 r, d = trunc(t),
+// r = t - d on r = x 2^-E (exact steps) for every level below 146 (beyond,
+// x 2^-E could underflow there).
+struct DigitCut {
+    uint64_t m7;  // M << 7
+    int f;        // shift of digit 0; digit s uses f - 7 s
+};
+
+__device__ __forceinline__ DigitCut digit_cut(double x, int E) {
+    const uint64_t a = (uint64_t)__double_as_longlong(x) & 0x7fffffffffffffffULL;
+    int be = (int)(a >> 52);
+    uint64_t M = a & ((1ULL << 52) - 1);
+    if (be)
+        M |= 1ULL << 52;
+    else
+        be = 1;
+    return DigitCut{M << 7, 1075 + E - be};
+}
+
+// |d_s| of a cut, with sh = f - 7 s.
+__device__ __forceinline__ uint32_t digit_mag(uint64_t m7, int sh) {
+    return (unsigned)sh < 64u ? (uint32_t)(m7 >> sh) & 127u : 0u;
+}
+
+// Four packed digit magnitudes (bytes) with the signs applied: the bytes
+// selected by `negmask` (0xff where x < 0) become 0 - |d| (two's complement).
+__device__ __forceinline__ uint32_t digits_signed(uint32_t w, uint32_t negmask) {
+    return (w & ~negmask) | (__vsub4(0u, w) & negmask);
+}
+
 }  // namespace ozb
