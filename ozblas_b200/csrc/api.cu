@@ -71,6 +71,11 @@ void EnvSwitches::read() {
     csr_slices = env_on("OZBLAS_CSR_SLICES");
     gemv_slices = env_on("OZBLAS_GEMV_SLICES");
     i8_levelwise = env_on("OZBLAS_I8_LEVELWISE");
+    {
+        const char *v = getenv("OZBLAS_I8_BLOCK");
+        i8_block = v ? atoi(v) : 0;
+        if (i8_block < 0 || i8_block > 4) i8_block = 0;
+    }
     cg_no_graph = env_on("OZBLAS_CG_NO_GRAPH");
     dot_trace = env_on("OZBLAS_DOT_TRACE");
     cg_trace = env_on("OZBLAS_CG_TRACE");

@@ -847,7 +847,7 @@ int i8_schedule(int nA, int nB, int nkb, bool triangular, std::vector<int4> &ite
 
 int i8_blk_launch(cuozblasHandle_t *h, const CUtensorMap &tmA, const CUtensorMap &tmB, int m, int n, int m_pad,
                   int n_pad, int k_pad, int nA, int nB, bool triangular, const int *ea, const int *eb, double alpha,
-                  double beta, double *C, int ldc, int strip, int *d_err, Arena &ar);  // gemm_i8_blk.cu
+                  double beta, double *C, int ldc, int strip, int width, int *d_err, Arena &ar);  // gemm_i8_blk.cu
 
 // Default digit cap when nSplitMax is 0 (enough for an exact split of
 // values whose lines span ~2^80; larger spans are truncated).
@@ -911,60 +911,70 @@ int gemm_i8_core(cuozblasHandle_t *h, char ta, char tb, int m, int n, int k, dou
     const int ntiles = p.tiles_m * p.tiles_n;
     const int grid = ntiles < nsm ? ntiles : nsm;
     OZB_CHECK(cudaFuncSetAttribute(k_i8_gemm<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, I8_SMEM));
-    // Rasterisation strip height: any value gives the same bits, the fastest is
-    // measured once per shape (candidates write a scratch product with beta = 0).
-    {
-        std::vector<int> cand;
-        for (int sv : {12, 4, 8, 16, 24}) {
-            const int v = sv < p.tiles_m ? sv : p.tiles_m;
-            if (std::find(cand.begin(), cand.end(), v) == cand.end()) cand.push_back(v);
+    // Launch shape, measured once per shape (every choice gives the same bits;
+    // candidates write a scratch product with beta = 0): the product kernel
+    // (level-blocked or level-wise), the block width of the level-blocked
+    // schedule (levels accumulated together: 4, 3 or 2) and the rasterisation
+    // strip height.  OZBLAS_I8_LEVELWISE keeps the level-wise kernel (strip
+    // tuned), OZBLAS_I8_BLOCK=w the level-blocked kernel at width w.
+    struct Shape {
+        int width;  // 0: level-wise kernel
+        int strip;
+    };
+    std::vector<Shape> cand;
+    auto add = [&](int w, int sv) {
+        const int v = sv < p.tiles_m ? sv : p.tiles_m;
+        for (const Shape &c : cand)
+            if (c.width == w && c.strip == v) return;
+        cand.push_back(Shape{w, v});
+    };
+    if (st->env.i8_levelwise) {
+        for (int sv : {12, 4, 8, 16, 24}) add(0, sv);
+    } else if (st->env.i8_block > 0) {
+        for (int sv : {12, 4, 8, 16, 24}) add(st->env.i8_block, sv);
+    } else {
+        for (int sv : {12, 4, 8, 16, 24}) add(4, sv);
+        add(3, 12);
+        add(2, 12);
+        add(0, 12);
+    }
+    auto launch = [&](const Shape &c, I8Params &pp) {
+        if (c.width > 0) {
+            const uint64_t mk2 = ar.mark();
+            const int r = i8_blk_launch(h, tmA, tmB, m, n, pp.m_pad, pp.n_pad, k_pad, nA, nB, h->fastMode != 0, da.e,
+                                        db.e, pp.alpha, pp.beta, pp.C, pp.ldc, c.strip, c.width, d_err, ar);
+            ar.release(mk2);
+            if (r != CUOZBLAS_STATUS_NOT_SUPPORTED) return r;
         }
-        int pick = 0;
-        if (cand.size() > 1) {
-            const uint64_t mk = ar.mark();
-            double *scratch = ar.take<double>((uint64_t)m * n);
-            if (ar.ok) {
-                // the kernel the call will run: level-blocked unless switched off
-                const bool blk = !st->env.i8_levelwise;
-                char key[160];
-                snprintf(key, sizeof(key), "%s:%d:%d:%d:%d:%d:%d:%d", blk ? "i8b" : "i8", p.tiles_m, p.tiles_n, nkb,
-                         nA, nB, h->fastMode != 0 ? 1 : 0, grid);
-                I8Params pt = p;
-                pt.C = scratch;
-                pt.ldc = m;
-                pt.alpha = 1.0;
-                pt.beta = 0.0;
-                pick = tune_pick(key, (int)cand.size(), 0, st->stream, [&](int i) {
-                    pt.strip = cand[(size_t)i];
-                    if (blk) {
-                        const uint64_t mk2 = ar.mark();
-                        const int r = i8_blk_launch(h, tmA, tmB, m, n, p.m_pad, p.n_pad, k_pad, nA, nB,
-                                                    h->fastMode != 0, da.e, db.e, 1.0, 0.0, scratch, m, pt.strip,
-                                                    d_err, ar);
-                        ar.release(mk2);
-                        if (r != CUOZBLAS_STATUS_NOT_SUPPORTED) return r;
-                    }
-                    k_i8_gemm<0><<<grid, I8_THREADS, I8_SMEM, st->stream>>>(tmA, tmB, pt);
-                    return cudaGetLastError() == cudaSuccess ? 0 : (int)CUOZBLAS_STATUS_CUDA_ERROR;
-                });
-            }
-            ar.ok = true;
-            ar.release(mk);
+        // the level-wise kernel: chosen, or where the blocked schedule does not apply
+        pp.strip = c.strip;
+        counted(h);
+        k_i8_gemm<0><<<grid, I8_THREADS, I8_SMEM, st->stream>>>(tmA, tmB, pp);
+        return cudaGetLastError() == cudaSuccess ? (int)CUOZBLAS_STATUS_SUCCESS : (int)CUOZBLAS_STATUS_CUDA_ERROR;
+    };
+    int pick = 0;
+    if (cand.size() > 1) {
+        const uint64_t mk = ar.mark();
+        double *scratch = ar.take<double>((uint64_t)m * n);
+        if (ar.ok) {
+            char key[160];
+            snprintf(key, sizeof(key), "i8s%d:%d:%d:%d:%d:%d:%d:%d",
+                     st->env.i8_levelwise ? -1 : st->env.i8_block, p.tiles_m, p.tiles_n, nkb, nA, nB,
+                     h->fastMode != 0 ? 1 : 0, grid);
+            I8Params pt = p;
+            pt.C = scratch;
+            pt.ldc = m;
+            pt.alpha = 1.0;
+            pt.beta = 0.0;
+            pick = tune_pick(key, (int)cand.size(), 0, st->stream, [&](int i) { return launch(cand[(size_t)i], pt); });
         }
-        p.strip = cand[(size_t)pick];
+        ar.ok = true;
+        ar.release(mk);
     }
     ev_record(h, 2);
-    // the level-blocked kernel (same bits, a quarter of the operand traffic) unless switched off
-    int blk = CUOZBLAS_STATUS_NOT_SUPPORTED;
-    if (!st->env.i8_levelwise)
-        blk = i8_blk_launch(h, tmA, tmB, m, n, p.m_pad, p.n_pad, k_pad, nA, nB, h->fastMode != 0, da.e, db.e, alpha,
-                            beta, C, ldc, p.strip, d_err, ar);
-    if (blk == CUOZBLAS_STATUS_NOT_SUPPORTED) {
-        counted(h);
-        k_i8_gemm<0><<<grid, I8_THREADS, I8_SMEM, st->stream>>>(tmA, tmB, p);
-        OZB_CHECK(cudaGetLastError());
-    } else if (blk != CUOZBLAS_STATUS_SUCCESS) {
-        return blk;
+    {
+        const int r = launch(cand[(size_t)pick], p);
+        if (r != CUOZBLAS_STATUS_SUCCESS) return r;
     }
     ev_record(h, 3);
     OZB_CHECK(cudaMemcpyAsync(st->h_ints, d_err, sizeof(int), cudaMemcpyDeviceToHost, st->stream));

@@ -34,7 +34,7 @@
 namespace ozb {
 
 constexpr int KB_BM = 128, KB_BN = 128, KB_BK = 128;
-constexpr int KB_W = 4;                       // levels per block (tensor-memory accumulators)
+constexpr int KB_W = 4;                       // most levels per block (tensor-memory accumulators)
 constexpr int KB_RA = 4, KB_RB = 8;           // ring slots for A and B planes
 constexpr int KB_TILE = KB_BM * KB_BK;        // 16 KB plane tile
 constexpr int KB_THREADS = 384;  // warp 0 producer, warp 1 MMA issuer, warps 2-3 idle, warps 4-11 epilogue
@@ -332,9 +332,10 @@ __global__ void __launch_bounds__(KB_THREADS, 1)
 
 // The per-tile schedule: runs of consecutive levels whose exact combination
 // stays below 2^53 (the same runs as i8_schedule), cut into blocks of at most
-// KB_W levels, each block cut into K chunks that keep every accumulator's
+// W <= KB_W levels, each block cut into K chunks that keep every accumulator's
 // INT32 sum exact.  Returns false when the levels exceed the tables' range.
-static bool blk_schedule(int nA, int nB, int nkb, bool triangular, std::vector<BlkStep> &steps) {
+static bool blk_schedule(int nA, int nB, int nkb, bool triangular, int W, std::vector<BlkStep> &steps) {
+    if (W < 1 || W > KB_W) return false;
     const int maxlevel = triangular ? (nA < nB ? nA : nB) - 1 : nA + nB - 2;
     if (maxlevel < 0 || maxlevel >= 128) return false;
     auto pairs = [&](int L) {
@@ -361,8 +362,8 @@ static bool blk_schedule(int nA, int nB, int nkb, bool triangular, std::vector<B
     steps.clear();
     for (size_t r = 0; r < run_lo.size(); r++) {
         const int next_hi = r + 1 < run_lo.size() ? run_hi[r + 1] : 0;
-        for (int L0 = run_lo[r]; L0 <= run_hi[r]; L0 += KB_W) {
-            const int L1 = L0 + KB_W - 1 < run_hi[r] ? L0 + KB_W - 1 : run_hi[r];
+        for (int L0 = run_lo[r]; L0 <= run_hi[r]; L0 += W) {
+            const int L1 = L0 + W - 1 < run_hi[r] ? L0 + W - 1 : run_hi[r];
             int pmax = 0;
             for (int L = L0; L <= L1; L++) pmax = pairs(L) > pmax ? pairs(L) : pmax;
             int chunk = (int)(KB_MAX_TERMS / ((int64_t)pmax * KB_BK));  // K steps per INT32 sum
@@ -399,13 +400,14 @@ int i8_test_hold_copies();
 
 // The level-blocked product kernel over digit operands laid out as for
 // k_i8_gemm (tensor maps over [S * lines_pad][k_pad], 128 x 128-byte boxes).
+// `width`: levels per block (1..4; every width gives the same bits).
 // Returns NOT_SUPPORTED (nothing launched) when the schedule does not apply.
 int i8_blk_launch(cuozblasHandle_t *h, const CUtensorMap &tmA, const CUtensorMap &tmB, int m, int n, int m_pad,
                   int n_pad, int k_pad, int nA, int nB, bool triangular, const int *ea, const int *eb, double alpha,
-                  double beta, double *C, int ldc, int strip, int *d_err, Arena &ar) {
+                  double beta, double *C, int ldc, int strip, int width, int *d_err, Arena &ar) {
     State *st = state(h);
     std::vector<BlkStep> steps;
-    if (!blk_schedule(nA, nB, k_pad / KB_BK, triangular, steps)) return CUOZBLAS_STATUS_NOT_SUPPORTED;
+    if (!blk_schedule(nA, nB, k_pad / KB_BK, triangular, width, steps)) return CUOZBLAS_STATUS_NOT_SUPPORTED;
     const int nsm = sm_count();
     const int tiles_m = m_pad / KB_BM, tiles_n = n_pad / KB_BN, ntiles = tiles_m * tiles_n;
     const int grid = ntiles < nsm ? ntiles : nsm;

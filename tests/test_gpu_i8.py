@@ -172,8 +172,8 @@ def test_i8_batched_accuracy_uneven(oracle, handle, ozb, cuda):
 # ---- autotuned launch choices: speed only, never bits ----
 
 def test_autotune_changes_no_bits(oracle, handle, ozb, cuda, tmp_path, monkeypatch):
-    """Strip height (single) and dealing order (grouped) are measured per shape; the results equal the
-    untuned defaults bit for bit, and a choice is recorded in $OZBLAS_TUNE_CACHE."""
+    """Product kernel, block width and strip height (single) and dealing order (grouped) are measured per shape;
+    the results equal the untuned defaults bit for bit, and a choice is recorded in $OZBLAS_TUNE_CACHE."""
     m, n, k = 700, 520, 300  # a shape no other test uses (6 tile rows: two strip heights to try)
     A = oracle.phi_matrix(m, k, 1.0, 31)
     B = oracle.phi_matrix(k, n, 1.0, 32)
@@ -185,7 +185,7 @@ def test_autotune_changes_no_bits(oracle, handle, ozb, cuda, tmp_path, monkeypat
     plain = run_i8(ozb, handle, cuda, A, B, m, n, k, fast=1)
     assert bits_equal(tuned, plain)
     text = cache.read_text()
-    assert "i8b:" in text or "i8:" in text  # level-blocked (default) or level-wise kernel's key
+    assert "i8s0:" in text  # the product's launch shape: kernel, block width and strip measured together
     shapes = [(100, 260, 300, 1.0), (390, 70, 129, 2.0), (64, 64, 64, 0.5), (257, 129, 513, 4.0)]
     probs = _batch_case(oracle, shapes, "n", "n", 3)
     outs = []
@@ -254,17 +254,23 @@ def test_i8_wait_timeout_reports_and_recovers(oracle, handle, ozb, cuda):
     (256, 128, 20000, 1.0, 0, "n", "n"),   # K chunks: a level's INT32 sum is split over K
     (130, 200, 20000, 2.0, 1, "t", "t"),
     (1, 1, 7, 1.0, 0, "n", "n"),
+    (1000, 900, 3000, 1.0, 1, "n", "n"),
 ])
 def test_i8_level_blocked_equals_levelwise(m, n, k, phi, fast, ta, tb, oracle, handle, ozb, cuda, monkeypatch):
-    """The level-blocked product kernel (k_i8_blk) gives the bits of the level-wise one (k_i8_gemm): the same
-    products and sums, in another order of the exact INT32 accumulations."""
+    """The level-blocked product kernel (k_i8_blk) gives the bits of the level-wise one (k_i8_gemm) at every block
+    width (levels accumulated together): the same products and sums, in another order of the exact INT32
+    accumulations."""
     A = oracle.phi_matrix(m, k, phi, 1) if ta == "n" else oracle.phi_matrix(k, m, phi, 1)
     B = oracle.phi_matrix(k, n, phi, 2) if tb == "n" else oracle.phi_matrix(n, k, phi, 2)
     C0 = oracle.phi_matrix(m, n, 1.0, 3)
-    a = run_i8(ozb, handle, cuda, A, B, m, n, k, ta=ta, tb=tb, fast=fast, alpha=-0.75, beta=0.5, C0=C0)
-    monkeypatch.setenv("OZBLAS_I8_LEVELWISE", "1")
+    outs = {}
+    for name, var, val in [("w4", "OZBLAS_I8_BLOCK", "4"), ("w3", "OZBLAS_I8_BLOCK", "3"),
+                           ("w2", "OZBLAS_I8_BLOCK", "2"), ("w1", "OZBLAS_I8_BLOCK", "1"),
+                           ("levelwise", "OZBLAS_I8_LEVELWISE", "1")]:
+        monkeypatch.setenv(var, val)
+        handle.read_env()
+        outs[name] = run_i8(ozb, handle, cuda, A, B, m, n, k, ta=ta, tb=tb, fast=fast, alpha=-0.75, beta=0.5, C0=C0)
+        monkeypatch.delenv(var)
     handle.read_env()
-    b = run_i8(ozb, handle, cuda, A, B, m, n, k, ta=ta, tb=tb, fast=fast, alpha=-0.75, beta=0.5, C0=C0)
-    monkeypatch.delenv("OZBLAS_I8_LEVELWISE")
-    handle.read_env()
-    assert bits_equal(a, b)
+    for w in ("w4", "w3", "w2", "w1"):
+        assert bits_equal(outs[w], outs["levelwise"]), w
