@@ -71,6 +71,7 @@ void EnvSwitches::read() {
     csr_slices = env_on("OZBLAS_CSR_SLICES");
     gemv_slices = env_on("OZBLAS_GEMV_SLICES");
     i8_levelwise = env_on("OZBLAS_I8_LEVELWISE");
+    g_split3 = env_on("OZBLAS_GROUPED_SPLIT3");
     {
         const char *v = getenv("OZBLAS_I8_BLOCK");
         i8_block = v ? atoi(v) : 0;

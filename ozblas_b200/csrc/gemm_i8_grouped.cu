@@ -52,6 +52,11 @@ struct GOp {
     int8_t *digits;          // S x tiles_l x nkb tiles
 };
 
+// Bytes of one operand's digit tiles, rounded up to 256 (the carving step).
+__host__ __device__ inline unsigned long long g_digit_bytes(int S, int tiles_l, int nkb) {
+    return ((unsigned long long)S * tiles_l * nkb * G_TILE_BYTES + 255ull) & ~255ull;
+}
+
 struct GProb {
     int m, n, ldc, nkb, tiles_m, tiles_n;
     int group0, n_groups;
@@ -172,9 +177,15 @@ __global__ void __launch_bounds__(256) k_g_lines(const GOp *__restrict__ ops, co
 // Digit tiles of one 128 x 128 block: S levels, truncated 7-bit digits of
 // x * 2^-E (as k_digit_write, cut with integer operations), written in the
 // swizzled tile layout.  Each thread holds 16 elements at a time.
-__global__ void __launch_bounds__(512) k_g_digits(const int4 *__restrict__ blocks, const GOp *__restrict__ ops) {
-    const int4 bk = blocks[blockIdx.x];
-    const GOp o = ops[bk.x];
+template <bool CG>
+__device__ __forceinline__ int g_line_e(const int *e, int l) {
+    return CG ? __ldcg(e + l) : e[l];
+}
+
+// One block of 512 threads cuts block bk of operand o.  CG: the line
+// exponents were written by other blocks of the same launch.
+template <bool CG>
+__device__ __forceinline__ void g_digits_tile(const int4 bk, const GOp &o) {
     const int l0 = bk.y * G_T, k0 = bk.z * G_T;
     const int t = threadIdx.x;
     const size_t level_stride = (size_t)o.tiles_l * o.nkb * G_TILE_BYTES;
@@ -185,7 +196,7 @@ __global__ void __launch_bounds__(512) k_g_digits(const int4 *__restrict__ block
     if (!o.kcontig) {
         // thread: row r, k quarter q (two halves of 16 values); lines contiguous across threads
         const int r = t & 127, q = t >> 7, l = l0 + r;
-        const int E = l < o.lines ? o.e[l] : 0;
+        const int E = l < o.lines ? g_line_e<CG>(o.e, l) : 0;
         for (int hh = 0; hh < 2; hh++) {
             neg[0] = neg[1] = neg[2] = neg[3] = 0u;
 #pragma unroll
@@ -220,7 +231,7 @@ __global__ void __launch_bounds__(512) k_g_digits(const int4 *__restrict__ block
 #pragma unroll
             for (int i = 0; i < 4; i++) {
                 const int l = l0 + w + 16 * (4 * pass + i);
-                E[i] = l < o.lines ? o.e[l] : 0;
+                E[i] = l < o.lines ? g_line_e<CG>(o.e, l) : 0;
 #pragma unroll
                 for (int qq = 0; qq < 4; qq++) {
                     const int kk = k0 + 4 * lane + qq;
@@ -247,6 +258,187 @@ __global__ void __launch_bounds__(512) k_g_digits(const int4 *__restrict__ block
                 }
             }
         }
+    }
+}
+
+__global__ void __launch_bounds__(512) k_g_digits(const int4 *__restrict__ blocks, const GOp *__restrict__ ops) {
+    const int4 bk = blocks[blockIdx.x];
+    g_digits_tile<false>(bk, ops[bk.x]);
+}
+
+// ---- the whole split in one launch ------------------------------------------
+// Statistics, line exponents, digit counts and digits of all operands as one
+// cooperative launch (every block resident): three grid barriers separate the
+// phases, each a bounded wait (2 s) that reports a timeout instead of hanging.
+// The digit buffers are carved, in operand order, from a region the host
+// reserved for the largest digit count; the host repeats the same carving
+// from the counts it reads back.  err: 1 a barrier timed out, 2 the digits
+// need more than the region (the host then allocates and cuts them itself).
+struct GSplitArgs {
+    const int4 *blocks;
+    int nblocks;
+    GOp *ops;
+    int nops;
+    const int *line0;
+    int total_lines;
+    int *need;
+    int cap;
+    int8_t *dig_base;
+    unsigned long long dig_capacity;
+    unsigned *bar;  // three barrier counters and two work counters, zero at launch
+    int *err;
+};
+
+__device__ __forceinline__ bool g_grid_barrier(unsigned *ctr, int *err) {
+    __shared__ int ok_sh;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        atomicAdd(ctr, 1u);
+        const uint64_t t0 = tc::globaltimer();
+        int ok = 1;
+        while (*(volatile unsigned *)ctr < gridDim.x) {
+            if (tc::globaltimer() - t0 > 2000000000ull) {
+                atomicExch(err, 1);
+                ok = 0;
+                break;
+            }
+            __nanosleep(128);
+        }
+        __threadfence();
+        ok_sh = ok && *(volatile int *)err == 0;
+    }
+    __syncthreads();
+    return ok_sh != 0;
+}
+
+// Statistics of one block with 512 threads (as k_g_stats).
+__device__ __forceinline__ void g_stats_tile512(const int4 bk, const GOp &o, double *smx, int *slsb) {
+    const int l0 = bk.y * G_T, k0 = bk.z * G_T;
+    const int t = threadIdx.x;
+    if (!o.kcontig) {
+        const int l = l0 + (t & 127), kh = k0 + (t >> 7) * 32;
+        double mx = 0.0;
+        int lsb = 0x7fffffff;
+        if (l < o.lines) {
+            double v[32];  // every load in flight before the first use
+#pragma unroll
+            for (int j = 0; j < 32; j++) {
+                const int kk = kh + j;
+                v[j] = kk < o.k ? o.X[(size_t)l + (size_t)kk * o.ld] : 0.0;
+            }
+#pragma unroll
+            for (int j = 0; j < 32; j++) g_stat(v[j], mx, lsb);
+        }
+        smx[t] = mx;
+        slsb[t] = lsb;
+        __syncthreads();
+        if (t < 128 && l < o.lines) {
+            mx = ref_max(ref_max(smx[t], smx[t + 128]), ref_max(smx[t + 256], smx[t + 384]));
+            lsb = min(min(slsb[t], slsb[t + 128]), min(slsb[t + 256], slsb[t + 384]));
+            if (mx > 0.0) atomicMax(&o.mx[l], (unsigned long long)__double_as_longlong(mx));
+            if (lsb != 0x7fffffff) atomicMin(&o.lsb[l], lsb);
+        }
+        __syncthreads();
+    } else {
+        const int w = t >> 5, lane = t & 31;
+        double v[G_T / 16][4];  // every load of the thread in flight together
+#pragma unroll
+        for (int i = 0; i < G_T / 16; i++) {
+            const int l = l0 + w + 16 * i;
+#pragma unroll
+            for (int q = 0; q < 4; q++) {
+                const int kk = k0 + 4 * lane + q;
+                v[i][q] = (l < o.lines && kk < o.k) ? o.X[(size_t)l * o.ld + kk] : 0.0;
+            }
+        }
+#pragma unroll
+        for (int i = 0; i < G_T / 16; i++) {
+            const int l = l0 + w + 16 * i;
+            if (l >= o.lines) break;  // uniform per warp
+            double mx = 0.0;
+            int lsb = 0x7fffffff;
+#pragma unroll
+            for (int q = 0; q < 4; q++) g_stat(v[i][q], mx, lsb);
+            for (int sft = 16; sft > 0; sft >>= 1) {
+                mx = ref_max(mx, __shfl_xor_sync(0xffffffffu, mx, sft));
+                lsb = min(lsb, __shfl_xor_sync(0xffffffffu, lsb, sft));
+            }
+            if (lane == 0) {
+                if (mx > 0.0) atomicMax(&o.mx[l], (unsigned long long)__double_as_longlong(mx));
+                if (lsb != 0x7fffffff) atomicMin(&o.lsb[l], lsb);
+            }
+        }
+    }
+}
+
+__device__ __forceinline__ GOp g_load_op(const GOp *p) {  // through L2: written in this launch
+    static_assert(sizeof(GOp) % 8 == 0, "GOp words");
+    GOp o;
+    unsigned long long w[sizeof(GOp) / 8];
+    const unsigned long long *src = reinterpret_cast<const unsigned long long *>(p);
+#pragma unroll
+    for (int i = 0; i < (int)(sizeof(GOp) / 8); i++) w[i] = __ldcg(src + i);
+    memcpy(&o, w, sizeof(GOp));
+    return o;
+}
+
+// The next block of the list for this CTA (taken in order from a counter, so
+// CTAs that finish early take more).
+__device__ __forceinline__ int g_next_block(unsigned *ctr, int *slot) {
+    __syncthreads();  // every thread is done with the previous block and its slot
+    if (threadIdx.x == 0) *slot = (int)atomicAdd(ctr, 1u);
+    __syncthreads();
+    return *slot;
+}
+
+__global__ void __launch_bounds__(512, 1) k_g_split(const GSplitArgs a) {
+    __shared__ double smx[512];
+    __shared__ int slsb[512];
+    __shared__ int next_sh;
+    // 1: per-line max and lowest set bit
+    for (int b = g_next_block(&a.bar[3], &next_sh); b < a.nblocks; b = g_next_block(&a.bar[3], &next_sh)) {
+        const int4 bk = a.blocks[b];
+        g_stats_tile512(bk, a.ops[bk.x], smx, slsb);
+    }
+    if (!g_grid_barrier(&a.bar[0], a.err)) return;
+    // 2: line exponents and each operand's digit need
+    for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < a.total_lines; g += gridDim.x * blockDim.x) {
+        int lo = 0, hi = a.nops - 1;  // operand with line0[op] <= g < line0[op + 1]
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (a.line0[mid] <= g)
+                lo = mid;
+            else
+                hi = mid - 1;
+        }
+        const GOp &o = a.ops[lo];
+        const int l = g - a.line0[lo];
+        const double mx = __longlong_as_double((long long)__ldcg(&o.mx[l]));
+        const int E = mx > 0.0 ? g_exp_above(mx) : 0;
+        o.e[l] = E;
+        if (mx > 0.0) atomicMax(&a.need[lo], (E - __ldcg(&o.lsb[l]) + 6) / 7);
+    }
+    if (!g_grid_barrier(&a.bar[1], a.err)) return;
+    // digit counts and buffers (the host carves the same ones)
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        unsigned long long off = 0;
+        for (int i = 0; i < a.nops; i++) {
+            int S = __ldcg(&a.need[i]);
+            S = S < 1 ? 1 : S;
+            if (a.cap > 0 && S > a.cap) S = a.cap;
+            a.ops[i].S = S;
+            a.ops[i].digits = a.dig_base + off;
+            off += g_digit_bytes(S, a.ops[i].tiles_l, a.ops[i].nkb);
+        }
+        if (off > a.dig_capacity) atomicExch(a.err, 2);
+    }
+    if (!g_grid_barrier(&a.bar[2], a.err)) return;
+    // 3: digits
+    for (int b = g_next_block(&a.bar[4], &next_sh); b < a.nblocks; b = g_next_block(&a.bar[4], &next_sh)) {
+        const int4 bk = a.blocks[b];
+        const GOp o = g_load_op(&a.ops[bk.x]);
+        g_digits_tile<true>(bk, o);
     }
 }
 
@@ -486,7 +678,8 @@ __global__ void __launch_bounds__(G_THREADS, 1) k_i8_grouped(const GParams p) {
 // ---------------------------------------------------------------------------
 // Host side
 // ---------------------------------------------------------------------------
-int i8_schedule(int nA, int nB, int nkb, bool triangular, std::vector<int4> &items, std::vector<int4> &groups);
+int i8_schedule_into(int nA, int nB, int nkb, bool triangular, int4 *items, int max_items, int *ni, int4 *groups,
+                     int max_groups, int *ng);  // gemm_i8.cu
 
 constexpr int kI8DefaultCapG = 19;  // as gemm_i8.cu's kI8DefaultCap
 
@@ -559,9 +752,9 @@ int gemm_i8_batched(cuozblasHandle_t *h, char ta, char tb, int count, const int 
         for (int o = 0; o < 2; o++) {
             const GOp &op = ops[(size_t)2 * b + o];
             line0[(size_t)2 * b + o + 1] = line0[(size_t)2 * b + o] + op.lines;
-            if (k[b] > 0)
-                for (int tl = 0; tl < op.tiles_l; tl++)
-                    for (int kb = 0; kb < op.nkb; kb++) blocks.push_back(make_int4(2 * b + o, tl, kb, 0));
+            // k = 0 included: its single block of zero digits makes C = beta * C
+            for (int tl = 0; tl < op.tiles_l; tl++)
+                for (int kb = 0; kb < op.nkb; kb++) blocks.push_back(make_int4(2 * b + o, tl, kb, 0));
         }
     }
     const int nops = 2 * count, total_lines = line0[(size_t)nops];
@@ -574,6 +767,8 @@ int gemm_i8_batched(cuozblasHandle_t *h, char ta, char tb, int count, const int 
     int *d_line0 = ar.take<int>((uint64_t)nops + 1);
     int *d_need = ar.take<int>((uint64_t)nops);
     int4 *d_blocks = ar.take<int4>(blocks.size() > 0 ? blocks.size() : 1);
+    unsigned *d_bar = ar.take<unsigned>(8);
+    int *d_serr = ar.take<int>(1);
     if (!ar.ok) return CUOZBLAS_STATUS_WORKSPACE;
     for (int o = 0; o < nops; o++) {
         GOp &op = ops[(size_t)o];
@@ -581,44 +776,121 @@ int gemm_i8_batched(cuozblasHandle_t *h, char ta, char tb, int count, const int 
         op.mx = all_mx + line0[(size_t)o];
         op.lsb = all_lsb + line0[(size_t)o];
     }
+    // The split in one cooperative launch when every block can be resident and
+    // the digits of the largest count fit a reserved region; otherwise three
+    // launches (statistics, lines, digits) with the digits allocated after the
+    // counts are read.
+    unsigned long long dig_bound = 0;
+    for (const GOp &op : ops) dig_bound += g_digit_bytes(cap, op.tiles_l, op.nkb);
+    const uint64_t mk_dig = ar.mark();
+    int8_t *dig_region = ar.take<int8_t>(dig_bound + 1);
+    int coop_grid = 0;
+    if (ar.ok && !blocks.empty() && total_lines > 0 && !st->env.g_split3) {
+        int dev = 0;
+        OZB_CHECK(cudaGetDevice(&dev));
+        static std::atomic<int> occ_cache[64];
+        int occ = dev >= 0 && dev < 64 ? occ_cache[dev].load() : 0;
+        if (occ == 0) {
+            int coop = 0;
+            if (cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev) == cudaSuccess && coop &&
+                cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_g_split, 512, 0) == cudaSuccess && occ > 0) {
+                if (dev >= 0 && dev < 64) occ_cache[dev].store(occ);
+            } else {
+                cudaGetLastError();
+                occ = -1;
+                if (dev >= 0 && dev < 64) occ_cache[dev].store(-1);
+            }
+        }
+        if (occ > 0) {
+            const int64_t g = (int64_t)occ * sm_count();
+            coop_grid = (int)((int64_t)blocks.size() < g ? (int64_t)blocks.size() : g);
+        }
+    }
+    if (coop_grid < 1) {
+        ar.ok = true;
+        ar.release(mk_dig);
+        dig_region = nullptr;
+    }
     OZB_CHECK(cudaMemsetAsync(all_mx, 0, tl_alloc * sizeof(unsigned long long), s));
     OZB_CHECK(cudaMemsetAsync(all_lsb, 0x7f, tl_alloc * sizeof(int), s));
     OZB_CHECK(cudaMemsetAsync(d_need, 0, (size_t)nops * sizeof(int), s));
+    OZB_CHECK(cudaMemsetAsync(d_bar, 0, 8 * sizeof(unsigned), s));
+    OZB_CHECK(cudaMemsetAsync(d_serr, 0, sizeof(int), s));
     OZB_CHECK(cudaMemcpyAsync(d_ops, ops.data(), sizeof(GOp) * nops, cudaMemcpyHostToDevice, s));
     OZB_CHECK(cudaMemcpyAsync(d_line0, line0.data(), sizeof(int) * (nops + 1), cudaMemcpyHostToDevice, s));
     if (!blocks.empty())
         OZB_CHECK(cudaMemcpyAsync(d_blocks, blocks.data(), sizeof(int4) * blocks.size(), cudaMemcpyHostToDevice, s));
     ev_record(h, 0);
-    if (!blocks.empty()) {
+    bool fused = coop_grid > 0;
+    if (fused) {
+        GSplitArgs ga;
+        ga.blocks = d_blocks;
+        ga.nblocks = (int)blocks.size();
+        ga.ops = d_ops;
+        ga.nops = nops;
+        ga.line0 = d_line0;
+        ga.total_lines = total_lines;
+        ga.need = d_need;
+        ga.cap = cap;
+        ga.dig_base = dig_region;
+        ga.dig_capacity = dig_bound;
+        ga.bar = d_bar;
+        ga.err = d_serr;
+        void *args[] = {&ga};
         counted(h);
-        k_g_stats<<<(unsigned)blocks.size(), 256, 0, s>>>(d_blocks, d_ops);
+        if (cudaLaunchCooperativeKernel((const void *)k_g_split, dim3(coop_grid), dim3(512), args, 0, s) !=
+            cudaSuccess) {
+            cudaGetLastError();  // not launched: the three-launch split
+            fused = false;
+            ar.release(mk_dig);
+            dig_region = nullptr;
+        }
     }
-    if (total_lines > 0) {
-        counted(h);
-        k_g_lines<<<(total_lines + 255) / 256, 256, 0, s>>>(d_ops, d_line0, nops, total_lines, d_need);
+    if (!fused) {
+        if (!blocks.empty()) {
+            counted(h);
+            k_g_stats<<<(unsigned)blocks.size(), 256, 0, s>>>(d_blocks, d_ops);
+        }
+        if (total_lines > 0) {
+            counted(h);
+            k_g_lines<<<(total_lines + 255) / 256, 256, 0, s>>>(d_ops, d_line0, nops, total_lines, d_need);
+        }
     }
     OZB_CHECK(cudaGetLastError());
-    std::vector<int> need((size_t)nops);
+    std::vector<int> need((size_t)nops + 1);
     OZB_CHECK(cudaMemcpyAsync(need.data(), d_need, sizeof(int) * nops, cudaMemcpyDeviceToHost, s));
+    OZB_CHECK(cudaMemcpyAsync(need.data() + nops, d_serr, sizeof(int), cudaMemcpyDeviceToHost, s));
     OZB_CHECK(cudaStreamSynchronize(s));
+    const int serr = fused ? need[(size_t)nops] : 0;
+    if (serr == 1) {
+        fprintf(stderr, "cuozblas: grouped INT8 split: a grid barrier timed out\n");
+        return CUOZBLAS_STATUS_DEVICE_TIMEOUT;
+    }
+    const bool carved = fused && serr == 0;  // the launch cut the digits into the region
+    if (!carved && dig_region) {
+        ar.release(mk_dig);
+        dig_region = nullptr;
+    }
     int maxA = 0, maxB = 0;
+    unsigned long long off = 0;
     for (int o = 0; o < nops; o++) {
         GOp &op = ops[(size_t)o];
         op.S = need[(size_t)o] < 1 ? 1 : need[(size_t)o];
         if (op.S > cap) op.S = cap;
-        op.digits = ar.take<int8_t>((uint64_t)op.S * op.tiles_l * op.nkb * G_TILE_BYTES + 1);
+        if (carved) {  // the same carving as the device's
+            op.digits = dig_region + off;
+            off += g_digit_bytes(op.S, op.tiles_l, op.nkb);
+        } else {
+            op.digits = ar.take<int8_t>((uint64_t)op.S * op.tiles_l * op.nkb * G_TILE_BYTES + 1);
+        }
         if (o & 1)
             maxB = op.S > maxB ? op.S : maxB;
         else
             maxA = op.S > maxA ? op.S : maxA;
     }
     if (!ar.ok) return CUOZBLAS_STATUS_WORKSPACE;
-    for (int o = 0; o < nops; o++)  // k = 0: zero digits, so C = beta * C
-        if (ops[(size_t)o].k == 0 && ops[(size_t)o].tiles_l > 0)
-            OZB_CHECK(cudaMemsetAsync(ops[(size_t)o].digits, 0,
-                                      (size_t)ops[(size_t)o].S * ops[(size_t)o].tiles_l * G_TILE_BYTES, s));
-    OZB_CHECK(cudaMemcpyAsync(d_ops, ops.data(), sizeof(GOp) * nops, cudaMemcpyHostToDevice, s));
-    if (!blocks.empty()) {
+    if (!carved && !blocks.empty()) {
+        OZB_CHECK(cudaMemcpyAsync(d_ops, ops.data(), sizeof(GOp) * nops, cudaMemcpyHostToDevice, s));
         counted(h);
         k_g_digits<<<(unsigned)blocks.size(), 512, 0, s>>>(d_blocks, d_ops);
         OZB_CHECK(cudaGetLastError());
@@ -629,25 +901,41 @@ int gemm_i8_batched(cuozblasHandle_t *h, char ta, char tb, int count, const int 
     std::vector<GProb> probs((size_t)count);
     std::vector<double> cost((size_t)count, 0.0);
     int npairs_max = 0;
-    for (int b = 0; b < count; b++) {
-        const GOp &oa = ops[(size_t)2 * b], &ob = ops[(size_t)2 * b + 1];
-        std::vector<int4> it, gr;
-        const int np = i8_schedule(oa.S, ob.S, oa.nkb, h->fastMode != 0, it, gr);
-        if (np < 0) return CUOZBLAS_STATUS_NOT_SUPPORTED;
-        npairs_max = np > npairs_max ? np : npairs_max;
-        const int ibase = (int)items.size();
-        for (auto &g : gr) {
-            g.x += ibase;
-            g.y += ibase;
+    {
+        // every problem's schedule written in place (no per-problem vectors):
+        // a pair spans at most nkb / (k-blocks per INT32 group) + 2 items, a
+        // group holds at least one item
+        size_t cap_items = 0;
+        for (int b = 0; b < count; b++) {
+            const GOp &oa = ops[(size_t)2 * b], &ob = ops[(size_t)2 * b + 1];
+            cap_items += (size_t)oa.S * ob.S * (size_t)(oa.nkb / (G_MAX_TERMS / G_T) + 2);
         }
-        double kbs = 0.0;
-        for (auto &i : it) kbs += i.w - i.z;
-        cost[(size_t)b] = kbs + 2.0 * gr.size();
-        GProb &pr = probs[(size_t)b];
-        pr = GProb{m[b], n[b], ldc[b], oa.nkb, oa.tiles_l, ob.tiles_l, (int)groups.size(), (int)gr.size(),
-                   oa.digits, ob.digits, oa.e, ob.e, alpha[b], beta[b], C[b]};
-        items.insert(items.end(), it.begin(), it.end());
-        groups.insert(groups.end(), gr.begin(), gr.end());
+        items.resize(cap_items > 0 ? cap_items : 1);
+        groups.resize(cap_items > 0 ? cap_items : 1);
+        size_t ni_tot = 0, ng_tot = 0;
+        for (int b = 0; b < count; b++) {
+            const GOp &oa = ops[(size_t)2 * b], &ob = ops[(size_t)2 * b + 1];
+            const size_t cap_b = (size_t)oa.S * ob.S * (size_t)(oa.nkb / (G_MAX_TERMS / G_T) + 2);
+            int ni = 0, ng = 0;
+            const int np = i8_schedule_into(oa.S, ob.S, oa.nkb, h->fastMode != 0, items.data() + ni_tot, (int)cap_b,
+                                            &ni, groups.data() + ng_tot, (int)cap_b, &ng);
+            if (np < 0) return CUOZBLAS_STATUS_NOT_SUPPORTED;
+            npairs_max = np > npairs_max ? np : npairs_max;
+            double kbs = 0.0;
+            for (int i = 0; i < ni; i++) kbs += items[ni_tot + (size_t)i].w - items[ni_tot + (size_t)i].z;
+            for (int g = 0; g < ng; g++) {
+                groups[ng_tot + (size_t)g].x += (int)ni_tot;
+                groups[ng_tot + (size_t)g].y += (int)ni_tot;
+            }
+            cost[(size_t)b] = kbs + 2.0 * ng;
+            GProb &pr = probs[(size_t)b];
+            pr = GProb{m[b], n[b], ldc[b], oa.nkb, oa.tiles_l, ob.tiles_l, (int)ng_tot, ng,
+                       oa.digits, ob.digits, oa.e, ob.e, alpha[b], beta[b], C[b]};
+            ni_tot += (size_t)ni;
+            ng_tot += (size_t)ng;
+        }
+        items.resize(ni_tot);
+        groups.resize(ng_tot);
     }
     std::vector<int> order((size_t)count);
     for (int b = 0; b < count; b++) order[(size_t)b] = b;

@@ -130,17 +130,33 @@ def _batch_case(oracle, shapes, ta, tb, seed):
 
 @pytest.mark.parametrize("ta,tb", [("n", "n"), ("t", "n"), ("n", "t"), ("t", "t")])
 @pytest.mark.parametrize("fast", [0, 1])
-def test_i8_batched_matches_single(ta, tb, fast, oracle, handle, ozb, cuda):
-    """Every problem of a grouped launch is bit-identical to its own cuozblasDgemmI8 call."""
+@pytest.mark.parametrize("split", ["one launch", "three launches"])
+def test_i8_batched_matches_single(ta, tb, fast, split, oracle, handle, ozb, cuda, monkeypatch):
+    """Every problem of a grouped launch is bit-identical to its own cuozblasDgemmI8 call, with the split of all
+    operands as one cooperative launch (then the whole call is two launches: split and products) or as three."""
+    if split == "three launches":
+        monkeypatch.setenv("OZBLAS_GROUPED_SPLIT3", "1")
+    handle.read_env()
     shapes = [(1, 1, 1, 1.0), (64, 300, 129, 0.5), (130, 70, 1000, 2.0), (200, 256, 512, 4.0), (7, 129, 33, 1.0),
               (256, 3, 256, 1.0), (129, 129, 128, 2.0), (90, 40, 0, 1.0), (0, 5, 10, 1.0), (300, 200, 64, 0.5)]
     probs = _batch_case(oracle, shapes, ta, tb, 7 + fast)
     handle.nSplitMax, handle.fastMode = 0, fast
     Cs = [dev(cuda, p[7]) for p in probs]
-    ozb.dgemm_i8_batched(handle, ta, tb, [p[0] for p in probs], [p[1] for p in probs], [p[2] for p in probs],
-                         [p[8] for p in probs], [dev(cuda, p[3]) for p in probs], [p[4] for p in probs],
-                         [dev(cuda, p[5]) for p in probs], [p[6] for p in probs], [p[9] for p in probs], Cs,
-                         [max(p[0], 1) for p in probs])
+
+    def grouped():
+        ozb.dgemm_i8_batched(handle, ta, tb, [p[0] for p in probs], [p[1] for p in probs], [p[2] for p in probs],
+                             [p[8] for p in probs], [dev(cuda, p[3]) for p in probs], [p[4] for p in probs],
+                             [dev(cuda, p[5]) for p in probs], [p[6] for p in probs], [p[9] for p in probs], Cs,
+                             [max(p[0], 1) for p in probs])
+
+    grouped()  # settles the dealing order's measurement
+    for c, p in zip(Cs, probs):
+        c.copy_(dev(cuda, p[7]))
+    l0 = handle.launch_count()
+    grouped()
+    assert handle.launch_count() - l0 == (2 if split == "one launch" else 4)
+    monkeypatch.delenv("OZBLAS_GROUPED_SPLIT3", raising=False)
+    handle.read_env()
     for i, p in enumerate(probs):
         m, n, k, A, lda, B, ldb, C0, al, be = p
         dC = dev(cuda, C0)
