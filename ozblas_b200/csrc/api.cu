@@ -280,6 +280,9 @@ int cuozblasHandleCreate(cuozblasHandle_t *h, uint64_t workSizeBytes) {
     if (e == cudaSuccess) e = cudaMemset(st->d_persist, 0, kPersistBytes);
     if (e == cudaSuccess) e = cudaMallocHost((void **)&st->h_ints, sizeof(int) * 64);
     if (e == cudaSuccess) e = cudaMallocHost((void **)&st->h_dbl, sizeof(double) * 64);
+    if (e == cudaSuccess) e = cudaMallocHost((void **)&st->h_stage, kStageBytes);
+    if (e == cudaSuccess) e = cudaHostAlloc((void **)&st->h_mail, sizeof(int) * kMailInts, cudaHostAllocMapped);
+    if (e == cudaSuccess) e = cudaHostGetDevicePointer((void **)&st->d_mail, st->h_mail, 0);
     for (int i = 0; i < 5 && e == cudaSuccess; i++) e = cudaEventCreate(&st->ev[i]);
     if (e != cudaSuccess) {
         fprintf(stderr, "cuozblas: work memory allocation error (%1.3e bytes requested): %s\n",
@@ -290,6 +293,8 @@ int cuozblasHandleCreate(cuozblasHandle_t *h, uint64_t workSizeBytes) {
         if (st->d_persist) cudaFree(st->d_persist);
         if (st->h_ints) cudaFreeHost(st->h_ints);
         if (st->h_dbl) cudaFreeHost(st->h_dbl);
+        if (st->h_stage) cudaFreeHost(st->h_stage);
+        if (st->h_mail) cudaFreeHost(st->h_mail);
         delete st;
         memset(h, 0, sizeof(*h));
         return CUOZBLAS_STATUS_CUDA_ERROR;
@@ -317,6 +322,8 @@ int cuozblasHandleDestroy(cuozblasHandle_t *h) {
     cudaFree(st->d_persist);
     cudaFreeHost(st->h_ints);
     cudaFreeHost(st->h_dbl);
+    if (st->h_stage) cudaFreeHost(st->h_stage);
+    if (st->h_mail) cudaFreeHost(st->h_mail);
     for (int i = 0; i < 5; i++)
         if (st->ev[i]) cudaEventDestroy(st->ev[i]);
     delete st;

@@ -20,6 +20,7 @@
 #include <cuda.h>
 
 #include <algorithm>
+#include <atomic>
 #include <functional>
 #include <queue>
 #include <vector>
@@ -287,6 +288,8 @@ struct GSplitArgs {
     unsigned long long dig_capacity;
     unsigned *bar;  // three barrier counters and two work counters, zero at launch
     int *err;
+    int *mail;      // host-mapped: [0] tag, [1] error so far, [2 + i] digit count of operand i (or null)
+    int tag;
 };
 
 __device__ __forceinline__ bool g_grid_barrier(unsigned *ctr, int *err) {
@@ -432,6 +435,13 @@ __global__ void __launch_bounds__(512, 1) k_g_split(const GSplitArgs a) {
             off += g_digit_bytes(S, a.ops[i].tiles_l, a.ops[i].nkb);
         }
         if (off > a.dig_capacity) atomicExch(a.err, 2);
+        if (a.mail) {  // post the counts: the host builds the schedules while the digits are cut
+            for (int i = 0; i < a.nops; i++) ((volatile int *)a.mail)[2 + i] = a.ops[i].S;
+            ((volatile int *)a.mail)[1] = *(volatile int *)a.err;
+            __threadfence_system();
+            ((volatile int *)a.mail)[0] = a.tag;
+            __threadfence_system();
+        }
     }
     if (!g_grid_barrier(&a.bar[2], a.err)) return;
     // 3: digits
@@ -816,10 +826,10 @@ int gemm_i8_batched(cuozblasHandle_t *h, char ta, char tb, int count, const int 
     OZB_CHECK(cudaMemsetAsync(d_need, 0, (size_t)nops * sizeof(int), s));
     OZB_CHECK(cudaMemsetAsync(d_bar, 0, 8 * sizeof(unsigned), s));
     OZB_CHECK(cudaMemsetAsync(d_serr, 0, sizeof(int), s));
-    OZB_CHECK(cudaMemcpyAsync(d_ops, ops.data(), sizeof(GOp) * nops, cudaMemcpyHostToDevice, s));
-    OZB_CHECK(cudaMemcpyAsync(d_line0, line0.data(), sizeof(int) * (nops + 1), cudaMemcpyHostToDevice, s));
-    if (!blocks.empty())
-        OZB_CHECK(cudaMemcpyAsync(d_blocks, blocks.data(), sizeof(int4) * blocks.size(), cudaMemcpyHostToDevice, s));
+    size_t staged = 0;  // bytes of the handle's pinned staging used by this call
+    OZB_CHECK(stage_upload(st, d_ops, ops.data(), sizeof(GOp) * nops, staged));
+    OZB_CHECK(stage_upload(st, d_line0, line0.data(), sizeof(int) * (nops + 1), staged));
+    OZB_CHECK(stage_upload(st, d_blocks, blocks.data(), sizeof(int4) * blocks.size(), staged));
     ev_record(h, 0);
     bool fused = coop_grid > 0;
     if (fused) {
@@ -836,6 +846,13 @@ int gemm_i8_batched(cuozblasHandle_t *h, char ta, char tb, int count, const int 
         ga.dig_capacity = dig_bound;
         ga.bar = d_bar;
         ga.err = d_serr;
+        const bool mail = st->h_mail != nullptr && nops + 2 <= kMailInts;
+        if (mail) {
+            st->mail_seq = st->mail_seq == 0x7fffffff ? 1 : st->mail_seq + 1;
+            ((volatile int *)st->h_mail)[0] = 0;
+        }
+        ga.mail = mail ? st->d_mail : nullptr;
+        ga.tag = st->mail_seq;
         void *args[] = {&ga};
         counted(h);
         if (cudaLaunchCooperativeKernel((const void *)k_g_split, dim3(coop_grid), dim3(512), args, 0, s) !=
@@ -858,14 +875,39 @@ int gemm_i8_batched(cuozblasHandle_t *h, char ta, char tb, int count, const int 
     }
     OZB_CHECK(cudaGetLastError());
     std::vector<int> need((size_t)nops + 1);
-    OZB_CHECK(cudaMemcpyAsync(need.data(), d_need, sizeof(int) * nops, cudaMemcpyDeviceToHost, s));
-    OZB_CHECK(cudaMemcpyAsync(need.data() + nops, d_serr, sizeof(int), cudaMemcpyDeviceToHost, s));
-    OZB_CHECK(cudaStreamSynchronize(s));
+    // The fused split posts the digit counts to host memory before it cuts
+    // the digits: wait for that post (bounded), not for the kernel.
+    bool posted = false;
+    if (fused && st->h_mail != nullptr && nops + 2 <= kMailInts) {
+        volatile int *mb = st->h_mail;
+        const double t0 = wall_seconds();
+        for (uint32_t it = 0;; it++) {
+            if (mb[0] == st->mail_seq) {
+                posted = true;
+                break;
+            }
+            if ((it & 1023) == 1023 && (cudaStreamQuery(s) != cudaErrorNotReady || wall_seconds() - t0 > 5.0)) {
+                posted = mb[0] == st->mail_seq;
+                break;
+            }
+        }
+        if (posted) {
+            std::atomic_thread_fence(std::memory_order_acquire);
+            for (int o = 0; o < nops; o++) need[(size_t)o] = mb[2 + o];
+            need[(size_t)nops] = mb[1];
+        }
+    }
+    if (!posted) {
+        OZB_CHECK(cudaMemcpyAsync(need.data(), d_need, sizeof(int) * nops, cudaMemcpyDeviceToHost, s));
+        OZB_CHECK(cudaMemcpyAsync(need.data() + nops, d_serr, sizeof(int), cudaMemcpyDeviceToHost, s));
+        OZB_CHECK(cudaStreamSynchronize(s));
+    }
     const int serr = fused ? need[(size_t)nops] : 0;
     if (serr == 1) {
         fprintf(stderr, "cuozblas: grouped INT8 split: a grid barrier timed out\n");
         return CUOZBLAS_STATUS_DEVICE_TIMEOUT;
     }
+    if (serr == 2 && posted) OZB_CHECK(cudaStreamSynchronize(s));  // the kernel stops there: digits below
     const bool carved = fused && serr == 0;  // the launch cut the digits into the region
     if (!carved && dig_region) {
         ar.release(mk_dig);
@@ -890,7 +932,7 @@ int gemm_i8_batched(cuozblasHandle_t *h, char ta, char tb, int count, const int 
     }
     if (!ar.ok) return CUOZBLAS_STATUS_WORKSPACE;
     if (!carved && !blocks.empty()) {
-        OZB_CHECK(cudaMemcpyAsync(d_ops, ops.data(), sizeof(GOp) * nops, cudaMemcpyHostToDevice, s));
+        OZB_CHECK(stage_upload(st, d_ops, ops.data(), sizeof(GOp) * nops, staged));
         counted(h);
         k_g_digits<<<(unsigned)blocks.size(), 512, 0, s>>>(d_blocks, d_ops);
         OZB_CHECK(cudaGetLastError());
@@ -954,16 +996,17 @@ int gemm_i8_batched(cuozblasHandle_t *h, char ta, char tb, int count, const int 
     int *d_cta = ar.take<int>(2 * ((uint64_t)grid + 1));
     int *d_err = ar.take<int>(1);
     if (!ar.ok) return CUOZBLAS_STATUS_WORKSPACE;
-    std::vector<int4> sched(items);
-    sched.insert(sched.end(), groups.begin(), groups.end());
-    sched.insert(sched.end(), tiles.begin(), tiles.end());
-    sched.insert(sched.end(), tiles_m1.begin(), tiles_m1.end());
-    std::vector<int> ctas(cta_begin);
-    ctas.insert(ctas.end(), cta_begin_m1.begin(), cta_begin_m1.end());
-    OZB_CHECK(cudaMemcpyAsync(d_probs, probs.data(), sizeof(GProb) * count, cudaMemcpyHostToDevice, s));
-    if (!sched.empty())
-        OZB_CHECK(cudaMemcpyAsync(d_sched, sched.data(), sizeof(int4) * sched.size(), cudaMemcpyHostToDevice, s));
-    OZB_CHECK(cudaMemcpyAsync(d_cta, ctas.data(), sizeof(int) * ctas.size(), cudaMemcpyHostToDevice, s));
+    OZB_CHECK(stage_upload(st, d_probs, probs.data(), sizeof(GProb) * count, staged));
+    {  // items, groups, both tile lists and both CTA ranges, one after the other
+        int4 *dst = d_sched;
+        for (const std::vector<int4> *v : {&items, &groups, &tiles, &tiles_m1}) {
+            OZB_CHECK(stage_upload(st, dst, v->data(), sizeof(int4) * v->size(), staged));
+            dst += v->size();
+        }
+        OZB_CHECK(stage_upload(st, d_cta, cta_begin.data(), sizeof(int) * cta_begin.size(), staged));
+        OZB_CHECK(stage_upload(st, d_cta + cta_begin.size(), cta_begin_m1.data(), sizeof(int) * cta_begin_m1.size(),
+                               staged));
+    }
     OZB_CHECK(cudaMemsetAsync(d_err, 0, sizeof(int), s));
     GParams gp;
     gp.probs = d_probs;
@@ -992,7 +1035,7 @@ int gemm_i8_batched(cuozblasHandle_t *h, char ta, char tb, int count, const int 
                 pr.beta = 0.0;
                 off += (size_t)(pr.m > 0 ? pr.m : 0) * (size_t)(pr.n > 0 ? pr.n : 0);
             }
-            OZB_CHECK(cudaMemcpyAsync(d_trial, trial.data(), sizeof(GProb) * count, cudaMemcpyHostToDevice, s));
+            OZB_CHECK(stage_upload(st, d_trial, trial.data(), sizeof(GProb) * count, staged));
             uint64_t hk = tune_hash(&count, sizeof(count));
             for (const GOp &o : ops) {
                 const int sig[3] = {o.lines, o.k, o.S};
@@ -1027,9 +1070,14 @@ int gemm_i8_batched(cuozblasHandle_t *h, char ta, char tb, int count, const int 
         OZB_CHECK(cudaGetLastError());
     }
     ev_record(h, 3);
-    int herr = 0;
+    int herr = 0, serr_end = 0;
     OZB_CHECK(cudaMemcpyAsync(&herr, d_err, sizeof(int), cudaMemcpyDeviceToHost, s));
+    if (carved) OZB_CHECK(cudaMemcpyAsync(&serr_end, d_serr, sizeof(int), cudaMemcpyDeviceToHost, s));
     OZB_CHECK(cudaStreamSynchronize(s));
+    if (serr_end != 0) {
+        fprintf(stderr, "cuozblas: grouped INT8 split: a grid barrier timed out\n");
+        return CUOZBLAS_STATUS_DEVICE_TIMEOUT;
+    }
     if (herr != 0) {
         fprintf(stderr, "cuozblas: grouped INT8 GEMM kernel wait timed out (code %d)\n", herr);
         return CUOZBLAS_STATUS_DEVICE_TIMEOUT;

@@ -1,5 +1,7 @@
 // ozb_internal.h — host-side state shared by the library's translation units.
 #pragma once
+#include <chrono>
+#include <string.h>
 #include <atomic>
 #include <vector>
 #include <cuda_runtime.h>
@@ -47,6 +49,10 @@ struct State {
     uint64_t high_water = 0;
     int *d_ints = nullptr;        // small device int scratch (counters, error word)
     int *h_ints = nullptr;        // pinned host mirror
+    char *h_stage = nullptr;      // pinned staging for schedule uploads (kStageBytes)
+    int *h_mail = nullptr;        // pinned, device-mapped: counts a running kernel posts to the host (kMailInts)
+    int *d_mail = nullptr;        // its device address
+    int mail_seq = 0;             // the last post's tag
     double *h_dbl = nullptr;      // pinned host doubles (scalar results)
     int last_error = 0;
     int64_t splitA_ld = 0;        // slice stride of the pre-split A (cuozblasDcsrmvSplitA)
@@ -92,6 +98,36 @@ inline void span_end(cuozblasHandle_t *h) {
     ev_record(h, 3);
     ev_record(h, 4);
     state(h)->plain_timers = true;
+}
+
+// Pinned staging of a handle, for host -> device uploads of schedules: a copy
+// from pinned memory is a plain asynchronous DMA, one from pageable memory is
+// staged by the driver on the calling thread.
+constexpr size_t kStageBytes = size_t(8) << 20;
+constexpr int kMailInts = 16384;
+
+// Monotonic wall clock (s), for bounded host waits.
+inline double wall_seconds() {
+    return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+
+// Upload `bytes` from host `src` to device `dst` on the handle's stream
+// through the staging buffer when it has room (`used`: staging bytes this call
+// has taken, 0 at its first upload, which first waits for the stream so that
+// no earlier copy still reads the buffer), else straight from `src`.
+inline cudaError_t stage_upload(State *st, void *dst, const void *src, size_t bytes, size_t &used) {
+    if (bytes == 0) return cudaSuccess;
+    const size_t at = (used + 15) & ~size_t(15);
+    if (st->h_stage && at + bytes <= kStageBytes) {
+        if (used == 0) {
+            const cudaError_t e = cudaStreamSynchronize(st->stream);
+            if (e != cudaSuccess) return e;
+        }
+        memcpy(st->h_stage + at, src, bytes);
+        used = at + bytes;
+        return cudaMemcpyAsync(dst, st->h_stage + at, bytes, cudaMemcpyHostToDevice, st->stream);
+    }
+    return cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, st->stream);
 }
 
 // Bump allocation from the handle's arena (no cudaMalloc on the call path).
