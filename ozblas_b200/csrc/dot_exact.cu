@@ -183,6 +183,59 @@ __device__ __forceinline__ void prove_element(double x0, double y0, double x1, d
     }
 }
 
+// The ring kernel's last block: the proof from every block's witness
+// candidates (largest and lowest-bit elements), which on ordinary data proves
+// every level.  Then status 1: the result is published and the scratch left
+// zeroed, as k_dot_prove's last block does; 2: some level still needs a
+// witness (k_dot_prove goes on from the levels proven here); 0: the one-pass
+// result cannot be used (invalid plan, incomplete split or uncertified
+// rounding; scratch left zeroed, the two-pass DOT runs).
+template <int G, bool SAME>
+__device__ void dot_ring_publish(DotScratch *sc, DotExactScratch *xs, int rho, int maxS, double res, int cert) {
+    __shared__ TreePlan pl;
+    const int t = threadIdx.x;
+    plan_in_block(&sc->vs, rho, maxS, SAME, pl);
+    __syncthreads();
+    const unsigned need0 = pl.need[0], need1 = SAME ? 0u : pl.need[1];
+    const int nA = pl.ns[0], nB = SAME ? pl.ns[0] : pl.ns[1];
+    const int zA = pl.z[0], zB = SAME ? pl.z[0] : pl.z[1];
+    const bool usable = pl.valid && cert && zA <= nA - 1 && zB <= nB - 1;
+    if (usable && (need0 | need1)) {
+        unsigned prov[2] = {0u, 0u};
+        const int ncand = (int)gridDim.x;
+        for (int base = 0; base < ncand; base += kXThreads) {  // uniform trip count
+            const int i = base + t;
+            DotCand c{0.0, 0.0, 0.0, 0.0};
+            if (i < ncand)
+                c = DotCand{__ldcg(&xs->cand[i].mx), __ldcg(&xs->cand[i].cx), __ldcg(&xs->cand[i].my),
+                            __ldcg(&xs->cand[i].cy)};
+            prove_element<G, SAME>(c.mx, c.my, c.cx, c.cy, pl, prov);
+        }
+        if ((t & 31) == 0) {
+            if (prov[0]) atomicOr(&xs->proven[0], prov[0]);
+            if (!SAME && prov[1]) atomicOr(&xs->proven[1], prov[1]);
+        }
+    }
+    __threadfence();
+    __syncthreads();
+    if (t != 0) return;
+    const bool proven =
+        (__ldcg(&xs->proven[0]) & need0) == need0 && (__ldcg(&xs->proven[1]) & need1) == need1;
+    if (usable && !proven) {
+        sc->out.status = 2;
+        return;
+    }
+    sc->out.ns0 = nA;
+    sc->out.ns1 = nB;
+    sc->out.status = usable ? 1 : 0;
+    sc->out.pad = 0;
+    sc->out.result = fma(1.0, res, 0.0 * 0.0);  // alpha = 1, beta = 0 as the DOT driver passes them
+    xs->proven[0] = xs->proven[1] = 0u;
+    xs->ticket2 = 0u;
+    xs->certified = 0;
+    sc->vs = VecStats{};
+}
+
 // The aligned form: each thread streams its double2 pairs of x and y through
 // a private cp.async ring (kXStages groups of kXU pairs per vector; a thread
 // reads back only its own copies, so no barrier), four products per group
@@ -197,10 +250,13 @@ __host__ __device__ constexpr int dot_ring_bytes() {
     return kXStages * (SAME ? 1 : 2) * kXU * kXThreads * (int)sizeof(double2);
 }
 
-template <bool SAME>
+template <int G, bool SAME>
+__device__ void dot_ring_publish(DotScratch *sc, DotExactScratch *xs, int rho, int maxS, double res, int cert);
+
+template <int G, bool SAME>
 __global__ void __launch_bounds__(kXThreads) k_dot_exact_ring(int n, const double *__restrict__ x,
                                                               const double *__restrict__ y, DotScratch *__restrict__ sc,
-                                                              DotExactScratch *__restrict__ xs) {
+                                                              DotExactScratch *__restrict__ xs, int rho, int maxS) {
     constexpr int V = SAME ? 1 : 2;
     static_assert(dot_ring_bytes<SAME>() >= 256 * (kXK2 + 3) * (int)sizeof(double), "ring too small for the scratch");
     extern __shared__ __align__(16) double2 dring[];
@@ -324,6 +380,7 @@ __global__ void __launch_bounds__(kXThreads) k_dot_exact_ring(int n, const doubl
         xs->result = res_sh;
         xs->certified = cert_sh;
     }
+    dot_ring_publish<G, SAME>(sc, xs, rho, maxS, res_sh, cert_sh);
 }
 
 template <int G, bool SAME>
@@ -437,44 +494,78 @@ int dot_exact(cuozblasHandle_t *h, int n, const double *x, const double *y, doub
     if (blocks > nsm * 4) blocks = nsm * 4;
     if (blocks > kXMaxBlocks) blocks = kXMaxBlocks;
     if (blocks < 1) blocks = 1;
+    const int G = chain_group(rho, 4);
     counted(h);
     int ncand = 0;  // blocks of the ring kernel, each leaving its witness candidates
+    static_assert(sizeof(DotStatus) == 24, "status block layout");
+    auto read_status = [&](DotStatus &res) -> int {
+        OZB_CHECK(cudaMemcpyAsync(st->h_dbl, &sc->out, sizeof(DotStatus), cudaMemcpyDeviceToHost, st->stream));
+        OZB_CHECK(cudaStreamSynchronize(st->stream));
+        memcpy(&res, st->h_dbl, sizeof(res));
+        return CUOZBLAS_STATUS_SUCCESS;
+    };
+    DotStatus res{};
+    bool need_prove = true;
     if (aligned) {
         // one wave of the ring kernel: its resident blocks per SM x SMs
-        static std::atomic<uint64_t> attr_s{0}, attr_d{0};
-        static std::atomic<int> occ_s{0}, occ_d{0};
-        const void *fn = same ? (const void *)k_dot_exact_ring<true> : (const void *)k_dot_exact_ring<false>;
+        static std::atomic<uint64_t> attr[2][4];
+        static std::atomic<int> occs[2][4];
+        const void *fn = nullptr;
+#define OZB_RING_FN(GG) fn = same ? (const void *)k_dot_exact_ring<GG, true> : (const void *)k_dot_exact_ring<GG, false>
+        switch (G) {
+            case 1: OZB_RING_FN(1); break;
+            case 2: OZB_RING_FN(2); break;
+            case 3: OZB_RING_FN(3); break;
+            default: OZB_RING_FN(4); break;
+        }
+#undef OZB_RING_FN
+        const int gi = (G < 1 ? 1 : (G > 4 ? 4 : G)) - 1, si = same ? 1 : 0;
         const int smem = same ? dot_ring_bytes<true>() : dot_ring_bytes<false>();
-        if (smem_optin(fn, smem, same ? attr_s : attr_d) != cudaSuccess) return CUOZBLAS_STATUS_CUDA_ERROR;
-        std::atomic<int> &oc = same ? occ_s : occ_d;
-        int occ = oc.load();
+        if (smem_optin(fn, smem, attr[si][gi]) != cudaSuccess) return CUOZBLAS_STATUS_CUDA_ERROR;
+        int occ = occs[si][gi].load();
         if (occ == 0) {
             if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, kXThreads, smem) != cudaSuccess || occ < 1)
                 occ = 1;
-            oc.store(occ);
+            occs[si][gi].store(occ);
         }
         int rb = (int)(((int64_t)n / 2 + (int64_t)kXU * kXThreads - 1) / ((int64_t)kXU * kXThreads));
         if (rb > nsm * occ) rb = nsm * occ;
         if (rb > kXMaxBlocks) rb = kXMaxBlocks;
         if (rb < 1) rb = 1;
         ncand = rb;
-        if (same)
-            k_dot_exact_ring<true><<<rb, kXThreads, smem, st->stream>>>(n, x, y, sc, xs);
-        else
-            k_dot_exact_ring<false><<<rb, kXThreads, smem, st->stream>>>(n, x, y, sc, xs);
+#define OZB_RING(GG)                                                                                          \
+    do {                                                                                                    \
+        if (same)                                                                                           \
+            k_dot_exact_ring<GG, true><<<rb, kXThreads, smem, st->stream>>>(n, x, y, sc, xs, rho, maxS);     \
+        else                                                                                                \
+            k_dot_exact_ring<GG, false><<<rb, kXThreads, smem, st->stream>>>(n, x, y, sc, xs, rho, maxS);    \
+    } while (0)
+        switch (G) {
+            case 1: OZB_RING(1); break;
+            case 2: OZB_RING(2); break;
+            case 3: OZB_RING(3); break;
+            default: OZB_RING(4); break;
+        }
+#undef OZB_RING
+        OZB_CHECK(cudaGetLastError());
+        span_end(h);
+        // the ring kernel's last block proved the chains from its candidates (status 1),
+        // found the one-pass result unusable (0), or left levels for the proof kernel (2)
+        OZB_TRY(read_status(res));
+        need_prove = res.status == 2;
     } else {
         if (same)
             k_dot_exact<true, false><<<blocks, kXThreads, 0, st->stream>>>(n, x, y, sc, xs);
         else
             k_dot_exact<false, false><<<blocks, kXThreads, 0, st->stream>>>(n, x, y, sc, xs);
+        OZB_CHECK(cudaGetLastError());
     }
-    OZB_CHECK(cudaGetLastError());
-    const int G = chain_group(rho, 4);
-    int pblocks = (int)((((int64_t)n + 1) / 2 + 4 * kXThreads - 1) / (4 * kXThreads));  // kPP = 4 pairs per lane
-    if (pblocks > nsm * 2) pblocks = nsm * 2;
-    if (pblocks < (ncand + kXThreads - 1) / kXThreads) pblocks = (ncand + kXThreads - 1) / kXThreads;
-    if (pblocks < 1) pblocks = 1;
-    counted(h);
+    if (need_prove) {
+        int pblocks = (int)((((int64_t)n + 1) / 2 + 4 * kXThreads - 1) / (4 * kXThreads));  // kPP = 4 pairs per lane
+        if (pblocks > nsm * 2) pblocks = nsm * 2;
+        if (pblocks < (ncand + kXThreads - 1) / kXThreads) pblocks = (ncand + kXThreads - 1) / kXThreads;
+        if (pblocks < 1) pblocks = 1;
+        counted(h);
 #define OZB_PROVE(GG)                                                                                       \
     do {                                                                                                  \
         if (same)                                                                                         \
@@ -482,20 +573,17 @@ int dot_exact(cuozblasHandle_t *h, int n, const double *x, const double *y, doub
         else                                                                                              \
             k_dot_prove<GG, false><<<pblocks, kXThreads, 0, st->stream>>>(n, x, y, rho, maxS, ncand, sc, xs); \
     } while (0)
-    switch (G) {
-        case 1: OZB_PROVE(1); break;
-        case 2: OZB_PROVE(2); break;
-        case 3: OZB_PROVE(3); break;
-        default: OZB_PROVE(4); break;
-    }
+        switch (G) {
+            case 1: OZB_PROVE(1); break;
+            case 2: OZB_PROVE(2); break;
+            case 3: OZB_PROVE(3); break;
+            default: OZB_PROVE(4); break;
+        }
 #undef OZB_PROVE
-    OZB_CHECK(cudaGetLastError());
-    span_end(h);
-    static_assert(sizeof(DotStatus) == 24, "status block layout");
-    OZB_CHECK(cudaMemcpyAsync(st->h_dbl, &sc->out, sizeof(DotStatus), cudaMemcpyDeviceToHost, st->stream));
-    OZB_CHECK(cudaStreamSynchronize(st->stream));
-    DotStatus res;
-    memcpy(&res, st->h_dbl, sizeof(res));
+        OZB_CHECK(cudaGetLastError());
+        span_end(h);
+        OZB_TRY(read_status(res));
+    }
     if (res.status == 1) {
         *done = true;
         *nA = res.ns0;

@@ -705,7 +705,7 @@ static int split_digits(cuozblasHandle_t *h, bool strided, int nl, int k, const 
             OZB_CHECK(cudaMemsetAsync(ticket, 0, sizeof(unsigned), st->stream));
             const int tiles = (nl + 127) / 128;
             int ky = (4 * sm_count() + tiles - 1) / tiles;
-            const int kmax = (k + 63) / 64;
+            const int kmax = (k + 255) / 256;  // at least 256 k per block (128 per thread)
             ky = ky < 1 ? 1 : (ky > kmax ? kmax : ky);
             counted(h);
             k_digit_count_rows<<<dim3(tiles, ky), 256, 0, st->stream>>>(k, nl, X, ldx, mxb, lsbm, ticket, op.e,

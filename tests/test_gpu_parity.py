@@ -268,15 +268,17 @@ def test_ddot_unaligned_and_odd(n, sm, oracle, handle, ozb, cuda):
 @pytest.mark.parametrize("n,phi", [((1 << 23) + 12345, 1.0), (5000001, 1.0)])
 @pytest.mark.parametrize("sm", [0, 1])
 def test_ddot_tensor_core_pass(n, phi, sm, oracle, handle, ozb, cuda):
-    """Long vectors (2 and 3 digits per level): pass 2 runs on the INT8 tensor cores.  The chains of
-    these vectors are the predicted ones, so the fused path must be the one that answers."""
+    """Long vectors (2 and 3 digits per level): with FSum pass 2 runs on the INT8 tensor cores; with NearSum the
+    one-pass exact DOT answers and its last block proves the predicted chains from the blocks' witness
+    candidates.  The chains of these vectors are the predicted ones, so the fused paths must be the ones that
+    answer: two launches (scan, tensor-core pass) with FSum, one with NearSum."""
     x = oracle.phi_vector(n, phi, 1)
     y = oracle.phi_vector(n, phi, 2)
     handle.sumMode = sm
     dx, dy = dev(cuda, x), dev(cuda, y)
     l0 = handle.launch_count()
     d = ozb.ddot(handle, n, dx, dy)
-    assert handle.launch_count() - l0 == 2  # scan, tensor-core pass: no fallback to the general path
+    assert handle.launch_count() - l0 == (2 if sm == 0 else 1)  # no fallback to the general path
     r, info = oracle.ddot(make_flags(sumMode=sm), x, y)
     assert np.float64(d).view(np.int64) == np.float64(r).view(np.int64), (d, r)
     assert (handle.nSplitA, handle.nSplitB) == (info.nSplitA, info.nSplitB)
@@ -702,7 +704,7 @@ ONE_PASS_CASES = [
 
 @pytest.mark.parametrize("case", ONE_PASS_CASES, ids=lambda c: c[0])
 def test_ddot_nearsum_one_pass(case, oracle, handle, ozb, cuda, monkeypatch):
-    """NearSum DOT and NRM2: the one-pass path (2 launches when it answers) gives the oracle's bits and exec-info
+    """NearSum DOT and NRM2: the one-pass path (one or two launches when it answers) gives the oracle's bits and exec-info
     counts, equal to the two-pass DOT's; wide ranges, cancellation, zeros, and products beyond the bins' range
     (which hand the call to the two-pass DOT) included."""
     name, n, build = case
@@ -726,7 +728,9 @@ def test_ddot_nearsum_one_pass(case, oracle, handle, ozb, cuda, monkeypatch):
     handle.read_env()
     assert np.float64(d2).view(np.int64) == np.float64(d).view(np.int64)
     if name in ("phi1", "odd_tiny"):
-        assert launches == 2, launches  # answered by the one-pass kernels
+        # answered by the one-pass kernels: the streaming kernel alone when its last block proves the chains
+        # from the witness candidates, with the proof kernel otherwise (or for unaligned vectors)
+        assert launches <= 2, launches
     # "cancel" sums to exactly zero while the bins hold the products' lowest bits only up to a bound: the
     # rounding of a sum within that bound of zero is not certified, so the two-pass DOT answers (same bits)
 
