@@ -37,6 +37,7 @@ constexpr int KB_BM = 128, KB_BN = 128, KB_BK = 128;
 constexpr int KB_W = 4;                       // most levels per block (tensor-memory accumulators)
 constexpr int KB_RA = 4, KB_RB = 8;           // ring slots for A and B planes
 constexpr int KB_TILE = KB_BM * KB_BK;        // 16 KB plane tile
+constexpr int KB_ISSUERS = 2;  // MMA issuing threads (warps 1 and 2), each owning alternate levels of a block
 constexpr int KB_THREADS = 384;  // warp 0 producer, warp 1 MMA issuer, warps 2-3 idle, warps 4-11 epilogue
 // Registers per thread: 168 at launch (65536 / 384, rounded down to 8); the
 // producer warpgroup drops to KB_REG_LO and the two epilogue warpgroups rise to
@@ -96,15 +97,15 @@ __global__ void __launch_bounds__(KB_THREADS, 1)
     if (threadIdx.x == 0) {
         for (int s = 0; s < KB_RA; s++) {
             tc::mbar_init(&fullA[s], 1);
-            tc::mbar_init(&emptyA[s], 1);
+            tc::mbar_init(&emptyA[s], KB_ISSUERS);
         }
         for (int s = 0; s < KB_RB; s++) {
             tc::mbar_init(&fullB[s], 1);
-            tc::mbar_init(&emptyB[s], 1);
+            tc::mbar_init(&emptyB[s], KB_ISSUERS);
         }
-        tc::mbar_init(acc_full, 1);
+        tc::mbar_init(acc_full, KB_ISSUERS);
         tc::mbar_init(acc_empty, 256);
-        tc::mbar_init(drain, 1);
+        for (int e = 0; e < KB_ISSUERS; e++) tc::mbar_init(drain + e, 1);
         abort_flag = 0;
         tc::fence_mbar_init();
         tc::prefetch_tmap(&tmA);
@@ -168,9 +169,14 @@ __global__ void __launch_bounds__(KB_THREADS, 1)
                 tc::drain_copies(fullB, KB_RB, issuedB, phaseB);
             }
         }
-      } else if (warp == 1) {
-        // ---------------------------------------------------------------- MMA issuer
+      } else if (warp == 1 || warp == 2) {
+        // ---------------------------------------------------------------- MMA issuers
+        // Two threads issue, each the pairs of alternate levels of a block
+        // (its own accumulators), so one thread's waits and commits between A
+        // planes overlap the other's queued MMAs.  Both wait for every plane,
+        // and every release and accumulator barrier counts both.
         if (lane == 0) {
+            const int issuer = warp - 1;
             const uint32_t idesc = tc::idesc_i8(KB_BM, KB_BN);
             uint32_t na = 0, nb = 0, nbw = 0;  // A planes consumed, B planes retired, B planes waited for
             uint32_t step_no = 0;
@@ -210,6 +216,7 @@ __global__ void __launch_bounds__(KB_THREADS, 1)
                             tc::fence_after_sync();
                             const uint64_t adesc = tc::smem_desc_k_sw128(tc::smem_u32(ringA + sa * KB_TILE));
                             for (int ib = wlo; ib <= whi; ib++) {
+                                if (((ia + ib - sp.L0) & 1) != issuer) continue;  // the other issuer's level
                                 const uint32_t sb = (b0 + (uint32_t)(whi0 - ib)) % KB_RB;
                                 const uint64_t bdesc = tc::smem_desc_k_sw128(tc::smem_u32(ringB + sb * KB_TILE));
                                 const int slot = ia + ib - sp.L0;
@@ -241,9 +248,9 @@ __global__ void __launch_bounds__(KB_THREADS, 1)
                 }
             }
             if (!ok && issued) {  // drain MMAs still in flight before tensor memory is released
-                tc::mma_commit(drain);
+                tc::mma_commit(drain + issuer);
                 const uint64_t t0 = tc::globaltimer();
-                while (!tc::mbar_try_wait(drain, 0) && tc::globaltimer() - t0 < 100000000ull) {
+                while (!tc::mbar_try_wait(drain + issuer, 0) && tc::globaltimer() - t0 < 100000000ull) {
                 }
             }
         }
