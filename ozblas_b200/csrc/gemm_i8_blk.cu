@@ -28,35 +28,12 @@
 
 #include <vector>
 
+#include "gemm_i8_blk.h"
 #include "ozb_device.cuh"
 #include "ozb_internal.h"
 #include "tc05.cuh"
 
 namespace ozb {
-
-constexpr int KB_BM = 128, KB_BN = 128, KB_BK = 128;
-constexpr int KB_W = 4;                       // most levels per block (tensor-memory accumulators)
-constexpr int KB_RA = 4, KB_RB = 8;           // ring slots for A and B planes
-constexpr int KB_TILE = KB_BM * KB_BK;        // 16 KB plane tile
-constexpr int KB_ISSUERS = 2;  // MMA issuing threads (warps 1 and 2), each owning alternate levels of a block
-                                // (three measured slower: 4.21 vs 4.00 ms at 4096^3)
-constexpr int KB_THREADS = 384;  // warp 0 producer, warp 1 MMA issuer, warps 2-3 idle, warps 4-11 epilogue
-// Registers per thread: 168 at launch (65536 / 384, rounded down to 8); the
-// producer warpgroup drops to KB_REG_LO and the two epilogue warpgroups rise to
-// KB_REG_HI: 4 x 56 + 8 x 224 = 12 x 168, and per SM sub-partition (one warp of
-// each warpgroup) 56 + 2 x 224 <= 512.
-constexpr uint32_t KB_REG_LO = 56, KB_REG_HI = 224;
-constexpr int KB_SMEM = (KB_RA + KB_RB) * KB_TILE + 1024 /*align*/ + 512 /*barriers*/;
-constexpr int64_t KB_MAX_TERMS = 2147483647LL / (127 * 127);
-
-// One (block of levels, K chunk) of the per-tile schedule.
-struct BlkStep {
-    int L0, L1;         // the block's levels
-    int kb0, kb1;       // K chunk, in 128-wide steps
-    int run_hi;         // last level of the run the block belongs to (shift 7 (run_hi - L))
-    int flags;          // 1: flush the run after this step, 2: first flush of the tile, 4: last step
-    int fexp, cexp;     // flush exponent -7 (run_hi + 2), the next run's carry exponent 7 (next_hi + 2)
-};
 
 struct BlkParams {
     int m, n, m_pad, n_pad, ldc;
@@ -78,11 +55,9 @@ __device__ __forceinline__ void blk_tile_coords(int tile, const BlkParams &p, in
     tn = w / rows;
 }
 
-__device__ __forceinline__ int blk_wlo(int L0, int ia) { return L0 - ia > 0 ? L0 - ia : 0; }
-__device__ __forceinline__ int blk_whi(int L1, int ia, int nB) { return L1 - ia < nB - 1 ? L1 - ia : nB - 1; }
 
 __global__ void __launch_bounds__(KB_THREADS, 1)
-    k_i8_blk(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, BlkParams p,
+    k_i8_blk(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, const __grid_constant__ BlkParams p,
              uint64_t wait_ns, int hold_copies) {
     extern __shared__ uint8_t smem_raw[];
     uint8_t *smem = (uint8_t *)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
@@ -343,7 +318,7 @@ __global__ void __launch_bounds__(KB_THREADS, 1)
 // stays below 2^53 (the same runs as i8_schedule), cut into blocks of at most
 // W <= KB_W levels, each block cut into K chunks that keep every accumulator's
 // INT32 sum exact.  Returns false when the levels exceed the tables' range.
-static bool blk_schedule(int nA, int nB, int nkb, bool triangular, int W, std::vector<BlkStep> &steps) {
+bool blk_schedule(int nA, int nB, int nkb, bool triangular, int W, std::vector<BlkStep> &steps) {
     if (W < 1 || W > KB_W) return false;
     const int maxlevel = triangular ? (nA < nB ? nA : nB) - 1 : nA + nB - 2;
     if (maxlevel < 0 || maxlevel >= 128) return false;
@@ -403,6 +378,12 @@ static bool blk_schedule(int nA, int nB, int nkb, bool triangular, int W, std::v
 }
 
 static std::atomic<uint64_t> g_blk_attr{0};
+
+int blk_kq_last(int k, int nkb) {
+    const int tail = k - (nkb - 1) * KB_BK;
+    const int q = (tail + 31) / 32;
+    return q < 1 ? 1 : (q > KB_BK / 32 ? KB_BK / 32 : q);
+}
 
 uint64_t i8_test_wait_ns();  // gemm_i8.cu: the wait limit and copy switch of cuozblasSetI8WaitTest
 int i8_test_hold_copies();

@@ -26,6 +26,7 @@
 #include <vector>
 
 #include "autotune.h"
+#include "gemm_i8_blk.h"
 #include "ozb_device.cuh"
 #include "ozb_internal.h"
 #include "tc05.cuh"
@@ -991,10 +992,40 @@ int gemm_i8_batched(cuozblasHandle_t *h, char ta, char tb, int count, const int 
     std::vector<int> cta_begin, cta_begin_m1;
     deal_tiles(0, grid, probs, order, cost, tiles, cta_begin);
     deal_tiles(1, grid, probs, order, cost, tiles_m1, cta_begin_m1);
+    // The level-blocked form of the same problems (k_i8_blk<true>): each
+    // problem's schedule in blocks of up to four levels, over the same tiles.
+    const bool want_lw = st->env.i8_levelwise || st->env.i8_block == 0;
+    const int bw = st->env.i8_block > 0 ? st->env.i8_block : kBlkMaxWidth;
+    std::vector<BlkStep> bsteps;
+    std::vector<BlkProb> bprobs;
+    bool blk = !st->env.i8_levelwise && ntile_total > 0;
+    if (blk) {
+        bprobs.resize((size_t)count);
+        std::vector<BlkStep> one;
+        for (int b = 0; b < count && blk; b++) {
+            const GOp &oa = ops[(size_t)2 * b], &ob = ops[(size_t)2 * b + 1];
+            const GProb &pr = probs[(size_t)b];
+            blk = blk_schedule(oa.S, ob.S, oa.nkb, h->fastMode != 0, bw, one);
+            bprobs[(size_t)b] = BlkProb{pr.m, pr.n, pr.ldc, pr.nkb, pr.tiles_m, pr.tiles_n, blk_kq_last(oa.k, pr.nkb),
+                                        oa.S, ob.S,
+                                        (int)bsteps.size(), (int)one.size(), pr.da, pr.db, pr.ea, pr.eb,
+                                        pr.alpha, pr.beta, pr.C};
+            bsteps.insert(bsteps.end(), one.begin(), one.end());
+        }
+    }
+    const bool lw = want_lw || !blk;
     GProb *d_probs = ar.take<GProb>((uint64_t)count);
     int4 *d_sched = ar.take<int4>(items.size() + groups.size() + 2 * tiles.size() + 1);
     int *d_cta = ar.take<int>(2 * ((uint64_t)grid + 1));
     int *d_err = ar.take<int>(1);
+    BlkProb *d_bprobs = nullptr;
+    BlkStep *d_bsteps = nullptr;
+    double *rbuf = nullptr;
+    if (blk) {
+        d_bprobs = ar.take<BlkProb>((uint64_t)count);
+        d_bsteps = ar.take<BlkStep>(bsteps.size() + 1);
+        rbuf = ar.take<double>((uint64_t)grid * G_T * G_T);
+    }
     if (!ar.ok) return CUOZBLAS_STATUS_WORKSPACE;
     OZB_CHECK(stage_upload(st, d_probs, probs.data(), sizeof(GProb) * count, staged));
     {  // items, groups, both tile lists and both CTA ranges, one after the other
@@ -1007,6 +1038,10 @@ int gemm_i8_batched(cuozblasHandle_t *h, char ta, char tb, int count, const int 
         OZB_CHECK(stage_upload(st, d_cta + cta_begin.size(), cta_begin_m1.data(), sizeof(int) * cta_begin_m1.size(),
                                staged));
     }
+    if (blk) {
+        OZB_CHECK(stage_upload(st, d_bprobs, bprobs.data(), sizeof(BlkProb) * count, staged));
+        OZB_CHECK(stage_upload(st, d_bsteps, bsteps.data(), sizeof(BlkStep) * bsteps.size(), staged));
+    }
     OZB_CHECK(cudaMemsetAsync(d_err, 0, sizeof(int), s));
     GParams gp;
     gp.probs = d_probs;
@@ -1015,50 +1050,72 @@ int gemm_i8_batched(cuozblasHandle_t *h, char ta, char tb, int count, const int 
     gp.tiles = d_sched + items.size() + groups.size();
     gp.cta_begin = d_cta;
     gp.err = d_err;
+    const int4 *tiles_dev[2] = {gp.tiles, gp.tiles + tiles.size()};
+    const int *cta_dev[2] = {d_cta, d_cta + grid + 1};
+    // candidates: {kernel (0 level-wise, 1 level-blocked), dealing order}
+    std::vector<std::pair<int, int>> cands;
+    if (blk) cands = {{1, 0}, {1, 1}};
+    if (lw) {
+        cands.push_back({0, 0});
+        cands.push_back({0, 1});
+    }
+    auto launch = [&](int kernel, int deal, const GProb *pl, const BlkProb *pb) -> int {
+        if (kernel == 1)
+            return i8_blk_grouped_kernel(grid, pb, d_bsteps, tiles_dev[deal], cta_dev[deal], rbuf, d_err, s) ==
+                           cudaSuccess
+                       ? 0
+                       : (int)CUOZBLAS_STATUS_CUDA_ERROR;
+        GParams gt = gp;
+        gt.probs = pl;
+        gt.tiles = tiles_dev[deal];
+        gt.cta_begin = cta_dev[deal];
+        k_i8_grouped<<<grid, G_THREADS, G_SMEM, s>>>(gt);
+        return cudaGetLastError() == cudaSuccess ? 0 : (int)CUOZBLAS_STATUS_CUDA_ERROR;
+    };
+    int pick = 0;
     if (ntile_total > 0) {
         static std::atomic<uint64_t> attr{0};  // devices already opted in
         OZB_CHECK(smem_optin((const void *)k_i8_grouped, G_SMEM, attr));
-        // dealing order: same bits either way, the faster one is measured once per
-        // problem set (candidates write scratch products with beta = 0)
+        // kernel and dealing order: same bits either way, the fastest is measured
+        // once per problem set (candidates write scratch products with beta = 0)
         const uint64_t mk = ar.mark();
         size_t outs = 0;
         for (const GProb &pr : probs) outs += (size_t)(pr.m > 0 ? pr.m : 0) * (size_t)(pr.n > 0 ? pr.n : 0);
         double *scratch = ar.take<double>(outs + 1);
         GProb *d_trial = ar.take<GProb>((uint64_t)count);
-        int pick = 0;
-        if (ar.ok) {
+        BlkProb *d_btrial = blk ? ar.take<BlkProb>((uint64_t)count) : nullptr;
+        if (ar.ok && cands.size() > 1) {
             std::vector<GProb> trial(probs);
+            std::vector<BlkProb> btrial(bprobs);
             size_t off = 0;
-            for (GProb &pr : trial) {
+            for (int b = 0; b < count; b++) {
+                GProb &pr = trial[(size_t)b];
                 pr.C = scratch + off;
                 pr.ldc = pr.m > 1 ? pr.m : 1;
                 pr.beta = 0.0;
+                if (blk) {
+                    btrial[(size_t)b].C = pr.C;
+                    btrial[(size_t)b].ldc = pr.ldc;
+                    btrial[(size_t)b].beta = 0.0;
+                }
                 off += (size_t)(pr.m > 0 ? pr.m : 0) * (size_t)(pr.n > 0 ? pr.n : 0);
             }
             OZB_CHECK(stage_upload(st, d_trial, trial.data(), sizeof(GProb) * count, staged));
+            if (blk) OZB_CHECK(stage_upload(st, d_btrial, btrial.data(), sizeof(BlkProb) * count, staged));
             uint64_t hk = tune_hash(&count, sizeof(count));
             for (const GOp &o : ops) {
                 const int sig[3] = {o.lines, o.k, o.S};
                 hk = tune_hash(sig, sizeof(sig), hk);
             }
-            char key[96];
-            snprintf(key, sizeof(key), "i8grouped:%016llx:%d:%d", (unsigned long long)hk, h->fastMode != 0 ? 1 : 0,
-                     grid);
-            pick = tune_pick(key, 2, 0, s, [&](int i) {
-                GParams gt = gp;
-                gt.probs = d_trial;
-                gt.tiles = d_sched + items.size() + groups.size() + (i ? tiles.size() : 0);
-                gt.cta_begin = d_cta + (i ? grid + 1 : 0);
-                k_i8_grouped<<<grid, G_THREADS, G_SMEM, s>>>(gt);
-                return cudaGetLastError() == cudaSuccess ? 0 : (int)CUOZBLAS_STATUS_CUDA_ERROR;
+            char key[112];
+            snprintf(key, sizeof(key), "i8grouped:%016llx:%d:%d:%d:%d", (unsigned long long)hk,
+                     h->fastMode != 0 ? 1 : 0, grid, blk ? bw : 0, lw ? 1 : 0);
+            pick = tune_pick(key, (int)cands.size(), 0, s, [&](int i) {
+                return launch(cands[(size_t)i].first, cands[(size_t)i].second, d_trial, d_btrial);
             });
         }
         ar.ok = true;
         ar.release(mk);
-        if (pick == 1) {
-            gp.tiles = d_sched + items.size() + groups.size() + tiles.size();
-            gp.cta_begin = d_cta + grid + 1;
-        }
     }
     h->nSplitA = (float)maxA;
     h->nSplitB = (float)maxB;
@@ -1066,8 +1123,11 @@ int gemm_i8_batched(cuozblasHandle_t *h, char ta, char tb, int count, const int 
     ev_record(h, 2);
     if (ntile_total > 0) {
         counted(h);
-        k_i8_grouped<<<grid, G_THREADS, G_SMEM, s>>>(gp);
-        OZB_CHECK(cudaGetLastError());
+        const int r = launch(cands[(size_t)pick].first, cands[(size_t)pick].second, d_probs, d_bprobs);
+        if (r != 0) {
+            OZB_CHECK(cudaGetLastError());
+            return r;
+        }
     }
     ev_record(h, 3);
     int herr = 0, serr_end = 0;

@@ -165,6 +165,38 @@ def test_i8_batched_matches_single(ta, tb, fast, split, oracle, handle, ozb, cud
         assert bits_equal(Cs[i].cpu().numpy(), dC.cpu().numpy()), (i, m, n, k)
 
 
+@pytest.mark.parametrize("fast", [0, 1])
+@pytest.mark.parametrize("ta,tb", [("n", "n"), ("t", "t")])
+def test_i8_batched_kernels_match_single(fast, ta, tb, oracle, handle, ozb, cuda, monkeypatch):
+    """The grouped launch's product kernel forced to the level-blocked form (widths 4, 3 and 1) and to the
+    level-wise form: every problem bit-identical to its own cuozblasDgemmI8 call in each case (a K-chunked
+    problem, ragged tiles, k = 0 and an empty problem included)."""
+    shapes = [(300, 200, 20000, 1.0), (129, 257, 500, 4.0), (1, 1, 1, 1.0), (64, 64, 0, 1.0), (0, 9, 9, 1.0),
+              (700, 130, 128, 0.5), (33, 500, 1000, 2.0)]
+    probs = _batch_case(oracle, shapes, ta, tb, 21 + fast)
+    handle.nSplitMax, handle.fastMode = 0, fast
+    singles = []
+    for p in probs:
+        m, n, k, A, lda, B, ldb, C0, al, be = p
+        dC = dev(cuda, C0)
+        if m and n:
+            ozb.dgemm_i8(handle, ta, tb, m, n, k, al, dev(cuda, A), lda, dev(cuda, B), ldb, be, dC, max(m, 1))
+        singles.append(dC.cpu().numpy())
+    for var, val in [("OZBLAS_I8_BLOCK", "4"), ("OZBLAS_I8_BLOCK", "3"), ("OZBLAS_I8_BLOCK", "1"),
+                     ("OZBLAS_I8_LEVELWISE", "1")]:
+        monkeypatch.setenv(var, val)
+        handle.read_env()
+        Cs = [dev(cuda, p[7]) for p in probs]
+        ozb.dgemm_i8_batched(handle, ta, tb, [p[0] for p in probs], [p[1] for p in probs], [p[2] for p in probs],
+                             [p[8] for p in probs], [dev(cuda, p[3]) for p in probs], [p[4] for p in probs],
+                             [dev(cuda, p[5]) for p in probs], [p[6] for p in probs], [p[9] for p in probs], Cs,
+                             [max(p[0], 1) for p in probs])
+        monkeypatch.delenv(var)
+        for i, p in enumerate(probs):
+            assert bits_equal(Cs[i].cpu().numpy(), singles[i]), (var, val, i, p[:3])
+    handle.read_env()
+
+
 def test_i8_batched_accuracy_uneven(oracle, handle, ozb, cuda):
     """48 log-uniform shapes in [16, 400], phi from {0.5, 1, 2, 4}: within 2 units of 2^-53 of the exact product."""
     rng = np.random.default_rng(5)
@@ -261,6 +293,38 @@ def test_i8_wait_timeout_reports_and_recovers(oracle, handle, ozb, cuda):
     cuda.cuda.synchronize()
     again = run_i8(ozb, handle, cuda, A, B, m, n, k)
     assert bits_equal(again, ref)
+
+
+def test_i8_batched_wait_timeout_reports_and_recovers(oracle, handle, ozb, cuda, monkeypatch):
+    """The same bounded wait in the grouped level-blocked kernel: with its producer holding back every copy and a
+    20 ms limit, cuozblasDgemmI8Batched returns CUOZBLAS_STATUS_DEVICE_TIMEOUT (6); restored, the same grouped call
+    on the same context gives the bits of the first one."""
+    monkeypatch.setenv("OZBLAS_I8_BLOCK", "4")
+    handle.read_env()
+    probs = _batch_case(oracle, [(200, 150, 300, 1.0), (64, 300, 129, 2.0), (1, 1, 1, 1.0)], "n", "n", 41)
+    handle.nSplitMax, handle.fastMode = 0, 0
+
+    def grouped():
+        Cs = [dev(cuda, p[7]) for p in probs]
+        ozb.dgemm_i8_batched(handle, "n", "n", [p[0] for p in probs], [p[1] for p in probs], [p[2] for p in probs],
+                             [p[8] for p in probs], [dev(cuda, p[3]) for p in probs], [p[4] for p in probs],
+                             [dev(cuda, p[5]) for p in probs], [p[6] for p in probs], [p[9] for p in probs], Cs,
+                             [max(p[0], 1) for p in probs])
+        return [c.cpu().numpy() for c in Cs]
+
+    ref = grouped()
+    ozb.set_i8_wait_test(20_000_000, hold_copies=True)
+    try:
+        with pytest.raises(ozb.OzblasError) as e:
+            grouped()
+        assert e.value.code == 6
+    finally:
+        ozb.set_i8_wait_test(0, hold_copies=False)
+    cuda.cuda.synchronize()
+    again = grouped()
+    monkeypatch.delenv("OZBLAS_I8_BLOCK")
+    handle.read_env()
+    assert all(bits_equal(a, b) for a, b in zip(again, ref))
 
 
 @pytest.mark.parametrize("m,n,k,phi,fast,ta,tb", [
