@@ -75,7 +75,7 @@ void EnvSwitches::read() {
     {
         const char *v = getenv("OZBLAS_I8_BLOCK");
         i8_block = v ? atoi(v) : 0;
-        if (i8_block < 0 || i8_block > 4) i8_block = 0;
+        if (i8_block < -4 || i8_block > 4) i8_block = 0;
     }
     cg_no_graph = env_on("OZBLAS_CG_NO_GRAPH");
     dot_trace = env_on("OZBLAS_DOT_TRACE");

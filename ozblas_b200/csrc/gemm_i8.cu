@@ -914,11 +914,13 @@ int gemm_i8_core(cuozblasHandle_t *h, char ta, char tb, int m, int n, int k, dou
     // Launch shape, measured once per shape (every choice gives the same bits;
     // candidates write a scratch product with beta = 0): the product kernel
     // (level-blocked or level-wise), the block width of the level-blocked
-    // schedule (levels accumulated together: 4, 3 or 2) and the rasterisation
+    // schedule (levels accumulated together: 4, 3 or 2 within the runs, or
+    // equal cuts of at most 4 or 3 levels across them) and the rasterisation
     // strip height.  OZBLAS_I8_LEVELWISE keeps the level-wise kernel (strip
-    // tuned), OZBLAS_I8_BLOCK=w the level-blocked kernel at width w.
+    // tuned), OZBLAS_I8_BLOCK=w the level-blocked kernel at width w (negative:
+    // the cuts across runs).
     struct Shape {
-        int width;  // 0: level-wise kernel
+        int width;  // 0: level-wise kernel; < 0: blocks of at most -width levels cut across runs
         int strip;
     };
     std::vector<Shape> cand;
@@ -930,16 +932,18 @@ int gemm_i8_core(cuozblasHandle_t *h, char ta, char tb, int m, int n, int k, dou
     };
     if (st->env.i8_levelwise) {
         for (int sv : {12, 4, 8, 16, 24}) add(0, sv);
-    } else if (st->env.i8_block > 0) {
+    } else if (st->env.i8_block != 0) {
         for (int sv : {12, 4, 8, 16, 24}) add(st->env.i8_block, sv);
     } else {
         for (int sv : {12, 4, 8, 16, 24}) add(4, sv);
+        add(-4, 12);
+        add(-3, 12);
         add(3, 12);
         add(2, 12);
         add(0, 12);
     }
     auto launch = [&](const Shape &c, I8Params &pp) {
-        if (c.width > 0) {
+        if (c.width != 0) {
             const uint64_t mk2 = ar.mark();
             const int r = i8_blk_launch(h, tmA, tmB, m, n, pp.m_pad, pp.n_pad, k_pad, nA, nB, h->fastMode != 0, da.e,
                                         db.e, pp.alpha, pp.beta, pp.C, pp.ldc, c.strip, c.width, d_err, ar);

@@ -255,7 +255,39 @@ __global__ void __launch_bounds__(KB_THREADS, 1)
                     break;
                 }
                 tc::fence_after_sync();
-                for (int L = sp.L0; L <= sp.L1; L++) {
+                if (sp.mid < sp.L1) {  // the block ends a run at mid: add its levels and flush it first
+                    for (int L = sp.L0; L <= sp.mid; L++) {
+                        const double sc = pow2(7 * (sp.mid - L));
+                        const uint32_t taddr = lane_base + (uint32_t)(L - sp.L0) * KB_BN + half * 64;
+                        uint32_t v[32];
+                        tc::tmem_ld_32x32b_x32(taddr, v);
+                        tc::tmem_ld_wait();
+#pragma unroll
+                        for (int c = 0; c < 32; c++) acc[c] += (double)(int32_t)v[c] * sc;
+                        tc::tmem_ld_32x32b_x32(taddr + 32, v);
+                        tc::tmem_ld_wait();
+#pragma unroll
+                        for (int c = 0; c < 32; c++) acc[32 + c] += (double)(int32_t)v[c] * sc;
+                    }
+                    const double fs = pow2(sp.fexp_mid), cs = pow2(sp.cexp_mid);
+                    const bool first = sp.first_mid != 0;
+#pragma unroll
+                    for (int c = 0; c < 64; c++) {
+                        double *rp = &R[(size_t)(half * 64 + c) * KB_BM + row];
+                        if (first) {
+                            *rp = acc[c] * fs;
+                            acc[c] = 0.0;
+                        } else {
+                            const double ro = *rp;
+                            const double a = acc[c] * fs;
+                            const double sm = ro + a;
+                            const double bb = sm - ro;
+                            acc[c] = ((ro - (sm - bb)) + (a - bb)) * cs;  // TwoSum error, in the next run's units
+                            *rp = sm;
+                        }
+                    }
+                }
+                for (int L = sp.mid < sp.L1 ? sp.mid + 1 : sp.L0; L <= sp.L1; L++) {
                     const double sc = pow2(7 * (sp.run_hi - L));
                     const uint32_t taddr = lane_base + (uint32_t)(L - sp.L0) * KB_BN + half * 64;
                     uint32_t v[32];
@@ -318,7 +350,10 @@ __global__ void __launch_bounds__(KB_THREADS, 1)
 // stays below 2^53 (the same runs as i8_schedule), cut into blocks of at most
 // W <= KB_W levels, each block cut into K chunks that keep every accumulator's
 // INT32 sum exact.  Returns false when the levels exceed the tables' range.
-bool blk_schedule(int nA, int nB, int nkb, bool triangular, int W, std::vector<BlkStep> &steps) {
+// The order of the products and flushes does not depend on the cut: each
+// accumulator and each run's sum is an exact integer, and the runs are flushed
+// in the same order with the same values, so every cut gives the same bits.
+bool blk_schedule(int nA, int nB, int nkb, bool triangular, int W, std::vector<BlkStep> &steps, bool across) {
     if (W < 1 || W > KB_W) return false;
     const int maxlevel = triangular ? (nA < nB ? nA : nB) - 1 : nA + nB - 2;
     if (maxlevel < 0 || maxlevel >= 128) return false;
@@ -331,7 +366,7 @@ bool blk_schedule(int nA, int nB, int nkb, bool triangular, int W, std::vector<B
     for (int L = 0; L <= maxlevel; L++)
         lbound[L] = (unsigned __int128)pairs(L) * (unsigned __int128)nkb * KB_BK * 127 * 127;
     const unsigned __int128 lim = (unsigned __int128)1 << 53;
-    std::vector<int> run_lo, run_hi;
+    std::vector<int> run_lo, run_hi, run_of(maxlevel + 1);
     for (int L0 = 0; L0 <= maxlevel;) {
         unsigned __int128 b = lbound[L0];
         int L1 = L0;
@@ -339,40 +374,66 @@ bool blk_schedule(int nA, int nB, int nkb, bool triangular, int W, std::vector<B
             b = (b << 7) + lbound[L1 + 1];
             L1++;
         }
+        for (int L = L0; L <= L1; L++) run_of[L] = (int)run_lo.size();
         run_lo.push_back(L0);
         run_hi.push_back(L1);
         L0 = L1 + 1;
     }
+    const int nruns = (int)run_lo.size();
+    // the blocks: within the runs, or equal cuts of all levels
+    std::vector<std::pair<int, int>> blocks;
+    if (across) {
+        const int n = maxlevel + 1, nb = (n + W - 1) / W, base = n / nb, extra = n % nb;
+        for (int i = 0, L0 = 0; i < nb; i++) {
+            const int size = base + (i >= nb - extra ? 1 : 0);
+            blocks.push_back({L0, L0 + size - 1});
+            L0 += size;
+        }
+    } else {
+        for (int r = 0; r < nruns; r++)
+            for (int L0 = run_lo[r]; L0 <= run_hi[r]; L0 += W)
+                blocks.push_back({L0, L0 + W - 1 < run_hi[r] ? L0 + W - 1 : run_hi[r]});
+    }
     steps.clear();
-    for (size_t r = 0; r < run_lo.size(); r++) {
-        const int next_hi = r + 1 < run_lo.size() ? run_hi[r + 1] : 0;
-        for (int L0 = run_lo[r]; L0 <= run_hi[r]; L0 += W) {
-            const int L1 = L0 + W - 1 < run_hi[r] ? L0 + W - 1 : run_hi[r];
-            int pmax = 0;
-            for (int L = L0; L <= L1; L++) pmax = pairs(L) > pmax ? pairs(L) : pmax;
-            int chunk = (int)(KB_MAX_TERMS / ((int64_t)pmax * KB_BK));  // K steps per INT32 sum
-            if (chunk < 1) return false;
-            for (int kb0 = 0; kb0 < nkb; kb0 += chunk) {
-                BlkStep s;
-                s.L0 = L0;
-                s.L1 = L1;
-                s.kb0 = kb0;
-                s.kb1 = kb0 + chunk < nkb ? kb0 + chunk : nkb;
-                s.run_hi = run_hi[r];
-                s.flags = 0;
-                if (L1 == run_hi[r] && s.kb1 == nkb) s.flags |= 1;
-                s.fexp = -7 * (run_hi[r] + 2);
-                s.cexp = 7 * (next_hi + 2);
-                steps.push_back(s);
-            }
+    for (const auto &bl : blocks) {
+        const int L0 = bl.first, L1 = bl.second;
+        const int ra = run_of[L0], rb = run_of[L1];
+        if (rb > ra + 1) return false;  // at most one run boundary inside a block
+        int pmax = 0;
+        for (int L = L0; L <= L1; L++) pmax = pairs(L) > pmax ? pairs(L) : pmax;
+        int chunk = (int)(KB_MAX_TERMS / ((int64_t)pmax * KB_BK));  // K steps per INT32 sum
+        if (chunk < 1) return false;
+        if (rb != ra && chunk < nkb) return false;  // a crossing block is one K chunk
+        const int next_hi = rb + 1 < nruns ? run_hi[rb + 1] : 0;
+        for (int kb0 = 0; kb0 < nkb; kb0 += chunk) {
+            BlkStep s;
+            s.L0 = L0;
+            s.L1 = L1;
+            s.kb0 = kb0;
+            s.kb1 = kb0 + chunk < nkb ? kb0 + chunk : nkb;
+            s.run_hi = run_hi[rb];
+            s.flags = 0;
+            if (L1 == run_hi[rb] && s.kb1 == nkb) s.flags |= 1;
+            s.fexp = -7 * (run_hi[rb] + 2);
+            s.cexp = 7 * (next_hi + 2);
+            s.mid = rb != ra ? run_hi[ra] : L1;
+            s.fexp_mid = -7 * (run_hi[ra] + 2);
+            s.cexp_mid = 7 * (run_hi[rb] + 2);
+            s.first_mid = 0;
+            steps.push_back(s);
         }
     }
     // the first flush of a tile writes R, the last one writes C
-    for (auto &s : steps)
+    for (auto &s : steps) {
+        if (s.mid < s.L1) {
+            s.first_mid = 1;
+            break;
+        }
         if (s.flags & 1) {
             s.flags |= 2;
             break;
         }
+    }
     steps.back().flags |= 4;
     return (steps.back().flags & 1) != 0;
 }
@@ -390,14 +451,16 @@ int i8_test_hold_copies();
 
 // The level-blocked product kernel over digit operands laid out as for
 // k_i8_gemm (tensor maps over [S * lines_pad][k_pad], 128 x 128-byte boxes).
-// `width`: levels per block (1..4; every width gives the same bits).
+// `width`: levels per block (1..4, within the runs; -4..-1: equal cuts of at
+// most -width levels across the runs; every width gives the same bits).
 // Returns NOT_SUPPORTED (nothing launched) when the schedule does not apply.
 int i8_blk_launch(cuozblasHandle_t *h, const CUtensorMap &tmA, const CUtensorMap &tmB, int m, int n, int m_pad,
                   int n_pad, int k_pad, int nA, int nB, bool triangular, const int *ea, const int *eb, double alpha,
                   double beta, double *C, int ldc, int strip, int width, int *d_err, Arena &ar) {
     State *st = state(h);
     std::vector<BlkStep> steps;
-    if (!blk_schedule(nA, nB, k_pad / KB_BK, triangular, width, steps)) return CUOZBLAS_STATUS_NOT_SUPPORTED;
+    if (!blk_schedule(nA, nB, k_pad / KB_BK, triangular, width < 0 ? -width : width, steps, width < 0))
+        return CUOZBLAS_STATUS_NOT_SUPPORTED;
     const int nsm = sm_count();
     const int tiles_m = m_pad / KB_BM, tiles_n = n_pad / KB_BN, ntiles = tiles_m * tiles_n;
     const int grid = ntiles < nsm ? ntiles : nsm;

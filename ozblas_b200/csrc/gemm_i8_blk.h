@@ -10,13 +10,19 @@
 
 namespace ozb {
 
-// One (block of levels, K chunk) of the per-tile schedule.
+// One (block of levels, K chunk) of the per-tile schedule.  A block may end
+// one run and begin the next (then it is the block's only K chunk): its levels
+// L0..mid belong to the run ending at mid, flushed before the levels above it
+// are read; mid = L1 when the block lies within one run.
 struct BlkStep {
     int L0, L1;         // the block's levels
     int kb0, kb1;       // K chunk, in 128-wide steps
-    int run_hi;         // last level of the run the block belongs to (shift 7 (run_hi - L))
+    int run_hi;         // last level of the run of levels mid+1..L1 (or of the whole block): shift 7 (run_hi - L)
     int flags;          // 1: flush the run after this step, 2: first flush of the tile, 4: last step
     int fexp, cexp;     // flush exponent -7 (run_hi + 2), the next run's carry exponent 7 (next_hi + 2)
+    int mid;            // last level of the first run when the block crosses a run boundary, else L1
+    int fexp_mid, cexp_mid;  // that run's flush exponent -7 (mid + 2) and carry exponent 7 (run_hi + 2)
+    int first_mid;      // 1: the flush at mid is the tile's first flush
 };
 
 // One problem of a grouped level-blocked launch.  Digit plane s of op(A) is
@@ -63,9 +69,13 @@ int blk_kq_last(int k, int nkb);
 
 // Runs of consecutive levels whose exact combination stays below 2^53 (the
 // runs of the level-wise schedule), cut into blocks of at most W levels, each
-// block cut into K chunks that keep every INT32 sum exact.  False when the
-// levels exceed the kernel's range.
-bool blk_schedule(int nA, int nB, int nkb, bool triangular, int W, std::vector<BlkStep> &steps);
+// block cut into K chunks that keep every INT32 sum exact.  With `across`, the
+// levels are cut into equal blocks of at most W levels regardless of the runs
+// (the larger blocks at the top), each crossing at most one run boundary and
+// then only when it needs a single K chunk; false where that does not hold.
+// False also when the levels exceed the kernel's range.
+bool blk_schedule(int nA, int nB, int nkb, bool triangular, int W, std::vector<BlkStep> &steps,
+                  bool across = false);
 
 // The grouped level-blocked launch: CTA c runs the tiles {problem, tm, tn, 0}
 // in [cta_begin[c], cta_begin[c + 1]); rbuf holds grid x 128 x 128 doubles;

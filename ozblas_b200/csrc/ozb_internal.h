@@ -33,7 +33,7 @@ struct EnvSwitches {
     bool gemv_slices = false;  // OZBLAS_GEMV_SLICES: NearSum GEMV 'n' through its slices
     bool i8_levelwise = false; // OZBLAS_I8_LEVELWISE: the INT8 form's products level by level (k_i8_gemm)
     bool g_split3 = false;     // OZBLAS_GROUPED_SPLIT3: the grouped INT8 split as three launches
-    int i8_block = 0;          // OZBLAS_I8_BLOCK: levels per block of the level-blocked INT8 kernel (1-4; 0: measured)
+    int i8_block = 0;          // OZBLAS_I8_BLOCK: levels per block of the level-blocked INT8 kernel (1-4; -4..-1: cut across runs; 0: measured)
     bool cg_no_graph = false;  // OZBLAS_CG_NO_GRAPH: CG iterations on the host loop
     bool dot_trace = false;    // OZBLAS_DOT_TRACE
     bool cg_trace = false;     // OZBLAS_CG_TRACE

@@ -338,7 +338,8 @@ def test_i8_batched_wait_timeout_reports_and_recovers(oracle, handle, ozb, cuda,
 ])
 def test_i8_level_blocked_equals_levelwise(m, n, k, phi, fast, ta, tb, oracle, handle, ozb, cuda, monkeypatch):
     """The level-blocked product kernel (k_i8_blk) gives the bits of the level-wise one (k_i8_gemm) at every block
-    width (levels accumulated together): the same products and sums, in another order of the exact INT32
+    width (levels accumulated together), with blocks within the runs of levels and with equal cuts across them (a
+    run flushed in the middle of a block): the same products and sums, in another order of the exact INT32
     accumulations."""
     A = oracle.phi_matrix(m, k, phi, 1) if ta == "n" else oracle.phi_matrix(k, m, phi, 1)
     B = oracle.phi_matrix(k, n, phi, 2) if tb == "n" else oracle.phi_matrix(n, k, phi, 2)
@@ -346,11 +347,12 @@ def test_i8_level_blocked_equals_levelwise(m, n, k, phi, fast, ta, tb, oracle, h
     outs = {}
     for name, var, val in [("w4", "OZBLAS_I8_BLOCK", "4"), ("w3", "OZBLAS_I8_BLOCK", "3"),
                            ("w2", "OZBLAS_I8_BLOCK", "2"), ("w1", "OZBLAS_I8_BLOCK", "1"),
+                           ("x4", "OZBLAS_I8_BLOCK", "-4"), ("x3", "OZBLAS_I8_BLOCK", "-3"),
                            ("levelwise", "OZBLAS_I8_LEVELWISE", "1")]:
         monkeypatch.setenv(var, val)
         handle.read_env()
         outs[name] = run_i8(ozb, handle, cuda, A, B, m, n, k, ta=ta, tb=tb, fast=fast, alpha=-0.75, beta=0.5, C0=C0)
         monkeypatch.delenv(var)
     handle.read_env()
-    for w in ("w4", "w3", "w2", "w1"):
+    for w in ("w4", "w3", "w2", "w1", "x4", "x3"):
         assert bits_equal(outs[w], outs["levelwise"]), w
