@@ -300,42 +300,50 @@ __global__ void __launch_bounds__(KB_THREADS, 1)
                     break;
                 }
                 tc::fence_after_sync();
-                for (int L = sp.L0; L <= sp.L1; L++) {
-                    const double sc = pow2(7 * (sp.run_hi - L));
-                    const uint32_t taddr = lane_base + (uint32_t)(L - sp.L0) * KB_BN + half * 64;
-                    uint32_t v[32];
-                    tc::tmem_ld_32x32b_x32(taddr, v);
-                    tc::tmem_ld_wait();
+                // one or two segments: levels L0..mid, ending a run flushed here, when
+                // the block crosses a run boundary; then the levels up to L1
+                int L = sp.L0;
+#pragma unroll 1
+                for (int seg = sp.mid < sp.L1 ? 0 : 1; seg < 2; seg++) {
+                    const int hi = seg == 0 ? sp.mid : sp.L1;
+                    const int run_hi = seg == 0 ? sp.mid : sp.run_hi;
+                    for (; L <= hi; L++) {
+                        const double sc = pow2(7 * (run_hi - L));
+                        const uint32_t taddr = lane_base + (uint32_t)(L - sp.L0) * KB_BN + half * 64;
+                        uint32_t v[32];
+                        tc::tmem_ld_32x32b_x32(taddr, v);
+                        tc::tmem_ld_wait();
 #pragma unroll
-                    for (int c = 0; c < 32; c++) acc[c] += (double)(int32_t)v[c] * sc;
-                    tc::tmem_ld_32x32b_x32(taddr + 32, v);
-                    tc::tmem_ld_wait();
+                        for (int c = 0; c < 32; c++) acc[c] += (double)(int32_t)v[c] * sc;
+                        tc::tmem_ld_32x32b_x32(taddr + 32, v);
+                        tc::tmem_ld_wait();
 #pragma unroll
-                    for (int c = 0; c < 32; c++) acc[32 + c] += (double)(int32_t)v[c] * sc;
-                }
-                tc::fence_before_sync();
-                tc::mbar_arrive(acc_empty);
-                if (sp.flags & 1) {  // end of a run: R += acc * 2^fexp, the exact error carried on
-                    const double fs = pow2(sp.fexp);
-                    const bool first = sp.flags & 2, last = sp.flags & 4;
-                    const double cs = last ? 0.0 : pow2(sp.cexp);
+                        for (int c = 0; c < 32; c++) acc[32 + c] += (double)(int32_t)v[c] * sc;
+                    }
+                    if (seg == 1) {
+                        tc::fence_before_sync();
+                        tc::mbar_arrive(acc_empty);
+                    }
+                    if (seg == 0 || (sp.flags & 1)) {  // end of a run: R += acc * 2^fexp, the exact error carried on
+                        const double fs = pow2(seg == 0 ? sp.fexp_mid : sp.fexp);
+                        const bool first = seg == 0 ? sp.first_mid != 0 : (sp.flags & 2) != 0;
+                        const bool last = seg == 1 && (sp.flags & 4);
+                        const double cs = last ? 0.0 : pow2(seg == 0 ? sp.cexp_mid : sp.cexp);
 #pragma unroll
-                    for (int c = 0; c < 64; c++) {
-                        const int col = half * 64 + c;
-                        double *rp = &R[(size_t)col * KB_BM + row];
-                        double r;
-                        if (first) {
-                            r = acc[c] * fs;
-                            acc[c] = 0.0;
-                        } else {
-                            const double ro = *rp;
-                            const double a = acc[c] * fs;
-                            const double sm = ro + a;
-                            const double bb = sm - ro;
-                            acc[c] = ((ro - (sm - bb)) + (a - bb)) * cs;  // TwoSum error, in the next run's units
-                            r = sm;
+                        for (int c = 0; c < 64; c++) {
+                            double *rp = &R[(size_t)(half * 64 + c) * KB_BM + row];
+                            if (first) {
+                                *rp = acc[c] * fs;
+                                acc[c] = 0.0;
+                            } else {
+                                const double ro = *rp;
+                                const double a = acc[c] * fs;
+                                const double sm = ro + a;
+                                const double bb = sm - ro;
+                                acc[c] = ((ro - (sm - bb)) + (a - bb)) * cs;  // TwoSum error, in the next run's units
+                                *rp = sm;
+                            }
                         }
-                        *rp = r;
                     }
                 }
             }

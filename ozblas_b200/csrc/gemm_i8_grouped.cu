@@ -992,24 +992,31 @@ int gemm_i8_batched(cuozblasHandle_t *h, char ta, char tb, int count, const int 
     std::vector<int> cta_begin, cta_begin_m1;
     deal_tiles(0, grid, probs, order, cost, tiles, cta_begin);
     deal_tiles(1, grid, probs, order, cost, tiles_m1, cta_begin_m1);
-    // The level-blocked form of the same problems (k_i8_blk<true>): each
-    // problem's schedule in blocks of up to four levels, over the same tiles.
-    const bool want_lw = st->env.i8_levelwise || st->env.i8_block == 0;
-    const int bw = st->env.i8_block > 0 ? st->env.i8_block : kBlkMaxWidth;
-    std::vector<BlkStep> bsteps;
-    std::vector<BlkProb> bprobs;
+    // The level-blocked form of the same problems (k_i8_blk_grouped): each
+    // problem's schedule in blocks of up to four levels, over the same tiles;
+    // form 0 cuts the blocks within the runs, form 1 across them (per problem,
+    // where the cut applies: a crossing block needs a single K chunk).
+    // OZBLAS_I8_BLOCK = w > 0 keeps form 0 at width w, w < 0 form 1 at -w.
+    const int eb = st->env.i8_block;
+    const bool want_lw = st->env.i8_levelwise || eb == 0;
+    const int bw = eb != 0 ? (eb < 0 ? -eb : eb) : kBlkMaxWidth;
+    std::vector<BlkStep> bsteps;  // both forms' step lists, one after the other
+    std::vector<BlkProb> bprobs[2];
     bool blk = !st->env.i8_levelwise && ntile_total > 0;
-    if (blk) {
-        bprobs.resize((size_t)count);
+    const bool forms[2] = {eb >= 0, eb <= 0};
+    for (int f = 0; f < 2 && blk; f++) {
+        if (!forms[f]) continue;
+        bprobs[f].resize((size_t)count);
         std::vector<BlkStep> one;
         for (int b = 0; b < count && blk; b++) {
             const GOp &oa = ops[(size_t)2 * b], &ob = ops[(size_t)2 * b + 1];
             const GProb &pr = probs[(size_t)b];
-            blk = blk_schedule(oa.S, ob.S, oa.nkb, h->fastMode != 0, bw, one);
-            bprobs[(size_t)b] = BlkProb{pr.m, pr.n, pr.ldc, pr.nkb, pr.tiles_m, pr.tiles_n, blk_kq_last(oa.k, pr.nkb),
-                                        oa.S, ob.S,
-                                        (int)bsteps.size(), (int)one.size(), pr.da, pr.db, pr.ea, pr.eb,
-                                        pr.alpha, pr.beta, pr.C};
+            blk = (f == 1 && blk_schedule(oa.S, ob.S, oa.nkb, h->fastMode != 0, bw, one, true)) ||
+                  blk_schedule(oa.S, ob.S, oa.nkb, h->fastMode != 0, bw, one);
+            bprobs[f][(size_t)b] = BlkProb{pr.m, pr.n, pr.ldc, pr.nkb, pr.tiles_m, pr.tiles_n,
+                                           blk_kq_last(oa.k, pr.nkb), oa.S, ob.S,
+                                           (int)bsteps.size(), (int)one.size(), pr.da, pr.db, pr.ea, pr.eb,
+                                           pr.alpha, pr.beta, pr.C};
             bsteps.insert(bsteps.end(), one.begin(), one.end());
         }
     }
@@ -1018,11 +1025,11 @@ int gemm_i8_batched(cuozblasHandle_t *h, char ta, char tb, int count, const int 
     int4 *d_sched = ar.take<int4>(items.size() + groups.size() + 2 * tiles.size() + 1);
     int *d_cta = ar.take<int>(2 * ((uint64_t)grid + 1));
     int *d_err = ar.take<int>(1);
-    BlkProb *d_bprobs = nullptr;
+    BlkProb *d_bprobs = nullptr;  // form 0's problems, then form 1's
     BlkStep *d_bsteps = nullptr;
     double *rbuf = nullptr;
     if (blk) {
-        d_bprobs = ar.take<BlkProb>((uint64_t)count);
+        d_bprobs = ar.take<BlkProb>((uint64_t)2 * count);
         d_bsteps = ar.take<BlkStep>(bsteps.size() + 1);
         rbuf = ar.take<double>((uint64_t)grid * G_T * G_T);
     }
@@ -1039,7 +1046,10 @@ int gemm_i8_batched(cuozblasHandle_t *h, char ta, char tb, int count, const int 
                                staged));
     }
     if (blk) {
-        OZB_CHECK(stage_upload(st, d_bprobs, bprobs.data(), sizeof(BlkProb) * count, staged));
+        for (int f = 0; f < 2; f++)
+            if (forms[f])
+                OZB_CHECK(stage_upload(st, d_bprobs + (size_t)f * count, bprobs[f].data(), sizeof(BlkProb) * count,
+                                       staged));
         OZB_CHECK(stage_upload(st, d_bsteps, bsteps.data(), sizeof(BlkStep) * bsteps.size(), staged));
     }
     OZB_CHECK(cudaMemsetAsync(d_err, 0, sizeof(int), s));
@@ -1052,16 +1062,25 @@ int gemm_i8_batched(cuozblasHandle_t *h, char ta, char tb, int count, const int 
     gp.err = d_err;
     const int4 *tiles_dev[2] = {gp.tiles, gp.tiles + tiles.size()};
     const int *cta_dev[2] = {d_cta, d_cta + grid + 1};
-    // candidates: {kernel (0 level-wise, 1 level-blocked), dealing order}
+    // candidates: {kernel (0 level-wise, 1 level-blocked within the runs, 2
+    // level-blocked across them), dealing order}
     std::vector<std::pair<int, int>> cands;
-    if (blk) cands = {{1, 0}, {1, 1}};
+    if (blk && forms[1]) {
+        cands.push_back({2, 0});
+        cands.push_back({2, 1});
+    }
+    if (blk && forms[0]) {
+        cands.push_back({1, 0});
+        cands.push_back({1, 1});
+    }
     if (lw) {
         cands.push_back({0, 0});
         cands.push_back({0, 1});
     }
     auto launch = [&](int kernel, int deal, const GProb *pl, const BlkProb *pb) -> int {
-        if (kernel == 1)
-            return i8_blk_grouped_kernel(grid, pb, d_bsteps, tiles_dev[deal], cta_dev[deal], rbuf, d_err, s) ==
+        if (kernel >= 1)
+            return i8_blk_grouped_kernel(grid, pb + (size_t)(kernel - 1) * count, d_bsteps, tiles_dev[deal],
+                                         cta_dev[deal], rbuf, d_err, s) ==
                            cudaSuccess
                        ? 0
                        : (int)CUOZBLAS_STATUS_CUDA_ERROR;
@@ -1083,33 +1102,38 @@ int gemm_i8_batched(cuozblasHandle_t *h, char ta, char tb, int count, const int 
         for (const GProb &pr : probs) outs += (size_t)(pr.m > 0 ? pr.m : 0) * (size_t)(pr.n > 0 ? pr.n : 0);
         double *scratch = ar.take<double>(outs + 1);
         GProb *d_trial = ar.take<GProb>((uint64_t)count);
-        BlkProb *d_btrial = blk ? ar.take<BlkProb>((uint64_t)count) : nullptr;
+        BlkProb *d_btrial = blk ? ar.take<BlkProb>((uint64_t)2 * count) : nullptr;
         if (ar.ok && cands.size() > 1) {
             std::vector<GProb> trial(probs);
-            std::vector<BlkProb> btrial(bprobs);
+            std::vector<BlkProb> btrial[2] = {bprobs[0], bprobs[1]};
             size_t off = 0;
             for (int b = 0; b < count; b++) {
                 GProb &pr = trial[(size_t)b];
                 pr.C = scratch + off;
                 pr.ldc = pr.m > 1 ? pr.m : 1;
                 pr.beta = 0.0;
-                if (blk) {
-                    btrial[(size_t)b].C = pr.C;
-                    btrial[(size_t)b].ldc = pr.ldc;
-                    btrial[(size_t)b].beta = 0.0;
-                }
+                for (int f = 0; f < 2; f++)
+                    if (blk && forms[f]) {
+                        btrial[f][(size_t)b].C = pr.C;
+                        btrial[f][(size_t)b].ldc = pr.ldc;
+                        btrial[f][(size_t)b].beta = 0.0;
+                    }
                 off += (size_t)(pr.m > 0 ? pr.m : 0) * (size_t)(pr.n > 0 ? pr.n : 0);
             }
             OZB_CHECK(stage_upload(st, d_trial, trial.data(), sizeof(GProb) * count, staged));
-            if (blk) OZB_CHECK(stage_upload(st, d_btrial, btrial.data(), sizeof(BlkProb) * count, staged));
+            for (int f = 0; f < 2; f++)
+                if (blk && forms[f])
+                    OZB_CHECK(stage_upload(st, d_btrial + (size_t)f * count, btrial[f].data(),
+                                           sizeof(BlkProb) * count, staged));
             uint64_t hk = tune_hash(&count, sizeof(count));
             for (const GOp &o : ops) {
                 const int sig[3] = {o.lines, o.k, o.S};
                 hk = tune_hash(sig, sizeof(sig), hk);
             }
             char key[112];
-            snprintf(key, sizeof(key), "i8grouped:%016llx:%d:%d:%d:%d", (unsigned long long)hk,
-                     h->fastMode != 0 ? 1 : 0, grid, blk ? bw : 0, lw ? 1 : 0);
+            snprintf(key, sizeof(key), "i8grouped:%016llx:%d:%d:%d:%d:%d", (unsigned long long)hk,
+                     h->fastMode != 0 ? 1 : 0, grid, blk ? bw : 0, blk ? (forms[0] ? 1 : 0) + (forms[1] ? 2 : 0) : 0,
+                     lw ? 1 : 0);
             pick = tune_pick(key, (int)cands.size(), 0, s, [&](int i) {
                 return launch(cands[(size_t)i].first, cands[(size_t)i].second, d_trial, d_btrial);
             });

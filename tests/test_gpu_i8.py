@@ -168,8 +168,8 @@ def test_i8_batched_matches_single(ta, tb, fast, split, oracle, handle, ozb, cud
 @pytest.mark.parametrize("fast", [0, 1])
 @pytest.mark.parametrize("ta,tb", [("n", "n"), ("t", "t")])
 def test_i8_batched_kernels_match_single(fast, ta, tb, oracle, handle, ozb, cuda, monkeypatch):
-    """The grouped launch's product kernel forced to the level-blocked form (widths 4, 3 and 1) and to the
-    level-wise form: every problem bit-identical to its own cuozblasDgemmI8 call in each case (a K-chunked
+    """The grouped launch's product kernel forced to the level-blocked form (widths 4, 3 and 1 within the runs of
+    levels, 4 and 3 cut across them) and to the level-wise form: every problem bit-identical to its own cuozblasDgemmI8 call in each case (a K-chunked
     problem, ragged tiles, k = 0 and an empty problem included)."""
     shapes = [(300, 200, 20000, 1.0), (129, 257, 500, 4.0), (1, 1, 1, 1.0), (64, 64, 0, 1.0), (0, 9, 9, 1.0),
               (700, 130, 128, 0.5), (33, 500, 1000, 2.0)]
@@ -183,7 +183,7 @@ def test_i8_batched_kernels_match_single(fast, ta, tb, oracle, handle, ozb, cuda
             ozb.dgemm_i8(handle, ta, tb, m, n, k, al, dev(cuda, A), lda, dev(cuda, B), ldb, be, dC, max(m, 1))
         singles.append(dC.cpu().numpy())
     for var, val in [("OZBLAS_I8_BLOCK", "4"), ("OZBLAS_I8_BLOCK", "3"), ("OZBLAS_I8_BLOCK", "1"),
-                     ("OZBLAS_I8_LEVELWISE", "1")]:
+                     ("OZBLAS_I8_BLOCK", "-4"), ("OZBLAS_I8_BLOCK", "-3"), ("OZBLAS_I8_LEVELWISE", "1")]:
         monkeypatch.setenv(var, val)
         handle.read_env()
         Cs = [dev(cuda, p[7]) for p in probs]
