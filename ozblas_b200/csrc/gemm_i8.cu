@@ -40,6 +40,7 @@
 #include <algorithm>
 
 #include "autotune.h"
+#include "gemm_i8_blk.h"
 #include "ozb_device.cuh"
 #include "ozb_internal.h"
 #include "tc05.cuh"
@@ -936,8 +937,9 @@ int gemm_i8_core(cuozblasHandle_t *h, char ta, char tb, int m, int n, int k, dou
         for (int sv : {12, 4, 8, 16, 24}) add(st->env.i8_block, sv);
     } else {
         for (int sv : {12, 4, 8, 16, 24}) add(4, sv);
-        add(-4, 12);
-        add(-3, 12);
+        std::vector<BlkStep> cut;  // the cuts across runs, where they apply (a crossing block is one K chunk)
+        for (int w : {4, 3})
+            if (blk_schedule(nA, nB, k_pad / I8_BK, h->fastMode != 0, w, cut, true)) add(-w, 12);
         add(3, 12);
         add(2, 12);
         add(0, 12);

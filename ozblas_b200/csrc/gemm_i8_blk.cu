@@ -56,9 +56,13 @@ __device__ __forceinline__ void blk_tile_coords(int tile, const BlkParams &p, in
 }
 
 
+// CROSS: the schedule has blocks that end one run and begin the next (the
+// epilogue flushes a run in the middle of a block); without them the epilogue
+// carries no code for it.
+template <bool CROSS>
 __global__ void __launch_bounds__(KB_THREADS, 1)
-    k_i8_blk(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, const __grid_constant__ BlkParams p,
-             uint64_t wait_ns, int hold_copies) {
+    k_i8_blk(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
+             const __grid_constant__ BlkParams p, uint64_t wait_ns, int hold_copies) {
     extern __shared__ uint8_t smem_raw[];
     uint8_t *smem = (uint8_t *)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
     uint8_t *ringA = smem, *ringB = smem + KB_RA * KB_TILE;
@@ -255,7 +259,7 @@ __global__ void __launch_bounds__(KB_THREADS, 1)
                     break;
                 }
                 tc::fence_after_sync();
-                if (sp.mid < sp.L1) {  // the block ends a run at mid: add its levels and flush it first
+                if (CROSS && sp.mid < sp.L1) {  // the block ends a run at mid: add its levels and flush it first
                     for (int L = sp.L0; L <= sp.mid; L++) {
                         const double sc = pow2(7 * (sp.mid - L));
                         const uint32_t taddr = lane_base + (uint32_t)(L - sp.L0) * KB_BN + half * 64;
@@ -287,7 +291,7 @@ __global__ void __launch_bounds__(KB_THREADS, 1)
                         }
                     }
                 }
-                for (int L = sp.mid < sp.L1 ? sp.mid + 1 : sp.L0; L <= sp.L1; L++) {
+                for (int L = (CROSS && sp.mid < sp.L1) ? sp.mid + 1 : sp.L0; L <= sp.L1; L++) {
                     const double sc = pow2(7 * (sp.run_hi - L));
                     const uint32_t taddr = lane_base + (uint32_t)(L - sp.L0) * KB_BN + half * 64;
                     uint32_t v[32];
@@ -438,7 +442,7 @@ bool blk_schedule(int nA, int nB, int nkb, bool triangular, int W, std::vector<B
     return (steps.back().flags & 1) != 0;
 }
 
-static std::atomic<uint64_t> g_blk_attr{0};
+static std::atomic<uint64_t> g_blk_attr{0}, g_blk_attr_cross{0};
 
 int blk_kq_last(int k, int nkb) {
     const int tail = k - (nkb - 1) * KB_BK;
@@ -489,9 +493,17 @@ int i8_blk_launch(cuozblasHandle_t *h, const CUtensorMap &tmA, const CUtensorMap
     p.C = C;
     p.rbuf = rbuf;
     p.err = d_err;
-    OZB_CHECK(smem_optin((const void *)k_i8_blk, KB_SMEM, g_blk_attr));
+    bool cross = false;
+    for (const BlkStep &sp : steps) cross = cross || sp.mid < sp.L1;
+    OZB_CHECK(smem_optin(cross ? (const void *)k_i8_blk<true> : (const void *)k_i8_blk<false>, KB_SMEM,
+                         cross ? g_blk_attr_cross : g_blk_attr));
     counted(h);
-    k_i8_blk<<<grid, KB_THREADS, KB_SMEM, st->stream>>>(tmA, tmB, p, i8_test_wait_ns(), i8_test_hold_copies());
+    if (cross)
+        k_i8_blk<true><<<grid, KB_THREADS, KB_SMEM, st->stream>>>(tmA, tmB, p, i8_test_wait_ns(),
+                                                                   i8_test_hold_copies());
+    else
+        k_i8_blk<false><<<grid, KB_THREADS, KB_SMEM, st->stream>>>(tmA, tmB, p, i8_test_wait_ns(),
+                                                                    i8_test_hold_copies());
     OZB_CHECK(cudaGetLastError());
     return CUOZBLAS_STATUS_SUCCESS;
 }
