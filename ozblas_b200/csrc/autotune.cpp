@@ -69,17 +69,33 @@ int tune_pick(const std::string &key, int ncand, int dflt, cudaStream_t stream, 
         if (e0) cudaEventDestroy(e0);
         return dflt;
     }
-    // Every candidate is timed once per round, in candidate order; a second
-    // round follows when the fastest first-round time is short (below 200 ms),
-    // and each candidate keeps its faster time, so a clock or power dip during
-    // one run does not decide the pick.
+    // Warm-up: the default runs until about 200 ms of work has passed (at most
+    // 8 runs), so the timed runs start near the clock the power cap settles at.
+    // Then every candidate is timed once per round: a second round in the
+    // reverse order follows when the fastest first-round time is below 200 ms,
+    // and a candidate's score is the sum of its rounds, so a clock that drifts
+    // during the measurement favours no position in the order.
     int best = dflt;
     float best_ms = 0.f;
     std::vector<float> t((size_t)ncand, 0.f);
-    bool ok = run(dflt) == 0;  // warm-up: first-touch costs land outside the timed runs
+    bool ok = true;
+    for (int w = 0; w < 8 && ok; w++) {
+        cudaEventRecord(e0, stream);
+        ok = run(dflt) == 0;
+        cudaEventRecord(e1, stream);
+        float ms = 0.f;
+        if (!ok || cudaEventSynchronize(e1) != cudaSuccess || cudaEventElapsedTime(&ms, e0, e1) != cudaSuccess) {
+            ok = false;
+            break;
+        }
+        best_ms += ms;
+        if (best_ms >= 200.f) break;
+    }
+    int rounds = 0;
     for (int round = 0; round < 2 && ok; round++) {
         if (round == 1 && best_ms >= 200.f) break;
-        for (int i = 0; i < ncand && ok; i++) {
+        for (int j = 0; j < ncand && ok; j++) {
+            const int i = round == 0 ? j : ncand - 1 - j;
             cudaEventRecord(e0, stream);
             if (run(i) != 0) {
                 ok = false;
@@ -92,12 +108,13 @@ int tune_pick(const std::string &key, int ncand, int dflt, cudaStream_t stream, 
             }
             float ms = 0.f;
             cudaEventElapsedTime(&ms, e0, e1);
-            if (round == 0 || ms < t[(size_t)i]) t[(size_t)i] = ms;
+            t[(size_t)i] += ms;
         }
+        rounds++;
         best = 0;
         for (int i = 1; i < ncand; i++)
             if (t[(size_t)i] < t[(size_t)best]) best = i;
-        best_ms = t[(size_t)best];
+        best_ms = t[(size_t)best] / rounds;
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);

@@ -21,10 +21,10 @@ namespace ozb {
 
 // Returns the chosen candidate index in [0, ncand).  `run(i)` launches
 // candidate i on `stream` and returns a cuozblas status; on the first use of
-// `key` every candidate runs once per round (after one untimed run of the
-// default), timed with CUDA events, in two rounds when the fastest time is
-// below 200 ms; each candidate keeps its faster time.  When measurement is off
-// or fails, `dflt`.
+// `key` the default runs untimed for about 200 ms of work, then every
+// candidate runs once per round, timed with CUDA events, in two rounds (the
+// second in reverse order, scores summed) when the fastest time is below
+// 200 ms.  When measurement is off or fails, `dflt`.
 int tune_pick(const std::string &key, int ncand, int dflt, cudaStream_t stream, const std::function<int(int)> &run);
 
 // 64-bit FNV-1a over a byte range (shape signatures).

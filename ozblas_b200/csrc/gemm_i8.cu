@@ -915,8 +915,8 @@ int gemm_i8_core(cuozblasHandle_t *h, char ta, char tb, int m, int n, int k, dou
     // Launch shape, measured once per shape (every choice gives the same bits;
     // candidates write a scratch product with beta = 0): the product kernel
     // (level-blocked or level-wise), the block width of the level-blocked
-    // schedule (levels accumulated together: 4, 3 or 2 within the runs, or
-    // equal cuts of at most 4 or 3 levels across them) and the rasterisation
+    // schedule (levels accumulated together: 4 or 3 within the runs, or equal
+    // cuts of at most 4 levels across them) and the rasterisation
     // strip height.  OZBLAS_I8_LEVELWISE keeps the level-wise kernel (strip
     // tuned), OZBLAS_I8_BLOCK=w the level-blocked kernel at width w (negative:
     // the cuts across runs).
@@ -937,11 +937,12 @@ int gemm_i8_core(cuozblasHandle_t *h, char ta, char tb, int m, int n, int k, dou
         for (int sv : {12, 4, 8, 16, 24}) add(st->env.i8_block, sv);
     } else {
         for (int sv : {12, 4, 8, 16, 24}) add(4, sv);
-        std::vector<BlkStep> cut;  // the cuts across runs, where they apply (a crossing block is one K chunk)
-        for (int w : {4, 3})
-            if (blk_schedule(nA, nB, k_pad / I8_BK, h->fastMode != 0, w, cut, true)) add(-w, 12);
+        // the cut across runs where it applies (a crossing block is one K chunk);
+        // narrower blocks measured slower on every bench shape and only add
+        // chances for timing noise to pick them (OZBLAS_I8_BLOCK still forces them)
+        std::vector<BlkStep> cut;
+        if (blk_schedule(nA, nB, k_pad / I8_BK, h->fastMode != 0, 4, cut, true)) add(-4, 12);
         add(3, 12);
-        add(2, 12);
         add(0, 12);
     }
     auto launch = [&](const Shape &c, I8Params &pp) {
