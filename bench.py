@@ -41,6 +41,7 @@ import os
 import statistics
 import subprocess
 import sys
+import tempfile
 import time
 
 ROOT = os.path.dirname(os.path.abspath(__file__))
@@ -93,7 +94,9 @@ class ClockSampler:
     def __init__(self, gpu_index):
         self.gpu = gpu_index
         self.proc = None
-        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_gpu{gpu_index}.csv")
+        # the raw samples: $OZBLAS_CLOCKS_DIR when set, else the system's temporary directory
+        out_dir = os.environ.get("OZBLAS_CLOCKS_DIR") or tempfile.gettempdir()
+        self.path = os.path.join(out_dir, f"clocks_gpu{gpu_index}.csv")
 
     def __enter__(self):
         os.makedirs(os.path.dirname(self.path), exist_ok=True)
@@ -598,7 +601,7 @@ def extras(ozb, h, torch, A, B, C, n, ms_headline, cpu=True, sizes=(), phis=()):
     out["int8_full_pairs"] = {"TFLOPS": flops / ms_full / 1e9, "pairs": h.nSplitC, "ms": ms_full}
     C_full = C.clone()
     h.nSplitMax = 0
-    # the plain form as the north star defines it: FP64 slices on the FP64 tensor pipe (DMMA)
+    # the plain form as the reference computes it: FP64 slices, here on the FP64 tensor pipe (DMMA)
     os.environ["OZBLAS_PLAIN_DMMA"] = "1"
     h.read_env()
     try:
