@@ -56,6 +56,15 @@ uint64_t tune_hash(const void *data, size_t bytes, uint64_t h) {
     return h;
 }
 
+int tune_cached(const std::string &key, int ncand, int dflt) {
+    if (ncand <= 1 || !tuning_enabled()) return dflt;
+    std::lock_guard<std::mutex> lock(g_mu);
+    load_file_locked();
+    auto it = g_cache.find(key);
+    if (it != g_cache.end() && it->second >= 0 && it->second < ncand) return it->second;
+    return -1;
+}
+
 int tune_pick(const std::string &key, int ncand, int dflt, cudaStream_t stream, const std::function<int(int)> &run) {
     if (ncand <= 1 || !tuning_enabled()) return dflt;
     {

@@ -27,6 +27,11 @@ namespace ozb {
 // 200 ms.  When measurement is off or fails, `dflt`.
 int tune_pick(const std::string &key, int ncand, int dflt, cudaStream_t stream, const std::function<int(int)> &run);
 
+// The choice tune_pick would return without measuring: the cached candidate
+// for `key`, `dflt` when measurement is off or ncand <= 1, or -1 when `key`
+// has not been measured yet.
+int tune_cached(const std::string &key, int ncand, int dflt);
+
 // 64-bit FNV-1a over a byte range (shape signatures).
 uint64_t tune_hash(const void *data, size_t bytes, uint64_t h = 1469598103934665603ULL);
 

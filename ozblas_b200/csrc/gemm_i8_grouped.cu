@@ -939,15 +939,110 @@ int gemm_i8_batched(cuozblasHandle_t *h, char ta, char tb, int count, const int 
         OZB_CHECK(cudaGetLastError());
     }
     ev_record(h, 1);
-    // schedules, problems and the tile deal
-    std::vector<int4> items, groups, tiles;
+    // This runs on the host while the split is still cutting digits, so it
+    // builds only what the launch needs: once the product kernel and dealing
+    // order of this problem set are measured, only that kernel's schedules and
+    // that dealing order.
+    const bool tri = h->fastMode != 0;
     std::vector<GProb> probs((size_t)count);
     std::vector<double> cost((size_t)count, 0.0);
     int npairs_max = 0;
     {
-        // every problem's schedule written in place (no per-problem vectors):
-        // a pair spans at most nkb / (k-blocks per INT32 group) + 2 items, a
-        // group holds at least one item
+        // per problem: its pairs and a tile cost for the deal (k-blocks over all
+        // pairs plus two per INT32 group of the level-wise schedule, whose
+        // groups fill G_MAX_TERMS / 128 k-blocks within one level)
+        const int64_t kb_cap = G_MAX_TERMS / G_T;
+        for (int b = 0; b < count; b++) {
+            const GOp &oa = ops[(size_t)2 * b], &ob = ops[(size_t)2 * b + 1];
+            const int nA = oa.S, nB = ob.S, nkb = oa.nkb;
+            const int maxlevel = tri ? (nA < nB ? nA : nB) - 1 : nA + nB - 2;
+            int64_t np = 0, ng = 0;
+            for (int L = 0; L <= maxlevel; L++) {
+                const int lo = L - (nB - 1) > 0 ? L - (nB - 1) : 0, hi = L < nA - 1 ? L : nA - 1;
+                np += hi - lo + 1;
+                ng += ((int64_t)(hi - lo + 1) * nkb + kb_cap - 1) / kb_cap;
+            }
+            npairs_max = np > npairs_max ? (int)np : npairs_max;
+            cost[(size_t)b] = (double)np * nkb + 2.0 * (double)ng;
+            probs[(size_t)b] = GProb{m[b], n[b], ldc[b], nkb, oa.tiles_l, ob.tiles_l, 0, 0,
+                                     oa.digits, ob.digits, oa.e, ob.e, alpha[b], beta[b], C[b]};
+        }
+    }
+    std::vector<int> order((size_t)count);
+    for (int b = 0; b < count; b++) order[(size_t)b] = b;
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return cost[(size_t)a] > cost[(size_t)b]; });
+    const int nsm = sm_count();
+    int ntile_total = 0;
+    for (int b = 0; b < count; b++)
+        if (m[b] > 0 && n[b] > 0) ntile_total += probs[(size_t)b].tiles_m * probs[(size_t)b].tiles_n;
+    const int grid = ntile_total < nsm ? (ntile_total > 0 ? ntile_total : 1) : nsm;
+    // Candidates {kernel, dealing order}: kernel 2 level-blocked with blocks cut
+    // across the runs (per problem, where the cut applies: a crossing block
+    // needs a single K chunk), 1 level-blocked within the runs, 0 level-wise.
+    // OZBLAS_I8_BLOCK = w > 0 keeps kernel 1 at width w, w < 0 kernel 2 at -w;
+    // OZBLAS_I8_LEVELWISE kernel 0.
+    const int eb = st->env.i8_block;
+    const bool want_lw = st->env.i8_levelwise || eb == 0;
+    const int bw = eb != 0 ? (eb < 0 ? -eb : eb) : kBlkMaxWidth;
+    const bool blk_on = !st->env.i8_levelwise && ntile_total > 0;
+    const bool forms[2] = {blk_on && eb >= 0, blk_on && eb <= 0};
+    std::vector<std::pair<int, int>> cands;
+    for (int f = 1; f >= 0; f--)
+        if (forms[f]) {
+            cands.push_back({f + 1, 0});
+            cands.push_back({f + 1, 1});
+        }
+    if (want_lw || cands.empty()) {
+        cands.push_back({0, 0});
+        cands.push_back({0, 1});
+    }
+    uint64_t hk = tune_hash(&count, sizeof(count));
+    for (const GOp &o : ops) {
+        const int sig[3] = {o.lines, o.k, o.S};
+        hk = tune_hash(sig, sizeof(sig), hk);
+    }
+    char key[112];
+    snprintf(key, sizeof(key), "i8grouped:%016llx:%d:%d:%d:%d:%d", (unsigned long long)hk, tri ? 1 : 0, grid, bw,
+             (forms[0] ? 1 : 0) + (forms[1] ? 2 : 0), want_lw ? 1 : 0);
+    int pick = ntile_total > 0 ? tune_cached(key, (int)cands.size(), 0) : 0;  // -1: not measured yet
+    auto needed = [&](int kernel, int deal) {
+        if (pick >= 0) return cands[(size_t)pick].first == kernel && (deal < 0 || cands[(size_t)pick].second == deal);
+        for (const auto &c : cands)
+            if (c.first == kernel && (deal < 0 || c.second == deal)) return true;
+        return false;
+    };
+    // the level-blocked schedules of the forms needed
+    std::vector<BlkStep> bsteps;  // the forms' step lists, one after the other
+    std::vector<BlkProb> bprobs[2];
+    bool blk_failed = false;
+    for (int f = 0; f < 2 && !blk_failed; f++) {
+        if (!forms[f] || !needed(f + 1, -1)) continue;
+        bprobs[f].resize((size_t)count);
+        std::vector<BlkStep> one;
+        for (int b = 0; b < count && !blk_failed; b++) {
+            const GOp &oa = ops[(size_t)2 * b], &ob = ops[(size_t)2 * b + 1];
+            const GProb &pr = probs[(size_t)b];
+            blk_failed = !((f == 1 && blk_schedule(oa.S, ob.S, oa.nkb, tri, bw, one, true)) ||
+                           blk_schedule(oa.S, ob.S, oa.nkb, tri, bw, one));
+            bprobs[f][(size_t)b] = BlkProb{pr.m, pr.n, pr.ldc, pr.nkb, pr.tiles_m, pr.tiles_n,
+                                           blk_kq_last(oa.k, pr.nkb), oa.S, ob.S,
+                                           (int)bsteps.size(), (int)one.size(), pr.da, pr.db, pr.ea, pr.eb,
+                                           pr.alpha, pr.beta, pr.C};
+            bsteps.insert(bsteps.end(), one.begin(), one.end());
+        }
+    }
+    if (blk_failed) {  // levels beyond the level-blocked kernel's range: the level-wise kernel, measured
+        cands = {{0, 0}, {0, 1}};
+        pick = -1;
+        bsteps.clear();
+        bprobs[0].clear();
+        bprobs[1].clear();
+    }
+    const bool blk = !bsteps.empty();
+    // the level-wise schedules, written in place: a pair spans at most
+    // nkb / (k-blocks per INT32 group) + 2 items, a group holds at least one item
+    std::vector<int4> items, groups;
+    if (needed(0, -1)) {
         size_t cap_items = 0;
         for (int b = 0; b < count; b++) {
             const GOp &oa = ops[(size_t)2 * b], &ob = ops[(size_t)2 * b + 1];
@@ -960,69 +1055,32 @@ int gemm_i8_batched(cuozblasHandle_t *h, char ta, char tb, int count, const int 
             const GOp &oa = ops[(size_t)2 * b], &ob = ops[(size_t)2 * b + 1];
             const size_t cap_b = (size_t)oa.S * ob.S * (size_t)(oa.nkb / (G_MAX_TERMS / G_T) + 2);
             int ni = 0, ng = 0;
-            const int np = i8_schedule_into(oa.S, ob.S, oa.nkb, h->fastMode != 0, items.data() + ni_tot, (int)cap_b,
-                                            &ni, groups.data() + ng_tot, (int)cap_b, &ng);
+            const int np = i8_schedule_into(oa.S, ob.S, oa.nkb, tri, items.data() + ni_tot, (int)cap_b, &ni,
+                                            groups.data() + ng_tot, (int)cap_b, &ng);
             if (np < 0) return CUOZBLAS_STATUS_NOT_SUPPORTED;
-            npairs_max = np > npairs_max ? np : npairs_max;
-            double kbs = 0.0;
-            for (int i = 0; i < ni; i++) kbs += items[ni_tot + (size_t)i].w - items[ni_tot + (size_t)i].z;
             for (int g = 0; g < ng; g++) {
                 groups[ng_tot + (size_t)g].x += (int)ni_tot;
                 groups[ng_tot + (size_t)g].y += (int)ni_tot;
             }
-            cost[(size_t)b] = kbs + 2.0 * ng;
-            GProb &pr = probs[(size_t)b];
-            pr = GProb{m[b], n[b], ldc[b], oa.nkb, oa.tiles_l, ob.tiles_l, (int)ng_tot, ng,
-                       oa.digits, ob.digits, oa.e, ob.e, alpha[b], beta[b], C[b]};
+            probs[(size_t)b].group0 = (int)ng_tot;
+            probs[(size_t)b].n_groups = ng;
             ni_tot += (size_t)ni;
             ng_tot += (size_t)ng;
         }
         items.resize(ni_tot);
         groups.resize(ng_tot);
     }
-    std::vector<int> order((size_t)count);
-    for (int b = 0; b < count; b++) order[(size_t)b] = b;
-    std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return cost[(size_t)a] > cost[(size_t)b]; });
-    const int nsm = sm_count();
-    int ntile_total = 0;
-    for (int b = 0; b < count; b++)
-        if (m[b] > 0 && n[b] > 0) ntile_total += probs[(size_t)b].tiles_m * probs[(size_t)b].tiles_n;
-    const int grid = ntile_total < nsm ? (ntile_total > 0 ? ntile_total : 1) : nsm;
-    std::vector<int4> tiles_m1;
-    std::vector<int> cta_begin, cta_begin_m1;
-    deal_tiles(0, grid, probs, order, cost, tiles, cta_begin);
-    deal_tiles(1, grid, probs, order, cost, tiles_m1, cta_begin_m1);
-    // The level-blocked form of the same problems (k_i8_blk_grouped): each
-    // problem's schedule in blocks of up to four levels, over the same tiles;
-    // form 0 cuts the blocks within the runs, form 1 across them (per problem,
-    // where the cut applies: a crossing block needs a single K chunk).
-    // OZBLAS_I8_BLOCK = w > 0 keeps form 0 at width w, w < 0 form 1 at -w.
-    const int eb = st->env.i8_block;
-    const bool want_lw = st->env.i8_levelwise || eb == 0;
-    const int bw = eb != 0 ? (eb < 0 ? -eb : eb) : kBlkMaxWidth;
-    std::vector<BlkStep> bsteps;  // both forms' step lists, one after the other
-    std::vector<BlkProb> bprobs[2];
-    bool blk = !st->env.i8_levelwise && ntile_total > 0;
-    const bool forms[2] = {eb >= 0, eb <= 0};
-    for (int f = 0; f < 2 && blk; f++) {
-        if (!forms[f]) continue;
-        bprobs[f].resize((size_t)count);
-        std::vector<BlkStep> one;
-        for (int b = 0; b < count && blk; b++) {
-            const GOp &oa = ops[(size_t)2 * b], &ob = ops[(size_t)2 * b + 1];
-            const GProb &pr = probs[(size_t)b];
-            blk = (f == 1 && blk_schedule(oa.S, ob.S, oa.nkb, h->fastMode != 0, bw, one, true)) ||
-                  blk_schedule(oa.S, ob.S, oa.nkb, h->fastMode != 0, bw, one);
-            bprobs[f][(size_t)b] = BlkProb{pr.m, pr.n, pr.ldc, pr.nkb, pr.tiles_m, pr.tiles_n,
-                                           blk_kq_last(oa.k, pr.nkb), oa.S, ob.S,
-                                           (int)bsteps.size(), (int)one.size(), pr.da, pr.db, pr.ea, pr.eb,
-                                           pr.alpha, pr.beta, pr.C};
-            bsteps.insert(bsteps.end(), one.begin(), one.end());
-        }
+    // the tile deals needed
+    std::vector<int4> tiles[2];
+    std::vector<int> cta_begin[2];
+    for (int d = 0; d < 2; d++) {
+        bool use = false;
+        for (int kernel = 0; kernel < 3; kernel++) use = use || needed(kernel, d);
+        if (use) deal_tiles(d, grid, probs, order, cost, tiles[d], cta_begin[d]);
+        cta_begin[d].resize((size_t)grid + 1, 0);
     }
-    const bool lw = want_lw || !blk;
     GProb *d_probs = ar.take<GProb>((uint64_t)count);
-    int4 *d_sched = ar.take<int4>(items.size() + groups.size() + 2 * tiles.size() + 1);
+    int4 *d_sched = ar.take<int4>(items.size() + groups.size() + tiles[0].size() + tiles[1].size() + 1);
     int *d_cta = ar.take<int>(2 * ((uint64_t)grid + 1));
     int *d_err = ar.take<int>(1);
     BlkProb *d_bprobs = nullptr;  // form 0's problems, then form 1's
@@ -1037,17 +1095,17 @@ int gemm_i8_batched(cuozblasHandle_t *h, char ta, char tb, int count, const int 
     OZB_CHECK(stage_upload(st, d_probs, probs.data(), sizeof(GProb) * count, staged));
     {  // items, groups, both tile lists and both CTA ranges, one after the other
         int4 *dst = d_sched;
-        for (const std::vector<int4> *v : {&items, &groups, &tiles, &tiles_m1}) {
+        for (const std::vector<int4> *v : {&items, &groups, &tiles[0], &tiles[1]}) {
             OZB_CHECK(stage_upload(st, dst, v->data(), sizeof(int4) * v->size(), staged));
             dst += v->size();
         }
-        OZB_CHECK(stage_upload(st, d_cta, cta_begin.data(), sizeof(int) * cta_begin.size(), staged));
-        OZB_CHECK(stage_upload(st, d_cta + cta_begin.size(), cta_begin_m1.data(), sizeof(int) * cta_begin_m1.size(),
-                               staged));
+        for (int d = 0; d < 2; d++)
+            OZB_CHECK(stage_upload(st, d_cta + (size_t)d * (grid + 1), cta_begin[d].data(),
+                                   sizeof(int) * cta_begin[d].size(), staged));
     }
     if (blk) {
         for (int f = 0; f < 2; f++)
-            if (forms[f])
+            if (!bprobs[f].empty())
                 OZB_CHECK(stage_upload(st, d_bprobs + (size_t)f * count, bprobs[f].data(), sizeof(BlkProb) * count,
                                        staged));
         OZB_CHECK(stage_upload(st, d_bsteps, bsteps.data(), sizeof(BlkStep) * bsteps.size(), staged));
@@ -1060,23 +1118,8 @@ int gemm_i8_batched(cuozblasHandle_t *h, char ta, char tb, int count, const int 
     gp.tiles = d_sched + items.size() + groups.size();
     gp.cta_begin = d_cta;
     gp.err = d_err;
-    const int4 *tiles_dev[2] = {gp.tiles, gp.tiles + tiles.size()};
+    const int4 *tiles_dev[2] = {gp.tiles, gp.tiles + tiles[0].size()};
     const int *cta_dev[2] = {d_cta, d_cta + grid + 1};
-    // candidates: {kernel (0 level-wise, 1 level-blocked within the runs, 2
-    // level-blocked across them), dealing order}
-    std::vector<std::pair<int, int>> cands;
-    if (blk && forms[1]) {
-        cands.push_back({2, 0});
-        cands.push_back({2, 1});
-    }
-    if (blk && forms[0]) {
-        cands.push_back({1, 0});
-        cands.push_back({1, 1});
-    }
-    if (lw) {
-        cands.push_back({0, 0});
-        cands.push_back({0, 1});
-    }
     auto launch = [&](int kernel, int deal, const GProb *pl, const BlkProb *pb) -> int {
         if (kernel >= 1)
             return i8_blk_grouped_kernel(grid, pb + (size_t)(kernel - 1) * count, d_bsteps, tiles_dev[deal],
@@ -1091,12 +1134,14 @@ int gemm_i8_batched(cuozblasHandle_t *h, char ta, char tb, int count, const int 
         k_i8_grouped<<<grid, G_THREADS, G_SMEM, s>>>(gt);
         return cudaGetLastError() == cudaSuccess ? 0 : (int)CUOZBLAS_STATUS_CUDA_ERROR;
     };
-    int pick = 0;
     if (ntile_total > 0) {
         static std::atomic<uint64_t> attr{0};  // devices already opted in
         OZB_CHECK(smem_optin((const void *)k_i8_grouped, G_SMEM, attr));
+    }
+    if (ntile_total > 0 && pick < 0) {
         // kernel and dealing order: same bits either way, the fastest is measured
         // once per problem set (candidates write scratch products with beta = 0)
+        pick = 0;
         const uint64_t mk = ar.mark();
         size_t outs = 0;
         for (const GProb &pr : probs) outs += (size_t)(pr.m > 0 ? pr.m : 0) * (size_t)(pr.n > 0 ? pr.n : 0);
@@ -1113,7 +1158,7 @@ int gemm_i8_batched(cuozblasHandle_t *h, char ta, char tb, int count, const int 
                 pr.ldc = pr.m > 1 ? pr.m : 1;
                 pr.beta = 0.0;
                 for (int f = 0; f < 2; f++)
-                    if (blk && forms[f]) {
+                    if (!btrial[f].empty()) {
                         btrial[f][(size_t)b].C = pr.C;
                         btrial[f][(size_t)b].ldc = pr.ldc;
                         btrial[f][(size_t)b].beta = 0.0;
@@ -1122,18 +1167,9 @@ int gemm_i8_batched(cuozblasHandle_t *h, char ta, char tb, int count, const int 
             }
             OZB_CHECK(stage_upload(st, d_trial, trial.data(), sizeof(GProb) * count, staged));
             for (int f = 0; f < 2; f++)
-                if (blk && forms[f])
+                if (!btrial[f].empty())
                     OZB_CHECK(stage_upload(st, d_btrial + (size_t)f * count, btrial[f].data(),
                                            sizeof(BlkProb) * count, staged));
-            uint64_t hk = tune_hash(&count, sizeof(count));
-            for (const GOp &o : ops) {
-                const int sig[3] = {o.lines, o.k, o.S};
-                hk = tune_hash(sig, sizeof(sig), hk);
-            }
-            char key[112];
-            snprintf(key, sizeof(key), "i8grouped:%016llx:%d:%d:%d:%d:%d", (unsigned long long)hk,
-                     h->fastMode != 0 ? 1 : 0, grid, blk ? bw : 0, blk ? (forms[0] ? 1 : 0) + (forms[1] ? 2 : 0) : 0,
-                     lw ? 1 : 0);
             pick = tune_pick(key, (int)cands.size(), 0, s, [&](int i) {
                 return launch(cands[(size_t)i].first, cands[(size_t)i].second, d_trial, d_btrial);
             });
@@ -1141,6 +1177,7 @@ int gemm_i8_batched(cuozblasHandle_t *h, char ta, char tb, int count, const int 
         ar.ok = true;
         ar.release(mk);
     }
+    if (pick < 0) pick = 0;
     h->nSplitA = (float)maxA;
     h->nSplitB = (float)maxB;
     h->nSplitC = (float)npairs_max;
