@@ -21,7 +21,11 @@
 //    the batch's small problems have k tails of every length;
 //  * at the end of a tile the epilogue scales R into C in a pass of its own,
 //    so the problem's output fields are not held in registers across the
-//    steps (with them held, the epilogue warps spilled).
+//    steps (with them held, the epilogue warps spilled);
+//  * a problem's schedule may cut its blocks across the runs of levels (as
+//    k_i8_blk<true> does): the epilogue then walks a block in one or two
+//    segments, flushing the run that ends inside the block before it reads
+//    the levels above.
 #include <cuda.h>
 
 #include <atomic>
