@@ -456,14 +456,19 @@ int i8_test_hold_copies();
 // The level-blocked product kernel over digit operands laid out as for
 // k_i8_gemm (tensor maps over [S * lines_pad][k_pad], 128 x 128-byte boxes).
 // `width`: levels per block (1..4, within the runs; -4..-1: equal cuts of at
-// most -width levels across the runs; every width gives the same bits).
+// most -width levels across the runs, or blocks of -width levels within the
+// runs where the cut does not apply; every width gives the same bits).
 // Returns NOT_SUPPORTED (nothing launched) when the schedule does not apply.
 int i8_blk_launch(cuozblasHandle_t *h, const CUtensorMap &tmA, const CUtensorMap &tmB, int m, int n, int m_pad,
                   int n_pad, int k_pad, int nA, int nB, bool triangular, const int *ea, const int *eb, double alpha,
                   double beta, double *C, int ldc, int strip, int width, int *d_err, Arena &ar) {
     State *st = state(h);
     std::vector<BlkStep> steps;
-    if (!blk_schedule(nA, nB, k_pad / KB_BK, triangular, width < 0 ? -width : width, steps, width < 0))
+    const int w = width < 0 ? -width : width;
+    // a cut across the runs that does not apply (a crossing block would need
+    // several K chunks) falls back to blocks within the runs
+    if (!blk_schedule(nA, nB, k_pad / KB_BK, triangular, w, steps, width < 0) &&
+        !(width < 0 && blk_schedule(nA, nB, k_pad / KB_BK, triangular, w, steps, false)))
         return CUOZBLAS_STATUS_NOT_SUPPORTED;
     const int nsm = sm_count();
     const int tiles_m = m_pad / KB_BM, tiles_n = n_pad / KB_BN, ntiles = tiles_m * tiles_n;
