@@ -293,6 +293,16 @@ double cuozblasRuleScale2(double v, int32_t e);
  * (int) rho, tau at b (out: remainder, then the slice as a double),
  * 5 (double)*a * 2^(int)*b.  Values are 16-byte IEEE binary128. */
 int cuozblasRuleQ128(int op, const void *a, const void *b, const void *c, void *out);
+/* The INT8 form's level-blocked schedule, on the host (the steps the product
+ * kernels run): digit counts nA, nB, nkb 128-wide K steps, the triangular or
+ * full pair set, `width` levels per block within the runs of levels (1-4) or,
+ * negative, equal cuts of at most -width levels across them.  Writes 12 int32
+ * per step (L0, L1, kb0, kb1, run_hi, flags, fexp, cexp, mid, fexp_mid,
+ * cexp_mid, first_mid) into out and returns the number of steps; -1 when the
+ * schedule does not apply (for a cut across runs: a crossing block would need
+ * several K chunks), -2 when max_steps is too small. */
+int cuozblasRuleI8Schedule(int32_t nA, int32_t nB, int32_t nkb, int32_t triangular, int32_t width, int32_t *out,
+                           int32_t max_steps);
 int cuozblasRuleRho(int32_t dim, int32_t splitEpsMode);
 /* Certified fast path of the correctly rounded sum (the NearSum result when it
  * returns 1; 0: not proven, the library then runs NearSum itself). */

@@ -123,7 +123,7 @@ C_ABI_SYMBOLS = [
     "cuozblasDaxpy", "cuozblasDgemv", "cuozblasDgemm", "cuozblasDcsrmv", "cuozblasDcsrmvSplitA", "cuozblasDcg",
     "cuozblasDgemmI8", "cuozblasDgemmI8Static", "cuozblasDgemmI8Batched", "cuozblasRuleTau", "cuozblasRuleRho",
     "cuozblasRuleCrSum", "cuozblasDSgemm", "cuozblasDSgemv", "cuozblasDSdot", "cuozblasDSnrm2",
-    "cuozblasRuleTauF32", "cuozblasRuleQ128", "cuozblasRuleScale2", "cuozblasQgemm", "cuozblasQgemv", "cuozblasQdot", "cuozblasQnrm2",
+    "cuozblasRuleTauF32", "cuozblasRuleQ128", "cuozblasRuleScale2", "cuozblasRuleI8Schedule", "cuozblasQgemm", "cuozblasQgemv", "cuozblasQdot", "cuozblasQnrm2",
     "cuozblasSDgemm", "cuozblasSDgemv", "cuozblasSDdot", "cuozblasSDnrm2",
     "cuozblasVersion",
 ]

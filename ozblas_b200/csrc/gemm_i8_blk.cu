@@ -514,3 +514,18 @@ int i8_blk_launch(cuozblasHandle_t *h, const CUtensorMap &tmA, const CUtensorMap
 }
 
 }  // namespace ozb
+
+extern "C" int cuozblasRuleI8Schedule(int32_t nA, int32_t nB, int32_t nkb, int32_t triangular, int32_t width,
+                                      int32_t *out, int32_t max_steps) {
+    if (width == 0 || width < -ozb::KB_W || width > ozb::KB_W || nA < 1 || nB < 1 || nkb < 1 || !out) return -1;
+    std::vector<ozb::BlkStep> steps;
+    if (!ozb::blk_schedule(nA, nB, nkb, triangular != 0, width < 0 ? -width : width, steps, width < 0)) return -1;
+    if ((int64_t)steps.size() > max_steps) return -2;
+    for (size_t i = 0; i < steps.size(); i++) {
+        const ozb::BlkStep &s = steps[i];
+        const int32_t v[12] = {s.L0, s.L1, s.kb0, s.kb1, s.run_hi, s.flags, s.fexp, s.cexp,
+                               s.mid, s.fexp_mid, s.cexp_mid, s.first_mid};
+        for (int j = 0; j < 12; j++) out[12 * i + j] = v[j];
+    }
+    return (int)steps.size();
+}
