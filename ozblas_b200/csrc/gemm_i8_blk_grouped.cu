@@ -29,7 +29,6 @@
 #include <cuda.h>
 
 #include <atomic>
-#include <cstring>
 
 #include "gemm_i8_blk.h"
 #include "ozb_device.cuh"
